@@ -1,0 +1,137 @@
+/*
+ * voronoid_b200.h -- C ABI of the B200 tessellation library.
+ *
+ * A GPU-backed drop-in for the reference crate `voronoid`'s 3D path:
+ * Tessellation<3, Cell3DFaces, Algorithm3DGrid> with plane and sphere walls.
+ * Every entry point below names the reference interface it replaces
+ * (file:line within the reference crate).  Plain pointers and sizes only; no
+ * framework types cross this boundary.
+ *
+ * Conventions
+ *  - Every call returns an int status (VD_OK on success); the message of the
+ *    last failure on a handle is available from vd_last_error().
+ *  - A handle owns its device buffers and one CUDA stream.  A handle is not
+ *    thread-safe (the reference's calculate takes &mut self); distinct
+ *    handles may be used from different threads concurrently.
+ *  - Host output buffers are owned by the caller and sized by query calls.
+ *  - There is no CPU fallback: without a usable CUDA device every compute
+ *    call returns VD_ECUDA.
+ */
+#ifndef VORONOID_B200_H
+#define VORONOID_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define VD_OK 0
+#define VD_EINVAL 1     /* bad argument; e.g. wall id > -1000 (reference panics, wall/mod.rs:25-27) */
+#define VD_ENOMEM 2     /* device allocation failed or HBM budget exceeded */
+#define VD_EOVERFLOW 3  /* a cell exceeded every polytope capacity */
+#define VD_ETIMEOUT 4   /* a bounded device wait gave up */
+#define VD_ECUDA 5      /* CUDA runtime error / no device */
+#define VD_ESTATE 6     /* call out of order (e.g. results before calculate) */
+
+/* precision of the clipping path */
+#define VD_PREC_FP64 0  /* plain FP64, bitwise the reference's arithmetic */
+#define VD_PREC_MIXED 1 /* FP32 classification under an error bound, FP64 construction */
+
+/* WALL_ID_MAX (wall/mod.rs:8) */
+#define VD_WALL_ID_MAX (-1000)
+
+typedef struct vd_tess vd_tess;
+
+/* ---- Tessellation::new + Algorithm3DGrid::new
+ *      (tessellation.rs:25-36, algo_3d_grid.rs:47-95) ---- */
+int vd_tess_create(const double bmin[3], const double bmax[3], int nx, int ny, int nz,
+                   vd_tess** out);
+/* drop of Tessellation */
+int vd_tess_destroy(vd_tess* t);
+/* message of the last failed call on t (or of the last failed create when t is NULL) */
+const char* vd_last_error(const vd_tess* t);
+
+/* ---- walls: Wall::new + PlaneGeometry/SphereGeometry + Tessellation::add_wall
+ *      (wall/mod.rs:24-32, wall_3d.rs:23-27,66-68, tessellation.rs:197-200).
+ *      Adding a wall prunes generators outside it (tessellation.rs:175-194). ---- */
+int vd_tess_add_wall_plane(vd_tess* t, const double point[3], const double normal[3], int id);
+int vd_tess_add_wall_sphere(vd_tess* t, const double center[3], double radius, int id);
+/* Tessellation::clear_walls (tessellation.rs:203-205) */
+int vd_tess_clear_walls(vd_tess* t);
+
+/* ---- generators ---- */
+/* Tessellation::set_generators (tessellation.rs:43-67): keep points inside all
+ * walls, in order, then bin them (algo_3d_grid.rs:111-130). xyz is AoS, host. */
+int vd_tess_set_generators(vd_tess* t, const double* xyz, size_t n, size_t* n_kept);
+/* same, from a device pointer (the caller's CUDA memory, read on t's stream) */
+int vd_tess_set_generators_device(vd_tess* t, const double* d_xyz, size_t n, size_t* n_kept);
+/* Tessellation::set_generator (tessellation.rs:71-92): ignored when out of
+ * range or outside a wall, as in the reference */
+int vd_tess_set_generator(vd_tess* t, size_t index, const double xyz[3]);
+/* Tessellation::count_generators / generators (tessellation.rs:498-500,519-521) */
+int vd_tess_count_generators(const vd_tess* t, size_t* n);
+int vd_tess_get_generators(vd_tess* t, double* xyz);
+
+/* ---- the hot path ---- */
+/* select VD_PREC_FP64 (default) or VD_PREC_MIXED for the next calculate */
+int vd_tess_set_precision(vd_tess* t, int precision);
+/* Tessellation::calculate (tessellation.rs:213-230) over compute_cell
+ * (:414-475), Algorithm3DGrid::visit_neighbors (algo_3d_grid.rs:145-202) and
+ * Cell3DFaces::clip_with_scratch (cell_3d_faces.rs:288-503), with the volume,
+ * centroid and face-area reductions (cell_3d_faces.rs:106-254) fused in. */
+int vd_tess_calculate(vd_tess* t);
+/* Tessellation::relax (tessellation.rs:482-495), on the device */
+int vd_tess_relax(vd_tess* t);
+/* Tessellation::count_cells (tessellation.rs:503-505) */
+int vd_tess_count_cells(const vd_tess* t, size_t* n);
+
+/* ---- results (host buffers) ----
+ * Per-cell summaries: Cell3DFaces::volume / centroid (cell_3d_faces.rs:106-205)
+ * and the face count; any pointer may be NULL. */
+int vd_tess_get_cell_summaries(vd_tess* t, double* volume, double* centroid3, int32_t* n_faces);
+/* total faces over all cells (size of the CSR payloads below) */
+int vd_tess_total_faces(vd_tess* t, int64_t* total);
+/* Cell3DFaces::face_neighbors (cell_3d_faces.rs:97-99) of every cell as CSR:
+ * offsets[n_cells+1], ids[total]; offsets may be NULL */
+int vd_tess_get_neighbors(vd_tess* t, int64_t* offsets, int32_t* ids);
+/* Cell3DFaces::face_area for every face of every cell (cell_3d_faces.rs:207-254) */
+int vd_tess_get_face_areas(vd_tess* t, int64_t* offsets, double* areas);
+/* Tessellation::get_cell (tessellation.rs:514-516): the full polytope of cell i
+ * in the layout of Cell3DFaces (cell_3d_faces.rs:24-34).  Call with NULL
+ * buffers to get the sizes, then again with buffers of those sizes. */
+int vd_tess_get_cell(vd_tess* t, size_t i, int32_t* n_vertices, int32_t* n_faces,
+                     int32_t* n_face_indices, double* vertices, uint32_t* face_counts,
+                     uint32_t* face_indices, int32_t* face_neighbors);
+
+/* ---- device-resident results (for callers that keep data on the GPU) ---- */
+int vd_tess_device_results(vd_tess* t, const double** d_volume, const double** d_centroid3,
+                           const int32_t** d_n_faces);
+
+/* ---- instrumentation ---- */
+/* the CUDA stream (cudaStream_t) all work of t is ordered on */
+int vd_tess_stream(vd_tess* t, void** stream);
+/* device time (ms, CUDA events) of the phases of the last calculate:
+ * [0] binning, [1] clip kernel, [2] overflow/fallback passes, [3] total */
+int vd_tess_timings(vd_tess* t, float* ms4);
+/* algorithmic event counters of the last calculate (same meaning as the
+ * oracle's): candidates, clips, classified, modifying, intersections, kept,
+ * triangles, offsets */
+int vd_tess_counters(vd_tess* t, uint64_t* out8);
+/* cells that needed a fallback pass in the last calculate:
+ * [0] polytope-capacity overflow, [1] search-order extension */
+int vd_tess_fallback_counts(vd_tess* t, uint64_t* out2);
+
+/* ---- pinned host memory for callers staging large inputs/outputs ---- */
+int vd_host_alloc(size_t bytes, void** ptr);
+int vd_host_free(void* ptr);
+
+/* ---- device measurement helper: FP64 / FP32 FMA-chain peak (TFLOP/s) ---- */
+int vd_measure_fma_peak(int fp64, double* tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

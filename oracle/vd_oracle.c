@@ -1,0 +1,781 @@
+/*
+ * vd_oracle.c -- CPU oracle for the 3D tessellation path (TEST INFRASTRUCTURE).
+ *
+ * A plain-C restatement of the reference crate `voronoid`:
+ *   src/tessellation.rs        set_generators :43-67, add_wall/prune :175-200,
+ *                              calculate :213-230, compute_cell :414-475,
+ *                              relax :482-495
+ *   src/algorithm/algo_3d_grid.rs  new + search order :47-95,
+ *                              get_bin_index :98-107, set_generators :111-130,
+ *                              visit_neighbors :145-202
+ *   src/cell/cell_3d_faces.rs  new :37-74, volume :106-143, centroid :145-205,
+ *                              face_area :207-254, max_radius_sq :271-286,
+ *                              clip_with_scratch :288-503
+ *   src/wall/wall_3d.rs        PlaneGeometry :23-46, SphereGeometry :72-101
+ *   src/wall/mod.rs            WALL_ID_MAX and the id check :8,24-27
+ *   src/bounds/mod.rs          box_side :21-22
+ *
+ * Arithmetic is written in the reference's evaluation order and must be
+ * compiled with -ffp-contract=off (Rust never fuses a multiply and an add),
+ * so that every double matches what the reference computes.
+ *
+ * Only the tests, the smoke check and the CPU-baseline leg of the benchmark
+ * use this file, as a checker; the product never links it.
+ */
+#include "vd_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define VDO_TOL 1e-9 /* cell_3d_faces.rs:310-315,346,383-384 */
+#define VDO_WALL_ID_MAX (-1000)
+#define VDO_MAX_WALLS 64
+#define U16_NONE 0xFFFFu
+
+/* ------------------------------------------------------------------ */
+/* growable arrays                                                      */
+/* ------------------------------------------------------------------ */
+static void* grow(void* p, size_t* cap, size_t need, size_t elem) {
+  if (need <= *cap) return p;
+  size_t nc = *cap ? *cap : 16;
+  while (nc < need) nc *= 2;
+  void* q = realloc(p, nc * elem);
+  if (!q) abort();
+  *cap = nc;
+  return q;
+}
+#define GROW(arr, cap, need) ((arr) = grow((arr), &(cap), (need), sizeof(*(arr))))
+
+/* ------------------------------------------------------------------ */
+/* cell (cell_3d_faces.rs:24-34)                                        */
+/* ------------------------------------------------------------------ */
+struct vdo_cell {
+  size_t id;
+  double* v;     size_t nv, cap_v;  /* nv vertices, 3 doubles each */
+  uint8_t* fc;   size_t nf, cap_fc; /* face counts, u8 as in the reference */
+  int32_t* fn;   size_t cap_fn;     /* face neighbours */
+  uint16_t* fi;  size_t nh, cap_fi; /* flattened face indices, u16 */
+};
+
+typedef struct {
+  double* v;      size_t nv, cap_v;
+  uint8_t* fc;    size_t nf, cap_fc;
+  int32_t* fn;    size_t cap_fn;
+  uint16_t* fi;   size_t nh, cap_fi;
+  double* dists;  size_t cap_d;
+  uint8_t* is_int; size_t cap_ii;
+  int32_t* o2n;   size_t cap_o2n;     /* Option<u16>: -1 = None */
+  uint32_t* ikey; uint16_t* iid; size_t ni, cap_ik, cap_iid;
+  uint16_t* lseg; size_t nseg, cap_ls; /* pairs */
+  uint16_t* fbuf; size_t nfb, cap_fb;
+  uint16_t* lbuf; size_t nlb, cap_lb;
+  uint16_t* lmap; size_t cap_lm;
+} scratch_t;
+
+static void scratch_free(scratch_t* s) {
+  free(s->v); free(s->fc); free(s->fn); free(s->fi); free(s->dists);
+  free(s->is_int); free(s->o2n); free(s->ikey); free(s->iid); free(s->lseg);
+  free(s->fbuf); free(s->lbuf); free(s->lmap);
+  memset(s, 0, sizeof(*s));
+}
+
+/* box_side (bounds/mod.rs:21-22): x- -1, x+ -2, y- -3, y+ -4, z- -5, z+ -6 */
+static int32_t box_side(int axis, int is_max) { return -1 - (axis * 2 + (is_max ? 1 : 0)); }
+
+/* Cell3DFaces::new (cell_3d_faces.rs:37-74) */
+static void cell_init_box(vdo_cell* c, size_t id, const double* mn, const double* mx) {
+  static const uint16_t idx[24] = {3, 2, 1, 0, 4, 5, 6, 7, 0, 1, 5, 4,
+                                   2, 3, 7, 6, 0, 4, 7, 3, 1, 2, 6, 5};
+  const double vv[24] = {mn[0], mn[1], mn[2], mx[0], mn[1], mn[2], mx[0], mx[1], mn[2],
+                         mn[0], mx[1], mn[2], mn[0], mn[1], mx[2], mx[0], mn[1], mx[2],
+                         mx[0], mx[1], mx[2], mn[0], mx[1], mx[2]};
+  c->id = id;
+  GROW(c->v, c->cap_v, 24);
+  memcpy(c->v, vv, sizeof(vv));
+  c->nv = 8;
+  GROW(c->fc, c->cap_fc, 6);
+  GROW(c->fn, c->cap_fn, 6);
+  for (int f = 0; f < 6; ++f) c->fc[f] = 4;
+  c->fn[0] = box_side(2, 0); c->fn[1] = box_side(2, 1);
+  c->fn[2] = box_side(1, 0); c->fn[3] = box_side(1, 1);
+  c->fn[4] = box_side(0, 0); c->fn[5] = box_side(0, 1);
+  c->nf = 6;
+  GROW(c->fi, c->cap_fi, 24);
+  memcpy(c->fi, idx, sizeof(idx));
+  c->nh = 24;
+}
+
+/* max_radius_sq (cell_3d_faces.rs:271-286) */
+static double cell_max_radius_sq(const vdo_cell* c, const double* g) {
+  double m = 0.0;
+  for (size_t k = 0; k < c->nv; ++k) {
+    double dx = c->v[3 * k] - g[0];
+    double dy = c->v[3 * k + 1] - g[1];
+    double dz = c->v[3 * k + 2] - g[2];
+    double d2 = dx * dx + dy * dy + dz * dz;
+    if (d2 > m) m = d2;
+  }
+  return m;
+}
+
+static inline double clamp01(double x) {
+  /* f64::clamp(0.0, 1.0): NaN passes through */
+  if (x < 0.0) return 0.0;
+  if (x > 1.0) return 1.0;
+  return x;
+}
+
+/* intersection lookup/creation shared by both crossing cases
+ * (cell_3d_faces.rs:391-417 and :422-448) */
+static uint16_t intersect(const vdo_cell* c, scratch_t* s, size_t is, size_t ie,
+                          const double* g, double* max_d2, uint64_t* cnt) {
+  uint32_t key = is < ie ? ((uint32_t)is << 16 | (uint32_t)ie) : ((uint32_t)ie << 16 | (uint32_t)is);
+  for (size_t k = 0; k < s->ni; ++k)
+    if (s->ikey[k] == key) return s->iid[k];
+  double ds = s->dists[is], de = s->dists[ie];
+  double t = clamp01(ds / (ds - de));
+  double ax = c->v[is * 3], ay = c->v[is * 3 + 1], az = c->v[is * 3 + 2];
+  double bx = c->v[ie * 3], by = c->v[ie * 3 + 1], bz = c->v[ie * 3 + 2];
+  uint16_t nid = (uint16_t)s->nv;
+  double nx = ax + t * (bx - ax);
+  double ny = ay + t * (by - ay);
+  double nz = az + t * (bz - az);
+  GROW(s->v, s->cap_v, 3 * (s->nv + 1));
+  s->v[3 * s->nv] = nx; s->v[3 * s->nv + 1] = ny; s->v[3 * s->nv + 2] = nz;
+  s->nv++;
+  if (g) {
+    double dx = nx - g[0], dy = ny - g[1], dz = nz - g[2];
+    double d2 = dx * dx + dy * dy + dz * dz;
+    if (d2 > *max_d2) *max_d2 = d2;
+  }
+  GROW(s->is_int, s->cap_ii, s->nv);
+  s->is_int[s->nv - 1] = 1;
+  GROW(s->ikey, s->cap_ik, s->ni + 1);
+  GROW(s->iid, s->cap_iid, s->ni + 1);
+  s->ikey[s->ni] = key; s->iid[s->ni] = nid; s->ni++;
+  if (cnt) cnt[VDO_CNT_INTERSECTIONS]++;
+  return nid;
+}
+
+static inline void fbuf_push(scratch_t* s, uint16_t x) {
+  GROW(s->fbuf, s->cap_fb, s->nfb + 1);
+  s->fbuf[s->nfb++] = x;
+}
+
+/* clip_with_scratch (cell_3d_faces.rs:288-503).  Returns modified; *r2 gets
+ * the new max radius over the new vertex set when g != NULL, else 0. */
+static int cell_clip(vdo_cell* c, const double* p, const double* n, int32_t nbr,
+                     scratch_t* s, const double* g, double* r2, uint64_t* cnt) {
+  const double px = p[0], py = p[1], pz = p[2];
+  const double nx = n[0], ny = n[1], nz = n[2];
+  const size_t nv = c->nv;
+  int all_in = 1, all_out = 1;
+  *r2 = 0.0;
+  if (cnt) { cnt[VDO_CNT_CLIPS]++; cnt[VDO_CNT_CLASSIFIED] += nv; }
+  GROW(s->dists, s->cap_d, nv);
+  /* 1. distances (:302-315) */
+  for (size_t i = 0; i < nv; ++i) {
+    double vx = c->v[3 * i], vy = c->v[3 * i + 1], vz = c->v[3 * i + 2];
+    double d = (vx - px) * nx + (vy - py) * ny + (vz - pz) * nz;
+    s->dists[i] = d;
+    if (d > VDO_TOL) all_in = 0;
+    else if (d < -VDO_TOL) all_out = 0;
+  }
+  if (all_in) return 0;
+  if (all_out) {
+    c->nv = 0; c->nf = 0; c->nh = 0;
+    return 1;
+  }
+  if (cnt) cnt[VDO_CNT_MODIFYING]++;
+  /* 2. new structures (:328-340) */
+  s->nv = 0; s->nf = 0; s->nh = 0; s->ni = 0; s->nseg = 0;
+  GROW(s->o2n, s->cap_o2n, nv);
+  for (size_t i = 0; i < nv; ++i) s->o2n[i] = -1;
+  double max_d2 = 0.0;
+  /* keep inside vertices in order (:344-362) */
+  for (size_t i = 0; i < nv; ++i) {
+    if (s->dists[i] <= VDO_TOL) {
+      uint16_t nid = (uint16_t)s->nv;
+      GROW(s->v, s->cap_v, 3 * (s->nv + 1));
+      s->v[3 * s->nv] = c->v[3 * i];
+      s->v[3 * s->nv + 1] = c->v[3 * i + 1];
+      s->v[3 * s->nv + 2] = c->v[3 * i + 2];
+      s->nv++;
+      s->o2n[i] = nid;
+      GROW(s->is_int, s->cap_ii, s->nv);
+      s->is_int[s->nv - 1] = 0;
+      if (g) {
+        double dx = c->v[3 * i] - g[0];
+        double dy = c->v[3 * i + 1] - g[1];
+        double dz = c->v[3 * i + 2] - g[2];
+        double d2 = dx * dx + dy * dy + dz * dz;
+        if (d2 > max_d2) max_d2 = d2;
+        if (cnt) cnt[VDO_CNT_KEPT]++;
+      }
+    }
+  }
+  /* 3. clip each face (:369-468) */
+  size_t off = 0;
+  for (size_t f = 0; f < c->nf; ++f) {
+    size_t count = c->fc[f];
+    int32_t fnb = c->fn[f];
+    const uint16_t* cur = &c->fi[off];
+    off += count;
+    s->nfb = 0;
+    for (size_t i = 0; i < count; ++i) {
+      size_t is = cur[i], ie = cur[(i + 1) % count];
+      double ds = s->dists[is], de = s->dists[ie];
+      int s_in = ds <= VDO_TOL, e_in = de <= VDO_TOL;
+      if (s_in) {
+        if (e_in) {
+          if (s->o2n[ie] >= 0) fbuf_push(s, (uint16_t)s->o2n[ie]);
+        } else {
+          fbuf_push(s, intersect(c, s, is, ie, g, &max_d2, cnt));
+        }
+      } else if (e_in) {
+        fbuf_push(s, intersect(c, s, is, ie, g, &max_d2, cnt));
+        if (s->o2n[ie] >= 0) fbuf_push(s, (uint16_t)s->o2n[ie]);
+      }
+    }
+    if (s->nfb >= 3) {
+      GROW(s->fc, s->cap_fc, s->nf + 1);
+      GROW(s->fn, s->cap_fn, s->nf + 1);
+      s->fc[s->nf] = (uint8_t)s->nfb;
+      s->fn[s->nf] = fnb;
+      s->nf++;
+      for (size_t i = 0; i < s->nfb; ++i) {
+        uint16_t u = s->fbuf[i], v = s->fbuf[(i + 1) % s->nfb];
+        if (s->is_int[u] && s->is_int[v]) {
+          GROW(s->lseg, s->cap_ls, 2 * (s->nseg + 1));
+          s->lseg[2 * s->nseg] = v;
+          s->lseg[2 * s->nseg + 1] = u;
+          s->nseg++;
+        }
+      }
+      GROW(s->fi, s->cap_fi, s->nh + s->nfb);
+      memcpy(&s->fi[s->nh], s->fbuf, s->nfb * sizeof(uint16_t));
+      s->nh += s->nfb;
+    }
+  }
+  /* 4. lid face (:470-495) */
+  if (s->nseg > 0) {
+    s->nlb = 0;
+    GROW(s->lmap, s->cap_lm, s->nv);
+    for (size_t k = 0; k < s->nv; ++k) s->lmap[k] = U16_NONE;
+    for (size_t k = 0; k < s->nseg; ++k) s->lmap[s->lseg[2 * k]] = s->lseg[2 * k + 1];
+    uint16_t start = s->lseg[0], next = s->lseg[1];
+    GROW(s->lbuf, s->cap_lb, s->nlb + 1);
+    s->lbuf[s->nlb++] = start;
+    uint16_t curv = next;
+    while (curv != start && s->nlb <= s->nseg) {
+      GROW(s->lbuf, s->cap_lb, s->nlb + 1);
+      s->lbuf[s->nlb++] = curv;
+      curv = s->lmap[curv];
+      if (curv == U16_NONE) break;
+    }
+    if (s->nlb >= 3) {
+      GROW(s->fc, s->cap_fc, s->nf + 1);
+      GROW(s->fn, s->cap_fn, s->nf + 1);
+      s->fc[s->nf] = (uint8_t)s->nlb;
+      s->fn[s->nf] = nbr;
+      s->nf++;
+      GROW(s->fi, s->cap_fi, s->nh + s->nlb);
+      memcpy(&s->fi[s->nh], s->lbuf, s->nlb * sizeof(uint16_t));
+      s->nh += s->nlb;
+    }
+  }
+  /* swap (:497-500) */
+#define SWAPP(a, b) do { void* tmp_ = (void*)(a); (a) = (void*)(b); (b) = tmp_; } while (0)
+#define SWAPZ(a, b) do { size_t tmp_ = (a); (a) = (b); (b) = tmp_; } while (0)
+  { double* t0 = c->v; c->v = s->v; s->v = t0; SWAPZ(c->cap_v, s->cap_v); c->nv = s->nv; }
+  { uint8_t* t0 = c->fc; c->fc = s->fc; s->fc = t0; SWAPZ(c->cap_fc, s->cap_fc); c->nf = s->nf; }
+  { int32_t* t0 = c->fn; c->fn = s->fn; s->fn = t0; SWAPZ(c->cap_fn, s->cap_fn); }
+  { uint16_t* t0 = c->fi; c->fi = s->fi; s->fi = t0; SWAPZ(c->cap_fi, s->cap_fi); c->nh = s->nh; }
+#undef SWAPP
+#undef SWAPZ
+  *r2 = max_d2;
+  return 1;
+}
+
+/* volume (cell_3d_faces.rs:106-143) and centroid (:145-205).  The two share
+ * the per-triangle determinant expression, so one pass yields both with the
+ * same bits as two separate passes. */
+static void cell_measure(const vdo_cell* c, double* vol, double* cen, uint64_t* cnt) {
+  double volume = 0.0, cx = 0.0, cy = 0.0, cz = 0.0, total = 0.0;
+  size_t off = 0;
+  for (size_t f = 0; f < c->nf; ++f) {
+    size_t count = c->fc[f];
+    if (count < 3) { off += count; continue; }
+    size_t i0 = c->fi[off];
+    double v0x = c->v[i0 * 3], v0y = c->v[i0 * 3 + 1], v0z = c->v[i0 * 3 + 2];
+    for (size_t i = 1; i < count - 1; ++i) {
+      size_t i1 = c->fi[off + i], i2 = c->fi[off + i + 1];
+      double v1x = c->v[i1 * 3], v1y = c->v[i1 * 3 + 1], v1z = c->v[i1 * 3 + 2];
+      double v2x = c->v[i2 * 3], v2y = c->v[i2 * 3 + 1], v2z = c->v[i2 * 3 + 2];
+      volume += v0x * (v1y * v2z - v1z * v2y) + v0y * (v1z * v2x - v1x * v2z) +
+                v0z * (v1x * v2y - v1y * v2x);
+      double crx = v1y * v2z - v1z * v2y;
+      double cry = v1z * v2x - v1x * v2z;
+      double crz = v1x * v2y - v1y * v2x;
+      double det = v0x * crx + v0y * cry + v0z * crz;
+      total += det;
+      double tx = v0x + v1x + v2x, ty = v0y + v1y + v2y, tz = v0z + v1z + v2z;
+      cx += det * tx; cy += det * ty; cz += det * tz;
+      if (cnt) cnt[VDO_CNT_TRIANGLES]++;
+    }
+    off += count;
+  }
+  if (vol) *vol = fabs(volume / 6.0);
+  if (cen) {
+    if (fabs(total) < 1e-9) {
+      cen[0] = cen[1] = cen[2] = 0.0;
+    } else {
+      double factor = 1.0 / (4.0 * total);
+      cen[0] = cx * factor; cen[1] = cy * factor; cen[2] = cz * factor;
+    }
+  }
+}
+
+/* face_area (cell_3d_faces.rs:207-254) for a face starting at `off` */
+static double face_area_at(const vdo_cell* c, size_t off, size_t count) {
+  if (count < 3) return 0.0;
+  double area = 0.0;
+  size_t p0 = c->fi[off];
+  double p0x = c->v[p0 * 3], p0y = c->v[p0 * 3 + 1], p0z = c->v[p0 * 3 + 2];
+  for (size_t i = 1; i < count - 1; ++i) {
+    size_t p1 = c->fi[off + i], p2 = c->fi[off + i + 1];
+    double v1x = c->v[p1 * 3] - p0x, v1y = c->v[p1 * 3 + 1] - p0y, v1z = c->v[p1 * 3 + 2] - p0z;
+    double v2x = c->v[p2 * 3] - p0x, v2y = c->v[p2 * 3 + 1] - p0y, v2z = c->v[p2 * 3 + 2] - p0z;
+    double crx = v1y * v2z - v1z * v2y;
+    double cry = v1z * v2x - v1x * v2z;
+    double crz = v1x * v2y - v1y * v2x;
+    area += 0.5 * sqrt(crx * crx + cry * cry + crz * crz);
+  }
+  return area;
+}
+
+/* ------------------------------------------------------------------ */
+/* walls (wall_3d.rs:8-101, wall/mod.rs)                                */
+/* ------------------------------------------------------------------ */
+typedef struct {
+  int kind; /* 0 plane, 1 sphere */
+  int32_t id;
+  double a[3]; /* plane point / sphere centre */
+  double n[3]; /* plane normal (normalised, points IN) */
+  double r;
+} wall_t;
+
+static int wall_contains(const wall_t* w, const double* p) {
+  double dx = p[0] - w->a[0], dy = p[1] - w->a[1], dz = p[2] - w->a[2];
+  if (w->kind == 0) return (dx * w->n[0] + dy * w->n[1] + dz * w->n[2]) >= 0.0;
+  return (dx * dx + dy * dy + dz * dz) <= w->r * w->r;
+}
+
+/* cut: emits one plane (point, outward normal); returns 0 if none */
+static int wall_cut(const wall_t* w, const double* g, double* p, double* n) {
+  if (w->kind == 0) {
+    p[0] = w->a[0]; p[1] = w->a[1]; p[2] = w->a[2];
+    n[0] = -w->n[0]; n[1] = -w->n[1]; n[2] = -w->n[2];
+    return 1;
+  }
+  double dx = g[0] - w->a[0], dy = g[1] - w->a[1], dz = g[2] - w->a[2];
+  double dist = sqrt(dx * dx + dy * dy + dz * dz);
+  if (dist == 0.0) return 0;
+  double scale = w->r / dist;
+  p[0] = w->a[0] + dx * scale; p[1] = w->a[1] + dy * scale; p[2] = w->a[2] + dz * scale;
+  n[0] = dx / dist; n[1] = dy / dist; n[2] = dz / dist;
+  return 1;
+}
+
+/* ------------------------------------------------------------------ */
+/* tessellation + grid                                                  */
+/* ------------------------------------------------------------------ */
+typedef struct {
+  int32_t dx, dy, dz;
+  int32_t lin; /* enumeration index: ties keep this order */
+  double min_d2;
+} offset_t;
+
+struct vdo_tess {
+  double bmin[3], bmax[3];
+  size_t nx, ny, nz;
+  double sx, sy, sz;       /* grid_scale */
+  double lx, ly, lz;       /* grid_limit = n - 1e-5 */
+  offset_t* order; size_t norder;
+  wall_t walls[VDO_MAX_WALLS]; int nwalls;
+  double* gen; size_t ngen;
+  size_t* bin_of;          /* generator_bin_ids */
+  size_t* bin_start;       /* CSR of grid_bins, members ascending */
+  size_t* bin_members;
+  vdo_cell* cells; size_t ncells;
+  uint64_t counters[VDO_NCOUNTERS];
+};
+
+static int cmp_offset(const void* a, const void* b) {
+  const offset_t* x = (const offset_t*)a;
+  const offset_t* y = (const offset_t*)b;
+  if (x->min_d2 < y->min_d2) return -1;
+  if (x->min_d2 > y->min_d2) return 1;
+  return (x->lin > y->lin) - (x->lin < y->lin);
+}
+
+/* Algorithm3DGrid::new (algo_3d_grid.rs:47-95), stable tie order */
+vdo_tess* vdo_create(const double bmin[3], const double bmax[3], int nx, int ny, int nz) {
+  if (nx <= 0 || ny <= 0 || nz <= 0) return NULL;
+  vdo_tess* t = (vdo_tess*)calloc(1, sizeof(vdo_tess));
+  memcpy(t->bmin, bmin, 3 * sizeof(double));
+  memcpy(t->bmax, bmax, 3 * sizeof(double));
+  t->nx = (size_t)nx; t->ny = (size_t)ny; t->nz = (size_t)nz;
+  t->sx = (double)nx / (bmax[0] - bmin[0]);
+  t->sy = (double)ny / (bmax[1] - bmin[1]);
+  t->sz = (double)nz / (bmax[2] - bmin[2]);
+  t->lx = (double)nx - 1e-5; t->ly = (double)ny - 1e-5; t->lz = (double)nz - 1e-5;
+  double csx = 1.0 / t->sx, csy = 1.0 / t->sy, csz = 1.0 / t->sz;
+  size_t n = (size_t)(2 * nx + 1) * (size_t)(2 * ny + 1) * (size_t)(2 * nz + 1);
+  t->order = (offset_t*)malloc(n * sizeof(offset_t));
+  size_t k = 0;
+  for (int z = -nz; z <= nz; ++z)
+    for (int y = -ny; y <= ny; ++y)
+      for (int x = -nx; x <= nx; ++x) {
+        double mx = x > 0 ? (double)(x - 1) * csx : (x < 0 ? (double)(-x - 1) * csx : 0.0);
+        double my = y > 0 ? (double)(y - 1) * csy : (y < 0 ? (double)(-y - 1) * csy : 0.0);
+        double mz = z > 0 ? (double)(z - 1) * csz : (z < 0 ? (double)(-z - 1) * csz : 0.0);
+        offset_t o = {x, y, z, (int32_t)k, mx * mx + my * my + mz * mz};
+        t->order[k++] = o;
+      }
+  qsort(t->order, n, sizeof(offset_t), cmp_offset);
+  t->norder = n;
+  t->bin_start = (size_t*)calloc(t->nx * t->ny * t->nz + 1, sizeof(size_t));
+  return t;
+}
+
+static void free_cells(vdo_tess* t) {
+  for (size_t i = 0; i < t->ncells; ++i) {
+    free(t->cells[i].v); free(t->cells[i].fc); free(t->cells[i].fn); free(t->cells[i].fi);
+  }
+  free(t->cells);
+  t->cells = NULL;
+  t->ncells = 0;
+}
+
+void vdo_destroy(vdo_tess* t) {
+  if (!t) return;
+  free_cells(t);
+  free(t->order); free(t->gen); free(t->bin_of); free(t->bin_start); free(t->bin_members);
+  free(t);
+}
+
+static inline size_t to_index(double v) {
+  /* `f64 as usize`: saturating, NaN -> 0 */
+  if (!(v > 0.0)) return 0;
+  return (size_t)v;
+}
+static inline double clampd(double v, double lo, double hi) {
+  if (v < lo) return lo;
+  if (v > hi) return hi;
+  return v;
+}
+
+/* get_bin_index (algo_3d_grid.rs:98-107) */
+size_t vdo_bin_index(const vdo_tess* t, double x, double y, double z) {
+  size_t ix = to_index(clampd((x - t->bmin[0]) * t->sx, 0.0, t->lx));
+  size_t iy = to_index(clampd((y - t->bmin[1]) * t->sy, 0.0, t->ly));
+  size_t iz = to_index(clampd((z - t->bmin[2]) * t->sz, 0.0, t->lz));
+  return ix + iy * t->nx + iz * t->nx * t->ny;
+}
+
+/* Algorithm3DGrid::set_generators (algo_3d_grid.rs:111-130) */
+static void grid_rebin(vdo_tess* t) {
+  size_t nb = t->nx * t->ny * t->nz;
+  free(t->bin_of); free(t->bin_members);
+  t->bin_of = (size_t*)malloc((t->ngen ? t->ngen : 1) * sizeof(size_t));
+  t->bin_members = (size_t*)malloc((t->ngen ? t->ngen : 1) * sizeof(size_t));
+  memset(t->bin_start, 0, (nb + 1) * sizeof(size_t));
+  for (size_t i = 0; i < t->ngen; ++i) {
+    size_t b = vdo_bin_index(t, t->gen[3 * i], t->gen[3 * i + 1], t->gen[3 * i + 2]);
+    t->bin_of[i] = b;
+    t->bin_start[b + 1]++;
+  }
+  for (size_t b = 0; b < nb; ++b) t->bin_start[b + 1] += t->bin_start[b];
+  size_t* cur = (size_t*)malloc((nb ? nb : 1) * sizeof(size_t));
+  memcpy(cur, t->bin_start, nb * sizeof(size_t));
+  for (size_t i = 0; i < t->ngen; ++i) t->bin_members[cur[t->bin_of[i]]++] = i;
+  free(cur);
+}
+
+static int walls_contain(const vdo_tess* t, const double* p) {
+  for (int w = 0; w < t->nwalls; ++w)
+    if (!wall_contains(&t->walls[w], p)) return 0;
+  return 1;
+}
+
+/* Tessellation::set_generators (tessellation.rs:43-67): walls only */
+size_t vdo_set_generators(vdo_tess* t, const double* xyz, size_t n) {
+  double* keep = (double*)malloc((n ? n : 1) * 3 * sizeof(double));
+  size_t m = 0;
+  for (size_t i = 0; i < n; ++i) {
+    if (walls_contain(t, &xyz[3 * i])) {
+      memcpy(&keep[3 * m], &xyz[3 * i], 3 * sizeof(double));
+      m++;
+    }
+  }
+  free(t->gen);
+  t->gen = keep;
+  t->ngen = m;
+  grid_rebin(t);
+  return m;
+}
+
+/* prune_outside_generators + add_wall (tessellation.rs:175-200) */
+static int add_wall(vdo_tess* t, const wall_t* w) {
+  if (w->id > VDO_WALL_ID_MAX || t->nwalls >= VDO_MAX_WALLS) return -1;
+  t->walls[t->nwalls++] = *w;
+  size_t m = 0;
+  for (size_t i = 0; i < t->ngen; ++i) {
+    if (walls_contain(t, &t->gen[3 * i])) {
+      if (m != i) memmove(&t->gen[3 * m], &t->gen[3 * i], 3 * sizeof(double));
+      m++;
+    }
+  }
+  if (m != t->ngen) {
+    t->ngen = m;
+    grid_rebin(t);
+  }
+  return 0;
+}
+
+int vdo_add_wall_plane(vdo_tess* t, const double point[3], const double normal[3], int id) {
+  wall_t w;
+  memset(&w, 0, sizeof(w));
+  w.kind = 0; w.id = id;
+  memcpy(w.a, point, 3 * sizeof(double));
+  /* PlaneGeometry::new (wall_3d.rs:23-27) */
+  double len = sqrt(normal[0] * normal[0] + normal[1] * normal[1] + normal[2] * normal[2]);
+  if (len == 0.0) { w.n[0] = 0.0; w.n[1] = 0.0; w.n[2] = 1.0; }
+  else { w.n[0] = normal[0] / len; w.n[1] = normal[1] / len; w.n[2] = normal[2] / len; }
+  return add_wall(t, &w);
+}
+
+int vdo_add_wall_sphere(vdo_tess* t, const double center[3], double radius, int id) {
+  wall_t w;
+  memset(&w, 0, sizeof(w));
+  w.kind = 1; w.id = id; w.r = radius;
+  memcpy(w.a, center, 3 * sizeof(double));
+  return add_wall(t, &w);
+}
+
+void vdo_clear_walls(vdo_tess* t) { t->nwalls = 0; }
+
+/* compute_cell (tessellation.rs:414-475) with visit_neighbors
+ * (algo_3d_grid.rs:145-202) and the visitor (tessellation.rs:446-471) */
+static void compute_cell(const vdo_tess* t, size_t i, vdo_cell* cell, scratch_t* s, uint64_t* cnt) {
+  const double g[3] = {t->gen[3 * i], t->gen[3 * i + 1], t->gen[3 * i + 2]};
+  double r2;
+  cell_init_box(cell, i, t->bmin, t->bmax);
+  for (int w = 0; w < t->nwalls; ++w) {
+    double p[3], n[3];
+    if (wall_cut(&t->walls[w], g, p, n)) cell_clip(cell, p, n, t->walls[w].id, s, NULL, &r2, cnt);
+    if (cell->nv == 0) return;
+  }
+  double cur = cell_max_radius_sq(cell, g);
+
+  size_t b = t->bin_of[i];
+  size_t nxy = t->nx * t->ny;
+  size_t iz = b / nxy, rem = b % nxy, iy = rem / t->nx, ix = rem % t->nx;
+  double csx = 1.0 / t->sx, csy = 1.0 / t->sy, csz = 1.0 / t->sz;
+  double rx = (g[0] - t->bmin[0]) * t->sx - (double)ix;
+  double ry = (g[1] - t->bmin[1]) * t->sy - (double)iy;
+  double rz = (g[2] - t->bmin[2]) * t->sz - (double)iz;
+  for (size_t k = 0; k < t->norder; ++k) {
+    const offset_t* o = &t->order[k];
+    if (cnt) cnt[VDO_CNT_OFFSETS]++;
+    if (o->min_d2 > 4.0 * cur) break;
+    long bx = (long)ix + o->dx, by = (long)iy + o->dy, bz = (long)iz + o->dz;
+    if (bx < 0 || bx >= (long)t->nx || by < 0 || by >= (long)t->ny || bz < 0 || bz >= (long)t->nz)
+      continue;
+    double ddx = o->dx > 0 ? ((double)o->dx - rx) * csx : (o->dx < 0 ? ((double)(-(o->dx + 1)) + rx) * csx : 0.0);
+    double ddy = o->dy > 0 ? ((double)o->dy - ry) * csy : (o->dy < 0 ? ((double)(-(o->dy + 1)) + ry) * csy : 0.0);
+    double ddz = o->dz > 0 ? ((double)o->dz - rz) * csz : (o->dz < 0 ? ((double)(-(o->dz + 1)) + rz) * csz : 0.0);
+    double bdx = fmax(ddx, 0.0), bdy = fmax(ddy, 0.0), bdz = fmax(ddz, 0.0);
+    if (!(bdx * bdx + bdy * bdy + bdz * bdz <= 4.0 * cur)) continue;
+    size_t bin = (size_t)bx + (size_t)by * t->nx + (size_t)bz * nxy;
+    for (size_t m = t->bin_start[bin]; m < t->bin_start[bin + 1]; ++m) {
+      size_t j = t->bin_members[m];
+      if (j == i) continue;
+      if (cnt) cnt[VDO_CNT_CANDIDATES]++;
+      const double* q = &t->gen[3 * j];
+      double dist_sq = 0.0, mid[3], nrm[3];
+      for (int a = 0; a < 3; ++a) {
+        double d = q[a] - g[a];
+        dist_sq += d * d;
+        mid[a] = g[a] + d * 0.5;
+        nrm[a] = d;
+      }
+      if (dist_sq > 4.0 * cur) continue;
+      if (cell_clip(cell, mid, nrm, (int32_t)j, s, g, &r2, cnt)) {
+        cur = (cell->nv == 0) ? 0.0 : r2;
+      }
+    }
+  }
+}
+
+void vdo_calculate_range(vdo_tess* t, size_t begin, size_t end, int nthreads) {
+  free_cells(t);
+  t->ncells = t->ngen;
+  t->cells = (vdo_cell*)calloc(t->ncells ? t->ncells : 1, sizeof(vdo_cell));
+  memset(t->counters, 0, sizeof(t->counters));
+  if (end > t->ngen) end = t->ngen;
+#ifdef _OPENMP
+  if (nthreads <= 0) nthreads = omp_get_max_threads();
+#pragma omp parallel num_threads(nthreads)
+#endif
+  {
+    scratch_t s;
+    memset(&s, 0, sizeof(s));
+    uint64_t cnt[VDO_NCOUNTERS];
+    memset(cnt, 0, sizeof(cnt));
+#ifdef _OPENMP
+#pragma omp for schedule(dynamic, 64)
+#endif
+    for (long long i = (long long)begin; i < (long long)end; ++i) {
+      compute_cell(t, (size_t)i, &t->cells[i], &s, cnt);
+      cell_measure(&t->cells[i], NULL, NULL, cnt);
+    }
+#ifdef _OPENMP
+#pragma omp critical
+#endif
+    for (int k = 0; k < VDO_NCOUNTERS; ++k) t->counters[k] += cnt[k];
+    scratch_free(&s);
+  }
+  (void)nthreads;
+}
+
+void vdo_calculate(vdo_tess* t, int nthreads) { vdo_calculate_range(t, 0, t->ngen, nthreads); }
+
+/* Tessellation::relax (tessellation.rs:482-495) */
+void vdo_relax(vdo_tess* t) {
+  size_t n = t->ncells < t->ngen ? t->ncells : t->ngen;
+  double* ng = (double*)malloc((n ? n : 1) * 3 * sizeof(double));
+  for (size_t i = 0; i < n; ++i) {
+    if (t->cells[i].nv == 0) memcpy(&ng[3 * i], &t->gen[3 * i], 3 * sizeof(double));
+    else cell_measure(&t->cells[i], NULL, &ng[3 * i], NULL);
+  }
+  vdo_set_generators(t, ng, n);
+  free(ng);
+}
+
+size_t vdo_count_generators(const vdo_tess* t) { return t->ngen; }
+size_t vdo_count_cells(const vdo_tess* t) { return t->ncells; }
+void vdo_get_generators(const vdo_tess* t, double* xyz) { memcpy(xyz, t->gen, t->ngen * 3 * sizeof(double)); }
+size_t vdo_search_order_len(const vdo_tess* t) { return t->norder; }
+void vdo_get_search_order(const vdo_tess* t, int32_t* dxyz, double* min_d2) {
+  for (size_t k = 0; k < t->norder; ++k) {
+    if (dxyz) { dxyz[3 * k] = t->order[k].dx; dxyz[3 * k + 1] = t->order[k].dy; dxyz[3 * k + 2] = t->order[k].dz; }
+    if (min_d2) min_d2[k] = t->order[k].min_d2;
+  }
+}
+
+void vdo_get_summaries(const vdo_tess* t, double* vol, double* cen, int32_t* nfaces) {
+  for (size_t i = 0; i < t->ncells; ++i) {
+    double v, c[3];
+    cell_measure(&t->cells[i], &v, c, NULL);
+    if (vol) vol[i] = v;
+    if (cen) { cen[3 * i] = c[0]; cen[3 * i + 1] = c[1]; cen[3 * i + 2] = c[2]; }
+    if (nfaces) nfaces[i] = (int32_t)t->cells[i].nf;
+  }
+}
+
+int64_t vdo_total_faces(const vdo_tess* t) {
+  int64_t s = 0;
+  for (size_t i = 0; i < t->ncells; ++i) s += (int64_t)t->cells[i].nf;
+  return s;
+}
+
+void vdo_get_neighbors(const vdo_tess* t, int64_t* offsets, int32_t* ids) {
+  int64_t o = 0;
+  for (size_t i = 0; i < t->ncells; ++i) {
+    if (offsets) offsets[i] = o;
+    for (size_t f = 0; f < t->cells[i].nf; ++f) ids[o++] = t->cells[i].fn[f];
+  }
+  if (offsets) offsets[t->ncells] = o;
+}
+
+void vdo_get_face_areas(const vdo_tess* t, int64_t* offsets, double* areas) {
+  int64_t o = 0;
+  for (size_t i = 0; i < t->ncells; ++i) {
+    const vdo_cell* c = &t->cells[i];
+    if (offsets) offsets[i] = o;
+    size_t off = 0;
+    for (size_t f = 0; f < c->nf; ++f) {
+      areas[o++] = face_area_at(c, off, c->fc[f]);
+      off += c->fc[f];
+    }
+  }
+  if (offsets) offsets[t->ncells] = o;
+}
+
+void vdo_get_counters(const vdo_tess* t, uint64_t* out) { memcpy(out, t->counters, sizeof(t->counters)); }
+
+const vdo_cell* vdo_get_cell(const vdo_tess* t, size_t i) { return i < t->ncells ? &t->cells[i] : NULL; }
+
+/* ---- single-cell API ---- */
+vdo_cell* vdo_cell_new(size_t id, const double bmin[3], const double bmax[3]) {
+  vdo_cell* c = (vdo_cell*)calloc(1, sizeof(vdo_cell));
+  cell_init_box(c, id, bmin, bmax);
+  return c;
+}
+
+vdo_cell* vdo_cell_clone(const vdo_cell* c) {
+  vdo_cell* d = (vdo_cell*)calloc(1, sizeof(vdo_cell));
+  d->id = c->id;
+  GROW(d->v, d->cap_v, 3 * c->nv + 1); memcpy(d->v, c->v, 3 * c->nv * sizeof(double)); d->nv = c->nv;
+  GROW(d->fc, d->cap_fc, c->nf + 1); memcpy(d->fc, c->fc, c->nf); d->nf = c->nf;
+  GROW(d->fn, d->cap_fn, c->nf + 1); memcpy(d->fn, c->fn, c->nf * sizeof(int32_t));
+  GROW(d->fi, d->cap_fi, c->nh + 1); memcpy(d->fi, c->fi, c->nh * sizeof(uint16_t)); d->nh = c->nh;
+  return d;
+}
+
+void vdo_cell_free(vdo_cell* c) {
+  if (!c) return;
+  free(c->v); free(c->fc); free(c->fn); free(c->fi); free(c);
+}
+
+int vdo_cell_clip(vdo_cell* c, const double point[3], const double normal[3], int neighbor_id) {
+  scratch_t s;
+  memset(&s, 0, sizeof(s));
+  double r2;
+  int m = cell_clip(c, point, normal, neighbor_id, &s, NULL, &r2, NULL);
+  scratch_free(&s);
+  return m;
+}
+
+int vdo_cell_num_vertices(const vdo_cell* c) { return (int)c->nv; }
+int vdo_cell_num_faces(const vdo_cell* c) { return (int)c->nf; }
+int vdo_cell_num_face_indices(const vdo_cell* c) { return (int)c->nh; }
+size_t vdo_cell_id(const vdo_cell* c) { return c->id; }
+
+void vdo_cell_export(const vdo_cell* c, double* verts, uint32_t* face_counts,
+                     uint32_t* face_indices, int32_t* face_neighbors) {
+  if (verts) memcpy(verts, c->v, 3 * c->nv * sizeof(double));
+  for (size_t f = 0; f < c->nf; ++f) {
+    if (face_counts) face_counts[f] = c->fc[f];
+    if (face_neighbors) face_neighbors[f] = c->fn[f];
+  }
+  if (face_indices)
+    for (size_t h = 0; h < c->nh; ++h) face_indices[h] = c->fi[h];
+}
+
+double vdo_cell_volume(const vdo_cell* c) { double v; cell_measure(c, &v, NULL, NULL); return v; }
+void vdo_cell_centroid(const vdo_cell* c, double out[3]) { cell_measure(c, NULL, out, NULL); }
+double vdo_cell_max_radius_sq(const vdo_cell* c, const double center[3]) { return cell_max_radius_sq(c, center); }
+
+double vdo_cell_face_area(const vdo_cell* c, size_t face) {
+  if (face >= c->nf) return 0.0;
+  size_t off = 0;
+  for (size_t f = 0; f < face; ++f) off += c->fc[f];
+  return face_area_at(c, off, c->fc[face]);
+}

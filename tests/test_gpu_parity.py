@@ -1,0 +1,225 @@
+"""GPU parity: the CUDA path through the C ABI against the oracle.
+
+The plain FP64 path performs the reference's arithmetic in the reference's
+order, so every per-cell result is compared for exact (bitwise) equality:
+volumes, centroids, face counts, neighbour ids in face order, face areas, the
+full polytope of sampled cells, and the algorithmic event counters.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from common import blobs, csr_lists, golden, uniform
+
+pytestmark = pytest.mark.gpu
+
+WALL = -1000
+
+
+def gpu_tess(bmin, bmax, grid, pts, walls=(), walls_first=False):
+    import vorothree_b200 as v
+    t = v.Tessellation(v.BoundingBox(bmin, bmax), v.Algorithm3DGrid(*grid))
+    if walls_first:
+        for w in walls:
+            t.add_wall(w)
+        t.set_generators(pts)
+    else:
+        t.set_generators(pts)
+        for w in walls:
+            t.add_wall(w)
+    t.calculate()
+    return t
+
+
+def oracle_tess(oracle_mod, bmin, bmax, grid, pts, walls=(), walls_first=False):
+    t = oracle_mod.OracleTessellation(bmin, bmax, *grid)
+
+    def add(w):
+        g = w.geometry
+        if hasattr(g, "radius"):
+            t.add_wall_sphere(g.center, g.radius, w.id())
+        else:
+            t.add_wall_plane(g.point, g.normal, w.id())
+    if walls_first:
+        for w in walls:
+            add(w)
+        t.set_generators(pts)
+    else:
+        t.set_generators(pts)
+        for w in walls:
+            add(w)
+    t.calculate()
+    return t
+
+
+def assert_same(g, o, check_counters=True, sample_cells=8):
+    assert g.count_generators() == o.count_generators()
+    assert g.count_cells() == o.count_cells()
+    assert np.array_equal(g.generators(), o.generators())
+    gv, gc, gn = g.summaries()
+    ov, oc, on = o.summaries()
+    assert np.array_equal(gn, on), np.nonzero(gn != on)[0][:10]
+    assert np.array_equal(gv, ov), np.nonzero(gv != ov)[0][:10]
+    assert np.array_equal(gc, oc)
+    goff, gids = g.neighbors()
+    ooff, oids = o.neighbors()
+    assert np.array_equal(goff, ooff)
+    assert np.array_equal(gids, oids)
+    _, gar = g.face_areas()
+    _, oar = o.face_areas()
+    assert np.array_equal(gar, oar)
+    if check_counters and sum(g.fallback_counts().values()) == 0:
+        assert g.counters() == o.counters()
+    n = g.count_cells()
+    for i in sorted(set(np.linspace(0, n - 1, min(n, sample_cells)).astype(int))):
+        gcell = g.get_cell(int(i))
+        ocell = o.get_cell(int(i))
+        ov_, ofc, ofi, ofn = ocell.export()
+        assert np.array_equal(gcell.vertices(), ov_)
+        assert np.array_equal(gcell.face_counts(), ofc)
+        assert np.array_equal(gcell.face_indices(), ofi)
+        assert np.array_equal(gcell.face_neighbors(), ofn)
+
+
+def test_known_answers():
+    import vorothree_b200 as v
+    t = gpu_tess([0, 0, 0], [100, 100, 100], (10, 10, 10), [10, 10, 10, 90, 90, 90])
+    vol, _, _ = t.summaries()
+    assert t.count_cells() == 2 and abs(vol.sum() - 1e6) < 1e-3
+    pts = np.asarray([[x, y, z] for x in (25, 75) for y in (25, 75) for z in (25, 75)], float)
+    t = gpu_tess([0, 0, 0], [100, 100, 100], (10, 10, 10), pts)
+    vol, _, _ = t.summaries()
+    assert np.all(np.abs(vol - 125000.0) < 1e-3)
+    pts = np.asarray([[x, y, z] for x in (0.25, 0.75) for y in (0.25, 0.75) for z in (0.25, 0.75)])
+    t = v.Tessellation(v.BoundingBox([0, 0, 0], [1, 1, 1]), v.Algorithm3DGrid(4, 4, 4))
+    t.set_generators(pts)
+    assert t.map(lambda c: len(c.face_counts())) == [6] * 8
+    t = gpu_tess([0, 0, 0], [10, 10, 10], (1, 1, 1), [2.5, 5, 5, 7.5, 5, 5])
+    assert 1 in t.get_cell(0).face_neighbors() and 0 in t.get_cell(1).face_neighbors()
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_config_a_bitwise(oracle_mod, seed):
+    pts = uniform(1000, 0.0, 10.0, seed)
+    g = gpu_tess([0, 0, 0], [10, 10, 10], (10, 10, 10), pts)
+    o = oracle_tess(oracle_mod, [0, 0, 0], [10, 10, 10], (10, 10, 10), pts)
+    assert_same(g, o)
+    vol, _, _ = g.summaries()
+    assert abs(vol.sum() - 1000.0) < 1e-9 * 1000
+
+
+def test_voro_golden_through_gpu():
+    import vorothree_b200 as v
+    gf = golden("voro_face_counts.json")
+    t = gpu_tess(gf["bounds_min"], gf["bounds_max"], gf["grid"], np.asarray([r[1:] for r in gf["generators"]]))
+    _, _, nf = t.summaries()
+    exp = np.asarray([gf["face_counts"][str(r[0])] for r in gf["generators"]])
+    assert np.array_equal(nf, exp)
+    gv = golden("voro_vertex_positions.json")
+    w = gv["walls"][0]
+    t = gpu_tess(gv["bounds_min"], gv["bounds_max"], gv["grid"], np.asarray([r[1:] for r in gv["generators"]]),
+                 walls=[v.Wall(w["id"], v.SphereGeometry(w["center"], w["radius"]))], walls_first=True)
+    for cid, exp in gv["cells"].items():
+        vv = t.get_cell(int(cid)).vertices().reshape(-1, 3)
+        exp = np.asarray(exp)
+        assert len(vv) == len(exp)
+        for e in exp:
+            assert np.any(np.all(np.abs(vv - e) < 1e-4, axis=1))
+
+
+def test_walls_bitwise(oracle_mod):
+    import vorothree_b200 as v
+    pts = uniform(3000, 0.0, 30.0, 5)
+    walls = [v.Wall(WALL, v.SphereGeometry([15, 15, 15], 12.0)),
+             v.Wall(WALL - 1, v.PlaneGeometry([15, 15, 15], [1.0, 0.3, 0.0]))]
+    g = gpu_tess([0, 0, 0], [30, 30, 30], (8, 8, 8), pts, walls)
+    o = oracle_tess(oracle_mod, [0, 0, 0], [30, 30, 30], (8, 8, 8), pts, walls)
+    assert_same(g, o)
+
+
+def test_sphere_lattice_volume(oracle_mod):
+    import vorothree_b200 as v
+    n = 20
+    step = 10.0 / n
+    pts = np.asarray([[x * step + step / 2, y * step + step / 2, z * step + step / 2]
+                      for x in range(n) for y in range(n) for z in range(n)])
+    walls = [v.Wall(WALL, v.SphereGeometry([5, 5, 5], 4.0))]
+    g = gpu_tess([0, 0, 0], [10, 10, 10], (5, 5, 5), pts, walls)
+    o = oracle_tess(oracle_mod, [0, 0, 0], [10, 10, 10], (5, 5, 5), pts, walls)
+    assert_same(g, o)
+    vol, _, _ = g.summaries()
+    exp = 4.0 / 3.0 * math.pi * 64.0
+    assert abs(vol.sum() - exp) / exp < 0.01
+
+
+def test_blobs_bitwise(oracle_mod):
+    import vorothree_b200 as v
+    pts = blobs(20000, 8, 0.01, 0.7, 11)
+    walls = [v.Wall(WALL, v.SphereGeometry([0.5, 0.5, 0.5], 0.45))]
+    g = gpu_tess([0, 0, 0], [1, 1, 1], (20, 20, 20), pts, walls)
+    o = oracle_tess(oracle_mod, [0, 0, 0], [1, 1, 1], (20, 20, 20), pts, walls)
+    assert_same(g, o)
+
+
+def test_uniform_100k_bitwise(oracle_mod):
+    pts = uniform(100_000, 0.0, 1.0, 3)
+    g = gpu_tess([0, 0, 0], [1, 1, 1], (46, 46, 46), pts)
+    o = oracle_tess(oracle_mod, [0, 0, 0], [1, 1, 1], (46, 46, 46), pts)
+    assert_same(g, o)
+
+
+def test_edge_cases(oracle_mod):
+    import vorothree_b200 as v
+    # empty input
+    t = gpu_tess([0, 0, 0], [1, 1, 1], (3, 3, 3), np.zeros((0, 3)))
+    assert t.count_cells() == 0 and t.total_faces() == 0
+    # single generator: the whole box
+    t = gpu_tess([0, 0, 0], [2, 3, 4], (3, 3, 3), [0.5, 0.5, 0.5])
+    vol, cen, nf = t.summaries()
+    assert vol[0] == 24.0 and nf[0] == 6
+    # duplicate generators and points outside the box (kept, as in the reference)
+    pts = np.concatenate([uniform(200, 0, 1, 9), uniform(5, 0, 1, 9), [[1.5, 0.5, 0.5], [-0.2, 0.1, 0.3]]])
+    g = gpu_tess([0, 0, 0], [1, 1, 1], (4, 4, 4), pts)
+    o = oracle_tess(oracle_mod, [0, 0, 0], [1, 1, 1], (4, 4, 4), pts)
+    assert_same(g, o)
+    # a wall that removes everything
+    walls = [v.Wall(WALL, v.SphereGeometry([5, 5, 5], 0.1))]
+    t = gpu_tess([0, 0, 0], [1, 1, 1], (2, 2, 2), uniform(50, 0, 1, 1), walls)
+    assert t.count_generators() == 0
+
+
+def test_relax_bitwise(oracle_mod):
+    import vorothree_b200 as v
+    pts = uniform(2000, 0.0, 1.0, 4)
+    walls = [v.Wall(WALL, v.SphereGeometry([0.5, 0.5, 0.5], 0.48))]
+    g = gpu_tess([0, 0, 0], [1, 1, 1], (12, 12, 12), pts, walls)
+    o = oracle_tess(oracle_mod, [0, 0, 0], [1, 1, 1], (12, 12, 12), pts, walls)
+    for _ in range(3):
+        g.relax()
+        o.relax()
+        g.calculate()
+        o.calculate()
+        assert_same(g, o, sample_cells=2)
+
+
+def test_table_extension(oracle_mod):
+    # a large grid (truncated search order) with few generators: cells must
+    # walk far and the table is extended on demand
+    pts = uniform(300, 0.0, 1.0, 6)
+    g = gpu_tess([0, 0, 0], [1, 1, 1], (80, 80, 80), pts)
+    o = oracle_tess(oracle_mod, [0, 0, 0], [1, 1, 1], (80, 80, 80), pts)
+    assert g.fallback_counts()["table"] > 0
+    assert_same(g, o, check_counters=False)
+
+
+def test_set_generator_moves_bin(oracle_mod):
+    import vorothree_b200 as v
+    pts = uniform(500, 0.0, 1.0, 8)
+    t = v.Tessellation(v.BoundingBox([0, 0, 0], [1, 1, 1]), v.Algorithm3DGrid(5, 5, 5))
+    t.set_generators(pts)
+    t.set_generator(3, [0.91, 0.92, 0.93])
+    t.calculate()
+    assert np.allclose(t.get_generator(3), [0.91, 0.92, 0.93])
+    vol, _, _ = t.summaries()
+    assert abs(vol.sum() - 1.0) < 1e-9

@@ -1,0 +1,14 @@
+"""vorothree_b200 -- B200-native 3D Voronoi tessellation.
+
+A GPU drop-in for the reference crate ``voronoid``'s 3D path
+(Tessellation::calculate over Algorithm3DGrid + Cell3DFaces, with plane and
+sphere walls).  The work runs in hand-written sm_100a CUDA kernels behind a C
+ABI (include/voronoid_b200.h); this package is the Python mirror of the
+reference's API over that ABI.
+"""
+from ._lib import VoronoidError, load
+from .tessellation import (WALL_ID_MAX, Algorithm3DGrid, BoundingBox, Cell3DFaces, PlaneGeometry,
+                           SphereGeometry, Tessellation, Wall, box_side)
+
+__all__ = ["Algorithm3DGrid", "BoundingBox", "Cell3DFaces", "PlaneGeometry", "SphereGeometry",
+           "Tessellation", "Wall", "WALL_ID_MAX", "box_side", "VoronoidError", "load"]

@@ -1,0 +1,96 @@
+"""ctypes binding of libvoronoid_b200.so (the C ABI in include/voronoid_b200.h).
+
+The library is loaded from this package directory.  There is no CPU
+fallback: if the library is missing, or no CUDA device is usable, every
+compute call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libvoronoid_b200.so")
+
+VD_OK = 0
+VD_EINVAL = 1
+VD_ENOMEM = 2
+VD_EOVERFLOW = 3
+VD_ETIMEOUT = 4
+VD_ECUDA = 5
+VD_ESTATE = 6
+VD_PREC_FP64 = 0
+VD_PREC_MIXED = 1
+
+STATUS_NAMES = {VD_EINVAL: "VD_EINVAL", VD_ENOMEM: "VD_ENOMEM", VD_EOVERFLOW: "VD_EOVERFLOW",
+                VD_ETIMEOUT: "VD_ETIMEOUT", VD_ECUDA: "VD_ECUDA", VD_ESTATE: "VD_ESTATE"}
+
+# every symbol the header declares, with its ctypes signature
+_d = C.POINTER(C.c_double)
+_vp = C.c_void_p
+_i32p = C.POINTER(C.c_int32)
+_i64p = C.POINTER(C.c_int64)
+_u32p = C.POINTER(C.c_uint32)
+_u64p = C.POINTER(C.c_uint64)
+_szp = C.POINTER(C.c_size_t)
+SIGNATURES = {
+    "vd_tess_create": (C.c_int, [_d, _d, C.c_int, C.c_int, C.c_int, C.POINTER(_vp)]),
+    "vd_tess_destroy": (C.c_int, [_vp]),
+    "vd_last_error": (C.c_char_p, [_vp]),
+    "vd_tess_add_wall_plane": (C.c_int, [_vp, _d, _d, C.c_int]),
+    "vd_tess_add_wall_sphere": (C.c_int, [_vp, _d, C.c_double, C.c_int]),
+    "vd_tess_clear_walls": (C.c_int, [_vp]),
+    "vd_tess_set_generators": (C.c_int, [_vp, _d, C.c_size_t, _szp]),
+    "vd_tess_set_generators_device": (C.c_int, [_vp, _vp, C.c_size_t, _szp]),
+    "vd_tess_set_generator": (C.c_int, [_vp, C.c_size_t, _d]),
+    "vd_tess_count_generators": (C.c_int, [_vp, _szp]),
+    "vd_tess_get_generators": (C.c_int, [_vp, _d]),
+    "vd_tess_set_precision": (C.c_int, [_vp, C.c_int]),
+    "vd_tess_calculate": (C.c_int, [_vp]),
+    "vd_tess_relax": (C.c_int, [_vp]),
+    "vd_tess_count_cells": (C.c_int, [_vp, _szp]),
+    "vd_tess_get_cell_summaries": (C.c_int, [_vp, _vp, _vp, _vp]),
+    "vd_tess_total_faces": (C.c_int, [_vp, _i64p]),
+    "vd_tess_get_neighbors": (C.c_int, [_vp, _vp, _vp]),
+    "vd_tess_get_face_areas": (C.c_int, [_vp, _vp, _vp]),
+    "vd_tess_get_cell": (C.c_int, [_vp, C.c_size_t, _i32p, _i32p, _i32p, _vp, _vp, _vp, _vp]),
+    "vd_tess_device_results": (C.c_int, [_vp, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp)]),
+    "vd_tess_stream": (C.c_int, [_vp, C.POINTER(_vp)]),
+    "vd_tess_timings": (C.c_int, [_vp, C.POINTER(C.c_float)]),
+    "vd_tess_counters": (C.c_int, [_vp, _u64p]),
+    "vd_tess_fallback_counts": (C.c_int, [_vp, _u64p]),
+    "vd_host_alloc": (C.c_int, [C.c_size_t, C.POINTER(_vp)]),
+    "vd_host_free": (C.c_int, [_vp]),
+    "vd_measure_fma_peak": (C.c_int, [C.c_int, _d]),
+}
+
+_lib = None
+
+
+class VoronoidError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{STATUS_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+def load():
+    """Load the library (building it first if this checkout has nvcc)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        from . import build as _build
+        _build.build()
+    L = C.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+def check(rc: int, handle=None):
+    if rc != VD_OK:
+        msg = load().vd_last_error(handle)
+        raise VoronoidError(rc, msg.decode() if msg else "")

@@ -1,0 +1,796 @@
+// vd_clip.cuh -- warp-per-cell Voronoi cell construction (FP64, bit-exact path).
+//
+// One warp owns one cell.  The convex polytope (vertex list + face loops, the
+// layout of Cell3DFaces, cell_3d_faces.rs:24-34) lives in a per-warp
+// WarpPoly: shared memory on the fast path, a global-memory slice on the
+// large-capacity pass.  Every step of Cell3DFaces::clip_with_scratch
+// (cell_3d_faces.rs:288-503) is done warp-parallel but produces exactly the
+// reference's output order:
+//   * vertex classification: one vertex per lane, ballots give all-in/all-out;
+//   * kept vertices: ballot-compacted in their original order;
+//   * crossing edges: ballot-compacted in face-walk order; the first
+//     occurrence of each (min,max) edge key (match.any) creates the
+//     intersection vertex, later ones reuse it -- the reference's
+//     intersection_map semantics, including its numbering;
+//   * face rewiring: per-position emit counts (0/1/2) and a warp scan give
+//     every surviving entry its slot; faces with < 3 entries are dropped;
+//   * the lid: segments between consecutive intersection vertices, a
+//     last-writer-wins lid_map, and one lane following the chain.
+// Arithmetic is written in the reference's evaluation order; the translation
+// unit is compiled with -fmad=false so no multiply-add is fused, and division
+// and square root are IEEE correctly rounded, so every double equals the
+// reference's.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "vd_common.cuh"
+
+namespace vd {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+template <int V, int F, int H, int CC, int NC, int SC, typename VIdT, typename FIdT>
+struct PolyCfg {
+  static constexpr int VCAP = V;   // vertices
+  static constexpr int FCAP = F;   // faces
+  static constexpr int HCAP = H;   // flattened face-index entries
+  static constexpr int CCAP = CC;  // crossing positions per clip
+  static constexpr int NCAP = NC;  // new (intersection) vertices per clip
+  static constexpr int SCAP = SC;  // lid segments per clip
+  using VId = VIdT;
+  using FId = FIdT;
+  static constexpr unsigned VNONE = (unsigned)(VIdT)~(VIdT)0;
+  static constexpr unsigned FNONE = (unsigned)(FIdT)~(FIdT)0;
+  static_assert(V < (int)VNONE, "vertex ids must leave room for the none marker");
+  static_assert(F < (int)FNONE, "face ids must leave room for the none marker");
+};
+
+// Fast path: sized from the oracle's distribution (max 72 vertices, 38 faces,
+// 216 face entries over 7.5M uniform-input polytopes); anything larger goes
+// to the large-capacity pass.
+using FastCfg = PolyCfg<96, 48, 288, 64, 40, 32, uint8_t, uint8_t>;
+// Large-capacity pass (global-memory storage): vertex ids stay u16 like the
+// reference's face_indices (cell_3d_faces.rs:31).
+using BigCfg = PolyCfg<2048, 512, 6144, 1024, 512, 512, uint16_t, uint16_t>;
+
+template <class C>
+struct alignas(16) WarpPoly {
+  double vx[C::VCAP], vy[C::VCAP], vz[C::VCAP];
+  double dist[C::VCAP];
+  double tx[C::NCAP], ty[C::NCAP], tz[C::NCAP];
+  unsigned long long cnt[kNumCounters];
+  int32_t fn[2][C::FCAP];
+  uint32_t ckey[C::CCAP];
+  uint16_t E[C::HCAP + 1];
+  uint16_t fs[2][C::FCAP + 1];
+  uint16_t fns[C::FCAP];
+  uint16_t cpos[C::CCAP];
+  typename C::VId cid[C::CCAP];
+  typename C::VId fi[2][C::HCAP];
+  typename C::FId pf[2][C::HCAP];
+  typename C::FId fnew[C::FCAP];
+  typename C::VId o2n[C::VCAP];
+  typename C::VId lidmap[C::VCAP];
+  typename C::VId sega[C::SCAP], segb[C::SCAP];
+};
+
+struct PolyState {
+  int nv, nf, nh, cb;
+};
+
+__device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
+
+__device__ __forceinline__ int warp_incl_scan(int x) {
+  const unsigned lane = lane_id();
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(kFull, x, o);
+    if ((int)lane >= o) x += y;
+  }
+  return x;
+}
+
+__device__ __forceinline__ double warp_max(double x) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) x = fmax(x, __shfl_xor_sync(kFull, x, o));
+  return x;
+}
+
+__device__ __forceinline__ double clamp01(double t) {
+  // f64::clamp(0.0, 1.0); NaN passes through
+  if (t < 0.0) return 0.0;
+  if (t > 1.0) return 1.0;
+  return t;
+}
+
+template <class C>
+__device__ __forceinline__ void cnt_add(WarpPoly<C>& P, int k, unsigned long long v) {
+  if (lane_id() == 0) P.cnt[k] += v;
+}
+
+// Cell3DFaces::new (cell_3d_faces.rs:37-74): the box, faces z-, z+, y-, y+,
+// x-, x+ with ids box_side (bounds/mod.rs:21-22).
+template <class C>
+__device__ void poly_init_box(WarpPoly<C>& P, PolyState& S, const Grid& g) {
+  const unsigned lane = lane_id();
+  if (lane < 8) {
+    const unsigned hx = (lane == 1 || lane == 2 || lane == 5 || lane == 6);
+    const unsigned hy = (lane == 2 || lane == 3 || lane == 6 || lane == 7);
+    const unsigned hz = lane >= 4;
+    P.vx[lane] = hx ? g.bmax[0] : g.bmin[0];
+    P.vy[lane] = hy ? g.bmax[1] : g.bmin[1];
+    P.vz[lane] = hz ? g.bmax[2] : g.bmin[2];
+  }
+  // face loops 3210 4567 0154 2376 0473 1265 packed as nibbles, lane = entry
+  if (lane < 24) {
+    const unsigned long long lo = 0x6732451076540123ull, hi = 0x56213740ull;
+    const unsigned idx = (unsigned)((lane < 16 ? lo >> (4 * lane) : hi >> (4 * (lane - 16))) & 0xFull);
+    P.fi[0][lane] = (typename C::VId)idx;
+    P.pf[0][lane] = (typename C::FId)(lane >> 2);
+  }
+  if (lane < 7) P.fs[0][lane] = (uint16_t)(4 * lane);
+  // face ids z-, z+, y-, y+, x-, x+ = box_side(axis, is_max) = -1 - (2*axis + is_max)
+  if (lane < 6) P.fn[0][lane] = -1 - (2 * (2 - (int)(lane >> 1)) + (int)(lane & 1));
+  S.nv = 8;
+  S.nf = 6;
+  S.nh = 24;
+  S.cb = 0;
+  __syncwarp();
+}
+
+// max_radius_sq (cell_3d_faces.rs:271-286)
+template <class C>
+__device__ double poly_max_radius_sq(const WarpPoly<C>& P, const PolyState& S, double gx, double gy,
+                                     double gz) {
+  double m = 0.0;
+  for (int v = lane_id(); v < S.nv; v += 32) {
+    double dx = P.vx[v] - gx;
+    double dy = P.vy[v] - gy;
+    double dz = P.vz[v] - gz;
+    double d2 = dx * dx + dy * dy + dz * dz;
+    m = fmax(m, d2);
+  }
+  return warp_max(m);
+}
+
+// clip_with_scratch (cell_3d_faces.rs:288-503).  All lanes call it with the
+// same (uniform) arguments.  *r2 gets the max squared distance of the new
+// vertex set from (gx,gy,gz) when with_gen, else 0.
+template <class C>
+__device__ int warp_clip(WarpPoly<C>& P, PolyState& S, double px, double py, double pz, double nx,
+                         double ny, double nz, int nbr, bool with_gen, double gx, double gy, double gz,
+                         double* r2out) {
+  using VId = typename C::VId;
+  using FId = typename C::FId;
+  const unsigned lane = lane_id();
+  const unsigned lt = (1u << lane) - 1u;
+  const int nv = S.nv, nf = S.nf, nh = S.nh, cb = S.cb, nb = cb ^ 1;
+  cnt_add(P, kCntClips, 1);
+  cnt_add(P, kCntClassified, (unsigned long long)nv);
+
+  // 1. signed distances and the 3-band flags (:302-326)
+  bool out = false, sin = false;
+  for (int v = lane; v < nv; v += 32) {
+    double d = (P.vx[v] - px) * nx + (P.vy[v] - py) * ny + (P.vz[v] - pz) * nz;
+    P.dist[v] = d;
+    out |= d > kTol;
+    sin |= d < -kTol;
+  }
+  if (!__any_sync(kFull, out)) {
+    *r2out = 0.0;
+    return kClipNoop;
+  }
+  if (!__any_sync(kFull, sin)) {
+    S.nv = S.nf = S.nh = 0;
+    *r2out = 0.0;
+    return kClipEmpty;
+  }
+  cnt_add(P, kCntModifying, 1);
+  __syncwarp();
+
+  // 2. keep the inside vertices in order (:344-362)
+  int nkept = 0;
+  double r2 = 0.0;
+  for (int b = 0; b < nv; b += 32) {
+    const int v = b + lane;
+    const bool k = v < nv && P.dist[v] <= kTol;
+    const unsigned m = __ballot_sync(kFull, k);
+    if (v < nv) P.o2n[v] = k ? (VId)(nkept + __popc(m & lt)) : (VId)C::VNONE;
+    if (k && with_gen) {
+      double dx = P.vx[v] - gx;
+      double dy = P.vy[v] - gy;
+      double dz = P.vz[v] - gz;
+      double d2 = dx * dx + dy * dy + dz * dz;
+      r2 = fmax(r2, d2);
+    }
+    nkept += __popc(m);
+  }
+  if (with_gen) cnt_add(P, kCntKept, (unsigned long long)nkept);
+
+  // 3. crossing positions of the face walk, in walk order (:369-452)
+  int ncross = 0;
+  for (int b = 0; b < nh; b += 32) {
+    const int p = b + lane;
+    bool cr = false;
+    unsigned s = 0, e = 0;
+    if (p < nh) {
+      const int f = P.pf[cb][p];
+      const int q = (p + 1 == P.fs[cb][f + 1]) ? P.fs[cb][f] : p + 1;
+      s = P.fi[cb][p];
+      e = P.fi[cb][q];
+      cr = (P.dist[s] <= kTol) != (P.dist[e] <= kTol);
+    }
+    const unsigned m = __ballot_sync(kFull, cr);
+    if (cr) {
+      const int k = ncross + __popc(m & lt);
+      if (k < C::CCAP) {
+        P.cpos[k] = (uint16_t)p;
+        P.ckey[k] = s < e ? (s << 16 | e) : (e << 16 | s);
+      }
+    }
+    ncross += __popc(m);
+  }
+  if (ncross > C::CCAP) return kClipOverflow;
+  __syncwarp();
+
+  // 4. intersection vertices: first occurrence of an edge key creates the
+  //    vertex (numbered in discovery order after the kept ones), repeats reuse
+  //    it (the intersection_map lookups of :391-417 / :422-448)
+  int nnew = 0;
+  for (int b = 0; b < ncross; b += 32) {
+    const int k = b + lane;
+    const bool act = k < ncross;
+    const unsigned key = act ? P.ckey[k] : (0xFFFF0000u | lane);
+    const unsigned mm = __match_any_sync(kFull, key);
+    const int leader = __ffs(mm) - 1;
+    const bool isleader = act && leader == (int)lane;
+    int id = -1;
+    if (isleader && b > 0) {
+      for (int j = 0; j < b; ++j)
+        if (P.ckey[j] == key) {
+          id = P.cid[j];
+          break;
+        }
+    }
+    const bool disc = isleader && id < 0;
+    const unsigned dm = __ballot_sync(kFull, disc);
+    if (disc) id = nkept + nnew + __popc(dm & lt);
+    id = __shfl_sync(kFull, id, leader);
+    if (act) P.cid[k] = (VId)id;
+    if (disc) {
+      const int r = id - nkept;
+      if (r < C::NCAP) {
+        const int p = P.cpos[k];
+        const int f = P.pf[cb][p];
+        const int q = (p + 1 == P.fs[cb][f + 1]) ? P.fs[cb][f] : p + 1;
+        const int s = P.fi[cb][p], e = P.fi[cb][q];
+        const double ds = P.dist[s], de = P.dist[e];
+        const double t = clamp01(ds / (ds - de));
+        const double ax = P.vx[s], ay = P.vy[s], az = P.vz[s];
+        const double bx = P.vx[e], by = P.vy[e], bz = P.vz[e];
+        const double ix = ax + t * (bx - ax);
+        const double iy = ay + t * (by - ay);
+        const double iz = az + t * (bz - az);
+        P.tx[r] = ix;
+        P.ty[r] = iy;
+        P.tz[r] = iz;
+        if (with_gen) {
+          double dx = ix - gx;
+          double dy = iy - gy;
+          double dz = iz - gz;
+          double d2 = dx * dx + dy * dy + dz * dz;
+          r2 = fmax(r2, d2);
+        }
+      }
+    }
+    nnew += __popc(dm);
+    __syncwarp();
+  }
+  cnt_add(P, kCntIntersections, (unsigned long long)nnew);
+  const int nvn = nkept + nnew;
+  if (nnew > C::NCAP || nvn > C::VCAP) return kClipOverflow;
+
+  // 5. new vertex list: kept vertices compacted in place, then intersections
+  for (int b = 0; b < nv; b += 32) {
+    const int v = b + lane;
+    unsigned o = C::VNONE;
+    double x = 0.0, y = 0.0, z = 0.0;
+    if (v < nv) {
+      o = P.o2n[v];
+      x = P.vx[v];
+      y = P.vy[v];
+      z = P.vz[v];
+    }
+    __syncwarp();
+    if (o != C::VNONE) {
+      P.vx[o] = x;
+      P.vy[o] = y;
+      P.vz[o] = z;
+    }
+    __syncwarp();
+  }
+  for (int r = lane; r < nnew; r += 32) {
+    P.vx[nkept + r] = P.tx[r];
+    P.vy[nkept + r] = P.ty[r];
+    P.vz[nkept + r] = P.tz[r];
+  }
+
+  // 6. rewire faces.  Emit per position: in->in 1 (end), in->out 1 (X),
+  //    out->in 2 (X, end), out->out 0.  E = exclusive prefix of emits.
+  {
+    int run = 0;
+    for (int b = 0; b < nh; b += 32) {
+      const int p = b + lane;
+      int em = 0;
+      if (p < nh) {
+        const int f = P.pf[cb][p];
+        const int q = (p + 1 == P.fs[cb][f + 1]) ? P.fs[cb][f] : p + 1;
+        const bool si = P.dist[P.fi[cb][p]] <= kTol;
+        const bool ei = P.dist[P.fi[cb][q]] <= kTol;
+        em = si ? 1 : (ei ? 2 : 0);
+      }
+      const int inc = warp_incl_scan(em);
+      if (p < nh) P.E[p] = (uint16_t)(run + inc - em);
+      run += __shfl_sync(kFull, inc, 31);
+    }
+    if (lane == 0) P.E[nh] = (uint16_t)run;
+  }
+  __syncwarp();
+  int nfk = 0, hk = 0;
+  bool longface = false;
+  for (int b = 0; b < nf; b += 32) {
+    const int f = b + lane;
+    int L = 0;
+    if (f < nf) L = (int)P.E[P.fs[cb][f + 1]] - (int)P.E[P.fs[cb][f]];
+    const bool kept = L >= 3;
+    longface |= L > 255;  // the reference stores face sizes as u8
+    const unsigned km = __ballot_sync(kFull, kept);
+    const int Lk = kept ? L : 0;
+    const int inc = warp_incl_scan(Lk);
+    if (f < nf) {
+      P.fnew[f] = kept ? (FId)(nfk + __popc(km & lt)) : (FId)C::FNONE;
+      P.fns[f] = (uint16_t)(hk + inc - Lk);
+    }
+    nfk += __popc(km);
+    hk += __shfl_sync(kFull, inc, 31);
+  }
+  if (__any_sync(kFull, longface) || hk > C::HCAP) return kClipOverflow;
+  __syncwarp();
+  {
+    int crun = 0;
+    for (int b = 0; b < nh; b += 32) {
+      const int p = b + lane;
+      bool si = false, ei = false, cr = false;
+      int f = 0, e = 0;
+      if (p < nh) {
+        f = P.pf[cb][p];
+        const int q = (p + 1 == P.fs[cb][f + 1]) ? P.fs[cb][f] : p + 1;
+        e = P.fi[cb][q];
+        si = P.dist[P.fi[cb][p]] <= kTol;
+        ei = P.dist[e] <= kTol;
+        cr = si != ei;
+      }
+      const unsigned m = __ballot_sync(kFull, cr);
+      const int kc = crun + __popc(m & lt);
+      crun += __popc(m);
+      if (p < nh) {
+        const unsigned fw = P.fnew[f];
+        if (fw != C::FNONE) {
+          const int o = P.fns[f] + ((int)P.E[p] - (int)P.E[P.fs[cb][f]]);
+          if (si) {
+            P.fi[nb][o] = ei ? P.o2n[e] : P.cid[kc];
+            P.pf[nb][o] = (FId)fw;
+          } else if (ei) {
+            P.fi[nb][o] = P.cid[kc];
+            P.pf[nb][o] = (FId)fw;
+            P.fi[nb][o + 1] = P.o2n[e];
+            P.pf[nb][o + 1] = (FId)fw;
+          }
+        }
+      }
+    }
+  }
+  for (int f = lane; f < nf; f += 32) {
+    const unsigned fw = P.fnew[f];
+    if (fw != C::FNONE) {
+      P.fs[nb][fw] = P.fns[f];
+      P.fn[nb][fw] = P.fn[cb][f];
+    }
+  }
+  if (lane == 0) P.fs[nb][nfk] = (uint16_t)hk;
+  __syncwarp();
+
+  // 7. lid (:454-495): segments (v,u) between consecutive intersection
+  //    vertices of the new faces, in order; lid_map last writer wins; the
+  //    chain from the first segment becomes the last face.
+  int nseg = 0;
+  for (int b = 0; b < hk; b += 32) {
+    const int q = b + lane;
+    bool sg = false;
+    unsigned u = 0, v = 0;
+    if (q < hk) {
+      const int f2 = P.pf[nb][q];
+      const int q2 = (q + 1 == P.fs[nb][f2 + 1]) ? P.fs[nb][f2] : q + 1;
+      u = P.fi[nb][q];
+      v = P.fi[nb][q2];
+      sg = (int)u >= nkept && (int)v >= nkept;
+    }
+    const unsigned m = __ballot_sync(kFull, sg);
+    if (sg) {
+      const int k = nseg + __popc(m & lt);
+      if (k < C::SCAP) {
+        P.sega[k] = (VId)v;
+        P.segb[k] = (VId)u;
+      }
+    }
+    nseg += __popc(m);
+  }
+  if (nseg > C::SCAP) return kClipOverflow;
+  int nhn = hk, nfn = nfk;
+  if (nseg > 0) {
+    __syncwarp();
+    for (int v = nkept + lane; v < nvn; v += 32) P.lidmap[v] = (VId)C::VNONE;
+    __syncwarp();
+    for (int b = 0; b < nseg; b += 32) {
+      const int k = b + lane;
+      const bool act = k < nseg;
+      const unsigned key = act ? (unsigned)P.sega[k] : (0xFFFF0000u | lane);
+      const unsigned mm = __match_any_sync(kFull, key);
+      const int last = 31 - __clz(mm);
+      if (act && last == (int)lane) P.lidmap[key] = P.segb[k];
+      __syncwarp();
+    }
+    int len = 0, ovf = 0;
+    if (lane == 0) {
+      const unsigned start = P.sega[0];
+      unsigned cur = P.segb[0];
+      if (hk < C::HCAP) {
+        P.fi[nb][hk] = (VId)start;
+        len = 1;
+        while (cur != start && len <= nseg) {
+          if (hk + len >= C::HCAP) {
+            ovf = 1;
+            break;
+          }
+          P.fi[nb][hk + len] = (VId)cur;
+          ++len;
+          cur = P.lidmap[cur];
+          if (cur == C::VNONE) break;
+        }
+      } else {
+        ovf = 1;
+      }
+    }
+    len = __shfl_sync(kFull, len, 0);
+    ovf = __shfl_sync(kFull, ovf, 0);
+    if (ovf) return kClipOverflow;
+    if (len >= 3) {
+      if (nfk + 1 > C::FCAP || len > 255) return kClipOverflow;
+      for (int q = lane; q < len; q += 32) P.pf[nb][hk + q] = (FId)nfk;
+      if (lane == 0) {
+        P.fs[nb][nfk] = (uint16_t)hk;
+        P.fn[nb][nfk] = nbr;
+        P.fs[nb][nfk + 1] = (uint16_t)(hk + len);
+      }
+      nhn = hk + len;
+      nfn = nfk + 1;
+    }
+  }
+  __syncwarp();
+  S.nv = nvn;
+  S.nf = nfn;
+  S.nh = nhn;
+  S.cb = nb;
+  *r2out = with_gen ? warp_max(r2) : 0.0;
+  return kClipMod;
+}
+
+// Wall::cut for the two wall kinds (wall_3d.rs:37-41, :80-100).  Returns
+// false when the wall emits no plane (sphere centre == generator).
+__device__ __forceinline__ bool wall_plane(const Wall& w, double gx, double gy, double gz, double* p,
+                                           double* n) {
+  if (w.kind == 0) {
+    p[0] = w.a[0];
+    p[1] = w.a[1];
+    p[2] = w.a[2];
+    n[0] = -w.n[0];
+    n[1] = -w.n[1];
+    n[2] = -w.n[2];
+    return true;
+  }
+  const double dx = gx - w.a[0], dy = gy - w.a[1], dz = gz - w.a[2];
+  const double dist = sqrt(dx * dx + dy * dy + dz * dz);
+  if (dist == 0.0) return false;
+  const double scale = w.r / dist;
+  p[0] = w.a[0] + dx * scale;
+  p[1] = w.a[1] + dy * scale;
+  p[2] = w.a[2] + dz * scale;
+  n[0] = dx / dist;
+  n[1] = dy / dist;
+  n[2] = dz / dist;
+  return true;
+}
+
+// compute_cell (tessellation.rs:414-475) with Algorithm3DGrid::visit_neighbors
+// (algo_3d_grid.rs:145-202) and the bisector visitor (tessellation.rs:446-471).
+//
+// The search order is consumed 32 entries at a time: each lane decodes one
+// entry (bin, exact bin lower bound, member range).  Ballots against the
+// CURRENT radius then pick, in order, exactly the entries the reference
+// visits: the first entry with min_d2 > 4R^2 ends the walk, and only bins
+// whose bound is <= 4R^2 are opened -- re-evaluated after every clip that
+// changes R.  Members of an opened bin are loaded by the lanes together and
+// visited in ascending id order.
+template <class C>
+__device__ int compute_cell(const TessDesc& T, uint32_t i, WarpPoly<C>& P, PolyState& S) {
+  const unsigned lane = lane_id();
+  const double gx = T.gen[3 * (size_t)i], gy = T.gen[3 * (size_t)i + 1], gz = T.gen[3 * (size_t)i + 2];
+  double r2;
+  poly_init_box(P, S, T.grid);
+  for (int w = 0; w < T.nwalls; ++w) {
+    double p[3], n[3];
+    if (wall_plane(T.walls[w], gx, gy, gz, p, n)) {
+      const int r = warp_clip(P, S, p[0], p[1], p[2], n[0], n[1], n[2], T.walls[w].id, false, gx, gy,
+                              gz, &r2);
+      if (r == kClipOverflow) return kCellOverflow;
+    }
+    if (S.nv == 0) return kCellOk;
+  }
+  double cur = poly_max_radius_sq(P, S, gx, gy, gz);
+
+  const Grid& G = T.grid;
+  const uint32_t bin = T.bin_of[i];
+  const uint32_t nxy = (uint32_t)G.n[0] * (uint32_t)G.n[1];
+  const int iz = (int)(bin / nxy);
+  const uint32_t rem = bin % nxy;
+  const int iy = (int)(rem / (uint32_t)G.n[0]);
+  const int ix = (int)(rem % (uint32_t)G.n[0]);
+  const double rx = (gx - G.bmin[0]) * G.scale[0] - (double)ix;
+  const double ry = (gy - G.bmin[1]) * G.scale[1] - (double)iy;
+  const double rz = (gz - G.bmin[2]) * G.scale[2] - (double)iz;
+
+  bool done = false;
+  for (int base = 0; base < T.norder && !done; base += 32) {
+    const int k = base + (int)lane;
+    const bool valid = k < T.norder;
+    double md2 = 0.0, b2 = 0.0;
+    bool inr = false;
+    uint32_t bs = 0, be = 0;
+    if (valid) {
+      const Offset o = T.order[k];
+      md2 = o.min_d2;
+      const int bx = ix + o.dx, by = iy + o.dy, bz = iz + o.dz;
+      inr = bx >= 0 && bx < G.n[0] && by >= 0 && by < G.n[1] && bz >= 0 && bz < G.n[2];
+      if (inr) {
+        const double ddx = o.dx > 0 ? ((double)o.dx - rx) * G.cs[0]
+                                    : (o.dx < 0 ? ((double)(-(o.dx + 1)) + rx) * G.cs[0] : 0.0);
+        const double ddy = o.dy > 0 ? ((double)o.dy - ry) * G.cs[1]
+                                    : (o.dy < 0 ? ((double)(-(o.dy + 1)) + ry) * G.cs[1] : 0.0);
+        const double ddz = o.dz > 0 ? ((double)o.dz - rz) * G.cs[2]
+                                    : (o.dz < 0 ? ((double)(-(o.dz + 1)) + rz) * G.cs[2] : 0.0);
+        const double bdx = fmax(ddx, 0.0), bdy = fmax(ddy, 0.0), bdz = fmax(ddz, 0.0);
+        b2 = bdx * bdx + bdy * bdy + bdz * bdz;
+        const uint32_t bb = (uint32_t)bx + (uint32_t)by * (uint32_t)G.n[0] + (uint32_t)bz * nxy;
+        bs = T.bin_start[bb];
+        be = T.bin_start[bb + 1];
+      }
+    }
+    const int nvalid = min(32, T.norder - base);
+    int pos = 0;
+    while (true) {
+      const double c4 = 4.0 * cur;
+      const unsigned ge = pos >= 32 ? 0u : ~((1u << pos) - 1u);
+      const unsigned brk = __ballot_sync(kFull, valid && md2 > c4) & ge;
+      unsigned pass = __ballot_sync(kFull, valid && inr && !(md2 > c4) && b2 <= c4 && be > bs) & ge;
+      if (brk) {
+        const int fb = __ffs(brk) - 1;
+        pass &= (1u << fb) - 1u;
+        if (!pass) {
+          cnt_add(P, kCntOffsets, (unsigned long long)(fb + 1));
+          done = true;
+          break;
+        }
+      }
+      if (!pass) {
+        cnt_add(P, kCntOffsets, (unsigned long long)nvalid);
+        break;
+      }
+      const int l = __ffs(pass) - 1;
+      const uint32_t s0 = __shfl_sync(kFull, bs, l);
+      const uint32_t s1 = __shfl_sync(kFull, be, l);
+      for (uint32_t mb = s0; mb < s1; mb += 32) {
+        SortedGen sg = {0.0, 0.0, 0.0, -1};
+        if (mb + lane < s1) sg = T.sorted[mb + lane];
+        const int cntm = (int)min(32u, s1 - mb);
+        for (int j = 0; j < cntm; ++j) {
+          const long long jid = __shfl_sync(kFull, sg.id, j);
+          if (jid == (long long)i) continue;
+          const double qx = __shfl_sync(kFull, sg.x, j);
+          const double qy = __shfl_sync(kFull, sg.y, j);
+          const double qz = __shfl_sync(kFull, sg.z, j);
+          cnt_add(P, kCntCandidates, 1);
+          const double d0 = qx - gx, d1 = qy - gy, d2 = qz - gz;
+          const double dist_sq = d0 * d0 + d1 * d1 + d2 * d2;
+          if (dist_sq > 4.0 * cur) continue;
+          const double mx = gx + d0 * 0.5, my = gy + d1 * 0.5, mz = gz + d2 * 0.5;
+          const int r = warp_clip(P, S, mx, my, mz, d0, d1, d2, (int)jid, true, gx, gy, gz, &r2);
+          if (r == kClipOverflow) return kCellOverflow;
+          if (r == kClipMod) cur = r2;
+          else if (r == kClipEmpty) cur = 0.0;
+        }
+      }
+      pos = l + 1;
+      if (pos >= 32) {
+        cnt_add(P, kCntOffsets, (unsigned long long)nvalid);
+        break;
+      }
+    }
+  }
+  if (!done && !T.order_complete && !(T.order_bound > 4.0 * cur)) return kCellTable;
+  return kCellOk;
+}
+
+// volume + centroid (cell_3d_faces.rs:106-205) summed in the reference's
+// order, and face_area (:207-254) per face; writes the cell's outputs.
+template <class C>
+__device__ void finalize_cell(const TessDesc& T, uint32_t i, WarpPoly<C>& P, const PolyState& S) {
+  const unsigned lane = lane_id();
+  const int cb = S.cb, nb = cb ^ 1;
+  const int nf = S.nf;
+  // triangle prefix over faces; triangle -> face map in the spare buffer
+  int ntri = 0;
+  for (int b = 0; b < nf; b += 32) {
+    const int f = b + lane;
+    int t = 0;
+    if (f < nf) {
+      const int c = (int)P.fs[cb][f + 1] - (int)P.fs[cb][f];
+      t = c >= 3 ? c - 2 : 0;
+    }
+    const int inc = warp_incl_scan(t);
+    if (f < nf) P.E[f] = (uint16_t)(ntri + inc - t);
+    ntri += __shfl_sync(kFull, inc, 31);
+  }
+  __syncwarp();
+  for (int f = lane; f < nf; f += 32) {
+    const int c = (int)P.fs[cb][f + 1] - (int)P.fs[cb][f];
+    for (int j = 0; j < c - 2; ++j) P.pf[nb][P.E[f] + j] = (typename C::FId)f;
+  }
+  __syncwarp();
+  double av = 0.0, ax = 0.0, ay = 0.0, az = 0.0;
+  for (int b = 0; b < ntri; b += 32) {
+    const int t = b + lane;
+    double det = 0.0, dtx = 0.0, dty = 0.0, dtz = 0.0;
+    if (t < ntri) {
+      const int f = P.pf[nb][t];
+      const int base = P.fs[cb][f];
+      const int j = t - (int)P.E[f] + 1;
+      const int i0 = P.fi[cb][base], i1 = P.fi[cb][base + j], i2 = P.fi[cb][base + j + 1];
+      const double v0x = P.vx[i0], v0y = P.vy[i0], v0z = P.vz[i0];
+      const double v1x = P.vx[i1], v1y = P.vy[i1], v1z = P.vz[i1];
+      const double v2x = P.vx[i2], v2y = P.vy[i2], v2z = P.vz[i2];
+      const double crx = v1y * v2z - v1z * v2y;
+      const double cry = v1z * v2x - v1x * v2z;
+      const double crz = v1x * v2y - v1y * v2x;
+      det = v0x * crx + v0y * cry + v0z * crz;
+      dtx = det * (v0x + v1x + v2x);
+      dty = det * (v0y + v1y + v2y);
+      dtz = det * (v0z + v1z + v2z);
+    }
+    const int cntt = min(32, ntri - b);
+    for (int j = 0; j < cntt; ++j) {
+      av += __shfl_sync(kFull, det, j);
+      ax += __shfl_sync(kFull, dtx, j);
+      ay += __shfl_sync(kFull, dty, j);
+      az += __shfl_sync(kFull, dtz, j);
+    }
+  }
+  cnt_add(P, kCntTriangles, (unsigned long long)ntri);
+  const int fout = T.fout;
+  int32_t* fnb_out = nullptr;
+  double* far_out = nullptr;
+  if (nf <= fout) {
+    fnb_out = T.fnb + (size_t)i * fout;
+    far_out = T.farea + (size_t)i * fout;
+  } else if (T.pool_cursor) {
+    unsigned long long off = 0;
+    if (lane == 0) off = atomicAdd(T.pool_cursor, (unsigned long long)nf);
+    off = __shfl_sync(kFull, off, 0);
+    if ((long long)(off + nf) <= T.pool_cap) {
+      fnb_out = T.pool_fnb + off;
+      far_out = T.pool_farea + off;
+      if (lane == 0) T.pool_off[i] = (long long)off;
+    }
+  }
+  for (int f = lane; f < nf; f += 32) {
+    const int base = P.fs[cb][f];
+    const int c = (int)P.fs[cb][f + 1] - base;
+    double area = 0.0;
+    if (c >= 3) {
+      const int p0 = P.fi[cb][base];
+      const double p0x = P.vx[p0], p0y = P.vy[p0], p0z = P.vz[p0];
+      for (int j = 1; j < c - 1; ++j) {
+        const int p1 = P.fi[cb][base + j], p2 = P.fi[cb][base + j + 1];
+        const double v1x = P.vx[p1] - p0x, v1y = P.vy[p1] - p0y, v1z = P.vz[p1] - p0z;
+        const double v2x = P.vx[p2] - p0x, v2y = P.vy[p2] - p0y, v2z = P.vz[p2] - p0z;
+        const double crx = v1y * v2z - v1z * v2y;
+        const double cry = v1z * v2x - v1x * v2z;
+        const double crz = v1x * v2y - v1y * v2x;
+        area += 0.5 * sqrt(crx * crx + cry * cry + crz * crz);
+      }
+    }
+    if (fnb_out) {
+      fnb_out[f] = P.fn[cb][f];
+      far_out[f] = area;
+    }
+  }
+  if (lane == 0) {
+    T.vol[i] = fabs(av / 6.0);
+    if (fabs(av) < 1e-9) {
+      T.cen[3 * (size_t)i] = 0.0;
+      T.cen[3 * (size_t)i + 1] = 0.0;
+      T.cen[3 * (size_t)i + 2] = 0.0;
+    } else {
+      const double factor = 1.0 / (4.0 * av);
+      T.cen[3 * (size_t)i] = ax * factor;
+      T.cen[3 * (size_t)i + 1] = ay * factor;
+      T.cen[3 * (size_t)i + 2] = az * factor;
+    }
+    T.nfaces[i] = (fnb_out || nf == 0) ? nf : -1;
+    T.nverts[i] = S.nv;
+    T.status[i] = (fnb_out || nf == 0) ? kCellOk : kCellHardFail;
+  }
+}
+
+template <class C>
+__device__ void export_cell(const WorkList& W, const WarpPoly<C>& P, const PolyState& S) {
+  const unsigned lane = lane_id();
+  if (lane == 0) {
+    W.ex_sizes[0] = S.nv;
+    W.ex_sizes[1] = S.nf;
+    W.ex_sizes[2] = S.nh;
+  }
+  if (S.nv <= W.ex_cap_v)
+    for (int v = lane; v < S.nv; v += 32) {
+      W.ex_verts[3 * v] = P.vx[v];
+      W.ex_verts[3 * v + 1] = P.vy[v];
+      W.ex_verts[3 * v + 2] = P.vz[v];
+    }
+  if (S.nf <= W.ex_cap_f)
+    for (int f = lane; f < S.nf; f += 32) {
+      W.ex_fc[f] = (uint32_t)(P.fs[S.cb][f + 1] - P.fs[S.cb][f]);
+      W.ex_fn[f] = P.fn[S.cb][f];
+    }
+  if (S.nh <= W.ex_cap_h)
+    for (int h = lane; h < S.nh; h += 32) W.ex_fi[h] = P.fi[S.cb][h];
+}
+
+// Persistent warps pull cells from the work list and build them.
+template <class C>
+__device__ void clip_worker(const TessDesc& T, const WorkList& W, WarpPoly<C>& P) {
+  const unsigned lane = lane_id();
+  if (lane < kNumCounters) P.cnt[lane] = 0;
+  __syncwarp();
+  while (true) {
+    unsigned idx = 0;
+    if (lane == 0) idx = atomicAdd(W.cursor, 1u);
+    idx = __shfl_sync(kFull, idx, 0);
+    if (idx >= W.nitems) break;
+    const uint32_t cell = W.items ? W.items[idx] : (uint32_t)T.sorted[idx].id;
+    PolyState S;
+    const int st = compute_cell<C>(T, cell, P, S);
+    if (st == kCellOk) {
+      finalize_cell<C>(T, cell, P, S);
+      if (W.ex_verts) export_cell<C>(W, P, S);
+    } else if (lane == 0) {
+      T.status[cell] = (uint8_t)st;
+      if (st == kCellOverflow && W.ovf_list) W.ovf_list[atomicAdd(W.ovf_count, 1u)] = cell;
+      if (st == kCellTable && W.tab_list) W.tab_list[atomicAdd(W.tab_count, 1u)] = cell;
+    }
+    __syncwarp();
+  }
+  __syncwarp();
+  if (lane < kNumCounters && W.counters) atomicAdd(&W.counters[lane], P.cnt[lane]);
+}
+
+}  // namespace vd

@@ -1,0 +1,118 @@
+// vd_common.cuh -- device-side data layout shared by the tessellation kernels.
+//
+// One tessellation on the device (HBM):
+//   gen        double[3N]   generators, AoS, in the caller's order (index = cell id)
+//   bin_of     u32[N]       bin of each generator (Algorithm3DGrid::generator_bin_ids)
+//   bin_start  u32[B+1]     CSR of the bins; members ascending by generator id
+//                           (Vec<Vec<usize>> grid_bins with push order, algo_3d_grid.rs:121-129)
+//   sorted     SortedGen[N] generators in bin order (x, y, z, id), 32 B each, so a
+//                           bin's members are one contiguous, aligned read
+//   order      Offset[M]    shell search order (algo_3d_grid.rs:56-76), 16 B each
+//   per-cell outputs: volume, centroid, face count, status, and per-face
+//   neighbour ids and areas in fixed slots of FOUT faces per cell.
+#pragma once
+#include <cstdint>
+
+namespace vd {
+
+constexpr int kMaxWalls = 16;
+constexpr double kTol = 1e-9;  // cell_3d_faces.rs:310-315,346,383-384
+
+enum CellStatus : uint8_t {
+  kCellOk = 0,
+  kCellOverflow = 1,   // polytope exceeded the fast-path capacities
+  kCellTable = 2,      // walked past the end of a truncated search order
+  kCellHardFail = 3,   // exceeded even the large capacities
+};
+
+enum ClipResult : int { kClipNoop = 0, kClipMod = 1, kClipEmpty = 2, kClipOverflow = -1 };
+
+enum Counter : int {
+  kCntCandidates = 0,
+  kCntClips,
+  kCntClassified,
+  kCntModifying,
+  kCntIntersections,
+  kCntKept,
+  kCntTriangles,
+  kCntOffsets,
+  kNumCounters
+};
+
+struct Grid {
+  double bmin[3], bmax[3];
+  int n[3];
+  double scale[3];  // grid_scale = n / extent
+  double limit[3];  // grid_limit = n - 1e-5
+  double cs[3];     // cell size = 1 / grid_scale
+};
+
+struct Wall {
+  int kind;  // 0 plane, 1 sphere
+  int id;
+  double a[3];  // plane point / sphere centre
+  double n[3];  // plane normal, normalised, pointing into the valid region
+  double r;     // sphere radius
+};
+
+struct alignas(16) Offset {
+  int16_t dx, dy, dz, pad;
+  double min_d2;
+};
+
+struct alignas(32) SortedGen {
+  double x, y, z;
+  long long id;
+};
+
+// Everything a clip kernel needs for one tessellation.
+struct TessDesc {
+  Grid grid;
+  int nwalls;
+  Wall walls[kMaxWalls];
+  const Offset* order;
+  int norder;
+  int order_complete;   // 1 when order holds every offset of the grid
+  double order_bound;   // truncated table: every missing entry has min_d2 >= this
+  const double* gen;
+  const uint32_t* bin_of;
+  const uint32_t* bin_start;
+  const SortedGen* sorted;
+  uint32_t ncells;
+  // outputs
+  double* vol;
+  double* cen;
+  int32_t* nfaces;
+  int32_t* nverts;     // vertex count (0 = empty cell, Cell::is_empty)
+  int32_t* fnb;        // [ncells * fout]
+  double* farea;       // [ncells * fout]
+  uint8_t* status;
+  int fout;
+  // faces of cells with more than fout faces (large-capacity pass only)
+  int32_t* pool_fnb;
+  double* pool_farea;
+  long long* pool_off;  // per cell; valid when nfaces > fout
+  unsigned long long* pool_cursor;
+  long long pool_cap;
+};
+
+// Work description of one launch of a clip kernel.
+struct WorkList {
+  const uint32_t* items;     // cell ids; nullptr = sorted order over all cells
+  uint32_t nitems;
+  unsigned int* cursor;      // persistent-warp work counter
+  uint32_t* ovf_list;        // cells that overflowed the capacities
+  unsigned int* ovf_count;
+  uint32_t* tab_list;        // cells that ran off a truncated search order
+  unsigned int* tab_count;
+  unsigned long long* counters;  // kNumCounters
+  // optional full-polytope export of a single cell (get_cell)
+  double* ex_verts;
+  uint32_t* ex_fc;
+  uint32_t* ex_fi;
+  int32_t* ex_fn;
+  int32_t* ex_sizes;  // nv, nf, nh
+  int ex_cap_v, ex_cap_f, ex_cap_h;
+};
+
+}  // namespace vd

@@ -1,0 +1,985 @@
+// vd_host.cu -- host side of the C ABI (include/voronoid_b200.h).
+//
+// A vd_tess owns one CUDA stream and every device buffer of one
+// tessellation: the generators, their bins, the search order, and the
+// per-cell outputs.  Data stays resident in HBM between calls; the host only
+// sees it through the result getters.
+//
+// Compiled with -fmad=false: the host-side wall normalisation and the
+// device-side wall tests and bin indices must round exactly like the
+// reference.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <string>
+#include <vector>
+
+#include "../../include/voronoid_b200.h"
+#include "vd_binning.cuh"
+#include "vd_internal.h"
+
+using namespace vd;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+template <typename T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t cap = 0;  // elements
+  cudaError_t ensure(size_t n) {
+    if (n <= cap && p) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    const size_t want = std::max<size_t>(n, 1);
+    cudaError_t e = cudaMalloc(&p, want * sizeof(T));
+    if (e == cudaSuccess) cap = want;
+    else p = nullptr;
+    return e;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+  }
+};
+
+// offsets of the small device-side control block
+enum : int {
+  kCtlCursor = 0,
+  kCtlOvfCount,
+  kCtlTabCount,
+  kCtlBigCount,
+  kCtlWords = 8,
+};
+
+}  // namespace
+
+struct vd_tess {
+  std::string err;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  Grid grid{};
+  std::vector<Wall> walls;
+  int precision = VD_PREC_FP64;
+
+  // search order
+  int order_k = 0;
+  bool order_complete = false;
+  double order_bound = 0.0;
+  int norder = 0;
+  DevBuf<Offset> d_order;
+
+  // generators and bins
+  size_t ngen = 0;
+  size_t nbins = 0;
+  DevBuf<double> d_gen, d_in, d_tmp3;
+  DevBuf<uint32_t> d_flags, d_pos;
+  DevBuf<uint32_t> d_bin_of, d_bin_count, d_bin_start, d_cursor, d_ids, d_ids_tmp, d_big_list;
+  DevBuf<SortedGen> d_sorted;
+
+  // outputs
+  size_t ncells = 0;
+  bool calculated = false;
+  int fout = 48;
+  DevBuf<double> d_vol, d_cen, d_pool_area, d_csr_area;
+  DevBuf<int32_t> d_nf, d_nv, d_fnb, d_pool_fnb, d_csr_ids;
+  DevBuf<double> d_farea;
+  DevBuf<uint8_t> d_status;
+  DevBuf<long long> d_pool_off, d_csr_off, d_nf64;
+  bool csr_valid = false;
+  long long csr_total = 0;
+
+  // control
+  DevBuf<unsigned int> d_ctl;
+  DevBuf<unsigned long long> d_counters, d_pool_cursor;
+  DevBuf<uint32_t> d_list[3];
+  DevBuf<unsigned char> d_big;
+  size_t big_warps = 0;
+  long long pool_cap = 0;
+
+  // scan scratch
+  std::vector<DevBuf<uint32_t>> scan32;
+  std::vector<DevBuf<long long>> scan64;
+
+  // export buffers for get_cell
+  DevBuf<double> d_ex_v;
+  DevBuf<uint32_t> d_ex_fc, d_ex_fi;
+  DevBuf<int32_t> d_ex_fn, d_ex_sizes;
+
+  // instrumentation
+  cudaEvent_t ev[8] = {};
+  float timings[4] = {0, 0, 0, 0};
+  unsigned long long counters[kNumCounters] = {};
+  unsigned long long fallback[2] = {0, 0};
+  ClipLaunchInfo info64{}, infomx{};
+  int num_sms = 0;
+};
+
+namespace {
+
+int fail(vd_tess* t, int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  if (t) t->err = buf;
+  else g_create_error = buf;
+  return code;
+}
+
+#define VD_CK(t, call)                                                                          \
+  do {                                                                                          \
+    cudaError_t e_ = (call);                                                                    \
+    if (e_ != cudaSuccess)                                                                      \
+      return fail((t), e_ == cudaErrorMemoryAllocation ? VD_ENOMEM : VD_ECUDA, "%s: %s (%s:%d)", \
+                  #call, cudaGetErrorString(e_), __FILE__, __LINE__);                            \
+  } while (0)
+
+int grid_blocks(const vd_tess* t, size_t n, int threads) {
+  const size_t want = (n + threads - 1) / threads;
+  const size_t cap = (size_t)std::max(1, t->num_sms) * 16;
+  return (int)std::max<size_t>(1, std::min(want, cap));
+}
+
+// exclusive scan of n values of `in` into out[0..n); out must hold n+1 and
+// gets the total at out[n] when `with_total`.
+template <typename Tin, typename T>
+int scan_excl(vd_tess* t, const Tin* in, T* out, size_t n, std::vector<DevBuf<T>>& pool, int level = 0) {
+  if (n == 0) return VD_OK;
+  const size_t nt = (n + kScanTile - 1) / kScanTile;
+  if ((int)pool.size() <= level) pool.resize(level + 1);
+  VD_CK(t, pool[level].ensure(nt + 1));
+  T* sums = pool[level].p;
+  k_scan_tiles<Tin, T><<<(unsigned)nt, kScanThreads, 0, t->stream>>>(in, out, n, sums);
+  VD_CK(t, cudaGetLastError());
+  if (nt > 1) {
+    // scan the tile sums in place (needs its own level of scratch)
+    if ((int)pool.size() <= level + 1) pool.resize(level + 2);
+    VD_CK(t, pool[level + 1].ensure(nt + 1));
+    T* sscan = pool[level + 1].p;
+    int r = scan_excl<T, T>(t, sums, sscan, nt, pool, level + 2);
+    if (r != VD_OK) return r;
+    k_scan_add<T><<<(unsigned)nt, kScanThreads, 0, t->stream>>>(out, n, sscan);
+    VD_CK(t, cudaGetLastError());
+  }
+  return VD_OK;
+}
+
+// Algorithm3DGrid::new's search order (algo_3d_grid.rs:56-76): every offset
+// of [-n,n]^3 (z outer, x inner) with its min_d2, sorted by min_d2.  Ties
+// keep the enumeration order (a stable sort; the reference's unstable sort has
+// no reproducible tie order).  With k < n the table holds exactly the offsets
+// with min_d2 < bound, where bound = min over truncated axes of (k*cs)^2 is a
+// lower bound of min_d2 for every offset left out.
+void build_order(const Grid& g, int k, std::vector<Offset>& out, bool& complete, double& bound) {
+  int r[3];
+  complete = true;
+  bound = std::numeric_limits<double>::infinity();
+  for (int a = 0; a < 3; ++a) {
+    r[a] = std::min(k, g.n[a]);
+    if (r[a] < g.n[a]) {
+      complete = false;
+      const double m = (double)k * g.cs[a];
+      bound = std::min(bound, m * m);
+    }
+  }
+  struct E {
+    Offset o;
+    uint32_t lin;
+  };
+  std::vector<E> v;
+  v.reserve((size_t)(2 * r[0] + 1) * (2 * r[1] + 1) * (2 * r[2] + 1));
+  uint32_t lin = 0;
+  for (int z = -r[2]; z <= r[2]; ++z)
+    for (int y = -r[1]; y <= r[1]; ++y)
+      for (int x = -r[0]; x <= r[0]; ++x) {
+        const double mx = x > 0 ? (double)(x - 1) * g.cs[0] : (x < 0 ? (double)(-x - 1) * g.cs[0] : 0.0);
+        const double my = y > 0 ? (double)(y - 1) * g.cs[1] : (y < 0 ? (double)(-y - 1) * g.cs[1] : 0.0);
+        const double mz = z > 0 ? (double)(z - 1) * g.cs[2] : (z < 0 ? (double)(-z - 1) * g.cs[2] : 0.0);
+        const double d2 = mx * mx + my * my + mz * mz;
+        if (complete || d2 < bound) {
+          E e;
+          e.o.dx = (int16_t)x;
+          e.o.dy = (int16_t)y;
+          e.o.dz = (int16_t)z;
+          e.o.pad = 0;
+          e.o.min_d2 = d2;
+          e.lin = lin;
+          v.push_back(e);
+        }
+        ++lin;
+      }
+  std::stable_sort(v.begin(), v.end(), [](const E& a, const E& b) { return a.o.min_d2 < b.o.min_d2; });
+  out.resize(v.size());
+  for (size_t i = 0; i < v.size(); ++i) out[i] = v[i].o;
+}
+
+int upload_order(vd_tess* t, int k) {
+  std::vector<Offset> h;
+  bool complete;
+  double bound;
+  build_order(t->grid, k, h, complete, bound);
+  VD_CK(t, t->d_order.ensure(h.size()));
+  VD_CK(t, cudaMemcpyAsync(t->d_order.p, h.data(), h.size() * sizeof(Offset), cudaMemcpyHostToDevice, t->stream));
+  VD_CK(t, cudaStreamSynchronize(t->stream));
+  t->order_k = k;
+  t->order_complete = complete;
+  t->order_bound = bound;
+  t->norder = (int)h.size();
+  return VD_OK;
+}
+
+WallSet wallset(const vd_tess* t) {
+  WallSet ws;
+  memset(&ws, 0, sizeof(ws));
+  ws.n = (int)t->walls.size();
+  for (int i = 0; i < ws.n; ++i) ws.w[i] = t->walls[i];
+  return ws;
+}
+
+// Algorithm3DGrid::set_generators on the device: bin index, counting sort
+// with members in ascending id order, then the bin-ordered copy.
+int rebin(vd_tess* t) {
+  const size_t n = t->ngen, nb = t->nbins;
+  cudaStream_t s = t->stream;
+  VD_CK(t, t->d_bin_of.ensure(n));
+  VD_CK(t, t->d_bin_count.ensure(nb + 1));
+  VD_CK(t, t->d_bin_start.ensure(nb + 1));
+  VD_CK(t, t->d_cursor.ensure(nb + 1));
+  VD_CK(t, t->d_ids.ensure(n));
+  VD_CK(t, t->d_ids_tmp.ensure(n));
+  VD_CK(t, t->d_big_list.ensure(nb));
+  VD_CK(t, t->d_sorted.ensure(n));
+  VD_CK(t, t->d_ctl.ensure(kCtlWords));
+  VD_CK(t, cudaMemsetAsync(t->d_bin_count.p, 0, (nb + 1) * sizeof(uint32_t), s));
+  VD_CK(t, cudaMemsetAsync(t->d_ctl.p + kCtlBigCount, 0, sizeof(unsigned int), s));
+  if (n > 0) {
+    k_bin_count<<<grid_blocks(t, n, 256), 256, 0, s>>>(t->d_gen.p, n, t->grid, t->d_bin_of.p, t->d_bin_count.p);
+    VD_CK(t, cudaGetLastError());
+  }
+  int r = scan_excl<uint32_t, uint32_t>(t, t->d_bin_count.p, t->d_bin_start.p, nb + 1, t->scan32);
+  if (r != VD_OK) return r;
+  if (n > 0) {
+    VD_CK(t, cudaMemcpyAsync(t->d_cursor.p, t->d_bin_start.p, nb * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+    k_bin_scatter<<<grid_blocks(t, n, 256), 256, 0, s>>>(t->d_bin_of.p, n, t->d_cursor.p, t->d_ids.p);
+    VD_CK(t, cudaGetLastError());
+    k_bin_fix<<<grid_blocks(t, nb, 256), 256, 0, s>>>(t->d_bin_start.p, nb, t->d_ids.p, t->d_big_list.p,
+                                                       t->d_ctl.p + kCtlBigCount);
+    VD_CK(t, cudaGetLastError());
+    k_bin_sort_big<<<std::max(1, t->num_sms), kBigSortThreads, 0, s>>>(
+        t->d_bin_start.p, t->d_big_list.p, t->d_ctl.p + kCtlBigCount, t->d_ids.p, t->d_ids_tmp.p);
+    VD_CK(t, cudaGetLastError());
+    k_gather_sorted<<<grid_blocks(t, n, 256), 256, 0, s>>>(t->d_ids.p, t->d_gen.p, n, t->d_sorted.p);
+    VD_CK(t, cudaGetLastError());
+  }
+  t->calculated = false;
+  t->csr_valid = false;
+  return VD_OK;
+}
+
+// keep the rows of d_in inside every wall (stable), into d_gen
+int filter_into_gen(vd_tess* t, const double* d_src, size_t n, size_t* n_kept) {
+  cudaStream_t s = t->stream;
+  if (t->walls.empty()) {
+    VD_CK(t, t->d_gen.ensure(3 * n));
+    if (n && d_src != t->d_gen.p)
+      VD_CK(t, cudaMemcpyAsync(t->d_gen.p, d_src, 3 * n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    t->ngen = n;
+    if (n_kept) *n_kept = n;
+    return VD_OK;
+  }
+  VD_CK(t, t->d_flags.ensure(n + 1));
+  VD_CK(t, t->d_pos.ensure(n + 1));
+  VD_CK(t, t->d_tmp3.ensure(3 * n));
+  if (n) {
+    k_wall_flags<<<grid_blocks(t, n, 256), 256, 0, s>>>(d_src, n, wallset(t), t->d_flags.p);
+    VD_CK(t, cudaGetLastError());
+  }
+  VD_CK(t, cudaMemsetAsync(t->d_flags.p + n, 0, sizeof(uint32_t), s));
+  int r = scan_excl<uint32_t, uint32_t>(t, t->d_flags.p, t->d_pos.p, n + 1, t->scan32);
+  if (r != VD_OK) return r;
+  if (n) {
+    k_compact3<<<grid_blocks(t, n, 256), 256, 0, s>>>(d_src, n, t->d_flags.p, t->d_pos.p, t->d_tmp3.p);
+    VD_CK(t, cudaGetLastError());
+  }
+  uint32_t kept = 0;
+  VD_CK(t, cudaMemcpyAsync(&kept, t->d_pos.p + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  VD_CK(t, cudaStreamSynchronize(s));
+  std::swap(t->d_gen, t->d_tmp3);
+  t->ngen = kept;
+  if (n_kept) *n_kept = kept;
+  return VD_OK;
+}
+
+TessDesc make_desc(vd_tess* t) {
+  TessDesc T;
+  memset(&T, 0, sizeof(T));
+  T.grid = t->grid;
+  T.nwalls = (int)t->walls.size();
+  for (int i = 0; i < T.nwalls; ++i) T.walls[i] = t->walls[i];
+  T.order = t->d_order.p;
+  T.norder = t->norder;
+  T.order_complete = t->order_complete ? 1 : 0;
+  T.order_bound = t->order_bound;
+  T.gen = t->d_gen.p;
+  T.bin_of = t->d_bin_of.p;
+  T.bin_start = t->d_bin_start.p;
+  T.sorted = t->d_sorted.p;
+  T.ncells = (uint32_t)t->ngen;
+  T.vol = t->d_vol.p;
+  T.cen = t->d_cen.p;
+  T.nfaces = t->d_nf.p;
+  T.nverts = t->d_nv.p;
+  T.fnb = t->d_fnb.p;
+  T.farea = t->d_farea.p;
+  T.status = t->d_status.p;
+  T.fout = t->fout;
+  T.pool_fnb = t->d_pool_fnb.p;
+  T.pool_farea = t->d_pool_area.p;
+  T.pool_off = t->d_pool_off.p;
+  T.pool_cursor = t->d_pool_cursor.p;
+  T.pool_cap = t->pool_cap;
+  return T;
+}
+
+int ensure_outputs(vd_tess* t, size_t n) {
+  VD_CK(t, t->d_vol.ensure(n));
+  VD_CK(t, t->d_cen.ensure(3 * n));
+  VD_CK(t, t->d_nf.ensure(n));
+  VD_CK(t, t->d_nv.ensure(n));
+  VD_CK(t, t->d_fnb.ensure(n * (size_t)t->fout));
+  VD_CK(t, t->d_farea.ensure(n * (size_t)t->fout));
+  VD_CK(t, t->d_status.ensure(n));
+  VD_CK(t, t->d_pool_off.ensure(n));
+  VD_CK(t, t->d_ctl.ensure(kCtlWords));
+  VD_CK(t, t->d_counters.ensure(kNumCounters));
+  VD_CK(t, t->d_pool_cursor.ensure(1));
+  for (int k = 0; k < 3; ++k) VD_CK(t, t->d_list[k].ensure(n));
+  return VD_OK;
+}
+
+int ensure_big(vd_tess* t, size_t cells) {
+  // enough warps to spread the listed cells, capped to bound the scratch
+  // the big kernel runs 4 warps per block: scratch covers whole blocks
+  size_t want = std::min<size_t>(std::max<size_t>(cells, 1), (size_t)std::max(1, t->num_sms) * 4);
+  want = (want + 3) / 4 * 4;
+  if (t->big_warps < want) {
+    VD_CK(t, t->d_big.ensure(want * t->info64.big_scratch_per_warp));
+    t->big_warps = want;
+  }
+  if (t->pool_cap == 0) {
+    const long long cap = 1 << 20;
+    VD_CK(t, t->d_pool_fnb.ensure(cap));
+    VD_CK(t, t->d_pool_area.ensure(cap));
+    t->pool_cap = cap;
+  }
+  return VD_OK;
+}
+
+// one pass of the clip kernel over `items` (nullptr = all cells in bin order)
+int clip_pass(vd_tess* t, bool big, const uint32_t* items, uint32_t nitems, uint32_t* ovf_list,
+              uint32_t* tab_list, const WorkList* extra = nullptr) {
+  cudaStream_t s = t->stream;
+  VD_CK(t, cudaMemsetAsync(t->d_ctl.p, 0, 3 * sizeof(unsigned int), s));
+  WorkList W;
+  memset(&W, 0, sizeof(W));
+  if (extra) W = *extra;
+  W.items = items;
+  W.nitems = nitems;
+  W.cursor = t->d_ctl.p + kCtlCursor;
+  W.ovf_list = ovf_list;
+  W.ovf_count = t->d_ctl.p + kCtlOvfCount;
+  W.tab_list = tab_list;
+  W.tab_count = t->d_ctl.p + kCtlTabCount;
+  W.counters = t->d_counters.p;
+  TessDesc T = make_desc(t);
+  if (!big) {
+    const bool mixed = t->precision == VD_PREC_MIXED;
+    const ClipLaunchInfo& li = mixed ? t->infomx : t->info64;
+    const size_t warps_needed = (nitems + li.warps_per_block - 1) / li.warps_per_block;
+    const int nblocks = (int)std::max<size_t>(
+        1, std::min<size_t>(warps_needed, (size_t)t->num_sms * std::max(1, li.blocks_per_sm)));
+    VD_CK(t, mixed ? launch_clip_mixed_fast(T, W, nblocks, s) : launch_clip_fp64_fast(T, W, nblocks, s));
+  } else {
+    int r = ensure_big(t, nitems);
+    if (r != VD_OK) return r;
+    T = make_desc(t);
+    VD_CK(t, launch_clip_fp64_big(T, W, t->d_big.p, (int)t->big_warps, s));
+  }
+  return VD_OK;
+}
+
+int read_ctl(vd_tess* t, unsigned int* ovf, unsigned int* tab) {
+  unsigned int h[3];
+  VD_CK(t, cudaMemcpyAsync(h, t->d_ctl.p, sizeof(h), cudaMemcpyDeviceToHost, t->stream));
+  VD_CK(t, cudaStreamSynchronize(t->stream));
+  *ovf = h[kCtlOvfCount];
+  *tab = h[kCtlTabCount];
+  return VD_OK;
+}
+
+// Runs the fast pass over all cells, then resolves the cells it could not
+// finish: a longer search order for cells that walked off a truncated one,
+// the large-capacity pass for polytopes that outgrew shared memory.
+int run_calculate(vd_tess* t, const WorkList* extra = nullptr, const uint32_t* only_cell = nullptr) {
+  cudaStream_t s = t->stream;
+  const size_t n = t->ngen;
+  int r = ensure_outputs(t, n);
+  if (r != VD_OK) return r;
+  VD_CK(t, cudaMemsetAsync(t->d_counters.p, 0, kNumCounters * sizeof(unsigned long long), s));
+  VD_CK(t, cudaMemsetAsync(t->d_pool_cursor.p, 0, sizeof(unsigned long long), s));
+  t->fallback[0] = t->fallback[1] = 0;
+  VD_CK(t, cudaEventRecord(t->ev[2], s));
+  uint32_t* in_list = nullptr;
+  uint32_t nin = only_cell ? 1u : (uint32_t)n;
+  if (only_cell) {
+    VD_CK(t, cudaMemcpyAsync(t->d_list[2].p, only_cell, sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+    in_list = t->d_list[2].p;
+  }
+  if (nin > 0) {
+    r = clip_pass(t, false, in_list, nin, t->d_list[0].p, t->d_list[1].p, extra);
+    if (r != VD_OK) return r;
+  }
+  VD_CK(t, cudaEventRecord(t->ev[3], s));
+  unsigned int novf = 0, ntab = 0;
+  if (nin > 0) {
+    r = read_ctl(t, &novf, &ntab);
+    if (r != VD_OK) return r;
+  }
+  t->fallback[0] += novf;
+  t->fallback[1] += ntab;
+  // lists: [0] overflow, [1] table; [2] spare
+  for (int guard = 0; guard < 64 && (novf > 0 || ntab > 0); ++guard) {
+    if (ntab > 0) {
+      if (t->order_complete) return fail(t, VD_ECUDA, "search order exhausted on a complete table");
+      int k = std::max(1, t->order_k) * 2;
+      r = upload_order(t, k);
+      if (r != VD_OK) return r;
+      // rerun table cells; overflows go to a fresh list, appended after novf
+      std::swap(t->d_list[1], t->d_list[2]);
+      r = clip_pass(t, false, t->d_list[2].p, ntab, t->d_list[0].p + novf, t->d_list[1].p, extra);
+      if (r != VD_OK) return r;
+      unsigned int o2, t2;
+      r = read_ctl(t, &o2, &t2);
+      if (r != VD_OK) return r;
+      t->fallback[1] += t2;
+      t->fallback[0] += o2;
+      novf += o2;
+      ntab = t2;
+      continue;
+    }
+    if (novf > 0) {
+      std::swap(t->d_list[0], t->d_list[2]);
+      r = clip_pass(t, true, t->d_list[2].p, novf, t->d_list[0].p, t->d_list[1].p, extra);
+      if (r != VD_OK) return r;
+      unsigned int o2, t2;
+      r = read_ctl(t, &o2, &t2);
+      if (r != VD_OK) return r;
+      if (o2 > 0) return fail(t, VD_EOVERFLOW, "%u cells exceed the large polytope capacity", o2);
+      novf = 0;
+      ntab = t2;
+      t->fallback[1] += t2;
+    }
+  }
+  VD_CK(t, cudaEventRecord(t->ev[4], s));
+  VD_CK(t, cudaMemcpyAsync(t->counters, t->d_counters.p, sizeof(t->counters), cudaMemcpyDeviceToHost, s));
+  VD_CK(t, cudaStreamSynchronize(s));
+  float a = 0, b = 0;
+  cudaEventElapsedTime(&a, t->ev[2], t->ev[3]);
+  cudaEventElapsedTime(&b, t->ev[3], t->ev[4]);
+  t->timings[1] = a;
+  t->timings[2] = b;
+  t->timings[3] = t->timings[0] + a + b;
+  return VD_OK;
+}
+
+int ensure_csr(vd_tess* t) {
+  if (t->csr_valid) return VD_OK;
+  const size_t n = t->ncells;
+  cudaStream_t s = t->stream;
+  VD_CK(t, t->d_nf64.ensure(n + 1));
+  VD_CK(t, t->d_csr_off.ensure(n + 1));
+  if (n) {
+    k_nfaces_to_i64<<<grid_blocks(t, n, 256), 256, 0, s>>>(t->d_nf.p, n, t->d_nf64.p);
+    VD_CK(t, cudaGetLastError());
+  }
+  VD_CK(t, cudaMemsetAsync(t->d_nf64.p + n, 0, sizeof(long long), s));
+  int r = scan_excl<long long, long long>(t, t->d_nf64.p, t->d_csr_off.p, n + 1, t->scan64);
+  if (r != VD_OK) return r;
+  long long total = 0;
+  VD_CK(t, cudaMemcpyAsync(&total, t->d_csr_off.p + n, sizeof(long long), cudaMemcpyDeviceToHost, s));
+  VD_CK(t, cudaStreamSynchronize(s));
+  t->csr_total = total;
+  t->csr_valid = true;
+  return VD_OK;
+}
+
+int check_ready(vd_tess* t) {
+  if (!t) return VD_EINVAL;
+  if (!t->calculated) return fail(t, VD_ESTATE, "no results: call vd_tess_calculate first");
+  VD_CK(t, cudaSetDevice(t->device));
+  return VD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* vd_last_error(const vd_tess* t) { return t ? t->err.c_str() : g_create_error.c_str(); }
+
+int vd_tess_create(const double bmin[3], const double bmax[3], int nx, int ny, int nz, vd_tess** out) {
+  if (!out || !bmin || !bmax) return fail(nullptr, VD_EINVAL, "null argument");
+  *out = nullptr;
+  if (nx <= 0 || ny <= 0 || nz <= 0 || nx > 16000 || ny > 16000 || nz > 16000)
+    return fail(nullptr, VD_EINVAL, "grid resolution must be in [1, 16000]");
+  if ((double)nx * ny * nz > 2.0e9) return fail(nullptr, VD_EINVAL, "too many bins");
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return fail(nullptr, VD_ECUDA, "no CUDA device: %s", cudaGetErrorString(e));
+  vd_tess* t = new vd_tess();
+  t->device = dev;
+  cudaDeviceGetAttribute(&t->num_sms, cudaDevAttrMultiProcessorCount, dev);
+  e = cudaStreamCreateWithFlags(&t->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete t;
+    return fail(nullptr, VD_ECUDA, "cudaStreamCreate: %s", cudaGetErrorString(e));
+  }
+  for (auto& ev : t->ev) cudaEventCreate(&ev);
+  e = clip_fp64_info(&t->info64);
+  if (e == cudaSuccess) e = clip_mixed_info(&t->infomx);
+  if (e != cudaSuccess) {
+    const std::string m = cudaGetErrorString(e);
+    vd_tess_destroy(t);
+    return fail(nullptr, VD_ECUDA, "kernel setup: %s", m.c_str());
+  }
+  // Algorithm3DGrid::new (algo_3d_grid.rs:47-95)
+  Grid& g = t->grid;
+  const int n[3] = {nx, ny, nz};
+  for (int a = 0; a < 3; ++a) {
+    g.bmin[a] = bmin[a];
+    g.bmax[a] = bmax[a];
+    g.n[a] = n[a];
+    g.scale[a] = (double)n[a] / (bmax[a] - bmin[a]);
+    g.limit[a] = (double)n[a] - 1e-5;
+    g.cs[a] = 1.0 / g.scale[a];
+  }
+  t->nbins = (size_t)nx * ny * nz;
+  const double full = (2.0 * nx + 1) * (2.0 * ny + 1) * (2.0 * nz + 1);
+  int r = upload_order(t, full <= (double)(1 << 21) ? std::max(nx, std::max(ny, nz)) : 8);
+  if (r == VD_OK) r = rebin(t);
+  if (r != VD_OK) {
+    g_create_error = t->err;
+    vd_tess_destroy(t);
+    return r;
+  }
+  *out = t;
+  return VD_OK;
+}
+
+int vd_tess_destroy(vd_tess* t) {
+  if (!t) return VD_OK;
+  cudaSetDevice(t->device);
+  if (t->stream) cudaStreamSynchronize(t->stream);
+  t->d_order.release();
+  t->d_gen.release(); t->d_in.release(); t->d_tmp3.release();
+  t->d_flags.release(); t->d_pos.release();
+  t->d_bin_of.release(); t->d_bin_count.release(); t->d_bin_start.release(); t->d_cursor.release();
+  t->d_ids.release(); t->d_ids_tmp.release(); t->d_big_list.release(); t->d_sorted.release();
+  t->d_vol.release(); t->d_cen.release(); t->d_pool_area.release(); t->d_csr_area.release();
+  t->d_nf.release(); t->d_nv.release(); t->d_fnb.release(); t->d_pool_fnb.release(); t->d_csr_ids.release();
+  t->d_farea.release(); t->d_status.release(); t->d_pool_off.release(); t->d_csr_off.release();
+  t->d_nf64.release(); t->d_ctl.release(); t->d_counters.release(); t->d_pool_cursor.release();
+  for (auto& l : t->d_list) l.release();
+  t->d_big.release();
+  for (auto& b : t->scan32) b.release();
+  for (auto& b : t->scan64) b.release();
+  t->d_ex_v.release(); t->d_ex_fc.release(); t->d_ex_fi.release(); t->d_ex_fn.release(); t->d_ex_sizes.release();
+  for (auto& ev : t->ev)
+    if (ev) cudaEventDestroy(ev);
+  if (t->stream) cudaStreamDestroy(t->stream);
+  delete t;
+  return VD_OK;
+}
+
+static int add_wall(vd_tess* t, const Wall& w) {
+  if (w.id > VD_WALL_ID_MAX) return fail(t, VD_EINVAL, "Wall ID must be <= %d", VD_WALL_ID_MAX);
+  if ((int)t->walls.size() >= kMaxWalls) return fail(t, VD_EINVAL, "at most %d walls", kMaxWalls);
+  VD_CK(t, cudaSetDevice(t->device));
+  t->walls.push_back(w);
+  // prune_outside_generators (tessellation.rs:175-194)
+  if (t->ngen == 0) return VD_OK;
+  const size_t before = t->ngen;
+  size_t kept = 0;
+  int r = filter_into_gen(t, t->d_gen.p, before, &kept);
+  if (r != VD_OK) return r;
+  if (kept != before) return rebin(t);
+  return VD_OK;
+}
+
+int vd_tess_add_wall_plane(vd_tess* t, const double point[3], const double normal[3], int id) {
+  if (!t || !point || !normal) return VD_EINVAL;
+  Wall w;
+  memset(&w, 0, sizeof(w));
+  w.kind = 0;
+  w.id = id;
+  for (int a = 0; a < 3; ++a) w.a[a] = point[a];
+  // PlaneGeometry::new (wall_3d.rs:23-27)
+  const double len = std::sqrt(normal[0] * normal[0] + normal[1] * normal[1] + normal[2] * normal[2]);
+  if (len == 0.0) {
+    w.n[0] = 0.0;
+    w.n[1] = 0.0;
+    w.n[2] = 1.0;
+  } else {
+    for (int a = 0; a < 3; ++a) w.n[a] = normal[a] / len;
+  }
+  return add_wall(t, w);
+}
+
+int vd_tess_add_wall_sphere(vd_tess* t, const double center[3], double radius, int id) {
+  if (!t || !center) return VD_EINVAL;
+  Wall w;
+  memset(&w, 0, sizeof(w));
+  w.kind = 1;
+  w.id = id;
+  w.r = radius;
+  for (int a = 0; a < 3; ++a) w.a[a] = center[a];
+  return add_wall(t, w);
+}
+
+int vd_tess_clear_walls(vd_tess* t) {
+  if (!t) return VD_EINVAL;
+  t->walls.clear();
+  return VD_OK;
+}
+
+static int set_generators_from_device(vd_tess* t, const double* d_src, size_t n, size_t* n_kept) {
+  VD_CK(t, cudaEventRecord(t->ev[0], t->stream));
+  int r = filter_into_gen(t, d_src, n, n_kept);
+  if (r != VD_OK) return r;
+  r = rebin(t);
+  if (r != VD_OK) return r;
+  VD_CK(t, cudaEventRecord(t->ev[1], t->stream));
+  VD_CK(t, cudaEventSynchronize(t->ev[1]));
+  cudaEventElapsedTime(&t->timings[0], t->ev[0], t->ev[1]);
+  return VD_OK;
+}
+
+int vd_tess_set_generators(vd_tess* t, const double* xyz, size_t n, size_t* n_kept) {
+  if (!t || (!xyz && n)) return VD_EINVAL;
+  VD_CK(t, cudaSetDevice(t->device));
+  if (n > 0xFFFFFFF0ull / 3) return fail(t, VD_EINVAL, "too many generators");
+  // land the host copy in d_gen directly when no wall can drop rows
+  DevBuf<double>& dst = t->walls.empty() ? t->d_gen : t->d_in;
+  VD_CK(t, dst.ensure(3 * n));
+  if (n) VD_CK(t, cudaMemcpyAsync(dst.p, xyz, 3 * n * sizeof(double), cudaMemcpyHostToDevice, t->stream));
+  return set_generators_from_device(t, dst.p, n, n_kept);
+}
+
+int vd_tess_set_generators_device(vd_tess* t, const double* d_xyz, size_t n, size_t* n_kept) {
+  if (!t || (!d_xyz && n)) return VD_EINVAL;
+  VD_CK(t, cudaSetDevice(t->device));
+  if (n > 0xFFFFFFF0ull / 3) return fail(t, VD_EINVAL, "too many generators");
+  // the filter reads d_xyz and writes d_gen, so the caller's buffer is never modified
+  if (t->walls.empty()) {
+    VD_CK(t, t->d_gen.ensure(3 * n));
+    if (n)
+      VD_CK(t, cudaMemcpyAsync(t->d_gen.p, d_xyz, 3 * n * sizeof(double), cudaMemcpyDeviceToDevice, t->stream));
+    return set_generators_from_device(t, t->d_gen.p, n, n_kept);
+  }
+  return set_generators_from_device(t, d_xyz, n, n_kept);
+}
+
+// Tessellation::set_generator + Algorithm3DGrid::update_generator
+// (tessellation.rs:71-92, algo_3d_grid.rs:132-143).  The bin change uses the
+// reference's swap_remove/push, so in-bin order follows the reference's.
+int vd_tess_set_generator(vd_tess* t, size_t index, const double xyz[3]) {
+  if (!t || !xyz) return VD_EINVAL;
+  VD_CK(t, cudaSetDevice(t->device));
+  if (index >= t->ngen) return VD_OK;
+  for (const Wall& w : t->walls) {
+    const double dx = xyz[0] - w.a[0], dy = xyz[1] - w.a[1], dz = xyz[2] - w.a[2];
+    const bool in = w.kind == 0 ? (dx * w.n[0] + dy * w.n[1] + dz * w.n[2]) >= 0.0
+                                : (dx * dx + dy * dy + dz * dz) <= w.r * w.r;
+    if (!in) return VD_OK;
+  }
+  cudaStream_t s = t->stream;
+  const size_t n = t->ngen, nb = t->nbins;
+  std::vector<uint32_t> start(nb + 1), ids(n), bin_of(n);
+  VD_CK(t, cudaMemcpyAsync(start.data(), t->d_bin_start.p, (nb + 1) * 4, cudaMemcpyDeviceToHost, s));
+  VD_CK(t, cudaMemcpyAsync(ids.data(), t->d_ids.p, n * 4, cudaMemcpyDeviceToHost, s));
+  VD_CK(t, cudaMemcpyAsync(bin_of.data(), t->d_bin_of.p, n * 4, cudaMemcpyDeviceToHost, s));
+  VD_CK(t, cudaStreamSynchronize(s));
+  const Grid& g = t->grid;
+  auto axis = [](double v, double lo, double sc, double lim) -> uint32_t {
+    double u = (v - lo) * sc;
+    if (u < 0.0) u = 0.0;
+    if (u > lim) u = lim;
+    return u > 0.0 ? (uint32_t)u : 0u;
+  };
+  const uint32_t nbin = axis(xyz[0], g.bmin[0], g.scale[0], g.limit[0]) +
+                        axis(xyz[1], g.bmin[1], g.scale[1], g.limit[1]) * (uint32_t)g.n[0] +
+                        axis(xyz[2], g.bmin[2], g.scale[2], g.limit[2]) * (uint32_t)g.n[0] * (uint32_t)g.n[1];
+  const uint32_t obin = bin_of[index];
+  if (nbin != obin) {
+    std::vector<std::vector<uint32_t>> bins(nb);
+    for (size_t b = 0; b < nb; ++b) bins[b].assign(ids.begin() + start[b], ids.begin() + start[b + 1]);
+    auto& ob = bins[obin];
+    for (size_t k = 0; k < ob.size(); ++k)
+      if (ob[k] == index) {
+        ob[k] = ob.back();  // swap_remove
+        ob.pop_back();
+        break;
+      }
+    bins[nbin].push_back((uint32_t)index);
+    bin_of[index] = nbin;
+    size_t o = 0;
+    for (size_t b = 0; b < nb; ++b) {
+      start[b] = (uint32_t)o;
+      for (uint32_t v : bins[b]) ids[o++] = v;
+    }
+    start[nb] = (uint32_t)o;
+    VD_CK(t, cudaMemcpyAsync(t->d_bin_start.p, start.data(), (nb + 1) * 4, cudaMemcpyHostToDevice, s));
+    VD_CK(t, cudaMemcpyAsync(t->d_ids.p, ids.data(), n * 4, cudaMemcpyHostToDevice, s));
+    VD_CK(t, cudaMemcpyAsync(t->d_bin_of.p, bin_of.data(), n * 4, cudaMemcpyHostToDevice, s));
+  }
+  VD_CK(t, cudaMemcpyAsync(t->d_gen.p + 3 * index, xyz, 3 * sizeof(double), cudaMemcpyHostToDevice, s));
+  k_gather_sorted<<<grid_blocks(t, n, 256), 256, 0, s>>>(t->d_ids.p, t->d_gen.p, n, t->d_sorted.p);
+  VD_CK(t, cudaGetLastError());
+  VD_CK(t, cudaStreamSynchronize(s));
+  t->calculated = false;
+  t->csr_valid = false;
+  return VD_OK;
+}
+
+int vd_tess_count_generators(const vd_tess* t, size_t* n) {
+  if (!t || !n) return VD_EINVAL;
+  *n = t->ngen;
+  return VD_OK;
+}
+
+int vd_tess_get_generators(vd_tess* t, double* xyz) {
+  if (!t || (!xyz && t->ngen)) return VD_EINVAL;
+  VD_CK(t, cudaSetDevice(t->device));
+  if (t->ngen)
+    VD_CK(t, cudaMemcpyAsync(xyz, t->d_gen.p, 3 * t->ngen * sizeof(double), cudaMemcpyDeviceToHost, t->stream));
+  VD_CK(t, cudaStreamSynchronize(t->stream));
+  return VD_OK;
+}
+
+int vd_tess_set_precision(vd_tess* t, int precision) {
+  if (!t) return VD_EINVAL;
+  if (precision != VD_PREC_FP64 && precision != VD_PREC_MIXED) return fail(t, VD_EINVAL, "unknown precision");
+  t->precision = precision;
+  return VD_OK;
+}
+
+int vd_tess_calculate(vd_tess* t) {
+  if (!t) return VD_EINVAL;
+  VD_CK(t, cudaSetDevice(t->device));
+  t->calculated = false;
+  t->csr_valid = false;
+  int r = run_calculate(t);
+  if (r != VD_OK) return r;
+  t->ncells = t->ngen;
+  t->calculated = true;
+  return VD_OK;
+}
+
+int vd_tess_relax(vd_tess* t) {
+  int r = check_ready(t);
+  if (r != VD_OK) return r;
+  const size_t n = std::min(t->ncells, t->ngen);
+  VD_CK(t, t->d_in.ensure(3 * n));
+  if (n) {
+    k_relax<<<grid_blocks(t, n, 256), 256, 0, t->stream>>>(t->d_gen.p, t->d_nv.p, t->d_cen.p, n, t->d_in.p);
+    VD_CK(t, cudaGetLastError());
+  }
+  // Tessellation::set_generators on the new positions (re-filter, re-bin)
+  if (t->walls.empty()) {
+    std::swap(t->d_gen, t->d_in);
+    r = set_generators_from_device(t, t->d_gen.p, n, nullptr);
+  } else {
+    r = set_generators_from_device(t, t->d_in.p, n, nullptr);
+  }
+  return r;
+}
+
+int vd_tess_count_cells(const vd_tess* t, size_t* n) {
+  if (!t || !n) return VD_EINVAL;
+  *n = t->calculated ? t->ncells : 0;
+  return VD_OK;
+}
+
+int vd_tess_get_cell_summaries(vd_tess* t, double* volume, double* centroid3, int32_t* n_faces) {
+  int r = check_ready(t);
+  if (r != VD_OK) return r;
+  const size_t n = t->ncells;
+  cudaStream_t s = t->stream;
+  if (n) {
+    if (volume) VD_CK(t, cudaMemcpyAsync(volume, t->d_vol.p, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (centroid3)
+      VD_CK(t, cudaMemcpyAsync(centroid3, t->d_cen.p, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (n_faces) VD_CK(t, cudaMemcpyAsync(n_faces, t->d_nf.p, n * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  }
+  VD_CK(t, cudaStreamSynchronize(s));
+  return VD_OK;
+}
+
+int vd_tess_total_faces(vd_tess* t, int64_t* total) {
+  int r = check_ready(t);
+  if (r != VD_OK) return r;
+  if (!total) return VD_EINVAL;
+  r = ensure_csr(t);
+  if (r != VD_OK) return r;
+  *total = t->csr_total;
+  return VD_OK;
+}
+
+static int get_csr(vd_tess* t, int64_t* offsets, int32_t* ids, double* areas) {
+  int r = check_ready(t);
+  if (r != VD_OK) return r;
+  r = ensure_csr(t);
+  if (r != VD_OK) return r;
+  const size_t n = t->ncells;
+  cudaStream_t s = t->stream;
+  const size_t tot = (size_t)t->csr_total;
+  if (ids) VD_CK(t, t->d_csr_ids.ensure(tot));
+  if (areas) VD_CK(t, t->d_csr_area.ensure(tot));
+  if (n && tot) {
+    const int blocks = grid_blocks(t, n * 32, 256);
+    k_csr_gather<<<blocks, 256, 0, s>>>(t->d_nf.p, n, t->d_csr_off.p, t->fout, t->d_fnb.p, t->d_farea.p,
+                                        t->d_pool_fnb.p, t->d_pool_area.p, t->d_pool_off.p,
+                                        ids ? t->d_csr_ids.p : nullptr, areas ? t->d_csr_area.p : nullptr);
+    VD_CK(t, cudaGetLastError());
+    if (ids) VD_CK(t, cudaMemcpyAsync(ids, t->d_csr_ids.p, tot * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    if (areas) VD_CK(t, cudaMemcpyAsync(areas, t->d_csr_area.p, tot * sizeof(double), cudaMemcpyDeviceToHost, s));
+  }
+  if (offsets)
+    VD_CK(t, cudaMemcpyAsync(offsets, t->d_csr_off.p, (n + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+  VD_CK(t, cudaStreamSynchronize(s));
+  return VD_OK;
+}
+
+int vd_tess_get_neighbors(vd_tess* t, int64_t* offsets, int32_t* ids) {
+  if (!ids) return VD_EINVAL;
+  return get_csr(t, offsets, ids, nullptr);
+}
+
+int vd_tess_get_face_areas(vd_tess* t, int64_t* offsets, double* areas) {
+  if (!areas) return VD_EINVAL;
+  return get_csr(t, offsets, nullptr, areas);
+}
+
+// Recomputes cell i alone with polytope export.  The computation is
+// deterministic, so the polytope is the one calculate() built.
+int vd_tess_get_cell(vd_tess* t, size_t i, int32_t* n_vertices, int32_t* n_faces, int32_t* n_face_indices,
+                     double* vertices, uint32_t* face_counts, uint32_t* face_indices, int32_t* face_neighbors) {
+  int r = check_ready(t);
+  if (r != VD_OK) return r;
+  if (i >= t->ncells) return fail(t, VD_EINVAL, "cell index %zu out of range", i);
+  cudaStream_t s = t->stream;
+  const int cv = 2048, cf = 512, ch = 6144;
+  VD_CK(t, t->d_ex_v.ensure(3 * cv));
+  VD_CK(t, t->d_ex_fc.ensure(cf));
+  VD_CK(t, t->d_ex_fi.ensure(ch));
+  VD_CK(t, t->d_ex_fn.ensure(cf));
+  VD_CK(t, t->d_ex_sizes.ensure(4));
+  VD_CK(t, cudaMemsetAsync(t->d_ex_sizes.p, 0, 4 * sizeof(int32_t), s));
+  WorkList ex;
+  memset(&ex, 0, sizeof(ex));
+  ex.ex_verts = t->d_ex_v.p;
+  ex.ex_fc = t->d_ex_fc.p;
+  ex.ex_fi = t->d_ex_fi.p;
+  ex.ex_fn = t->d_ex_fn.p;
+  ex.ex_sizes = t->d_ex_sizes.p;
+  ex.ex_cap_v = cv;
+  ex.ex_cap_f = cf;
+  ex.ex_cap_h = ch;
+  // keep the calculate() counters and timings of the full run
+  unsigned long long saved[kNumCounters];
+  memcpy(saved, t->counters, sizeof(saved));
+  float st[4];
+  memcpy(st, t->timings, sizeof(st));
+  unsigned long long sf[2] = {t->fallback[0], t->fallback[1]};
+  const uint32_t cell = (uint32_t)i;
+  r = run_calculate(t, &ex, &cell);
+  memcpy(t->counters, saved, sizeof(saved));
+  memcpy(t->timings, st, sizeof(st));
+  t->fallback[0] = sf[0];
+  t->fallback[1] = sf[1];
+  if (r != VD_OK) return r;
+  int32_t sz[4];
+  VD_CK(t, cudaMemcpyAsync(sz, t->d_ex_sizes.p, sizeof(sz), cudaMemcpyDeviceToHost, s));
+  VD_CK(t, cudaStreamSynchronize(s));
+  if (n_vertices) *n_vertices = sz[0];
+  if (n_faces) *n_faces = sz[1];
+  if (n_face_indices) *n_face_indices = sz[2];
+  if (vertices && sz[0])
+    VD_CK(t, cudaMemcpyAsync(vertices, t->d_ex_v.p, 3 * (size_t)sz[0] * sizeof(double), cudaMemcpyDeviceToHost, s));
+  if (face_counts && sz[1])
+    VD_CK(t, cudaMemcpyAsync(face_counts, t->d_ex_fc.p, (size_t)sz[1] * 4, cudaMemcpyDeviceToHost, s));
+  if (face_neighbors && sz[1])
+    VD_CK(t, cudaMemcpyAsync(face_neighbors, t->d_ex_fn.p, (size_t)sz[1] * 4, cudaMemcpyDeviceToHost, s));
+  if (face_indices && sz[2])
+    VD_CK(t, cudaMemcpyAsync(face_indices, t->d_ex_fi.p, (size_t)sz[2] * 4, cudaMemcpyDeviceToHost, s));
+  VD_CK(t, cudaStreamSynchronize(s));
+  return VD_OK;
+}
+
+int vd_tess_device_results(vd_tess* t, const double** d_volume, const double** d_centroid3,
+                           const int32_t** d_n_faces) {
+  int r = check_ready(t);
+  if (r != VD_OK) return r;
+  if (d_volume) *d_volume = t->d_vol.p;
+  if (d_centroid3) *d_centroid3 = t->d_cen.p;
+  if (d_n_faces) *d_n_faces = t->d_nf.p;
+  return VD_OK;
+}
+
+int vd_tess_stream(vd_tess* t, void** stream) {
+  if (!t || !stream) return VD_EINVAL;
+  *stream = (void*)t->stream;
+  return VD_OK;
+}
+
+int vd_tess_timings(vd_tess* t, float* ms4) {
+  if (!t || !ms4) return VD_EINVAL;
+  memcpy(ms4, t->timings, sizeof(t->timings));
+  return VD_OK;
+}
+
+int vd_tess_counters(vd_tess* t, uint64_t* out8) {
+  if (!t || !out8) return VD_EINVAL;
+  for (int k = 0; k < kNumCounters; ++k) out8[k] = t->counters[k];
+  return VD_OK;
+}
+
+int vd_tess_fallback_counts(vd_tess* t, uint64_t* out2) {
+  if (!t || !out2) return VD_EINVAL;
+  out2[0] = t->fallback[0];
+  out2[1] = t->fallback[1];
+  return VD_OK;
+}
+
+int vd_host_alloc(size_t bytes, void** ptr) {
+  if (!ptr) return VD_EINVAL;
+  cudaError_t e = cudaHostAlloc(ptr, std::max<size_t>(bytes, 1), cudaHostAllocDefault);
+  if (e != cudaSuccess) return fail(nullptr, VD_ENOMEM, "cudaHostAlloc: %s", cudaGetErrorString(e));
+  return VD_OK;
+}
+
+int vd_host_free(void* ptr) {
+  if (ptr) cudaFreeHost(ptr);
+  return VD_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,30 @@
+// vd_internal.h -- interface between the host library and the kernel
+// translation units (not part of the public C ABI).
+#pragma once
+#include <cuda_runtime.h>
+#include <cstddef>
+#include <cstdint>
+
+#include "vd_common.cuh"
+
+namespace vd {
+
+// Fast-path geometry, exported so the host can size launches and buffers.
+struct ClipLaunchInfo {
+  size_t smem_per_warp;
+  int warps_per_block;
+  int blocks_per_sm;
+  size_t big_scratch_per_warp;
+};
+
+// FP64 bit-exact path (vd_kernels_fp64.cu, compiled with -fmad=false)
+cudaError_t clip_fp64_info(ClipLaunchInfo* info);
+cudaError_t launch_clip_fp64_fast(const TessDesc& T, const WorkList& W, int nblocks, cudaStream_t s);
+cudaError_t launch_clip_fp64_big(const TessDesc& T, const WorkList& W, void* scratch, int nwarps,
+                                 cudaStream_t s);
+
+// Mixed path (vd_kernels_mixed.cu)
+cudaError_t clip_mixed_info(ClipLaunchInfo* info);
+cudaError_t launch_clip_mixed_fast(const TessDesc& T, const WorkList& W, int nblocks, cudaStream_t s);
+
+}  // namespace vd

@@ -1,0 +1,369 @@
+"""Python mirror of the reference crate's 3D API, backed by the CUDA library.
+
+Names, argument meanings and error behaviour follow the reference crate
+``voronoid``:
+
+* ``BoundingBox`` / ``box_side``         -- src/bounds/mod.rs:3-22
+* ``Algorithm3DGrid``                   -- src/algorithm/algo_3d_grid.rs:10-95
+* ``Wall``, ``WALL_ID_MAX``             -- src/wall/mod.rs:8-49 (id > -1000 is an error)
+* ``PlaneGeometry``, ``SphereGeometry`` -- src/wall/wall_3d.rs:8-101
+* ``Cell3DFaces``                       -- src/cell/cell_3d_faces.rs:22-270
+* ``Tessellation``                      -- src/tessellation.rs:13-527
+
+Every computation runs on the GPU through the C ABI; results come back as
+numpy arrays.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from typing import Callable, List, Optional, Sequence
+
+import numpy as np
+
+from ._lib import VD_PREC_FP64, VD_PREC_MIXED, check, load
+
+WALL_ID_MAX = -1000
+
+
+def box_side(axis: int, is_max: bool) -> int:
+    """Id of a bounding-box face: x- -1, x+ -2, y- -3, y+ -4, z- -5, z+ -6."""
+    return -1 - (axis * 2 + (1 if is_max else 0))
+
+
+@dataclass
+class BoundingBox:
+    min: Sequence[float]
+    max: Sequence[float]
+
+    def __post_init__(self):
+        self.min = [float(v) for v in self.min]
+        self.max = [float(v) for v in self.max]
+
+
+class Algorithm3DGrid:
+    """Uniform bin grid with a shell-ordered neighbour walk (built on device)."""
+
+    def __init__(self, nx: int, ny: int, nz: int, bounds: Optional[BoundingBox] = None):
+        if nx <= 0 or ny <= 0 or nz <= 0:
+            raise ValueError("grid resolution must be positive")
+        self.grid_res_x, self.grid_res_y, self.grid_res_z = int(nx), int(ny), int(nz)
+        self.bounds = bounds
+
+
+class PlaneGeometry:
+    """Plane wall; ``normal`` points into the valid region and is normalised."""
+
+    def __init__(self, point: Sequence[float], normal: Sequence[float]):
+        self.point = [float(v) for v in point]
+        self.normal = [float(v) for v in normal]
+
+    def is_planar(self) -> bool:
+        return True
+
+
+class SphereGeometry:
+    """Spherical wall; the valid region is inside."""
+
+    def __init__(self, center: Sequence[float], radius: float):
+        self.center = [float(v) for v in center]
+        self.radius = float(radius)
+
+    def is_planar(self) -> bool:
+        return False
+
+
+class Wall:
+    """A wall geometry with an id <= WALL_ID_MAX (the reference panics otherwise)."""
+
+    def __init__(self, id: int, geometry):
+        if id > WALL_ID_MAX:
+            raise ValueError(f"Wall ID must be <= {WALL_ID_MAX}")
+        if not isinstance(geometry, (PlaneGeometry, SphereGeometry)):
+            raise TypeError("only PlaneGeometry and SphereGeometry walls are supported")
+        self._id = int(id)
+        self.geometry = geometry
+
+    def id(self) -> int:
+        return self._id
+
+    def is_planar(self) -> bool:
+        return self.geometry.is_planar()
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _vp(a: np.ndarray):
+    return C.c_void_p(a.ctypes.data)
+
+
+class Cell3DFaces:
+    """One computed cell: the polytope in the reference layout plus the
+    measures the GPU computed for it (volume, centroid, per-face areas)."""
+
+    def __init__(self, id: int, vertices, face_counts, face_indices, face_neighbors,
+                 volume: float, centroid, face_areas):
+        self._id = int(id)
+        self._vertices = np.asarray(vertices, np.float64)
+        self._face_counts = np.asarray(face_counts, np.uint32)
+        self._face_indices = np.asarray(face_indices, np.uint32)
+        self._face_neighbors = np.asarray(face_neighbors, np.int32)
+        self._volume = float(volume)
+        self._centroid = np.asarray(centroid, np.float64)
+        self._face_areas = np.asarray(face_areas, np.float64)
+
+    def id(self) -> int:
+        return self._id
+
+    def vertices(self) -> np.ndarray:
+        return self._vertices.copy()
+
+    def face_counts(self) -> np.ndarray:
+        return self._face_counts.copy()
+
+    def face_indices(self) -> np.ndarray:
+        return self._face_indices.copy()
+
+    def face_neighbors(self) -> np.ndarray:
+        return self._face_neighbors.copy()
+
+    def neighbors(self) -> np.ndarray:
+        return self._face_neighbors
+
+    def faces(self) -> List[List[int]]:
+        out, off = [], 0
+        for c in self._face_counts:
+            out.append([int(v) for v in self._face_indices[off:off + c]])
+            off += int(c)
+        return out
+
+    def is_empty(self) -> bool:
+        return self._vertices.size == 0
+
+    def volume(self) -> float:
+        return self._volume
+
+    def centroid(self) -> np.ndarray:
+        return self._centroid.copy()
+
+    def face_area(self, face_index: int) -> float:
+        if face_index >= self._face_areas.size:
+            return 0.0
+        return float(self._face_areas[face_index])
+
+
+class Tessellation:
+    """Tessellation<3, Cell3DFaces, Algorithm3DGrid> on one GPU."""
+
+    def __init__(self, bounds: BoundingBox, algorithm: Algorithm3DGrid):
+        self.bounds = bounds
+        self.algorithm = algorithm
+        self.walls: List[Wall] = []
+        self._L = load()
+        h = C.c_void_p()
+        mn = np.asarray(bounds.min, np.float64)
+        mx = np.asarray(bounds.max, np.float64)
+        check(self._L.vd_tess_create(_dp(mn), _dp(mx), algorithm.grid_res_x, algorithm.grid_res_y,
+                                     algorithm.grid_res_z, C.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self._L.vd_tess_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _ck(self, rc: int):
+        check(rc, self._h)
+
+    # ---- configuration -------------------------------------------------
+    def set_precision(self, precision: str):
+        """'fp64' (default, bitwise the reference's arithmetic) or 'mixed'."""
+        code = {"fp64": VD_PREC_FP64, "mixed": VD_PREC_MIXED}[precision]
+        self._ck(self._L.vd_tess_set_precision(self._h, code))
+
+    def add_wall(self, wall: Wall):
+        g = wall.geometry
+        if isinstance(g, PlaneGeometry):
+            p = np.asarray(g.point, np.float64)
+            n = np.asarray(g.normal, np.float64)
+            self._ck(self._L.vd_tess_add_wall_plane(self._h, _dp(p), _dp(n), wall.id()))
+        else:
+            c = np.asarray(g.center, np.float64)
+            self._ck(self._L.vd_tess_add_wall_sphere(self._h, _dp(c), g.radius, wall.id()))
+        self.walls.append(wall)
+
+    def clear_walls(self):
+        self._ck(self._L.vd_tess_clear_walls(self._h))
+        self.walls = []
+
+    # ---- generators ----------------------------------------------------
+    def set_generators(self, generators) -> int:
+        a = np.ascontiguousarray(np.asarray(generators, np.float64).reshape(-1))
+        n = a.size // 3
+        a = a[:3 * n]
+        kept = C.c_size_t()
+        self._ck(self._L.vd_tess_set_generators(self._h, _dp(a), n, C.byref(kept)))
+        return kept.value
+
+    def set_generators_device(self, ptr: int, n: int) -> int:
+        """Generators already in device memory (AoS doubles at ``ptr``)."""
+        kept = C.c_size_t()
+        self._ck(self._L.vd_tess_set_generators_device(self._h, C.c_void_p(ptr), int(n), C.byref(kept)))
+        return kept.value
+
+    def set_generator(self, index: int, generator: Sequence[float]):
+        g = np.asarray(generator, np.float64)
+        self._ck(self._L.vd_tess_set_generator(self._h, int(index), _dp(g)))
+
+    def read_generators(self, text: str):
+        """Tessellation::read_generators (tessellation.rs:153-171): one
+        ``id x y z`` per line, id ignored, missing/unparsable coordinates 0."""
+        pts = []
+        for line in text.splitlines():
+            parts = line.split()
+            if not parts:
+                continue
+            for k in range(3):
+                try:
+                    pts.append(float(parts[1 + k]))
+                except (IndexError, ValueError):
+                    pts.append(0.0)
+        return self.set_generators(np.asarray(pts, np.float64))
+
+    def import_generators(self, path: str):
+        """Tessellation::import_generators (tessellation.rs:126-148)."""
+        with open(path) as f:
+            return self.read_generators(f.read())
+
+    def count_generators(self) -> int:
+        n = C.c_size_t()
+        self._ck(self._L.vd_tess_count_generators(self._h, C.byref(n)))
+        return n.value
+
+    def generators(self) -> np.ndarray:
+        out = np.zeros(3 * self.count_generators(), np.float64)
+        self._ck(self._L.vd_tess_get_generators(self._h, _dp(out)))
+        return out
+
+    def get_generator(self, index: int) -> np.ndarray:
+        return self.generators()[3 * index:3 * index + 3]
+
+    # ---- the hot path --------------------------------------------------
+    def calculate(self):
+        self._ck(self._L.vd_tess_calculate(self._h))
+
+    def relax(self):
+        self._ck(self._L.vd_tess_relax(self._h))
+
+    def count_cells(self) -> int:
+        n = C.c_size_t()
+        self._ck(self._L.vd_tess_count_cells(self._h, C.byref(n)))
+        return n.value
+
+    # ---- results -------------------------------------------------------
+    def summaries(self):
+        """(volume[n], centroid[n,3], n_faces[n]) of every cell."""
+        n = self.count_cells()
+        vol = np.zeros(n, np.float64)
+        cen = np.zeros((n, 3), np.float64)
+        nf = np.zeros(n, np.int32)
+        self._ck(self._L.vd_tess_get_cell_summaries(self._h, _vp(vol), _vp(cen), _vp(nf)))
+        return vol, cen, nf
+
+    def total_faces(self) -> int:
+        t = C.c_int64()
+        self._ck(self._L.vd_tess_total_faces(self._h, C.byref(t)))
+        return t.value
+
+    def neighbors(self):
+        """CSR (offsets[n+1], ids[total]) of every cell's face_neighbors."""
+        n = self.count_cells()
+        tot = self.total_faces()
+        off = np.zeros(n + 1, np.int64)
+        ids = np.zeros(max(tot, 1), np.int32)
+        self._ck(self._L.vd_tess_get_neighbors(self._h, _vp(off), _vp(ids)))
+        return off, ids[:tot]
+
+    def face_areas(self):
+        n = self.count_cells()
+        tot = self.total_faces()
+        off = np.zeros(n + 1, np.int64)
+        ar = np.zeros(max(tot, 1), np.float64)
+        self._ck(self._L.vd_tess_get_face_areas(self._h, _vp(off), _vp(ar)))
+        return off, ar[:tot]
+
+    def get_cell(self, index: int) -> Optional[Cell3DFaces]:
+        if index < 0 or index >= self.count_cells():
+            return None
+        nv, nf, nh = C.c_int32(), C.c_int32(), C.c_int32()
+        self._ck(self._L.vd_tess_get_cell(self._h, int(index), C.byref(nv), C.byref(nf), C.byref(nh),
+                                          None, None, None, None))
+        v = np.zeros(3 * max(nv.value, 1), np.float64)
+        fc = np.zeros(max(nf.value, 1), np.uint32)
+        fi = np.zeros(max(nh.value, 1), np.uint32)
+        fn = np.zeros(max(nf.value, 1), np.int32)
+        self._ck(self._L.vd_tess_get_cell(self._h, int(index), C.byref(nv), C.byref(nf), C.byref(nh),
+                                          _vp(v), _vp(fc), _vp(fi), _vp(fn)))
+        vol, cen, _ = self._summary_cache()
+        off, ar = self._area_cache()
+        return Cell3DFaces(index, v[:3 * nv.value], fc[:nf.value], fi[:nh.value], fn[:nf.value],
+                           vol[index], cen[index], ar[off[index]:off[index + 1]])
+
+    def _summary_cache(self):
+        key = ("sum", id(self))
+        if getattr(self, "_cache_key", None) != self._calc_stamp():
+            self._cache = {}
+            self._cache_key = self._calc_stamp()
+        if key not in self._cache:
+            self._cache[key] = self.summaries()
+        return self._cache[key]
+
+    def _area_cache(self):
+        self._summary_cache()
+        if "areas" not in self._cache:
+            self._cache["areas"] = self.face_areas()
+        return self._cache["areas"]
+
+    def _calc_stamp(self):
+        t = (C.c_float * 4)()
+        self._ck(self._L.vd_tess_timings(self._h, t))
+        return tuple(t) + (self.count_cells(),)
+
+    def cells(self) -> List[Cell3DFaces]:
+        return [self.get_cell(i) for i in range(self.count_cells())]
+
+    def map(self, f: Callable[[Cell3DFaces], object]) -> list:
+        """Tessellation::map (tessellation.rs:391-412): compute, then apply f."""
+        self.calculate()
+        return [f(self.get_cell(i)) for i in range(self.count_cells())]
+
+    # ---- instrumentation -------------------------------------------------
+    def stream(self) -> int:
+        s = C.c_void_p()
+        self._ck(self._L.vd_tess_stream(self._h, C.byref(s)))
+        return s.value or 0
+
+    def timings(self) -> dict:
+        t = (C.c_float * 4)()
+        self._ck(self._L.vd_tess_timings(self._h, t))
+        return {"bin_ms": t[0], "clip_ms": t[1], "fallback_ms": t[2], "total_ms": t[3]}
+
+    def counters(self) -> dict:
+        out = (C.c_uint64 * 8)()
+        self._ck(self._L.vd_tess_counters(self._h, out))
+        names = ("candidates", "clips", "classified", "modifying", "intersections", "kept",
+                 "triangles", "offsets")
+        return {k: int(v) for k, v in zip(names, out)}
+
+    def fallback_counts(self) -> dict:
+        out = (C.c_uint64 * 2)()
+        self._ck(self._L.vd_tess_fallback_counts(self._h, out))
+        return {"overflow": int(out[0]), "table": int(out[1])}
