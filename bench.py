@@ -1,0 +1,369 @@
+#!/usr/bin/env python
+"""Benchmark of the 3D tessellation hot path (cells/s) on B200.
+
+Workload (one step): 1,048,576 generators i.i.d. uniform in the unit cube
+(f64, seeded PCG64), Algorithm3DGrid 100^3 bins, Cell3DFaces, no walls:
+set_generators (wall filter + binning) followed by calculate(), i.e. every
+cell's polytope with its volume, centroid, face areas and neighbour ids.
+
+    python bench.py [--gpus N --steps K --warmup W] [--precision fp64|mixed]
+    python bench.py --impl reference ...   # the reference's algorithm on the host cores
+
+`value` times device-resident input (CUDA events on the library's stream,
+L2 flushed between steps); `e2e` times the same step through the C ABI with
+host buffers, including the host->device copy of the generators and the
+device->host copy of every result (summaries, neighbour ids, face areas).
+With N GPUs (torchrun) every rank builds its own independent tessellation
+(weak scaling, no collective on the data path); the step time is the max over
+ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+N_GEN = 1_048_576
+GRID = 100
+METRIC = "3D cells/s @1M gens"
+WORKLOAD = "1,048,576 uniform generators in the unit cube, grid 100^3, no walls"
+
+# Algorithmic FP64 operations per counted event ("flop model").
+FLOPS_PER = {
+    "classified": 8,      # (v-p).n: 3 sub, 3 mul, 2 add
+    "candidates": 15,     # d = q-g, |d|^2, midpoint, 4R^2
+    "intersections": 19,  # t = ds/(ds-de), v = a + t(b-a), radius
+    "kept": 8,            # radius of a kept vertex
+    "triangles": 50,      # volume/centroid fan triangle (27) + face-area triangle (23)
+}
+
+
+def set_workload(n: int, grid: int):
+    global N_GEN, GRID, WORKLOAD
+    N_GEN, GRID = n, grid
+    WORKLOAD = f"{n:,} uniform generators in the unit cube, grid {grid}^3, no walls"
+
+
+def flop_count(cnt: dict) -> int:
+    return sum(FLOPS_PER[k] * int(cnt[k]) for k in FLOPS_PER)
+
+
+def uniform(n, seed):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    return rng.uniform(0.0, 1.0, size=(n, 3))
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                p = [x.strip() for x in line.split(",")]
+                if len(p) >= 9:
+                    rows.append(p)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        sm = [num(r[1]) for r in rows if num(r[1]) is not None]
+        mx = [num(r[2]) for r in rows if num(r[2]) is not None]
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def load_traffic(precision: str):
+    """DRAM bytes per clip-kernel launch from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", f"clip_{precision}_uniform_1M.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        return json.load(f).get("dram_bytes_per_launch")
+
+
+def cpu_baseline(pts, nthreads: int, sample: int):
+    """The oracle (a C restatement of the reference's calculate) on the host
+    cores over a bounded sample of the same tessellation's cells."""
+    from oracle.oracle import OracleTessellation
+    t = OracleTessellation([0, 0, 0], [1, 1, 1], GRID, GRID, GRID)
+    t.set_generators(pts)
+    begin = (len(pts) - sample) // 2
+    t0 = time.perf_counter()
+    t.calculate_range(begin, begin + sample, nthreads)
+    dt = time.perf_counter() - t0
+    return sample / dt, dt
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    nthreads = os.cpu_count() or 1
+    pts = uniform(N_GEN, 0)
+    from oracle.oracle import OracleTessellation
+    t = OracleTessellation([0, 0, 0], [1, 1, 1], GRID, GRID, GRID)
+    t.set_generators(pts)
+    sample = args.ref_sample
+    begin = (N_GEN - sample) // 2
+    for _ in range(args.warmup):
+        t.calculate_range(begin, begin + sample, nthreads)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        t.calculate_range(begin, begin + sample, nthreads)
+        times.append(time.perf_counter() - t0)
+    ms = 1e3 * statistics.mean(times)
+    value = sample / (ms / 1e3)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": 0,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded PCG64 uniform)",
+        "config": {"workload": WORKLOAD, "n_generators": N_GEN, "grid": [GRID] * 3,
+                   "step": f"calculate() over a bounded sample of {sample} cells of the tessellation"},
+        "cpu_baseline": {"value": value, "unit": "cells/s", "cores": nthreads, "kind": "port",
+                         "sample": f"{sample} of {N_GEN} cells per step, OpenMP dynamic schedule"},
+        "e2e": {"value": value, "unit": "cells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference is Rust and no Rust toolchain exists here; this arm times the oracle, "
+                "a C restatement of the reference's calculate()",
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def e2e_leg(args, L, _lib, tess, pts):
+    """Same step through the C ABI with pinned host buffers: H2D of the
+    generators, calculate, D2H of summaries, neighbour ids and face areas."""
+    h_in = C.c_void_p()
+    _lib.check(L.vd_host_alloc(3 * N_GEN * 8, C.byref(h_in)))
+    C.memmove(h_in, pts.ctypes.data, 3 * N_GEN * 8)
+    vol_b = C.c_void_p()
+    cen_b = C.c_void_p()
+    nf_b = C.c_void_p()
+    _lib.check(L.vd_host_alloc(N_GEN * 8, C.byref(vol_b)))
+    _lib.check(L.vd_host_alloc(3 * N_GEN * 8, C.byref(cen_b)))
+    _lib.check(L.vd_host_alloc(N_GEN * 4, C.byref(nf_b)))
+    tot = tess.total_faces()
+    off_b = C.c_void_p()
+    ids_b = C.c_void_p()
+    ar_b = C.c_void_p()
+    _lib.check(L.vd_host_alloc((N_GEN + 1) * 8, C.byref(off_b)))
+    _lib.check(L.vd_host_alloc(int(tot * 1.2) * 4, C.byref(ids_b)))
+    _lib.check(L.vd_host_alloc(int(tot * 1.2) * 8, C.byref(ar_b)))
+    h = tess._h
+    kept = C.c_size_t()
+    e2e_ms = []
+    total_faces = C.c_int64()
+    for it in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        _lib.check(L.vd_tess_set_generators(h, C.cast(h_in, C.POINTER(C.c_double)), N_GEN, C.byref(kept)), h)
+        _lib.check(L.vd_tess_calculate(h), h)
+        _lib.check(L.vd_tess_get_cell_summaries(h, vol_b, cen_b, nf_b), h)
+        _lib.check(L.vd_tess_total_faces(h, C.byref(total_faces)), h)
+        _lib.check(L.vd_tess_get_neighbors(h, off_b, ids_b), h)
+        _lib.check(L.vd_tess_get_face_areas(h, None, ar_b), h)
+        dt = time.perf_counter() - t0
+        if it >= args.warmup:
+            e2e_ms.append(1e3 * dt)
+    e2e = statistics.mean(e2e_ms)
+    tf = total_faces.value
+    h2d = 3 * N_GEN * 8
+    d2h = N_GEN * (8 + 24 + 4) + (N_GEN + 1) * 8 + tf * (4 + 8)
+    for b in (h_in, vol_b, cen_b, nf_b, off_b, ids_b, ar_b):
+        L.vd_host_free(b)
+
+    return e2e, h2d, d2h
+
+
+def run_ours(args):
+    import torch
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    import vorothree_b200 as v
+    from vorothree_b200 import _lib
+
+    L = v.load()
+    pts = uniform(N_GEN, rank)
+    d_pts = torch.from_numpy(pts).to(f"cuda:{local}")
+    tess = v.Tessellation(v.BoundingBox([0, 0, 0], [1, 1, 1]), v.Algorithm3DGrid(GRID, GRID, GRID))
+    tess.set_precision(args.precision)
+    stream = torch.cuda.ExternalStream(tess.stream(), device=f"cuda:{local}")
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+
+    def step():
+        tess.set_generators_device(d_pts.data_ptr(), N_GEN)
+        tess.calculate()
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    launches0 = C.c_uint64()
+    L.vd_launch_count(C.byref(launches0))
+
+    def barrier():
+        if ws > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    clocks = ClockSampler(local)
+    barrier()
+    clocks.start()
+    step_ms, clip_ms, bin_ms = [], [], []
+    counters = None
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step()
+        e1.record(stream)
+        e1.synchronize()
+        step_ms.append(e0.elapsed_time(e1))
+        tm = tess.timings()
+        clip_ms.append(tm["clip_ms"])
+        bin_ms.append(tm["bin_ms"])
+        counters = tess.counters()
+    barrier()
+    clk = clocks.stop()
+    launches1 = C.c_uint64()
+    L.vd_launch_count(C.byref(launches1))
+    ms = statistics.mean(step_ms)
+    if ws > 1:
+        tt = torch.tensor([ms], device=f"cuda:{local}", dtype=torch.float64)
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        ms = float(tt.item())
+    value = ws * N_GEN / (ms / 1e3)
+    fb = tess.fallback_counts()
+
+    # ---- end to end through the C ABI with pinned host buffers ----
+    e2e, h2d, d2h = e2e_leg(args, L, _lib, tess, pts) if not args.no_e2e else (None, None, None)
+    if e2e is not None and ws > 1:
+        tt = torch.tensor([e2e], device=f"cuda:{local}", dtype=torch.float64)
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        e2e = float(tt.item())
+    line = None
+    if rank == 0:
+        flops = flop_count(counters)
+        clip = statistics.mean(clip_ms)
+        peak = C.c_double()
+        _lib.check(L.vd_measure_fma_peak(1, C.byref(peak)))
+        achieved = flops / (clip / 1e3) / 1e12
+        traffic = load_traffic(args.precision)
+        line = {
+            "metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32-classify/f64",
+            "data": "synthetic (seeded PCG64 uniform; rank r uses seed r)",
+            "config": {"workload": WORKLOAD, "n_generators": N_GEN, "grid": [GRID] * 3,
+                       "precision": args.precision, "step": "set_generators (device input) + calculate",
+                       "l2": "flushed (512 MiB write) before every timed step",
+                       "parallelism": f"{ws} independent tessellations, one per GPU"},
+            "phases_ms": {"binning": statistics.mean(bin_ms), "clip_kernel": clip},
+            "roofline": {"bound": "fp64", "kernel": "k_clip_fast (warp-per-cell clip + reductions)",
+                         "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
+                         "frac": achieved / peak.value,
+                         "peak_source": "FP64 FMA-chain microbenchmark run live by bench.py on this GPU",
+                         "flops_per_launch": flops, "traffic": traffic},
+            "e2e": None if e2e is None else {
+                "value": N_GEN / (e2e / 1e3) * ws, "unit": "cells/s", "ms_per_step": e2e,
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": int(launches1.value - launches0.value),
+            "clocks": clk,
+            "fallback_cells": fb,
+        }
+        if ws == 1 and not args.no_cpu_baseline:
+            nthreads = os.cpu_count() or 1
+            cv, cdt = cpu_baseline(pts, nthreads, args.cpu_sample)
+            line["cpu_baseline"] = {"value": cv, "unit": "cells/s", "cores": nthreads, "kind": "port",
+                                    "sample": f"{args.cpu_sample} of {N_GEN} cells of the same tessellation "
+                                              f"({cdt:.2f} s wall)"}
+        print(json.dumps(line), flush=True)
+    tess.close()
+    if ws > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--cpu-sample", type=int, default=262144)
+    ap.add_argument("--ref-sample", type=int, default=131072)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
+    ap.add_argument("--n", type=int, default=N_GEN, help="generators (profiling runs use a smaller case)")
+    ap.add_argument("--grid", type=int, default=GRID)
+    args = ap.parse_args()
+    set_workload(args.n, args.grid)
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

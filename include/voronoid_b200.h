@@ -124,6 +124,9 @@ int vd_tess_counters(vd_tess* t, uint64_t* out8);
  * [0] polytope-capacity overflow, [1] search-order extension */
 int vd_tess_fallback_counts(vd_tess* t, uint64_t* out2);
 
+/* kernels this library has launched in this process, over all handles */
+int vd_launch_count(uint64_t* n);
+
 /* ---- pinned host memory for callers staging large inputs/outputs ---- */
 int vd_host_alloc(size_t bytes, void** ptr);
 int vd_host_free(void* ptr);

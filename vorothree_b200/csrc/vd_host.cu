@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -28,6 +29,8 @@ using namespace vd;
 namespace {
 
 thread_local std::string g_create_error;
+// kernels this library has launched in this process (all handles)
+std::atomic<unsigned long long> g_launches{0};
 
 template <typename T>
 struct DevBuf {
@@ -160,6 +163,7 @@ int scan_excl(vd_tess* t, const Tin* in, T* out, size_t n, std::vector<DevBuf<T>
   VD_CK(t, pool[level].ensure(nt + 1));
   T* sums = pool[level].p;
   k_scan_tiles<Tin, T><<<(unsigned)nt, kScanThreads, 0, t->stream>>>(in, out, n, sums);
+  g_launches++;
   VD_CK(t, cudaGetLastError());
   if (nt > 1) {
     // scan the tile sums in place (needs its own level of scratch)
@@ -169,6 +173,7 @@ int scan_excl(vd_tess* t, const Tin* in, T* out, size_t n, std::vector<DevBuf<T>
     int r = scan_excl<T, T>(t, sums, sscan, nt, pool, level + 2);
     if (r != VD_OK) return r;
     k_scan_add<T><<<(unsigned)nt, kScanThreads, 0, t->stream>>>(out, n, sscan);
+    g_launches++;
     VD_CK(t, cudaGetLastError());
   }
   return VD_OK;
@@ -264,6 +269,7 @@ int rebin(vd_tess* t) {
   VD_CK(t, cudaMemsetAsync(t->d_ctl.p + kCtlBigCount, 0, sizeof(unsigned int), s));
   if (n > 0) {
     k_bin_count<<<grid_blocks(t, n, 256), 256, 0, s>>>(t->d_gen.p, n, t->grid, t->d_bin_of.p, t->d_bin_count.p);
+    g_launches++;
     VD_CK(t, cudaGetLastError());
   }
   int r = scan_excl<uint32_t, uint32_t>(t, t->d_bin_count.p, t->d_bin_start.p, nb + 1, t->scan32);
@@ -271,14 +277,18 @@ int rebin(vd_tess* t) {
   if (n > 0) {
     VD_CK(t, cudaMemcpyAsync(t->d_cursor.p, t->d_bin_start.p, nb * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
     k_bin_scatter<<<grid_blocks(t, n, 256), 256, 0, s>>>(t->d_bin_of.p, n, t->d_cursor.p, t->d_ids.p);
+    g_launches++;
     VD_CK(t, cudaGetLastError());
     k_bin_fix<<<grid_blocks(t, nb, 256), 256, 0, s>>>(t->d_bin_start.p, nb, t->d_ids.p, t->d_big_list.p,
                                                        t->d_ctl.p + kCtlBigCount);
+    g_launches++;
     VD_CK(t, cudaGetLastError());
     k_bin_sort_big<<<std::max(1, t->num_sms), kBigSortThreads, 0, s>>>(
         t->d_bin_start.p, t->d_big_list.p, t->d_ctl.p + kCtlBigCount, t->d_ids.p, t->d_ids_tmp.p);
+    g_launches++;
     VD_CK(t, cudaGetLastError());
     k_gather_sorted<<<grid_blocks(t, n, 256), 256, 0, s>>>(t->d_ids.p, t->d_gen.p, n, t->d_sorted.p);
+    g_launches++;
     VD_CK(t, cudaGetLastError());
   }
   t->calculated = false;
@@ -302,6 +312,7 @@ int filter_into_gen(vd_tess* t, const double* d_src, size_t n, size_t* n_kept) {
   VD_CK(t, t->d_tmp3.ensure(3 * n));
   if (n) {
     k_wall_flags<<<grid_blocks(t, n, 256), 256, 0, s>>>(d_src, n, wallset(t), t->d_flags.p);
+    g_launches++;
     VD_CK(t, cudaGetLastError());
   }
   VD_CK(t, cudaMemsetAsync(t->d_flags.p + n, 0, sizeof(uint32_t), s));
@@ -309,6 +320,7 @@ int filter_into_gen(vd_tess* t, const double* d_src, size_t n, size_t* n_kept) {
   if (r != VD_OK) return r;
   if (n) {
     k_compact3<<<grid_blocks(t, n, 256), 256, 0, s>>>(d_src, n, t->d_flags.p, t->d_pos.p, t->d_tmp3.p);
+    g_launches++;
     VD_CK(t, cudaGetLastError());
   }
   uint32_t kept = 0;
@@ -409,11 +421,13 @@ int clip_pass(vd_tess* t, bool big, const uint32_t* items, uint32_t nitems, uint
     const int nblocks = (int)std::max<size_t>(
         1, std::min<size_t>(warps_needed, (size_t)t->num_sms * std::max(1, li.blocks_per_sm)));
     VD_CK(t, mixed ? launch_clip_mixed_fast(T, W, nblocks, s) : launch_clip_fp64_fast(T, W, nblocks, s));
+    g_launches++;
   } else {
     int r = ensure_big(t, nitems);
     if (r != VD_OK) return r;
     T = make_desc(t);
     VD_CK(t, launch_clip_fp64_big(T, W, t->d_big.p, (int)t->big_warps, s));
+    g_launches++;
   }
   return VD_OK;
 }
@@ -510,6 +524,7 @@ int ensure_csr(vd_tess* t) {
   VD_CK(t, t->d_csr_off.ensure(n + 1));
   if (n) {
     k_nfaces_to_i64<<<grid_blocks(t, n, 256), 256, 0, s>>>(t->d_nf.p, n, t->d_nf64.p);
+    g_launches++;
     VD_CK(t, cudaGetLastError());
   }
   VD_CK(t, cudaMemsetAsync(t->d_nf64.p + n, 0, sizeof(long long), s));
@@ -753,6 +768,7 @@ int vd_tess_set_generator(vd_tess* t, size_t index, const double xyz[3]) {
   }
   VD_CK(t, cudaMemcpyAsync(t->d_gen.p + 3 * index, xyz, 3 * sizeof(double), cudaMemcpyHostToDevice, s));
   k_gather_sorted<<<grid_blocks(t, n, 256), 256, 0, s>>>(t->d_ids.p, t->d_gen.p, n, t->d_sorted.p);
+  g_launches++;
   VD_CK(t, cudaGetLastError());
   VD_CK(t, cudaStreamSynchronize(s));
   t->calculated = false;
@@ -801,6 +817,7 @@ int vd_tess_relax(vd_tess* t) {
   VD_CK(t, t->d_in.ensure(3 * n));
   if (n) {
     k_relax<<<grid_blocks(t, n, 256), 256, 0, t->stream>>>(t->d_gen.p, t->d_nv.p, t->d_cen.p, n, t->d_in.p);
+    g_launches++;
     VD_CK(t, cudaGetLastError());
   }
   // Tessellation::set_generators on the new positions (re-filter, re-bin)
@@ -859,6 +876,7 @@ static int get_csr(vd_tess* t, int64_t* offsets, int32_t* ids, double* areas) {
     k_csr_gather<<<blocks, 256, 0, s>>>(t->d_nf.p, n, t->d_csr_off.p, t->fout, t->d_fnb.p, t->d_farea.p,
                                         t->d_pool_fnb.p, t->d_pool_area.p, t->d_pool_off.p,
                                         ids ? t->d_csr_ids.p : nullptr, areas ? t->d_csr_area.p : nullptr);
+    g_launches++;
     VD_CK(t, cudaGetLastError());
     if (ids) VD_CK(t, cudaMemcpyAsync(ids, t->d_csr_ids.p, tot * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
     if (areas) VD_CK(t, cudaMemcpyAsync(areas, t->d_csr_area.p, tot * sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -967,6 +985,12 @@ int vd_tess_fallback_counts(vd_tess* t, uint64_t* out2) {
   if (!t || !out2) return VD_EINVAL;
   out2[0] = t->fallback[0];
   out2[1] = t->fallback[1];
+  return VD_OK;
+}
+
+int vd_launch_count(uint64_t* n) {
+  if (!n) return VD_EINVAL;
+  *n = g_launches.load();
   return VD_OK;
 }
 
