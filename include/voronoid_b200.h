@@ -131,6 +131,27 @@ int vd_launch_count(uint64_t* n);
 int vd_host_alloc(size_t bytes, void** ptr);
 int vd_host_free(void* ptr);
 
+/* ---- allocation-free variant (no counterpart in the reference) ----
+ * set_generators + calculate for a small tessellation without any device
+ * allocation, for callers that cannot call cudaMalloc: a plugin inside an
+ * application that owns the GPU's memory and hands out fixed buffers, code
+ * bound to a framework's memory pool, or a latency-critical loop that cannot
+ * take the device-wide synchronisation an allocation can cause.  The caller
+ * passes device buffers: d_xyz (n generators, AoS) and per-cell outputs
+ * d_volume[n], d_centroid3[3n], d_n_faces[n].  All intermediate data lives in
+ * one fixed __device__ array (about 8 MiB) that every GPU loading the library
+ * holds until exit.  Limits: n <= 8192 generators and a grid whose complete
+ * search order fits, (2nx+1)(2ny+1)(2nz+1) <= 68921 (e.g. 20x20x20); larger
+ * requests return VD_EINVAL (message via vd_last_error(NULL)).  No walls.
+ * Calls share the array: calls that overlap on the GPU race, so order them
+ * (e.g. on one stream).  The first call on a device resolves the array's
+ * device address; make it before any stream capture.  stream may be NULL
+ * (the default stream).  Results equal vd_tess_set_generators_device +
+ * vd_tess_calculate bit for bit. */
+int vd_calculate_noalloc(const double bmin[3], const double bmax[3], int nx, int ny, int nz,
+                         const double* d_xyz, size_t n, double* d_volume, double* d_centroid3,
+                         int32_t* d_n_faces, void* stream);
+
 /* ---- device measurement helper: FP64 / FP32 FMA-chain peak (TFLOP/s) ---- */
 int vd_measure_fma_peak(int fp64, double* tflops);
 

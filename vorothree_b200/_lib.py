@@ -63,6 +63,8 @@ SIGNATURES = {
     "vd_host_alloc": (C.c_int, [C.c_size_t, C.POINTER(_vp)]),
     "vd_host_free": (C.c_int, [_vp]),
     "vd_measure_fma_peak": (C.c_int, [C.c_int, _d]),
+    "vd_calculate_noalloc": (C.c_int, [_d, _d, C.c_int, C.c_int, C.c_int, _vp, C.c_size_t, _vp, _vp, _vp,
+                                       _vp]),
 }
 
 _lib = None

@@ -26,6 +26,7 @@ SOURCES = [
     ("vd_kernels_mixed.cu", True),
     ("vd_host.cu", False),
     ("vd_measure.cu", True),
+    ("vd_noalloc.cu", False),
 ]
 
 

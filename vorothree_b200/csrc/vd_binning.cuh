@@ -13,6 +13,8 @@
 #include "vd_common.cuh"
 
 namespace vd {
+// internal linkage: every translation unit that launches these gets its own copy
+namespace {
 
 constexpr int kScanThreads = 256;
 constexpr int kScanItems = 4;
@@ -296,4 +298,5 @@ __global__ void k_relax(const double* __restrict__ gen, const int32_t* __restric
   }
 }
 
+}  // namespace
 }  // namespace vd

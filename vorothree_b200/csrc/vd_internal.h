@@ -23,6 +23,9 @@ cudaError_t launch_clip_fp64_fast(const TessDesc& T, const WorkList& W, int nblo
 cudaError_t launch_clip_fp64_big(const TessDesc& T, const WorkList& W, void* scratch, int nwarps,
                                  cudaStream_t s);
 
+// message returned by vd_last_error(NULL) on the calling thread
+void set_thread_error(const char* msg);
+
 // Mixed path (vd_kernels_mixed.cu)
 cudaError_t clip_mixed_info(ClipLaunchInfo* info);
 cudaError_t launch_clip_mixed_fast(const TessDesc& T, const WorkList& W, int nblocks, cudaStream_t s);
