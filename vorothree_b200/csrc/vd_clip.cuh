@@ -30,7 +30,8 @@ namespace vd {
 
 constexpr unsigned kFull = 0xffffffffu;
 
-template <int V, int F, int H, int CC, int NC, int SC, typename VIdT, typename FIdT>
+template <int V, int F, int H, int CC, int NC, int SC, typename VIdT, typename FIdT, typename KeyT,
+          typename CIdT>
 struct PolyCfg {
   static constexpr int VCAP = V;   // vertices
   static constexpr int FCAP = F;   // faces
@@ -40,6 +41,9 @@ struct PolyCfg {
   static constexpr int SCAP = SC;  // lid segments per clip
   using VId = VIdT;
   using FId = FIdT;
+  using Key = KeyT;  // (min, max) vertex pair of an edge
+  using CId = CIdT;  // crossing index
+  static constexpr int KSHIFT = 8 * (int)sizeof(VIdT);
   static constexpr unsigned VNONE = (unsigned)(VIdT)~(VIdT)0;
   static constexpr unsigned FNONE = (unsigned)(FIdT)~(FIdT)0;
   static_assert(V < (int)VNONE, "vertex ids must leave room for the none marker");
@@ -49,10 +53,10 @@ struct PolyCfg {
 // Fast path: sized from the oracle's distribution (max 72 vertices, 38 faces,
 // 216 face entries over 7.5M uniform-input polytopes); anything larger goes
 // to the large-capacity pass.
-using FastCfg = PolyCfg<96, 48, 288, 64, 40, 32, uint8_t, uint8_t>;
+using FastCfg = PolyCfg<96, 48, 288, 64, 32, 32, uint8_t, uint8_t, uint16_t, uint8_t>;
 // Large-capacity pass (global-memory storage): vertex ids stay u16 like the
 // reference's face_indices (cell_3d_faces.rs:31).
-using BigCfg = PolyCfg<2048, 512, 6144, 1024, 512, 512, uint16_t, uint16_t>;
+using BigCfg = PolyCfg<2048, 512, 6144, 1024, 512, 512, uint16_t, uint16_t, uint32_t, uint16_t>;
 
 template <class C>
 struct alignas(16) WarpPoly {
@@ -61,14 +65,16 @@ struct alignas(16) WarpPoly {
   double tx[C::NCAP], ty[C::NCAP], tz[C::NCAP];
   unsigned long long cnt[kNumCounters];
   int32_t fn[2][C::FCAP];
-  uint32_t ckey[C::CCAP];
   uint16_t E[C::HCAP + 1];
   uint16_t fs[2][C::FCAP + 1];
   uint16_t fns[C::FCAP];
   uint16_t cpos[C::CCAP];
+  typename C::Key ckey[C::CCAP];
   typename C::VId cid[C::CCAP];
   typename C::VId fi[2][C::HCAP];
   typename C::FId pf[2][C::HCAP];
+  typename C::VId fe[C::HCAP];    // per clip: end vertex of each position's edge
+  typename C::CId cidx[C::HCAP];  // per clip: crossing index of a crossing position
   typename C::FId fnew[C::FCAP];
   typename C::VId o2n[C::VCAP];
   typename C::VId lidmap[C::VCAP];
@@ -154,6 +160,13 @@ __device__ double poly_max_radius_sq(const WarpPoly<C>& P, const PolyState& S, d
   return warp_max(m);
 }
 
+// position after p in its face loop (the (i + 1) % count of :380)
+template <class C>
+__device__ __forceinline__ int next_pos(const WarpPoly<C>& P, int cb, int p) {
+  const int f = P.pf[cb][p];
+  return (p + 1 == P.fs[cb][f + 1]) ? P.fs[cb][f] : p + 1;
+}
+
 // clip_with_scratch (cell_3d_faces.rs:288-503).  All lanes call it with the
 // same (uniform) arguments.  *r2 gets the max squared distance of the new
 // vertex set from (gx,gy,gz) when with_gen, else 0.
@@ -208,47 +221,62 @@ __device__ int warp_clip(WarpPoly<C>& P, PolyState& S, double px, double py, dou
   }
   if (with_gen) cnt_add(P, kCntKept, (unsigned long long)nkept);
 
-  // 3. crossing positions of the face walk, in walk order (:369-452)
+  __syncwarp();
+
+  // 3. one pass over the face positions (the face walk of :369-452): the
+  //    edge's end vertex, the crossing positions in walk order, and the
+  //    exclusive prefix E of the entries each position emits into the new
+  //    faces: in->in 1 (end), in->out 1 (X), out->in 2 (X, end), out->out 0.
   int ncross = 0;
-  for (int b = 0; b < nh; b += 32) {
-    const int p = b + lane;
-    bool cr = false;
-    unsigned s = 0, e = 0;
-    if (p < nh) {
-      const int f = P.pf[cb][p];
-      const int q = (p + 1 == P.fs[cb][f + 1]) ? P.fs[cb][f] : p + 1;
-      s = P.fi[cb][p];
-      e = P.fi[cb][q];
-      cr = (P.dist[s] <= kTol) != (P.dist[e] <= kTol);
-    }
-    const unsigned m = __ballot_sync(kFull, cr);
-    if (cr) {
-      const int k = ncross + __popc(m & lt);
-      if (k < C::CCAP) {
-        P.cpos[k] = (uint16_t)p;
-        P.ckey[k] = s < e ? (s << 16 | e) : (e << 16 | s);
+  {
+    int run = 0;
+    for (int b = 0; b < nh; b += 32) {
+      const int p = b + lane;
+      bool cr = false;
+      int em = 0;
+      unsigned s = 0, e = 0;
+      if (p < nh) {
+        s = P.fi[cb][p];
+        e = P.fi[cb][next_pos(P, cb, p)];
+        const bool si = P.o2n[s] != C::VNONE, ei = P.o2n[e] != C::VNONE;
+        P.fe[p] = (VId)e;
+        cr = si != ei;
+        em = si ? 1 : (ei ? 2 : 0);
       }
+      const unsigned m = __ballot_sync(kFull, cr);
+      if (cr) {
+        const int k = ncross + __popc(m & lt);
+        if (k < C::CCAP) {
+          P.cpos[k] = (uint16_t)p;
+          P.ckey[k] = (typename C::Key)(s < e ? (s << C::KSHIFT | e) : (e << C::KSHIFT | s));
+          P.cidx[p] = (typename C::CId)k;
+        }
+      }
+      ncross += __popc(m);
+      const int inc = warp_incl_scan(em);
+      if (p < nh) P.E[p] = (uint16_t)(run + inc - em);
+      run += __shfl_sync(kFull, inc, 31);
     }
-    ncross += __popc(m);
+    if (lane == 0) P.E[nh] = (uint16_t)run;
   }
   if (ncross > C::CCAP) return kClipOverflow;
   __syncwarp();
 
-  // 4. intersection vertices: first occurrence of an edge key creates the
+  // 4. intersection vertices: the first occurrence of an edge key creates the
   //    vertex (numbered in discovery order after the kept ones), repeats reuse
   //    it (the intersection_map lookups of :391-417 / :422-448)
   int nnew = 0;
   for (int b = 0; b < ncross; b += 32) {
     const int k = b + lane;
     const bool act = k < ncross;
-    const unsigned key = act ? P.ckey[k] : (0xFFFF0000u | lane);
+    const unsigned key = act ? (unsigned)P.ckey[k] : (0xFFFF0000u | lane);
     const unsigned mm = __match_any_sync(kFull, key);
     const int leader = __ffs(mm) - 1;
     const bool isleader = act && leader == (int)lane;
     int id = -1;
     if (isleader && b > 0) {
       for (int j = 0; j < b; ++j)
-        if (P.ckey[j] == key) {
+        if ((unsigned)P.ckey[j] == key) {
           id = P.cid[j];
           break;
         }
@@ -262,9 +290,7 @@ __device__ int warp_clip(WarpPoly<C>& P, PolyState& S, double px, double py, dou
       const int r = id - nkept;
       if (r < C::NCAP) {
         const int p = P.cpos[k];
-        const int f = P.pf[cb][p];
-        const int q = (p + 1 == P.fs[cb][f + 1]) ? P.fs[cb][f] : p + 1;
-        const int s = P.fi[cb][p], e = P.fi[cb][q];
+        const int s = P.fi[cb][p], e = P.fe[p];
         const double ds = P.dist[s], de = P.dist[e];
         const double t = clamp01(ds / (ds - de));
         const double ax = P.vx[s], ay = P.vy[s], az = P.vz[s];
@@ -316,27 +342,7 @@ __device__ int warp_clip(WarpPoly<C>& P, PolyState& S, double px, double py, dou
     P.vz[nkept + r] = P.tz[r];
   }
 
-  // 6. rewire faces.  Emit per position: in->in 1 (end), in->out 1 (X),
-  //    out->in 2 (X, end), out->out 0.  E = exclusive prefix of emits.
-  {
-    int run = 0;
-    for (int b = 0; b < nh; b += 32) {
-      const int p = b + lane;
-      int em = 0;
-      if (p < nh) {
-        const int f = P.pf[cb][p];
-        const int q = (p + 1 == P.fs[cb][f + 1]) ? P.fs[cb][f] : p + 1;
-        const bool si = P.dist[P.fi[cb][p]] <= kTol;
-        const bool ei = P.dist[P.fi[cb][q]] <= kTol;
-        em = si ? 1 : (ei ? 2 : 0);
-      }
-      const int inc = warp_incl_scan(em);
-      if (p < nh) P.E[p] = (uint16_t)(run + inc - em);
-      run += __shfl_sync(kFull, inc, 31);
-    }
-    if (lane == 0) P.E[nh] = (uint16_t)run;
-  }
-  __syncwarp();
+  // 6. surviving faces (>= 3 entries, :454-467) and their new starts
   int nfk = 0, hk = 0;
   bool longface = false;
   for (int b = 0; b < nf; b += 32) {
@@ -357,39 +363,53 @@ __device__ int warp_clip(WarpPoly<C>& P, PolyState& S, double px, double py, dou
   }
   if (__any_sync(kFull, longface) || hk > C::HCAP) return kClipOverflow;
   __syncwarp();
-  {
-    int crun = 0;
-    for (int b = 0; b < nh; b += 32) {
-      const int p = b + lane;
-      bool si = false, ei = false, cr = false;
-      int f = 0, e = 0;
-      if (p < nh) {
-        f = P.pf[cb][p];
-        const int q = (p + 1 == P.fs[cb][f + 1]) ? P.fs[cb][f] : p + 1;
-        e = P.fi[cb][q];
-        si = P.dist[P.fi[cb][p]] <= kTol;
-        ei = P.dist[e] <= kTol;
-        cr = si != ei;
-      }
-      const unsigned m = __ballot_sync(kFull, cr);
-      const int kc = crun + __popc(m & lt);
-      crun += __popc(m);
-      if (p < nh) {
-        const unsigned fw = P.fnew[f];
-        if (fw != C::FNONE) {
-          const int o = P.fns[f] + ((int)P.E[p] - (int)P.E[P.fs[cb][f]]);
-          if (si) {
-            P.fi[nb][o] = ei ? P.o2n[e] : P.cid[kc];
-            P.pf[nb][o] = (FId)fw;
-          } else if (ei) {
-            P.fi[nb][o] = P.cid[kc];
-            P.pf[nb][o] = (FId)fw;
-            P.fi[nb][o + 1] = P.o2n[e];
-            P.pf[nb][o + 1] = (FId)fw;
-          }
+
+  // 7. write the surviving faces' entries, and collect the lid segments.  In
+  //    a face buffer two intersection entries are adjacent exactly when an
+  //    in->out position is followed (after out->out positions) by an out->in
+  //    one; the reference records (v, u) = (X of the out->in, X of the
+  //    in->out), ordered by u's place in the buffer, i.e. by position.
+  int nseg = 0;
+  for (int b = 0; b < nh; b += 32) {
+    const int p = b + lane;
+    bool segsrc = false;
+    if (p < nh) {
+      const int f = P.pf[cb][p];
+      const unsigned os = P.o2n[P.fi[cb][p]], oe = P.o2n[P.fe[p]];
+      const bool si = os != C::VNONE, ei = oe != C::VNONE;
+      const unsigned fw = P.fnew[f];
+      if (fw != C::FNONE) {
+        const int o = P.fns[f] + ((int)P.E[p] - (int)P.E[P.fs[cb][f]]);
+        if (si) {
+          P.fi[nb][o] = (VId)(ei ? oe : (unsigned)P.cid[P.cidx[p]]);
+          P.pf[nb][o] = (FId)fw;
+          segsrc = !ei;
+        } else if (ei) {
+          P.fi[nb][o] = P.cid[P.cidx[p]];
+          P.pf[nb][o] = (FId)fw;
+          P.fi[nb][o + 1] = (VId)oe;
+          P.pf[nb][o + 1] = (FId)fw;
         }
       }
     }
+    const unsigned sm = __ballot_sync(kFull, segsrc);
+    if (segsrc) {
+      const int k = nseg + __popc(sm & lt);
+      if (k < C::SCAP) {
+        // forward along the face to the out->in position (one exists in a
+        // kept face: its walk must re-enter the inside)
+        const int f = P.pf[cb][p];
+        const int len = (int)P.fs[cb][f + 1] - (int)P.fs[cb][f];
+        int q = next_pos(P, cb, p);
+        for (int g2 = 0; g2 < len; ++g2) {
+          if (P.o2n[P.fe[q]] != C::VNONE) break;
+          q = next_pos(P, cb, q);
+        }
+        P.sega[k] = P.cid[P.cidx[q]];
+        P.segb[k] = P.cid[P.cidx[p]];
+      }
+    }
+    nseg += __popc(sm);
   }
   for (int f = lane; f < nf; f += 32) {
     const unsigned fw = P.fnew[f];
@@ -399,34 +419,10 @@ __device__ int warp_clip(WarpPoly<C>& P, PolyState& S, double px, double py, dou
     }
   }
   if (lane == 0) P.fs[nb][nfk] = (uint16_t)hk;
-  __syncwarp();
-
-  // 7. lid (:454-495): segments (v,u) between consecutive intersection
-  //    vertices of the new faces, in order; lid_map last writer wins; the
-  //    chain from the first segment becomes the last face.
-  int nseg = 0;
-  for (int b = 0; b < hk; b += 32) {
-    const int q = b + lane;
-    bool sg = false;
-    unsigned u = 0, v = 0;
-    if (q < hk) {
-      const int f2 = P.pf[nb][q];
-      const int q2 = (q + 1 == P.fs[nb][f2 + 1]) ? P.fs[nb][f2] : q + 1;
-      u = P.fi[nb][q];
-      v = P.fi[nb][q2];
-      sg = (int)u >= nkept && (int)v >= nkept;
-    }
-    const unsigned m = __ballot_sync(kFull, sg);
-    if (sg) {
-      const int k = nseg + __popc(m & lt);
-      if (k < C::SCAP) {
-        P.sega[k] = (VId)v;
-        P.segb[k] = (VId)u;
-      }
-    }
-    nseg += __popc(m);
-  }
   if (nseg > C::SCAP) return kClipOverflow;
+
+  // 8. lid (:470-495): lid_map (last writer wins) and the chain from the
+  //    first segment, appended as the last face
   int nhn = hk, nfn = nfk;
   if (nseg > 0) {
     __syncwarp();
@@ -599,25 +595,34 @@ __device__ int compute_cell(const TessDesc& T, uint32_t i, WarpPoly<C>& P, PolyS
       const int l = __ffs(pass) - 1;
       const uint32_t s0 = __shfl_sync(kFull, bs, l);
       const uint32_t s1 = __shfl_sync(kFull, be, l);
+      // the bin's members in ascending id order; each lane holds one member
+      // and its distance, and a ballot against the current radius yields the
+      // members the reference clips with (dist^2 <= 4R^2), re-evaluated
+      // after every clip that changes R
       for (uint32_t mb = s0; mb < s1; mb += 32) {
+        const bool have = mb + lane < s1;
         SortedGen sg = {0.0, 0.0, 0.0, -1};
-        if (mb + lane < s1) sg = T.sorted[mb + lane];
-        const int cntm = (int)min(32u, s1 - mb);
-        for (int j = 0; j < cntm; ++j) {
-          const long long jid = __shfl_sync(kFull, sg.id, j);
-          if (jid == (long long)i) continue;
-          const double qx = __shfl_sync(kFull, sg.x, j);
-          const double qy = __shfl_sync(kFull, sg.y, j);
-          const double qz = __shfl_sync(kFull, sg.z, j);
-          cnt_add(P, kCntCandidates, 1);
-          const double d0 = qx - gx, d1 = qy - gy, d2 = qz - gz;
-          const double dist_sq = d0 * d0 + d1 * d1 + d2 * d2;
-          if (dist_sq > 4.0 * cur) continue;
-          const double mx = gx + d0 * 0.5, my = gy + d1 * 0.5, mz = gz + d2 * 0.5;
-          const int r = warp_clip(P, S, mx, my, mz, d0, d1, d2, (int)jid, true, gx, gy, gz, &r2);
+        if (have) sg = T.sorted[mb + lane];
+        const bool cand = have && sg.id != (long long)i;
+        const double d0 = sg.x - gx, d1 = sg.y - gy, d2 = sg.z - gz;
+        const double dist_sq = d0 * d0 + d1 * d1 + d2 * d2;
+        cnt_add(P, kCntCandidates, (unsigned long long)__popc(__ballot_sync(kFull, cand)));
+        int mpos = 0;
+        while (mpos < 32) {
+          const unsigned mge = ~((1u << mpos) - 1u);
+          const unsigned mpass = __ballot_sync(kFull, cand && !(dist_sq > 4.0 * cur)) & mge;
+          if (!mpass) break;
+          const int j = __ffs(mpass) - 1;
+          const int jid = (int)__shfl_sync(kFull, sg.id, j);
+          const double e0 = __shfl_sync(kFull, d0, j);
+          const double e1 = __shfl_sync(kFull, d1, j);
+          const double e2 = __shfl_sync(kFull, d2, j);
+          const double mx = gx + e0 * 0.5, my = gy + e1 * 0.5, mz = gz + e2 * 0.5;
+          const int r = warp_clip(P, S, mx, my, mz, e0, e1, e2, jid, true, gx, gy, gz, &r2);
           if (r == kClipOverflow) return kCellOverflow;
           if (r == kClipMod) cur = r2;
           else if (r == kClipEmpty) cur = 0.0;
+          mpos = j + 1;
         }
       }
       pos = l + 1;
