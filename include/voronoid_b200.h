@@ -116,9 +116,12 @@ int vd_tess_stream(vd_tess* t, void** stream);
 /* device time (ms, CUDA events) of the phases of the last calculate:
  * [0] binning, [1] clip kernel, [2] overflow/fallback passes, [3] total */
 int vd_tess_timings(vd_tess* t, float* ms4);
-/* algorithmic event counters of the last calculate (same meaning as the
- * oracle's): candidates, clips, classified, modifying, intersections, kept,
- * triangles, offsets */
+/* run calculate with the instrumented kernel variant (off by default; the
+ * counters cost a few percent of the clip kernel's time) */
+int vd_tess_set_instrumentation(vd_tess* t, int on);
+/* algorithmic event counters of the last instrumented calculate (same
+ * meaning as the oracle's): candidates, clips, classified, modifying,
+ * intersections, kept, triangles, offsets; VD_ESTATE when not instrumented */
 int vd_tess_counters(vd_tess* t, uint64_t* out8);
 /* cells that needed a fallback pass in the last calculate:
  * [0] polytope-capacity overflow, [1] search-order extension */

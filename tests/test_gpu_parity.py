@@ -20,6 +20,7 @@ WALL = -1000
 def gpu_tess(bmin, bmax, grid, pts, walls=(), walls_first=False):
     import vorothree_b200 as v
     t = v.Tessellation(v.BoundingBox(bmin, bmax), v.Algorithm3DGrid(*grid))
+    t.set_instrumentation(True)
     if walls_first:
         for w in walls:
             t.add_wall(w)

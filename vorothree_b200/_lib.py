@@ -58,6 +58,7 @@ SIGNATURES = {
     "vd_tess_stream": (C.c_int, [_vp, C.POINTER(_vp)]),
     "vd_tess_timings": (C.c_int, [_vp, C.POINTER(C.c_float)]),
     "vd_tess_counters": (C.c_int, [_vp, _u64p]),
+    "vd_tess_set_instrumentation": (C.c_int, [_vp, C.c_int]),
     "vd_tess_fallback_counts": (C.c_int, [_vp, _u64p]),
     "vd_launch_count": (C.c_int, [_u64p]),
     "vd_host_alloc": (C.c_int, [C.c_size_t, C.POINTER(_vp)]),

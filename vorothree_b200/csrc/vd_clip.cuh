@@ -31,8 +31,9 @@ namespace vd {
 constexpr unsigned kFull = 0xffffffffu;
 
 template <int V, int F, int H, int CC, int NC, int SC, typename VIdT, typename FIdT, typename KeyT,
-          typename CIdT>
+          typename CIdT, bool kCount>
 struct PolyCfg {
+  static constexpr bool COUNT = kCount;  // maintain the algorithmic event counters
   static constexpr int VCAP = V;   // vertices
   static constexpr int FCAP = F;   // faces
   static constexpr int HCAP = H;   // flattened face-index entries
@@ -53,10 +54,12 @@ struct PolyCfg {
 // Fast path: sized from the oracle's distribution (max 72 vertices, 38 faces,
 // 216 face entries over 7.5M uniform-input polytopes); anything larger goes
 // to the large-capacity pass.
-using FastCfg = PolyCfg<96, 48, 288, 64, 32, 32, uint8_t, uint8_t, uint16_t, uint8_t>;
+using FastCfg = PolyCfg<96, 48, 288, 64, 32, 32, uint8_t, uint8_t, uint16_t, uint8_t, false>;
+// the same with the event counters (instrumented runs)
+using FastCfgCount = PolyCfg<96, 48, 288, 64, 32, 32, uint8_t, uint8_t, uint16_t, uint8_t, true>;
 // Large-capacity pass (global-memory storage): vertex ids stay u16 like the
 // reference's face_indices (cell_3d_faces.rs:31).
-using BigCfg = PolyCfg<2048, 512, 6144, 1024, 512, 512, uint16_t, uint16_t, uint32_t, uint16_t>;
+using BigCfg = PolyCfg<2048, 512, 6144, 1024, 512, 512, uint16_t, uint16_t, uint32_t, uint16_t, true>;
 
 template <class C>
 struct alignas(16) WarpPoly {
@@ -112,7 +115,9 @@ __device__ __forceinline__ double clamp01(double t) {
 
 template <class C>
 __device__ __forceinline__ void cnt_add(WarpPoly<C>& P, int k, unsigned long long v) {
-  if (lane_id() == 0) P.cnt[k] += v;
+  if constexpr (C::COUNT) {
+    if (lane_id() == 0) P.cnt[k] += v;
+  }
 }
 
 // Cell3DFaces::new (cell_3d_faces.rs:37-74): the box, faces z-, z+, y-, y+,
@@ -508,6 +513,39 @@ __device__ __forceinline__ bool wall_plane(const Wall& w, double gx, double gy, 
   return true;
 }
 
+// The visitor of tessellation.rs:446-471 over the members of one bin held
+// one per lane (lanes in `mask`, ascending id order): members with
+// dist^2 <= 4R^2 are clipped in order, the ballot re-evaluated after every
+// clip that changes R.
+template <class C>
+__device__ __forceinline__ int visit_members(WarpPoly<C>& P, PolyState& S, const SortedGen& sg, unsigned mask,
+                                             uint32_t i, double gx, double gy, double gz, double& cur) {
+  const unsigned lane = lane_id();
+  const bool cand = ((mask >> lane) & 1u) && sg.id != (long long)i;
+  const double d0 = sg.x - gx, d1 = sg.y - gy, d2 = sg.z - gz;
+  const double dist_sq = d0 * d0 + d1 * d1 + d2 * d2;
+  if constexpr (C::COUNT) cnt_add(P, kCntCandidates, (unsigned long long)__popc(__ballot_sync(kFull, cand)));
+  double r2;
+  int mpos = 0;
+  while (mpos < 32) {
+    const unsigned mge = ~((1u << mpos) - 1u);
+    const unsigned mpass = __ballot_sync(kFull, cand && !(dist_sq > 4.0 * cur)) & mge;
+    if (!mpass) break;
+    const int j = __ffs(mpass) - 1;
+    const int jid = (int)__shfl_sync(kFull, sg.id, j);
+    const double e0 = __shfl_sync(kFull, d0, j);
+    const double e1 = __shfl_sync(kFull, d1, j);
+    const double e2 = __shfl_sync(kFull, d2, j);
+    const double mx = gx + e0 * 0.5, my = gy + e1 * 0.5, mz = gz + e2 * 0.5;
+    const int r = warp_clip(P, S, mx, my, mz, e0, e1, e2, jid, true, gx, gy, gz, &r2);
+    if (r == kClipOverflow) return kCellOverflow;
+    if (r == kClipMod) cur = r2;
+    else if (r == kClipEmpty) cur = 0.0;
+    mpos = j + 1;
+  }
+  return kCellOk;
+}
+
 // compute_cell (tessellation.rs:414-475) with Algorithm3DGrid::visit_neighbors
 // (algo_3d_grid.rs:145-202) and the bisector visitor (tessellation.rs:446-471).
 //
@@ -595,35 +633,11 @@ __device__ int compute_cell(const TessDesc& T, uint32_t i, WarpPoly<C>& P, PolyS
       const int l = __ffs(pass) - 1;
       const uint32_t s0 = __shfl_sync(kFull, bs, l);
       const uint32_t s1 = __shfl_sync(kFull, be, l);
-      // the bin's members in ascending id order; each lane holds one member
-      // and its distance, and a ballot against the current radius yields the
-      // members the reference clips with (dist^2 <= 4R^2), re-evaluated
-      // after every clip that changes R
       for (uint32_t mb = s0; mb < s1; mb += 32) {
-        const bool have = mb + lane < s1;
         SortedGen sg = {0.0, 0.0, 0.0, -1};
-        if (have) sg = T.sorted[mb + lane];
-        const bool cand = have && sg.id != (long long)i;
-        const double d0 = sg.x - gx, d1 = sg.y - gy, d2 = sg.z - gz;
-        const double dist_sq = d0 * d0 + d1 * d1 + d2 * d2;
-        cnt_add(P, kCntCandidates, (unsigned long long)__popc(__ballot_sync(kFull, cand)));
-        int mpos = 0;
-        while (mpos < 32) {
-          const unsigned mge = ~((1u << mpos) - 1u);
-          const unsigned mpass = __ballot_sync(kFull, cand && !(dist_sq > 4.0 * cur)) & mge;
-          if (!mpass) break;
-          const int j = __ffs(mpass) - 1;
-          const int jid = (int)__shfl_sync(kFull, sg.id, j);
-          const double e0 = __shfl_sync(kFull, d0, j);
-          const double e1 = __shfl_sync(kFull, d1, j);
-          const double e2 = __shfl_sync(kFull, d2, j);
-          const double mx = gx + e0 * 0.5, my = gy + e1 * 0.5, mz = gz + e2 * 0.5;
-          const int r = warp_clip(P, S, mx, my, mz, e0, e1, e2, jid, true, gx, gy, gz, &r2);
-          if (r == kClipOverflow) return kCellOverflow;
-          if (r == kClipMod) cur = r2;
-          else if (r == kClipEmpty) cur = 0.0;
-          mpos = j + 1;
-        }
+        if (mb + lane < s1) sg = T.sorted[mb + lane];
+        const unsigned rmask = s1 - mb >= 32 ? kFull : ((1u << (s1 - mb)) - 1u);
+        if (visit_members<C>(P, S, sg, rmask, i, gx, gy, gz, cur) != kCellOk) return kCellOverflow;
       }
       pos = l + 1;
       if (pos >= 32) {
@@ -795,7 +809,9 @@ __device__ void clip_worker(const TessDesc& T, const WorkList& W, WarpPoly<C>& P
     __syncwarp();
   }
   __syncwarp();
-  if (lane < kNumCounters && W.counters) atomicAdd(&W.counters[lane], P.cnt[lane]);
+  if constexpr (C::COUNT) {
+    if (lane < kNumCounters && W.counters) atomicAdd(&W.counters[lane], P.cnt[lane]);
+  }
 }
 
 }  // namespace vd

@@ -77,6 +77,7 @@ struct vd_tess {
   Grid grid{};
   std::vector<Wall> walls;
   int precision = VD_PREC_FP64;
+  bool instrument = false;  // run the counting kernel variant
 
   // search order
   int order_k = 0;
@@ -376,7 +377,8 @@ int clip_pass(vd_tess* t, bool big, const uint32_t* items, uint32_t nitems, uint
     const size_t warps_needed = (nitems + li.warps_per_block - 1) / li.warps_per_block;
     const int nblocks = (int)std::max<size_t>(
         1, std::min<size_t>(warps_needed, (size_t)t->num_sms * std::max(1, li.blocks_per_sm)));
-    VD_CK(t, mixed ? launch_clip_mixed_fast(T, W, nblocks, s) : launch_clip_fp64_fast(T, W, nblocks, s));
+    VD_CK(t, mixed ? launch_clip_mixed_fast(T, W, nblocks, t->instrument, s)
+                   : launch_clip_fp64_fast(T, W, nblocks, t->instrument, s));
     g_launches++;
   } else {
     int r = ensure_big(t, nitems);
@@ -754,6 +756,12 @@ int vd_tess_set_precision(vd_tess* t, int precision) {
   return VD_OK;
 }
 
+int vd_tess_set_instrumentation(vd_tess* t, int on) {
+  if (!t) return VD_EINVAL;
+  t->instrument = on != 0;
+  return VD_OK;
+}
+
 int vd_tess_calculate(vd_tess* t) {
   if (!t) return VD_EINVAL;
   VD_CK(t, cudaSetDevice(t->device));
@@ -933,6 +941,7 @@ int vd_tess_timings(vd_tess* t, float* ms4) {
 
 int vd_tess_counters(vd_tess* t, uint64_t* out8) {
   if (!t || !out8) return VD_EINVAL;
+  if (!t->instrument) return fail(t, VD_ESTATE, "counters need vd_tess_set_instrumentation(t, 1)");
   for (int k = 0; k < kNumCounters; ++k) out8[k] = t->counters[k];
   return VD_OK;
 }

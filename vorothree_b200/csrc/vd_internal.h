@@ -19,7 +19,9 @@ struct ClipLaunchInfo {
 
 // FP64 bit-exact path (vd_kernels_fp64.cu, compiled with -fmad=false)
 cudaError_t clip_fp64_info(ClipLaunchInfo* info);
-cudaError_t launch_clip_fp64_fast(const TessDesc& T, const WorkList& W, int nblocks, cudaStream_t s);
+// count: the instrumented variant that maintains the algorithmic event counters
+cudaError_t launch_clip_fp64_fast(const TessDesc& T, const WorkList& W, int nblocks, bool count,
+                                  cudaStream_t s);
 cudaError_t launch_clip_fp64_big(const TessDesc& T, const WorkList& W, void* scratch, int nwarps,
                                  cudaStream_t s);
 
@@ -28,6 +30,7 @@ void set_thread_error(const char* msg);
 
 // Mixed path (vd_kernels_mixed.cu)
 cudaError_t clip_mixed_info(ClipLaunchInfo* info);
-cudaError_t launch_clip_mixed_fast(const TessDesc& T, const WorkList& W, int nblocks, cudaStream_t s);
+cudaError_t launch_clip_mixed_fast(const TessDesc& T, const WorkList& W, int nblocks, bool count,
+                                   cudaStream_t s);
 
 }  // namespace vd

@@ -23,6 +23,8 @@ __global__ void __launch_bounds__(128) k_clip_big(const TessDesc T, const WorkLi
   clip_worker<C>(T, W, scratch[gw]);
 }
 
+static_assert(sizeof(WarpPoly<FastCfg>) == sizeof(WarpPoly<FastCfgCount>), "same layout");
+
 cudaError_t clip_fp64_info(ClipLaunchInfo* info) {
   info->smem_per_warp = sizeof(WarpPoly<FastCfg>);
   info->warps_per_block = kFastWarpsPerBlock;
@@ -31,6 +33,9 @@ cudaError_t clip_fp64_info(ClipLaunchInfo* info) {
   cudaError_t e = cudaFuncSetAttribute(k_clip_fast<FastCfg, kFastWarpsPerBlock>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(k_clip_fast<FastCfgCount, kFastWarpsPerBlock>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
   int nb = 0;
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_clip_fast<FastCfg, kFastWarpsPerBlock>,
                                                     kFastWarpsPerBlock * 32, smem);
@@ -38,9 +43,13 @@ cudaError_t clip_fp64_info(ClipLaunchInfo* info) {
   return e;
 }
 
-cudaError_t launch_clip_fp64_fast(const TessDesc& T, const WorkList& W, int nblocks, cudaStream_t s) {
+cudaError_t launch_clip_fp64_fast(const TessDesc& T, const WorkList& W, int nblocks, bool count,
+                                  cudaStream_t s) {
   const size_t smem = sizeof(WarpPoly<FastCfg>) * kFastWarpsPerBlock;
-  k_clip_fast<FastCfg, kFastWarpsPerBlock><<<nblocks, kFastWarpsPerBlock * 32, smem, s>>>(T, W);
+  if (count)
+    k_clip_fast<FastCfgCount, kFastWarpsPerBlock><<<nblocks, kFastWarpsPerBlock * 32, smem, s>>>(T, W);
+  else
+    k_clip_fast<FastCfg, kFastWarpsPerBlock><<<nblocks, kFastWarpsPerBlock * 32, smem, s>>>(T, W);
   return cudaGetLastError();
 }
 

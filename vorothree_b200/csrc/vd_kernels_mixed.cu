@@ -8,7 +8,7 @@ cudaError_t clip_mixed_info(ClipLaunchInfo* info) {
   return cudaSuccess;
 }
 
-cudaError_t launch_clip_mixed_fast(const TessDesc&, const WorkList&, int, cudaStream_t) {
+cudaError_t launch_clip_mixed_fast(const TessDesc&, const WorkList&, int, bool, cudaStream_t) {
   return cudaErrorNotSupported;
 }
 

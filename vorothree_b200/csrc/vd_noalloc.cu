@@ -287,7 +287,7 @@ extern "C" int vd_calculate_noalloc(const double bmin[3], const double bmax[3], 
   const size_t warps_needed = (n + wpb - 1) / wpb;
   const int nblocks = (int)std::max<size_t>(
       1, std::min<size_t>(warps_needed, (size_t)D->sms * std::max(1, D->info.blocks_per_sm)));
-  NA_CK(launch_clip_fp64_fast(T, W, nblocks, s));
+  NA_CK(launch_clip_fp64_fast(T, W, nblocks, false, s));
   unsigned int h[3] = {0, 0, 0};
   NA_CK(cudaMemcpyAsync(h, ctl, sizeof(h), cudaMemcpyDeviceToHost, s));
   NA_CK(cudaStreamSynchronize(s));

@@ -356,6 +356,10 @@ class Tessellation:
         self._ck(self._L.vd_tess_timings(self._h, t))
         return {"bin_ms": t[0], "clip_ms": t[1], "fallback_ms": t[2], "total_ms": t[3]}
 
+    def set_instrumentation(self, on: bool):
+        """Count the algorithmic events (candidates, clips, ...) in calculate()."""
+        self._ck(self._L.vd_tess_set_instrumentation(self._h, 1 if on else 0))
+
     def counters(self) -> dict:
         out = (C.c_uint64 * 8)()
         self._ck(self._L.vd_tess_counters(self._h, out))
