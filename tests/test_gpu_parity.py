@@ -17,10 +17,11 @@ pytestmark = pytest.mark.gpu
 WALL = -1000
 
 
-def gpu_tess(bmin, bmax, grid, pts, walls=(), walls_first=False):
+def gpu_tess(bmin, bmax, grid, pts, walls=(), walls_first=False, precision="fp64"):
     import vorothree_b200 as v
     t = v.Tessellation(v.BoundingBox(bmin, bmax), v.Algorithm3DGrid(*grid))
     t.set_instrumentation(True)
+    t.set_precision(precision)
     if walls_first:
         for w in walls:
             t.add_wall(w)
@@ -100,10 +101,14 @@ def test_known_answers():
     assert 1 in t.get_cell(0).face_neighbors() and 0 in t.get_cell(1).face_neighbors()
 
 
+PRECISIONS = ["fp64", "mixed"]
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
 @pytest.mark.parametrize("seed", [0, 1, 2])
-def test_config_a_bitwise(oracle_mod, seed):
+def test_config_a_bitwise(oracle_mod, seed, precision):
     pts = uniform(1000, 0.0, 10.0, seed)
-    g = gpu_tess([0, 0, 0], [10, 10, 10], (10, 10, 10), pts)
+    g = gpu_tess([0, 0, 0], [10, 10, 10], (10, 10, 10), pts, precision=precision)
     o = oracle_tess(oracle_mod, [0, 0, 0], [10, 10, 10], (10, 10, 10), pts)
     assert_same(g, o)
     vol, _, _ = g.summaries()
@@ -129,12 +134,13 @@ def test_voro_golden_through_gpu():
             assert np.any(np.all(np.abs(vv - e) < 1e-4, axis=1))
 
 
-def test_walls_bitwise(oracle_mod):
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_walls_bitwise(oracle_mod, precision):
     import vorothree_b200 as v
     pts = uniform(3000, 0.0, 30.0, 5)
     walls = [v.Wall(WALL, v.SphereGeometry([15, 15, 15], 12.0)),
              v.Wall(WALL - 1, v.PlaneGeometry([15, 15, 15], [1.0, 0.3, 0.0]))]
-    g = gpu_tess([0, 0, 0], [30, 30, 30], (8, 8, 8), pts, walls)
+    g = gpu_tess([0, 0, 0], [30, 30, 30], (8, 8, 8), pts, walls, precision=precision)
     o = oracle_tess(oracle_mod, [0, 0, 0], [30, 30, 30], (8, 8, 8), pts, walls)
     assert_same(g, o)
 
@@ -154,18 +160,20 @@ def test_sphere_lattice_volume(oracle_mod):
     assert abs(vol.sum() - exp) / exp < 0.01
 
 
-def test_blobs_bitwise(oracle_mod):
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_blobs_bitwise(oracle_mod, precision):
     import vorothree_b200 as v
     pts = blobs(20000, 8, 0.01, 0.7, 11)
     walls = [v.Wall(WALL, v.SphereGeometry([0.5, 0.5, 0.5], 0.45))]
-    g = gpu_tess([0, 0, 0], [1, 1, 1], (20, 20, 20), pts, walls)
+    g = gpu_tess([0, 0, 0], [1, 1, 1], (20, 20, 20), pts, walls, precision=precision)
     o = oracle_tess(oracle_mod, [0, 0, 0], [1, 1, 1], (20, 20, 20), pts, walls)
     assert_same(g, o)
 
 
-def test_uniform_100k_bitwise(oracle_mod):
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_uniform_100k_bitwise(oracle_mod, precision):
     pts = uniform(100_000, 0.0, 1.0, 3)
-    g = gpu_tess([0, 0, 0], [1, 1, 1], (46, 46, 46), pts)
+    g = gpu_tess([0, 0, 0], [1, 1, 1], (46, 46, 46), pts, precision=precision)
     o = oracle_tess(oracle_mod, [0, 0, 0], [1, 1, 1], (46, 46, 46), pts)
     assert_same(g, o)
 
@@ -224,3 +232,17 @@ def test_set_generator_moves_bin(oracle_mod):
     assert np.allclose(t.get_generator(3), [0.91, 0.92, 0.93])
     vol, _, _ = t.summaries()
     assert abs(vol.sum() - 1.0) < 1e-9
+
+
+@pytest.mark.parametrize("scale,offset", [(1000.0, 0.0), (1e-3, 0.0), (1.0, 5000.0)])
+def test_mixed_equals_fp64_across_scales(scale, offset):
+    """The FP32 classification's error bound must hold at every coordinate
+    scale: mixed results equal the FP64 path bit for bit."""
+    pts = uniform(20000, 0.0, 1.0, 12) * scale + offset
+    lo, hi = [offset] * 3, [offset + scale] * 3
+    a = gpu_tess(lo, hi, (27, 27, 27), pts)
+    b = gpu_tess(lo, hi, (27, 27, 27), pts, precision="mixed")
+    av, ac, an = a.summaries()
+    bv, bc, bn = b.summaries()
+    assert np.array_equal(an, bn) and np.array_equal(av, bv) and np.array_equal(ac, bc)
+    assert np.array_equal(a.neighbors()[1], b.neighbors()[1])

@@ -31,9 +31,10 @@ namespace vd {
 constexpr unsigned kFull = 0xffffffffu;
 
 template <int V, int F, int H, int CC, int NC, int SC, typename VIdT, typename FIdT, typename KeyT,
-          typename CIdT, bool kCount>
+          typename CIdT, bool kCount, bool kMixed>
 struct PolyCfg {
   static constexpr bool COUNT = kCount;  // maintain the algorithmic event counters
+  static constexpr bool MIXED = kMixed;  // FP32 classification under an error bound
   static constexpr int VCAP = V;   // vertices
   static constexpr int FCAP = F;   // faces
   static constexpr int HCAP = H;   // flattened face-index entries
@@ -54,17 +55,23 @@ struct PolyCfg {
 // Fast path: sized from the oracle's distribution (max 72 vertices, 38 faces,
 // 216 face entries over 7.5M uniform-input polytopes); anything larger goes
 // to the large-capacity pass.
-using FastCfg = PolyCfg<96, 48, 288, 64, 32, 32, uint8_t, uint8_t, uint16_t, uint8_t, false>;
+using FastCfg = PolyCfg<96, 48, 288, 64, 32, 32, uint8_t, uint8_t, uint16_t, uint8_t, false, false>;
 // the same with the event counters (instrumented runs)
-using FastCfgCount = PolyCfg<96, 48, 288, 64, 32, 32, uint8_t, uint8_t, uint16_t, uint8_t, true>;
+using FastCfgCount = PolyCfg<96, 48, 288, 64, 32, 32, uint8_t, uint8_t, uint16_t, uint8_t, true, false>;
+// mixed precision: same capacities, FP32 generator-relative copies of the vertices
+using MixedCfg = PolyCfg<96, 48, 288, 64, 32, 32, uint8_t, uint8_t, uint16_t, uint8_t, false, true>;
+using MixedCfgCount = PolyCfg<96, 48, 288, 64, 32, 32, uint8_t, uint8_t, uint16_t, uint8_t, true, true>;
 // Large-capacity pass (global-memory storage): vertex ids stay u16 like the
 // reference's face_indices (cell_3d_faces.rs:31).
-using BigCfg = PolyCfg<2048, 512, 6144, 1024, 512, 512, uint16_t, uint16_t, uint32_t, uint16_t, true>;
+using BigCfg = PolyCfg<2048, 512, 6144, 1024, 512, 512, uint16_t, uint16_t, uint32_t, uint16_t, true, false>;
 
 template <class C>
 struct alignas(16) WarpPoly {
   double vx[C::VCAP], vy[C::VCAP], vz[C::VCAP];
-  double dist[C::VCAP];
+  // plain path: the FP64 signed distances of the current clip
+  double dist[C::MIXED ? 1 : C::VCAP];
+  // mixed path: FP32 copies of the vertices relative to the generator
+  float ux[C::MIXED ? C::VCAP : 1], uy[C::MIXED ? C::VCAP : 1], uz[C::MIXED ? C::VCAP : 1];
   double tx[C::NCAP], ty[C::NCAP], tz[C::NCAP];
   unsigned long long cnt[kNumCounters];
   int32_t fn[2][C::FCAP];
@@ -86,6 +93,7 @@ struct alignas(16) WarpPoly {
 
 struct PolyState {
   int nv, nf, nh, cb;
+  double umax;  // mixed path: bound on |v - g| (max norm) over the vertices
 };
 
 __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
@@ -123,7 +131,7 @@ __device__ __forceinline__ void cnt_add(WarpPoly<C>& P, int k, unsigned long lon
 // Cell3DFaces::new (cell_3d_faces.rs:37-74): the box, faces z-, z+, y-, y+,
 // x-, x+ with ids box_side (bounds/mod.rs:21-22).
 template <class C>
-__device__ void poly_init_box(WarpPoly<C>& P, PolyState& S, const Grid& g) {
+__device__ void poly_init_box(WarpPoly<C>& P, PolyState& S, const Grid& g, double gx, double gy, double gz) {
   const unsigned lane = lane_id();
   if (lane < 8) {
     const unsigned hx = (lane == 1 || lane == 2 || lane == 5 || lane == 6);
@@ -147,6 +155,18 @@ __device__ void poly_init_box(WarpPoly<C>& P, PolyState& S, const Grid& g) {
   S.nf = 6;
   S.nh = 24;
   S.cb = 0;
+  S.umax = 0.0;
+  if constexpr (C::MIXED) {
+    double m = 0.0;
+    if (lane < 8) {
+      const float fx = (float)(P.vx[lane] - gx), fy = (float)(P.vy[lane] - gy), fz = (float)(P.vz[lane] - gz);
+      P.ux[lane] = fx;
+      P.uy[lane] = fy;
+      P.uz[lane] = fz;
+      m = fmax(fabs((double)fx), fmax(fabs((double)fy), fabs((double)fz)));
+    }
+    S.umax = warp_max(m) * (1.0 + 0x1p-20);
+  }
   __syncwarp();
 }
 
@@ -187,13 +207,50 @@ __device__ int warp_clip(WarpPoly<C>& P, PolyState& S, double px, double py, dou
   cnt_add(P, kCntClips, 1);
   cnt_add(P, kCntClassified, (unsigned long long)nv);
 
-  // 1. signed distances and the 3-band flags (:302-326)
+  // 1. signed distances and the 3-band flags (:302-326); o2n marks the
+  //    vertices to keep (d <= 1e-9) until step 2 numbers them
   bool out = false, sin = false;
-  for (int v = lane; v < nv; v += 32) {
-    double d = (P.vx[v] - px) * nx + (P.vy[v] - py) * ny + (P.vz[v] - pz) * nz;
-    P.dist[v] = d;
-    out |= d > kTol;
-    sin |= d < -kTol;
+  if constexpr (!C::MIXED) {
+    for (int v = lane; v < nv; v += 32) {
+      double d = (P.vx[v] - px) * nx + (P.vy[v] - py) * ny + (P.vz[v] - pz) * nz;
+      P.dist[v] = d;
+      P.o2n[v] = d > kTol ? (VId)C::VNONE : (VId)0;
+      out |= d > kTol;
+      sin |= d < -kTol;
+    }
+  } else {
+    // FP32 distance on generator-relative coordinates, d32 = u.n - c with
+    // c = (p - g).n.  Forward error bound against the FP64 value
+    // d64 = (v - p).n of the plain path (u = fl32(fl64(v - g))):
+    //   |d32 - d64| <= 2^-21 (|u|_inf |n|_1 + |c| + sum_k |(p_k - g_k) n_k|) + 1e-30.
+    // A vertex whose d32 lies within that bound of +-1e-9 is re-evaluated
+    // with the plain path's FP64 formula, so every decision equals it.
+    const double qx = px - gx, qy = py - gy, qz = pz - gz;
+    const double c = qx * nx + qy * ny + qz * nz;
+    const double qn = fabs(qx * nx) + fabs(qy * ny) + fabs(qz * nz);
+    const double scale = S.umax * (fabs(nx) + fabs(ny) + fabs(nz)) + fabs(c);
+    const double bound = 0x1p-21 * (scale + qn) + 1e-30;
+    const bool fp32_ok = scale > 1e-24 && scale < 1e24;
+    const float fnx = (float)nx, fny = (float)ny, fnz = (float)nz, fc = (float)c;
+    const double hi_out = kTol + bound, lo_sin = -kTol - bound;
+    const double band_lo = -kTol + bound, band_hi = kTol - bound;
+    for (int v = lane; v < nv; v += 32) {
+      bool o = false, si = false, exact = !fp32_ok;
+      if (fp32_ok) {
+        const double d32 = (double)(fmaf(P.ux[v], fnx, fmaf(P.uy[v], fny, P.uz[v] * fnz)) - fc);
+        if (d32 > hi_out) o = true;
+        else if (d32 < lo_sin) si = true;
+        else exact = !(d32 >= band_lo && d32 <= band_hi);
+      }
+      if (exact) {
+        const double d = (P.vx[v] - px) * nx + (P.vy[v] - py) * ny + (P.vz[v] - pz) * nz;
+        o = d > kTol;
+        si = d < -kTol;
+      }
+      P.o2n[v] = o ? (VId)C::VNONE : (VId)0;
+      out |= o;
+      sin |= si;
+    }
   }
   if (!__any_sync(kFull, out)) {
     *r2out = 0.0;
@@ -212,7 +269,7 @@ __device__ int warp_clip(WarpPoly<C>& P, PolyState& S, double px, double py, dou
   double r2 = 0.0;
   for (int b = 0; b < nv; b += 32) {
     const int v = b + lane;
-    const bool k = v < nv && P.dist[v] <= kTol;
+    const bool k = v < nv && P.o2n[v] != C::VNONE;
     const unsigned m = __ballot_sync(kFull, k);
     if (v < nv) P.o2n[v] = k ? (VId)(nkept + __popc(m & lt)) : (VId)C::VNONE;
     if (k && with_gen) {
@@ -296,7 +353,14 @@ __device__ int warp_clip(WarpPoly<C>& P, PolyState& S, double px, double py, dou
       if (r < C::NCAP) {
         const int p = P.cpos[k];
         const int s = P.fi[cb][p], e = P.fe[p];
-        const double ds = P.dist[s], de = P.dist[e];
+        double ds, de;
+        if constexpr (!C::MIXED) {
+          ds = P.dist[s];
+          de = P.dist[e];
+        } else {  // the plain path's FP64 distances, needed only here
+          ds = (P.vx[s] - px) * nx + (P.vy[s] - py) * ny + (P.vz[s] - pz) * nz;
+          de = (P.vx[e] - px) * nx + (P.vy[e] - py) * ny + (P.vz[e] - pz) * nz;
+        }
         const double t = clamp01(ds / (ds - de));
         const double ax = P.vx[s], ay = P.vy[s], az = P.vz[s];
         const double bx = P.vx[e], by = P.vy[e], bz = P.vz[e];
@@ -323,21 +387,34 @@ __device__ int warp_clip(WarpPoly<C>& P, PolyState& S, double px, double py, dou
   if (nnew > C::NCAP || nvn > C::VCAP) return kClipOverflow;
 
   // 5. new vertex list: kept vertices compacted in place, then intersections
+  double um = 0.0;
   for (int b = 0; b < nv; b += 32) {
     const int v = b + lane;
     unsigned o = C::VNONE;
     double x = 0.0, y = 0.0, z = 0.0;
+    float fx = 0.f, fy = 0.f, fz = 0.f;
     if (v < nv) {
       o = P.o2n[v];
       x = P.vx[v];
       y = P.vy[v];
       z = P.vz[v];
+      if constexpr (C::MIXED) {
+        fx = P.ux[v];
+        fy = P.uy[v];
+        fz = P.uz[v];
+      }
     }
     __syncwarp();
     if (o != C::VNONE) {
       P.vx[o] = x;
       P.vy[o] = y;
       P.vz[o] = z;
+      if constexpr (C::MIXED) {
+        P.ux[o] = fx;
+        P.uy[o] = fy;
+        P.uz[o] = fz;
+        um = fmax(um, fmax(fabs((double)fx), fmax(fabs((double)fy), fabs((double)fz))));
+      }
     }
     __syncwarp();
   }
@@ -345,7 +422,15 @@ __device__ int warp_clip(WarpPoly<C>& P, PolyState& S, double px, double py, dou
     P.vx[nkept + r] = P.tx[r];
     P.vy[nkept + r] = P.ty[r];
     P.vz[nkept + r] = P.tz[r];
+    if constexpr (C::MIXED) {
+      const float fx = (float)(P.tx[r] - gx), fy = (float)(P.ty[r] - gy), fz = (float)(P.tz[r] - gz);
+      P.ux[nkept + r] = fx;
+      P.uy[nkept + r] = fy;
+      P.uz[nkept + r] = fz;
+      um = fmax(um, fmax(fabs((double)fx), fmax(fabs((double)fy), fabs((double)fz))));
+    }
   }
+  if constexpr (C::MIXED) S.umax = warp_max(um) * (1.0 + 0x1p-20);
 
   // 6. surviving faces (>= 3 entries, :454-467) and their new starts
   int nfk = 0, hk = 0;
@@ -561,7 +646,7 @@ __device__ int compute_cell(const TessDesc& T, uint32_t i, WarpPoly<C>& P, PolyS
   const unsigned lane = lane_id();
   const double gx = T.gen[3 * (size_t)i], gy = T.gen[3 * (size_t)i + 1], gz = T.gen[3 * (size_t)i + 2];
   double r2;
-  poly_init_box(P, S, T.grid);
+  poly_init_box(P, S, T.grid, gx, gy, gz);
   for (int w = 0; w < T.nwalls; ++w) {
     double p[3], n[3];
     if (wall_plane(T.walls[w], gx, gy, gz, p, n)) {
@@ -812,6 +897,25 @@ __device__ void clip_worker(const TessDesc& T, const WorkList& W, WarpPoly<C>& P
   if constexpr (C::COUNT) {
     if (lane < kNumCounters && W.counters) atomicAdd(&W.counters[lane], P.cnt[lane]);
   }
+}
+
+// The kernels: persistent warps over a work list; the fast path keeps each
+// warp's polytope in shared memory, the large-capacity pass in a slice of a
+// global scratch buffer.
+constexpr int kFastWarpsPerBlock = 4;
+
+// MINB: blocks per SM the register budget must admit (shared memory sets it)
+template <class C, int WPB, int MINB>
+__global__ void __launch_bounds__(WPB * 32, MINB) k_clip_fast(const TessDesc T, const WorkList W) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  WarpPoly<C>* polys = reinterpret_cast<WarpPoly<C>*>(smem);
+  clip_worker<C>(T, W, polys[threadIdx.x >> 5]);
+}
+
+template <class C>
+__global__ void __launch_bounds__(128) k_clip_big(const TessDesc T, const WorkList W, WarpPoly<C>* scratch) {
+  const size_t gw = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  clip_worker<C>(T, W, scratch[gw]);
 }
 
 }  // namespace vd

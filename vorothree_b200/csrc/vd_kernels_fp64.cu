@@ -8,36 +8,25 @@
 
 namespace vd {
 
-constexpr int kFastWarpsPerBlock = 4;
-
-template <class C, int WPB>
-__global__ void __launch_bounds__(WPB * 32) k_clip_fast(const TessDesc T, const WorkList W) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  WarpPoly<C>* polys = reinterpret_cast<WarpPoly<C>*>(smem);
-  clip_worker<C>(T, W, polys[threadIdx.x >> 5]);
-}
-
-template <class C>
-__global__ void __launch_bounds__(128) k_clip_big(const TessDesc T, const WorkList W, WarpPoly<C>* scratch) {
-  const size_t gw = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  clip_worker<C>(T, W, scratch[gw]);
-}
-
 static_assert(sizeof(WarpPoly<FastCfg>) == sizeof(WarpPoly<FastCfgCount>), "same layout");
+
+// shared memory admits 7 blocks of 4 warps per SM; keep registers in step
+// (without the bound ptxas takes ~100 registers and only 4 blocks fit)
+constexpr int kFp64MinBlocks = 7;
 
 cudaError_t clip_fp64_info(ClipLaunchInfo* info) {
   info->smem_per_warp = sizeof(WarpPoly<FastCfg>);
   info->warps_per_block = kFastWarpsPerBlock;
   info->big_scratch_per_warp = sizeof(WarpPoly<BigCfg>);
   const size_t smem = sizeof(WarpPoly<FastCfg>) * kFastWarpsPerBlock;
-  cudaError_t e = cudaFuncSetAttribute(k_clip_fast<FastCfg, kFastWarpsPerBlock>,
+  cudaError_t e = cudaFuncSetAttribute(k_clip_fast<FastCfg, kFastWarpsPerBlock, kFp64MinBlocks>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(k_clip_fast<FastCfgCount, kFastWarpsPerBlock>,
+  e = cudaFuncSetAttribute(k_clip_fast<FastCfgCount, kFastWarpsPerBlock, kFp64MinBlocks>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int nb = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_clip_fast<FastCfg, kFastWarpsPerBlock>,
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_clip_fast<FastCfg, kFastWarpsPerBlock, kFp64MinBlocks>,
                                                     kFastWarpsPerBlock * 32, smem);
   info->blocks_per_sm = nb;
   return e;
@@ -47,9 +36,9 @@ cudaError_t launch_clip_fp64_fast(const TessDesc& T, const WorkList& W, int nblo
                                   cudaStream_t s) {
   const size_t smem = sizeof(WarpPoly<FastCfg>) * kFastWarpsPerBlock;
   if (count)
-    k_clip_fast<FastCfgCount, kFastWarpsPerBlock><<<nblocks, kFastWarpsPerBlock * 32, smem, s>>>(T, W);
+    k_clip_fast<FastCfgCount, kFastWarpsPerBlock, kFp64MinBlocks><<<nblocks, kFastWarpsPerBlock * 32, smem, s>>>(T, W);
   else
-    k_clip_fast<FastCfg, kFastWarpsPerBlock><<<nblocks, kFastWarpsPerBlock * 32, smem, s>>>(T, W);
+    k_clip_fast<FastCfg, kFastWarpsPerBlock, kFp64MinBlocks><<<nblocks, kFastWarpsPerBlock * 32, smem, s>>>(T, W);
   return cudaGetLastError();
 }
 
