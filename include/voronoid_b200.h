@@ -134,6 +134,48 @@ int vd_launch_count(uint64_t* n);
 int vd_host_alloc(size_t bytes, void** ptr);
 int vd_host_free(void* ptr);
 
+/* ---- batches: many independent tessellations in one persistent launch ----
+ * Each member is a Tessellation with its own bounds, grid, walls and
+ * generators and computes exactly what a vd_tess with the same inputs
+ * computes; the batch only shares the launches (no counterpart in the
+ * reference, which computes one tessellation per call). */
+typedef struct vd_batch vd_batch;
+/* a wall of a batch member: kind 0 = PlaneGeometry (a = point, n = normal
+ * into the valid region, normalised here as in wall_3d.rs:23-27),
+ * kind 1 = SphereGeometry (a = centre, r = radius); id <= VD_WALL_ID_MAX */
+typedef struct {
+  int kind;
+  int id;
+  double a[3];
+  double n[3];
+  double r;
+} vd_wall_desc;
+int vd_batch_create(vd_batch** out);
+int vd_batch_destroy(vd_batch* b);
+const char* vd_batch_last_error(const vd_batch* b);
+/* add a member: Tessellation::new + add_wall(s) + set_generators (host AoS);
+ * *index receives its position in the batch */
+int vd_batch_add(vd_batch* b, const double bmin[3], const double bmax[3], int nx, int ny, int nz,
+                 const vd_wall_desc* walls, int nwalls, const double* xyz, size_t n, int* index);
+int vd_batch_set_precision(vd_batch* b, int precision);
+int vd_batch_set_instrumentation(vd_batch* b, int on);
+/* upload every member and bin it (after the last vd_batch_add) */
+int vd_batch_commit(vd_batch* b);
+/* Tessellation::calculate for every member, one persistent launch */
+int vd_batch_calculate(vd_batch* b);
+/* steps x (Tessellation::relax then calculate) for every member, on the
+ * device; a step is captured once in a CUDA graph and replayed */
+int vd_batch_lloyd(vd_batch* b, int steps);
+int vd_batch_count(const vd_batch* b, int* ntess);
+int vd_batch_count_cells(const vd_batch* b, int index, size_t* n);
+int vd_batch_total_cells(const vd_batch* b, size_t* n);
+int vd_batch_get_generators(vd_batch* b, int index, double* xyz);
+int vd_batch_get_summaries(vd_batch* b, int index, double* volume, double* centroid3, int32_t* n_faces);
+/* device time (ms) of the last calculate / lloyd call */
+int vd_batch_timing(const vd_batch* b, float* ms);
+int vd_batch_counters(const vd_batch* b, uint64_t* out8);
+int vd_batch_stream(vd_batch* b, void** stream);
+
 /* ---- allocation-free variant (no counterpart in the reference) ----
  * set_generators + calculate for a small tessellation without any device
  * allocation, for callers that cannot call cudaMalloc: a plugin inside an

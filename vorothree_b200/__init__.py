@@ -7,8 +7,9 @@ ABI (include/voronoid_b200.h); this package is the Python mirror of the
 reference's API over that ABI.
 """
 from ._lib import VoronoidError, load
+from .batch import TessellationBatch
 from .tessellation import (WALL_ID_MAX, Algorithm3DGrid, BoundingBox, Cell3DFaces, PlaneGeometry,
                            SphereGeometry, Tessellation, Wall, box_side)
 
 __all__ = ["Algorithm3DGrid", "BoundingBox", "Cell3DFaces", "PlaneGeometry", "SphereGeometry",
-           "Tessellation", "Wall", "WALL_ID_MAX", "box_side", "VoronoidError", "load"]
+           "Tessellation", "TessellationBatch", "Wall", "WALL_ID_MAX", "box_side", "VoronoidError", "load"]

@@ -64,6 +64,24 @@ SIGNATURES = {
     "vd_host_alloc": (C.c_int, [C.c_size_t, C.POINTER(_vp)]),
     "vd_host_free": (C.c_int, [_vp]),
     "vd_measure_fma_peak": (C.c_int, [C.c_int, _d]),
+    "vd_batch_create": (C.c_int, [C.POINTER(_vp)]),
+    "vd_batch_destroy": (C.c_int, [_vp]),
+    "vd_batch_last_error": (C.c_char_p, [_vp]),
+    "vd_batch_add": (C.c_int, [_vp, _d, _d, C.c_int, C.c_int, C.c_int, _vp, C.c_int, _d, C.c_size_t,
+                               C.POINTER(C.c_int)]),
+    "vd_batch_set_precision": (C.c_int, [_vp, C.c_int]),
+    "vd_batch_set_instrumentation": (C.c_int, [_vp, C.c_int]),
+    "vd_batch_commit": (C.c_int, [_vp]),
+    "vd_batch_calculate": (C.c_int, [_vp]),
+    "vd_batch_lloyd": (C.c_int, [_vp, C.c_int]),
+    "vd_batch_count": (C.c_int, [_vp, C.POINTER(C.c_int)]),
+    "vd_batch_count_cells": (C.c_int, [_vp, C.c_int, _szp]),
+    "vd_batch_total_cells": (C.c_int, [_vp, _szp]),
+    "vd_batch_get_generators": (C.c_int, [_vp, C.c_int, _d]),
+    "vd_batch_get_summaries": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp]),
+    "vd_batch_timing": (C.c_int, [_vp, C.POINTER(C.c_float)]),
+    "vd_batch_counters": (C.c_int, [_vp, _u64p]),
+    "vd_batch_stream": (C.c_int, [_vp, C.POINTER(_vp)]),
     "vd_calculate_noalloc": (C.c_int, [_d, _d, C.c_int, C.c_int, C.c_int, _vp, C.c_size_t, _vp, _vp, _vp,
                                        _vp]),
 }

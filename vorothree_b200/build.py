@@ -27,6 +27,7 @@ SOURCES = [
     ("vd_host.cu", False),
     ("vd_measure.cu", True),
     ("vd_noalloc.cu", False),
+    ("vd_batch.cu", False),
 ]
 
 

@@ -899,6 +899,55 @@ __device__ void clip_worker(const TessDesc& T, const WorkList& W, WarpPoly<C>& P
   }
 }
 
+// Batched mode: one work item per cell of many tessellations.  Items are
+// global positions in the concatenated bin-ordered generator array;
+// tess_off[t] is tessellation t's first position (tess_off[ntess] = total).
+__device__ __forceinline__ int find_tess(const uint32_t* tess_off, int ntess, uint32_t item) {
+  int lo = 0, hi = ntess;  // largest t with tess_off[t] <= item
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (tess_off[mid] <= item) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+template <class C>
+__device__ void clip_worker_batched(const TessDesc* descs, const uint32_t* tess_off, int ntess,
+                                    const WorkList& W, WarpPoly<C>& P) {
+  const unsigned lane = lane_id();
+  if (lane < kNumCounters) P.cnt[lane] = 0;
+  const uint32_t nitems = W.nitems_dev ? *W.nitems_dev : W.nitems;
+  __syncwarp();
+  while (true) {
+    unsigned idx = 0;
+    if (lane == 0) idx = atomicAdd(W.cursor, 1u);
+    idx = __shfl_sync(kFull, idx, 0);
+    if (idx >= nitems) break;
+    const uint32_t item = W.items ? W.items[idx] : idx;
+    const int t = find_tess(tess_off, ntess, item);
+    const TessDesc& T = descs[t];
+    const uint32_t cell = (uint32_t)T.sorted[item].id;
+    PolyState S;
+    const int st = compute_cell<C>(T, cell, P, S);
+    if (st == kCellOk) {
+      finalize_cell<C>(T, cell, P, S);
+    } else if (lane == 0) {
+      T.status[cell] = (uint8_t)st;
+      if (st == kCellOverflow && W.ovf_list) W.ovf_list[atomicAdd(W.ovf_count, 1u)] = item;
+      if (st == kCellTable) {
+        if (W.tab_list) W.tab_list[atomicAdd(W.tab_count, 1u)] = item;
+        if (W.tess_flags) atomicOr(&W.tess_flags[t], 1u);
+      }
+    }
+    __syncwarp();
+  }
+  __syncwarp();
+  if constexpr (C::COUNT) {
+    if (lane < kNumCounters && W.counters) atomicAdd(&W.counters[lane], P.cnt[lane]);
+  }
+}
+
 // The kernels: persistent warps over a work list; the fast path keeps each
 // warp's polytope in shared memory, the large-capacity pass in a slice of a
 // global scratch buffer.
@@ -916,6 +965,22 @@ template <class C>
 __global__ void __launch_bounds__(128) k_clip_big(const TessDesc T, const WorkList W, WarpPoly<C>* scratch) {
   const size_t gw = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   clip_worker<C>(T, W, scratch[gw]);
+}
+
+template <class C, int WPB, int MINB>
+__global__ void __launch_bounds__(WPB * 32, MINB)
+    k_clip_fast_batched(const TessDesc* descs, const uint32_t* tess_off, int ntess, const WorkList W) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  WarpPoly<C>* polys = reinterpret_cast<WarpPoly<C>*>(smem);
+  clip_worker_batched<C>(descs, tess_off, ntess, W, polys[threadIdx.x >> 5]);
+}
+
+template <class C>
+__global__ void __launch_bounds__(128)
+    k_clip_big_batched(const TessDesc* descs, const uint32_t* tess_off, int ntess, const WorkList W,
+                       WarpPoly<C>* scratch) {
+  const size_t gw = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  clip_worker_batched<C>(descs, tess_off, ntess, W, scratch[gw]);
 }
 
 }  // namespace vd

@@ -98,14 +98,16 @@ struct TessDesc {
 
 // Work description of one launch of a clip kernel.
 struct WorkList {
-  const uint32_t* items;     // cell ids; nullptr = sorted order over all cells
+  const uint32_t* items;     // cell ids (batched: sorted positions); nullptr = all, in bin order
   uint32_t nitems;
+  const uint32_t* nitems_dev;  // when set, the item count is read from device memory
   unsigned int* cursor;      // persistent-warp work counter
   uint32_t* ovf_list;        // cells that overflowed the capacities
   unsigned int* ovf_count;
   uint32_t* tab_list;        // cells that ran off a truncated search order
   unsigned int* tab_count;
   unsigned long long* counters;  // kNumCounters
+  unsigned int* tess_flags;      // batched: per tessellation, set when a cell needs a longer search order
   // optional full-polytope export of a single cell (get_cell)
   double* ex_verts;
   uint32_t* ex_fc;

@@ -25,6 +25,16 @@ cudaError_t launch_clip_fp64_fast(const TessDesc& T, const WorkList& W, int nblo
 cudaError_t launch_clip_fp64_big(const TessDesc& T, const WorkList& W, void* scratch, int nwarps,
                                  cudaStream_t s);
 
+// batched mode (descriptors in device memory; see clip_worker_batched)
+cudaError_t clip_fp64_batched_setup();
+cudaError_t clip_mixed_batched_setup();
+cudaError_t launch_clip_fp64_fast_batched(const TessDesc* descs, const uint32_t* tess_off, int ntess,
+                                          const WorkList& W, int nblocks, bool count, cudaStream_t s);
+cudaError_t launch_clip_mixed_fast_batched(const TessDesc* descs, const uint32_t* tess_off, int ntess,
+                                           const WorkList& W, int nblocks, bool count, cudaStream_t s);
+cudaError_t launch_clip_fp64_big_batched(const TessDesc* descs, const uint32_t* tess_off, int ntess,
+                                         const WorkList& W, void* scratch, int nwarps, cudaStream_t s);
+
 // message returned by vd_last_error(NULL) on the calling thread
 void set_thread_error(const char* msg);
 

@@ -49,4 +49,32 @@ cudaError_t launch_clip_fp64_big(const TessDesc& T, const WorkList& W, void* scr
   return cudaGetLastError();
 }
 
+cudaError_t launch_clip_fp64_fast_batched(const TessDesc* descs, const uint32_t* tess_off, int ntess,
+                                          const WorkList& W, int nblocks, bool count, cudaStream_t s) {
+  const size_t smem = sizeof(WarpPoly<FastCfg>) * kFastWarpsPerBlock;
+  if (count)
+    k_clip_fast_batched<FastCfgCount, kFastWarpsPerBlock, kFp64MinBlocks>
+        <<<nblocks, kFastWarpsPerBlock * 32, smem, s>>>(descs, tess_off, ntess, W);
+  else
+    k_clip_fast_batched<FastCfg, kFastWarpsPerBlock, kFp64MinBlocks>
+        <<<nblocks, kFastWarpsPerBlock * 32, smem, s>>>(descs, tess_off, ntess, W);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_clip_fp64_big_batched(const TessDesc* descs, const uint32_t* tess_off, int ntess,
+                                         const WorkList& W, void* scratch, int nwarps, cudaStream_t s) {
+  k_clip_big_batched<BigCfg><<<nwarps / 4, 128, 0, s>>>(descs, tess_off, ntess, W,
+                                                       reinterpret_cast<WarpPoly<BigCfg>*>(scratch));
+  return cudaGetLastError();
+}
+
+cudaError_t clip_fp64_batched_setup() {
+  const size_t smem = sizeof(WarpPoly<FastCfg>) * kFastWarpsPerBlock;
+  cudaError_t e = cudaFuncSetAttribute(k_clip_fast_batched<FastCfg, kFastWarpsPerBlock, kFp64MinBlocks>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_clip_fast_batched<FastCfgCount, kFastWarpsPerBlock, kFp64MinBlocks>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
 }  // namespace vd

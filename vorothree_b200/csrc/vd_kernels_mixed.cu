@@ -45,4 +45,25 @@ cudaError_t launch_clip_mixed_fast(const TessDesc& T, const WorkList& W, int nbl
   return cudaGetLastError();
 }
 
+cudaError_t launch_clip_mixed_fast_batched(const TessDesc* descs, const uint32_t* tess_off, int ntess,
+                                           const WorkList& W, int nblocks, bool count, cudaStream_t s) {
+  const size_t smem = sizeof(WarpPoly<MixedCfg>) * kFastWarpsPerBlock;
+  if (count)
+    k_clip_fast_batched<MixedCfgCount, kFastWarpsPerBlock, kMixedMinBlocks>
+        <<<nblocks, kFastWarpsPerBlock * 32, smem, s>>>(descs, tess_off, ntess, W);
+  else
+    k_clip_fast_batched<MixedCfg, kFastWarpsPerBlock, kMixedMinBlocks>
+        <<<nblocks, kFastWarpsPerBlock * 32, smem, s>>>(descs, tess_off, ntess, W);
+  return cudaGetLastError();
+}
+
+cudaError_t clip_mixed_batched_setup() {
+  const size_t smem = sizeof(WarpPoly<MixedCfg>) * kFastWarpsPerBlock;
+  cudaError_t e = cudaFuncSetAttribute(k_clip_fast_batched<MixedCfg, kFastWarpsPerBlock, kMixedMinBlocks>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_clip_fast_batched<MixedCfgCount, kFastWarpsPerBlock, kMixedMinBlocks>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
 }  // namespace vd
