@@ -122,3 +122,13 @@ def test_batch_volumes_fill_boxes():
         vol, _, _ = b.summaries(k)
         box = np.prod(np.subtract(bmax, bmin))
         assert abs(vol.sum() - box) < 1e-9 * box
+
+
+def test_batch_dense_blob_overflow_tiers():
+    rng = np.random.Generator(np.random.PCG64(18))
+    dense = np.concatenate([0.5 + rng.normal(0.0, 0.01, size=(2500, 3)), rng.uniform(0, 1, size=(300, 3))])
+    ms = [([0, 0, 0], [1, 1, 1], (4, 4, 4), dense, []),
+          ([0, 0, 0], [1, 1, 1], (10, 10, 10), uniform(1000, 0, 1, 19), [])]
+    b = build_batch(ms)
+    for k, m in enumerate(ms):
+        assert_member_equal(b, k, standalone(m))

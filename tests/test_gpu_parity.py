@@ -246,3 +246,17 @@ def test_mixed_equals_fp64_across_scales(scale, offset):
     bv, bc, bn = b.summaries()
     assert np.array_equal(an, bn) and np.array_equal(av, bv) and np.array_equal(ac, bc)
     assert np.array_equal(a.neighbors()[1], b.neighbors()[1])
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_dense_blob_overflow_tiers(oracle_mod, precision):
+    """A dense blob on a coarse grid: the reference's bin-order walk clips each
+    cell with thousands of candidates and the intermediate polytopes outgrow
+    the fast path; the medium and large-capacity passes must give the oracle's
+    bits."""
+    rng = np.random.Generator(np.random.PCG64(17))
+    pts = np.concatenate([0.5 + rng.normal(0.0, 0.01, size=(2500, 3)), rng.uniform(0, 1, size=(300, 3))])
+    g = gpu_tess([0, 0, 0], [1, 1, 1], (4, 4, 4), pts, precision=precision)
+    o = oracle_tess(oracle_mod, [0, 0, 0], [1, 1, 1], (4, 4, 4), pts)
+    assert g.fallback_counts()["overflow"] > 0
+    assert_same(g, o, check_counters=False)

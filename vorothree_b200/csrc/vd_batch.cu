@@ -179,7 +179,9 @@ __global__ void k_brelax(const double* __restrict__ gen, const int32_t* __restri
   }
 }
 
-enum : int { kBCursor = 0, kBOvf, kBTab, kBBig, kBCursor2, kBWords = 8 };
+// control words: work cursors of the three passes, the overflow counts they
+// hand on, the search-order list count, and the big-bin sort count
+enum : int { kBCursor = 0, kBOvf, kBTab, kBBig, kBCursor2, kBMedOvf, kBCursor3, kBBigOvf, kBWords = 8 };
 
 }  // namespace vd_batch_impl
 
@@ -199,11 +201,11 @@ struct vd_batch {
   uint32_t nmax = 0;        // generators at commit (upper bound of every later count)
   uint32_t nbins = 0;       // bins of all members
   std::vector<uint32_t> h_in_off, h_bin_off, h_off;
-  ClipLaunchInfo info64{}, infomx{};
+  ClipLaunchInfo info64{}, infomx{}, infomed{};
 
   Buf<double> d_in, d_gen, d_vol, d_cen, d_farea, d_pool_area;
   Buf<uint32_t> d_flags, d_pos, d_off, d_off_next, d_in_off, d_total, d_bin_off, d_bin_of, d_counts, d_start,
-      d_cursor, d_ids, d_ids_tmp, d_big_list, d_list0, d_list1, d_list2;
+      d_cursor, d_ids, d_ids_tmp, d_big_list, d_list0, d_list1, d_list2, d_list3;
   Buf<SortedGen> d_sorted;
   Buf<Offset> d_order;
   Buf<TessDesc> d_descs;
@@ -371,17 +373,20 @@ int filter_and_bin(vd_batch* b, const double* d_src, const uint32_t* src_off) {
   return VD_OK;
 }
 
-// fast pass over every cell, then the large-capacity pass over its overflow
-// list (both sized on the device)
-int clip_all(vd_batch* b) {
+// The clip chain over a work list: the fast pass, then the medium-capacity
+// pass over its overflow list, then the large-capacity pass over what still
+// overflows -- every count lives on the device, so the chain can be captured.
+// items == nullptr: every cell (the count is the batch total).
+int clip_chain(vd_batch* b, const uint32_t* items, uint32_t nitems) {
   cudaStream_t s = b->stream;
   const int nt = (int)b->m.size();
   B_CK(b, cudaMemsetAsync(b->d_ctl.p, 0, 3 * sizeof(unsigned int), s));
-  B_CK(b, cudaMemsetAsync(b->d_ctl.p + kBCursor2, 0, sizeof(unsigned int), s));
-  B_CK(b, cudaMemsetAsync(b->d_pool_cursor.p, 0, sizeof(unsigned long long), s));
+  B_CK(b, cudaMemsetAsync(b->d_ctl.p + kBCursor2, 0, 4 * sizeof(unsigned int), s));
   WorkList W;
   memset(&W, 0, sizeof(W));
-  W.nitems_dev = b->d_total.p;
+  W.items = items;
+  W.nitems = nitems;
+  W.nitems_dev = items ? nullptr : b->d_total.p;
   W.cursor = b->d_ctl.p + kBCursor;
   W.ovf_list = b->d_list0.p;
   W.ovf_count = b->d_ctl.p + kBOvf;
@@ -394,16 +399,31 @@ int clip_all(vd_batch* b) {
   const int nblocks = std::max(1, b->num_sms * std::max(1, li.blocks_per_sm));
   B_CK(b, mixed ? launch_clip_mixed_fast_batched(b->d_descs.p, b->d_off.p, nt, W, nblocks, b->instrument, s)
                 : launch_clip_fp64_fast_batched(b->d_descs.p, b->d_off.p, nt, W, nblocks, b->instrument, s));
-  // overflowed cells: the FP64 large-capacity pass (same decisions, larger storage)
+  // medium capacity (FP64; the same decisions as both precisions)
   WorkList W2 = W;
   W2.items = b->d_list0.p;
+  W2.nitems = 0;
   W2.nitems_dev = b->d_ctl.p + kBOvf;
   W2.cursor = b->d_ctl.p + kBCursor2;
-  W2.ovf_list = b->d_list2.p;  // a second overflow cannot be served; counted below
-  W2.ovf_count = b->d_ctl.p + kBCursor2 + 1;
-  B_CK(b, cudaMemsetAsync(b->d_ctl.p + kBCursor2 + 1, 0, sizeof(unsigned int), s));
-  B_CK(b, launch_clip_fp64_big_batched(b->d_descs.p, b->d_off.p, nt, W2, b->d_big.p, b->big_warps, s));
+  W2.ovf_list = b->d_list2.p;
+  W2.ovf_count = b->d_ctl.p + kBMedOvf;
+  B_CK(b, launch_clip_med_batched(b->d_descs.p, b->d_off.p, nt, W2,
+                                  std::max(1, b->num_sms * std::max(1, b->infomed.blocks_per_sm)), s));
+  // large capacity (global-memory storage); what overflows here is an error
+  WorkList W3 = W;
+  W3.items = b->d_list2.p;
+  W3.nitems = 0;
+  W3.nitems_dev = b->d_ctl.p + kBMedOvf;
+  W3.cursor = b->d_ctl.p + kBCursor3;
+  W3.ovf_list = b->d_list0.p;
+  W3.ovf_count = b->d_ctl.p + kBBigOvf;
+  B_CK(b, launch_clip_fp64_big_batched(b->d_descs.p, b->d_off.p, nt, W3, b->d_big.p, b->big_warps, s));
   return VD_OK;
+}
+
+int clip_all(vd_batch* b) {
+  B_CK(b, cudaMemsetAsync(b->d_pool_cursor.p, 0, sizeof(unsigned long long), b->stream));
+  return clip_chain(b, nullptr, 0);
 }
 
 // cells that ran off a truncated search order: lengthen that member's table
@@ -415,8 +435,7 @@ int resolve_tables(vd_batch* b) {
     unsigned int h[kBWords];
     B_CK(b, cudaMemcpyAsync(h, b->d_ctl.p, sizeof(h), cudaMemcpyDeviceToHost, s));
     B_CK(b, cudaStreamSynchronize(s));
-    if (h[kBCursor2 + 1] > 0)
-      return bfail(b, VD_EOVERFLOW, "%u cells exceed the large polytope capacity", h[kBCursor2 + 1]);
+    if (h[kBBigOvf] > 0) return bfail(b, VD_EOVERFLOW, "%u cells exceed the large polytope capacity", h[kBBigOvf]);
     const unsigned ntab = h[kBTab];
     if (ntab == 0) return VD_OK;
     std::vector<unsigned int> flags(nt);
@@ -435,31 +454,12 @@ int resolve_tables(vd_batch* b) {
     // upload_static rewrote whole descriptors: restore the per-step parts
     k_bdesc_update<<<blocks_for(b, nt, 128), 128, 0, s>>>(b->d_descs.p, nt, b->d_off.p, b->d_bin_off.p, bases(b));
     B_CK(b, cudaGetLastError());
-    B_CK(b, cudaMemcpyAsync(b->d_list2.p, b->d_list1.p, ntab * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
-    B_CK(b, cudaMemsetAsync(b->d_ctl.p, 0, kBWords * sizeof(unsigned int), s));
-    WorkList W;
-    memset(&W, 0, sizeof(W));
-    W.items = b->d_list2.p;
-    W.nitems = ntab;
-    W.cursor = b->d_ctl.p + kBCursor;
-    W.ovf_list = b->d_list0.p;
-    W.ovf_count = b->d_ctl.p + kBOvf;
-    W.tab_list = b->d_list1.p;
-    W.tab_count = b->d_ctl.p + kBTab;
-    W.counters = b->d_counters.p;
-    W.tess_flags = b->d_tess_flags.p;
-    B_CK(b, launch_clip_fp64_fast_batched(b->d_descs.p, b->d_off.p, nt, W,
-                                          std::max(1, b->num_sms * std::max(1, b->info64.blocks_per_sm)),
-                                          b->instrument, s));
+    // rerun the listed cells (from a copy: the chain refills the lists)
+    B_CK(b, b->d_list3.ensure(b->nmax));
+    B_CK(b, cudaMemcpyAsync(b->d_list3.p, b->d_list1.p, ntab * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+    r = clip_chain(b, b->d_list3.p, ntab);
+    if (r != VD_OK) return r;
     b->table_reruns += ntab;
-    WorkList W2 = W;
-    W2.items = b->d_list0.p;
-    W2.nitems = 0;
-    W2.nitems_dev = b->d_ctl.p + kBOvf;
-    W2.cursor = b->d_ctl.p + kBCursor2;
-    W2.ovf_list = b->d_list2.p;
-    W2.ovf_count = b->d_ctl.p + kBCursor2 + 1;
-    B_CK(b, launch_clip_fp64_big_batched(b->d_descs.p, b->d_off.p, nt, W2, b->d_big.p, b->big_warps, s));
   }
   return bfail(b, VD_ECUDA, "search-order extension did not converge");
 }
@@ -504,6 +504,7 @@ int vd_batch_create(vd_batch** out) {
   e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = clip_fp64_info(&b->info64);
   if (e == cudaSuccess) e = clip_mixed_info(&b->infomx);
+  if (e == cudaSuccess) e = clip_med_setup(&b->infomed);
   if (e == cudaSuccess) e = clip_fp64_batched_setup();
   if (e == cudaSuccess) e = clip_mixed_batched_setup();
   if (e == cudaSuccess) e = cudaEventCreate(&b->ev0);
@@ -527,7 +528,7 @@ int vd_batch_destroy(vd_batch* b) {
   b->d_pool_area.release(); b->d_flags.release(); b->d_pos.release(); b->d_off.release(); b->d_off_next.release();
   b->d_in_off.release(); b->d_total.release(); b->d_bin_off.release(); b->d_bin_of.release(); b->d_counts.release();
   b->d_start.release(); b->d_cursor.release(); b->d_ids.release(); b->d_ids_tmp.release(); b->d_big_list.release();
-  b->d_list0.release(); b->d_list1.release(); b->d_list2.release(); b->d_sorted.release(); b->d_order.release();
+  b->d_list0.release(); b->d_list1.release(); b->d_list2.release(); b->d_list3.release(); b->d_sorted.release(); b->d_order.release();
   b->d_descs.release(); b->d_nf.release(); b->d_nv.release(); b->d_fnb.release(); b->d_pool_fnb.release();
   b->d_status.release(); b->d_pool_off.release(); b->d_ctl.release(); b->d_tess_flags.release();
   b->d_counters.release(); b->d_pool_cursor.release(); b->d_big.release();

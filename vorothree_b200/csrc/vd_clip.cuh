@@ -61,6 +61,10 @@ using FastCfgCount = PolyCfg<96, 48, 288, 64, 32, 32, uint8_t, uint8_t, uint16_t
 // mixed precision: same capacities, FP32 generator-relative copies of the vertices
 using MixedCfg = PolyCfg<96, 48, 288, 64, 32, 32, uint8_t, uint8_t, uint16_t, uint8_t, false, true>;
 using MixedCfgCount = PolyCfg<96, 48, 288, 64, 32, 32, uint8_t, uint8_t, uint16_t, uint8_t, true, true>;
+// Medium tier (shared memory, 2 warps per block): cells whose polytope
+// outgrew the fast capacities -- typical of dense clustered inputs, where
+// the reference's bin-order walk clips a cell with thousands of candidates.
+using MedCfg = PolyCfg<224, 112, 672, 128, 64, 64, uint8_t, uint8_t, uint16_t, uint8_t, true, false>;
 // Large-capacity pass (global-memory storage): vertex ids stay u16 like the
 // reference's face_indices (cell_3d_faces.rs:31).
 using BigCfg = PolyCfg<2048, 512, 6144, 1024, 512, 512, uint16_t, uint16_t, uint32_t, uint16_t, true, false>;

@@ -128,7 +128,7 @@ struct vd_tess {
   float timings[4] = {0, 0, 0, 0};
   unsigned long long counters[kNumCounters] = {};
   unsigned long long fallback[2] = {0, 0};
-  ClipLaunchInfo info64{}, infomx{};
+  ClipLaunchInfo info64{}, infomx{}, infomed{};
   int num_sms = 0;
 };
 
@@ -354,8 +354,9 @@ int ensure_big(vd_tess* t, size_t cells) {
   return VD_OK;
 }
 
-// one pass of the clip kernel over `items` (nullptr = all cells in bin order)
-int clip_pass(vd_tess* t, bool big, const uint32_t* items, uint32_t nitems, uint32_t* ovf_list,
+// one pass of the clip kernel over `items` (nullptr = all cells in bin order);
+// tier 0 = fast (shared memory), 1 = medium capacity, 2 = large capacity
+int clip_pass(vd_tess* t, int tier, const uint32_t* items, uint32_t nitems, uint32_t* ovf_list,
               uint32_t* tab_list, const WorkList* extra = nullptr) {
   cudaStream_t s = t->stream;
   VD_CK(t, cudaMemsetAsync(t->d_ctl.p, 0, 3 * sizeof(unsigned int), s));
@@ -371,7 +372,12 @@ int clip_pass(vd_tess* t, bool big, const uint32_t* items, uint32_t nitems, uint
   W.tab_count = t->d_ctl.p + kCtlTabCount;
   W.counters = t->d_counters.p;
   TessDesc T = make_desc(t);
-  if (!big) {
+  if (tier == 1) {
+    const int nblocks = (int)std::max<size_t>(
+        1, std::min<size_t>((nitems + 1) / 2, (size_t)t->num_sms * std::max(1, t->infomed.blocks_per_sm)));
+    VD_CK(t, launch_clip_med(T, W, nblocks, s));
+    g_launches++;
+  } else if (tier == 0) {
     const bool mixed = t->precision == VD_PREC_MIXED;
     const ClipLaunchInfo& li = mixed ? t->infomx : t->info64;
     const size_t warps_needed = (nitems + li.warps_per_block - 1) / li.warps_per_block;
@@ -418,7 +424,7 @@ int run_calculate(vd_tess* t, const WorkList* extra = nullptr, const uint32_t* o
     in_list = t->d_list[2].p;
   }
   if (nin > 0) {
-    r = clip_pass(t, false, in_list, nin, t->d_list[0].p, t->d_list[1].p, extra);
+    r = clip_pass(t, 0, in_list, nin, t->d_list[0].p, t->d_list[1].p, extra);
     if (r != VD_OK) return r;
   }
   VD_CK(t, cudaEventRecord(t->ev[3], s));
@@ -438,7 +444,7 @@ int run_calculate(vd_tess* t, const WorkList* extra = nullptr, const uint32_t* o
       if (r != VD_OK) return r;
       // rerun table cells; overflows go to a fresh list, appended after novf
       std::swap(t->d_list[1], t->d_list[2]);
-      r = clip_pass(t, false, t->d_list[2].p, ntab, t->d_list[0].p + novf, t->d_list[1].p, extra);
+      r = clip_pass(t, 0, t->d_list[2].p, ntab, t->d_list[0].p + novf, t->d_list[1].p, extra);
       if (r != VD_OK) return r;
       unsigned int o2, t2;
       r = read_ctl(t, &o2, &t2);
@@ -450,16 +456,22 @@ int run_calculate(vd_tess* t, const WorkList* extra = nullptr, const uint32_t* o
       continue;
     }
     if (novf > 0) {
-      std::swap(t->d_list[0], t->d_list[2]);
-      r = clip_pass(t, true, t->d_list[2].p, novf, t->d_list[0].p, t->d_list[1].p, extra);
-      if (r != VD_OK) return r;
-      unsigned int o2, t2;
-      r = read_ctl(t, &o2, &t2);
-      if (r != VD_OK) return r;
-      if (o2 > 0) return fail(t, VD_EOVERFLOW, "%u cells exceed the large polytope capacity", o2);
+      // medium capacity first, then the large-capacity pass for what remains
+      unsigned int ntab_all = 0;
+      for (int tier = 1; tier <= 2 && novf > 0; ++tier) {
+        std::swap(t->d_list[0], t->d_list[2]);
+        r = clip_pass(t, tier, t->d_list[2].p, novf, t->d_list[0].p, t->d_list[1].p + ntab_all, extra);
+        if (r != VD_OK) return r;
+        unsigned int o2, t2;
+        r = read_ctl(t, &o2, &t2);
+        if (r != VD_OK) return r;
+        ntab_all += t2;
+        if (tier == 2 && o2 > 0) return fail(t, VD_EOVERFLOW, "%u cells exceed the large polytope capacity", o2);
+        novf = o2;
+      }
       novf = 0;
-      ntab = t2;
-      t->fallback[1] += t2;
+      ntab = ntab_all;
+      t->fallback[1] += ntab_all;
     }
   }
   VD_CK(t, cudaEventRecord(t->ev[4], s));
@@ -529,6 +541,7 @@ int vd_tess_create(const double bmin[3], const double bmax[3], int nx, int ny, i
   for (auto& ev : t->ev) cudaEventCreate(&ev);
   e = clip_fp64_info(&t->info64);
   if (e == cudaSuccess) e = clip_mixed_info(&t->infomx);
+  if (e == cudaSuccess) e = clip_med_setup(&t->infomed);
   if (e != cudaSuccess) {
     const std::string m = cudaGetErrorString(e);
     vd_tess_destroy(t);

@@ -25,6 +25,12 @@ cudaError_t launch_clip_fp64_fast(const TessDesc& T, const WorkList& W, int nblo
 cudaError_t launch_clip_fp64_big(const TessDesc& T, const WorkList& W, void* scratch, int nwarps,
                                  cudaStream_t s);
 
+// medium-capacity tier (FP64, shared memory) for cells that overflow the fast path
+cudaError_t clip_med_setup(ClipLaunchInfo* info);
+cudaError_t launch_clip_med(const TessDesc& T, const WorkList& W, int nblocks, cudaStream_t s);
+cudaError_t launch_clip_med_batched(const TessDesc* descs, const uint32_t* tess_off, int ntess,
+                                    const WorkList& W, int nblocks, cudaStream_t s);
+
 // batched mode (descriptors in device memory; see clip_worker_batched)
 cudaError_t clip_fp64_batched_setup();
 cudaError_t clip_mixed_batched_setup();

@@ -77,4 +77,37 @@ cudaError_t clip_fp64_batched_setup() {
                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
+constexpr int kMedWarpsPerBlock = 2;
+
+cudaError_t clip_med_setup(ClipLaunchInfo* info) {
+  const size_t smem = sizeof(WarpPoly<MedCfg>) * kMedWarpsPerBlock;
+  info->smem_per_warp = sizeof(WarpPoly<MedCfg>);
+  info->warps_per_block = kMedWarpsPerBlock;
+  cudaError_t e = cudaFuncSetAttribute(k_clip_fast<MedCfg, kMedWarpsPerBlock, 1>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(k_clip_fast_batched<MedCfg, kMedWarpsPerBlock, 1>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int nb = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_clip_fast<MedCfg, kMedWarpsPerBlock, 1>,
+                                                    kMedWarpsPerBlock * 32, smem);
+  info->blocks_per_sm = nb;
+  return e;
+}
+
+cudaError_t launch_clip_med(const TessDesc& T, const WorkList& W, int nblocks, cudaStream_t s) {
+  const size_t smem = sizeof(WarpPoly<MedCfg>) * kMedWarpsPerBlock;
+  k_clip_fast<MedCfg, kMedWarpsPerBlock, 1><<<nblocks, kMedWarpsPerBlock * 32, smem, s>>>(T, W);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_clip_med_batched(const TessDesc* descs, const uint32_t* tess_off, int ntess,
+                                    const WorkList& W, int nblocks, cudaStream_t s) {
+  const size_t smem = sizeof(WarpPoly<MedCfg>) * kMedWarpsPerBlock;
+  k_clip_fast_batched<MedCfg, kMedWarpsPerBlock, 1>
+      <<<nblocks, kMedWarpsPerBlock * 32, smem, s>>>(descs, tess_off, ntess, W);
+  return cudaGetLastError();
+}
+
 }  // namespace vd
