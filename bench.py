@@ -257,38 +257,52 @@ def run_ours(args):
     step()
     counters = tess.counters()
     tess.set_instrumentation(False)
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
-    launches0 = C.c_uint64()
-    L.vd_launch_count(C.byref(launches0))
 
     def barrier():
         if ws > 1:
             torch.distributed.barrier()
         torch.cuda.synchronize()
 
+    def timed(precision):
+        """K device-timed steps (L2 flushed before each), after W warm-up steps."""
+        tess.set_precision(precision)
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        sm, cm, bm = [], [], []
+        c0 = C.c_uint64()
+        L.vd_launch_count(C.byref(c0))
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            step()
+            e1.record(stream)
+            e1.synchronize()
+            sm.append(e0.elapsed_time(e1))
+            tm = tess.timings()
+            cm.append(tm["clip_ms"])
+            bm.append(tm["bin_ms"])
+        c1 = C.c_uint64()
+        L.vd_launch_count(C.byref(c1))
+        launches.append(int(c1.value - c0.value))
+        return sm, cm, bm
+
+    launches = []
     clocks = ClockSampler(local)
     barrier()
     clocks.start()
-    step_ms, clip_ms, bin_ms = [], [], []
-    for _ in range(args.steps):
-        flush.zero_()
-        torch.cuda.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        step()
-        e1.record(stream)
-        e1.synchronize()
-        step_ms.append(e0.elapsed_time(e1))
-        tm = tess.timings()
-        clip_ms.append(tm["clip_ms"])
-        bin_ms.append(tm["bin_ms"])
+    step_ms, clip_ms, bin_ms = timed(args.precision)
+    other = None
+    if not args.no_mixed:
+        alt = "mixed" if args.precision == "fp64" else "fp64"
+        osm, ocm, _ = timed(alt)
+        other = (alt, osm, ocm)
+        tess.set_precision(args.precision)
     barrier()
     clk = clocks.stop()
-    launches1 = C.c_uint64()
-    L.vd_launch_count(C.byref(launches1))
     ms = statistics.mean(step_ms)
     if ws > 1:
         tt = torch.tensor([ms], device=f"cuda:{local}", dtype=torch.float64)
@@ -329,10 +343,27 @@ def run_ours(args):
             "e2e": None if e2e is None else {
                 "value": N_GEN / (e2e / 1e3) * ws, "unit": "cells/s", "ms_per_step": e2e,
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-            "gpu_launches": int(launches1.value - launches0.value),
+            "gpu_launches": launches[0],
+            "gpu_launches_note": "kernels this library launched during the K timed steps (binning + clip)",
             "clocks": clk,
             "fallback_cells": fb,
         }
+        if other is not None:
+            alt, osm, ocm = other
+            oms = statistics.mean(osm)
+            line[alt] = {"value": ws * N_GEN / (oms / 1e3), "ms_per_step": oms,
+                         "clip_kernel_ms": statistics.mean(ocm),
+                         f"speedup_vs_{args.precision}": ms / oms,
+                         "note": "same outputs bit for bit (mixed decisions equal FP64's)"}
+        if ws == 1 and not args.no_serving:
+            reqs = serving_requests(24)
+            srv = v.TessellationServer(slots=4, hbm_budget_bytes=32 << 30, precision=args.precision)
+            for r in reqs[:2]:
+                srv.take(srv.submit(*r))
+            res = serve_at_rate(srv, reqs, 30.0)
+            srv.close()
+            line["serving"] = dict(res, note="Poisson arrivals; sizes log-uniform [1e3,1e6], half clustered, "
+                                             "0-2 walls; 4 slots; p50/p99 = submit-to-result latency")
         if ws == 1 and not args.no_cpu_baseline:
             nthreads = os.cpu_count() or 1
             cv, cdt = cpu_baseline(pts, nthreads, args.cpu_sample)
@@ -410,6 +441,94 @@ def run_batched(args):
     return 0
 
 
+def serving_requests(count: int, seed: int = 0):
+    """Requests of the serving workload: sizes log-uniform in [1e3, 1e6];
+    half uniform, half clustered (8 Gaussian blobs, sigma 0.03, 70% of the
+    points); 0-2 walls drawn from {plane through the centre with a random
+    normal, centred sphere of radius U[0.3, 0.5]}; grid ~ N^(1/3) per axis
+    (2.5x finer for clustered requests)."""
+    import vorothree_b200 as v
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    for k in range(count):
+        n = int(round(np.exp(rng.uniform(np.log(1e3), np.log(1e6)))))
+        clustered = rng.uniform() < 0.5
+        if clustered:
+            nb = int(0.7 * n)
+            c = rng.uniform(0.1, 0.9, size=(8, 3))
+            pts = np.concatenate([c[np.arange(nb) % 8] + rng.normal(0.0, 0.03, size=(nb, 3)),
+                                  rng.uniform(0.0, 1.0, size=(n - nb, 3))])
+            g = int(np.ceil(2.5 * n ** (1 / 3)))
+        else:
+            pts = rng.uniform(0.0, 1.0, size=(n, 3))
+            g = int(np.ceil(n ** (1 / 3)))
+        walls = []
+        for w in range(int(rng.integers(0, 3))):
+            if rng.uniform() < 0.5:
+                walls.append(v.Wall(v.WALL_ID_MAX - w, v.PlaneGeometry([0.5, 0.5, 0.5], list(rng.normal(size=3)))))
+            else:
+                walls.append(v.Wall(v.WALL_ID_MAX - w, v.SphereGeometry([0.5, 0.5, 0.5], float(rng.uniform(0.3, 0.5)))))
+        out.append((v.BoundingBox([0, 0, 0], [1, 1, 1]), (g, g, g), pts, walls))
+    return out
+
+
+def serve_at_rate(srv, reqs, rate: float, seed: int = 1):
+    """Submit reqs at Poisson arrival times of the given rate (req/s) from one
+    thread, collect them from another; returns p50/p99 latency and cells/s."""
+    import threading
+    rng = np.random.Generator(np.random.PCG64(seed))
+    gaps = rng.exponential(1.0 / rate, size=len(reqs))
+    tickets = [None] * len(reqs)
+    ready = [threading.Event() for _ in reqs]
+    srv.reset_stats()
+    t0 = time.perf_counter()
+
+    def submitter():
+        due = t0
+        for k, r in enumerate(reqs):
+            due += gaps[k]
+            delay = due - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            tickets[k] = srv.submit(*r)
+            ready[k].set()
+    th = threading.Thread(target=submitter)
+    th.start()
+    cells = 0
+    for k in range(len(reqs)):
+        ready[k].wait()
+        n, _ = srv.wait(tickets[k])
+        srv.take(tickets[k])
+        cells += n
+    th.join()
+    wall = time.perf_counter() - t0
+    st = srv.stats()
+    return {"rate_req_s": rate, "requests": len(reqs), "p50_ms": 1e3 * st["p50_s"], "p99_ms": 1e3 * st["p99_s"],
+            "cells": cells, "cells_per_s": cells / wall, "wall_s": wall, "peak_admitted_bytes": st["peak_bytes"]}
+
+
+def run_serving(args):
+    import torch
+    import vorothree_b200 as v
+    torch.cuda.set_device(0)
+    reqs = serving_requests(args.serve_requests)
+    srv = v.TessellationServer(slots=args.serve_slots, hbm_budget_bytes=args.serve_budget_gb << 30,
+                               precision=args.precision)
+    for r in reqs[:4]:  # warm the slots' buffers
+        srv.take(srv.submit(*r))
+    sweep = [serve_at_rate(srv, reqs, rate) for rate in args.serve_rates]
+    srv.close()
+    line = {"metric": "serve p50/p99 latency", "workload": "serving", "unit": "ms", "n_gpus": 1,
+            "higher_is_better": False, "value": sweep[0]["p99_ms"], "precision": args.precision,
+            "data": "synthetic (seeded PCG64)",
+            "config": {"slots": args.serve_slots, "hbm_budget_gb": args.serve_budget_gb,
+                       "sizes": "log-uniform [1e3, 1e6]", "mix": "half uniform, half 8-blob clustered",
+                       "walls": "0-2 of plane / centred sphere", "arrivals": "Poisson"},
+            "sweep": sweep}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_blobs(args):
     """Config: 4,194,304 generators, 70% in 64 isotropic Gaussian blobs
     (sigma 0.01, centres uniform) + 30% uniform background, clipped by a
@@ -450,10 +569,16 @@ def run_blobs(args):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--workload", choices=["uniform", "batched", "blobs"], default="uniform",
+    ap.add_argument("--workload", choices=["uniform", "batched", "blobs", "serving"], default="uniform",
                     help="uniform: 1M uniform generators (the headline); batched: many tessellations "
                          "+ Lloyd steps; blobs: 4M clustered generators with a sphere wall")
     ap.add_argument("--ntess", type=int, default=4096)
+    ap.add_argument("--serve-requests", type=int, default=48)
+    ap.add_argument("--serve-slots", type=int, default=4)
+    ap.add_argument("--serve-budget-gb", type=int, default=32)
+    ap.add_argument("--serve-rates", type=float, nargs="+", default=[10.0, 30.0, 60.0])
+    ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--lloyd-steps", type=int, default=20)
     ap.add_argument("--blob-grids", type=int, nargs="+", default=[160, 256, 320, 400])
     ap.add_argument("--gpus", type=int, default=1)
@@ -477,6 +602,8 @@ def main():
         return run_batched(args)
     if args.workload == "blobs":
         return run_blobs(args)
+    if args.workload == "serving":
+        return run_serving(args)
     return run_ours(args)
 
 

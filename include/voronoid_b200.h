@@ -51,6 +51,9 @@ int vd_tess_create(const double bmin[3], const double bmax[3], int nx, int ny, i
                    vd_tess** out);
 /* drop of Tessellation */
 int vd_tess_destroy(vd_tess* t);
+/* a fresh Tessellation::new on an existing handle (new bounds and grid, no
+ * walls, no generators) that keeps the handle's device buffers */
+int vd_tess_reset(vd_tess* t, const double bmin[3], const double bmax[3], int nx, int ny, int nz);
 /* message of the last failed call on t (or of the last failed create when t is NULL) */
 const char* vd_last_error(const vd_tess* t);
 
@@ -175,6 +178,30 @@ int vd_batch_get_summaries(vd_batch* b, int index, double* volume, double* centr
 int vd_batch_timing(const vd_batch* b, float* ms);
 int vd_batch_counters(const vd_batch* b, uint64_t* out8);
 int vd_batch_stream(vd_batch* b, void** stream);
+
+/* ---- serving: a request loop with continuous batching (no counterpart in
+ * the reference) ----
+ * `slots` worker threads each keep one resident tessellation handle with its
+ * own CUDA stream.  Requests (one Tessellation job each) are admitted FIFO
+ * as soon as a slot is free and their estimated device footprint fits in
+ * hbm_budget_bytes beside the running ones; running requests overlap on the
+ * device.  A request's result equals a standalone vd_tess's for the same
+ * inputs. */
+typedef struct vd_server vd_server;
+int vd_server_create(int slots, size_t hbm_budget_bytes, int precision, vd_server** out);
+int vd_server_destroy(vd_server* s);
+const char* vd_server_last_error(const vd_server* s);
+/* copies the inputs; *ticket identifies the request */
+int vd_server_submit(vd_server* s, const double bmin[3], const double bmax[3], int nx, int ny, int nz,
+                     const vd_wall_desc* walls, int nwalls, const double* xyz, size_t n, uint64_t* ticket);
+/* blocks until the request is done: its cell count and submit-to-done latency */
+int vd_server_wait(vd_server* s, uint64_t ticket, size_t* n_cells, double* latency_s);
+/* copies the per-cell results (any pointer may be NULL) and releases the request */
+int vd_server_take(vd_server* s, uint64_t ticket, double* volume, double* centroid3, int32_t* n_faces);
+/* completed requests, their cells, latency p50/p99 (s), peak admitted bytes */
+int vd_server_stats(vd_server* s, uint64_t* completed, uint64_t* cells, double* p50_s, double* p99_s,
+                    size_t* peak_bytes);
+int vd_server_reset_stats(vd_server* s);
 
 /* ---- allocation-free variant (no counterpart in the reference) ----
  * set_generators + calculate for a small tessellation without any device

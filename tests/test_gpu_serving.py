@@ -1,0 +1,89 @@
+"""GPU: the serving loop.  Requests of different sizes, distributions and
+walls are submitted together (they overlap on the device); each result must
+equal, bit for bit, the same request computed alone by a standalone
+Tessellation."""
+import threading
+
+import numpy as np
+import pytest
+
+from common import blobs, uniform
+
+pytestmark = pytest.mark.gpu
+
+WALL = -1000
+
+
+def requests(seed):
+    import vorothree_b200 as v
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    for k in range(12):
+        n = int(round(np.exp(rng.uniform(np.log(500), np.log(60000)))))
+        pts = blobs(n, 6, 0.02, 0.7, seed * 100 + k) if k % 3 == 0 else uniform(n, 0, 1, seed * 100 + k)
+        walls = []
+        if k % 4 == 1:
+            walls.append(v.Wall(WALL, v.SphereGeometry([0.5, 0.5, 0.5], rng.uniform(0.3, 0.5))))
+        if k % 4 == 2:
+            nrm = rng.normal(size=3)
+            walls.append(v.Wall(WALL - 1, v.PlaneGeometry([0.5, 0.5, 0.5], list(nrm))))
+        g = max(1, int(np.ceil(n ** (1 / 3))))
+        out.append((v.BoundingBox([0, 0, 0], [1, 1, 1]), (g, g, g), pts, walls))
+    return out
+
+
+def alone(req):
+    import vorothree_b200 as v
+    b, grid, pts, walls = req
+    t = v.Tessellation(b, v.Algorithm3DGrid(*grid))
+    for w in walls:
+        t.add_wall(w)
+    t.set_generators(pts)
+    t.calculate()
+    return t.summaries()
+
+
+def test_served_results_equal_alone():
+    import vorothree_b200 as v
+    reqs = requests(3)
+    srv = v.TessellationServer(slots=4, hbm_budget_bytes=8 << 30)
+    tickets = [srv.submit(*r) for r in reqs]
+    got = [srv.take(t) for t in tickets]
+    st = srv.stats()
+    assert st["completed"] == len(reqs) and st["p99_s"] >= st["p50_s"] > 0
+    for r, (vol, cen, nf) in zip(reqs, got):
+        av, ac, an = alone(r)
+        assert np.array_equal(nf, an) and np.array_equal(vol, av) and np.array_equal(cen, ac)
+    srv.close()
+
+
+def test_admission_respects_budget_and_threads():
+    import vorothree_b200 as v
+    reqs = requests(4)
+    # a budget that admits about one large request at a time still serves all
+    srv = v.TessellationServer(slots=3, hbm_budget_bytes=64 << 20)
+    results = {}
+
+    def client(idx):
+        t = srv.submit(*reqs[idx])
+        results[idx] = srv.take(t)
+    th = [threading.Thread(target=client, args=(i,)) for i in range(len(reqs))]
+    for x in th:
+        x.start()
+    for x in th:
+        x.join()
+    st = srv.stats()
+    assert st["completed"] == len(reqs) and st["peak_bytes"] <= (64 << 20)
+    for i, r in enumerate(reqs):
+        av, ac, an = alone(r)
+        vol, cen, nf = results[i]
+        assert np.array_equal(vol, av)
+    srv.close()
+
+
+def test_request_over_budget_rejected():
+    import vorothree_b200 as v
+    srv = v.TessellationServer(slots=1, hbm_budget_bytes=1 << 20)
+    with pytest.raises(v.VoronoidError):
+        srv.submit(v.BoundingBox([0, 0, 0], [1, 1, 1]), (10, 10, 10), uniform(20000, 0, 1, 1))
+    srv.close()

@@ -8,8 +8,9 @@ reference's API over that ABI.
 """
 from ._lib import VoronoidError, load
 from .batch import TessellationBatch
+from .server import TessellationServer
 from .tessellation import (WALL_ID_MAX, Algorithm3DGrid, BoundingBox, Cell3DFaces, PlaneGeometry,
                            SphereGeometry, Tessellation, Wall, box_side)
 
 __all__ = ["Algorithm3DGrid", "BoundingBox", "Cell3DFaces", "PlaneGeometry", "SphereGeometry",
-           "Tessellation", "TessellationBatch", "Wall", "WALL_ID_MAX", "box_side", "VoronoidError", "load"]
+           "Tessellation", "TessellationBatch", "TessellationServer", "Wall", "WALL_ID_MAX", "box_side", "VoronoidError", "load"]

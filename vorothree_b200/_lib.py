@@ -36,6 +36,7 @@ _szp = C.POINTER(C.c_size_t)
 SIGNATURES = {
     "vd_tess_create": (C.c_int, [_d, _d, C.c_int, C.c_int, C.c_int, C.POINTER(_vp)]),
     "vd_tess_destroy": (C.c_int, [_vp]),
+    "vd_tess_reset": (C.c_int, [_vp, _d, _d, C.c_int, C.c_int, C.c_int]),
     "vd_last_error": (C.c_char_p, [_vp]),
     "vd_tess_add_wall_plane": (C.c_int, [_vp, _d, _d, C.c_int]),
     "vd_tess_add_wall_sphere": (C.c_int, [_vp, _d, C.c_double, C.c_int]),
@@ -82,6 +83,15 @@ SIGNATURES = {
     "vd_batch_timing": (C.c_int, [_vp, C.POINTER(C.c_float)]),
     "vd_batch_counters": (C.c_int, [_vp, _u64p]),
     "vd_batch_stream": (C.c_int, [_vp, C.POINTER(_vp)]),
+    "vd_server_create": (C.c_int, [C.c_int, C.c_size_t, C.c_int, C.POINTER(_vp)]),
+    "vd_server_destroy": (C.c_int, [_vp]),
+    "vd_server_last_error": (C.c_char_p, [_vp]),
+    "vd_server_submit": (C.c_int, [_vp, _d, _d, C.c_int, C.c_int, C.c_int, _vp, C.c_int, _d, C.c_size_t,
+                                   C.POINTER(C.c_uint64)]),
+    "vd_server_wait": (C.c_int, [_vp, C.c_uint64, _szp, _d]),
+    "vd_server_take": (C.c_int, [_vp, C.c_uint64, _vp, _vp, _vp]),
+    "vd_server_stats": (C.c_int, [_vp, _u64p, _u64p, _d, _d, _szp]),
+    "vd_server_reset_stats": (C.c_int, [_vp]),
     "vd_calculate_noalloc": (C.c_int, [_d, _d, C.c_int, C.c_int, C.c_int, _vp, C.c_size_t, _vp, _vp, _vp,
                                        _vp]),
 }

@@ -28,6 +28,7 @@ SOURCES = [
     ("vd_measure.cu", True),
     ("vd_noalloc.cu", False),
     ("vd_batch.cu", False),
+    ("vd_server.cu", False),
 ]
 
 

@@ -55,12 +55,14 @@ struct PolyCfg {
 // Fast path: sized from the oracle's distribution (max 72 vertices, 38 faces,
 // 216 face entries over 7.5M uniform-input polytopes); anything larger goes
 // to the large-capacity pass.
-using FastCfg = PolyCfg<96, 48, 288, 64, 32, 32, uint8_t, uint8_t, uint16_t, uint8_t, false, false>;
+// With at most 32 crossing positions per clip, each new vertex stays in the
+// register of the lane that discovered it until the vertex list is rebuilt.
+using FastCfg = PolyCfg<96, 48, 288, 32, 32, 32, uint8_t, uint8_t, uint16_t, uint8_t, false, false>;
 // the same with the event counters (instrumented runs)
-using FastCfgCount = PolyCfg<96, 48, 288, 64, 32, 32, uint8_t, uint8_t, uint16_t, uint8_t, true, false>;
+using FastCfgCount = PolyCfg<96, 48, 288, 32, 32, 32, uint8_t, uint8_t, uint16_t, uint8_t, true, false>;
 // mixed precision: same capacities, FP32 generator-relative copies of the vertices
-using MixedCfg = PolyCfg<96, 48, 288, 64, 32, 32, uint8_t, uint8_t, uint16_t, uint8_t, false, true>;
-using MixedCfgCount = PolyCfg<96, 48, 288, 64, 32, 32, uint8_t, uint8_t, uint16_t, uint8_t, true, true>;
+using MixedCfg = PolyCfg<96, 48, 288, 32, 32, 32, uint8_t, uint8_t, uint16_t, uint8_t, false, true>;
+using MixedCfgCount = PolyCfg<96, 48, 288, 32, 32, 32, uint8_t, uint8_t, uint16_t, uint8_t, true, true>;
 // Medium tier (shared memory, 2 warps per block): cells whose polytope
 // outgrew the fast capacities -- typical of dense clustered inputs, where
 // the reference's bin-order walk clips a cell with thousands of candidates.
@@ -76,8 +78,10 @@ struct alignas(16) WarpPoly {
   double dist[C::MIXED ? 1 : C::VCAP];
   // mixed path: FP32 copies of the vertices relative to the generator
   float ux[C::MIXED ? C::VCAP : 1], uy[C::MIXED ? C::VCAP : 1], uz[C::MIXED ? C::VCAP : 1];
-  double tx[C::NCAP], ty[C::NCAP], tz[C::NCAP];
-  unsigned long long cnt[kNumCounters];
+  // new vertices awaiting the rebuilt list (only when a clip can have more
+  // than 32 crossings; otherwise they wait in registers)
+  double tx[C::CCAP > 32 ? C::NCAP : 1], ty[C::CCAP > 32 ? C::NCAP : 1], tz[C::CCAP > 32 ? C::NCAP : 1];
+  unsigned long long cnt[C::COUNT ? kNumCounters : 1];
   int32_t fn[2][C::FCAP];
   uint16_t E[C::HCAP + 1];
   uint16_t fs[2][C::FCAP + 1];
@@ -332,6 +336,9 @@ __device__ int warp_clip(WarpPoly<C>& P, PolyState& S, double px, double py, dou
   //    vertex (numbered in discovery order after the kept ones), repeats reuse
   //    it (the intersection_map lookups of :391-417 / :422-448)
   int nnew = 0;
+  constexpr bool kRegX = C::CCAP <= 32;  // a single chunk: keep new vertices in registers
+  double rx = 0.0, ry = 0.0, rz = 0.0;
+  int rslot = -1;
   for (int b = 0; b < ncross; b += 32) {
     const int k = b + lane;
     const bool act = k < ncross;
@@ -371,9 +378,16 @@ __device__ int warp_clip(WarpPoly<C>& P, PolyState& S, double px, double py, dou
         const double ix = ax + t * (bx - ax);
         const double iy = ay + t * (by - ay);
         const double iz = az + t * (bz - az);
-        P.tx[r] = ix;
-        P.ty[r] = iy;
-        P.tz[r] = iz;
+        if constexpr (kRegX) {
+          rx = ix;
+          ry = iy;
+          rz = iz;
+          rslot = r;
+        } else {
+          P.tx[r] = ix;
+          P.ty[r] = iy;
+          P.tz[r] = iz;
+        }
         if (with_gen) {
           double dx = ix - gx;
           double dy = iy - gy;
@@ -422,17 +436,22 @@ __device__ int warp_clip(WarpPoly<C>& P, PolyState& S, double px, double py, dou
     }
     __syncwarp();
   }
-  for (int r = lane; r < nnew; r += 32) {
-    P.vx[nkept + r] = P.tx[r];
-    P.vy[nkept + r] = P.ty[r];
-    P.vz[nkept + r] = P.tz[r];
+  auto place = [&](int r, double x, double y, double z) {
+    P.vx[nkept + r] = x;
+    P.vy[nkept + r] = y;
+    P.vz[nkept + r] = z;
     if constexpr (C::MIXED) {
-      const float fx = (float)(P.tx[r] - gx), fy = (float)(P.ty[r] - gy), fz = (float)(P.tz[r] - gz);
+      const float fx = (float)(x - gx), fy = (float)(y - gy), fz = (float)(z - gz);
       P.ux[nkept + r] = fx;
       P.uy[nkept + r] = fy;
       P.uz[nkept + r] = fz;
       um = fmax(um, fmax(fabs((double)fx), fmax(fabs((double)fy), fabs((double)fz))));
     }
+  };
+  if constexpr (kRegX) {
+    if (rslot >= 0) place(rslot, rx, ry, rz);
+  } else {
+    for (int r = lane; r < nnew; r += 32) place(r, P.tx[r], P.ty[r], P.tz[r]);
   }
   if constexpr (C::MIXED) S.umax = warp_max(um) * (1.0 + 0x1p-20);
 
@@ -877,7 +896,9 @@ __device__ void export_cell(const WorkList& W, const WarpPoly<C>& P, const PolyS
 template <class C>
 __device__ void clip_worker(const TessDesc& T, const WorkList& W, WarpPoly<C>& P) {
   const unsigned lane = lane_id();
-  if (lane < kNumCounters) P.cnt[lane] = 0;
+  if constexpr (C::COUNT) {
+    if (lane < kNumCounters) P.cnt[lane] = 0;
+  }
   __syncwarp();
   while (true) {
     unsigned idx = 0;
@@ -920,7 +941,9 @@ template <class C>
 __device__ void clip_worker_batched(const TessDesc* descs, const uint32_t* tess_off, int ntess,
                                     const WorkList& W, WarpPoly<C>& P) {
   const unsigned lane = lane_id();
-  if (lane < kNumCounters) P.cnt[lane] = 0;
+  if constexpr (C::COUNT) {
+    if (lane < kNumCounters) P.cnt[lane] = 0;
+  }
   const uint32_t nitems = W.nitems_dev ? *W.nitems_dev : W.nitems;
   __syncwarp();
   while (true) {

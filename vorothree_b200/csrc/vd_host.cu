@@ -30,6 +30,9 @@ using namespace vd;
 namespace {
 
 thread_local std::string g_create_error;
+// grids whose complete search order has at most this many entries get the
+// complete table; larger ones start truncated (k = 8) and grow on demand
+constexpr int kCompleteOrderMax = 1 << 15;
 // kernels this library has launched in this process (all handles)
 std::atomic<unsigned long long> g_launches{0};
 
@@ -560,7 +563,7 @@ int vd_tess_create(const double bmin[3], const double bmax[3], int nx, int ny, i
   }
   t->nbins = (size_t)nx * ny * nz;
   const double full = (2.0 * nx + 1) * (2.0 * ny + 1) * (2.0 * nz + 1);
-  int r = upload_order(t, full <= (double)(1 << 21) ? std::max(nx, std::max(ny, nz)) : 8);
+  int r = upload_order(t, full <= (double)kCompleteOrderMax ? std::max(nx, std::max(ny, nz)) : 8);
   if (r == VD_OK) r = rebin(t);
   if (r != VD_OK) {
     g_create_error = t->err;
@@ -569,6 +572,36 @@ int vd_tess_create(const double bmin[3], const double bmax[3], int nx, int ny, i
   }
   *out = t;
   return VD_OK;
+}
+
+// A new bounding box and grid on an existing handle: device buffers are kept
+// (they only grow), walls and generators are cleared.
+int vd_tess_reset(vd_tess* t, const double bmin[3], const double bmax[3], int nx, int ny, int nz) {
+  if (!t || !bmin || !bmax) return VD_EINVAL;
+  if (nx <= 0 || ny <= 0 || nz <= 0 || nx > 16000 || ny > 16000 || nz > 16000)
+    return fail(t, VD_EINVAL, "grid resolution must be in [1, 16000]");
+  if ((double)nx * ny * nz > 2.0e9) return fail(t, VD_EINVAL, "too many bins");
+  VD_CK(t, cudaSetDevice(t->device));
+  Grid& g = t->grid;
+  const int n[3] = {nx, ny, nz};
+  for (int a = 0; a < 3; ++a) {
+    g.bmin[a] = bmin[a];
+    g.bmax[a] = bmax[a];
+    g.n[a] = n[a];
+    g.scale[a] = (double)n[a] / (bmax[a] - bmin[a]);
+    g.limit[a] = (double)n[a] - 1e-5;
+    g.cs[a] = 1.0 / g.scale[a];
+  }
+  t->nbins = (size_t)nx * ny * nz;
+  t->walls.clear();
+  t->ngen = 0;
+  t->ncells = 0;
+  t->calculated = false;
+  t->csr_valid = false;
+  const double full = (2.0 * nx + 1) * (2.0 * ny + 1) * (2.0 * nz + 1);
+  int r = upload_order(t, full <= (double)kCompleteOrderMax ? std::max(nx, std::max(ny, nz)) : 8);
+  if (r != VD_OK) return r;
+  return rebin(t);
 }
 
 int vd_tess_destroy(vd_tess* t) {

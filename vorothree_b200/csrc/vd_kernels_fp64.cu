@@ -8,7 +8,6 @@
 
 namespace vd {
 
-static_assert(sizeof(WarpPoly<FastCfg>) == sizeof(WarpPoly<FastCfgCount>), "same layout");
 
 // shared memory admits 7 blocks of 4 warps per SM; keep registers in step
 // (without the bound ptxas takes ~100 registers and only 4 blocks fit)
@@ -19,11 +18,12 @@ cudaError_t clip_fp64_info(ClipLaunchInfo* info) {
   info->warps_per_block = kFastWarpsPerBlock;
   info->big_scratch_per_warp = sizeof(WarpPoly<BigCfg>);
   const size_t smem = sizeof(WarpPoly<FastCfg>) * kFastWarpsPerBlock;
+  const size_t smemc = sizeof(WarpPoly<FastCfgCount>) * kFastWarpsPerBlock;
   cudaError_t e = cudaFuncSetAttribute(k_clip_fast<FastCfg, kFastWarpsPerBlock, kFp64MinBlocks>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(k_clip_fast<FastCfgCount, kFastWarpsPerBlock, kFp64MinBlocks>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemc);
   if (e != cudaSuccess) return e;
   int nb = 0;
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_clip_fast<FastCfg, kFastWarpsPerBlock, kFp64MinBlocks>,
@@ -35,8 +35,9 @@ cudaError_t clip_fp64_info(ClipLaunchInfo* info) {
 cudaError_t launch_clip_fp64_fast(const TessDesc& T, const WorkList& W, int nblocks, bool count,
                                   cudaStream_t s) {
   const size_t smem = sizeof(WarpPoly<FastCfg>) * kFastWarpsPerBlock;
+  const size_t smemc = sizeof(WarpPoly<FastCfgCount>) * kFastWarpsPerBlock;
   if (count)
-    k_clip_fast<FastCfgCount, kFastWarpsPerBlock, kFp64MinBlocks><<<nblocks, kFastWarpsPerBlock * 32, smem, s>>>(T, W);
+    k_clip_fast<FastCfgCount, kFastWarpsPerBlock, kFp64MinBlocks><<<nblocks, kFastWarpsPerBlock * 32, smemc, s>>>(T, W);
   else
     k_clip_fast<FastCfg, kFastWarpsPerBlock, kFp64MinBlocks><<<nblocks, kFastWarpsPerBlock * 32, smem, s>>>(T, W);
   return cudaGetLastError();
@@ -52,9 +53,10 @@ cudaError_t launch_clip_fp64_big(const TessDesc& T, const WorkList& W, void* scr
 cudaError_t launch_clip_fp64_fast_batched(const TessDesc* descs, const uint32_t* tess_off, int ntess,
                                           const WorkList& W, int nblocks, bool count, cudaStream_t s) {
   const size_t smem = sizeof(WarpPoly<FastCfg>) * kFastWarpsPerBlock;
+  const size_t smemc = sizeof(WarpPoly<FastCfgCount>) * kFastWarpsPerBlock;
   if (count)
     k_clip_fast_batched<FastCfgCount, kFastWarpsPerBlock, kFp64MinBlocks>
-        <<<nblocks, kFastWarpsPerBlock * 32, smem, s>>>(descs, tess_off, ntess, W);
+        <<<nblocks, kFastWarpsPerBlock * 32, smemc, s>>>(descs, tess_off, ntess, W);
   else
     k_clip_fast_batched<FastCfg, kFastWarpsPerBlock, kFp64MinBlocks>
         <<<nblocks, kFastWarpsPerBlock * 32, smem, s>>>(descs, tess_off, ntess, W);
@@ -70,11 +72,12 @@ cudaError_t launch_clip_fp64_big_batched(const TessDesc* descs, const uint32_t* 
 
 cudaError_t clip_fp64_batched_setup() {
   const size_t smem = sizeof(WarpPoly<FastCfg>) * kFastWarpsPerBlock;
+  const size_t smemc = sizeof(WarpPoly<FastCfgCount>) * kFastWarpsPerBlock;
   cudaError_t e = cudaFuncSetAttribute(k_clip_fast_batched<FastCfg, kFastWarpsPerBlock, kFp64MinBlocks>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(k_clip_fast_batched<FastCfgCount, kFastWarpsPerBlock, kFp64MinBlocks>,
-                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemc);
 }
 
 constexpr int kMedWarpsPerBlock = 2;

@@ -12,21 +12,21 @@
 
 namespace vd {
 
-static_assert(sizeof(WarpPoly<MixedCfg>) == sizeof(WarpPoly<MixedCfgCount>), "same layout");
 
-// shared memory admits 6 blocks of 4 warps per SM; keep registers in step
-constexpr int kMixedMinBlocks = 6;
+// shared memory admits 7 blocks of 4 warps per SM; keep registers in step
+constexpr int kMixedMinBlocks = 7;
 
 cudaError_t clip_mixed_info(ClipLaunchInfo* info) {
   info->smem_per_warp = sizeof(WarpPoly<MixedCfg>);
   info->warps_per_block = kFastWarpsPerBlock;
   info->big_scratch_per_warp = sizeof(WarpPoly<BigCfg>);
   const size_t smem = sizeof(WarpPoly<MixedCfg>) * kFastWarpsPerBlock;
+  const size_t smemc = sizeof(WarpPoly<MixedCfgCount>) * kFastWarpsPerBlock;
   cudaError_t e = cudaFuncSetAttribute(k_clip_fast<MixedCfg, kFastWarpsPerBlock, kMixedMinBlocks>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(k_clip_fast<MixedCfgCount, kFastWarpsPerBlock, kMixedMinBlocks>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemc);
   if (e != cudaSuccess) return e;
   int nb = 0;
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_clip_fast<MixedCfg, kFastWarpsPerBlock, kMixedMinBlocks>,
@@ -38,8 +38,9 @@ cudaError_t clip_mixed_info(ClipLaunchInfo* info) {
 cudaError_t launch_clip_mixed_fast(const TessDesc& T, const WorkList& W, int nblocks, bool count,
                                    cudaStream_t s) {
   const size_t smem = sizeof(WarpPoly<MixedCfg>) * kFastWarpsPerBlock;
+  const size_t smemc = sizeof(WarpPoly<MixedCfgCount>) * kFastWarpsPerBlock;
   if (count)
-    k_clip_fast<MixedCfgCount, kFastWarpsPerBlock, kMixedMinBlocks><<<nblocks, kFastWarpsPerBlock * 32, smem, s>>>(T, W);
+    k_clip_fast<MixedCfgCount, kFastWarpsPerBlock, kMixedMinBlocks><<<nblocks, kFastWarpsPerBlock * 32, smemc, s>>>(T, W);
   else
     k_clip_fast<MixedCfg, kFastWarpsPerBlock, kMixedMinBlocks><<<nblocks, kFastWarpsPerBlock * 32, smem, s>>>(T, W);
   return cudaGetLastError();
@@ -48,9 +49,10 @@ cudaError_t launch_clip_mixed_fast(const TessDesc& T, const WorkList& W, int nbl
 cudaError_t launch_clip_mixed_fast_batched(const TessDesc* descs, const uint32_t* tess_off, int ntess,
                                            const WorkList& W, int nblocks, bool count, cudaStream_t s) {
   const size_t smem = sizeof(WarpPoly<MixedCfg>) * kFastWarpsPerBlock;
+  const size_t smemc = sizeof(WarpPoly<MixedCfgCount>) * kFastWarpsPerBlock;
   if (count)
     k_clip_fast_batched<MixedCfgCount, kFastWarpsPerBlock, kMixedMinBlocks>
-        <<<nblocks, kFastWarpsPerBlock * 32, smem, s>>>(descs, tess_off, ntess, W);
+        <<<nblocks, kFastWarpsPerBlock * 32, smemc, s>>>(descs, tess_off, ntess, W);
   else
     k_clip_fast_batched<MixedCfg, kFastWarpsPerBlock, kMixedMinBlocks>
         <<<nblocks, kFastWarpsPerBlock * 32, smem, s>>>(descs, tess_off, ntess, W);
@@ -59,11 +61,12 @@ cudaError_t launch_clip_mixed_fast_batched(const TessDesc* descs, const uint32_t
 
 cudaError_t clip_mixed_batched_setup() {
   const size_t smem = sizeof(WarpPoly<MixedCfg>) * kFastWarpsPerBlock;
+  const size_t smemc = sizeof(WarpPoly<MixedCfgCount>) * kFastWarpsPerBlock;
   cudaError_t e = cudaFuncSetAttribute(k_clip_fast_batched<MixedCfg, kFastWarpsPerBlock, kMixedMinBlocks>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(k_clip_fast_batched<MixedCfgCount, kFastWarpsPerBlock, kMixedMinBlocks>,
-                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemc);
 }
 
 }  // namespace vd

@@ -1,0 +1,311 @@
+// vd_server.cu -- a request loop serving tessellations with continuous batching.
+//
+// Each request is one reference Tessellation job (bounds, grid, walls,
+// generators) answered with per-cell volume, centroid and face count.  The
+// server owns `slots` worker threads; each keeps one tessellation handle
+// (vd_tess, with its own CUDA stream) whose device buffers stay resident and
+// only grow, so a request costs no allocation once the slot has seen one of
+// its size.  Admission is FIFO by HBM budget: the head of the queue starts
+// as soon as a slot is free and its estimated footprint fits beside the
+// requests already running.  Requests that arrive while others are on the
+// GPU are admitted without waiting for them, and the slots' streams overlap
+// on the device.  Each request's result is computed by the same kernels as a
+// standalone vd_tess, so it is the same alone and in the mix.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/voronoid_b200.h"
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Request {
+  uint64_t id = 0;
+  double bmin[3], bmax[3];
+  int n[3];
+  std::vector<vd_wall_desc> walls;
+  std::vector<double> pts;
+  size_t est_bytes = 0;
+  Clock::time_point t_submit, t_start, t_done;
+  bool done = false;
+  int status = VD_OK;
+  std::string err;
+  size_t ncells = 0;
+  std::vector<double> vol, cen;
+  std::vector<int32_t> nf;
+};
+
+// device bytes a request of n generators on b bins needs (the buffers of a
+// vd_tess: generators, bins, bin-ordered copy, per-cell outputs and 48 face
+// slots, fallback lists) plus its search order
+size_t estimate_bytes(size_t n, size_t bins) {
+  const size_t per_cell = 24 * 3 + 32 + 4 * 6 + (8 + 24 + 4 + 4 + 1 + 8) + 48 * 12 + 3 * 4 + 8;
+  return n * per_cell + bins * 16 + (1u << 20);
+}
+
+double percentile(std::vector<double> v, double q) {
+  if (v.empty()) return 0.0;
+  std::sort(v.begin(), v.end());
+  const double pos = q * (double)(v.size() - 1);
+  const size_t lo = (size_t)pos;
+  const size_t hi = std::min(lo + 1, v.size() - 1);
+  return v[lo] + (v[hi] - v[lo]) * (pos - (double)lo);
+}
+
+}  // namespace
+
+struct vd_server {
+  int device = 0;
+  size_t budget = 0;
+  int precision = VD_PREC_FP64;
+  std::string err;
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  std::deque<std::shared_ptr<Request>> queue;
+  std::unordered_map<uint64_t, std::shared_ptr<Request>> live;
+  size_t in_use = 0, peak = 0;
+  uint64_t next_id = 1;
+  bool stop = false;
+  std::vector<std::thread> workers;
+  std::vector<vd_tess*> handles;
+  std::vector<double> latencies;
+  uint64_t completed = 0, cells = 0;
+};
+
+namespace {
+
+thread_local std::string g_server_create_error;
+
+int sfail(vd_server* s, int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  if (s) {
+    std::lock_guard<std::mutex> lock(s->mu);
+    s->err = buf;
+  } else {
+    g_server_create_error = buf;
+  }
+  return code;
+}
+
+int run_request(vd_tess* t, int precision, Request& r) {
+  int rc = vd_tess_reset(t, r.bmin, r.bmax, r.n[0], r.n[1], r.n[2]);
+  if (rc == VD_OK) rc = vd_tess_set_precision(t, precision);
+  for (const vd_wall_desc& w : r.walls) {
+    if (rc != VD_OK) break;
+    rc = w.kind == 0 ? vd_tess_add_wall_plane(t, w.a, w.n, w.id) : vd_tess_add_wall_sphere(t, w.a, w.r, w.id);
+  }
+  size_t kept = 0;
+  if (rc == VD_OK) rc = vd_tess_set_generators(t, r.pts.data(), r.pts.size() / 3, &kept);
+  if (rc == VD_OK) rc = vd_tess_calculate(t);
+  if (rc == VD_OK) {
+    r.ncells = kept;
+    r.vol.resize(kept);
+    r.cen.resize(3 * kept);
+    r.nf.resize(kept);
+    rc = vd_tess_get_cell_summaries(t, r.vol.data(), r.cen.data(), r.nf.data());
+  }
+  if (rc != VD_OK) r.err = vd_last_error(t);
+  return rc;
+}
+
+void worker(vd_server* s, int slot) {
+  cudaSetDevice(s->device);
+  vd_tess* t = s->handles[slot];
+  for (;;) {
+    std::shared_ptr<Request> r;
+    {
+      std::unique_lock<std::mutex> lock(s->mu);
+      s->cv_work.wait(lock, [&] {
+        if (s->stop) return true;
+        if (s->queue.empty()) return false;
+        const size_t need = s->queue.front()->est_bytes;
+        return s->in_use == 0 || s->in_use + need <= s->budget;
+      });
+      if (s->stop) return;
+      r = s->queue.front();
+      s->queue.pop_front();
+      s->in_use += r->est_bytes;
+      s->peak = std::max(s->peak, s->in_use);
+      r->t_start = Clock::now();
+    }
+    // the next queued request may fit beside this one
+    s->cv_work.notify_all();
+    const int rc = run_request(t, s->precision, *r);
+    {
+      std::lock_guard<std::mutex> lock(s->mu);
+      s->in_use -= r->est_bytes;
+      r->status = rc;
+      r->t_done = Clock::now();
+      r->done = true;
+      r->pts.clear();
+      r->pts.shrink_to_fit();
+      if (rc == VD_OK) {
+        s->latencies.push_back(std::chrono::duration<double>(r->t_done - r->t_submit).count());
+        s->completed++;
+        s->cells += r->ncells;
+      }
+    }
+    s->cv_done.notify_all();
+    s->cv_work.notify_all();
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* vd_server_last_error(const vd_server* s) {
+  return s ? s->err.c_str() : g_server_create_error.c_str();
+}
+
+int vd_server_create(int slots, size_t hbm_budget_bytes, int precision, vd_server** out) {
+  if (!out || slots <= 0 || slots > 256) return sfail(nullptr, VD_EINVAL, "slots must be in [1, 256]");
+  if (precision != VD_PREC_FP64 && precision != VD_PREC_MIXED) return sfail(nullptr, VD_EINVAL, "unknown precision");
+  *out = nullptr;
+  vd_server* s = new vd_server();
+  if (cudaGetDevice(&s->device) != cudaSuccess) {
+    delete s;
+    return sfail(nullptr, VD_ECUDA, "no CUDA device");
+  }
+  s->budget = hbm_budget_bytes;
+  s->precision = precision;
+  const double lo[3] = {0, 0, 0}, hi[3] = {1, 1, 1};
+  for (int k = 0; k < slots; ++k) {
+    vd_tess* t = nullptr;
+    const int rc = vd_tess_create(lo, hi, 1, 1, 1, &t);
+    if (rc != VD_OK) {
+      const std::string m = vd_last_error(nullptr);
+      for (vd_tess* h : s->handles) vd_tess_destroy(h);
+      delete s;
+      return sfail(nullptr, rc, "slot setup: %s", m.c_str());
+    }
+    s->handles.push_back(t);
+  }
+  for (int k = 0; k < slots; ++k) s->workers.emplace_back(worker, s, k);
+  *out = s;
+  return VD_OK;
+}
+
+int vd_server_destroy(vd_server* s) {
+  if (!s) return VD_OK;
+  {
+    std::lock_guard<std::mutex> lock(s->mu);
+    s->stop = true;
+  }
+  s->cv_work.notify_all();
+  for (auto& w : s->workers) w.join();
+  for (vd_tess* t : s->handles) vd_tess_destroy(t);
+  delete s;
+  return VD_OK;
+}
+
+int vd_server_submit(vd_server* s, const double bmin[3], const double bmax[3], int nx, int ny, int nz,
+                     const vd_wall_desc* walls, int nwalls, const double* xyz, size_t n, uint64_t* ticket) {
+  if (!s || !bmin || !bmax || !ticket || (!xyz && n) || (nwalls > 0 && !walls) || nwalls < 0)
+    return VD_EINVAL;
+  if (nx <= 0 || ny <= 0 || nz <= 0) return sfail(s, VD_EINVAL, "grid resolution must be positive");
+  for (int k = 0; k < nwalls; ++k)
+    if (walls[k].id > VD_WALL_ID_MAX || (walls[k].kind != 0 && walls[k].kind != 1))
+      return sfail(s, VD_EINVAL, "bad wall %d", k);
+  auto r = std::make_shared<Request>();
+  for (int a = 0; a < 3; ++a) {
+    r->bmin[a] = bmin[a];
+    r->bmax[a] = bmax[a];
+  }
+  r->n[0] = nx;
+  r->n[1] = ny;
+  r->n[2] = nz;
+  r->walls.assign(walls, walls + nwalls);
+  r->pts.assign(xyz, xyz + 3 * n);
+  r->est_bytes = estimate_bytes(n, (size_t)nx * ny * nz);
+  if (r->est_bytes > s->budget) return sfail(s, VD_ENOMEM, "request needs %zu bytes, budget %zu", r->est_bytes, s->budget);
+  {
+    std::lock_guard<std::mutex> lock(s->mu);
+    r->id = s->next_id++;
+    r->t_submit = Clock::now();
+    s->live[r->id] = r;
+    s->queue.push_back(r);
+    *ticket = r->id;
+  }
+  s->cv_work.notify_all();
+  return VD_OK;
+}
+
+int vd_server_wait(vd_server* s, uint64_t ticket, size_t* n_cells, double* latency_s) {
+  if (!s) return VD_EINVAL;
+  std::unique_lock<std::mutex> lock(s->mu);
+  auto it = s->live.find(ticket);
+  if (it == s->live.end()) {
+    s->err = "unknown ticket";
+    return VD_EINVAL;
+  }
+  std::shared_ptr<Request> r = it->second;
+  s->cv_done.wait(lock, [&] { return r->done; });
+  if (n_cells) *n_cells = r->ncells;
+  if (latency_s) *latency_s = std::chrono::duration<double>(r->t_done - r->t_submit).count();
+  if (r->status != VD_OK) s->err = r->err;
+  return r->status;
+}
+
+int vd_server_take(vd_server* s, uint64_t ticket, double* volume, double* centroid3, int32_t* n_faces) {
+  if (!s) return VD_EINVAL;
+  std::shared_ptr<Request> r;
+  {
+    std::unique_lock<std::mutex> lock(s->mu);
+    auto it = s->live.find(ticket);
+    if (it == s->live.end()) {
+      s->err = "unknown ticket";
+      return VD_EINVAL;
+    }
+    r = it->second;
+    s->cv_done.wait(lock, [&] { return r->done; });
+    s->live.erase(it);
+  }
+  if (r->status != VD_OK) return r->status;
+  if (volume) memcpy(volume, r->vol.data(), r->ncells * sizeof(double));
+  if (centroid3) memcpy(centroid3, r->cen.data(), 3 * r->ncells * sizeof(double));
+  if (n_faces) memcpy(n_faces, r->nf.data(), r->ncells * sizeof(int32_t));
+  return VD_OK;
+}
+
+int vd_server_stats(vd_server* s, uint64_t* completed, uint64_t* cells, double* p50_s, double* p99_s,
+                    size_t* peak_bytes) {
+  if (!s) return VD_EINVAL;
+  std::lock_guard<std::mutex> lock(s->mu);
+  if (completed) *completed = s->completed;
+  if (cells) *cells = s->cells;
+  if (p50_s) *p50_s = percentile(s->latencies, 0.50);
+  if (p99_s) *p99_s = percentile(s->latencies, 0.99);
+  if (peak_bytes) *peak_bytes = s->peak;
+  return VD_OK;
+}
+
+int vd_server_reset_stats(vd_server* s) {
+  if (!s) return VD_EINVAL;
+  std::lock_guard<std::mutex> lock(s->mu);
+  s->latencies.clear();
+  s->completed = 0;
+  s->cells = 0;
+  s->peak = s->in_use;
+  return VD_OK;
+}
+
+}  // extern "C"

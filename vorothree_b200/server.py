@@ -1,0 +1,86 @@
+"""Serving tessellations with continuous batching (vd_server_* C ABI).
+
+Worker slots keep resident device buffers; requests are admitted FIFO by an
+HBM budget as soon as a slot frees, and concurrent requests overlap on the
+GPU.  A request's result equals a standalone Tessellation's.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Sequence
+
+import numpy as np
+
+from ._lib import VD_PREC_FP64, VD_PREC_MIXED, VoronoidError, load
+from .batch import _walls
+from .tessellation import BoundingBox, Wall
+
+
+class TessellationServer:
+    def __init__(self, slots: int = 4, hbm_budget_bytes: int = 32 << 30, precision: str = "fp64"):
+        self._L = load()
+        h = C.c_void_p()
+        rc = self._L.vd_server_create(int(slots), int(hbm_budget_bytes),
+                                      {"fp64": VD_PREC_FP64, "mixed": VD_PREC_MIXED}[precision], C.byref(h))
+        if rc != 0:
+            raise VoronoidError(rc, self._L.vd_server_last_error(None).decode())
+        self._h = h
+
+    def _chk(self, rc):
+        if rc != 0:
+            msg = self._L.vd_server_last_error(self._h)
+            raise VoronoidError(rc, msg.decode() if msg else "")
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self._L.vd_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, bounds: BoundingBox, grid: Sequence[int], generators, walls: Sequence[Wall] = ()) -> int:
+        mn = np.asarray(bounds.min, np.float64)
+        mx = np.asarray(bounds.max, np.float64)
+        pts = np.ascontiguousarray(np.asarray(generators, np.float64).reshape(-1))
+        wd = _walls(walls)
+        t = C.c_uint64()
+        d = C.POINTER(C.c_double)
+        self._chk(self._L.vd_server_submit(self._h, mn.ctypes.data_as(d), mx.ctypes.data_as(d), int(grid[0]),
+                                           int(grid[1]), int(grid[2]), C.cast(wd, C.c_void_p), len(walls),
+                                           pts.ctypes.data_as(d), pts.size // 3, C.byref(t)))
+        return t.value
+
+    def wait(self, ticket: int):
+        """(n_cells, latency_seconds) once the request is done."""
+        n = C.c_size_t()
+        lat = C.c_double()
+        self._chk(self._L.vd_server_wait(self._h, C.c_uint64(ticket), C.byref(n), C.byref(lat)))
+        return n.value, lat.value
+
+    def take(self, ticket: int):
+        """(volume[n], centroid[n,3], n_faces[n]); releases the request."""
+        n, _ = self.wait(ticket)
+        vol = np.zeros(n, np.float64)
+        cen = np.zeros((n, 3), np.float64)
+        nf = np.zeros(n, np.int32)
+        self._chk(self._L.vd_server_take(self._h, C.c_uint64(ticket), C.c_void_p(vol.ctypes.data),
+                                         C.c_void_p(cen.ctypes.data), C.c_void_p(nf.ctypes.data)))
+        return vol, cen, nf
+
+    def stats(self) -> dict:
+        done = C.c_uint64()
+        cells = C.c_uint64()
+        p50 = C.c_double()
+        p99 = C.c_double()
+        peak = C.c_size_t()
+        self._chk(self._L.vd_server_stats(self._h, C.byref(done), C.byref(cells), C.byref(p50), C.byref(p99),
+                                          C.byref(peak)))
+        return {"completed": done.value, "cells": cells.value, "p50_s": p50.value, "p99_s": p99.value,
+                "peak_bytes": peak.value}
+
+    def reset_stats(self):
+        self._chk(self._L.vd_server_reset_stats(self._h))
