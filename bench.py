@@ -156,7 +156,7 @@ def run_reference(args):
     from oracle.oracle import OracleTessellation
     t = OracleTessellation([0, 0, 0], [1, 1, 1], GRID, GRID, GRID)
     t.set_generators(pts)
-    sample = args.ref_sample
+    sample = min(args.ref_sample or N_GEN, N_GEN)
     begin = (N_GEN - sample) // 2
     for _ in range(args.warmup):
         t.calculate_range(begin, begin + sample, nthreads)
@@ -366,9 +366,10 @@ def run_ours(args):
                                              "0-2 walls; 4 slots; p50/p99 = submit-to-result latency")
         if ws == 1 and not args.no_cpu_baseline:
             nthreads = os.cpu_count() or 1
-            cv, cdt = cpu_baseline(pts, nthreads, args.cpu_sample)
+            sample = min(args.cpu_sample or N_GEN, N_GEN)
+            cv, cdt = cpu_baseline(pts, nthreads, sample)
             line["cpu_baseline"] = {"value": cv, "unit": "cells/s", "cores": nthreads, "kind": "port",
-                                    "sample": f"{args.cpu_sample} of {N_GEN} cells of the same tessellation "
+                                    "sample": f"{sample} of {N_GEN} cells of the same tessellation "
                                               f"({cdt:.2f} s wall)"}
         print(json.dumps(line), flush=True)
     tess.close()
@@ -586,8 +587,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
-    ap.add_argument("--cpu-sample", type=int, default=262144)
-    ap.add_argument("--ref-sample", type=int, default=131072)
+    ap.add_argument("--cpu-sample", type=int, default=0,
+                    help="cells of the CPU baseline (0 = every cell of the workload)")
+    ap.add_argument("--ref-sample", type=int, default=0,
+                    help="cells per step of the reference arm (0 = every cell of the workload)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--n", type=int, default=N_GEN, help="generators (profiling runs use a smaller case)")

@@ -86,6 +86,13 @@ int vd_tess_set_precision(vd_tess* t, int precision);
  * Cell3DFaces::clip_with_scratch (cell_3d_faces.rs:288-503), with the volume,
  * centroid and face-area reductions (cell_3d_faces.rs:106-254) fused in. */
 int vd_tess_calculate(vd_tess* t);
+/* The same computation restricted to the cells with ids in [begin, end): the
+ * shard of one process when a tessellation's cells are split across GPUs
+ * (each GPU holds all generators and computes its own id range).  Cells
+ * outside the range read as empty (volume 0, centroid 0, no faces), as in
+ * the reference's per-cell map (tessellation.rs:223-229) restricted to the
+ * range.  VD_EINVAL unless begin <= end <= count_generators. */
+int vd_tess_calculate_range(vd_tess* t, size_t begin, size_t end);
 /* Tessellation::relax (tessellation.rs:482-495), on the device */
 int vd_tess_relax(vd_tess* t);
 /* Tessellation::count_cells (tessellation.rs:503-505) */

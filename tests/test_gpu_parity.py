@@ -260,3 +260,43 @@ def test_dense_blob_overflow_tiers(oracle_mod, precision):
     o = oracle_tess(oracle_mod, [0, 0, 0], [1, 1, 1], (4, 4, 4), pts)
     assert g.fallback_counts()["overflow"] > 0
     assert_same(g, o, check_counters=False)
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_calculate_range_shards(oracle_mod, precision):
+    """calculate_range computes exactly the oracle's cells of the range and
+    leaves the others empty; the shards of a split put together equal one
+    full calculate()."""
+    import vorothree_b200 as v
+    from vorothree_b200.shard import cell_range
+    pts = uniform(30000, 0.0, 1.0, 21)
+    walls = [v.Wall(WALL, v.SphereGeometry([0.5, 0.5, 0.5], 0.47))]
+    g = gpu_tess([0, 0, 0], [1, 1, 1], (24, 24, 24), pts, walls, precision=precision)
+    full_v, full_c, full_n = g.summaries()
+    full_off, full_ids = g.neighbors()
+    n = g.count_generators()
+    o = oracle_mod.OracleTessellation([0, 0, 0], [1, 1, 1], 24, 24, 24)
+    o.set_generators(pts)
+    o.add_wall_sphere([0.5, 0.5, 0.5], 0.47, WALL)
+    world = 3
+    got_v, got_c, got_n = np.zeros(n), np.zeros((n, 3)), np.zeros(n, np.int32)
+    for rank in range(world):
+        b, e = cell_range(n, rank, world)
+        g.calculate_range(b, e)
+        o.calculate_range(b, e)
+        assert_same(g, o, sample_cells=4)
+        gv, gc, gn = g.summaries()
+        outside = np.ones(n, bool)
+        outside[b:e] = False
+        assert np.all(gv[outside] == 0) and np.all(gn[outside] == 0) and np.all(gc[outside] == 0)
+        got_v[b:e], got_c[b:e], got_n[b:e] = gv[b:e], gc[b:e], gn[b:e]
+    assert np.array_equal(got_v, full_v) and np.array_equal(got_c, full_c) and np.array_equal(got_n, full_n)
+    # an empty range and the full range
+    g.calculate_range(5, 5)
+    assert g.summaries()[2].sum() == 0 and g.total_faces() == 0
+    g.calculate_range(0, n)
+    assert np.array_equal(g.neighbors()[1], full_ids)
+    with pytest.raises(v.VoronoidError):
+        g.calculate_range(0, n + 1)
+    with pytest.raises(ValueError):
+        g.calculate_range(4, 3)

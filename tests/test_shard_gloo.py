@@ -1,0 +1,81 @@
+"""Sharding one tessellation's cells over processes (CPU, gloo, world 2).
+
+Each rank computes its id range -- here with the oracle, standing in for the
+GPU on this CPU-only test -- and gather_summaries assembles the full result
+on every rank; it must equal one full calculate() bit for bit.  The GPU
+side of the split (calculate_range) is checked in test_gpu_parity.py.
+"""
+import os
+import socket
+
+import numpy as np
+import pytest
+
+from common import uniform
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank(rank, world, port, q):
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, root)
+    sys.path.insert(0, os.path.join(root, "tests"))
+    import datetime
+    import torch.distributed as dist
+    from oracle.oracle import OracleTessellation
+    from vorothree_b200.shard import cell_range, gather_summaries
+    try:
+        dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world,
+                                timeout=datetime.timedelta(seconds=60))
+        pts = uniform(6000, 0.0, 1.0, 31)
+        t = OracleTessellation([0, 0, 0], [1, 1, 1], 12, 12, 12)
+        t.add_wall_sphere([0.5, 0.5, 0.5], 0.46, -1000)
+        n = t.set_generators(pts)
+        b, e = cell_range(n, rank, world)
+        t.calculate_range(b, e, 1)
+        vol, cen, nf = t.summaries()
+        gv, gc, gn = gather_summaries(vol[b:e], cen[b:e], nf[b:e], n)
+        full = OracleTessellation([0, 0, 0], [1, 1, 1], 12, 12, 12)
+        full.add_wall_sphere([0.5, 0.5, 0.5], 0.46, -1000)
+        full.set_generators(pts)
+        full.calculate(1)
+        fv, fc, fn = full.summaries()
+        ok = np.array_equal(gv, fv) and np.array_equal(gc, fc) and np.array_equal(gn, fn)
+        dist.destroy_process_group()
+        q.put((rank, ok, None))
+    except Exception as ex:  # reported to the parent
+        q.put((rank, False, repr(ex)))
+
+
+def test_cell_range_partition():
+    from vorothree_b200.shard import cell_range
+    for n in (0, 1, 7, 1000, 1 << 20):
+        for world in (1, 2, 3, 8):
+            ranges = [cell_range(n, r, world) for r in range(world)]
+            assert ranges[0][0] == 0 and ranges[-1][1] == n
+            assert all(ranges[k][1] == ranges[k + 1][0] for k in range(world - 1))
+            sizes = [e - b for b, e in ranges]
+            assert max(sizes) - min(sizes) <= 1
+    with pytest.raises(ValueError):
+        cell_range(10, 2, 2)
+
+
+def test_sharded_summaries_gloo_world2(oracle_mod):
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    results = [q.get(timeout=180) for _ in procs]
+    for p in procs:
+        p.join(timeout=60)
+    for rank, ok, err in sorted(results):
+        assert err is None, f"rank {rank}: {err}"
+        assert ok, f"rank {rank}: gathered summaries differ from a full calculate"

@@ -9,8 +9,10 @@ reference's API over that ABI.
 from ._lib import VoronoidError, load
 from .batch import TessellationBatch
 from .server import TessellationServer
+from .shard import calculate_sharded, cell_range, gather_summaries
 from .tessellation import (WALL_ID_MAX, Algorithm3DGrid, BoundingBox, Cell3DFaces, PlaneGeometry,
                            SphereGeometry, Tessellation, Wall, box_side)
 
 __all__ = ["Algorithm3DGrid", "BoundingBox", "Cell3DFaces", "PlaneGeometry", "SphereGeometry",
-           "Tessellation", "TessellationBatch", "TessellationServer", "Wall", "WALL_ID_MAX", "box_side", "VoronoidError", "load"]
+           "Tessellation", "TessellationBatch", "TessellationServer", "Wall", "WALL_ID_MAX", "box_side", "VoronoidError", "load",
+           "calculate_sharded", "cell_range", "gather_summaries"]

@@ -48,6 +48,7 @@ SIGNATURES = {
     "vd_tess_get_generators": (C.c_int, [_vp, _d]),
     "vd_tess_set_precision": (C.c_int, [_vp, C.c_int]),
     "vd_tess_calculate": (C.c_int, [_vp]),
+    "vd_tess_calculate_range": (C.c_int, [_vp, C.c_size_t, C.c_size_t]),
     "vd_tess_relax": (C.c_int, [_vp]),
     "vd_tess_count_cells": (C.c_int, [_vp, _szp]),
     "vd_tess_get_cell_summaries": (C.c_int, [_vp, _vp, _vp, _vp]),

@@ -298,5 +298,36 @@ __global__ void k_relax(const double* __restrict__ gen, const int32_t* __restric
   }
 }
 
+// ---- cell-id ranges (calculate_range) ------------------------------------------
+// flags[k] = 1 when the generator at bin-order position k has an id in
+// [begin, end); the scan of the flags then lists the range in bin order, so a
+// shard's warps still walk neighbouring cells one after another.
+__global__ void k_range_flags(const SortedGen* __restrict__ sorted, size_t n, long long begin, long long end,
+                              uint32_t* __restrict__ flags) {
+  for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    const long long id = sorted[k].id;
+    flags[k] = (id >= begin && id < end) ? 1u : 0u;
+  }
+}
+
+__global__ void k_range_compact(const SortedGen* __restrict__ sorted, size_t n, const uint32_t* __restrict__ flags,
+                                const uint32_t* __restrict__ pos, uint32_t* __restrict__ list) {
+  for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
+    if (flags[k]) list[pos[k]] = (uint32_t)sorted[k].id;
+}
+
+// cells outside a computed range read as empty (volume 0, centroid 0, no faces)
+__global__ void k_clear_cells(size_t n, double* __restrict__ vol, double* __restrict__ cen,
+                              int32_t* __restrict__ nfaces, int32_t* __restrict__ nverts) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    vol[i] = 0.0;
+    cen[3 * i] = 0.0;
+    cen[3 * i + 1] = 0.0;
+    cen[3 * i + 2] = 0.0;
+    nfaces[i] = 0;
+    nverts[i] = 0;
+  }
+}
+
 }  // namespace
 }  // namespace vd

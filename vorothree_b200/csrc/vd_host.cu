@@ -108,6 +108,7 @@ struct vd_tess {
   DevBuf<long long> d_pool_off, d_csr_off, d_nf64;
   bool csr_valid = false;
   long long csr_total = 0;
+  size_t range_begin = 0, range_end = 0;  // cells computed by the last calculate
 
   // control
   DevBuf<unsigned int> d_ctl;
@@ -411,7 +412,11 @@ int read_ctl(vd_tess* t, unsigned int* ovf, unsigned int* tab) {
 // Runs the fast pass over all cells, then resolves the cells it could not
 // finish: a longer search order for cells that walked off a truncated one,
 // the large-capacity pass for polytopes that outgrew shared memory.
-int run_calculate(vd_tess* t, const WorkList* extra = nullptr, const uint32_t* only_cell = nullptr) {
+//
+// only_cell: compute that one cell (get_cell's export).  range: compute the
+// cells with ids in [range[0], range[1]) and clear the others.
+int run_calculate(vd_tess* t, const WorkList* extra = nullptr, const uint32_t* only_cell = nullptr,
+                  const size_t* range = nullptr) {
   cudaStream_t s = t->stream;
   const size_t n = t->ngen;
   int r = ensure_outputs(t, n);
@@ -425,6 +430,29 @@ int run_calculate(vd_tess* t, const WorkList* extra = nullptr, const uint32_t* o
   if (only_cell) {
     VD_CK(t, cudaMemcpyAsync(t->d_list[2].p, only_cell, sizeof(uint32_t), cudaMemcpyHostToDevice, s));
     in_list = t->d_list[2].p;
+  } else if (range && (range[0] > 0 || range[1] < n)) {
+    VD_CK(t, t->d_flags.ensure(n + 1));
+    VD_CK(t, t->d_pos.ensure(n + 1));
+    if (n) {
+      k_clear_cells<<<grid_blocks(t, n, 256), 256, 0, s>>>(n, t->d_vol.p, t->d_cen.p, t->d_nf.p, t->d_nv.p);
+      g_launches++;
+      VD_CK(t, cudaGetLastError());
+      k_range_flags<<<grid_blocks(t, n, 256), 256, 0, s>>>(t->d_sorted.p, n, (long long)range[0],
+                                                           (long long)range[1], t->d_flags.p);
+      g_launches++;
+      VD_CK(t, cudaGetLastError());
+    }
+    VD_CK(t, cudaMemsetAsync(t->d_flags.p + n, 0, sizeof(uint32_t), s));
+    r = scan_excl<uint32_t, uint32_t>(t, t->d_flags.p, t->d_pos.p, n + 1, t->scan32);
+    if (r != VD_OK) return r;
+    if (n) {
+      k_range_compact<<<grid_blocks(t, n, 256), 256, 0, s>>>(t->d_sorted.p, n, t->d_flags.p, t->d_pos.p,
+                                                             t->d_list[2].p);
+      g_launches++;
+      VD_CK(t, cudaGetLastError());
+    }
+    in_list = t->d_list[2].p;
+    nin = (uint32_t)(range[1] - range[0]);
   }
   if (nin > 0) {
     r = clip_pass(t, 0, in_list, nin, t->d_list[0].p, t->d_list[1].p, extra);
@@ -816,6 +844,25 @@ int vd_tess_calculate(vd_tess* t) {
   int r = run_calculate(t);
   if (r != VD_OK) return r;
   t->ncells = t->ngen;
+  t->range_begin = 0;
+  t->range_end = t->ngen;
+  t->calculated = true;
+  return VD_OK;
+}
+
+int vd_tess_calculate_range(vd_tess* t, size_t begin, size_t end) {
+  if (!t) return VD_EINVAL;
+  if (begin > end || end > t->ngen)
+    return fail(t, VD_EINVAL, "cell range [%zu, %zu) is not inside [0, %zu)", begin, end, t->ngen);
+  VD_CK(t, cudaSetDevice(t->device));
+  t->calculated = false;
+  t->csr_valid = false;
+  const size_t range[2] = {begin, end};
+  int r = run_calculate(t, nullptr, nullptr, range);
+  if (r != VD_OK) return r;
+  t->ncells = t->ngen;
+  t->range_begin = begin;
+  t->range_end = end;
   t->calculated = true;
   return VD_OK;
 }
@@ -914,6 +961,13 @@ int vd_tess_get_cell(vd_tess* t, size_t i, int32_t* n_vertices, int32_t* n_faces
   int r = check_ready(t);
   if (r != VD_OK) return r;
   if (i >= t->ncells) return fail(t, VD_EINVAL, "cell index %zu out of range", i);
+  if (i < t->range_begin || i >= t->range_end) {
+    // outside the range of the last calculate_range: an empty cell
+    if (n_vertices) *n_vertices = 0;
+    if (n_faces) *n_faces = 0;
+    if (n_face_indices) *n_face_indices = 0;
+    return VD_OK;
+  }
   cudaStream_t s = t->stream;
   const int cv = 2048, cf = 512, ch = 6144;
   VD_CK(t, t->d_ex_v.ensure(3 * cv));

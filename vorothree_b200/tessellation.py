@@ -260,6 +260,14 @@ class Tessellation:
     def calculate(self):
         self._ck(self._L.vd_tess_calculate(self._h))
 
+    def calculate_range(self, begin: int, end: int):
+        """calculate() for the cells with ids in [begin, end) only (one
+        shard of a tessellation split across GPUs); the other cells read as
+        empty.  ValueError unless 0 <= begin <= end <= count_generators()."""
+        if begin < 0 or end < begin:
+            raise ValueError(f"bad cell range [{begin}, {end})")
+        self._ck(self._L.vd_tess_calculate_range(self._h, int(begin), int(end)))
+
     def relax(self):
         self._ck(self._L.vd_tess_relax(self._h))
 
