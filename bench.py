@@ -382,19 +382,25 @@ def run_ours(args):
 def batched_members(ntess: int, seed: int = 0):
     """4096 tessellations (configurable), N log-uniform in [64, 65536], box
     edges U[1,10], even members with a centred sphere wall of radius
-    0.5*min(edge); bins per axis proportional to the edges with about one
-    generator per bin (near-cubic bins)."""
+    0.5*min(edge); near-cubic bins at the autotuner's density for uniform
+    input of the member's size."""
+    from vorothree_b200 import autotune
     rng = np.random.Generator(np.random.PCG64(seed))
     out = []
     for k in range(ntess):
         n = int(round(np.exp(rng.uniform(np.log(64), np.log(65536)))))
         edge = rng.uniform(1.0, 10.0, size=3)
-        per = (n / float(np.prod(edge))) ** (1.0 / 3.0)
-        grid = [max(1, int(round(e * per))) for e in edge]
+        # bin density from the autotuner's table for uniform input of this size
+        grid = list(autotune.grid_for(n, bounds_of(edge), autotune.lookup("uniform", n)))
         pts = rng.uniform(0.0, 1.0, size=(n, 3)) * edge
         sphere = (list(edge / 2.0), 0.5 * float(edge.min())) if k % 2 == 0 else None
         out.append((edge, grid, pts, sphere))
     return out
+
+
+def bounds_of(edge):
+    import vorothree_b200 as v
+    return v.BoundingBox([0, 0, 0], list(edge))
 
 
 def run_batched(args):
@@ -446,9 +452,10 @@ def serving_requests(count: int, seed: int = 0):
     """Requests of the serving workload: sizes log-uniform in [1e3, 1e6];
     half uniform, half clustered (8 Gaussian blobs, sigma 0.03, 70% of the
     points); 0-2 walls drawn from {plane through the centre with a random
-    normal, centred sphere of radius U[0.3, 0.5]}; grid ~ N^(1/3) per axis
-    (2.5x finer for clustered requests)."""
+    normal, centred sphere of radius U[0.3, 0.5]}; grid from the autotuner."""
     import vorothree_b200 as v
+    from vorothree_b200 import autotune
+    bounds = v.BoundingBox([0, 0, 0], [1, 1, 1])
     rng = np.random.Generator(np.random.PCG64(seed))
     out = []
     for k in range(count):
@@ -459,17 +466,16 @@ def serving_requests(count: int, seed: int = 0):
             c = rng.uniform(0.1, 0.9, size=(8, 3))
             pts = np.concatenate([c[np.arange(nb) % 8] + rng.normal(0.0, 0.03, size=(nb, 3)),
                                   rng.uniform(0.0, 1.0, size=(n - nb, 3))])
-            g = int(np.ceil(2.5 * n ** (1 / 3)))
         else:
             pts = rng.uniform(0.0, 1.0, size=(n, 3))
-            g = int(np.ceil(n ** (1 / 3)))
+        grid = autotune.choose_grid(pts, bounds)
         walls = []
         for w in range(int(rng.integers(0, 3))):
             if rng.uniform() < 0.5:
                 walls.append(v.Wall(v.WALL_ID_MAX - w, v.PlaneGeometry([0.5, 0.5, 0.5], list(rng.normal(size=3)))))
             else:
                 walls.append(v.Wall(v.WALL_ID_MAX - w, v.SphereGeometry([0.5, 0.5, 0.5], float(rng.uniform(0.3, 0.5)))))
-        out.append((v.BoundingBox([0, 0, 0], [1, 1, 1]), (g, g, g), pts, walls))
+        out.append((bounds, grid, pts, walls))
     return out
 
 
@@ -543,9 +549,13 @@ def run_blobs(args):
     centres = rng.uniform(0.0, 1.0, size=(64, 3))
     pts = np.concatenate([centres[np.arange(nb) % 64] + rng.normal(0.0, 0.01, size=(nb, 3)),
                           rng.uniform(0.0, 1.0, size=(n - nb, 3))])
+    from vorothree_b200 import autotune
+    bounds = v.BoundingBox([0, 0, 0], [1, 1, 1])
+    tuned = autotune.choose_grid(pts, bounds)
+    grids = [tuned] + [(g, g, g) for g in args.blob_grids if (g, g, g) != tuned]
     res = []
-    for g in args.blob_grids:
-        t = v.Tessellation(v.BoundingBox([0, 0, 0], [1, 1, 1]), v.Algorithm3DGrid(g, g, g))
+    for g in grids:
+        t = v.Tessellation(bounds, v.Algorithm3DGrid(*g))
         t.set_precision(args.precision)
         t.add_wall(v.Wall(v.WALL_ID_MAX, v.SphereGeometry([0.5, 0.5, 0.5], 0.45)))
         kept = t.set_generators(pts)
@@ -554,15 +564,16 @@ def run_blobs(args):
             t.calculate()
             times.append(t.timings()["clip_ms"] + t.timings()["fallback_ms"])
         ms = statistics.mean(times[args.warmup:])
-        res.append({"grid": g, "kept": kept, "ms": ms, "cells_per_s": kept / (ms / 1e3),
+        res.append({"grid": list(g), "kept": kept, "ms": ms, "cells_per_s": kept / (ms / 1e3),
                     "fallback_cells": t.fallback_counts()})
         t.close()
-    best = min(res, key=lambda r: r["ms"])
     line = {"metric": "3D cells/s, clustered generators", "workload": "blobs", "unit": "cells/s",
-            "value": best["cells_per_s"], "n_gpus": 1, "higher_is_better": True, "dtype": "f64",
+            "value": res[0]["cells_per_s"], "n_gpus": 1, "higher_is_better": True, "dtype": "f64",
             "precision": args.precision, "data": "synthetic (seeded PCG64)",
             "config": {"generators": n, "blobs": 64, "sigma": 0.01, "blob_fraction": 0.7,
-                       "wall": "sphere r=0.45 at (0.5,0.5,0.5)", "grids_tried": args.blob_grids},
+                       "wall": "sphere r=0.45 at (0.5,0.5,0.5)", "grid": list(tuned),
+                       "grid_source": "autotuner table (vorothree_b200/autotune_table.json)",
+                       "distribution_class": autotune.distribution_class(pts, bounds)},
             "per_grid": res}
     print(json.dumps(line), flush=True)
     return 0
@@ -581,7 +592,8 @@ def main():
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--lloyd-steps", type=int, default=20)
-    ap.add_argument("--blob-grids", type=int, nargs="+", default=[160, 256, 320, 400])
+    ap.add_argument("--blob-grids", type=int, nargs="*", default=[],
+                    help="cubic grids timed beside the autotuned one (blobs workload)")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)

@@ -140,6 +140,44 @@ int vd_tess_fallback_counts(vd_tess* t, uint64_t* out2);
 /* kernels this library has launched in this process, over all handles */
 int vd_launch_count(uint64_t* n);
 
+/* ---- one cell on its own: Cell3DFaces (cell_3d_faces.rs:22-270) behind the
+ *      Cell trait (cell/mod.rs:8-43) ----
+ * The polytope lives in device memory (up to 2048 vertices, 512 faces, 6144
+ * face entries) and every operation runs the tessellation kernels' own warp
+ * routines, one small launch per call.  A handle is not thread-safe. */
+typedef struct vd_cell vd_cell;
+/* message of the last failed call on c (of the last failed create when c is NULL) */
+const char* vd_cell_last_error(const vd_cell* c);
+/* Cell3DFaces::new(id, bounds) (cell_3d_faces.rs:37-74): the box cell */
+int vd_cell_create_box(size_t id, const double bmin[3], const double bmax[3], vd_cell** out);
+/* a cell holding a given polytope in the Cell3DFaces layout (cell_3d_faces.rs:24-34),
+ * e.g. one exported by vd_tess_get_cell; VD_EINVAL when a face entry names a
+ * missing vertex or the polytope exceeds the capacities */
+int vd_cell_create(size_t id, int32_t n_vertices, int32_t n_faces, const double* vertices,
+                   const uint32_t* face_counts, const uint32_t* face_indices, const int32_t* face_neighbors,
+                   vd_cell** out);
+int vd_cell_destroy(vd_cell* c);
+/* Cell3DFaces::id (cell_3d_faces.rs:77-79) */
+int vd_cell_id(const vd_cell* c, size_t* id);
+/* Cell::clip = Cell3DFaces::clip_with_scratch (cell_3d_faces.rs:288-503):
+ * clip by the plane (point, normal); the kept side is (v - point).normal <= 1e-9
+ * and the new face gets neighbor_id.  *modified and *max_radius_sq are the
+ * reference's returned (bool, f64): the max squared distance of the new
+ * vertices from `generator`, 0 when generator is NULL or nothing changed. */
+int vd_cell_clip(vd_cell* c, const double point[3], const double normal[3], int32_t neighbor_id,
+                 const double* generator, int* modified, double* max_radius_sq);
+/* Cell3DFaces::max_radius_sq (cell_3d_faces.rs:271-286) */
+int vd_cell_max_radius_sq(vd_cell* c, const double center[3], double* out);
+/* volume, centroid, face count, and the area and neighbour of every face
+ * (cell_3d_faces.rs:106-254, 97-99); face_areas / face_neighbors hold
+ * n_faces entries (call once with NULL to learn n_faces); any pointer may be NULL */
+int vd_cell_measure(vd_cell* c, double* volume, double centroid3[3], int32_t* n_faces, double* face_areas,
+                    int32_t* face_neighbors);
+/* the polytope (vertices, face_counts, face_indices, face_neighbors); call
+ * with NULL buffers to get the sizes */
+int vd_cell_get(vd_cell* c, int32_t* n_vertices, int32_t* n_faces, int32_t* n_face_indices, double* vertices,
+                uint32_t* face_counts, uint32_t* face_indices, int32_t* face_neighbors);
+
 /* ---- pinned host memory for callers staging large inputs/outputs ---- */
 int vd_host_alloc(size_t bytes, void** ptr);
 int vd_host_free(void* ptr);

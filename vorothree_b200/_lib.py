@@ -93,6 +93,15 @@ SIGNATURES = {
     "vd_server_take": (C.c_int, [_vp, C.c_uint64, _vp, _vp, _vp]),
     "vd_server_stats": (C.c_int, [_vp, _u64p, _u64p, _d, _d, _szp]),
     "vd_server_reset_stats": (C.c_int, [_vp]),
+    "vd_cell_last_error": (C.c_char_p, [_vp]),
+    "vd_cell_create_box": (C.c_int, [C.c_size_t, _d, _d, C.POINTER(_vp)]),
+    "vd_cell_create": (C.c_int, [C.c_size_t, C.c_int32, C.c_int32, _vp, _vp, _vp, _vp, C.POINTER(_vp)]),
+    "vd_cell_destroy": (C.c_int, [_vp]),
+    "vd_cell_id": (C.c_int, [_vp, _szp]),
+    "vd_cell_clip": (C.c_int, [_vp, _d, _d, C.c_int32, _d, C.POINTER(C.c_int), _d]),
+    "vd_cell_max_radius_sq": (C.c_int, [_vp, _d, _d]),
+    "vd_cell_measure": (C.c_int, [_vp, _d, _d, _i32p, _vp, _vp]),
+    "vd_cell_get": (C.c_int, [_vp, _i32p, _i32p, _i32p, _vp, _vp, _vp, _vp]),
     "vd_calculate_noalloc": (C.c_int, [_d, _d, C.c_int, C.c_int, C.c_int, _vp, C.c_size_t, _vp, _vp, _vp,
                                        _vp]),
 }

@@ -29,6 +29,7 @@ SOURCES = [
     ("vd_noalloc.cu", False),
     ("vd_batch.cu", False),
     ("vd_server.cu", False),
+    ("vd_cell.cu", False),
 ]
 
 
@@ -55,15 +56,21 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if not force and up_to_date():
         return LIB
     os.makedirs(BUILD_DIR, exist_ok=True)
-    objs = []
+    objs, procs = [], []
+    # translation units compile in parallel; any failure fails the build
     for src, fma in SOURCES:
         obj = os.path.join(BUILD_DIR, src.replace(".cu", ".o"))
+        if os.path.exists(obj):
+            os.unlink(obj)
         cmd = [nvcc(), *ARCH, *COMMON, "-fmad=" + ("true" if fma else "false"),
                "-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:
             print(" ".join(cmd), flush=True)
-        subprocess.run(cmd, check=True)
+        procs.append((src, subprocess.Popen(cmd)))
         objs.append(obj)
+    failed = [src for src, p in procs if p.wait() != 0]
+    if failed:
+        raise RuntimeError("nvcc failed on " + ", ".join(failed))
     tmp = LIB + ".tmp"
     cmd = [nvcc(), *ARCH, "-shared", "-o", tmp, *objs]
     subprocess.run(cmd, check=True)

@@ -100,39 +100,166 @@ def _vp(a: np.ndarray):
 
 
 class Cell3DFaces:
-    """One computed cell: the polytope in the reference layout plus the
-    measures the GPU computed for it (volume, centroid, per-face areas)."""
+    """Cell3DFaces (cell_3d_faces.rs:22-270), the reference's 3D cell type.
+
+    Two ways to get one:
+
+    * ``Tessellation.get_cell(i)``: the computed cell i of a tessellation,
+      with the volume, centroid and face areas the GPU computed for it;
+    * ``Cell3DFaces.new(id, bounds)``: the box cell (cell_3d_faces.rs:37-74),
+      held in device memory and clipped call by call like the reference's
+      (``clip`` = Cell::clip / clip_with_scratch, cell_3d_faces.rs:288-503).
+
+    A computed cell moves to the device on its first ``clip``.  Every clip and
+    every measure runs on the GPU (the tessellation kernels' warp routines);
+    the accessors return copies of the device polytope.
+    """
 
     def __init__(self, id: int, vertices, face_counts, face_indices, face_neighbors,
-                 volume: float, centroid, face_areas):
+                 volume: Optional[float] = None, centroid=None, face_areas=None):
         self._id = int(id)
+        self._h = None
+        self._L = None
+        self._set(vertices, face_counts, face_indices, face_neighbors, volume, centroid, face_areas)
+
+    def _set(self, vertices, face_counts, face_indices, face_neighbors, volume, centroid, face_areas):
         self._vertices = np.asarray(vertices, np.float64)
         self._face_counts = np.asarray(face_counts, np.uint32)
         self._face_indices = np.asarray(face_indices, np.uint32)
         self._face_neighbors = np.asarray(face_neighbors, np.int32)
-        self._volume = float(volume)
-        self._centroid = np.asarray(centroid, np.float64)
-        self._face_areas = np.asarray(face_areas, np.float64)
+        self._volume = None if volume is None else float(volume)
+        self._centroid = None if centroid is None else np.asarray(centroid, np.float64)
+        self._face_areas = None if face_areas is None else np.asarray(face_areas, np.float64)
+        self._stale = False
 
+    @classmethod
+    def new(cls, id: int, bounds: BoundingBox) -> "Cell3DFaces":
+        """Cell3DFaces::new(id, bounds): the box, on the device."""
+        L = load()
+        h = C.c_void_p()
+        lo = np.asarray(bounds.min, np.float64)
+        hi = np.asarray(bounds.max, np.float64)
+        rc = L.vd_cell_create_box(int(id), _dp(lo), _dp(hi), C.byref(h))
+        cls._cell_check(L, rc, None)
+        c = cls.__new__(cls)
+        c._id = int(id)
+        c._set([], [], [], [], None, None, None)
+        c._L = L
+        c._h = h
+        c._stale = True
+        return c
+
+    @staticmethod
+    def _cell_check(L, rc, h):
+        if rc != 0:
+            from ._lib import VoronoidError
+            msg = L.vd_cell_last_error(h)
+            raise VoronoidError(rc, msg.decode() if msg else "")
+
+    def _device(self):
+        """The device handle, uploading this cell's polytope on first use."""
+        if self._h is not None:
+            return self._h
+        L = load()
+        h = C.c_void_p()
+        v = np.ascontiguousarray(self._vertices, np.float64)
+        fc = np.ascontiguousarray(self._face_counts, np.uint32)
+        fi = np.ascontiguousarray(self._face_indices, np.uint32)
+        fn = np.ascontiguousarray(self._face_neighbors, np.int32)
+        rc = L.vd_cell_create(self._id, v.size // 3, fc.size, _vp(v), _vp(fc), _vp(fi), _vp(fn), C.byref(h))
+        self._cell_check(L, rc, None)
+        self._L, self._h = L, h
+        return h
+
+    def _sync(self):
+        """Refresh the host copies from the device after a clip."""
+        if not self._stale:
+            return
+        L, h = self._L, self._h
+        nv, nf, nh = C.c_int32(), C.c_int32(), C.c_int32()
+        self._cell_check(L, L.vd_cell_get(h, C.byref(nv), C.byref(nf), C.byref(nh), None, None, None, None), h)
+        v = np.zeros(3 * max(nv.value, 1), np.float64)
+        fc = np.zeros(max(nf.value, 1), np.uint32)
+        fi = np.zeros(max(nh.value, 1), np.uint32)
+        fn = np.zeros(max(nf.value, 1), np.int32)
+        self._cell_check(L, L.vd_cell_get(h, C.byref(nv), C.byref(nf), C.byref(nh), _vp(v), _vp(fc), _vp(fi),
+                                          _vp(fn)), h)
+        vol = C.c_double()
+        cen = np.zeros(3, np.float64)
+        nfo = C.c_int32()
+        ar = np.zeros(max(nf.value, 1), np.float64)
+        self._cell_check(L, L.vd_cell_measure(h, C.byref(vol), _dp(cen), C.byref(nfo), _vp(ar), None), h)
+        self._set(v[:3 * nv.value], fc[:nf.value], fi[:nh.value], fn[:nf.value], vol.value, cen, ar[:nf.value])
+
+    def close(self):
+        if self._h is not None:
+            self._L.vd_cell_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- Cell trait (cell/mod.rs:8-43) ---------------------------------
+    def clip(self, point: Sequence[float], normal: Sequence[float], neighbor_id: int,
+             generator: Optional[Sequence[float]] = None):
+        """Clip by the plane through `point` with `normal` (the kept side is
+        (v - point).normal <= 1e-9); returns (modified, new max radius^2 from
+        `generator`, 0 without one), like Cell::clip."""
+        h = self._device()
+        self._sync()
+        p = np.asarray(point, np.float64)
+        n = np.asarray(normal, np.float64)
+        g = None if generator is None else np.asarray(generator, np.float64)
+        mod = C.c_int()
+        r2 = C.c_double()
+        self._cell_check(self._L, self._L.vd_cell_clip(h, _dp(p), _dp(n), int(neighbor_id),
+                                                       None if g is None else _dp(g), C.byref(mod),
+                                                       C.byref(r2)), h)
+        self._stale = True
+        return bool(mod.value), r2.value
+
+    def max_radius_sq(self, center: Sequence[float]) -> float:
+        h = self._device()
+        c = np.asarray(center, np.float64)
+        out = C.c_double()
+        self._cell_check(self._L, self._L.vd_cell_max_radius_sq(h, _dp(c), C.byref(out)), h)
+        return out.value
+
+    def _measured(self):
+        if self._volume is None:
+            self._device()
+            self._stale = True
+        self._sync()
+
+    # ---- accessors (cell_3d_faces.rs:76-104, 255-269) -------------------
     def id(self) -> int:
         return self._id
 
     def vertices(self) -> np.ndarray:
+        self._sync()
         return self._vertices.copy()
 
     def face_counts(self) -> np.ndarray:
+        self._sync()
         return self._face_counts.copy()
 
     def face_indices(self) -> np.ndarray:
+        self._sync()
         return self._face_indices.copy()
 
     def face_neighbors(self) -> np.ndarray:
+        self._sync()
         return self._face_neighbors.copy()
 
     def neighbors(self) -> np.ndarray:
+        self._sync()
         return self._face_neighbors
 
     def faces(self) -> List[List[int]]:
+        self._sync()
         out, off = [], 0
         for c in self._face_counts:
             out.append([int(v) for v in self._face_indices[off:off + c]])
@@ -140,15 +267,33 @@ class Cell3DFaces:
         return out
 
     def is_empty(self) -> bool:
+        self._sync()
         return self._vertices.size == 0
 
+    def shared_vertices(self, neighbor_a: int, neighbor_b: int) -> np.ndarray:
+        """Cell::shared_vertices (cell_3d_faces.rs:537-565): the vertices on
+        both the face(s) of neighbour a and those of neighbour b, flat xyz."""
+        self._sync()
+        a, b = [], []
+        for f, face in enumerate(self.faces()):
+            nb = int(self._face_neighbors[f])
+            for lst, want in ((a, neighbor_a), (b, neighbor_b)):
+                if nb == want:
+                    lst.extend(v for v in face if v not in lst)
+        keep = [v for v in a if v in b]
+        return self._vertices.reshape(-1, 3)[keep].reshape(-1).copy()
+
+    # ---- measures (cell_3d_faces.rs:106-254) ----------------------------
     def volume(self) -> float:
+        self._measured()
         return self._volume
 
     def centroid(self) -> np.ndarray:
+        self._measured()
         return self._centroid.copy()
 
     def face_area(self, face_index: int) -> float:
+        self._measured()
         if face_index >= self._face_areas.size:
             return 0.0
         return float(self._face_areas[face_index])
