@@ -227,6 +227,38 @@ def e2e_leg(args, L, _lib, tess, pts):
     return e2e, h2d, d2h
 
 
+def autotuned_leg(args, v, d_pts, flush):
+    """The same generators on the grid the autotuner picks for them (a
+    different bin grid, so a different but equally exact tessellation: each
+    grid's results equal the oracle's on that grid); device-timed like
+    `value`, L2 flushed before each step."""
+    import torch
+    from vorothree_b200 import autotune
+    pts = d_pts.cpu().numpy()
+    bounds = v.BoundingBox([0, 0, 0], [1, 1, 1])
+    g = autotune.choose_grid(pts, bounds)
+    t = v.Tessellation(bounds, v.Algorithm3DGrid(*g))
+    t.set_precision(args.precision)
+    stream = torch.cuda.ExternalStream(t.stream(), device=d_pts.device)
+    times = []
+    for it in range(args.warmup + args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        t.set_generators_device(d_pts.data_ptr(), N_GEN)
+        t.calculate()
+        e1.record(stream)
+        e1.synchronize()
+        if it >= args.warmup:
+            times.append(e0.elapsed_time(e1))
+    t.close()
+    ms = statistics.mean(times)
+    return {"grid": list(g), "value": N_GEN / (ms / 1e3), "ms_per_step": ms,
+            "note": "same step on the autotuner's grid for this input"}
+
+
 def run_ours(args):
     import torch
     ws, rank, local = dist_env()
@@ -348,6 +380,8 @@ def run_ours(args):
             "clocks": clk,
             "fallback_cells": fb,
         }
+        if ws == 1 and not args.no_autotuned:
+            line["autotuned_grid"] = autotuned_leg(args, v, d_pts, flush)
         if other is not None:
             alt, osm, ocm = other
             oms = statistics.mean(osm)
@@ -591,6 +625,7 @@ def main():
     ap.add_argument("--serve-rates", type=float, nargs="+", default=[10.0, 30.0, 60.0])
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--no-autotuned", action="store_true", help="skip the autotuned-grid leg (uniform workload)")
     ap.add_argument("--lloyd-steps", type=int, default=20)
     ap.add_argument("--blob-grids", type=int, nargs="*", default=[],
                     help="cubic grids timed beside the autotuned one (blobs workload)")
