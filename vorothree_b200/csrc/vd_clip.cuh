@@ -93,6 +93,8 @@ struct alignas(16) WarpPoly {
   typename C::FId pf[2][C::HCAP];
   typename C::VId fe[C::HCAP];    // per clip: end vertex of each position's edge
   typename C::CId cidx[C::HCAP];  // per clip: crossing index of a crossing position
+  typename C::CId fcr[C::FCAP];   // per clip: index of each face's first crossing
+  uint8_t cand_e[32];             // walk: search-order entry (lane) of each candidate of a round
   typename C::FId fnew[C::FCAP];
   typename C::VId o2n[C::VCAP];
   typename C::VId lidmap[C::VCAP];
@@ -193,13 +195,6 @@ __device__ double poly_max_radius_sq(const WarpPoly<C>& P, const PolyState& S, d
   return warp_max(m);
 }
 
-// position after p in its face loop (the (i + 1) % count of :380)
-template <class C>
-__device__ __forceinline__ int next_pos(const WarpPoly<C>& P, int cb, int p) {
-  const int f = P.pf[cb][p];
-  return (p + 1 == P.fs[cb][f + 1]) ? P.fs[cb][f] : p + 1;
-}
-
 // clip_with_scratch (cell_3d_faces.rs:288-503).  All lanes call it with the
 // same (uniform) arguments.  *r2 gets the max squared distance of the new
 // vertex set from (gx,gy,gz) when with_gen, else 0.
@@ -297,17 +292,24 @@ __device__ int warp_clip(WarpPoly<C>& P, PolyState& S, double px, double py, dou
   //    edge's end vertex, the crossing positions in walk order, and the
   //    exclusive prefix E of the entries each position emits into the new
   //    faces: in->in 1 (end), in->out 1 (X), out->in 2 (X, end), out->out 0.
+  //    A crossing is its face's first when no earlier crossing lies at or
+  //    after the face's first position; step 7 finds a segment's partner
+  //    through it.
   int ncross = 0;
   {
     int run = 0;
+    int lastcross = -1;  // position of the last crossing of earlier chunks
     for (int b = 0; b < nh; b += 32) {
       const int p = b + lane;
       bool cr = false;
-      int em = 0;
+      int em = 0, f = 0, f0 = 0;
       unsigned s = 0, e = 0;
       if (p < nh) {
+        f = P.pf[cb][p];
+        f0 = P.fs[cb][f];
         s = P.fi[cb][p];
-        e = P.fi[cb][next_pos(P, cb, p)];
+        // the edge's end: the next entry of the face loop ((i + 1) % count, :380)
+        e = P.fi[cb][(p + 1 == P.fs[cb][f + 1]) ? f0 : p + 1];
         const bool si = P.o2n[s] != C::VNONE, ei = P.o2n[e] != C::VNONE;
         P.fe[p] = (VId)e;
         cr = si != ei;
@@ -316,12 +318,16 @@ __device__ int warp_clip(WarpPoly<C>& P, PolyState& S, double px, double py, dou
       const unsigned m = __ballot_sync(kFull, cr);
       if (cr) {
         const int k = ncross + __popc(m & lt);
+        const unsigned before = m & lt;
+        const int prevp = before ? b + 31 - __clz(before) : lastcross;
         if (k < C::CCAP) {
           P.cpos[k] = (uint16_t)p;
           P.ckey[k] = (typename C::Key)(s < e ? (s << C::KSHIFT | e) : (e << C::KSHIFT | s));
           P.cidx[p] = (typename C::CId)k;
+          if (prevp < f0) P.fcr[f] = (typename C::CId)k;
         }
       }
+      if (m) lastcross = b + 31 - __clz(m);
       ncross += __popc(m);
       const int inc = warp_incl_scan(em);
       if (p < nh) P.E[p] = (uint16_t)(run + inc - em);
@@ -509,17 +515,16 @@ __device__ int warp_clip(WarpPoly<C>& P, PolyState& S, double px, double py, dou
     if (segsrc) {
       const int k = nseg + __popc(sm & lt);
       if (k < C::SCAP) {
-        // forward along the face to the out->in position (one exists in a
-        // kept face: its walk must re-enter the inside)
+        // the out->in position that closes this in->out one is the next
+        // crossing along the face (the positions between are out->out):
+        // the next crossing in walk order if it lies in the same face, else
+        // the face's first crossing
         const int f = P.pf[cb][p];
-        const int len = (int)P.fs[cb][f + 1] - (int)P.fs[cb][f];
-        int q = next_pos(P, cb, p);
-        for (int g2 = 0; g2 < len; ++g2) {
-          if (P.o2n[P.fe[q]] != C::VNONE) break;
-          q = next_pos(P, cb, q);
-        }
-        P.sega[k] = P.cid[P.cidx[q]];
-        P.segb[k] = P.cid[P.cidx[p]];
+        const int kc = P.cidx[p];
+        int kn = kc + 1;
+        if (kn >= ncross || (int)P.cpos[kn] >= (int)P.fs[cb][f + 1]) kn = P.fcr[f];
+        P.sega[k] = P.cid[kn];
+        P.segb[k] = P.cid[kc];
       }
     }
     nseg += __popc(sm);
@@ -625,45 +630,34 @@ __device__ __forceinline__ bool wall_plane(const Wall& w, double gx, double gy, 
 // one per lane (lanes in `mask`, ascending id order): members with
 // dist^2 <= 4R^2 are clipped in order, the ballot re-evaluated after every
 // clip that changes R.
+// instrumented runs: the candidates of the bins the walk opens when it
+// reaches entries (elo, ehi] of this chunk at radius^2 c4/4 -- every member
+// but the cell's own generator (algo_3d_grid.rs:190-196)
 template <class C>
-__device__ __forceinline__ int visit_members(WarpPoly<C>& P, PolyState& S, const SortedGen& sg, unsigned mask,
-                                             uint32_t i, double gx, double gy, double gz, double& cur) {
-  const unsigned lane = lane_id();
-  const bool cand = ((mask >> lane) & 1u) && sg.id != (long long)i;
-  const double d0 = sg.x - gx, d1 = sg.y - gy, d2 = sg.z - gz;
-  const double dist_sq = d0 * d0 + d1 * d1 + d2 * d2;
-  if constexpr (C::COUNT) cnt_add(P, kCntCandidates, (unsigned long long)__popc(__ballot_sync(kFull, cand)));
-  double r2;
-  int mpos = 0;
-  while (mpos < 32) {
-    const unsigned mge = ~((1u << mpos) - 1u);
-    const unsigned mpass = __ballot_sync(kFull, cand && !(dist_sq > 4.0 * cur)) & mge;
-    if (!mpass) break;
-    const int j = __ffs(mpass) - 1;
-    const int jid = (int)__shfl_sync(kFull, sg.id, j);
-    const double e0 = __shfl_sync(kFull, d0, j);
-    const double e1 = __shfl_sync(kFull, d1, j);
-    const double e2 = __shfl_sync(kFull, d2, j);
-    const double mx = gx + e0 * 0.5, my = gy + e1 * 0.5, mz = gz + e2 * 0.5;
-    const int r = warp_clip(P, S, mx, my, mz, e0, e1, e2, jid, true, gx, gy, gz, &r2);
-    if (r == kClipOverflow) return kCellOverflow;
-    if (r == kClipMod) cur = r2;
-    else if (r == kClipEmpty) cur = 0.0;
-    mpos = j + 1;
-  }
-  return kCellOk;
+__device__ __forceinline__ void count_opened(WarpPoly<C>& P, int elo, int ehi, bool valid, bool inr, bool own,
+                                             double md2, double b2, uint32_t members, double c4) {
+  const int l = (int)lane_id();
+  const bool open = l > elo && l <= ehi && valid && inr && !(md2 > c4) && b2 <= c4;
+  int c = open ? (int)members - (own ? 1 : 0) : 0;
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(kFull, c, o);
+  cnt_add(P, kCntCandidates, (unsigned long long)c);
 }
 
 // compute_cell (tessellation.rs:414-475) with Algorithm3DGrid::visit_neighbors
 // (algo_3d_grid.rs:145-202) and the bisector visitor (tessellation.rs:446-471).
 //
-// The search order is consumed 32 entries at a time: each lane decodes one
-// entry (bin, exact bin lower bound, member range).  Ballots against the
-// CURRENT radius then pick, in order, exactly the entries the reference
-// visits: the first entry with min_d2 > 4R^2 ends the walk, and only bins
-// whose bound is <= 4R^2 are opened -- re-evaluated after every clip that
-// changes R.  Members of an opened bin are loaded by the lanes together and
-// visited in ascending id order.
+// The search order is consumed 32 entries at a time, one entry per lane
+// (bin, exact bin lower bound, member range).  The members of the bins that
+// can still open are flattened into one candidate list, 32 candidates per
+// round, one per lane, loaded together.  Ballots against the CURRENT radius
+// then pick, in order, exactly the candidates the reference clips with:
+//  - the walk ends at the first entry past the bin being processed whose
+//    min_d2 > 4R^2 (min_d2 ascends along the order; R only shrinks);
+//  - a bin opens when its lower bound is <= 4R^2 at the moment the walk
+//    reaches it -- for every bin past the last clipped candidate's, that is
+//    the current R; the bin being processed already opened;
+//  - a member is clipped with when dist^2 <= 4R^2 at its turn.
+// Each clip may shrink R, and the ballots are re-evaluated after it.
 template <class C>
 __device__ int compute_cell(const TessDesc& T, uint32_t i, WarpPoly<C>& P, PolyState& S) {
   const unsigned lane = lane_id();
@@ -694,14 +688,16 @@ __device__ int compute_cell(const TessDesc& T, uint32_t i, WarpPoly<C>& P, PolyS
 
   bool done = false;
   for (int base = 0; base < T.norder && !done; base += 32) {
+    // ---- this lane's search-order entry ----
     const int k = base + (int)lane;
     const bool valid = k < T.norder;
     double md2 = 0.0, b2 = 0.0;
-    bool inr = false;
+    bool inr = false, own = false;
     uint32_t bs = 0, be = 0;
     if (valid) {
       const Offset o = T.order[k];
       md2 = o.min_d2;
+      own = o.dx == 0 && o.dy == 0 && o.dz == 0;
       const int bx = ix + o.dx, by = iy + o.dy, bz = iz + o.dz;
       inr = bx >= 0 && bx < G.n[0] && by >= 0 && by < G.n[1] && bz >= 0 && bz < G.n[2];
       if (inr) {
@@ -719,40 +715,67 @@ __device__ int compute_cell(const TessDesc& T, uint32_t i, WarpPoly<C>& P, PolyS
       }
     }
     const int nvalid = min(32, T.norder - base);
-    int pos = 0;
-    while (true) {
-      const double c4 = 4.0 * cur;
-      const unsigned ge = pos >= 32 ? 0u : ~((1u << pos) - 1u);
-      const unsigned brk = __ballot_sync(kFull, valid && md2 > c4) & ge;
-      unsigned pass = __ballot_sync(kFull, valid && inr && !(md2 > c4) && b2 <= c4 && be > bs) & ge;
-      if (brk) {
-        const int fb = __ffs(brk) - 1;
-        pass &= (1u << fb) - 1u;
-        if (!pass) {
-          cnt_add(P, kCntOffsets, (unsigned long long)(fb + 1));
-          done = true;
-          break;
-        }
+    // bins that can still open (R only shrinks), flattened: members of entry
+    // e are candidates [start, start + cnt)
+    const bool pot = valid && inr && be > bs && !(md2 > 4.0 * cur) && b2 <= 4.0 * cur;
+    const int cnt = pot ? (int)(be - bs) : 0;
+    const int incl = warp_incl_scan(cnt);
+    const int start = incl - cnt;
+    const int total = __shfl_sync(kFull, incl, 31);
+    int ecur = -1;  // entry of the bin being processed (opened)
+    int pos = 0;    // next candidate to consider
+    int fb = 32;    // entry that ends the walk (32: none in this chunk)
+    for (int r0 = 0;; r0 += 32) {
+      if (r0 < total) {
+        const int lo = max(start, r0), hi = min(start + cnt, r0 + 32);
+        for (int q = lo; q < hi; ++q) P.cand_e[q - r0] = (uint8_t)lane;
       }
-      if (!pass) {
-        cnt_add(P, kCntOffsets, (unsigned long long)nvalid);
-        break;
+      __syncwarp();
+      const int idx = r0 + (int)lane;
+      const bool have = idx < total;
+      const int ce = have ? (int)P.cand_e[lane] : 0;
+      __syncwarp();
+      const uint32_t cbs = __shfl_sync(kFull, bs, ce);
+      const int cst = __shfl_sync(kFull, start, ce);
+      const double cb2 = __shfl_sync(kFull, b2, ce);
+      SortedGen sg = {0.0, 0.0, 0.0, -1};
+      if (have) sg = T.sorted[cbs + (uint32_t)(idx - cst)];
+      const bool cand = have && sg.id != (long long)i;
+      const double d0 = sg.x - gx, d1 = sg.y - gy, d2 = sg.z - gz;
+      const double dist_sq = d0 * d0 + d1 * d1 + d2 * d2;
+      while (true) {
+        const double c4 = 4.0 * cur;
+        const unsigned later = ecur < 0 ? kFull : (ecur >= 31 ? 0u : ~((2u << ecur) - 1u));
+        const unsigned brk = __ballot_sync(kFull, valid && md2 > c4) & later;
+        fb = brk ? __ffs(brk) - 1 : 32;
+        const bool ok = cand && idx >= pos && ce < fb && !(dist_sq > c4) && (ce == ecur || cb2 <= c4);
+        const unsigned pass = __ballot_sync(kFull, ok);
+        if (!pass) break;
+        const int j = __ffs(pass) - 1;
+        const int ej = __shfl_sync(kFull, ce, j);
+        if constexpr (C::COUNT) count_opened(P, ecur, ej, valid, inr, own, md2, b2, be - bs, c4);
+        const int jid = (int)__shfl_sync(kFull, sg.id, j);
+        const double e0 = __shfl_sync(kFull, d0, j);
+        const double e1 = __shfl_sync(kFull, d1, j);
+        const double e2 = __shfl_sync(kFull, d2, j);
+        const double mx = gx + e0 * 0.5, my = gy + e1 * 0.5, mz = gz + e2 * 0.5;
+        const int r = warp_clip(P, S, mx, my, mz, e0, e1, e2, jid, true, gx, gy, gz, &r2);
+        if (r == kClipOverflow) return kCellOverflow;
+        if (r == kClipMod) cur = r2;
+        else if (r == kClipEmpty) cur = 0.0;
+        ecur = ej;
+        pos = r0 + j + 1;
       }
-      const int l = __ffs(pass) - 1;
-      const uint32_t s0 = __shfl_sync(kFull, bs, l);
-      const uint32_t s1 = __shfl_sync(kFull, be, l);
-      for (uint32_t mb = s0; mb < s1; mb += 32) {
-        SortedGen sg = {0.0, 0.0, 0.0, -1};
-        if (mb + lane < s1) sg = T.sorted[mb + lane];
-        const unsigned rmask = s1 - mb >= 32 ? kFull : ((1u << (s1 - mb)) - 1u);
-        if (visit_members<C>(P, S, sg, rmask, i, gx, gy, gz, cur) != kCellOk) return kCellOverflow;
-      }
-      pos = l + 1;
-      if (pos >= 32) {
-        cnt_add(P, kCntOffsets, (unsigned long long)nvalid);
-        break;
-      }
+      if (r0 + 32 >= total) break;
+      // the next round starts at an entry the walk no longer reaches
+      const unsigned nxt = __ballot_sync(kFull, cnt > 0 && start <= r0 + 32);
+      if (fb < 32 && 31 - __clz(nxt) >= fb) break;
     }
+    if constexpr (C::COUNT) {
+      count_opened(P, ecur, fb < 32 ? fb - 1 : 31, valid, inr, own, md2, b2, be - bs, 4.0 * cur);
+      cnt_add(P, kCntOffsets, (unsigned long long)(fb < 32 ? fb + 1 : nvalid));
+    }
+    if (fb < 32) done = true;
   }
   if (!done && !T.order_complete && !(T.order_bound > 4.0 * cur)) return kCellTable;
   return kCellOk;
