@@ -71,6 +71,12 @@ using MedCfg = PolyCfg<224, 112, 672, 128, 64, 64, uint8_t, uint8_t, uint16_t, u
 // reference's face_indices (cell_3d_faces.rs:31).
 using BigCfg = PolyCfg<2048, 512, 6144, 1024, 512, 512, uint16_t, uint16_t, uint32_t, uint16_t, true, false>;
 
+// the new ids of the two ends of one face position's edge
+template <typename V>
+struct alignas(2 * sizeof(V)) VPair {
+  V s, e;
+};
+
 template <class C>
 struct alignas(16) WarpPoly {
   double vx[C::VCAP], vy[C::VCAP], vz[C::VCAP];
@@ -94,6 +100,8 @@ struct alignas(16) WarpPoly {
   typename C::VId fe[C::HCAP];    // per clip: end vertex of each position's edge
   typename C::CId cidx[C::HCAP];  // per clip: crossing index of a crossing position
   typename C::CId fcr[C::FCAP];   // per clip: index of each face's first crossing
+  VPair<typename C::VId> pve[C::HCAP];  // per clip: new ids of each position's edge ends (or none)
+  int16_t fdel[C::FCAP];          // per clip: new entry offset of a face minus its first position's E
   uint8_t cand_e[32];             // walk: search-order entry (lane) of each candidate of a round
   typename C::FId fnew[C::FCAP];
   typename C::VId o2n[C::VCAP];
@@ -301,8 +309,8 @@ __device__ int warp_clip(WarpPoly<C>& P, PolyState& S, double px, double py, dou
     int lastcross = -1;  // position of the last crossing of earlier chunks
     for (int b = 0; b < nh; b += 32) {
       const int p = b + lane;
-      bool cr = false;
-      int em = 0, f = 0, f0 = 0;
+      bool cr = false, si = false, ei = false;
+      int f = 0, f0 = 0;
       unsigned s = 0, e = 0;
       if (p < nh) {
         f = P.pf[cb][p];
@@ -310,10 +318,12 @@ __device__ int warp_clip(WarpPoly<C>& P, PolyState& S, double px, double py, dou
         s = P.fi[cb][p];
         // the edge's end: the next entry of the face loop ((i + 1) % count, :380)
         e = P.fi[cb][(p + 1 == P.fs[cb][f + 1]) ? f0 : p + 1];
-        const bool si = P.o2n[s] != C::VNONE, ei = P.o2n[e] != C::VNONE;
+        const VId os = P.o2n[s], oe = P.o2n[e];
+        si = os != C::VNONE;
+        ei = oe != C::VNONE;
         P.fe[p] = (VId)e;
+        P.pve[p] = VPair<VId>{os, oe};
         cr = si != ei;
-        em = si ? 1 : (ei ? 2 : 0);
       }
       const unsigned m = __ballot_sync(kFull, cr);
       if (cr) {
@@ -329,9 +339,12 @@ __device__ int warp_clip(WarpPoly<C>& P, PolyState& S, double px, double py, dou
       }
       if (m) lastcross = b + 31 - __clz(m);
       ncross += __popc(m);
-      const int inc = warp_incl_scan(em);
-      if (p < nh) P.E[p] = (uint16_t)(run + inc - em);
-      run += __shfl_sync(kFull, inc, 31);
+      // emit counts are 1 (start inside) or 2 (out->in): the prefix is two
+      // ballot populations
+      const unsigned m1 = __ballot_sync(kFull, si);
+      const unsigned m2 = __ballot_sync(kFull, !si && ei);
+      if (p < nh) P.E[p] = (uint16_t)(run + __popc(m1 & lt) + 2 * __popc(m2 & lt));
+      run += __popc(m1) + 2 * __popc(m2);
     }
     if (lane == 0) P.E[nh] = (uint16_t)run;
   }
@@ -476,6 +489,7 @@ __device__ int warp_clip(WarpPoly<C>& P, PolyState& S, double px, double py, dou
     if (f < nf) {
       P.fnew[f] = kept ? (FId)(nfk + __popc(km & lt)) : (FId)C::FNONE;
       P.fns[f] = (uint16_t)(hk + inc - Lk);
+      P.fdel[f] = (int16_t)(hk + inc - Lk - (int)P.E[P.fs[cb][f]]);
     }
     nfk += __popc(km);
     hk += __shfl_sync(kFull, inc, 31);
@@ -494,11 +508,12 @@ __device__ int warp_clip(WarpPoly<C>& P, PolyState& S, double px, double py, dou
     bool segsrc = false;
     if (p < nh) {
       const int f = P.pf[cb][p];
-      const unsigned os = P.o2n[P.fi[cb][p]], oe = P.o2n[P.fe[p]];
+      const VPair<VId> ve = P.pve[p];
+      const unsigned os = ve.s, oe = ve.e;
       const bool si = os != C::VNONE, ei = oe != C::VNONE;
       const unsigned fw = P.fnew[f];
       if (fw != C::FNONE) {
-        const int o = P.fns[f] + ((int)P.E[p] - (int)P.E[P.fs[cb][f]]);
+        const int o = (int)P.fdel[f] + (int)P.E[p];
         if (si) {
           P.fi[nb][o] = (VId)(ei ? oe : (unsigned)P.cid[P.cidx[p]]);
           P.pf[nb][o] = (FId)fw;
@@ -546,6 +561,51 @@ __device__ int warp_clip(WarpPoly<C>& P, PolyState& S, double px, double py, dou
     __syncwarp();
     for (int v = nkept + lane; v < nvn; v += 32) P.lidmap[v] = (VId)C::VNONE;
     __syncwarp();
+    int len = 0, ovf = 0;
+    // Common case: at most 32 segments, their starts distinct, their ends
+    // distinct, every end the start of a segment.  The lid map is then a
+    // permutation of the segments, and the chain from segment 0 (which the
+    // serial walk below follows) is ranked by pointer jumping: the cycle is
+    // cut before segment 0 and each segment's distance to the cut gives its
+    // place in the lid face.
+    bool fastlid = false;
+    if (nseg <= 32) {
+      const bool act = (int)lane < nseg;
+      const unsigned a = act ? (unsigned)P.sega[lane] : (0xFFFF0000u | lane);
+      const unsigned bend = act ? (unsigned)P.segb[lane] : (0xFFFE0000u | lane);
+      const unsigned ma = __match_any_sync(kFull, a);
+      const unsigned mb = __match_any_sync(kFull, bend);
+      if (act) P.lidmap[a] = (VId)lane;
+      __syncwarp();
+      unsigned succ = lane;
+      bool good = true;
+      if (act) {
+        succ = P.lidmap[bend];
+        good = __popc(ma) == 1 && __popc(mb) == 1 && succ < (unsigned)nseg;
+      }
+      __syncwarp();
+      if (__all_sync(kFull, good)) {
+        fastlid = true;
+        const int term = __ffs(__ballot_sync(kFull, act && succ == 0u)) - 1;
+        int nxt = (act && (int)lane != term) ? (int)succ : (int)lane;
+        int d = nxt != (int)lane ? 1 : 0;
+        for (int span = 1; span < nseg; span <<= 1) {
+          const int dn = __shfl_sync(kFull, d, nxt);
+          const int nn = __shfl_sync(kFull, nxt, nxt);
+          d += dn;
+          nxt = nn;
+        }
+        const int d0 = __shfl_sync(kFull, d, 0);
+        len = d0 + 1;
+        if (hk + len > C::HCAP) ovf = 1;
+        else if (act && nxt == term) P.fi[nb][hk + d0 - d] = (VId)a;
+      } else {
+        // restore the lid map's empty entries for the serial walk
+        if (act) P.lidmap[a] = (VId)C::VNONE;
+        __syncwarp();
+      }
+    }
+    if (!fastlid) {
     for (int b = 0; b < nseg; b += 32) {
       const int k = b + lane;
       const bool act = k < nseg;
@@ -555,7 +615,6 @@ __device__ int warp_clip(WarpPoly<C>& P, PolyState& S, double px, double py, dou
       if (act && last == (int)lane) P.lidmap[key] = P.segb[k];
       __syncwarp();
     }
-    int len = 0, ovf = 0;
     if (lane == 0) {
       const unsigned start = P.sega[0];
       unsigned cur = P.segb[0];
@@ -578,6 +637,7 @@ __device__ int warp_clip(WarpPoly<C>& P, PolyState& S, double px, double py, dou
     }
     len = __shfl_sync(kFull, len, 0);
     ovf = __shfl_sync(kFull, ovf, 0);
+    }
     if (ovf) return kClipOverflow;
     if (len >= 3) {
       if (nfk + 1 > C::FCAP || len > 255) return kClipOverflow;

@@ -17,6 +17,8 @@
 #include <cstdio>
 #include <cstring>
 #include <limits>
+#include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -36,23 +38,63 @@ constexpr int kCompleteOrderMax = 1 << 15;
 // kernels this library has launched in this process (all handles)
 std::atomic<unsigned long long> g_launches{0};
 
+// The library's memory pool on each device: stream-ordered allocations that
+// stay reserved for the process once freed (release threshold = max), so a
+// buffer that grows reuses memory without going back to the driver.
+cudaError_t lib_pool(cudaMemPool_t* out) {
+  static std::mutex mu;
+  static std::map<int, cudaMemPool_t> pools;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = pools.find(dev);
+  if (it != pools.end()) {
+    *out = it->second;
+    return cudaSuccess;
+  }
+  cudaMemPoolProps props;
+  memset(&props, 0, sizeof(props));
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = dev;
+  cudaMemPool_t pool;
+  e = cudaMemPoolCreate(&pool, &props);
+  if (e != cudaSuccess) return e;
+  uint64_t keep = ~0ull;
+  e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  if (e != cudaSuccess) return e;
+  pools[dev] = pool;
+  *out = pool;
+  return cudaSuccess;
+}
+
+// A device buffer that only grows.  Allocation is stream-ordered, on the
+// handle's stream from the library's pool: growing one handle's buffers
+// never synchronises the device (as cudaFree does), so handles serving
+// concurrent requests do not stall each other.
 template <typename T>
 struct DevBuf {
   T* p = nullptr;
   size_t cap = 0;  // elements
-  cudaError_t ensure(size_t n) {
+  cudaStream_t s = nullptr;  // stream of the last allocation (frees are ordered on it)
+  cudaError_t ensure(size_t n, cudaStream_t stream) {
     if (n <= cap && p) return cudaSuccess;
-    if (p) cudaFree(p);
+    if (p) cudaFreeAsync(p, s);
     p = nullptr;
     cap = 0;
+    s = stream;
     const size_t want = std::max<size_t>(n, 1);
-    cudaError_t e = cudaMalloc(&p, want * sizeof(T));
+    cudaMemPool_t pool;
+    cudaError_t e = lib_pool(&pool);
+    if (e != cudaSuccess) return e;
+    e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&p), want * sizeof(T), pool, stream);
     if (e == cudaSuccess) cap = want;
     else p = nullptr;
     return e;
   }
   void release() {
-    if (p) cudaFree(p);
+    if (p) cudaFreeAsync(p, s);
     p = nullptr;
     cap = 0;
   }
@@ -71,6 +113,18 @@ enum : int {
 
 namespace vd {
 void set_thread_error(const char* msg) { g_create_error = msg; }
+
+cudaError_t reserve_pool(size_t bytes, cudaStream_t s) {
+  cudaMemPool_t pool;
+  cudaError_t e = lib_pool(&pool);
+  if (e != cudaSuccess || bytes == 0) return e;
+  void* p = nullptr;
+  e = cudaMallocFromPoolAsync(&p, bytes, pool, s);
+  if (e != cudaSuccess) return e;
+  e = cudaFreeAsync(p, s);
+  if (e != cudaSuccess) return e;
+  return cudaStreamSynchronize(s);
+}
 }  // namespace vd
 
 struct vd_tess {
@@ -170,7 +224,7 @@ int scan_excl(vd_tess* t, const Tin* in, T* out, size_t n, std::vector<DevBuf<T>
   if (n == 0) return VD_OK;
   const size_t nt = (n + kScanTile - 1) / kScanTile;
   if ((int)pool.size() <= level) pool.resize(level + 1);
-  VD_CK(t, pool[level].ensure(nt + 1));
+  VD_CK(t, pool[level].ensure(nt + 1, t->stream));
   T* sums = pool[level].p;
   k_scan_tiles<Tin, T><<<(unsigned)nt, kScanThreads, 0, t->stream>>>(in, out, n, sums);
   g_launches++;
@@ -178,7 +232,7 @@ int scan_excl(vd_tess* t, const Tin* in, T* out, size_t n, std::vector<DevBuf<T>
   if (nt > 1) {
     // scan the tile sums in place (needs its own level of scratch)
     if ((int)pool.size() <= level + 1) pool.resize(level + 2);
-    VD_CK(t, pool[level + 1].ensure(nt + 1));
+    VD_CK(t, pool[level + 1].ensure(nt + 1, t->stream));
     T* sscan = pool[level + 1].p;
     int r = scan_excl<T, T>(t, sums, sscan, nt, pool, level + 2);
     if (r != VD_OK) return r;
@@ -194,7 +248,7 @@ int upload_order(vd_tess* t, int k) {
   bool complete;
   double bound;
   build_order(t->grid, k, h, complete, bound);
-  VD_CK(t, t->d_order.ensure(h.size()));
+  VD_CK(t, t->d_order.ensure(h.size(), t->stream));
   VD_CK(t, cudaMemcpyAsync(t->d_order.p, h.data(), h.size() * sizeof(Offset), cudaMemcpyHostToDevice, t->stream));
   VD_CK(t, cudaStreamSynchronize(t->stream));
   t->order_k = k;
@@ -217,15 +271,15 @@ WallSet wallset(const vd_tess* t) {
 int rebin(vd_tess* t) {
   const size_t n = t->ngen, nb = t->nbins;
   cudaStream_t s = t->stream;
-  VD_CK(t, t->d_bin_of.ensure(n));
-  VD_CK(t, t->d_bin_count.ensure(nb + 1));
-  VD_CK(t, t->d_bin_start.ensure(nb + 1));
-  VD_CK(t, t->d_cursor.ensure(nb + 1));
-  VD_CK(t, t->d_ids.ensure(n));
-  VD_CK(t, t->d_ids_tmp.ensure(n));
-  VD_CK(t, t->d_big_list.ensure(nb));
-  VD_CK(t, t->d_sorted.ensure(n));
-  VD_CK(t, t->d_ctl.ensure(kCtlWords));
+  VD_CK(t, t->d_bin_of.ensure(n, t->stream));
+  VD_CK(t, t->d_bin_count.ensure(nb + 1, t->stream));
+  VD_CK(t, t->d_bin_start.ensure(nb + 1, t->stream));
+  VD_CK(t, t->d_cursor.ensure(nb + 1, t->stream));
+  VD_CK(t, t->d_ids.ensure(n, t->stream));
+  VD_CK(t, t->d_ids_tmp.ensure(n, t->stream));
+  VD_CK(t, t->d_big_list.ensure(nb, t->stream));
+  VD_CK(t, t->d_sorted.ensure(n, t->stream));
+  VD_CK(t, t->d_ctl.ensure(kCtlWords, t->stream));
   VD_CK(t, cudaMemsetAsync(t->d_bin_count.p, 0, (nb + 1) * sizeof(uint32_t), s));
   VD_CK(t, cudaMemsetAsync(t->d_ctl.p + kCtlBigCount, 0, sizeof(unsigned int), s));
   if (n > 0) {
@@ -261,16 +315,16 @@ int rebin(vd_tess* t) {
 int filter_into_gen(vd_tess* t, const double* d_src, size_t n, size_t* n_kept) {
   cudaStream_t s = t->stream;
   if (t->walls.empty()) {
-    VD_CK(t, t->d_gen.ensure(3 * n));
+    VD_CK(t, t->d_gen.ensure(3 * n, t->stream));
     if (n && d_src != t->d_gen.p)
       VD_CK(t, cudaMemcpyAsync(t->d_gen.p, d_src, 3 * n * sizeof(double), cudaMemcpyDeviceToDevice, s));
     t->ngen = n;
     if (n_kept) *n_kept = n;
     return VD_OK;
   }
-  VD_CK(t, t->d_flags.ensure(n + 1));
-  VD_CK(t, t->d_pos.ensure(n + 1));
-  VD_CK(t, t->d_tmp3.ensure(3 * n));
+  VD_CK(t, t->d_flags.ensure(n + 1, t->stream));
+  VD_CK(t, t->d_pos.ensure(n + 1, t->stream));
+  VD_CK(t, t->d_tmp3.ensure(3 * n, t->stream));
   if (n) {
     k_wall_flags<<<grid_blocks(t, n, 256), 256, 0, s>>>(d_src, n, wallset(t), t->d_flags.p);
     g_launches++;
@@ -325,18 +379,18 @@ TessDesc make_desc(vd_tess* t) {
 }
 
 int ensure_outputs(vd_tess* t, size_t n) {
-  VD_CK(t, t->d_vol.ensure(n));
-  VD_CK(t, t->d_cen.ensure(3 * n));
-  VD_CK(t, t->d_nf.ensure(n));
-  VD_CK(t, t->d_nv.ensure(n));
-  VD_CK(t, t->d_fnb.ensure(n * (size_t)t->fout));
-  VD_CK(t, t->d_farea.ensure(n * (size_t)t->fout));
-  VD_CK(t, t->d_status.ensure(n));
-  VD_CK(t, t->d_pool_off.ensure(n));
-  VD_CK(t, t->d_ctl.ensure(kCtlWords));
-  VD_CK(t, t->d_counters.ensure(kNumCounters));
-  VD_CK(t, t->d_pool_cursor.ensure(1));
-  for (int k = 0; k < 3; ++k) VD_CK(t, t->d_list[k].ensure(n));
+  VD_CK(t, t->d_vol.ensure(n, t->stream));
+  VD_CK(t, t->d_cen.ensure(3 * n, t->stream));
+  VD_CK(t, t->d_nf.ensure(n, t->stream));
+  VD_CK(t, t->d_nv.ensure(n, t->stream));
+  VD_CK(t, t->d_fnb.ensure(n * (size_t)t->fout, t->stream));
+  VD_CK(t, t->d_farea.ensure(n * (size_t)t->fout, t->stream));
+  VD_CK(t, t->d_status.ensure(n, t->stream));
+  VD_CK(t, t->d_pool_off.ensure(n, t->stream));
+  VD_CK(t, t->d_ctl.ensure(kCtlWords, t->stream));
+  VD_CK(t, t->d_counters.ensure(kNumCounters, t->stream));
+  VD_CK(t, t->d_pool_cursor.ensure(1, t->stream));
+  for (int k = 0; k < 3; ++k) VD_CK(t, t->d_list[k].ensure(n, t->stream));
   return VD_OK;
 }
 
@@ -346,13 +400,13 @@ int ensure_big(vd_tess* t, size_t cells) {
   size_t want = std::min<size_t>(std::max<size_t>(cells, 1), (size_t)std::max(1, t->num_sms) * 4);
   want = (want + 3) / 4 * 4;
   if (t->big_warps < want) {
-    VD_CK(t, t->d_big.ensure(want * t->info64.big_scratch_per_warp));
+    VD_CK(t, t->d_big.ensure(want * t->info64.big_scratch_per_warp, t->stream));
     t->big_warps = want;
   }
   if (t->pool_cap == 0) {
     const long long cap = 1 << 20;
-    VD_CK(t, t->d_pool_fnb.ensure(cap));
-    VD_CK(t, t->d_pool_area.ensure(cap));
+    VD_CK(t, t->d_pool_fnb.ensure(cap, t->stream));
+    VD_CK(t, t->d_pool_area.ensure(cap, t->stream));
     t->pool_cap = cap;
   }
   return VD_OK;
@@ -431,8 +485,8 @@ int run_calculate(vd_tess* t, const WorkList* extra = nullptr, const uint32_t* o
     VD_CK(t, cudaMemcpyAsync(t->d_list[2].p, only_cell, sizeof(uint32_t), cudaMemcpyHostToDevice, s));
     in_list = t->d_list[2].p;
   } else if (range && (range[0] > 0 || range[1] < n)) {
-    VD_CK(t, t->d_flags.ensure(n + 1));
-    VD_CK(t, t->d_pos.ensure(n + 1));
+    VD_CK(t, t->d_flags.ensure(n + 1, t->stream));
+    VD_CK(t, t->d_pos.ensure(n + 1, t->stream));
     if (n) {
       k_clear_cells<<<grid_blocks(t, n, 256), 256, 0, s>>>(n, t->d_vol.p, t->d_cen.p, t->d_nf.p, t->d_nv.p);
       g_launches++;
@@ -521,8 +575,8 @@ int ensure_csr(vd_tess* t) {
   if (t->csr_valid) return VD_OK;
   const size_t n = t->ncells;
   cudaStream_t s = t->stream;
-  VD_CK(t, t->d_nf64.ensure(n + 1));
-  VD_CK(t, t->d_csr_off.ensure(n + 1));
+  VD_CK(t, t->d_nf64.ensure(n + 1, t->stream));
+  VD_CK(t, t->d_csr_off.ensure(n + 1, t->stream));
   if (n) {
     k_nfaces_to_i64<<<grid_blocks(t, n, 256), 256, 0, s>>>(t->d_nf.p, n, t->d_nf64.p);
     g_launches++;
@@ -650,6 +704,7 @@ int vd_tess_destroy(vd_tess* t) {
   for (auto& b : t->scan32) b.release();
   for (auto& b : t->scan64) b.release();
   t->d_ex_v.release(); t->d_ex_fc.release(); t->d_ex_fi.release(); t->d_ex_fn.release(); t->d_ex_sizes.release();
+  if (t->stream) cudaStreamSynchronize(t->stream);
   for (auto& ev : t->ev)
     if (ev) cudaEventDestroy(ev);
   if (t->stream) cudaStreamDestroy(t->stream);
@@ -726,7 +781,7 @@ int vd_tess_set_generators(vd_tess* t, const double* xyz, size_t n, size_t* n_ke
   if (n > 0xFFFFFFF0ull / 3) return fail(t, VD_EINVAL, "too many generators");
   // land the host copy in d_gen directly when no wall can drop rows
   DevBuf<double>& dst = t->walls.empty() ? t->d_gen : t->d_in;
-  VD_CK(t, dst.ensure(3 * n));
+  VD_CK(t, dst.ensure(3 * n, t->stream));
   if (n) VD_CK(t, cudaMemcpyAsync(dst.p, xyz, 3 * n * sizeof(double), cudaMemcpyHostToDevice, t->stream));
   return set_generators_from_device(t, dst.p, n, n_kept);
 }
@@ -737,7 +792,7 @@ int vd_tess_set_generators_device(vd_tess* t, const double* d_xyz, size_t n, siz
   if (n > 0xFFFFFFF0ull / 3) return fail(t, VD_EINVAL, "too many generators");
   // the filter reads d_xyz and writes d_gen, so the caller's buffer is never modified
   if (t->walls.empty()) {
-    VD_CK(t, t->d_gen.ensure(3 * n));
+    VD_CK(t, t->d_gen.ensure(3 * n, t->stream));
     if (n)
       VD_CK(t, cudaMemcpyAsync(t->d_gen.p, d_xyz, 3 * n * sizeof(double), cudaMemcpyDeviceToDevice, t->stream));
     return set_generators_from_device(t, t->d_gen.p, n, n_kept);
@@ -871,7 +926,7 @@ int vd_tess_relax(vd_tess* t) {
   int r = check_ready(t);
   if (r != VD_OK) return r;
   const size_t n = std::min(t->ncells, t->ngen);
-  VD_CK(t, t->d_in.ensure(3 * n));
+  VD_CK(t, t->d_in.ensure(3 * n, t->stream));
   if (n) {
     k_relax<<<grid_blocks(t, n, 256), 256, 0, t->stream>>>(t->d_gen.p, t->d_nv.p, t->d_cen.p, n, t->d_in.p);
     g_launches++;
@@ -926,8 +981,8 @@ static int get_csr(vd_tess* t, int64_t* offsets, int32_t* ids, double* areas) {
   const size_t n = t->ncells;
   cudaStream_t s = t->stream;
   const size_t tot = (size_t)t->csr_total;
-  if (ids) VD_CK(t, t->d_csr_ids.ensure(tot));
-  if (areas) VD_CK(t, t->d_csr_area.ensure(tot));
+  if (ids) VD_CK(t, t->d_csr_ids.ensure(tot, t->stream));
+  if (areas) VD_CK(t, t->d_csr_area.ensure(tot, t->stream));
   if (n && tot) {
     const int blocks = grid_blocks(t, n * 32, 256);
     k_csr_gather<<<blocks, 256, 0, s>>>(t->d_nf.p, n, t->d_csr_off.p, t->fout, t->d_fnb.p, t->d_farea.p,
@@ -970,11 +1025,11 @@ int vd_tess_get_cell(vd_tess* t, size_t i, int32_t* n_vertices, int32_t* n_faces
   }
   cudaStream_t s = t->stream;
   const int cv = 2048, cf = 512, ch = 6144;
-  VD_CK(t, t->d_ex_v.ensure(3 * cv));
-  VD_CK(t, t->d_ex_fc.ensure(cf));
-  VD_CK(t, t->d_ex_fi.ensure(ch));
-  VD_CK(t, t->d_ex_fn.ensure(cf));
-  VD_CK(t, t->d_ex_sizes.ensure(4));
+  VD_CK(t, t->d_ex_v.ensure(3 * cv, t->stream));
+  VD_CK(t, t->d_ex_fc.ensure(cf, t->stream));
+  VD_CK(t, t->d_ex_fi.ensure(ch, t->stream));
+  VD_CK(t, t->d_ex_fn.ensure(cf, t->stream));
+  VD_CK(t, t->d_ex_sizes.ensure(4, t->stream));
   VD_CK(t, cudaMemsetAsync(t->d_ex_sizes.p, 0, 4 * sizeof(int32_t), s));
   WorkList ex;
   memset(&ex, 0, sizeof(ex));

@@ -44,6 +44,11 @@ cudaError_t launch_clip_fp64_big_batched(const TessDesc* descs, const uint32_t* 
 // message returned by vd_last_error(NULL) on the calling thread
 void set_thread_error(const char* msg);
 
+// Reserve `bytes` in the library's memory pool on the current device (an
+// allocation freed at once; the pool keeps freed memory), so that later
+// buffer growth is served from the pool without going to the driver.
+cudaError_t reserve_pool(size_t bytes, cudaStream_t s);
+
 // Mixed path (vd_kernels_mixed.cu)
 cudaError_t clip_mixed_info(ClipLaunchInfo* info);
 cudaError_t launch_clip_mixed_fast(const TessDesc& T, const WorkList& W, int nblocks, bool count,

@@ -28,6 +28,7 @@
 #include <vector>
 
 #include "../../include/voronoid_b200.h"
+#include "vd_internal.h"
 
 namespace {
 
@@ -198,6 +199,17 @@ int vd_server_create(int slots, size_t hbm_budget_bytes, int precision, vd_serve
       return sfail(nullptr, rc, "slot setup: %s", m.c_str());
     }
     s->handles.push_back(t);
+  }
+  // Reserve the budget in the library's memory pool up front (as much of it
+  // as the device has free): a request that grows its slot's buffers is then
+  // served from the pool instead of the driver.  Best effort.
+  size_t free_b = 0, total_b = 0;
+  if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
+    void* st = nullptr;
+    vd_tess_stream(s->handles[0], &st);
+    for (size_t want = std::min(hbm_budget_bytes, free_b / 10 * 9); want >= ((size_t)1 << 28); want /= 2)
+      if (vd::reserve_pool(want, (cudaStream_t)st) == cudaSuccess) break;
+    cudaGetLastError();
   }
   for (int k = 0; k < slots; ++k) s->workers.emplace_back(worker, s, k);
   *out = s;
