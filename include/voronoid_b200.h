@@ -2,7 +2,8 @@
  * voronoid_b200.h -- C ABI of the B200 tessellation library.
  *
  * A GPU-backed drop-in for the reference crate `voronoid`'s 3D path:
- * Tessellation<3, Cell3DFaces, Algorithm3DGrid> with plane and sphere walls.
+ * Tessellation<3, Cell3DFaces, Algorithm3DGrid> with plane, sphere, cylinder,
+ * cone, torus and convex-polyhedron walls.
  * Every entry point below names the reference interface it replaces
  * (file:line within the reference crate).  Plain pointers and sizes only; no
  * framework types cross this boundary.
@@ -62,6 +63,20 @@ const char* vd_last_error(const vd_tess* t);
  *      Adding a wall prunes generators outside it (tessellation.rs:175-194). ---- */
 int vd_tess_add_wall_plane(vd_tess* t, const double point[3], const double normal[3], int id);
 int vd_tess_add_wall_sphere(vd_tess* t, const double center[3], double radius, int id);
+/* CylinderGeometry (wall_3d.rs:107-174): inside an infinite cylinder; the
+ * axis is normalised as the reference's constructor does */
+int vd_tess_add_wall_cylinder(vd_tess* t, const double center[3], const double axis[3], double radius, int id);
+/* ConeGeometry (wall_3d.rs:177-262): inside an infinite cone with apex `tip`,
+ * axis pointing into the cone, half-angle in radians */
+int vd_tess_add_wall_cone(vd_tess* t, const double tip[3], const double axis[3], double angle, int id);
+/* TorusGeometry (wall_3d.rs:265-365): inside the tube of a torus */
+int vd_tess_add_wall_torus(vd_tess* t, const double center[3], const double axis[3], double major_radius,
+                           double minor_radius, int id);
+/* ConvexPolyhedronGeometry::new (wall_3d.rs:462-492, 690-708): the
+ * intersection of half-spaces given as planes (point, normal pointing OUT of
+ * the valid region), points and normals AoS [nplanes * 3]; at most 256
+ * planes over all polyhedron walls of a tessellation */
+int vd_tess_add_wall_polyhedron(vd_tess* t, const double* points, const double* normals, int nplanes, int id);
 /* Tessellation::clear_walls (tessellation.rs:203-205) */
 int vd_tess_clear_walls(vd_tess* t);
 

@@ -42,6 +42,11 @@ def lib():
     L.vdo_destroy.argtypes = [vp]
     L.vdo_add_wall_plane.argtypes = [vp, d3, d3, C.c_int]
     L.vdo_add_wall_sphere.argtypes = [vp, d3, C.c_double, C.c_int]
+    L.vdo_add_wall_cylinder.argtypes = [vp, d3, d3, C.c_double, C.c_int]
+    L.vdo_add_wall_cone.argtypes = [vp, d3, d3, C.c_double, C.c_int]
+    L.vdo_add_wall_torus.argtypes = [vp, d3, d3, C.c_double, C.c_double, C.c_int]
+    L.vdo_add_wall_polyhedron.argtypes = [vp, d3, d3, C.c_int, C.c_int]
+    L.vdo_regular_polyhedron.argtypes = [C.c_int, d3, C.c_double, d3, d3]
     L.vdo_clear_walls.argtypes = [vp]
     L.vdo_set_generators.restype = C.c_size_t
     L.vdo_set_generators.argtypes = [vp, d3, C.c_size_t]
@@ -173,6 +178,19 @@ class OracleCell:
         return float(lib().vdo_cell_max_radius_sq(self._h, pc))
 
 
+def regular_polyhedron(faces: int, center, radius: float):
+    """(points, normals) of ConvexPolyhedronGeometry::new_* with `faces` faces
+    (4, 6, 8, 12 or 20), restated in C."""
+    c, pc = _d(center)
+    pts = np.zeros(60, np.float64)
+    nrm = np.zeros(60, np.float64)
+    m = lib().vdo_regular_polyhedron(int(faces), pc, float(radius), pts.ctypes.data_as(C.POINTER(C.c_double)),
+                                     nrm.ctypes.data_as(C.POINTER(C.c_double)))
+    if m < 0:
+        raise ValueError(faces)
+    return pts[:3 * m].reshape(-1, 3), nrm[:3 * m].reshape(-1, 3)
+
+
 class OracleTessellation:
     """Tessellation<3, Cell3DFaces, Algorithm3DGrid> restated on the CPU."""
 
@@ -198,6 +216,30 @@ class OracleTessellation:
         c, pc = _d(center)
         if lib().vdo_add_wall_sphere(self._h, pc, float(radius), int(wall_id)) != 0:
             raise ValueError("Wall ID must be <= -1000")
+
+    def add_wall_cylinder(self, center, axis, radius: float, wall_id: int):
+        c, pc = _d(center)
+        a, pa = _d(axis)
+        if lib().vdo_add_wall_cylinder(self._h, pc, pa, float(radius), int(wall_id)) != 0:
+            raise ValueError("Wall ID must be <= -1000")
+
+    def add_wall_cone(self, tip, axis, angle: float, wall_id: int):
+        c, pc = _d(tip)
+        a, pa = _d(axis)
+        if lib().vdo_add_wall_cone(self._h, pc, pa, float(angle), int(wall_id)) != 0:
+            raise ValueError("Wall ID must be <= -1000")
+
+    def add_wall_torus(self, center, axis, major: float, minor: float, wall_id: int):
+        c, pc = _d(center)
+        a, pa = _d(axis)
+        if lib().vdo_add_wall_torus(self._h, pc, pa, float(major), float(minor), int(wall_id)) != 0:
+            raise ValueError("Wall ID must be <= -1000")
+
+    def add_wall_polyhedron(self, points, normals, wall_id: int):
+        p, pp = _d(np.asarray(points, np.float64).reshape(-1))
+        n, pn = _d(np.asarray(normals, np.float64).reshape(-1))
+        if lib().vdo_add_wall_polyhedron(self._h, pp, pn, p.size // 3, int(wall_id)) != 0:
+            raise ValueError("bad polyhedron wall")
 
     def clear_walls(self):
         lib().vdo_clear_walls(self._h)

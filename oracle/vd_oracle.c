@@ -11,7 +11,9 @@
  *   src/cell/cell_3d_faces.rs  new :37-74, volume :106-143, centroid :145-205,
  *                              face_area :207-254, max_radius_sq :271-286,
  *                              clip_with_scratch :288-503
- *   src/wall/wall_3d.rs        PlaneGeometry :23-46, SphereGeometry :72-101
+ *   src/wall/wall_3d.rs        PlaneGeometry :23-46, SphereGeometry :72-101,
+ *                              CylinderGeometry :107-174, ConeGeometry :177-262,
+ *                              TorusGeometry :265-365, ConvexPolyhedronGeometry :462-708
  *   src/wall/mod.rs            WALL_ID_MAX and the id check :8,24-27
  *   src/bounds/mod.rs          box_side :21-22
  *
@@ -361,34 +363,141 @@ static double face_area_at(const vdo_cell* c, size_t off, size_t count) {
 /* ------------------------------------------------------------------ */
 /* walls (wall_3d.rs:8-101, wall/mod.rs)                                */
 /* ------------------------------------------------------------------ */
+#define VDO_MAX_PLANES 64
 typedef struct {
-  int kind; /* 0 plane, 1 sphere */
+  int kind; /* 0 plane, 1 sphere, 2 cylinder, 3 cone, 4 torus, 5 convex polyhedron */
   int32_t id;
-  double a[3]; /* plane point / sphere centre */
-  double n[3]; /* plane normal (normalised, points IN) */
-  double r;
+  double a[3]; /* plane point / sphere, cylinder, torus centre / cone tip */
+  double n[3]; /* plane normal (points IN) / cylinder, cone, torus axis (normalised) */
+  double r;    /* sphere, cylinder radius / torus major radius / cone half-angle */
+  double r2;   /* torus minor radius */
+  int np;      /* convex polyhedron: planes (point, normal pointing OUT) */
+  double planes[VDO_MAX_PLANES][6];
 } wall_t;
 
+/* WallGeometry::contains for each kind (wall_3d.rs:31-36, 73-78, 132-143,
+ * 202-214, 293-309, 691-701) */
 static int wall_contains(const wall_t* w, const double* p) {
   double dx = p[0] - w->a[0], dy = p[1] - w->a[1], dz = p[2] - w->a[2];
-  if (w->kind == 0) return (dx * w->n[0] + dy * w->n[1] + dz * w->n[2]) >= 0.0;
-  return (dx * dx + dy * dy + dz * dz) <= w->r * w->r;
+  switch (w->kind) {
+    case 0: return (dx * w->n[0] + dy * w->n[1] + dz * w->n[2]) >= 0.0;
+    case 1: return (dx * dx + dy * dy + dz * dz) <= w->r * w->r;
+    case 2: {
+      double dot = dx * w->n[0] + dy * w->n[1] + dz * w->n[2];
+      double px = dx - dot * w->n[0], py = dy - dot * w->n[1], pz = dz - dot * w->n[2];
+      return (px * px + py * py + pz * pz) <= w->r * w->r;
+    }
+    case 3: {
+      double h = dx * w->n[0] + dy * w->n[1] + dz * w->n[2];
+      double px = dx - h * w->n[0], py = dy - h * w->n[1], pz = dz - h * w->n[2];
+      double r = sqrt(px * px + py * py + pz * pz);
+      return h >= 0.0 && r <= h * tan(w->r);
+    }
+    case 4: {
+      double dot = dx * w->n[0] + dy * w->n[1] + dz * w->n[2];
+      double px = dx - dot * w->n[0], py = dy - dot * w->n[1], pz = dz - dot * w->n[2];
+      double dp = sqrt(px * px + py * py + pz * pz);
+      double q = dp - w->r;
+      return sqrt(q * q + dot * dot) <= w->r2;
+    }
+    default:
+      for (int k = 0; k < w->np; ++k) {
+        const double* pl = w->planes[k];
+        double ex = p[0] - pl[0], ey = p[1] - pl[1], ez = p[2] - pl[2];
+        if (ex * pl[3] + ey * pl[4] + ez * pl[5] > 0.0) return 0;
+      }
+      return 1;
+  }
 }
 
-/* cut: emits one plane (point, outward normal); returns 0 if none */
+/* WallGeometry::cut for one generator: the planes (point, outward normal) it
+ * emits, in order, into p/n; returns their count */
 static int wall_cut(const wall_t* w, const double* g, double* p, double* n) {
-  if (w->kind == 0) {
-    p[0] = w->a[0]; p[1] = w->a[1]; p[2] = w->a[2];
-    n[0] = -w->n[0]; n[1] = -w->n[1]; n[2] = -w->n[2];
-    return 1;
+  switch (w->kind) {
+    case 0: /* wall_3d.rs:38-42 */
+      p[0] = w->a[0]; p[1] = w->a[1]; p[2] = w->a[2];
+      n[0] = -w->n[0]; n[1] = -w->n[1]; n[2] = -w->n[2];
+      return 1;
+    case 1: { /* wall_3d.rs:80-100 */
+      double dx = g[0] - w->a[0], dy = g[1] - w->a[1], dz = g[2] - w->a[2];
+      double dist = sqrt(dx * dx + dy * dy + dz * dz);
+      if (dist == 0.0) return 0;
+      double scale = w->r / dist;
+      p[0] = w->a[0] + dx * scale; p[1] = w->a[1] + dy * scale; p[2] = w->a[2] + dz * scale;
+      n[0] = dx / dist; n[1] = dy / dist; n[2] = dz / dist;
+      return 1;
+    }
+    case 2: { /* wall_3d.rs:145-173 */
+      double dx = g[0] - w->a[0], dy = g[1] - w->a[1], dz = g[2] - w->a[2];
+      double dot = dx * w->n[0] + dy * w->n[1] + dz * w->n[2];
+      double px = dx - dot * w->n[0], py = dy - dot * w->n[1], pz = dz - dot * w->n[2];
+      double dist = sqrt(px * px + py * py + pz * pz);
+      if (dist == 0.0) return 0;
+      double scale = w->r / dist;
+      p[0] = w->a[0] + dot * w->n[0] + px * scale;
+      p[1] = w->a[1] + dot * w->n[1] + py * scale;
+      p[2] = w->a[2] + dot * w->n[2] + pz * scale;
+      n[0] = px / dist; n[1] = py / dist; n[2] = pz / dist;
+      return 1;
+    }
+    case 3: { /* wall_3d.rs:216-261 */
+      double dx = g[0] - w->a[0], dy = g[1] - w->a[1], dz = g[2] - w->a[2];
+      double h = dx * w->n[0] + dy * w->n[1] + dz * w->n[2];
+      double px = dx - h * w->n[0], py = dy - h * w->n[1], pz = dz - h * w->n[2];
+      double r = sqrt(px * px + py * py + pz * pz);
+      if (r == 0.0) return 0;
+      double rdx = px / r, rdy = py / r, rdz = pz / r;
+      double ca = cos(w->r), sa = sin(w->r);
+      double dist = r * ca - h * sa;
+      double pr = r - dist * ca;
+      double ph = h + dist * sa;
+      if (ph < 0.0) {
+        double dt = sqrt(dx * dx + dy * dy + dz * dz);
+        if (dt == 0.0) return 0;
+        p[0] = w->a[0]; p[1] = w->a[1]; p[2] = w->a[2];
+        n[0] = dx / dt; n[1] = dy / dt; n[2] = dz / dt;
+        return 1;
+      }
+      p[0] = w->a[0] + ph * w->n[0] + pr * rdx;
+      p[1] = w->a[1] + ph * w->n[1] + pr * rdy;
+      p[2] = w->a[2] + ph * w->n[2] + pr * rdz;
+      n[0] = ca * rdx - sa * w->n[0];
+      n[1] = ca * rdy - sa * w->n[1];
+      n[2] = ca * rdz - sa * w->n[2];
+      return 1;
+    }
+    case 4: { /* wall_3d.rs:311-364 */
+      double dx = g[0] - w->a[0], dy = g[1] - w->a[1], dz = g[2] - w->a[2];
+      double dot = dx * w->n[0] + dy * w->n[1] + dz * w->n[2];
+      double px = dx - dot * w->n[0], py = dy - dot * w->n[1], pz = dz - dot * w->n[2];
+      double dp = sqrt(px * px + py * py + pz * pz);
+      double ux, uy, uz;
+      if (dp < 1e-9) {
+        double tx = 1.0, ty = 0.0, tz = 0.0;
+        if (fabs(w->n[0]) > 0.9) { tx = 0.0; ty = 1.0; }
+        double td = tx * w->n[0] + ty * w->n[1] + tz * w->n[2];
+        double ax = tx - td * w->n[0], ay = ty - td * w->n[1], az = tz - td * w->n[2];
+        double len = sqrt(ax * ax + ay * ay + az * az);
+        if (len == 0.0) return 0;
+        ux = ax / len; uy = ay / len; uz = az / len;
+      } else {
+        ux = px / dp; uy = py / dp; uz = pz / dp;
+      }
+      double cx = w->a[0] + ux * w->r, cy = w->a[1] + uy * w->r, cz = w->a[2] + uz * w->r;
+      double vx = g[0] - cx, vy = g[1] - cy, vz = g[2] - cz;
+      double dc = sqrt(vx * vx + vy * vy + vz * vz);
+      if (dc == 0.0) return 0;
+      n[0] = vx / dc; n[1] = vy / dc; n[2] = vz / dc;
+      p[0] = cx + n[0] * w->r2; p[1] = cy + n[1] * w->r2; p[2] = cz + n[2] * w->r2;
+      return 1;
+    }
+    default: /* wall_3d.rs:703-707 */
+      for (int k = 0; k < w->np; ++k) {
+        memcpy(&p[3 * k], &w->planes[k][0], 3 * sizeof(double));
+        memcpy(&n[3 * k], &w->planes[k][3], 3 * sizeof(double));
+      }
+      return w->np;
   }
-  double dx = g[0] - w->a[0], dy = g[1] - w->a[1], dz = g[2] - w->a[2];
-  double dist = sqrt(dx * dx + dy * dy + dz * dz);
-  if (dist == 0.0) return 0;
-  double scale = w->r / dist;
-  p[0] = w->a[0] + dx * scale; p[1] = w->a[1] + dy * scale; p[2] = w->a[2] + dz * scale;
-  n[0] = dx / dist; n[1] = dy / dist; n[2] = dz / dist;
-  return 1;
 }
 
 /* ------------------------------------------------------------------ */
@@ -568,6 +677,115 @@ int vdo_add_wall_sphere(vdo_tess* t, const double center[3], double radius, int 
   return add_wall(t, &w);
 }
 
+/* an axis normalised as in CylinderGeometry/ConeGeometry/TorusGeometry::new
+ * (wall_3d.rs:124-128, 194-198, 285-289) */
+static void unit_axis(const double axis[3], double out[3]) {
+  double len = sqrt(axis[0] * axis[0] + axis[1] * axis[1] + axis[2] * axis[2]);
+  if (len == 0.0) { out[0] = 0.0; out[1] = 0.0; out[2] = 1.0; }
+  else { out[0] = axis[0] / len; out[1] = axis[1] / len; out[2] = axis[2] / len; }
+}
+
+int vdo_add_wall_cylinder(vdo_tess* t, const double center[3], const double axis[3], double radius, int id) {
+  wall_t w;
+  memset(&w, 0, sizeof(w));
+  w.kind = 2; w.id = id; w.r = radius;
+  memcpy(w.a, center, 3 * sizeof(double));
+  unit_axis(axis, w.n);
+  return add_wall(t, &w);
+}
+
+int vdo_add_wall_cone(vdo_tess* t, const double tip[3], const double axis[3], double angle, int id) {
+  wall_t w;
+  memset(&w, 0, sizeof(w));
+  w.kind = 3; w.id = id; w.r = angle;
+  memcpy(w.a, tip, 3 * sizeof(double));
+  unit_axis(axis, w.n);
+  return add_wall(t, &w);
+}
+
+int vdo_add_wall_torus(vdo_tess* t, const double center[3], const double axis[3], double major, double minor,
+                       int id) {
+  wall_t w;
+  memset(&w, 0, sizeof(w));
+  w.kind = 4; w.id = id; w.r = major; w.r2 = minor;
+  memcpy(w.a, center, 3 * sizeof(double));
+  unit_axis(axis, w.n);
+  return add_wall(t, &w);
+}
+
+/* ConvexPolyhedronGeometry::new (wall_3d.rs:476-492): planes (point, normal
+ * pointing OUT), taken as given */
+int vdo_add_wall_polyhedron(vdo_tess* t, const double* points, const double* normals, int nplanes, int id) {
+  if (nplanes < 0 || nplanes > VDO_MAX_PLANES) return -1;
+  wall_t w;
+  memset(&w, 0, sizeof(w));
+  w.kind = 5; w.id = id; w.np = nplanes;
+  for (int k = 0; k < nplanes; ++k) {
+    memcpy(&w.planes[k][0], &points[3 * k], 3 * sizeof(double));
+    memcpy(&w.planes[k][3], &normals[3 * k], 3 * sizeof(double));
+  }
+  return add_wall(t, &w);
+}
+
+/* the regular polyhedra of ConvexPolyhedronGeometry::new_* (wall_3d.rs:499-688):
+ * kind 4 tetrahedron, 6 hexahedron, 8 octahedron, 12 dodecahedron,
+ * 20 icosahedron; returns the plane count or -1 */
+int vdo_regular_polyhedron(int kind, const double center[3], double radius, double* points, double* normals) {
+  double bn[20][3];
+  int m = 0, unit = 1;
+  double dist;
+  if (kind == 4) {
+    static const double b[4][3] = {{-1, -1, -1}, {-1, 1, 1}, {1, -1, 1}, {1, 1, -1}};
+    memcpy(bn, b, sizeof(b)); m = 4;
+    dist = radius / 3.0;
+  } else if (kind == 6) {
+    static const double b[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+    memcpy(bn, b, sizeof(b)); m = 6; unit = 0; /* used as given, not normalised */
+    dist = radius / sqrt(3.0);
+  } else if (kind == 8) {
+    for (int x = -1; x <= 1; x += 2)
+      for (int y = -1; y <= 1; y += 2)
+        for (int z = -1; z <= 1; z += 2) { bn[m][0] = x; bn[m][1] = y; bn[m][2] = z; ++m; }
+    dist = radius / sqrt(3.0);
+  } else if (kind == 12) {
+    double phi = (1.0 + sqrt(5.0)) / 2.0;
+    double xi = sqrt((5.0 + 2.0 * sqrt(5.0)) / 15.0);
+    dist = radius * xi;
+    const double b[12][3] = {{0.0, phi, 1.0}, {0.0, -phi, 1.0}, {0.0, phi, -1.0}, {0.0, -phi, -1.0},
+                             {1.0, 0.0, phi}, {1.0, 0.0, -phi}, {-1.0, 0.0, phi}, {-1.0, 0.0, -phi},
+                             {phi, 1.0, 0.0}, {phi, -1.0, 0.0}, {-phi, 1.0, 0.0}, {-phi, -1.0, 0.0}};
+    memcpy(bn, b, sizeof(b)); m = 12;
+  } else if (kind == 20) {
+    double phi = (1.0 + sqrt(5.0)) / 2.0;
+    double xi = sqrt((5.0 + 2.0 * sqrt(5.0)) / 15.0);
+    dist = radius * xi;
+    double ip = 1.0 / phi;
+    for (int x = -1; x <= 1; x += 2)
+      for (int y = -1; y <= 1; y += 2)
+        for (int z = -1; z <= 1; z += 2) { bn[m][0] = x; bn[m][1] = y; bn[m][2] = z; ++m; }
+    for (int y = -1; y <= 1; y += 2)
+      for (int z = -1; z <= 1; z += 2) { bn[m][0] = 0.0; bn[m][1] = y * phi; bn[m][2] = z * ip; ++m; }
+    for (int x = -1; x <= 1; x += 2)
+      for (int z = -1; z <= 1; z += 2) { bn[m][0] = x * ip; bn[m][1] = 0.0; bn[m][2] = z * phi; ++m; }
+    for (int x = -1; x <= 1; x += 2)
+      for (int y = -1; y <= 1; y += 2) { bn[m][0] = x * phi; bn[m][1] = y * ip; bn[m][2] = 0.0; ++m; }
+  } else {
+    return -1;
+  }
+  for (int k = 0; k < m; ++k) {
+    double nx = bn[k][0], ny = bn[k][1], nz = bn[k][2];
+    if (unit) {
+      double len = sqrt(nx * nx + ny * ny + nz * nz);
+      nx = nx / len; ny = ny / len; nz = nz / len;
+    }
+    normals[3 * k] = nx; normals[3 * k + 1] = ny; normals[3 * k + 2] = nz;
+    points[3 * k] = center[0] + nx * dist;
+    points[3 * k + 1] = center[1] + ny * dist;
+    points[3 * k + 2] = center[2] + nz * dist;
+  }
+  return m;
+}
+
 void vdo_clear_walls(vdo_tess* t) { t->nwalls = 0; }
 
 /* compute_cell (tessellation.rs:414-475) with visit_neighbors
@@ -577,8 +795,9 @@ static void compute_cell(const vdo_tess* t, size_t i, vdo_cell* cell, scratch_t*
   double r2;
   cell_init_box(cell, i, t->bmin, t->bmax);
   for (int w = 0; w < t->nwalls; ++w) {
-    double p[3], n[3];
-    if (wall_cut(&t->walls[w], g, p, n)) cell_clip(cell, p, n, t->walls[w].id, s, NULL, &r2, cnt);
+    double p[3 * VDO_MAX_PLANES], n[3 * VDO_MAX_PLANES];
+    int np = wall_cut(&t->walls[w], g, p, n);
+    for (int k = 0; k < np; ++k) cell_clip(cell, &p[3 * k], &n[3 * k], t->walls[w].id, s, NULL, &r2, cnt);
     if (cell->nv == 0) return;
   }
   double cur = cell_max_radius_sq(cell, g);

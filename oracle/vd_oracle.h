@@ -3,8 +3,9 @@
  *
  * This is a plain-C restatement of the reference crate `voronoid` (Rust) for
  * the path Tessellation::calculate over Algorithm3DGrid + Cell3DFaces, with
- * plane and sphere walls.  It exists only to check the CUDA product path and
- * to time a CPU baseline; nothing in the product links or calls it.
+ * plane, sphere, cylinder, cone, torus and convex-polyhedron walls.  It
+ * exists only to check the CUDA product path and to time a CPU baseline;
+ * nothing in the product links or calls it.
  *
  * Parity pins: the reference cannot be compiled here (it is Rust and no Rust
  * toolchain exists), so this restatement is pinned against the reference's
@@ -49,6 +50,16 @@ void vdo_destroy(vdo_tess* t);
 /* returns 0, or -1 if id > -1000 (the reference panics, wall/mod.rs:25) */
 int vdo_add_wall_plane(vdo_tess* t, const double point[3], const double normal[3], int id);
 int vdo_add_wall_sphere(vdo_tess* t, const double center[3], double radius, int id);
+/* CylinderGeometry / ConeGeometry / TorusGeometry / ConvexPolyhedronGeometry
+ * (wall_3d.rs:107-365, 462-708); axes are normalised as the reference does */
+int vdo_add_wall_cylinder(vdo_tess* t, const double center[3], const double axis[3], double radius, int id);
+int vdo_add_wall_cone(vdo_tess* t, const double tip[3], const double axis[3], double angle, int id);
+int vdo_add_wall_torus(vdo_tess* t, const double center[3], const double axis[3], double major, double minor,
+                       int id);
+int vdo_add_wall_polyhedron(vdo_tess* t, const double* points, const double* normals, int nplanes, int id);
+/* planes of ConvexPolyhedronGeometry::new_{tetrahedron,hexahedron,octahedron,
+ * dodecahedron,icosahedron} (kind = face count 4/6/8/12/20); returns the count */
+int vdo_regular_polyhedron(int kind, const double center[3], double radius, double* points, double* normals);
 void vdo_clear_walls(vdo_tess* t);
 size_t vdo_set_generators(vdo_tess* t, const double* xyz, size_t n);
 void vdo_calculate(vdo_tess* t, int nthreads);

@@ -1,0 +1,113 @@
+"""GPU: cylinder, cone, torus and convex-polyhedron walls (wall_3d.rs:107-365,
+462-708) bit for bit against the oracle, alone and combined, with the walls
+added before and after the generators, in both precisions; plus the
+reference's own volume tests for these walls (tests/volumes.rs:68-105)."""
+import math
+
+import numpy as np
+import pytest
+
+from common import uniform
+from test_gpu_parity import PRECISIONS, assert_same, gpu_tess
+
+pytestmark = pytest.mark.gpu
+
+WALL = -1000
+
+
+def oracle_add(t, w):
+    import vorothree_b200 as v
+    g = w.geometry
+    if isinstance(g, v.PlaneGeometry):
+        t.add_wall_plane(g.point, g.normal, w.id())
+    elif isinstance(g, v.SphereGeometry):
+        t.add_wall_sphere(g.center, g.radius, w.id())
+    elif isinstance(g, v.CylinderGeometry):
+        t.add_wall_cylinder(g.center, g.axis, g.radius, w.id())
+    elif isinstance(g, v.ConeGeometry):
+        t.add_wall_cone(g.tip, g.axis, g.angle, w.id())
+    elif isinstance(g, v.TorusGeometry):
+        t.add_wall_torus(g.center, g.axis, g.major_radius, g.minor_radius, w.id())
+    else:
+        t.add_wall_polyhedron(g.points, g.normals, w.id())
+
+
+def oracle_tess(oracle_mod, bmin, bmax, grid, pts, walls, walls_first):
+    t = oracle_mod.OracleTessellation(bmin, bmax, *grid)
+    if walls_first:
+        for w in walls:
+            oracle_add(t, w)
+        t.set_generators(pts)
+    else:
+        t.set_generators(pts)
+        for w in walls:
+            oracle_add(t, w)
+    t.calculate()
+    return t
+
+
+def wall_sets():
+    import vorothree_b200 as v
+    P = v.ConvexPolyhedronGeometry
+    return {
+        "cylinder": [v.Wall(WALL, v.CylinderGeometry([5, 5, 5], [0.2, 0.1, 1.0], 4.0))],
+        "cone": [v.Wall(WALL, v.ConeGeometry([5, 5, -1], [0.1, 0.0, 1.0], 0.45))],
+        "torus": [v.Wall(WALL, v.TorusGeometry([5, 5, 5], [0.0, 0.3, 1.0], 3.0, 1.6))],
+        "tetrahedron": [v.Wall(WALL, P.new_tetrahedron([5, 5, 5], 4.5))],
+        "hexahedron": [v.Wall(WALL, P.new_hexahedron([5, 5, 5], 4.5))],
+        "octahedron": [v.Wall(WALL, P.new_octahedron([5, 5, 5], 4.5))],
+        "dodecahedron": [v.Wall(WALL, P.new_dodecahedron([5, 5, 5], 4.5))],
+        "icosahedron": [v.Wall(WALL, P.new_icosahedron([5, 5, 5], 4.5))],
+        "combined": [v.Wall(WALL, v.CylinderGeometry([5, 5, 5], [0, 0, 1], 4.5)),
+                     v.Wall(WALL - 1, v.PlaneGeometry([5, 5, 5], [0.3, -1.0, 0.2])),
+                     v.Wall(WALL - 2, P.new_dodecahedron([5, 5, 5], 6.0)),
+                     v.Wall(WALL - 3, v.SphereGeometry([5, 5, 5], 5.5))],
+    }
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+@pytest.mark.parametrize("name", ["cylinder", "cone", "torus", "tetrahedron", "hexahedron", "octahedron",
+                                  "dodecahedron", "icosahedron", "combined"])
+@pytest.mark.parametrize("walls_first", [True, False])
+def test_walls_bitwise(oracle_mod, name, walls_first, precision):
+    walls = wall_sets()[name]
+    pts = uniform(4000, 0.0, 10.0, 30)
+    g = gpu_tess([0, 0, 0], [10, 10, 10], (8, 8, 8), pts, walls, walls_first=walls_first, precision=precision)
+    o = oracle_tess(oracle_mod, [0, 0, 0], [10, 10, 10], (8, 8, 8), pts, walls, walls_first)
+    assert g.count_generators() > 100
+    assert_same(g, o, sample_cells=6)
+
+
+def lattice(size=10.0, n=20):
+    step = size / n
+    ax = np.arange(n) * step + step / 2
+    return np.array([[x, y, z] for x in ax for y in ax for z in ax])
+
+
+def test_reference_wall_volumes():
+    import vorothree_b200 as v
+    # tests/volumes.rs:68-105: cylinder and dodecahedron on the 20^3 lattice, grid 5^3, within 1%
+    cases = [(v.CylinderGeometry([5, 5, 5], [0, 0, 1], 4.0), math.pi * 16.0 * 10.0)]
+    xi = math.sqrt((5.0 + 2.0 * math.sqrt(5.0)) / 15.0)
+    a = 2.0 * 4.0 * xi * math.sqrt(10.0) / math.sqrt(25.0 + 11.0 * math.sqrt(5.0))
+    cases.append((v.ConvexPolyhedronGeometry.new_dodecahedron([5, 5, 5], 4.0),
+                  (15.0 + 7.0 * math.sqrt(5.0)) / 4.0 * a ** 3))
+    for geom, exp in cases:
+        t = v.Tessellation(v.BoundingBox([0, 0, 0], [10, 10, 10]), v.Algorithm3DGrid(5, 5, 5))
+        t.set_generators(lattice())
+        t.add_wall(v.Wall(WALL, geom))
+        t.calculate()
+        vol, _, _ = t.summaries()
+        assert abs(vol.sum() - exp) / exp < 0.01
+
+
+def test_wall_errors():
+    import vorothree_b200 as v
+    with pytest.raises(ValueError):
+        v.Wall(-5, v.CylinderGeometry([0, 0, 0], [0, 0, 1], 1.0))
+    with pytest.raises(ValueError):
+        v.ConvexPolyhedronGeometry([0, 0, 0, 1, 1, 1], [0, 0, 1])
+    t = v.Tessellation(v.BoundingBox([0, 0, 0], [1, 1, 1]), v.Algorithm3DGrid(2, 2, 2))
+    big = v.ConvexPolyhedronGeometry(np.zeros((257, 3)), np.tile([0.0, 0.0, 1.0], (257, 1)))
+    with pytest.raises(v.VoronoidError):
+        t.add_wall(v.Wall(WALL, big))

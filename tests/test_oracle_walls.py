@@ -1,0 +1,113 @@
+"""CPU: the oracle's cylinder, cone, torus and convex-polyhedron walls
+(wall_3d.rs:107-365, 462-708) against the reference's own known answers
+(tests/volumes.rs:68-105: cylinder and dodecahedron volumes on the 20^3
+lattice within 1%; tests/neighbors.rs:180-200: dodecahedron reciprocity) and
+against analytic volumes for the cone and the torus, which the reference's
+tests do not cover."""
+import math
+
+import numpy as np
+import pytest
+
+from common import uniform
+
+WALL = -1000
+
+
+def lattice(size=10.0, n=20):
+    step = size / n
+    ax = np.arange(n) * step + step / 2
+    return np.array([[x, y, z] for x in ax for y in ax for z in ax])
+
+
+def total_volume(o):
+    vol, _, _ = o.summaries()
+    return vol.sum()
+
+
+def box_tess(oracle_mod, pts, add):
+    t = oracle_mod.OracleTessellation([0, 0, 0], [10, 10, 10], 5, 5, 5)
+    t.set_generators(pts)
+    add(t)
+    t.calculate(1)
+    return t
+
+
+def test_cylinder_volume(oracle_mod):
+    t = box_tess(oracle_mod, lattice(), lambda t: t.add_wall_cylinder([5, 5, 5], [0, 0, 1], 4.0, WALL))
+    exp = math.pi * 16.0 * 10.0
+    assert abs(total_volume(t) - exp) / exp < 0.01
+
+
+def dodecahedron_volume(radius):
+    xi = math.sqrt((5.0 + 2.0 * math.sqrt(5.0)) / 15.0)
+    dist = radius * xi
+    a = 2.0 * dist * math.sqrt(10.0) / math.sqrt(25.0 + 11.0 * math.sqrt(5.0))
+    return (15.0 + 7.0 * math.sqrt(5.0)) / 4.0 * a ** 3
+
+
+def test_dodecahedron_volume(oracle_mod):
+    pts, nrm = oracle_mod.regular_polyhedron(12, [5, 5, 5], 4.0)
+    t = box_tess(oracle_mod, lattice(), lambda t: t.add_wall_polyhedron(pts, nrm, WALL))
+    exp = dodecahedron_volume(4.0)
+    assert abs(total_volume(t) - exp) / exp < 0.01
+
+
+@pytest.mark.parametrize("faces,vol_of_r1", [
+    (4, 8.0 / (9.0 * math.sqrt(3.0))),          # regular tetrahedron, circumradius 1
+    (6, 8.0 / (3.0 * math.sqrt(3.0))),          # cube
+    (8, 4.0 / 3.0),                              # octahedron
+    (20, 2.536150710120),                        # icosahedron
+])
+def test_regular_polyhedra_volumes(oracle_mod, faces, vol_of_r1):
+    pts, nrm = oracle_mod.regular_polyhedron(faces, [5, 5, 5], 4.0)
+    assert len(pts) == faces
+    # planar walls: every cell is cut exactly, so the total is the solid's volume
+    t = box_tess(oracle_mod, lattice(), lambda t: t.add_wall_polyhedron(pts, nrm, WALL))
+    exp = vol_of_r1 * 64.0
+    assert abs(total_volume(t) - exp) / exp < 1e-9
+
+
+def test_dodecahedron_reciprocity(oracle_mod):
+    pts_w, nrm_w = oracle_mod.regular_polyhedron(12, [15, 15, 15], 10.0)
+    t = oracle_mod.OracleTessellation([0, 0, 0], [30, 30, 30], 5, 5, 5)
+    t.set_generators(uniform(100, 0.0, 30.0, 3))
+    t.add_wall_polyhedron(pts_w, nrm_w, WALL)
+    t.calculate(1)
+    off, ids = t.neighbors()
+    nb = [set(int(x) for x in ids[off[i]:off[i + 1]] if x >= 0) for i in range(t.count_cells())]
+    for i, s in enumerate(nb):
+        for j in s:
+            assert i in nb[j]
+
+
+def test_cone_volume(oracle_mod):
+    ang = 0.4
+    t = box_tess(oracle_mod, lattice(), lambda t: t.add_wall_cone([5, 5, 0], [0, 0, 1], ang, WALL))
+    r = 10.0 * math.tan(ang)
+    exp = math.pi * r * r * 10.0 / 3.0
+    assert abs(total_volume(t) - exp) / exp < 0.03
+
+
+def test_torus_volume(oracle_mod):
+    t = box_tess(oracle_mod, lattice(), lambda t: t.add_wall_torus([5, 5, 5], [0, 0, 1], 3.0, 1.5, WALL))
+    exp = 2.0 * math.pi ** 2 * 3.0 * 1.5 ** 2
+    assert abs(total_volume(t) - exp) / exp < 0.03
+
+
+def test_wall_filters(oracle_mod):
+    # contains(): generators outside a wall are dropped at set_generators
+    pts = uniform(4000, 0.0, 10.0, 8)
+    t = oracle_mod.OracleTessellation([0, 0, 0], [10, 10, 10], 5, 5, 5)
+    t.add_wall_torus([5, 5, 5], [0, 0, 2], 3.0, 1.5, WALL)
+    kept = t.set_generators(pts)
+    d = pts - 5.0
+    rho = np.sqrt(d[:, 0] ** 2 + d[:, 1] ** 2)
+    inside = np.sqrt((rho - 3.0) ** 2 + d[:, 2] ** 2) <= 1.5
+    assert kept == int(inside.sum())
+    t = oracle_mod.OracleTessellation([0, 0, 0], [10, 10, 10], 5, 5, 5)
+    t.add_wall_cone([5, 5, 0], [0, 0, 3], 0.4, WALL)
+    kept = t.set_generators(pts)
+    h = pts[:, 2]
+    rr = np.sqrt((pts[:, 0] - 5) ** 2 + (pts[:, 1] - 5) ** 2)
+    assert kept == int(((h >= 0) & (rr <= h * math.tan(0.4))).sum())

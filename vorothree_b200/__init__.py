@@ -10,9 +10,11 @@ from ._lib import VoronoidError, load
 from .batch import TessellationBatch
 from .server import TessellationServer
 from .shard import calculate_sharded, cell_range, gather_summaries
-from .tessellation import (WALL_ID_MAX, Algorithm3DGrid, BoundingBox, Cell3DFaces, PlaneGeometry,
-                           SphereGeometry, Tessellation, Wall, box_side)
+from .tessellation import (WALL_ID_MAX, Algorithm3DGrid, BoundingBox, Cell3DFaces, ConeGeometry,
+                           ConvexPolyhedronGeometry, CylinderGeometry, PlaneGeometry, SphereGeometry, Tessellation,
+                           TorusGeometry, Wall, box_side)
 
-__all__ = ["Algorithm3DGrid", "BoundingBox", "Cell3DFaces", "PlaneGeometry", "SphereGeometry",
+__all__ = ["Algorithm3DGrid", "BoundingBox", "Cell3DFaces", "ConeGeometry", "ConvexPolyhedronGeometry",
+           "CylinderGeometry", "PlaneGeometry", "SphereGeometry", "TorusGeometry",
            "Tessellation", "TessellationBatch", "TessellationServer", "Wall", "WALL_ID_MAX", "box_side", "VoronoidError", "load",
            "calculate_sharded", "cell_range", "gather_summaries"]

@@ -40,6 +40,10 @@ SIGNATURES = {
     "vd_last_error": (C.c_char_p, [_vp]),
     "vd_tess_add_wall_plane": (C.c_int, [_vp, _d, _d, C.c_int]),
     "vd_tess_add_wall_sphere": (C.c_int, [_vp, _d, C.c_double, C.c_int]),
+    "vd_tess_add_wall_cylinder": (C.c_int, [_vp, _d, _d, C.c_double, C.c_int]),
+    "vd_tess_add_wall_cone": (C.c_int, [_vp, _d, _d, C.c_double, C.c_int]),
+    "vd_tess_add_wall_torus": (C.c_int, [_vp, _d, _d, C.c_double, C.c_double, C.c_int]),
+    "vd_tess_add_wall_polyhedron": (C.c_int, [_vp, _d, _d, C.c_int, C.c_int]),
     "vd_tess_clear_walls": (C.c_int, [_vp]),
     "vd_tess_set_generators": (C.c_int, [_vp, _d, C.c_size_t, _szp]),
     "vd_tess_set_generators_device": (C.c_int, [_vp, _vp, C.c_size_t, _szp]),

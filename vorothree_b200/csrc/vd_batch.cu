@@ -92,7 +92,7 @@ __global__ void k_bwall_flags(const double* __restrict__ in, const uint32_t* off
       const TessDesc& T = descs[find_tess(off, ntess, g)];
       const double x = in[3 * (size_t)g], y = in[3 * (size_t)g + 1], z = in[3 * (size_t)g + 2];
       bool ok = true;
-      for (int k = 0; k < T.nwalls && ok; ++k) ok = wall_contains(T.walls[k], x, y, z);
+      for (int k = 0; k < T.nwalls && ok; ++k) ok = wall_contains(T.walls[k], T.planes, x, y, z);
       f = ok ? 1u : 0u;
     }
     flags[g] = f;

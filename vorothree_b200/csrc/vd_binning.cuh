@@ -78,23 +78,53 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_add(T* out, size_t n, con
 }
 
 // ---- walls ------------------------------------------------------------------
-// Wall::contains (wall_3d.rs:31-36 plane, :72-78 sphere)
-__device__ __forceinline__ bool wall_contains(const Wall& w, double x, double y, double z) {
+// WallGeometry::contains of each wall kind (wall_3d.rs:31-36, 73-78, 132-143,
+// 202-214, 293-309, 691-701), in the reference's arithmetic order
+__device__ __forceinline__ bool wall_contains(const Wall& w, const double* planes, double x, double y, double z) {
   const double dx = x - w.a[0], dy = y - w.a[1], dz = z - w.a[2];
-  if (w.kind == 0) return (dx * w.n[0] + dy * w.n[1] + dz * w.n[2]) >= 0.0;
-  return (dx * dx + dy * dy + dz * dz) <= w.r * w.r;
+  switch (w.kind) {
+    case kWallPlane:
+      return (dx * w.n[0] + dy * w.n[1] + dz * w.n[2]) >= 0.0;
+    case kWallSphere:
+      return (dx * dx + dy * dy + dz * dz) <= w.r * w.r;
+    case kWallCylinder: {
+      const double dot = dx * w.n[0] + dy * w.n[1] + dz * w.n[2];
+      const double px = dx - dot * w.n[0], py = dy - dot * w.n[1], pz = dz - dot * w.n[2];
+      return (px * px + py * py + pz * pz) <= w.r * w.r;
+    }
+    case kWallCone: {
+      const double h = dx * w.n[0] + dy * w.n[1] + dz * w.n[2];
+      const double px = dx - h * w.n[0], py = dy - h * w.n[1], pz = dz - h * w.n[2];
+      const double r = sqrt(px * px + py * py + pz * pz);
+      return h >= 0.0 && r <= h * w.ta;
+    }
+    case kWallTorus: {
+      const double dot = dx * w.n[0] + dy * w.n[1] + dz * w.n[2];
+      const double px = dx - dot * w.n[0], py = dy - dot * w.n[1], pz = dz - dot * w.n[2];
+      const double q = sqrt(px * px + py * py + pz * pz) - w.r;
+      return sqrt(q * q + dot * dot) <= w.r2;
+    }
+    default:
+      for (int k = 0; k < w.np; ++k) {
+        const double* pl = planes + 6 * (w.p0 + k);
+        const double ex = x - pl[0], ey = y - pl[1], ez = z - pl[2];
+        if (ex * pl[3] + ey * pl[4] + ez * pl[5] > 0.0) return false;
+      }
+      return true;
+  }
 }
 
 struct WallSet {
   int n;
   Wall w[kMaxWalls];
+  const double* planes;
 };
 
 __global__ void k_wall_flags(const double* __restrict__ in, size_t n, const WallSet ws, uint32_t* flags) {
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     const double x = in[3 * i], y = in[3 * i + 1], z = in[3 * i + 2];
     bool ok = true;
-    for (int k = 0; k < ws.n && ok; ++k) ok = wall_contains(ws.w[k], x, y, z);
+    for (int k = 0; k < ws.n && ok; ++k) ok = wall_contains(ws.w[k], ws.planes, x, y, z);
     flags[i] = ok ? 1u : 0u;
   }
 }

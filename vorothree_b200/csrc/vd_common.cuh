@@ -47,13 +47,21 @@ struct Grid {
   double cs[3];     // cell size = 1 / grid_scale
 };
 
+enum WallKind : int { kWallPlane = 0, kWallSphere, kWallCylinder, kWallCone, kWallTorus, kWallPolyhedron };
+
 struct Wall {
-  int kind;  // 0 plane, 1 sphere
+  int kind;     // WallKind
   int id;
-  double a[3];  // plane point / sphere centre
-  double n[3];  // plane normal, normalised, pointing into the valid region
-  double r;     // sphere radius
+  double a[3];  // plane point / sphere, cylinder, torus centre / cone tip
+  double n[3];  // plane normal pointing into the valid region / cylinder, cone, torus axis (normalised)
+  double r;     // sphere, cylinder radius / torus major radius / cone half-angle
+  double r2;    // torus minor radius
+  double ca, sa, ta;  // cone: cos, sin and tan of the half-angle, computed on the host as libm does
+  int np, p0;   // convex polyhedron: its planes are [p0, p0 + np) of the plane table
 };
+
+// planes of convex-polyhedron walls: (point, normal pointing out), 6 doubles each
+constexpr int kMaxWallPlanes = 256;
 
 struct alignas(16) Offset {
   int16_t dx, dy, dz, pad;
@@ -70,6 +78,7 @@ struct TessDesc {
   Grid grid;
   int nwalls;
   Wall walls[kMaxWalls];
+  const double* planes;  // plane table of convex-polyhedron walls (device)
   const Offset* order;
   int norder;
   int order_complete;   // 1 when order holds every offset of the grid

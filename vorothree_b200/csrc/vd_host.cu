@@ -133,6 +133,8 @@ struct vd_tess {
   cudaStream_t stream = nullptr;
   Grid grid{};
   std::vector<Wall> walls;
+  std::vector<double> planes;  // plane table of convex-polyhedron walls (6 doubles each)
+  DevBuf<double> d_planes;
   int precision = VD_PREC_FP64;
   bool instrument = false;  // run the counting kernel variant
 
@@ -263,6 +265,7 @@ WallSet wallset(const vd_tess* t) {
   memset(&ws, 0, sizeof(ws));
   ws.n = (int)t->walls.size();
   for (int i = 0; i < ws.n; ++i) ws.w[i] = t->walls[i];
+  ws.planes = t->d_planes.p;
   return ws;
 }
 
@@ -353,6 +356,7 @@ TessDesc make_desc(vd_tess* t) {
   T.grid = t->grid;
   T.nwalls = (int)t->walls.size();
   for (int i = 0; i < T.nwalls; ++i) T.walls[i] = t->walls[i];
+  T.planes = t->d_planes.p;
   T.order = t->d_order.p;
   T.norder = t->norder;
   T.order_complete = t->order_complete ? 1 : 0;
@@ -676,6 +680,7 @@ int vd_tess_reset(vd_tess* t, const double bmin[3], const double bmax[3], int nx
   }
   t->nbins = (size_t)nx * ny * nz;
   t->walls.clear();
+  t->planes.clear();
   t->ngen = 0;
   t->ncells = 0;
   t->calculated = false;
@@ -691,6 +696,7 @@ int vd_tess_destroy(vd_tess* t) {
   cudaSetDevice(t->device);
   if (t->stream) cudaStreamSynchronize(t->stream);
   t->d_order.release();
+  t->d_planes.release();
   t->d_gen.release(); t->d_in.release(); t->d_tmp3.release();
   t->d_flags.release(); t->d_pos.release();
   t->d_bin_of.release(); t->d_bin_count.release(); t->d_bin_start.release(); t->d_cursor.release();
@@ -712,11 +718,24 @@ int vd_tess_destroy(vd_tess* t) {
   return VD_OK;
 }
 
-static int add_wall(vd_tess* t, const Wall& w) {
+static int add_wall(vd_tess* t, const Wall& w, const double* planes = nullptr) {
   if (w.id > VD_WALL_ID_MAX) return fail(t, VD_EINVAL, "Wall ID must be <= %d", VD_WALL_ID_MAX);
   if ((int)t->walls.size() >= kMaxWalls) return fail(t, VD_EINVAL, "at most %d walls", kMaxWalls);
   VD_CK(t, cudaSetDevice(t->device));
-  t->walls.push_back(w);
+  if (w.kind == kWallPolyhedron) {
+    if ((int)(t->planes.size() / 6) + w.np > kMaxWallPlanes)
+      return fail(t, VD_EINVAL, "at most %d polyhedron planes in all walls", kMaxWallPlanes);
+    Wall wp = w;
+    wp.p0 = (int)(t->planes.size() / 6);
+    t->planes.insert(t->planes.end(), planes, planes + 6 * (size_t)w.np);
+    VD_CK(t, t->d_planes.ensure(t->planes.size(), t->stream));
+    VD_CK(t, cudaMemcpyAsync(t->d_planes.p, t->planes.data(), t->planes.size() * sizeof(double),
+                             cudaMemcpyHostToDevice, t->stream));
+    VD_CK(t, cudaStreamSynchronize(t->stream));
+    t->walls.push_back(wp);
+  } else {
+    t->walls.push_back(w);
+  }
   // prune_outside_generators (tessellation.rs:175-194)
   if (t->ngen == 0) return VD_OK;
   const size_t before = t->ngen;
@@ -757,9 +776,82 @@ int vd_tess_add_wall_sphere(vd_tess* t, const double center[3], double radius, i
   return add_wall(t, w);
 }
 
+// an axis normalised as CylinderGeometry/ConeGeometry/TorusGeometry::new do
+// (wall_3d.rs:124-128, 194-198, 285-289)
+static void unit_axis(const double axis[3], double out[3]) {
+  const double len = std::sqrt(axis[0] * axis[0] + axis[1] * axis[1] + axis[2] * axis[2]);
+  if (len == 0.0) {
+    out[0] = 0.0;
+    out[1] = 0.0;
+    out[2] = 1.0;
+  } else {
+    for (int a = 0; a < 3; ++a) out[a] = axis[a] / len;
+  }
+}
+
+int vd_tess_add_wall_cylinder(vd_tess* t, const double center[3], const double axis[3], double radius, int id) {
+  if (!t || !center || !axis) return VD_EINVAL;
+  Wall w;
+  memset(&w, 0, sizeof(w));
+  w.kind = kWallCylinder;
+  w.id = id;
+  w.r = radius;
+  for (int a = 0; a < 3; ++a) w.a[a] = center[a];
+  unit_axis(axis, w.n);
+  return add_wall(t, w);
+}
+
+int vd_tess_add_wall_cone(vd_tess* t, const double tip[3], const double axis[3], double angle, int id) {
+  if (!t || !tip || !axis) return VD_EINVAL;
+  Wall w;
+  memset(&w, 0, sizeof(w));
+  w.kind = kWallCone;
+  w.id = id;
+  w.r = angle;
+  // the reference evaluates angle.cos(), .sin(), .tan() with the host libm on
+  // every call; they are evaluated here once, with the same libm
+  w.ca = std::cos(angle);
+  w.sa = std::sin(angle);
+  w.ta = std::tan(angle);
+  for (int a = 0; a < 3; ++a) w.a[a] = tip[a];
+  unit_axis(axis, w.n);
+  return add_wall(t, w);
+}
+
+int vd_tess_add_wall_torus(vd_tess* t, const double center[3], const double axis[3], double major_radius,
+                           double minor_radius, int id) {
+  if (!t || !center || !axis) return VD_EINVAL;
+  Wall w;
+  memset(&w, 0, sizeof(w));
+  w.kind = kWallTorus;
+  w.id = id;
+  w.r = major_radius;
+  w.r2 = minor_radius;
+  for (int a = 0; a < 3; ++a) w.a[a] = center[a];
+  unit_axis(axis, w.n);
+  return add_wall(t, w);
+}
+
+int vd_tess_add_wall_polyhedron(vd_tess* t, const double* points, const double* normals, int nplanes, int id) {
+  if (!t || nplanes < 0 || (nplanes > 0 && (!points || !normals))) return VD_EINVAL;
+  Wall w;
+  memset(&w, 0, sizeof(w));
+  w.kind = kWallPolyhedron;
+  w.id = id;
+  w.np = nplanes;
+  std::vector<double> pl(6 * (size_t)nplanes);
+  for (int k = 0; k < nplanes; ++k)
+    for (int a = 0; a < 3; ++a) {
+      pl[6 * k + a] = points[3 * k + a];
+      pl[6 * k + 3 + a] = normals[3 * k + a];
+    }
+  return add_wall(t, w, pl.data());
+}
+
 int vd_tess_clear_walls(vd_tess* t) {
   if (!t) return VD_EINVAL;
   t->walls.clear();
+  t->planes.clear();
   return VD_OK;
 }
 

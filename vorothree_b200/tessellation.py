@@ -7,6 +7,8 @@ Names, argument meanings and error behaviour follow the reference crate
 * ``Algorithm3DGrid``                   -- src/algorithm/algo_3d_grid.rs:10-95
 * ``Wall``, ``WALL_ID_MAX``             -- src/wall/mod.rs:8-49 (id > -1000 is an error)
 * ``PlaneGeometry``, ``SphereGeometry`` -- src/wall/wall_3d.rs:8-101
+* ``CylinderGeometry``, ``ConeGeometry``, ``TorusGeometry``,
+  ``ConvexPolyhedronGeometry``          -- src/wall/wall_3d.rs:107-365, 462-708
 * ``Cell3DFaces``                       -- src/cell/cell_3d_faces.rs:22-270
 * ``Tessellation``                      -- src/tessellation.rs:13-527
 
@@ -16,6 +18,7 @@ numpy arrays.
 from __future__ import annotations
 
 import ctypes as C
+import math
 from dataclasses import dataclass
 from typing import Callable, List, Optional, Sequence
 
@@ -73,14 +76,124 @@ class SphereGeometry:
         return False
 
 
+class CylinderGeometry:
+    """Infinite cylinder wall (wall_3d.rs:107-174); the valid region is inside.
+    ``axis`` is normalised on the device side as the reference's constructor does."""
+
+    def __init__(self, center: Sequence[float], axis: Sequence[float], radius: float):
+        self.center = [float(v) for v in center]
+        self.axis = [float(v) for v in axis]
+        self.radius = float(radius)
+
+    def is_planar(self) -> bool:
+        return False
+
+
+class ConeGeometry:
+    """Infinite cone wall (wall_3d.rs:177-262): apex ``tip``, ``axis`` pointing
+    into the cone, half-angle ``angle`` in radians; the valid region is inside."""
+
+    def __init__(self, tip: Sequence[float], axis: Sequence[float], angle: float):
+        self.tip = [float(v) for v in tip]
+        self.axis = [float(v) for v in axis]
+        self.angle = float(angle)
+
+    def is_planar(self) -> bool:
+        return False
+
+
+class TorusGeometry:
+    """Torus wall (wall_3d.rs:265-365); the valid region is inside the tube."""
+
+    def __init__(self, center: Sequence[float], axis: Sequence[float], major_radius: float,
+                 minor_radius: float):
+        self.center = [float(v) for v in center]
+        self.axis = [float(v) for v in axis]
+        self.major_radius = float(major_radius)
+        self.minor_radius = float(minor_radius)
+
+    def is_planar(self) -> bool:
+        return False
+
+
+class ConvexPolyhedronGeometry:
+    """Convex polyhedron wall (wall_3d.rs:462-708): the intersection of the
+    half-spaces behind planes (point, normal pointing OUT of the valid
+    region).  The ``new_*`` constructors build the regular solids exactly as
+    the reference's do (same arithmetic, in IEEE double)."""
+
+    def __init__(self, points, normals):
+        p = np.asarray(points, np.float64).reshape(-1)
+        n = np.asarray(normals, np.float64).reshape(-1)
+        if p.size != n.size or p.size % 3 != 0:
+            raise ValueError("Points and normals must have same length and be multiple of 3")
+        self.points = p.reshape(-1, 3)
+        self.normals = n.reshape(-1, 3)
+
+    def is_planar(self) -> bool:
+        return True
+
+    @classmethod
+    def _regular(cls, center, base, dist, normalise=True):
+        pts, nrm = [], []
+        for b in base:
+            nx, ny, nz = float(b[0]), float(b[1]), float(b[2])
+            if normalise:
+                ln = math.sqrt(nx * nx + ny * ny + nz * nz)
+                nx, ny, nz = nx / ln, ny / ln, nz / ln
+            nrm.append([nx, ny, nz])
+            pts.append([center[0] + nx * dist, center[1] + ny * dist, center[2] + nz * dist])
+        return cls(pts, nrm)
+
+    @classmethod
+    def new_tetrahedron(cls, center, radius: float):
+        base = [[-1.0, -1.0, -1.0], [-1.0, 1.0, 1.0], [1.0, -1.0, 1.0], [1.0, 1.0, -1.0]]
+        return cls._regular([float(c) for c in center], base, radius / 3.0)
+
+    @classmethod
+    def new_hexahedron(cls, center, radius: float):
+        base = [[1.0, 0.0, 0.0], [-1.0, 0.0, 0.0], [0.0, 1.0, 0.0], [0.0, -1.0, 0.0], [0.0, 0.0, 1.0],
+                [0.0, 0.0, -1.0]]
+        return cls._regular([float(c) for c in center], base, radius / math.sqrt(3.0), normalise=False)
+
+    @classmethod
+    def new_octahedron(cls, center, radius: float):
+        base = [[x, y, z] for x in (-1.0, 1.0) for y in (-1.0, 1.0) for z in (-1.0, 1.0)]
+        return cls._regular([float(c) for c in center], base, radius / math.sqrt(3.0))
+
+    @classmethod
+    def new_dodecahedron(cls, center, radius: float):
+        phi = (1.0 + math.sqrt(5.0)) / 2.0
+        xi = math.sqrt((5.0 + 2.0 * math.sqrt(5.0)) / 15.0)
+        base = [[0.0, phi, 1.0], [0.0, -phi, 1.0], [0.0, phi, -1.0], [0.0, -phi, -1.0],
+                [1.0, 0.0, phi], [1.0, 0.0, -phi], [-1.0, 0.0, phi], [-1.0, 0.0, -phi],
+                [phi, 1.0, 0.0], [phi, -1.0, 0.0], [-phi, 1.0, 0.0], [-phi, -1.0, 0.0]]
+        return cls._regular([float(c) for c in center], base, radius * xi)
+
+    @classmethod
+    def new_icosahedron(cls, center, radius: float):
+        phi = (1.0 + math.sqrt(5.0)) / 2.0
+        xi = math.sqrt((5.0 + 2.0 * math.sqrt(5.0)) / 15.0)
+        ip = 1.0 / phi
+        base = [[x, y, z] for x in (-1.0, 1.0) for y in (-1.0, 1.0) for z in (-1.0, 1.0)]
+        base += [[0.0, y * phi, z * ip] for y in (-1.0, 1.0) for z in (-1.0, 1.0)]
+        base += [[x * ip, 0.0, z * phi] for x in (-1.0, 1.0) for z in (-1.0, 1.0)]
+        base += [[x * phi, y * ip, 0.0] for x in (-1.0, 1.0) for y in (-1.0, 1.0)]
+        return cls._regular([float(c) for c in center], base, radius * xi)
+
+
+WALL_GEOMETRIES = (PlaneGeometry, SphereGeometry, CylinderGeometry, ConeGeometry, TorusGeometry,
+                   ConvexPolyhedronGeometry)
+
+
 class Wall:
     """A wall geometry with an id <= WALL_ID_MAX (the reference panics otherwise)."""
 
     def __init__(self, id: int, geometry):
         if id > WALL_ID_MAX:
             raise ValueError(f"Wall ID must be <= {WALL_ID_MAX}")
-        if not isinstance(geometry, (PlaneGeometry, SphereGeometry)):
-            raise TypeError("only PlaneGeometry and SphereGeometry walls are supported")
+        if not isinstance(geometry, WALL_GEOMETRIES):
+            raise TypeError("unsupported wall geometry")
         self._id = int(id)
         self.geometry = geometry
 
@@ -336,13 +449,30 @@ class Tessellation:
 
     def add_wall(self, wall: Wall):
         g = wall.geometry
+        L, h, wid = self._L, self._h, wall.id()
         if isinstance(g, PlaneGeometry):
             p = np.asarray(g.point, np.float64)
             n = np.asarray(g.normal, np.float64)
-            self._ck(self._L.vd_tess_add_wall_plane(self._h, _dp(p), _dp(n), wall.id()))
-        else:
+            self._ck(L.vd_tess_add_wall_plane(h, _dp(p), _dp(n), wid))
+        elif isinstance(g, SphereGeometry):
             c = np.asarray(g.center, np.float64)
-            self._ck(self._L.vd_tess_add_wall_sphere(self._h, _dp(c), g.radius, wall.id()))
+            self._ck(L.vd_tess_add_wall_sphere(h, _dp(c), g.radius, wid))
+        elif isinstance(g, CylinderGeometry):
+            c = np.asarray(g.center, np.float64)
+            a = np.asarray(g.axis, np.float64)
+            self._ck(L.vd_tess_add_wall_cylinder(h, _dp(c), _dp(a), g.radius, wid))
+        elif isinstance(g, ConeGeometry):
+            c = np.asarray(g.tip, np.float64)
+            a = np.asarray(g.axis, np.float64)
+            self._ck(L.vd_tess_add_wall_cone(h, _dp(c), _dp(a), g.angle, wid))
+        elif isinstance(g, TorusGeometry):
+            c = np.asarray(g.center, np.float64)
+            a = np.asarray(g.axis, np.float64)
+            self._ck(L.vd_tess_add_wall_torus(h, _dp(c), _dp(a), g.major_radius, g.minor_radius, wid))
+        else:
+            p = np.ascontiguousarray(g.points, np.float64)
+            n = np.ascontiguousarray(g.normals, np.float64)
+            self._ck(L.vd_tess_add_wall_polyhedron(h, _dp(p), _dp(n), len(p), wid))
         self.walls.append(wall)
 
     def clear_walls(self):
