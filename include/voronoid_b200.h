@@ -108,6 +108,25 @@ int vd_tess_calculate(vd_tess* t);
  * the reference's per-cell map (tessellation.rs:223-229) restricted to the
  * range.  VD_EINVAL unless begin <= end <= count_generators. */
 int vd_tess_calculate_range(vd_tess* t, size_t begin, size_t end);
+/* Tessellation::calculate_sealed (tessellation.rs:234-318): calculate, then
+ * every cell on a curved wall (sphere, cylinder, cone, torus) is clipped with
+ * the wall's tangent plane at each face neighbour on the same wall, when its
+ * own generator lies on that plane's valid side.  Fills the seal log. */
+int vd_tess_calculate_sealed(vd_tess* t);
+/* Tessellation::prune_boundaries (tessellation.rs:323-385): for every cell on
+ * a curved wall and every distinct neighbour on the same wall, the vertices
+ * the cell's wall faces share with its faces towards that neighbour
+ * (Cell::shared_vertices, cell_3d_faces.rs:536-565).  Fills the prune logs;
+ * the cells are unchanged. */
+int vd_tess_prune_boundaries(vd_tess* t);
+/* seal_log (tessellation.rs:19): (cell, neighbour, wall id) per seal clip
+ * that changed a cell, in cell order; *n = number of int32 values.  Call
+ * with out = NULL for the size.  Cleared by calculate. */
+int vd_tess_seal_log(vd_tess* t, int32_t* out, size_t* n);
+/* prune_log / prune_pos_log (tessellation.rs:20-21): (cell, neighbour, wall
+ * id, vertex count) per entry and the vertices' xyz; *n_entries and
+ * *n_positions count int32 and double values.  NULL buffers query sizes. */
+int vd_tess_prune_log(vd_tess* t, int32_t* entries, size_t* n_entries, double* positions, size_t* n_positions);
 /* Tessellation::relax (tessellation.rs:482-495), on the device */
 int vd_tess_relax(vd_tess* t);
 /* Tessellation::count_cells (tessellation.rs:503-505) */

@@ -47,6 +47,14 @@ def lib():
     L.vdo_add_wall_torus.argtypes = [vp, d3, d3, C.c_double, C.c_double, C.c_int]
     L.vdo_add_wall_polyhedron.argtypes = [vp, d3, d3, C.c_int, C.c_int]
     L.vdo_regular_polyhedron.argtypes = [C.c_int, d3, C.c_double, d3, d3]
+    L.vdo_calculate_sealed.argtypes = [vp, C.c_int]
+    L.vdo_prune_boundaries.argtypes = [vp]
+    for nm in ("seal_log", "prune_log", "prune_pos_log"):
+        getattr(L, f"vdo_{nm}_len").restype = C.c_size_t
+        getattr(L, f"vdo_{nm}_len").argtypes = [vp]
+    L.vdo_get_seal_log.argtypes = [vp, C.POINTER(C.c_int32)]
+    L.vdo_get_prune_log.argtypes = [vp, C.POINTER(C.c_int32)]
+    L.vdo_get_prune_pos_log.argtypes = [vp, d3]
     L.vdo_clear_walls.argtypes = [vp]
     L.vdo_set_generators.restype = C.c_size_t
     L.vdo_set_generators.argtypes = [vp, d3, C.c_size_t]
@@ -253,6 +261,30 @@ class OracleTessellation:
 
     def calculate_range(self, begin: int, end: int, nthreads: int = 0):
         lib().vdo_calculate_range(self._h, int(begin), int(end), int(nthreads))
+
+    def calculate_sealed(self, nthreads: int = 0):
+        lib().vdo_calculate_sealed(self._h, int(nthreads))
+
+    def prune_boundaries(self):
+        lib().vdo_prune_boundaries(self._h)
+
+    def seal_log(self):
+        n = int(lib().vdo_seal_log_len(self._h))
+        out = np.zeros(max(n, 1), np.int32)
+        lib().vdo_get_seal_log(self._h, out.ctypes.data_as(C.POINTER(C.c_int32)))
+        return out[:n]
+
+    def prune_log(self):
+        n = int(lib().vdo_prune_log_len(self._h))
+        out = np.zeros(max(n, 1), np.int32)
+        lib().vdo_get_prune_log(self._h, out.ctypes.data_as(C.POINTER(C.c_int32)))
+        return out[:n]
+
+    def prune_pos_log(self):
+        n = int(lib().vdo_prune_pos_log_len(self._h))
+        out = np.zeros(max(n, 1), np.float64)
+        lib().vdo_get_prune_pos_log(self._h, out.ctypes.data_as(C.POINTER(C.c_double)))
+        return out[:n]
 
     def relax(self):
         lib().vdo_relax(self._h)

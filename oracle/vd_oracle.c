@@ -522,6 +522,10 @@ struct vdo_tess {
   size_t* bin_members;
   vdo_cell* cells; size_t ncells;
   uint64_t counters[VDO_NCOUNTERS];
+  /* seal_log, prune_log, prune_pos_log (tessellation.rs:19-21) */
+  int32_t* seal_log; size_t nseal, cap_seal;
+  int32_t* prune_log; size_t nprune, cap_prune;
+  double* prune_pos; size_t nprune_pos, cap_prune_pos;
 };
 
 static int cmp_offset(const void* a, const void* b) {
@@ -575,6 +579,7 @@ void vdo_destroy(vdo_tess* t) {
   if (!t) return;
   free_cells(t);
   free(t->order); free(t->gen); free(t->bin_of); free(t->bin_start); free(t->bin_members);
+  free(t->seal_log); free(t->prune_log); free(t->prune_pos);
   free(t);
 }
 
@@ -843,6 +848,8 @@ static void compute_cell(const vdo_tess* t, size_t i, vdo_cell* cell, scratch_t*
 }
 
 void vdo_calculate_range(vdo_tess* t, size_t begin, size_t end, int nthreads) {
+  /* calculate clears the logs (tessellation.rs:214-216) */
+  t->nseal = 0; t->nprune = 0; t->nprune_pos = 0;
   free_cells(t);
   t->ncells = t->ngen;
   t->cells = (vdo_cell*)calloc(t->ncells ? t->ncells : 1, sizeof(vdo_cell));
@@ -874,6 +881,197 @@ void vdo_calculate_range(vdo_tess* t, size_t begin, size_t end, int nthreads) {
 }
 
 void vdo_calculate(vdo_tess* t, int nthreads) { vdo_calculate_range(t, 0, t->ngen, nthreads); }
+
+/* ------------------------------------------------------------------ */
+/* calculate_sealed / prune_boundaries (tessellation.rs:234-385)        */
+/* ------------------------------------------------------------------ */
+/* WallGeometry::is_planar: planes and convex polyhedra (wall_3d.rs:44-46, 710-712) */
+static int wall_planar(const wall_t* w) { return w->kind == 0 || w->kind == 5; }
+
+static int has_id(const int32_t* a, size_t n, int32_t x) {
+  for (size_t k = 0; k < n; ++k)
+    if (a[k] == x) return 1;
+  return 0;
+}
+
+/* a cell's neighbours (face neighbours in [0, count), face order; distinct
+ * only when `dedup`) and its curved walls: distinct face neighbour ids whose
+ * first wall with that id (walls.iter().find) is not planar
+ * (tessellation.rs:242-261, 333-353) */
+static void cell_topology(const vdo_tess* t, const vdo_cell* c, size_t count, int dedup, int32_t* nb,
+                          size_t* nnb, int32_t* cw, size_t* ncw) {
+  *nnb = 0;
+  *ncw = 0;
+  for (size_t f = 0; f < c->nf; ++f) {
+    int32_t x = c->fn[f];
+    if (x >= 0 && (size_t)x < count) {
+      if (!dedup || !has_id(nb, *nnb, x)) nb[(*nnb)++] = x;
+    } else {
+      for (int w = 0; w < t->nwalls; ++w) {
+        if (t->walls[w].id != x) continue;
+        if (!wall_planar(&t->walls[w]) && !has_id(cw, *ncw, x)) cw[(*ncw)++] = x;
+        break;
+      }
+    }
+  }
+}
+
+static void log_push_i(int32_t** a, size_t* n, size_t* cap, int32_t x) {
+  if (*n == *cap) {
+    *cap = *cap ? 2 * *cap : 64;
+    *a = (int32_t*)realloc(*a, *cap * sizeof(int32_t));
+  }
+  (*a)[(*n)++] = x;
+}
+
+static void log_push_d(double** a, size_t* n, size_t* cap, double x) {
+  if (*n == *cap) {
+    *cap = *cap ? 2 * *cap : 64;
+    *a = (double*)realloc(*a, *cap * sizeof(double));
+  }
+  (*a)[(*n)++] = x;
+}
+
+typedef struct {
+  int32_t* nb; size_t* nnb;  /* per cell, at most nf entries from offset[i] */
+  int32_t* cw; size_t* ncw;
+  size_t* off;
+} topo_t;
+
+static void topo_build(const vdo_tess* t, int dedup, topo_t* T) {
+  size_t count = t->ngen, tot = 0;
+  T->off = (size_t*)malloc((count + 1) * sizeof(size_t));
+  for (size_t i = 0; i < count; ++i) { T->off[i] = tot; tot += t->cells[i].nf; }
+  T->off[count] = tot;
+  T->nb = (int32_t*)malloc((tot ? tot : 1) * sizeof(int32_t));
+  T->cw = (int32_t*)malloc((tot ? tot : 1) * sizeof(int32_t));
+  T->nnb = (size_t*)malloc((count ? count : 1) * sizeof(size_t));
+  T->ncw = (size_t*)malloc((count ? count : 1) * sizeof(size_t));
+  for (size_t i = 0; i < count; ++i)
+    cell_topology(t, &t->cells[i], count, dedup, T->nb + T->off[i], &T->nnb[i], T->cw + T->off[i], &T->ncw[i]);
+}
+
+static void topo_free(topo_t* T) { free(T->nb); free(T->cw); free(T->nnb); free(T->ncw); free(T->off); }
+
+/* Tessellation::calculate_sealed (tessellation.rs:234-318): calculate, then
+ * clip every cell on a curved wall with the wall's tangent plane at each
+ * neighbour on the same wall, when its own generator lies on the plane's
+ * valid side; the topology is taken before any cell changes */
+void vdo_calculate_sealed(vdo_tess* t, int nthreads) {
+  vdo_calculate(t, nthreads);
+  size_t count = t->ngen;
+  topo_t T;
+  topo_build(t, 0, &T);
+  scratch_t s;
+  memset(&s, 0, sizeof(s));
+  for (size_t i = 0; i < count; ++i) {
+    if (T.ncw[i] == 0) continue;
+    const double* g = &t->gen[3 * i];
+    const int32_t* nb = T.nb + T.off[i];
+    for (size_t q = 0; q < T.nnb[i]; ++q) {
+      size_t j = (size_t)nb[q];
+      for (int w = 0; w < t->nwalls; ++w) {
+        const wall_t* W = &t->walls[w];
+        if (wall_planar(W) || !has_id(T.cw + T.off[i], T.ncw[i], W->id) || !has_id(T.cw + T.off[j], T.ncw[j], W->id))
+          continue;
+        double p[3 * VDO_MAX_PLANES], n[3 * VDO_MAX_PLANES];
+        int np = wall_cut(W, &t->gen[3 * j], p, n);
+        for (int k = 0; k < np; ++k) {
+          double dot = 0.0;
+          for (int d = 0; d < 3; ++d) dot += (g[d] - p[3 * k + d]) * n[3 * k + d];
+          if (dot <= 1e-9) {
+            double r2;
+            if (cell_clip(&t->cells[i], &p[3 * k], &n[3 * k], W->id, &s, NULL, &r2, NULL)) {
+              log_push_i(&t->seal_log, &t->nseal, &t->cap_seal, (int32_t)i);
+              log_push_i(&t->seal_log, &t->nseal, &t->cap_seal, (int32_t)j);
+              log_push_i(&t->seal_log, &t->nseal, &t->cap_seal, W->id);
+            }
+          }
+        }
+      }
+    }
+  }
+  scratch_free(&s);
+  topo_free(&T);
+}
+
+/* Cell::shared_vertices (cell_3d_faces.rs:536-565) */
+static size_t shared_vertices(const vdo_cell* c, int32_t a, int32_t b, double* out) {
+  size_t* av = (size_t*)malloc((c->nh ? c->nh : 1) * sizeof(size_t));
+  size_t* bv = (size_t*)malloc((c->nh ? c->nh : 1) * sizeof(size_t));
+  size_t na = 0, nbv = 0, off = 0, m = 0;
+  for (size_t f = 0; f < c->nf; ++f) {
+    size_t cnt = c->fc[f];
+    for (size_t k = 0; k < cnt; ++k) {
+      size_t v = c->fi[off + k];
+      if (c->fn[f] == a) {
+        size_t z = 0;
+        while (z < na && av[z] != v) ++z;
+        if (z == na) av[na++] = v;
+      }
+      if (c->fn[f] == b) {
+        size_t z = 0;
+        while (z < nbv && bv[z] != v) ++z;
+        if (z == nbv) bv[nbv++] = v;
+      }
+    }
+    off += cnt;
+  }
+  for (size_t x = 0; x < na; ++x) {
+    size_t z = 0;
+    while (z < nbv && bv[z] != av[x]) ++z;
+    if (z < nbv) {
+      memcpy(&out[3 * m], &c->v[3 * av[x]], 3 * sizeof(double));
+      ++m;
+    }
+  }
+  free(av);
+  free(bv);
+  return m;
+}
+
+/* Tessellation::prune_boundaries (tessellation.rs:323-385): for every cell
+ * on a curved wall and every distinct neighbour on the same wall, the
+ * vertices the cell's wall face shares with its face towards the neighbour */
+void vdo_prune_boundaries(vdo_tess* t) {
+  size_t count = t->ngen;
+  t->nprune = 0;
+  t->nprune_pos = 0;
+  topo_t T;
+  topo_build(t, 1, &T);
+  for (size_t i = 0; i < count; ++i) {
+    if (T.ncw[i] == 0) continue;
+    const vdo_cell* c = &t->cells[i];
+    double* sh = (double*)malloc((3 * c->nh + 3) * sizeof(double));
+    const int32_t* nb = T.nb + T.off[i];
+    for (size_t q = 0; q < T.nnb[i]; ++q) {
+      size_t j = (size_t)nb[q];
+      for (int w = 0; w < t->nwalls; ++w) {
+        const wall_t* W = &t->walls[w];
+        if (wall_planar(W) || !has_id(T.cw + T.off[i], T.ncw[i], W->id) || !has_id(T.cw + T.off[j], T.ncw[j], W->id))
+          continue;
+        size_t m = shared_vertices(c, W->id, (int32_t)j, sh);
+        if (m == 0) continue;
+        log_push_i(&t->prune_log, &t->nprune, &t->cap_prune, (int32_t)i);
+        log_push_i(&t->prune_log, &t->nprune, &t->cap_prune, (int32_t)j);
+        log_push_i(&t->prune_log, &t->nprune, &t->cap_prune, W->id);
+        log_push_i(&t->prune_log, &t->nprune, &t->cap_prune, (int32_t)m);
+        for (size_t k = 0; k < 3 * m; ++k) log_push_d(&t->prune_pos, &t->nprune_pos, &t->cap_prune_pos, sh[k]);
+      }
+    }
+    free(sh);
+  }
+  topo_free(&T);
+}
+
+size_t vdo_seal_log_len(const vdo_tess* t) { return t->nseal; }
+void vdo_get_seal_log(const vdo_tess* t, int32_t* out) { if (t->nseal) memcpy(out, t->seal_log, t->nseal * sizeof(int32_t)); }
+size_t vdo_prune_log_len(const vdo_tess* t) { return t->nprune; }
+void vdo_get_prune_log(const vdo_tess* t, int32_t* out) { if (t->nprune) memcpy(out, t->prune_log, t->nprune * sizeof(int32_t)); }
+size_t vdo_prune_pos_log_len(const vdo_tess* t) { return t->nprune_pos; }
+void vdo_get_prune_pos_log(const vdo_tess* t, double* out) {
+  if (t->nprune_pos) memcpy(out, t->prune_pos, t->nprune_pos * sizeof(double));
+}
 
 /* Tessellation::relax (tessellation.rs:482-495) */
 void vdo_relax(vdo_tess* t) {

@@ -66,6 +66,17 @@ void vdo_calculate(vdo_tess* t, int nthreads);
 /* calculate only cells [begin, end) (a bounded sample for timing) */
 void vdo_calculate_range(vdo_tess* t, size_t begin, size_t end, int nthreads);
 void vdo_relax(vdo_tess* t);
+/* Tessellation::calculate_sealed / prune_boundaries (tessellation.rs:234-385)
+ * and their logs: seal (cell, neighbour, wall id) triples; prune (cell,
+ * neighbour, wall id, vertex count) quadruples with the vertices' xyz */
+void vdo_calculate_sealed(vdo_tess* t, int nthreads);
+void vdo_prune_boundaries(vdo_tess* t);
+size_t vdo_seal_log_len(const vdo_tess* t);
+void vdo_get_seal_log(const vdo_tess* t, int32_t* out);
+size_t vdo_prune_log_len(const vdo_tess* t);
+void vdo_get_prune_log(const vdo_tess* t, int32_t* out);
+size_t vdo_prune_pos_log_len(const vdo_tess* t);
+void vdo_get_prune_pos_log(const vdo_tess* t, double* out);
 size_t vdo_count_generators(const vdo_tess* t);
 size_t vdo_count_cells(const vdo_tess* t);
 void vdo_get_generators(const vdo_tess* t, double* xyz);

@@ -111,3 +111,55 @@ def test_wall_filters(oracle_mod):
     h = pts[:, 2]
     rr = np.sqrt((pts[:, 0] - 5) ** 2 + (pts[:, 1] - 5) ** 2)
     assert kept == int(((h >= 0) & (rr <= h * math.tan(0.4))).sum())
+
+
+def sealed_pair(oracle_mod, walls, n=3000, seed=12):
+    pts = uniform(n, 0.0, 10.0, seed)
+    out = []
+    for sealed in (False, True):
+        t = oracle_mod.OracleTessellation([0, 0, 0], [10, 10, 10], 6, 6, 6)
+        t.set_generators(pts)
+        for kind, args in walls:
+            getattr(t, "add_wall_" + kind)(*args)
+        (t.calculate_sealed if sealed else t.calculate)(1)
+        out.append(t)
+    return out
+
+
+@pytest.mark.parametrize("walls", [
+    [("sphere", ([5, 5, 5], 4.5, WALL))],
+    [("cylinder", ([5, 5, 5], [0, 0.2, 1], 4.0, WALL)), ("plane", ([5, 5, 5], [1, 0, 0], WALL - 1))],
+    [("torus", ([5, 5, 5], [0, 0, 1], 3.0, 1.8, WALL))],
+])
+def test_calculate_sealed_structure(oracle_mod, walls):
+    """calculate_sealed only ever clips cells that touch a curved wall, with
+    a plane whose id is that wall's; the seal log lists each such clip."""
+    plain, sealed = sealed_pair(oracle_mod, walls)
+    pv, _, _ = plain.summaries()
+    sv, _, _ = sealed.summaries()
+    log = sealed.seal_log().reshape(-1, 3)
+    assert len(log) > 0
+    curved = {a[-1] for k, a in walls if k != "plane"}
+    assert set(log[:, 2]) <= curved
+    changed = set(np.nonzero(sv != pv)[0])
+    assert changed <= set(log[:, 0])
+    assert np.all(sv <= pv + 1e-12)
+    # every logged neighbour is a face neighbour of the cell before sealing
+    off, ids = plain.neighbors()
+    for i, j, _ in log[:50]:
+        assert j in ids[off[i]:off[i + 1]]
+    # calculate clears the log
+    sealed.calculate(1)
+    assert len(sealed.seal_log()) == 0
+
+
+def test_prune_boundaries_log(oracle_mod):
+    _, t = sealed_pair(oracle_mod, [("sphere", ([5, 5, 5], 4.5, WALL))])
+    t.prune_boundaries()
+    log = t.prune_log().reshape(-1, 4)
+    pos = t.prune_pos_log().reshape(-1, 3)
+    assert len(log) > 0 and log[:, 3].sum() == len(pos)
+    # the shared vertices lie on tangent planes of the sphere: just outside it
+    r = np.linalg.norm(pos - 5.0, axis=1)
+    assert np.all(r >= 4.5 - 1e-9) and np.all(r < 5.0)
+    assert set(log[:, 2]) == {WALL}

@@ -54,6 +54,10 @@ SIGNATURES = {
     "vd_tess_calculate": (C.c_int, [_vp]),
     "vd_tess_calculate_range": (C.c_int, [_vp, C.c_size_t, C.c_size_t]),
     "vd_tess_relax": (C.c_int, [_vp]),
+    "vd_tess_calculate_sealed": (C.c_int, [_vp]),
+    "vd_tess_prune_boundaries": (C.c_int, [_vp]),
+    "vd_tess_seal_log": (C.c_int, [_vp, _vp, _szp]),
+    "vd_tess_prune_log": (C.c_int, [_vp, _vp, _szp, _vp, _szp]),
     "vd_tess_count_cells": (C.c_int, [_vp, _szp]),
     "vd_tess_get_cell_summaries": (C.c_int, [_vp, _vp, _vp, _vp]),
     "vd_tess_total_faces": (C.c_int, [_vp, _i64p]),

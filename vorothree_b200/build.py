@@ -30,6 +30,7 @@ SOURCES = [
     ("vd_batch.cu", False),
     ("vd_server.cu", False),
     ("vd_cell.cu", False),
+    ("vd_seal.cu", False),
 ]
 
 

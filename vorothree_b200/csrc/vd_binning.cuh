@@ -346,6 +346,18 @@ __global__ void k_range_compact(const SortedGen* __restrict__ sorted, size_t n, 
     if (flags[k]) list[pos[k]] = (uint32_t)sorted[k].id;
 }
 
+// flags[i] = mask[i] != 0, and the flagged ids compacted in id order
+__global__ void k_nonzero_flags(const uint32_t* __restrict__ mask, size_t n, uint32_t* __restrict__ flags) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    flags[i] = mask[i] != 0u ? 1u : 0u;
+}
+
+__global__ void k_compact_ids(const uint32_t* __restrict__ flags, const uint32_t* __restrict__ pos, size_t n,
+                              uint32_t* __restrict__ out) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    if (flags[i]) out[pos[i]] = (uint32_t)i;
+}
+
 // cells outside a computed range read as empty (volume 0, centroid 0, no faces)
 __global__ void k_clear_cells(size_t n, double* __restrict__ vol, double* __restrict__ cen,
                               int32_t* __restrict__ nfaces, int32_t* __restrict__ nverts) {

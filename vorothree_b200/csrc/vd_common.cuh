@@ -126,4 +126,48 @@ struct WorkList {
   int ex_cap_v, ex_cap_f, ex_cap_h;
 };
 
+// The second pass of calculate_sealed and the pass of prune_boundaries
+// (tessellation.rs:234-385).  Both rebuild a cell (compute_cell), re-apply
+// the seal clips when the cells are sealed, then either finalize the cell
+// (seal) or log the vertices its curved-wall faces share with its
+// neighbours' faces (prune).
+struct SealLogRec {   // one clip of calculate_sealed
+  int32_t cell, seq, nbr, wall;
+};
+struct PruneRec {     // one (cell, neighbour, wall) entry of prune_boundaries
+  int32_t cell, seq, nbr, wall, count, pseq;
+};
+struct PrunePos {     // one shared vertex of a prune entry
+  int32_t cell, pseq;
+  double x, y, z;
+};
+
+struct SealArgs {
+  int mode;        // 1: seal and finalize; 2: prune (re-seal first when `sealed`)
+  int sealed;      // the current cells were sealed
+  uint32_t curved; // bit k: wall k is curved (not planar)
+  int fout;
+  // topology of the cells before sealing (calculate's result)
+  const int32_t* s_nf;
+  const int32_t* s_fnb;
+  const long long* s_pool_off;
+  const int32_t* s_pool_fnb;
+  const uint32_t* s_mask;   // bit k: wall k's id is a curved wall among the cell's faces
+  // topology of the current cells (prune)
+  const int32_t* c_nf;
+  const int32_t* c_fnb;
+  const long long* c_pool_off;
+  const int32_t* c_pool_fnb;
+  const uint32_t* c_mask;
+  // logs: records appended in any order, placed by (cell, seq) afterwards;
+  // per-cell counts are written only when the cell completes
+  SealLogRec* seal_rec;
+  PruneRec* prune_rec;
+  PrunePos* prune_pos;
+  unsigned int* rec_cursor;  // [0] seal / prune records, [1] positions
+  uint32_t rec_cap, pos_cap;
+  int32_t* cnt;    // per cell: log entries
+  int32_t* pcnt;   // per cell: prune positions
+};
+
 }  // namespace vd

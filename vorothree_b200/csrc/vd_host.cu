@@ -178,6 +178,21 @@ struct vd_tess {
   std::vector<DevBuf<uint32_t>> scan32;
   std::vector<DevBuf<long long>> scan64;
 
+  // calculate_sealed / prune_boundaries
+  bool sealed = false;
+  DevBuf<int32_t> d_s_nf, d_s_fnb, d_s_pool_fnb;
+  DevBuf<long long> d_s_pool_off;
+  DevBuf<uint32_t> d_s_mask, d_c_mask, d_sel;
+  DevBuf<SealLogRec> d_seal_rec;
+  DevBuf<PruneRec> d_prune_rec;
+  DevBuf<PrunePos> d_prune_posrec;
+  DevBuf<unsigned int> d_rec_cursor;
+  DevBuf<int32_t> d_lcnt, d_lpcnt;
+  DevBuf<long long> d_loff, d_lpoff;
+  DevBuf<int32_t> d_seal_log, d_prune_log;
+  DevBuf<double> d_prune_pos;
+  size_t nseal = 0, nprune = 0, nprune_pos = 0;
+
   // export buffers for get_cell
   DevBuf<double> d_ex_v;
   DevBuf<uint32_t> d_ex_fc, d_ex_fi;
@@ -597,6 +612,150 @@ int ensure_csr(vd_tess* t) {
   return VD_OK;
 }
 
+// bit k: wall k is curved (WallGeometry::is_planar false: every kind but
+// planes and convex polyhedra)
+uint32_t curved_bits(const vd_tess* t) {
+  uint32_t m = 0;
+  for (size_t k = 0; k < t->walls.size(); ++k)
+    if (t->walls[k].kind != kWallPlane && t->walls[k].kind != kWallPolyhedron) m |= 1u << k;
+  return m;
+}
+
+// bit k: the first wall with wall k's id is curved (walls.iter().find decides
+// whether a face's id counts as a curved wall, tessellation.rs:250-256)
+uint32_t first_curved_bits(const vd_tess* t) {
+  const uint32_t c = curved_bits(t);
+  uint32_t m = 0;
+  for (size_t k = 0; k < t->walls.size(); ++k) {
+    size_t f = 0;
+    while (t->walls[f].id != t->walls[k].id) ++f;
+    if ((c >> f) & 1u) m |= 1u << k;
+  }
+  return m;
+}
+
+// the ids of the cells whose mask is non-zero, in id order, into d_sel
+int select_cells(vd_tess* t, const uint32_t* d_mask, uint32_t* nsel) {
+  const size_t n = t->ngen;
+  cudaStream_t s = t->stream;
+  VD_CK(t, t->d_flags.ensure(n + 1, t->stream));
+  VD_CK(t, t->d_pos.ensure(n + 1, t->stream));
+  VD_CK(t, t->d_sel.ensure(n, t->stream));
+  if (n) {
+    k_nonzero_flags<<<grid_blocks(t, n, 256), 256, 0, s>>>(d_mask, n, t->d_flags.p);
+    g_launches++;
+    VD_CK(t, cudaGetLastError());
+  }
+  VD_CK(t, cudaMemsetAsync(t->d_flags.p + n, 0, sizeof(uint32_t), s));
+  int r = scan_excl<uint32_t, uint32_t>(t, t->d_flags.p, t->d_pos.p, n + 1, t->scan32);
+  if (r != VD_OK) return r;
+  if (n) {
+    k_compact_ids<<<grid_blocks(t, n, 256), 256, 0, s>>>(t->d_flags.p, t->d_pos.p, n, t->d_sel.p);
+    g_launches++;
+    VD_CK(t, cudaGetLastError());
+  }
+  uint32_t k = 0;
+  VD_CK(t, cudaMemcpyAsync(&k, t->d_pos.p + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  VD_CK(t, cudaStreamSynchronize(s));
+  *nsel = k;
+  return VD_OK;
+}
+
+// One seal or prune pass over the listed cells, with the fallbacks of
+// run_calculate: a longer search order for cells that walk off a truncated
+// one, the large-capacity kernel for polytopes that outgrow shared memory.
+int seal_pass(vd_tess* t, const SealArgs& A, const uint32_t* items, uint32_t nitems,
+              const WorkList* extra = nullptr) {
+  cudaStream_t s = t->stream;
+  if (nitems == 0) return VD_OK;
+  auto pass = [&](bool big, const uint32_t* list, uint32_t n, unsigned* novf, unsigned* ntab) -> int {
+    VD_CK(t, cudaMemsetAsync(t->d_ctl.p, 0, 3 * sizeof(unsigned int), s));
+    WorkList W;
+    memset(&W, 0, sizeof(W));
+    if (extra) W = *extra;
+    W.items = list;
+    W.nitems = n;
+    W.cursor = t->d_ctl.p + kCtlCursor;
+    W.ovf_list = t->d_list[0].p;
+    W.ovf_count = t->d_ctl.p + kCtlOvfCount;
+    W.tab_list = t->d_list[1].p;
+    W.tab_count = t->d_ctl.p + kCtlTabCount;
+    if (big) {
+      int r = ensure_big(t, n);
+      if (r != VD_OK) return r;
+      VD_CK(t, launch_seal_big(make_desc(t), W, A, t->d_big.p, (int)t->big_warps, s));
+    } else {
+      const ClipLaunchInfo& li = t->info64;
+      const size_t want = (n + li.warps_per_block - 1) / li.warps_per_block;
+      const int nblocks = (int)std::max<size_t>(1, std::min<size_t>(want, (size_t)t->num_sms * std::max(1, li.blocks_per_sm)));
+      VD_CK(t, launch_seal_fast(make_desc(t), W, A, nblocks, s));
+    }
+    g_launches++;
+    return read_ctl(t, novf, ntab);
+  };
+  // the input list lives in d_sel; overflow and table lists in d_list[0/1]
+  unsigned novf = 0, ntab = 0;
+  int r = pass(false, items, nitems, &novf, &ntab);
+  for (int guard = 0; r == VD_OK && guard < 64 && (novf > 0 || ntab > 0); ++guard) {
+    if (ntab > 0) {
+      if (t->order_complete) return fail(t, VD_ECUDA, "search order exhausted on a complete table");
+      r = upload_order(t, std::max(1, t->order_k) * 2);
+      if (r != VD_OK) return r;
+      // both lists are consumed before the pass refills them: move them aside
+      VD_CK(t, cudaMemcpyAsync(t->d_list[2].p, t->d_list[1].p, ntab * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+      VD_CK(t, cudaMemcpyAsync(t->d_list[2].p + ntab, t->d_list[0].p, novf * sizeof(uint32_t),
+                               cudaMemcpyDeviceToDevice, s));
+      const unsigned n2 = ntab + novf;
+      r = pass(false, t->d_list[2].p, n2, &novf, &ntab);
+      continue;
+    }
+    VD_CK(t, cudaMemcpyAsync(t->d_list[2].p, t->d_list[0].p, novf * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+    r = pass(true, t->d_list[2].p, novf, &novf, &ntab);
+    if (r == VD_OK && novf > 0) return fail(t, VD_EOVERFLOW, "%u cells exceed the large polytope capacity", novf);
+  }
+  return r;
+}
+
+// per-cell counts -> offsets (n + 1 entries, total at [n])
+int count_offsets(vd_tess* t, DevBuf<int32_t>& cnt, DevBuf<long long>& off, size_t* total) {
+  const size_t n = t->ngen;
+  VD_CK(t, off.ensure(n + 1, t->stream));
+  VD_CK(t, cudaMemsetAsync(cnt.p + n, 0, sizeof(int32_t), t->stream));
+  int r = scan_excl<int32_t, long long>(t, cnt.p, off.p, n + 1, t->scan64);
+  if (r != VD_OK) return r;
+  long long tot = 0;
+  VD_CK(t, cudaMemcpyAsync(&tot, off.p + n, sizeof(long long), cudaMemcpyDeviceToHost, t->stream));
+  VD_CK(t, cudaStreamSynchronize(t->stream));
+  *total = (size_t)tot;
+  return VD_OK;
+}
+
+SealArgs seal_args(vd_tess* t, int mode) {
+  SealArgs A;
+  memset(&A, 0, sizeof(A));
+  A.mode = mode;
+  A.sealed = t->sealed ? 1 : 0;
+  A.curved = curved_bits(t);
+  A.fout = t->fout;
+  A.s_nf = t->d_s_nf.p;
+  A.s_fnb = t->d_s_fnb.p;
+  A.s_pool_off = t->d_s_pool_off.p;
+  A.s_pool_fnb = t->d_s_pool_fnb.p;
+  A.s_mask = t->d_s_mask.p;
+  A.c_nf = t->d_nf.p;
+  A.c_fnb = t->d_fnb.p;
+  A.c_pool_off = t->d_pool_off.p;
+  A.c_pool_fnb = t->d_pool_fnb.p;
+  A.c_mask = t->d_c_mask.p;
+  A.seal_rec = t->d_seal_rec.p;
+  A.prune_rec = t->d_prune_rec.p;
+  A.prune_pos = t->d_prune_posrec.p;
+  A.rec_cursor = t->d_rec_cursor.p;
+  A.cnt = t->d_lcnt.p;
+  A.pcnt = t->d_lpcnt.p;
+  return A;
+}
+
 int check_ready(vd_tess* t) {
   if (!t) return VD_EINVAL;
   if (!t->calculated) return fail(t, VD_ESTATE, "no results: call vd_tess_calculate first");
@@ -631,6 +790,7 @@ int vd_tess_create(const double bmin[3], const double bmax[3], int nx, int ny, i
   e = clip_fp64_info(&t->info64);
   if (e == cudaSuccess) e = clip_mixed_info(&t->infomx);
   if (e == cudaSuccess) e = clip_med_setup(&t->infomed);
+  if (e == cudaSuccess) e = seal_setup();
   if (e != cudaSuccess) {
     const std::string m = cudaGetErrorString(e);
     vd_tess_destroy(t);
@@ -697,6 +857,11 @@ int vd_tess_destroy(vd_tess* t) {
   if (t->stream) cudaStreamSynchronize(t->stream);
   t->d_order.release();
   t->d_planes.release();
+  t->d_s_nf.release(); t->d_s_fnb.release(); t->d_s_pool_fnb.release(); t->d_s_pool_off.release();
+  t->d_s_mask.release(); t->d_c_mask.release(); t->d_sel.release();
+  t->d_seal_rec.release(); t->d_prune_rec.release(); t->d_prune_posrec.release(); t->d_rec_cursor.release();
+  t->d_lcnt.release(); t->d_lpcnt.release(); t->d_loff.release(); t->d_lpoff.release();
+  t->d_seal_log.release(); t->d_prune_log.release(); t->d_prune_pos.release();
   t->d_gen.release(); t->d_in.release(); t->d_tmp3.release();
   t->d_flags.release(); t->d_pos.release();
   t->d_bin_of.release(); t->d_bin_count.release(); t->d_bin_start.release(); t->d_cursor.release();
@@ -988,6 +1153,8 @@ int vd_tess_calculate(vd_tess* t) {
   VD_CK(t, cudaSetDevice(t->device));
   t->calculated = false;
   t->csr_valid = false;
+  t->sealed = false;
+  t->nseal = t->nprune = t->nprune_pos = 0;
   int r = run_calculate(t);
   if (r != VD_OK) return r;
   t->ncells = t->ngen;
@@ -1005,12 +1172,147 @@ int vd_tess_calculate_range(vd_tess* t, size_t begin, size_t end) {
   t->calculated = false;
   t->csr_valid = false;
   const size_t range[2] = {begin, end};
+  t->sealed = false;
+  t->nseal = t->nprune = t->nprune_pos = 0;
   int r = run_calculate(t, nullptr, nullptr, range);
   if (r != VD_OK) return r;
   t->ncells = t->ngen;
   t->range_begin = begin;
   t->range_end = end;
   t->calculated = true;
+  return VD_OK;
+}
+
+int vd_tess_calculate_sealed(vd_tess* t) {
+  int r = vd_tess_calculate(t);
+  if (r != VD_OK) return r;
+  const size_t n = t->ngen;
+  cudaStream_t s = t->stream;
+  // the topology before any cell changes (tessellation.rs:242-261)
+  unsigned long long pool_used = 0;
+  VD_CK(t, cudaMemcpyAsync(&pool_used, t->d_pool_cursor.p, sizeof(pool_used), cudaMemcpyDeviceToHost, s));
+  VD_CK(t, cudaStreamSynchronize(s));
+  VD_CK(t, t->d_s_nf.ensure(n, t->stream));
+  VD_CK(t, t->d_s_fnb.ensure(n * (size_t)t->fout, t->stream));
+  VD_CK(t, t->d_s_pool_off.ensure(n, t->stream));
+  VD_CK(t, t->d_s_pool_fnb.ensure(std::max<unsigned long long>(pool_used, 1), t->stream));
+  VD_CK(t, t->d_s_mask.ensure(n, t->stream));
+  if (n) {
+    VD_CK(t, cudaMemcpyAsync(t->d_s_nf.p, t->d_nf.p, n * sizeof(int32_t), cudaMemcpyDeviceToDevice, s));
+    VD_CK(t, cudaMemcpyAsync(t->d_s_fnb.p, t->d_fnb.p, n * (size_t)t->fout * sizeof(int32_t),
+                             cudaMemcpyDeviceToDevice, s));
+    VD_CK(t, cudaMemcpyAsync(t->d_s_pool_off.p, t->d_pool_off.p, n * sizeof(long long), cudaMemcpyDeviceToDevice, s));
+    if (pool_used)
+      VD_CK(t, cudaMemcpyAsync(t->d_s_pool_fnb.p, t->d_pool_fnb.p, pool_used * sizeof(int32_t),
+                               cudaMemcpyDeviceToDevice, s));
+  }
+  VD_CK(t, launch_curved_mask(t->d_s_nf.p, t->d_s_fnb.p, t->d_s_pool_off.p, t->d_s_pool_fnb.p, t->fout,
+                              (uint32_t)n, make_desc(t), first_curved_bits(t), t->d_s_mask.p,
+                              grid_blocks(t, n, 256), s));
+  g_launches++;
+  uint32_t nsel = 0;
+  r = select_cells(t, t->d_s_mask.p, &nsel);
+  if (r != VD_OK) return r;
+  // logs: at most one entry per (face, curved wall) of a selected cell;
+  // entries of an attempt that a larger pass redoes repeat, so twice that
+  const uint32_t cap = (uint32_t)std::min<size_t>((size_t)2 * nsel * t->fout * (size_t)std::max<int>(1, __builtin_popcount(curved_bits(t))) + 1024, 1u << 30);
+  VD_CK(t, t->d_seal_rec.ensure(cap, t->stream));
+  VD_CK(t, t->d_rec_cursor.ensure(2, t->stream));
+  VD_CK(t, t->d_lcnt.ensure(n + 1, t->stream));
+  VD_CK(t, cudaMemsetAsync(t->d_rec_cursor.p, 0, 2 * sizeof(unsigned int), s));
+  VD_CK(t, cudaMemsetAsync(t->d_lcnt.p, 0, (n + 1) * sizeof(int32_t), s));
+  SealArgs A = seal_args(t, 1);
+  A.rec_cap = cap;
+  r = seal_pass(t, A, t->d_sel.p, nsel);
+  if (r != VD_OK) return r;
+  unsigned int used[2];
+  VD_CK(t, cudaMemcpyAsync(used, t->d_rec_cursor.p, sizeof(used), cudaMemcpyDeviceToHost, s));
+  VD_CK(t, cudaStreamSynchronize(s));
+  if (used[0] > cap) return fail(t, VD_ENOMEM, "seal log exceeds its buffer (%u records)", used[0]);
+  size_t total = 0;
+  r = count_offsets(t, t->d_lcnt, t->d_loff, &total);
+  if (r != VD_OK) return r;
+  VD_CK(t, t->d_seal_log.ensure(3 * total, t->stream));
+  VD_CK(t, launch_seal_log_place(t->d_seal_rec.p, used[0], t->d_loff.p, t->d_seal_log.p,
+                                 grid_blocks(t, used[0], 256), s));
+  g_launches++;
+  VD_CK(t, cudaStreamSynchronize(s));
+  t->nseal = total;
+  t->sealed = true;
+  t->csr_valid = false;
+  return VD_OK;
+}
+
+int vd_tess_prune_boundaries(vd_tess* t) {
+  int r = check_ready(t);
+  if (r != VD_OK) return r;
+  const size_t n = t->ngen;
+  cudaStream_t s = t->stream;
+  VD_CK(t, t->d_c_mask.ensure(n, t->stream));
+  VD_CK(t, launch_curved_mask(t->d_nf.p, t->d_fnb.p, t->d_pool_off.p, t->d_pool_fnb.p, t->fout, (uint32_t)n,
+                              make_desc(t), first_curved_bits(t), t->d_c_mask.p, grid_blocks(t, n, 256), s));
+  g_launches++;
+  uint32_t nsel = 0;
+  r = select_cells(t, t->d_c_mask.p, &nsel);
+  if (r != VD_OK) return r;
+  const size_t per = (size_t)t->fout * (size_t)std::max<int>(1, __builtin_popcount(curved_bits(t)));
+  const uint32_t cap = (uint32_t)std::min<size_t>((size_t)nsel * per + 1024, 1u << 30);
+  const uint32_t pcap = (uint32_t)std::min<size_t>((size_t)nsel * per * 8 + 4096, 1u << 30);
+  VD_CK(t, t->d_prune_rec.ensure(cap, t->stream));
+  VD_CK(t, t->d_prune_posrec.ensure(pcap, t->stream));
+  VD_CK(t, t->d_rec_cursor.ensure(2, t->stream));
+  VD_CK(t, t->d_lcnt.ensure(n + 1, t->stream));
+  VD_CK(t, t->d_lpcnt.ensure(n + 1, t->stream));
+  VD_CK(t, cudaMemsetAsync(t->d_rec_cursor.p, 0, 2 * sizeof(unsigned int), s));
+  VD_CK(t, cudaMemsetAsync(t->d_lcnt.p, 0, (n + 1) * sizeof(int32_t), s));
+  VD_CK(t, cudaMemsetAsync(t->d_lpcnt.p, 0, (n + 1) * sizeof(int32_t), s));
+  SealArgs A = seal_args(t, 2);
+  A.rec_cap = cap;
+  A.pos_cap = pcap;
+  r = seal_pass(t, A, t->d_sel.p, nsel);
+  if (r != VD_OK) return r;
+  unsigned int used[2];
+  VD_CK(t, cudaMemcpyAsync(used, t->d_rec_cursor.p, sizeof(used), cudaMemcpyDeviceToHost, s));
+  VD_CK(t, cudaStreamSynchronize(s));
+  if (used[0] > cap || used[1] > pcap) return fail(t, VD_ENOMEM, "prune log exceeds its buffer");
+  size_t total = 0, ptotal = 0;
+  r = count_offsets(t, t->d_lcnt, t->d_loff, &total);
+  if (r != VD_OK) return r;
+  r = count_offsets(t, t->d_lpcnt, t->d_lpoff, &ptotal);
+  if (r != VD_OK) return r;
+  VD_CK(t, t->d_prune_log.ensure(4 * total, t->stream));
+  VD_CK(t, t->d_prune_pos.ensure(3 * ptotal, t->stream));
+  VD_CK(t, launch_prune_log_place(t->d_prune_rec.p, used[0], t->d_prune_posrec.p, used[1], t->d_loff.p,
+                                  t->d_lpoff.p, t->d_prune_log.p, t->d_prune_pos.p,
+                                  grid_blocks(t, std::max(used[0], used[1]), 256), s));
+  g_launches++;
+  VD_CK(t, cudaStreamSynchronize(s));
+  t->nprune = total;
+  t->nprune_pos = ptotal;
+  return VD_OK;
+}
+
+int vd_tess_seal_log(vd_tess* t, int32_t* out, size_t* n) {
+  if (!t || !n) return VD_EINVAL;
+  *n = 3 * t->nseal;
+  if (out && t->nseal) {
+    VD_CK(t, cudaMemcpyAsync(out, t->d_seal_log.p, 3 * t->nseal * sizeof(int32_t), cudaMemcpyDeviceToHost, t->stream));
+    VD_CK(t, cudaStreamSynchronize(t->stream));
+  }
+  return VD_OK;
+}
+
+int vd_tess_prune_log(vd_tess* t, int32_t* entries, size_t* n_entries, double* positions, size_t* n_positions) {
+  if (!t || !n_entries || !n_positions) return VD_EINVAL;
+  *n_entries = 4 * t->nprune;
+  *n_positions = 3 * t->nprune_pos;
+  if (entries && t->nprune)
+    VD_CK(t, cudaMemcpyAsync(entries, t->d_prune_log.p, 4 * t->nprune * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                             t->stream));
+  if (positions && t->nprune_pos)
+    VD_CK(t, cudaMemcpyAsync(positions, t->d_prune_pos.p, 3 * t->nprune_pos * sizeof(double),
+                             cudaMemcpyDeviceToHost, t->stream));
+  VD_CK(t, cudaStreamSynchronize(t->stream));
   return VD_OK;
 }
 
@@ -1140,7 +1442,17 @@ int vd_tess_get_cell(vd_tess* t, size_t i, int32_t* n_vertices, int32_t* n_faces
   memcpy(st, t->timings, sizeof(st));
   unsigned long long sf[2] = {t->fallback[0], t->fallback[1]};
   const uint32_t cell = (uint32_t)i;
-  r = run_calculate(t, &ex, &cell);
+  if (t->sealed) {
+    // the sealed polytope: rebuilt with the seal clips, nothing logged
+    VD_CK(t, t->d_sel.ensure(std::max<size_t>(t->ngen, 1), t->stream));
+    VD_CK(t, cudaMemcpyAsync(t->d_sel.p, &cell, sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+    SealArgs A = seal_args(t, 1);
+    A.cnt = nullptr;
+    A.rec_cap = 0;
+    r = seal_pass(t, A, t->d_sel.p, 1, &ex);
+  } else {
+    r = run_calculate(t, &ex, &cell);
+  }
   memcpy(t->counters, saved, sizeof(saved));
   memcpy(t->timings, st, sizeof(st));
   t->fallback[0] = sf[0];

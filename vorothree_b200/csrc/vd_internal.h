@@ -49,6 +49,20 @@ void set_thread_error(const char* msg);
 // buffer growth is served from the pool without going to the driver.
 cudaError_t reserve_pool(size_t bytes, cudaStream_t s);
 
+// second passes of calculate_sealed / prune_boundaries (vd_seal.cu)
+cudaError_t seal_setup();
+cudaError_t launch_seal_fast(const TessDesc& T, const WorkList& W, const SealArgs& A, int nblocks, cudaStream_t s);
+cudaError_t launch_seal_big(const TessDesc& T, const WorkList& W, const SealArgs& A, void* scratch, int nwarps,
+                            cudaStream_t s);
+cudaError_t launch_curved_mask(const int32_t* nf, const int32_t* fnb, const long long* pool_off,
+                               const int32_t* pool_fnb, int fout, uint32_t n, const TessDesc& T,
+                               uint32_t first_curved, uint32_t* mask, int nblocks, cudaStream_t s);
+cudaError_t launch_seal_log_place(const SealLogRec* rec, uint32_t nrec, const long long* off, int32_t* out,
+                                  int nblocks, cudaStream_t s);
+cudaError_t launch_prune_log_place(const PruneRec* rec, uint32_t nrec, const PrunePos* pos, uint32_t npos,
+                                   const long long* off, const long long* poff, int32_t* out, double* out_pos,
+                                   int nblocks, cudaStream_t s);
+
 // Mixed path (vd_kernels_mixed.cu)
 cudaError_t clip_mixed_info(ClipLaunchInfo* info);
 cudaError_t launch_clip_mixed_fast(const TessDesc& T, const WorkList& W, int nblocks, bool count,

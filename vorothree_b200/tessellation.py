@@ -543,6 +543,41 @@ class Tessellation:
             raise ValueError(f"bad cell range [{begin}, {end})")
         self._ck(self._L.vd_tess_calculate_range(self._h, int(begin), int(end)))
 
+    def calculate_sealed(self):
+        """Tessellation::calculate_sealed (tessellation.rs:234-318)."""
+        self._ck(self._L.vd_tess_calculate_sealed(self._h))
+
+    def prune_boundaries(self):
+        """Tessellation::prune_boundaries (tessellation.rs:323-385)."""
+        self._ck(self._L.vd_tess_prune_boundaries(self._h))
+
+    @property
+    def seal_log(self) -> np.ndarray:
+        """(cell, neighbour, wall id) triples, flat, as the reference's seal_log."""
+        n = C.c_size_t()
+        self._ck(self._L.vd_tess_seal_log(self._h, None, C.byref(n)))
+        out = np.zeros(max(n.value, 1), np.int32)
+        self._ck(self._L.vd_tess_seal_log(self._h, _vp(out), C.byref(n)))
+        return out[:n.value]
+
+    def _prune(self):
+        ne, npos = C.c_size_t(), C.c_size_t()
+        self._ck(self._L.vd_tess_prune_log(self._h, None, C.byref(ne), None, C.byref(npos)))
+        e = np.zeros(max(ne.value, 1), np.int32)
+        p = np.zeros(max(npos.value, 1), np.float64)
+        self._ck(self._L.vd_tess_prune_log(self._h, _vp(e), C.byref(ne), _vp(p), C.byref(npos)))
+        return e[:ne.value], p[:npos.value]
+
+    @property
+    def prune_log(self) -> np.ndarray:
+        """(cell, neighbour, wall id, vertex count) quadruples, flat."""
+        return self._prune()[0]
+
+    @property
+    def prune_pos_log(self) -> np.ndarray:
+        """xyz of the logged shared vertices, flat."""
+        return self._prune()[1]
+
     def relax(self):
         self._ck(self._L.vd_tess_relax(self._h))
 
