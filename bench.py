@@ -613,9 +613,64 @@ def run_blobs(args):
     return 0
 
 
+def run_sealed(args):
+    """Config: the 1,048,576 uniform generators with a sphere wall r = 0.45 at
+    the centre, computed by calculate and by calculate_sealed (the second pass
+    re-clips the cells on the curved wall with their neighbours' tangent
+    planes, tessellation.rs:234-318); the oracle times the same on the host."""
+    import torch
+    import vorothree_b200 as v
+    torch.cuda.set_device(0)
+    pts = uniform(N_GEN, 0)
+    wall = v.Wall(v.WALL_ID_MAX, v.SphereGeometry([0.5, 0.5, 0.5], 0.45))
+    t = v.Tessellation(v.BoundingBox([0, 0, 0], [1, 1, 1]), v.Algorithm3DGrid(GRID, GRID, GRID))
+    t.add_wall(wall)
+    kept = t.set_generators(pts)
+    res = {}
+    for name, fn in (("calculate", t.calculate), ("calculate_sealed", t.calculate_sealed)):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        ms = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            fn()
+            torch.cuda.synchronize()
+            ms.append(1e3 * (time.perf_counter() - t0))
+        res[name] = statistics.mean(ms)
+    nseal = len(t.seal_log) // 3
+    t0 = time.perf_counter()
+    t.prune_boundaries()
+    prune_ms = 1e3 * (time.perf_counter() - t0)
+    nprune = len(t.prune_log) // 4
+    t.close()
+    line = {"metric": "3D cells/s, calculate_sealed", "workload": "sealed", "unit": "cells/s",
+            "value": kept / (res["calculate_sealed"] / 1e3), "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "dtype": "f64", "data": "synthetic (seeded PCG64)",
+            "config": {"generators": N_GEN, "kept": kept, "grid": [GRID] * 3, "wall": "sphere r=0.45 at the centre",
+                       "timing": "host wall clock around each call with a device synchronize"},
+            "ms": {"calculate": res["calculate"], "calculate_sealed": res["calculate_sealed"],
+                   "seal_pass": res["calculate_sealed"] - res["calculate"], "prune_boundaries": prune_ms},
+            "seal_clips": nseal, "prune_entries": nprune}
+    if not args.no_cpu_baseline:
+        from oracle.oracle import OracleTessellation
+        o = OracleTessellation([0, 0, 0], [1, 1, 1], GRID, GRID, GRID)
+        o.add_wall_sphere([0.5, 0.5, 0.5], 0.45, v.WALL_ID_MAX)
+        o.set_generators(pts)
+        nthreads = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        o.calculate_sealed(nthreads)
+        cdt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": kept / cdt, "unit": "cells/s", "cores": nthreads, "kind": "port",
+                                "sample": f"all {kept} cells; calculate on {nthreads} threads, the seal pass "
+                                          f"on one ({cdt:.2f} s wall)"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--workload", choices=["uniform", "batched", "blobs", "serving"], default="uniform",
+    ap.add_argument("--workload", choices=["uniform", "batched", "blobs", "serving", "sealed"], default="uniform",
                     help="uniform: 1M uniform generators (the headline); batched: many tessellations "
                          "+ Lloyd steps; blobs: 4M clustered generators with a sphere wall")
     ap.add_argument("--ntess", type=int, default=4096)
@@ -654,6 +709,8 @@ def main():
         return run_blobs(args)
     if args.workload == "serving":
         return run_serving(args)
+    if args.workload == "sealed":
+        return run_sealed(args)
     return run_ours(args)
 
 

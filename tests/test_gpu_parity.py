@@ -300,3 +300,41 @@ def test_calculate_range_shards(oracle_mod, precision):
         g.calculate_range(0, n + 1)
     with pytest.raises(ValueError):
         g.calculate_range(4, 3)
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+@pytest.mark.parametrize("jitter", [0.0, 1e-13, 1e-9, 1e-6])
+def test_degenerate_lattices_bitwise(oracle_mod, jitter, precision):
+    """Generators on (or within `jitter` of) a cubic lattice: bisector planes
+    pass exactly through existing vertices, so vertices fall inside the 1e-9
+    band, intersection vertices coincide and lid segments share endpoints --
+    the degenerate cases of clip_with_scratch.  The GPU must still match the
+    oracle bit for bit."""
+    n = 9
+    ax = (np.arange(n) + 0.5) / n
+    pts = np.array([[x, y, z] for z in ax for y in ax for x in ax])
+    if jitter:
+        rng = np.random.Generator(np.random.PCG64(77))
+        pts = pts + rng.uniform(-jitter, jitter, size=pts.shape)
+    g = gpu_tess([0, 0, 0], [1, 1, 1], (5, 5, 5), pts, precision=precision)
+    o = oracle_tess(oracle_mod, [0, 0, 0], [1, 1, 1], (5, 5, 5), pts)
+    assert_same(g, o, sample_cells=16)
+    vol, _, _ = g.summaries()
+    assert abs(vol.sum() - 1.0) < 1e-9
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_degenerate_duplicates_and_planes(oracle_mod, precision):
+    """Repeated generators, generators on the box faces and on a wall plane."""
+    import vorothree_b200 as v
+    rng = np.random.Generator(np.random.PCG64(78))
+    base = rng.uniform(0, 1, size=(400, 3))
+    on_faces = base[:60].copy()
+    on_faces[:20, 0] = 0.0
+    on_faces[20:40, 1] = 1.0
+    on_faces[40:, 2] = 0.5
+    pts = np.concatenate([base, base[:50], on_faces])
+    walls = [v.Wall(WALL, v.PlaneGeometry([0.5, 0.5, 0.5], [0, 0, 1]))]
+    g = gpu_tess([0, 0, 0], [1, 1, 1], (6, 6, 6), pts, walls, precision=precision)
+    o = oracle_tess(oracle_mod, [0, 0, 0], [1, 1, 1], (6, 6, 6), pts, walls)
+    assert_same(g, o, sample_cells=16)

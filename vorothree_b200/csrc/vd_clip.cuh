@@ -867,6 +867,15 @@ __device__ int compute_cell(const TessDesc& T, uint32_t i, WarpPoly<C>& P, PolyS
     // bins that can still open (R only shrinks), flattened: members of entry
     // e are candidates [start, start + cnt)
     const bool pot = valid && inr && be > bs && !(md2 > 4.0 * cur) && b2 <= 4.0 * cur;
+    if (!__any_sync(kFull, pot)) {
+      // no bin of this chunk can open (sparse regions, fine grids): only
+      // the end of the walk is decided here
+      const unsigned brk = __ballot_sync(kFull, valid && md2 > 4.0 * cur);
+      const int fbe = brk ? __ffs(brk) - 1 : 32;
+      if constexpr (C::COUNT) cnt_add(P, kCntOffsets, (unsigned long long)(fbe < 32 ? fbe + 1 : nvalid));
+      if (fbe < 32) done = true;
+      continue;
+    }
     const int cnt = pot ? (int)(be - bs) : 0;
     const int incl = warp_incl_scan(cnt);
     const int start = incl - cnt;
