@@ -125,13 +125,19 @@ def dist_env():
     return ws, rank, local
 
 
-def load_traffic(precision: str):
-    """DRAM bytes per clip-kernel launch from the committed ncu summary."""
+def load_profile(precision: str) -> dict:
+    """The committed ncu summary of the clip kernel (DRAM bytes per launch,
+    warp instructions per cell)."""
     p = os.path.join(ROOT, "profiles", f"clip_{precision}_uniform_1M.json")
     if not os.path.exists(p):
-        return None
+        return {}
     with open(p) as f:
-        return json.load(f).get("dram_bytes_per_launch")
+        return json.load(f)
+
+
+def load_traffic(precision: str):
+    """DRAM bytes per clip-kernel launch from the committed ncu summary."""
+    return load_profile(precision).get("dram_bytes_per_launch")
 
 
 def cpu_baseline(pts, nthreads: int, sample: int):
@@ -225,6 +231,24 @@ def e2e_leg(args, L, _lib, tess, pts):
         L.vd_host_free(b)
 
     return e2e, h2d, d2h
+
+
+def issue_roof(args, clip_ms: float, clk: dict):
+    """The roof that binds this kernel: instruction issue.  Achieved warp
+    instructions per second (the ncu count per cell of the committed profile
+    x cells / the clip kernel's event time) against one instruction per cycle
+    per SM sub-partition (4 per SM) at the sampled SM clock."""
+    import torch
+    per_cell = load_profile(args.precision).get("warp_instructions_per_cell")
+    mhz = clk.get("sm_mhz") or clk.get("sm_max_mhz")
+    if not per_cell or not mhz:
+        return None
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    achieved = per_cell * N_GEN / (clip_ms / 1e3) / 1e9
+    peak = sms * 4 * mhz * 1e6 / 1e9
+    return {"achieved": achieved, "peak": peak, "unit": "G warp-instructions/s", "frac": achieved / peak,
+            "note": "instruction issue, the roof this kernel meets (ncu: issue active ~72%); "
+                    "warp instructions per cell from the committed ncu profile"}
 
 
 def autotuned_leg(args, v, d_pts, flush):
@@ -371,7 +395,8 @@ def run_ours(args):
                          "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
                          "frac": achieved / peak.value,
                          "peak_source": "FP64 FMA-chain microbenchmark run live by bench.py on this GPU",
-                         "flops_per_launch": flops, "traffic": traffic},
+                         "flops_per_launch": flops, "traffic": traffic,
+                         "issue": issue_roof(args, clip, clk)},
             "e2e": None if e2e is None else {
                 "value": N_GEN / (e2e / 1e3) * ws, "unit": "cells/s", "ms_per_step": e2e,
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},

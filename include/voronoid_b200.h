@@ -222,15 +222,25 @@ int vd_host_free(void* ptr);
  * computes; the batch only shares the launches (no counterpart in the
  * reference, which computes one tessellation per call). */
 typedef struct vd_batch vd_batch;
-/* a wall of a batch member: kind 0 = PlaneGeometry (a = point, n = normal
- * into the valid region, normalised here as in wall_3d.rs:23-27),
- * kind 1 = SphereGeometry (a = centre, r = radius); id <= VD_WALL_ID_MAX */
+/* a wall of a batch member or a served request (the geometries of
+ * wall_3d.rs, normalised as their constructors do):
+ *   kind 0 PlaneGeometry      a = point, n = normal into the valid region
+ *   kind 1 SphereGeometry     a = centre, r = radius
+ *   kind 2 CylinderGeometry   a = centre, n = axis, r = radius
+ *   kind 3 ConeGeometry       a = tip, n = axis (into the cone), r = half-angle (radians)
+ *   kind 4 TorusGeometry      a = centre, n = axis, r = major radius, r2 = minor radius
+ *   kind 5 ConvexPolyhedronGeometry  points / normals [3 * nplanes], normals pointing out
+ * id <= VD_WALL_ID_MAX; the plane arrays are copied by the call that takes the wall */
 typedef struct {
   int kind;
   int id;
   double a[3];
   double n[3];
   double r;
+  double r2;
+  const double* points;
+  const double* normals;
+  int nplanes;
 } vd_wall_desc;
 int vd_batch_create(vd_batch** out);
 int vd_batch_destroy(vd_batch* b);

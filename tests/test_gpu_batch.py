@@ -132,3 +132,27 @@ def test_batch_dense_blob_overflow_tiers():
     b = build_batch(ms)
     for k, m in enumerate(ms):
         assert_member_equal(b, k, standalone(m))
+
+
+def test_batch_and_server_take_every_wall_kind():
+    """Batch members and served requests with cylinder, cone, torus and
+    polyhedron walls equal standalone tessellations bit for bit."""
+    import vorothree_b200 as v
+    P = v.ConvexPolyhedronGeometry
+    wallsets = [
+        [v.Wall(WALL, v.CylinderGeometry([5, 5, 5], [0.1, 0.0, 1.0], 4.0))],
+        [v.Wall(WALL, v.ConeGeometry([5, 5, 0.5], [0, 0, 1], 0.5))],
+        [v.Wall(WALL, v.TorusGeometry([5, 5, 5], [0, 1, 1], 3.0, 1.7))],
+        [v.Wall(WALL, P.new_icosahedron([5, 5, 5], 4.5)), v.Wall(WALL - 1, P.new_tetrahedron([5, 5, 5], 6.0))],
+    ]
+    ms = [([0, 0, 0], [10, 10, 10], (7, 7, 7), uniform(3000, 0, 10, 60 + k), w) for k, w in enumerate(wallsets)]
+    b = build_batch(ms)
+    srv = v.TessellationServer(slots=2, hbm_budget_bytes=4 << 30)
+    tickets = [srv.submit(v.BoundingBox(m[0], m[1]), m[2], m[3], m[4]) for m in ms]
+    for k, m in enumerate(ms):
+        t = standalone(m)
+        assert_member_equal(b, k, t)
+        vol, cen, nf = srv.take(tickets[k])
+        tv, tc, tn = t.summaries()
+        assert np.array_equal(vol, tv) and np.array_equal(cen, tc) and np.array_equal(nf, tn)
+    srv.close()

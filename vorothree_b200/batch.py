@@ -1,7 +1,7 @@
 """Many independent tessellations computed together (vd_batch_* C ABI).
 
 Each member is a reference Tessellation (bounds, Algorithm3DGrid
-resolution, plane/sphere walls, generators); the batch runs every member's
+resolution, walls of any kind, generators); the batch runs every member's
 binning and clipping in shared persistent launches and keeps Lloyd steps on
 the device.  Results per member equal what a standalone Tessellation with
 the same inputs returns.
@@ -14,31 +14,63 @@ from typing import List, Sequence
 import numpy as np
 
 from ._lib import VD_PREC_FP64, VD_PREC_MIXED, VoronoidError, load
-from .tessellation import BoundingBox, PlaneGeometry, SphereGeometry, Wall
+from .tessellation import (BoundingBox, ConeGeometry, CylinderGeometry, PlaneGeometry, SphereGeometry,
+                           TorusGeometry, Wall)
 
 
 class _WallDesc(C.Structure):
     _fields_ = [("kind", C.c_int), ("id", C.c_int), ("a", C.c_double * 3), ("n", C.c_double * 3),
-                ("r", C.c_double)]
+                ("r", C.c_double), ("r2", C.c_double), ("points", C.c_void_p), ("normals", C.c_void_p),
+                ("nplanes", C.c_int)]
 
 
-def _walls(walls: Sequence[Wall]):
-    arr = (_WallDesc * max(len(walls), 1))()
-    for k, w in enumerate(walls):
-        g = w.geometry
-        d = arr[k]
-        d.id = w.id()
-        if isinstance(g, PlaneGeometry):
-            d.kind = 0
-            d.a[:] = list(g.point)
-            d.n[:] = list(g.normal)
-        elif isinstance(g, SphereGeometry):
-            d.kind = 1
-            d.a[:] = list(g.center)
-            d.r = g.radius
-        else:
-            raise TypeError("only plane and sphere walls")
-    return arr
+class _Walls:
+    """vd_wall_desc array for a batch member or a request; keeps the
+    polyhedron plane arrays it points at alive while it lives."""
+
+    def __init__(self, walls: Sequence[Wall]):
+        self.arr = (_WallDesc * max(len(walls), 1))()
+        self.keep = []
+        for k, w in enumerate(walls):
+            g = w.geometry
+            d = self.arr[k]
+            d.id = w.id()
+            if isinstance(g, PlaneGeometry):
+                d.kind = 0
+                d.a[:] = list(g.point)
+                d.n[:] = list(g.normal)
+            elif isinstance(g, SphereGeometry):
+                d.kind = 1
+                d.a[:] = list(g.center)
+                d.r = g.radius
+            elif isinstance(g, CylinderGeometry):
+                d.kind = 2
+                d.a[:] = list(g.center)
+                d.n[:] = list(g.axis)
+                d.r = g.radius
+            elif isinstance(g, ConeGeometry):
+                d.kind = 3
+                d.a[:] = list(g.tip)
+                d.n[:] = list(g.axis)
+                d.r = g.angle
+            elif isinstance(g, TorusGeometry):
+                d.kind = 4
+                d.a[:] = list(g.center)
+                d.n[:] = list(g.axis)
+                d.r = g.major_radius
+                d.r2 = g.minor_radius
+            else:
+                d.kind = 5
+                p = np.ascontiguousarray(g.points, np.float64)
+                n = np.ascontiguousarray(g.normals, np.float64)
+                self.keep += [p, n]
+                d.points = p.ctypes.data
+                d.normals = n.ctypes.data
+                d.nplanes = len(p)
+
+
+def _walls(walls: Sequence[Wall]) -> _Walls:
+    return _Walls(walls)
 
 
 class TessellationBatch:
@@ -74,7 +106,7 @@ class TessellationBatch:
         wd = _walls(walls)
         d = C.POINTER(C.c_double)
         self._chk(self._L.vd_batch_add(self._h, mn.ctypes.data_as(d), mx.ctypes.data_as(d), int(grid[0]),
-                                       int(grid[1]), int(grid[2]), C.cast(wd, C.c_void_p), len(walls),
+                                       int(grid[1]), int(grid[2]), C.cast(wd.arr, C.c_void_p), len(walls),
                                        pts.ctypes.data_as(d), n, C.byref(idx)))
         self._n += 1
         return idx.value

@@ -195,6 +195,7 @@ struct vd_batch {
   int precision = VD_PREC_FP64;
   bool instrument = false;
   std::vector<Member> m;
+  std::vector<double> planes;  // plane table of the members' convex-polyhedron walls
   bool committed = false;
   bool calculated = false;
 
@@ -209,6 +210,7 @@ struct vd_batch {
   Buf<SortedGen> d_sorted;
   Buf<Offset> d_order;
   Buf<TessDesc> d_descs;
+  Buf<double> d_planes;
   Buf<int32_t> d_nf, d_nv, d_fnb, d_pool_fnb;
   Buf<uint8_t> d_status;
   Buf<long long> d_pool_off;
@@ -307,6 +309,10 @@ int upload_static(vd_batch* b) {
   for (int t = 0; t < nt; ++t)
     std::copy(b->m[t].order.begin(), b->m[t].order.end(), cat.begin() + order_off[t]);
   B_CK(b, cudaMemcpyAsync(b->d_order.p, cat.data(), total_order * sizeof(Offset), cudaMemcpyHostToDevice, b->stream));
+  B_CK(b, b->d_planes.ensure(std::max<size_t>(b->planes.size(), 1)));
+  if (!b->planes.empty())
+    B_CK(b, cudaMemcpyAsync(b->d_planes.p, b->planes.data(), b->planes.size() * sizeof(double),
+                            cudaMemcpyHostToDevice, b->stream));
   std::vector<TessDesc> d(nt);
   for (int t = 0; t < nt; ++t) {
     TessDesc& T = d[t];
@@ -315,6 +321,7 @@ int upload_static(vd_batch* b) {
     T.grid = M.g;
     T.nwalls = (int)M.walls.size();
     for (int k = 0; k < T.nwalls; ++k) T.walls[k] = M.walls[k];
+    T.planes = b->d_planes.p;
     T.order = b->d_order.p + order_off[t];
     T.norder = (int)M.order.size();
     T.order_complete = M.complete ? 1 : 0;
@@ -529,7 +536,7 @@ int vd_batch_destroy(vd_batch* b) {
   b->d_in_off.release(); b->d_total.release(); b->d_bin_off.release(); b->d_bin_of.release(); b->d_counts.release();
   b->d_start.release(); b->d_cursor.release(); b->d_ids.release(); b->d_ids_tmp.release(); b->d_big_list.release();
   b->d_list0.release(); b->d_list1.release(); b->d_list2.release(); b->d_list3.release(); b->d_sorted.release(); b->d_order.release();
-  b->d_descs.release(); b->d_nf.release(); b->d_nv.release(); b->d_fnb.release(); b->d_pool_fnb.release();
+  b->d_descs.release(); b->d_planes.release(); b->d_nf.release(); b->d_nv.release(); b->d_fnb.release(); b->d_pool_fnb.release();
   b->d_status.release(); b->d_pool_off.release(); b->d_ctl.release(); b->d_tess_flags.release();
   b->d_counters.release(); b->d_pool_cursor.release(); b->d_big.release();
   for (auto& p : b->scan_pool) p.release();
@@ -557,25 +564,9 @@ int vd_batch_add(vd_batch* b, const double bmin[3], const double bmax[3], int nx
     M.g.cs[a] = 1.0 / M.g.scale[a];
   }
   for (int k = 0; k < nwalls; ++k) {
-    const vd_wall_desc& d = walls[k];
-    if (d.id > VD_WALL_ID_MAX) return bfail(b, VD_EINVAL, "Wall ID must be <= %d", VD_WALL_ID_MAX);
     Wall w;
-    memset(&w, 0, sizeof(w));
-    w.kind = d.kind;
-    w.id = d.id;
-    for (int a = 0; a < 3; ++a) w.a[a] = d.a[a];
-    if (d.kind == 0) {  // PlaneGeometry::new (wall_3d.rs:23-27)
-      const double len = std::sqrt(d.n[0] * d.n[0] + d.n[1] * d.n[1] + d.n[2] * d.n[2]);
-      if (len == 0.0) {
-        w.n[2] = 1.0;
-      } else {
-        for (int a = 0; a < 3; ++a) w.n[a] = d.n[a] / len;
-      }
-    } else if (d.kind == 1) {
-      w.r = d.r;
-    } else {
-      return bfail(b, VD_EINVAL, "unknown wall kind %d", d.kind);
-    }
+    std::string err;
+    if (!wall_from_desc(walls[k], &w, &b->planes, &err)) return bfail(b, VD_EINVAL, "wall %d: %s", k, err.c_str());
     M.walls.push_back(w);
   }
   M.pts.assign(xyz, xyz + 3 * n);

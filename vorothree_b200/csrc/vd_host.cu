@@ -111,6 +111,21 @@ enum : int {
 
 }  // namespace
 
+namespace {
+// an axis normalised as CylinderGeometry/ConeGeometry/TorusGeometry::new do
+// (wall_3d.rs:124-128, 194-198, 285-289)
+static void unit_axis(const double axis[3], double out[3]) {
+  const double len = std::sqrt(axis[0] * axis[0] + axis[1] * axis[1] + axis[2] * axis[2]);
+  if (len == 0.0) {
+    out[0] = 0.0;
+    out[1] = 0.0;
+    out[2] = 1.0;
+  } else {
+    for (int a = 0; a < 3; ++a) out[a] = axis[a] / len;
+  }
+}
+}  // namespace
+
 namespace vd {
 void set_thread_error(const char* msg) { g_create_error = msg; }
 
@@ -124,6 +139,58 @@ cudaError_t reserve_pool(size_t bytes, cudaStream_t s) {
   e = cudaFreeAsync(p, s);
   if (e != cudaSuccess) return e;
   return cudaStreamSynchronize(s);
+}
+}  // namespace vd
+
+namespace vd {
+bool wall_from_desc(const vd_wall_desc& d, Wall* w, std::vector<double>* planes, std::string* err) {
+  memset(w, 0, sizeof(*w));
+  w->kind = d.kind;
+  w->id = d.id;
+  if (d.id > VD_WALL_ID_MAX) {
+    *err = "Wall ID must be <= " + std::to_string(VD_WALL_ID_MAX);
+    return false;
+  }
+  for (int a = 0; a < 3; ++a) w->a[a] = d.a[a];
+  switch (d.kind) {
+    case kWallPlane: {  // PlaneGeometry::new (wall_3d.rs:23-27)
+      const double len = std::sqrt(d.n[0] * d.n[0] + d.n[1] * d.n[1] + d.n[2] * d.n[2]);
+      if (len == 0.0) w->n[2] = 1.0;
+      else
+        for (int a = 0; a < 3; ++a) w->n[a] = d.n[a] / len;
+      return true;
+    }
+    case kWallSphere:
+      w->r = d.r;
+      return true;
+    case kWallCylinder:
+    case kWallCone:
+    case kWallTorus:
+      unit_axis(d.n, w->n);
+      w->r = d.r;
+      w->r2 = d.r2;
+      if (d.kind == kWallCone) {
+        w->ca = std::cos(d.r);
+        w->sa = std::sin(d.r);
+        w->ta = std::tan(d.r);
+      }
+      return true;
+    case kWallPolyhedron:
+      if (d.nplanes < 0 || (d.nplanes > 0 && (!d.points || !d.normals))) {
+        *err = "bad polyhedron planes";
+        return false;
+      }
+      w->np = d.nplanes;
+      w->p0 = (int)(planes->size() / 6);
+      for (int k = 0; k < d.nplanes; ++k) {
+        for (int a = 0; a < 3; ++a) planes->push_back(d.points[3 * k + a]);
+        for (int a = 0; a < 3; ++a) planes->push_back(d.normals[3 * k + a]);
+      }
+      return true;
+    default:
+      *err = "unknown wall kind " + std::to_string(d.kind);
+      return false;
+  }
 }
 }  // namespace vd
 
@@ -941,18 +1008,7 @@ int vd_tess_add_wall_sphere(vd_tess* t, const double center[3], double radius, i
   return add_wall(t, w);
 }
 
-// an axis normalised as CylinderGeometry/ConeGeometry/TorusGeometry::new do
-// (wall_3d.rs:124-128, 194-198, 285-289)
-static void unit_axis(const double axis[3], double out[3]) {
-  const double len = std::sqrt(axis[0] * axis[0] + axis[1] * axis[1] + axis[2] * axis[2]);
-  if (len == 0.0) {
-    out[0] = 0.0;
-    out[1] = 0.0;
-    out[2] = 1.0;
-  } else {
-    for (int a = 0; a < 3; ++a) out[a] = axis[a] / len;
-  }
-}
+
 
 int vd_tess_add_wall_cylinder(vd_tess* t, const double center[3], const double axis[3], double radius, int id) {
   if (!t || !center || !axis) return VD_EINVAL;

@@ -4,7 +4,10 @@
 #include <cuda_runtime.h>
 #include <cstddef>
 #include <cstdint>
+#include <string>
+#include <vector>
 
+#include "../../include/voronoid_b200.h"
 #include "vd_common.cuh"
 
 namespace vd {
@@ -40,6 +43,12 @@ cudaError_t launch_clip_mixed_fast_batched(const TessDesc* descs, const uint32_t
                                            const WorkList& W, int nblocks, bool count, cudaStream_t s);
 cudaError_t launch_clip_fp64_big_batched(const TessDesc* descs, const uint32_t* tess_off, int ntess,
                                          const WorkList& W, void* scratch, int nwarps, cudaStream_t s);
+
+// a device wall from a public wall descriptor (axis normalisation, the
+// cone's trigonometry on the host); a polyhedron's planes are appended to
+// `planes` (6 doubles each) and the wall records their offset.  Returns
+// false with a message for a bad descriptor.
+bool wall_from_desc(const vd_wall_desc& d, Wall* w, std::vector<double>* planes, std::string* err);
 
 // message returned by vd_last_error(NULL) on the calling thread
 void set_thread_error(const char* msg);

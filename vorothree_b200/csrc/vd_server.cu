@@ -39,6 +39,7 @@ struct Request {
   double bmin[3], bmax[3];
   int n[3];
   std::vector<vd_wall_desc> walls;
+  std::vector<std::vector<double>> wall_planes;  // owned copies of polyhedron planes (points then normals)
   std::vector<double> pts;
   size_t est_bytes = 0;
   Clock::time_point t_submit, t_start, t_done;
@@ -109,9 +110,19 @@ int sfail(vd_server* s, int code, const char* fmt, ...) {
 int run_request(vd_tess* t, int precision, Request& r) {
   int rc = vd_tess_reset(t, r.bmin, r.bmax, r.n[0], r.n[1], r.n[2]);
   if (rc == VD_OK) rc = vd_tess_set_precision(t, precision);
-  for (const vd_wall_desc& w : r.walls) {
-    if (rc != VD_OK) break;
-    rc = w.kind == 0 ? vd_tess_add_wall_plane(t, w.a, w.n, w.id) : vd_tess_add_wall_sphere(t, w.a, w.r, w.id);
+  for (size_t k = 0; k < r.walls.size() && rc == VD_OK; ++k) {
+    const vd_wall_desc& w = r.walls[k];
+    switch (w.kind) {
+      case 0: rc = vd_tess_add_wall_plane(t, w.a, w.n, w.id); break;
+      case 1: rc = vd_tess_add_wall_sphere(t, w.a, w.r, w.id); break;
+      case 2: rc = vd_tess_add_wall_cylinder(t, w.a, w.n, w.r, w.id); break;
+      case 3: rc = vd_tess_add_wall_cone(t, w.a, w.n, w.r, w.id); break;
+      case 4: rc = vd_tess_add_wall_torus(t, w.a, w.n, w.r, w.r2, w.id); break;
+      default: {
+        const std::vector<double>& pl = r.wall_planes[k];
+        rc = vd_tess_add_wall_polyhedron(t, pl.data(), pl.data() + 3 * w.nplanes, w.nplanes, w.id);
+      }
+    }
   }
   size_t kept = 0;
   if (rc == VD_OK) rc = vd_tess_set_generators(t, r.pts.data(), r.pts.size() / 3, &kept);
@@ -234,9 +245,12 @@ int vd_server_submit(vd_server* s, const double bmin[3], const double bmax[3], i
   if (!s || !bmin || !bmax || !ticket || (!xyz && n) || (nwalls > 0 && !walls) || nwalls < 0)
     return VD_EINVAL;
   if (nx <= 0 || ny <= 0 || nz <= 0) return sfail(s, VD_EINVAL, "grid resolution must be positive");
-  for (int k = 0; k < nwalls; ++k)
-    if (walls[k].id > VD_WALL_ID_MAX || (walls[k].kind != 0 && walls[k].kind != 1))
+  for (int k = 0; k < nwalls; ++k) {
+    const vd_wall_desc& w = walls[k];
+    if (w.id > VD_WALL_ID_MAX || w.kind < 0 || w.kind > 5 ||
+        (w.kind == 5 && (w.nplanes < 0 || (w.nplanes > 0 && (!w.points || !w.normals)))))
       return sfail(s, VD_EINVAL, "bad wall %d", k);
+  }
   auto r = std::make_shared<Request>();
   for (int a = 0; a < 3; ++a) {
     r->bmin[a] = bmin[a];
@@ -246,6 +260,15 @@ int vd_server_submit(vd_server* s, const double bmin[3], const double bmax[3], i
   r->n[1] = ny;
   r->n[2] = nz;
   r->walls.assign(walls, walls + nwalls);
+  r->wall_planes.resize(nwalls);
+  for (int k = 0; k < nwalls; ++k) {
+    vd_wall_desc& w = r->walls[k];
+    if (w.kind == 5 && w.nplanes > 0) {
+      r->wall_planes[k].assign(w.points, w.points + 3 * w.nplanes);
+      r->wall_planes[k].insert(r->wall_planes[k].end(), w.normals, w.normals + 3 * w.nplanes);
+    }
+    w.points = w.normals = nullptr;  // the request keeps its own copy
+  }
   r->pts.assign(xyz, xyz + 3 * n);
   r->est_bytes = estimate_bytes(n, (size_t)nx * ny * nz);
   if (r->est_bytes > s->budget) return sfail(s, VD_ENOMEM, "request needs %zu bytes, budget %zu", r->est_bytes, s->budget);

@@ -50,7 +50,7 @@ class TessellationServer:
         t = C.c_uint64()
         d = C.POINTER(C.c_double)
         self._chk(self._L.vd_server_submit(self._h, mn.ctypes.data_as(d), mx.ctypes.data_as(d), int(grid[0]),
-                                           int(grid[1]), int(grid[2]), C.cast(wd, C.c_void_p), len(walls),
+                                           int(grid[1]), int(grid[2]), C.cast(wd.arr, C.c_void_p), len(walls),
                                            pts.ctypes.data_as(d), pts.size // 3, C.byref(t)))
         return t.value
 
