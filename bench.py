@@ -40,7 +40,7 @@ GRID = 100
 METRIC = "3D cells/s @1M gens"
 WORKLOAD = "1,048,576 uniform generators in the unit cube, grid 100^3, no walls"
 
-# Algorithmic FP64 operations per counted event ("flop model").
+# Algorithmic FP64 operations per counted event (the flop model of the clip kernel).
 FLOPS_PER = {
     "classified": 8,      # (v-p).n: 3 sub, 3 mul, 2 add
     "candidates": 15,     # d = q-g, |d|^2, midpoint, 4R^2

@@ -155,3 +155,27 @@ def test_volume_sum_uniform(oracle_mod):
     t.calculate()
     vol, _, _ = t.summaries()
     assert abs(vol.sum() - 1000.0) < 1e-9 * 1000
+
+
+def test_interior_neighbours_match_delaunay(oracle_mod):
+    """Independent cross-check: for cells that touch no box face, the
+    Voronoi neighbour set is the Delaunay neighbour set of the generators
+    (scipy.spatial.Delaunay), for random general-position inputs."""
+    import numpy as np
+    from scipy.spatial import Delaunay
+    rng = np.random.Generator(np.random.PCG64(90))
+    pts = rng.uniform(0.0, 1.0, size=(3000, 3))
+    t = oracle_mod.OracleTessellation([0, 0, 0], [1, 1, 1], 14, 14, 14)
+    t.set_generators(pts)
+    t.calculate(1)
+    off, ids = t.neighbors()
+    tri = Delaunay(pts)
+    indptr, nb = tri.vertex_neighbor_vertices
+    checked = 0
+    for i in range(len(pts)):
+        mine = ids[off[i]:off[i + 1]]
+        if np.any(mine < 0):
+            continue
+        assert set(int(x) for x in mine) == set(int(x) for x in nb[indptr[i]:indptr[i + 1]]), i
+        checked += 1
+    assert checked > 1500
