@@ -203,6 +203,7 @@ struct vd_batch {
   uint32_t nbins = 0;       // bins of all members
   std::vector<uint32_t> h_in_off, h_bin_off, h_off;
   ClipLaunchInfo info64{}, infomx{}, infomed{};
+  int blocks64 = 0, blocksmx = 0;  // resident blocks per SM of the batched fast kernels
 
   Buf<double> d_in, d_gen, d_vol, d_cen, d_farea, d_pool_area;
   Buf<uint32_t> d_flags, d_pos, d_off, d_off_next, d_in_off, d_total, d_bin_off, d_bin_of, d_counts, d_start,
@@ -402,8 +403,7 @@ int clip_chain(vd_batch* b, const uint32_t* items, uint32_t nitems) {
   W.counters = b->d_counters.p;
   W.tess_flags = b->d_tess_flags.p;
   const bool mixed = b->precision == VD_PREC_MIXED;
-  const ClipLaunchInfo& li = mixed ? b->infomx : b->info64;
-  const int nblocks = std::max(1, b->num_sms * std::max(1, li.blocks_per_sm));
+  const int nblocks = std::max(1, b->num_sms * std::max(1, mixed ? b->blocksmx : b->blocks64));
   B_CK(b, mixed ? launch_clip_mixed_fast_batched(b->d_descs.p, b->d_off.p, nt, W, nblocks, b->instrument, s)
                 : launch_clip_fp64_fast_batched(b->d_descs.p, b->d_off.p, nt, W, nblocks, b->instrument, s));
   // medium capacity (FP64; the same decisions as both precisions)
@@ -512,8 +512,8 @@ int vd_batch_create(vd_batch** out) {
   if (e == cudaSuccess) e = clip_fp64_info(&b->info64);
   if (e == cudaSuccess) e = clip_mixed_info(&b->infomx);
   if (e == cudaSuccess) e = clip_med_setup(&b->infomed);
-  if (e == cudaSuccess) e = clip_fp64_batched_setup();
-  if (e == cudaSuccess) e = clip_mixed_batched_setup();
+  if (e == cudaSuccess) e = clip_fp64_batched_setup(&b->blocks64);
+  if (e == cudaSuccess) e = clip_mixed_batched_setup(&b->blocksmx);
   if (e == cudaSuccess) e = cudaEventCreate(&b->ev0);
   if (e == cudaSuccess) e = cudaEventCreate(&b->ev1);
   if (e != cudaSuccess) {

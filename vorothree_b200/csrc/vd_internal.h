@@ -35,8 +35,9 @@ cudaError_t launch_clip_med_batched(const TessDesc* descs, const uint32_t* tess_
                                     const WorkList& W, int nblocks, cudaStream_t s);
 
 // batched mode (descriptors in device memory; see clip_worker_batched)
-cudaError_t clip_fp64_batched_setup();
-cudaError_t clip_mixed_batched_setup();
+// *blocks_per_sm: resident blocks of the batched fast kernel
+cudaError_t clip_fp64_batched_setup(int* blocks_per_sm);
+cudaError_t clip_mixed_batched_setup(int* blocks_per_sm);
 cudaError_t launch_clip_fp64_fast_batched(const TessDesc* descs, const uint32_t* tess_off, int ntess,
                                           const WorkList& W, int nblocks, bool count, cudaStream_t s);
 cudaError_t launch_clip_mixed_fast_batched(const TessDesc* descs, const uint32_t* tess_off, int ntess,

@@ -12,6 +12,10 @@ namespace vd {
 // shared memory admits 7 blocks of 4 warps per SM; keep registers in step
 // (without the bound ptxas takes ~100 registers and only 4 blocks fit)
 constexpr int kFp64MinBlocks = 7;
+// the batched kernel (member lookup, descriptors in device memory) needs
+// more registers: measured fastest at 5 blocks (96 registers; 7 blocks:
+// -13%, 6: -12%, 4: -9%)
+constexpr int kBatchMinBlocks = 5;
 
 cudaError_t clip_fp64_info(ClipLaunchInfo* info) {
   info->smem_per_warp = sizeof(WarpPoly<FastCfg>);
@@ -55,10 +59,10 @@ cudaError_t launch_clip_fp64_fast_batched(const TessDesc* descs, const uint32_t*
   const size_t smem = sizeof(WarpPoly<FastCfg>) * kFastWarpsPerBlock;
   const size_t smemc = sizeof(WarpPoly<FastCfgCount>) * kFastWarpsPerBlock;
   if (count)
-    k_clip_fast_batched<FastCfgCount, kFastWarpsPerBlock, kFp64MinBlocks>
+    k_clip_fast_batched<FastCfgCount, kFastWarpsPerBlock, kBatchMinBlocks>
         <<<nblocks, kFastWarpsPerBlock * 32, smemc, s>>>(descs, tess_off, ntess, W);
   else
-    k_clip_fast_batched<FastCfg, kFastWarpsPerBlock, kFp64MinBlocks>
+    k_clip_fast_batched<FastCfg, kFastWarpsPerBlock, kBatchMinBlocks>
         <<<nblocks, kFastWarpsPerBlock * 32, smem, s>>>(descs, tess_off, ntess, W);
   return cudaGetLastError();
 }
@@ -70,14 +74,17 @@ cudaError_t launch_clip_fp64_big_batched(const TessDesc* descs, const uint32_t* 
   return cudaGetLastError();
 }
 
-cudaError_t clip_fp64_batched_setup() {
+cudaError_t clip_fp64_batched_setup(int* blocks_per_sm) {
   const size_t smem = sizeof(WarpPoly<FastCfg>) * kFastWarpsPerBlock;
   const size_t smemc = sizeof(WarpPoly<FastCfgCount>) * kFastWarpsPerBlock;
-  cudaError_t e = cudaFuncSetAttribute(k_clip_fast_batched<FastCfg, kFastWarpsPerBlock, kFp64MinBlocks>,
+  cudaError_t e = cudaFuncSetAttribute(k_clip_fast_batched<FastCfg, kFastWarpsPerBlock, kBatchMinBlocks>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_clip_fast_batched<FastCfgCount, kFastWarpsPerBlock, kFp64MinBlocks>,
-                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemc);
+  e = cudaFuncSetAttribute(k_clip_fast_batched<FastCfgCount, kFastWarpsPerBlock, kBatchMinBlocks>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemc);
+  if (e != cudaSuccess) return e;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      blocks_per_sm, k_clip_fast_batched<FastCfg, kFastWarpsPerBlock, kBatchMinBlocks>, kFastWarpsPerBlock * 32, smem);
 }
 
 constexpr int kMedWarpsPerBlock = 2;
