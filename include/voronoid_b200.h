@@ -36,6 +36,7 @@ extern "C" {
 #define VD_ETIMEOUT 4   /* a bounded device wait gave up */
 #define VD_ECUDA 5      /* CUDA runtime error / no device */
 #define VD_ESTATE 6     /* call out of order (e.g. results before calculate) */
+#define VD_EIO 7        /* a file could not be read (import_generators) */
 
 /* precision of the clipping path */
 #define VD_PREC_FP64 0  /* plain FP64, bitwise the reference's arithmetic */
@@ -89,6 +90,21 @@ int vd_tess_set_generators_device(vd_tess* t, const double* d_xyz, size_t n, siz
 /* Tessellation::set_generator (tessellation.rs:71-92): ignored when out of
  * range or outside a wall, as in the reference */
 int vd_tess_set_generator(vd_tess* t, size_t index, const double xyz[3]);
+/* Tessellation::read_generators (tessellation.rs:153-171): one generator per
+ * line of `text` (len bytes of UTF-8): an id, ignored, then x y z; a missing
+ * or unparsable coordinate reads 0.0 (Rust's str::parse::<f64> grammar), a
+ * line with no token is skipped.  The points then go through set_generators.
+ * VD_EINVAL, with nothing changed, when the bytes are not UTF-8 (a Rust &str
+ * always is). */
+int vd_tess_read_generators(vd_tess* t, const char* text, size_t len, size_t* n_kept);
+/* Tessellation::import_generators (tessellation.rs:126-148): the same for a
+ * file; VD_EIO when it cannot be read, VD_EINVAL when it is not UTF-8 (the
+ * reference returns the io::Error); nothing is changed then. */
+int vd_tess_import_generators(vd_tess* t, const char* path, size_t* n_kept);
+/* the parser of vd_tess_read_generators alone (host only, no device): writes
+ * min(cap, *n_points) points (AoS) to xyz; *n_points = points in the text.
+ * Errors: VD_EINVAL (message via vd_last_error(NULL)). */
+int vd_parse_generators(const char* text, size_t len, double* xyz, size_t cap, size_t* n_points);
 /* Tessellation::count_generators / generators (tessellation.rs:498-500,519-521) */
 int vd_tess_count_generators(const vd_tess* t, size_t* n);
 int vd_tess_get_generators(vd_tess* t, double* xyz);

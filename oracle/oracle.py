@@ -58,6 +58,10 @@ def lib():
     L.vdo_clear_walls.argtypes = [vp]
     L.vdo_set_generators.restype = C.c_size_t
     L.vdo_set_generators.argtypes = [vp, d3, C.c_size_t]
+    L.vdo_set_generator.restype = None
+    L.vdo_set_generator.argtypes = [vp, C.c_size_t, d3]
+    L.vdo_get_bins.restype = None
+    L.vdo_get_bins.argtypes = [vp, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]
     L.vdo_calculate.argtypes = [vp, C.c_int]
     L.vdo_calculate_range.argtypes = [vp, C.c_size_t, C.c_size_t, C.c_int]
     L.vdo_relax.argtypes = [vp]
@@ -206,6 +210,7 @@ class OracleTessellation:
         mn, pmn = _d(bmin)
         mx, pmx = _d(bmax)
         self._h = lib().vdo_create(pmn, pmx, int(nx), int(ny), int(nz))
+        self.nx, self.ny, self.nz = int(nx), int(ny), int(nz)
         if not self._h:
             raise ValueError("invalid grid resolution")
 
@@ -256,6 +261,10 @@ class OracleTessellation:
         a, pa = _d(np.asarray(xyz, np.float64).reshape(-1))
         return int(lib().vdo_set_generators(self._h, pa, a.size // 3))
 
+    def set_generator(self, index: int, xyz):
+        a, pa = _d(np.asarray(xyz, np.float64).reshape(3))
+        lib().vdo_set_generator(self._h, int(index), pa)
+
     def calculate(self, nthreads: int = 0):
         lib().vdo_calculate(self._h, int(nthreads))
 
@@ -300,6 +309,14 @@ class OracleTessellation:
         out = np.zeros(3 * n, np.float64)
         lib().vdo_get_generators(self._h, out.ctypes.data_as(C.POINTER(C.c_double)))
         return out
+
+    def bins(self):
+        """grid_bins as a list of id lists, in visit order."""
+        start = np.zeros(self.nx * self.ny * self.nz + 1, np.uint64)
+        mem = np.zeros(max(self.count_generators(), 1), np.uint64)
+        lib().vdo_get_bins(self._h, start.ctypes.data_as(C.POINTER(C.c_size_t)),
+                           mem.ctypes.data_as(C.POINTER(C.c_size_t)))
+        return [mem[start[b]:start[b + 1]].tolist() for b in range(len(start) - 1)]
 
     def bin_index(self, x, y, z) -> int:
         return int(lib().vdo_bin_index(self._h, x, y, z))

@@ -518,7 +518,7 @@ struct vdo_tess {
   wall_t walls[VDO_MAX_WALLS]; int nwalls;
   double* gen; size_t ngen;
   size_t* bin_of;          /* generator_bin_ids */
-  size_t* bin_start;       /* CSR of grid_bins, members ascending */
+  size_t* bin_start;       /* CSR of grid_bins, members in the reference's push order */
   size_t* bin_members;
   vdo_cell* cells; size_t ncells;
   uint64_t counters[VDO_NCOUNTERS];
@@ -642,6 +642,36 @@ size_t vdo_set_generators(vdo_tess* t, const double* xyz, size_t n) {
   t->ngen = m;
   grid_rebin(t);
   return m;
+}
+
+/* Tessellation::set_generator (tessellation.rs:70-92) and
+   Algorithm3DGrid::update_generator (algo_3d_grid.rs:132-143): ignored when the
+   index is out of range or a wall does not contain the point; a bin change
+   swap_removes the id from its old bin and pushes it onto the new one, so the
+   in-bin visit order is the reference's. */
+void vdo_set_generator(vdo_tess* t, size_t index, const double xyz[3]) {
+  if (index >= t->ngen || !walls_contain(t, xyz)) return;
+  const size_t nb = t->nx * t->ny * t->nz;
+  const size_t nbin = vdo_bin_index(t, xyz[0], xyz[1], xyz[2]), ob = t->bin_of[index];
+  if (nbin != ob) {
+    size_t pos = t->bin_start[ob];
+    while (t->bin_members[pos] != index) ++pos;
+    const size_t last = t->bin_start[ob + 1] - 1;
+    t->bin_members[pos] = t->bin_members[last];
+    size_t* mem = (size_t*)malloc(t->ngen * sizeof(size_t));
+    size_t m = 0;
+    for (size_t b = 0; b < nb; ++b) {
+      const size_t s = t->bin_start[b], e = b == ob ? last : t->bin_start[b + 1];
+      t->bin_start[b] = m;
+      for (size_t k = s; k < e; ++k) mem[m++] = t->bin_members[k];
+      if (b == nbin) mem[m++] = index;
+    }
+    t->bin_start[nb] = m;
+    free(t->bin_members);
+    t->bin_members = mem;
+    t->bin_of[index] = nbin;
+  }
+  memcpy(&t->gen[3 * index], xyz, 3 * sizeof(double));
 }
 
 /* prune_outside_generators + add_wall (tessellation.rs:175-200) */
@@ -1086,6 +1116,10 @@ void vdo_relax(vdo_tess* t) {
 }
 
 size_t vdo_count_generators(const vdo_tess* t) { return t->ngen; }
+void vdo_get_bins(const vdo_tess* t, size_t* start, size_t* members) {
+  memcpy(start, t->bin_start, (t->nx * t->ny * t->nz + 1) * sizeof(size_t));
+  memcpy(members, t->bin_members, t->ngen * sizeof(size_t));
+}
 size_t vdo_count_cells(const vdo_tess* t) { return t->ncells; }
 void vdo_get_generators(const vdo_tess* t, double* xyz) { memcpy(xyz, t->gen, t->ngen * 3 * sizeof(double)); }
 size_t vdo_search_order_len(const vdo_tess* t) { return t->norder; }

@@ -62,6 +62,9 @@ int vdo_add_wall_polyhedron(vdo_tess* t, const double* points, const double* nor
 int vdo_regular_polyhedron(int kind, const double center[3], double radius, double* points, double* normals);
 void vdo_clear_walls(vdo_tess* t);
 size_t vdo_set_generators(vdo_tess* t, const double* xyz, size_t n);
+void vdo_set_generator(vdo_tess* t, size_t index, const double xyz[3]);
+/* grid_bins as CSR: start[nbins + 1], members[count_generators] */
+void vdo_get_bins(const vdo_tess* t, size_t* start, size_t* members);
 void vdo_calculate(vdo_tess* t, int nthreads);
 /* calculate only cells [begin, end) (a bounded sample for timing) */
 void vdo_calculate_range(vdo_tess* t, size_t begin, size_t end, int nthreads);

@@ -234,6 +234,46 @@ def test_set_generator_moves_bin(oracle_mod):
     assert abs(vol.sum() - 1.0) < 1e-9
 
 
+def test_read_and_import_generators(oracle_mod, tmp_path):
+    """Tessellation::read_generators / import_generators (tessellation.rs:126-171)
+    through the C ABI: the same generators, and the same cells, as
+    set_generators of the parsed points; a file that cannot be read is
+    VD_EIO and text that is not UTF-8 VD_EINVAL, with nothing changed."""
+    import vorothree_b200 as v
+    from vorothree_b200._lib import VD_EINVAL, VD_EIO
+    pts = uniform(1500, 0.0, 1.0, 40).tolist()
+    text = "".join(f"{i} {x!r} {y!r} {z!r}\n" for i, (x, y, z) in enumerate(pts))
+    text += "\n  \n9999 0.5\r\n7 0.25 bad 0.75 extra\n"
+    path = tmp_path / "generators.txt"
+    path.write_text(text)
+    wall = v.Wall(-1000, v.SphereGeometry([0.5, 0.5, 0.5], 0.45))
+
+    def fresh():
+        t = v.Tessellation(v.BoundingBox([0, 0, 0], [1, 1, 1]), v.Algorithm3DGrid(9, 9, 9))
+        t.set_instrumentation(True)
+        t.add_wall(wall)
+        return t
+    a, b = fresh(), fresh()
+    ka = a.read_generators(text)
+    kb = b.import_generators(str(path))
+    parsed = v.parse_generators(text)
+    assert parsed.shape == (len(pts) + 2, 3)
+    assert parsed[-2].tolist() == [0.5, 0.0, 0.0] and parsed[-1].tolist() == [0.25, 0.0, 0.75]
+    o = oracle_tess(oracle_mod, [0, 0, 0], [1, 1, 1], (9, 9, 9), parsed, [wall], walls_first=True)
+    assert ka == kb == o.count_generators()
+    for t in (a, b):
+        t.calculate()
+        assert_same(t, o, sample_cells=3)
+    before = a.generators()
+    with pytest.raises(v.VoronoidError) as e:
+        a.import_generators(str(tmp_path / "missing.txt"))
+    assert e.value.code == VD_EIO
+    with pytest.raises(v.VoronoidError) as e:
+        a.read_generators(b"0 0.5 0.5 0.5\n1 0.4 \xff 0.4\n")
+    assert e.value.code == VD_EINVAL
+    assert np.array_equal(a.generators(), before)
+
+
 @pytest.mark.parametrize("scale,offset", [(1000.0, 0.0), (1e-3, 0.0), (1.0, 5000.0)])
 def test_mixed_equals_fp64_across_scales(scale, offset):
     """The FP32 classification's error bound must hold at every coordinate

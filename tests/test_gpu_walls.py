@@ -111,3 +111,28 @@ def test_wall_errors():
     big = v.ConvexPolyhedronGeometry(np.zeros((257, 3)), np.tile([0.0, 0.0, 1.0], (257, 1)))
     with pytest.raises(v.VoronoidError):
         t.add_wall(v.Wall(WALL, big))
+
+
+@pytest.mark.parametrize("name", ["cylinder", "cone", "torus", "dodecahedron", "combined"])
+def test_set_generator_under_walls_bitwise(oracle_mod, name):
+    """Tessellation::set_generator (tessellation.rs:70-92) tests the new point
+    against every wall kind before Algorithm3DGrid::update_generator
+    (algo_3d_grid.rs:132-143) moves it between bins: moves the walls reject and
+    out-of-range indices change nothing, accepted ones follow the reference's
+    swap_remove/push bin order."""
+    walls = wall_sets()[name]
+    pts = uniform(3000, 0.0, 10.0, 31)
+    g = gpu_tess([0, 0, 0], [10, 10, 10], (8, 8, 8), pts, walls, walls_first=True)
+    o = oracle_tess(oracle_mod, [0, 0, 0], [10, 10, 10], (8, 8, 8), pts, walls, True)
+    n = g.count_generators()
+    assert n == o.count_generators()
+    rng = np.random.Generator(np.random.PCG64(32))
+    moves = [(int(rng.integers(0, n)), rng.uniform(0.0, 10.0, 3)) for _ in range(60)]
+    moves += [(n, [5.0, 5.0, 5.0]), (n + 7, [5.0, 5.0, 5.0])]
+    for i, p in moves:
+        g.set_generator(i, p)
+        o.set_generator(i, p)
+    assert np.array_equal(g.generators(), o.generators())
+    g.calculate()
+    o.calculate()
+    assert_same(g, o, sample_cells=6)

@@ -113,6 +113,47 @@ def test_wall_filters(oracle_mod):
     assert kept == int(((h >= 0) & (rr <= h * math.tan(0.4))).sum())
 
 
+def test_set_generator_bins(oracle_mod):
+    """set_generator (tessellation.rs:70-92) against a list-of-lists model of
+    Algorithm3DGrid's bins (algo_3d_grid.rs:109-143): swap_remove from the old
+    bin, push onto the new one; moves outside a wall and out-of-range indices
+    are ignored."""
+    pts = uniform(400, 0.0, 10.0, 9)
+    t = oracle_mod.OracleTessellation([0, 0, 0], [10, 10, 10], 4, 4, 4)
+    t.add_wall_cylinder([5, 5, 5], [0, 0, 1], 4.5, WALL)
+    n = t.set_generators(pts)
+    gens = t.generators().reshape(-1, 3).copy()
+    model = [[] for _ in range(64)]
+    bin_of = []
+    for i, p in enumerate(gens):
+        b = t.bin_index(*p)
+        model[b].append(i)
+        bin_of.append(b)
+    assert t.bins() == model
+    rng = np.random.Generator(np.random.PCG64(10))
+    moved = rejected = 0
+    for _ in range(300):
+        i = int(rng.integers(0, n + 3))
+        p = rng.uniform(0.0, 10.0, 3)
+        t.set_generator(i, p)
+        if i >= n or math.hypot(p[0] - 5, p[1] - 5) > 4.5:
+            rejected += 1
+            continue
+        moved += 1
+        b = t.bin_index(*p)
+        if b != bin_of[i]:
+            old = model[bin_of[i]]
+            k = old.index(i)
+            old[k] = old[-1]
+            old.pop()
+            model[b].append(i)
+            bin_of[i] = b
+        gens[i] = p
+    assert moved > 100 and rejected > 50
+    assert t.bins() == model
+    assert np.array_equal(t.generators().reshape(-1, 3), gens)
+
+
 def sealed_pair(oracle_mod, walls, n=3000, seed=12):
     pts = uniform(n, 0.0, 10.0, seed)
     out = []

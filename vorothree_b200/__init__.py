@@ -1,8 +1,8 @@
 """vorothree_b200 -- B200-native 3D Voronoi tessellation.
 
 A GPU drop-in for the reference crate ``voronoid``'s 3D path
-(Tessellation::calculate over Algorithm3DGrid + Cell3DFaces, with plane and
-sphere walls).  The work runs in hand-written sm_100a CUDA kernels behind a C
+(Tessellation::calculate over Algorithm3DGrid + Cell3DFaces, with plane,
+sphere, cylinder, cone, torus and convex-polyhedron walls).  The work runs in hand-written sm_100a CUDA kernels behind a C
 ABI (include/voronoid_b200.h); this package is the Python mirror of the
 reference's API over that ABI.
 """
@@ -12,9 +12,9 @@ from .server import TessellationServer
 from .shard import calculate_sharded, cell_range, gather_summaries
 from .tessellation import (WALL_ID_MAX, Algorithm3DGrid, BoundingBox, Cell3DFaces, ConeGeometry,
                            ConvexPolyhedronGeometry, CylinderGeometry, PlaneGeometry, SphereGeometry, Tessellation,
-                           TorusGeometry, Wall, box_side)
+                           TorusGeometry, Wall, box_side, parse_generators)
 
 __all__ = ["Algorithm3DGrid", "BoundingBox", "Cell3DFaces", "ConeGeometry", "ConvexPolyhedronGeometry",
            "CylinderGeometry", "PlaneGeometry", "SphereGeometry", "TorusGeometry",
            "Tessellation", "TessellationBatch", "TessellationServer", "Wall", "WALL_ID_MAX", "box_side", "VoronoidError", "load",
-           "calculate_sharded", "cell_range", "gather_summaries"]
+           "calculate_sharded", "cell_range", "gather_summaries", "parse_generators"]

@@ -19,11 +19,12 @@ VD_EOVERFLOW = 3
 VD_ETIMEOUT = 4
 VD_ECUDA = 5
 VD_ESTATE = 6
+VD_EIO = 7
 VD_PREC_FP64 = 0
 VD_PREC_MIXED = 1
 
 STATUS_NAMES = {VD_EINVAL: "VD_EINVAL", VD_ENOMEM: "VD_ENOMEM", VD_EOVERFLOW: "VD_EOVERFLOW",
-                VD_ETIMEOUT: "VD_ETIMEOUT", VD_ECUDA: "VD_ECUDA", VD_ESTATE: "VD_ESTATE"}
+                VD_ETIMEOUT: "VD_ETIMEOUT", VD_ECUDA: "VD_ECUDA", VD_ESTATE: "VD_ESTATE", VD_EIO: "VD_EIO"}
 
 # every symbol the header declares, with its ctypes signature
 _d = C.POINTER(C.c_double)
@@ -48,6 +49,9 @@ SIGNATURES = {
     "vd_tess_set_generators": (C.c_int, [_vp, _d, C.c_size_t, _szp]),
     "vd_tess_set_generators_device": (C.c_int, [_vp, _vp, C.c_size_t, _szp]),
     "vd_tess_set_generator": (C.c_int, [_vp, C.c_size_t, _d]),
+    "vd_tess_read_generators": (C.c_int, [_vp, C.c_char_p, C.c_size_t, _szp]),
+    "vd_tess_import_generators": (C.c_int, [_vp, C.c_char_p, _szp]),
+    "vd_parse_generators": (C.c_int, [C.c_char_p, C.c_size_t, _d, C.c_size_t, _szp]),
     "vd_tess_count_generators": (C.c_int, [_vp, _szp]),
     "vd_tess_get_generators": (C.c_int, [_vp, _d]),
     "vd_tess_set_precision": (C.c_int, [_vp, C.c_int]),

@@ -31,6 +31,7 @@ SOURCES = [
     ("vd_server.cu", False),
     ("vd_cell.cu", False),
     ("vd_seal.cu", False),
+    ("vd_text.cpp", False),
 ]
 
 
@@ -60,7 +61,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     objs, procs = [], []
     # translation units compile in parallel; any failure fails the build
     for src, fma in SOURCES:
-        obj = os.path.join(BUILD_DIR, src.replace(".cu", ".o"))
+        obj = os.path.join(BUILD_DIR, os.path.splitext(src)[0] + ".o")
         if os.path.exists(obj):
             os.unlink(obj)
         cmd = [nvcc(), *ARCH, *COMMON, "-fmad=" + ("true" if fma else "false"),

@@ -79,8 +79,9 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_add(T* out, size_t n, con
 
 // ---- walls ------------------------------------------------------------------
 // WallGeometry::contains of each wall kind (wall_3d.rs:31-36, 73-78, 132-143,
-// 202-214, 293-309, 691-701), in the reference's arithmetic order
-__device__ __forceinline__ bool wall_contains(const Wall& w, const double* planes, double x, double y, double z) {
+// 202-214, 293-309, 691-701), in the reference's arithmetic order; also run on
+// the host by set_generator (host code is built with -ffp-contract=off)
+__host__ __device__ __forceinline__ bool wall_contains(const Wall& w, const double* planes, double x, double y, double z) {
   const double dx = x - w.a[0], dy = y - w.a[1], dz = z - w.a[2];
   switch (w.kind) {
     case kWallPlane:

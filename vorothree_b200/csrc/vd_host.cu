@@ -1113,6 +1113,30 @@ int vd_tess_set_generators_device(vd_tess* t, const double* d_xyz, size_t n, siz
   return set_generators_from_device(t, d_xyz, n, n_kept);
 }
 
+// Tessellation::read_generators / import_generators (tessellation.rs:126-171):
+// parsed on the host, then the set_generators path
+int vd_tess_read_generators(vd_tess* t, const char* text, size_t len, size_t* n_kept) {
+  if (!t || (!text && len)) return VD_EINVAL;
+  std::vector<double> xyz;
+  std::string err;
+  if (!parse_generators(text, len, &xyz, &err)) return fail(t, VD_EINVAL, "%s", err.c_str());
+  return vd_tess_set_generators(t, xyz.data(), xyz.size() / 3, n_kept);
+}
+
+int vd_tess_import_generators(vd_tess* t, const char* path, size_t* n_kept) {
+  if (!t || !path) return VD_EINVAL;
+  FILE* f = std::fopen(path, "rb");
+  if (!f) return fail(t, VD_EIO, "cannot open %s", path);
+  std::string text;
+  char buf[1 << 16];
+  size_t got;
+  while ((got = std::fread(buf, 1, sizeof(buf), f)) > 0) text.append(buf, got);
+  const bool bad = std::ferror(f) != 0;
+  std::fclose(f);
+  if (bad) return fail(t, VD_EIO, "cannot read %s", path);
+  return vd_tess_read_generators(t, text.data(), text.size(), n_kept);
+}
+
 // Tessellation::set_generator + Algorithm3DGrid::update_generator
 // (tessellation.rs:71-92, algo_3d_grid.rs:132-143).  The bin change uses the
 // reference's swap_remove/push, so in-bin order follows the reference's.
@@ -1120,12 +1144,8 @@ int vd_tess_set_generator(vd_tess* t, size_t index, const double xyz[3]) {
   if (!t || !xyz) return VD_EINVAL;
   VD_CK(t, cudaSetDevice(t->device));
   if (index >= t->ngen) return VD_OK;
-  for (const Wall& w : t->walls) {
-    const double dx = xyz[0] - w.a[0], dy = xyz[1] - w.a[1], dz = xyz[2] - w.a[2];
-    const bool in = w.kind == 0 ? (dx * w.n[0] + dy * w.n[1] + dz * w.n[2]) >= 0.0
-                                : (dx * dx + dy * dy + dz * dz) <= w.r * w.r;
-    if (!in) return VD_OK;
-  }
+  for (const Wall& w : t->walls)
+    if (!wall_contains(w, t->planes.data(), xyz[0], xyz[1], xyz[2])) return VD_OK;
   cudaStream_t s = t->stream;
   const size_t n = t->ngen, nb = t->nbins;
   std::vector<uint32_t> start(nb + 1), ids(n), bin_of(n);

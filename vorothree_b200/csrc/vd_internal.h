@@ -51,6 +51,10 @@ cudaError_t launch_clip_fp64_big_batched(const TessDesc* descs, const uint32_t* 
 // false with a message for a bad descriptor.
 bool wall_from_desc(const vd_wall_desc& d, Wall* w, std::vector<double>* planes, std::string* err);
 
+// the generator text format of Tessellation::read_generators (vd_text.cpp):
+// false with a message when the text is not UTF-8
+bool parse_generators(const char* text, size_t len, std::vector<double>* xyz, std::string* err);
+
 // message returned by vd_last_error(NULL) on the calling thread
 void set_thread_error(const char* msg);
 

@@ -18,6 +18,7 @@ numpy arrays.
 from __future__ import annotations
 
 import ctypes as C
+import os
 import math
 from dataclasses import dataclass
 from typing import Callable, List, Optional, Sequence
@@ -412,6 +413,19 @@ class Cell3DFaces:
         return float(self._face_areas[face_index])
 
 
+def parse_generators(text) -> np.ndarray:
+    """The reader of Tessellation::read_generators (tessellation.rs:153-171),
+    host only: an (n, 3) array of the points in ``text`` (str or UTF-8 bytes),
+    before any wall filter."""
+    L = load()
+    data = text.encode("utf-8") if isinstance(text, str) else bytes(text)
+    n = C.c_size_t()
+    check(L.vd_parse_generators(data, len(data), None, 0, C.byref(n)))
+    out = np.zeros(3 * max(n.value, 1), np.float64)
+    check(L.vd_parse_generators(data, len(data), _dp(out), n.value, C.byref(n)))
+    return out[:3 * n.value].reshape(-1, 3)
+
+
 class Tessellation:
     """Tessellation<3, Cell3DFaces, Algorithm3DGrid> on one GPU."""
 
@@ -498,25 +512,20 @@ class Tessellation:
         g = np.asarray(generator, np.float64)
         self._ck(self._L.vd_tess_set_generator(self._h, int(index), _dp(g)))
 
-    def read_generators(self, text: str):
+    def read_generators(self, text):
         """Tessellation::read_generators (tessellation.rs:153-171): one
-        ``id x y z`` per line, id ignored, missing/unparsable coordinates 0."""
-        pts = []
-        for line in text.splitlines():
-            parts = line.split()
-            if not parts:
-                continue
-            for k in range(3):
-                try:
-                    pts.append(float(parts[1 + k]))
-                except (IndexError, ValueError):
-                    pts.append(0.0)
-        return self.set_generators(np.asarray(pts, np.float64))
+        ``id x y z`` per line, the id ignored, a missing or unparsable
+        coordinate 0.0 (parsed by the library's native reader)."""
+        data = text.encode("utf-8") if isinstance(text, str) else bytes(text)
+        kept = C.c_size_t()
+        self._ck(self._L.vd_tess_read_generators(self._h, data, len(data), C.byref(kept)))
+        return kept.value
 
     def import_generators(self, path: str):
         """Tessellation::import_generators (tessellation.rs:126-148)."""
-        with open(path) as f:
-            return self.read_generators(f.read())
+        kept = C.c_size_t()
+        self._ck(self._L.vd_tess_import_generators(self._h, os.fsencode(path), C.byref(kept)))
+        return kept.value
 
     def count_generators(self) -> int:
         n = C.c_size_t()
