@@ -90,6 +90,13 @@ int vd_tess_set_generators_device(vd_tess* t, const double* d_xyz, size_t n, siz
 /* Tessellation::set_generator (tessellation.rs:71-92): ignored when out of
  * range or outside a wall, as in the reference */
 int vd_tess_set_generator(vd_tess* t, size_t index, const double xyz[3]);
+/* Tessellation::random_generators (tessellation.rs:96-121), seeded: candidate
+ * a = 0, 1, ... has coordinates min[c] + u * (max[c] - min[c]) with
+ * u = (splitmix64 draw 3a + c of `seed`) >> 11, times 2^-53; the first `count`
+ * candidates inside every wall become the generators, out of at most
+ * count * 1000 attempts (*n_found may then be below count).  The reference
+ * seeds from thread_rng; a caller wanting that passes a random seed. */
+int vd_tess_random_generators(vd_tess* t, size_t count, uint64_t seed, size_t* n_found);
 /* Tessellation::read_generators (tessellation.rs:153-171): one generator per
  * line of `text` (len bytes of UTF-8): an id, ignored, then x y z; a missing
  * or unparsable coordinate reads 0.0 (Rust's str::parse::<f64> grammar), a

@@ -60,6 +60,8 @@ def lib():
     L.vdo_set_generators.argtypes = [vp, d3, C.c_size_t]
     L.vdo_set_generator.restype = None
     L.vdo_set_generator.argtypes = [vp, C.c_size_t, d3]
+    L.vdo_random_generators.restype = C.c_size_t
+    L.vdo_random_generators.argtypes = [vp, C.c_size_t, C.c_uint64]
     L.vdo_get_bins.restype = None
     L.vdo_get_bins.argtypes = [vp, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]
     L.vdo_calculate.argtypes = [vp, C.c_int]
@@ -309,6 +311,9 @@ class OracleTessellation:
         out = np.zeros(3 * n, np.float64)
         lib().vdo_get_generators(self._h, out.ctypes.data_as(C.POINTER(C.c_double)))
         return out
+
+    def random_generators(self, count: int, seed: int) -> int:
+        return int(lib().vdo_random_generators(self._h, int(count), int(seed)))
 
     def bins(self):
         """grid_bins as a list of id lists, in visit order."""

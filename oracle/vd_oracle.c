@@ -674,6 +674,41 @@ void vdo_set_generator(vdo_tess* t, size_t index, const double xyz[3]) {
   memcpy(&t->gen[3 * index], xyz, 3 * sizeof(double));
 }
 
+/* SplitMix64 (Steele, Lea & Flood, OOPSLA 2014) as a counter-based generator:
+   draw k of a seed mixes seed + (k + 1) * 0x9e3779b97f4a7c15. */
+static uint64_t splitmix64_at(uint64_t seed, uint64_t k) {
+  uint64_t z = seed + (k + 1) * 0x9e3779b97f4a7c15ull;
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+  return z ^ (z >> 31);
+}
+
+/* Tessellation::random_generators (tessellation.rs:96-121) with an explicit
+   seed in place of thread_rng: attempts one at a time, each coordinate
+   min + u * (max - min) with u = (draw >> 11) * 2^-53, kept when every wall
+   contains the point, until `count` are kept or count * 1000 attempts. */
+size_t vdo_random_generators(vdo_tess* t, size_t count, uint64_t seed) {
+  double* pts = (double*)malloc((count ? count : 1) * 3 * sizeof(double));
+  size_t found = 0;
+  const uint64_t max_attempts = (uint64_t)count * 1000u;
+  for (uint64_t a = 0; found < count && a < max_attempts; ++a) {
+    double p[3];
+    for (int c = 0; c < 3; ++c) {
+      const double u = (double)(splitmix64_at(seed, 3 * a + (uint64_t)c) >> 11) * 0x1p-53;
+      p[c] = t->bmin[c] + u * (t->bmax[c] - t->bmin[c]);
+    }
+    if (walls_contain(t, p)) {
+      memcpy(&pts[3 * found], p, sizeof(p));
+      found++;
+    }
+  }
+  free(t->gen);
+  t->gen = pts;
+  t->ngen = found;
+  grid_rebin(t);
+  return found;
+}
+
 /* prune_outside_generators + add_wall (tessellation.rs:175-200) */
 static int add_wall(vdo_tess* t, const wall_t* w) {
   if (w->id > VDO_WALL_ID_MAX || t->nwalls >= VDO_MAX_WALLS) return -1;

@@ -63,6 +63,7 @@ int vdo_regular_polyhedron(int kind, const double center[3], double radius, doub
 void vdo_clear_walls(vdo_tess* t);
 size_t vdo_set_generators(vdo_tess* t, const double* xyz, size_t n);
 void vdo_set_generator(vdo_tess* t, size_t index, const double xyz[3]);
+size_t vdo_random_generators(vdo_tess* t, size_t count, uint64_t seed);
 /* grid_bins as CSR: start[nbins + 1], members[count_generators] */
 void vdo_get_bins(const vdo_tess* t, size_t* start, size_t* members);
 void vdo_calculate(vdo_tess* t, int nthreads);

@@ -136,3 +136,38 @@ def test_set_generator_under_walls_bitwise(oracle_mod, name):
     g.calculate()
     o.calculate()
     assert_same(g, o, sample_cells=6)
+
+
+@pytest.mark.parametrize("name,count", [("torus", 3000), ("dodecahedron", 2500), ("combined", 20000)])
+def test_random_generators_bitwise(oracle_mod, name, count):
+    """Tessellation::random_generators (tessellation.rs:96-121), seeded: the
+    device's batched candidates and wall filter keep the oracle's points (the
+    first `count` inside the walls in attempt order), and the cells match."""
+    import vorothree_b200 as v
+    walls = wall_sets()[name]
+    g = v.Tessellation(v.BoundingBox([0, 0, 0], [10, 10, 10]), v.Algorithm3DGrid(8, 8, 8))
+    g.set_instrumentation(True)
+    o = oracle_mod.OracleTessellation([0, 0, 0], [10, 10, 10], 8, 8, 8)
+    for w in walls:
+        g.add_wall(w)
+        oracle_add(o, w)
+    seed = 0x5EED0000 + count
+    assert g.random_generators(count, seed) == o.random_generators(count, seed) == count
+    g.calculate()
+    o.calculate()
+    assert_same(g, o, sample_cells=4)
+
+
+def test_random_generators_attempt_cap(oracle_mod):
+    # ~2000 attempts per accepted point: the count * 1000 cap ends the loop
+    # early, after the same attempts on both sides
+    import vorothree_b200 as v
+    g = v.Tessellation(v.BoundingBox([0, 0, 0], [10, 10, 10]), v.Algorithm3DGrid(4, 4, 4))
+    o = oracle_mod.OracleTessellation([0, 0, 0], [10, 10, 10], 4, 4, 4)
+    g.add_wall(v.Wall(WALL, v.SphereGeometry([5, 5, 5], 0.492)))
+    o.add_wall_sphere([5, 5, 5], 0.492, WALL)
+    for seed in (7, 8, 9):
+        n = g.random_generators(50, seed)
+        assert n == o.random_generators(50, seed) and 5 < n < 50
+        assert np.array_equal(g.generators(), o.generators())
+    assert g.random_generators(0, 1) == 0 and g.count_generators() == 0

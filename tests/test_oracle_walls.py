@@ -204,3 +204,39 @@ def test_prune_boundaries_log(oracle_mod):
     r = np.linalg.norm(pos - 5.0, axis=1)
     assert np.all(r >= 4.5 - 1e-9) and np.all(r < 5.0)
     assert set(log[:, 2]) == {WALL}
+
+
+def _splitmix64_at(seed, k):
+    m = 2 ** 64 - 1
+    z = (seed + (k + 1) * 0x9E3779B97F4A7C15) & m
+    z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & m
+    z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & m
+    return z ^ (z >> 31)
+
+
+def test_random_generators_oracle(oracle_mod):
+    """random_generators (tessellation.rs:96-121) with a seed: SplitMix64's
+    published first outputs for seed 0, a pure-Python restatement of the
+    attempt loop, and the count * 1000 attempt cap."""
+    assert [_splitmix64_at(0, k) for k in range(4)] == [0xE220A8397B1DCDAF, 0x6E789E6AA1B965F4,
+                                                         0x06C45D188009454F, 0xF88BB8A8724C81EC]
+    lo, hi = [-1.0, 0.0, 2.0], [3.0, 10.0, 2.5]
+    t = oracle_mod.OracleTessellation(lo, hi, 4, 4, 4)
+    t.add_wall_sphere([1.0, 5.0, 2.25], 2.0, WALL)
+    seed = 0xDEADBEEF12345
+    assert t.random_generators(200, seed) == 200
+    want, a = [], 0
+    while len(want) < 200:
+        p = [lo[c] + float(_splitmix64_at(seed, 3 * a + c) >> 11) * 2.0 ** -53 * (hi[c] - lo[c]) for c in range(3)]
+        if (p[0] - 1.0) ** 2 + (p[1] - 5.0) ** 2 + (p[2] - 2.25) ** 2 <= 4.0:
+            want.append(p)
+        a += 1
+    assert np.array_equal(t.generators().reshape(-1, 3), np.asarray(want))
+    # a region that takes ~2000 attempts per point: the cap of 50 * 1000
+    # attempts stops the loop early
+    t = oracle_mod.OracleTessellation([0, 0, 0], [10, 10, 10], 4, 4, 4)
+    t.add_wall_sphere([5, 5, 5], 0.492, WALL)
+    n = t.random_generators(50, 7)
+    assert 5 < n < 50
+    t.calculate(1)
+    assert t.count_cells() == n

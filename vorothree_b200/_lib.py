@@ -49,6 +49,7 @@ SIGNATURES = {
     "vd_tess_set_generators": (C.c_int, [_vp, _d, C.c_size_t, _szp]),
     "vd_tess_set_generators_device": (C.c_int, [_vp, _vp, C.c_size_t, _szp]),
     "vd_tess_set_generator": (C.c_int, [_vp, C.c_size_t, _d]),
+    "vd_tess_random_generators": (C.c_int, [_vp, C.c_size_t, C.c_uint64, _szp]),
     "vd_tess_read_generators": (C.c_int, [_vp, C.c_char_p, C.c_size_t, _szp]),
     "vd_tess_import_generators": (C.c_int, [_vp, C.c_char_p, _szp]),
     "vd_parse_generators": (C.c_int, [C.c_char_p, C.c_size_t, _d, C.c_size_t, _szp]),

@@ -142,6 +142,54 @@ __global__ void k_compact3(const double* __restrict__ in, size_t n, const uint32
   }
 }
 
+// ---- random generators ------------------------------------------------------
+// SplitMix64 (Steele, Lea & Flood, "Fast splittable pseudorandom number
+// generators", OOPSLA 2014) as a counter-based generator: draw k of a seed is
+// the SplitMix64 output mix of seed + (k + 1) * 0x9e3779b97f4a7c15, so every
+// candidate's coordinates are fixed by (seed, index) alone.
+__host__ __device__ __forceinline__ uint64_t splitmix64_at(uint64_t seed, uint64_t k) {
+  uint64_t z = seed + (k + 1) * 0x9e3779b97f4a7c15ull;
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+  return z ^ (z >> 31);
+}
+
+// Candidate a of Tessellation::random_generators (tessellation.rs:96-121):
+// coordinate c = min[c] + u * (max[c] - min[c]), u = (draw 3a + c >> 11) * 2^-53
+// in [0, 1) (the 53-bit mapping of rand's Standard f64); flagged when every
+// wall contains it.
+__global__ void k_random_candidates(uint64_t seed, uint64_t a0, size_t n, const Grid g, const WallSet ws,
+                                    double* __restrict__ out, uint32_t* flags) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const uint64_t a = a0 + i;
+    double p[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const double u = (double)(splitmix64_at(seed, 3 * a + c) >> 11) * 0x1p-53;
+      p[c] = g.bmin[c] + u * (g.bmax[c] - g.bmin[c]);
+    }
+    bool ok = true;
+    for (int k = 0; k < ws.n && ok; ++k) ok = wall_contains(ws.w[k], ws.planes, p[0], p[1], p[2]);
+    out[3 * i] = p[0];
+    out[3 * i + 1] = p[1];
+    out[3 * i + 2] = p[2];
+    flags[i] = ok ? 1u : 0u;
+  }
+}
+
+// k_compact3 keeping only the flagged rows ranked below `limit`
+__global__ void k_compact3_first(const double* __restrict__ in, size_t n, const uint32_t* flags,
+                                 const uint32_t* pos, uint32_t limit, double* __restrict__ out) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    if (flags[i] && pos[i] < limit) {
+      const size_t o = pos[i];
+      out[3 * o] = in[3 * i];
+      out[3 * o + 1] = in[3 * i + 1];
+      out[3 * o + 2] = in[3 * i + 2];
+    }
+  }
+}
+
 // ---- binning ----------------------------------------------------------------
 __device__ __forceinline__ uint32_t axis_index(double v, double lo, double scale, double limit) {
   double t = (v - lo) * scale;  // clamp(0, limit) then `as usize` (NaN -> 0)

@@ -1113,6 +1113,51 @@ int vd_tess_set_generators_device(vd_tess* t, const double* d_xyz, size_t n, siz
   return set_generators_from_device(t, d_xyz, n, n_kept);
 }
 
+// Tessellation::random_generators (tessellation.rs:96-121) with an explicit
+// seed: candidates in attempt order, batches of them generated and filtered
+// on the device, the first `count` inside every wall kept, at most
+// count * 1000 attempts.  Candidates are counter-based (splitmix64_at), so the
+// batching does not change which points are kept.
+int vd_tess_random_generators(vd_tess* t, size_t count, uint64_t seed, size_t* n_found) {
+  if (!t) return VD_EINVAL;
+  VD_CK(t, cudaSetDevice(t->device));
+  if (count > 0xFFFFFFF0ull / 3) return fail(t, VD_EINVAL, "too many generators");
+  cudaStream_t s = t->stream;
+  const unsigned long long max_att = 1000ull * count;
+  constexpr unsigned long long kMaxBatch = 1ull << 24;
+  VD_CK(t, t->d_in.ensure(3 * count, s));
+  const WallSet ws = wallset(t);
+  size_t found = 0;
+  unsigned long long att = 0;
+  while (found < count && att < max_att) {
+    const unsigned long long want = 2ull * (count - found) + 4096;
+    const size_t B = (size_t)std::min(max_att - att, std::min(want, kMaxBatch));
+    VD_CK(t, t->d_tmp3.ensure(3 * B, s));
+    VD_CK(t, t->d_flags.ensure(B + 1, s));
+    VD_CK(t, t->d_pos.ensure(B + 1, s));
+    k_random_candidates<<<grid_blocks(t, B, 256), 256, 0, s>>>(seed, att, B, t->grid, ws, t->d_tmp3.p,
+                                                               t->d_flags.p);
+    g_launches++;
+    VD_CK(t, cudaGetLastError());
+    VD_CK(t, cudaMemsetAsync(t->d_flags.p + B, 0, sizeof(uint32_t), s));
+    int r = scan_excl<uint32_t, uint32_t>(t, t->d_flags.p, t->d_pos.p, B + 1, t->scan32);
+    if (r != VD_OK) return r;
+    k_compact3_first<<<grid_blocks(t, B, 256), 256, 0, s>>>(t->d_tmp3.p, B, t->d_flags.p, t->d_pos.p,
+                                                            (uint32_t)(count - found), t->d_in.p + 3 * found);
+    g_launches++;
+    VD_CK(t, cudaGetLastError());
+    uint32_t acc = 0;
+    VD_CK(t, cudaMemcpyAsync(&acc, t->d_pos.p + B, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    VD_CK(t, cudaStreamSynchronize(s));
+    found += std::min<size_t>(acc, count - found);
+    att += B;
+  }
+  size_t kept = 0;
+  const int r = set_generators_from_device(t, t->d_in.p, found, &kept);
+  if (r == VD_OK && n_found) *n_found = kept;
+  return r;
+}
+
 // Tessellation::read_generators / import_generators (tessellation.rs:126-171):
 // parsed on the host, then the set_generators path
 int vd_tess_read_generators(vd_tess* t, const char* text, size_t len, size_t* n_kept) {

@@ -512,6 +512,20 @@ class Tessellation:
         g = np.asarray(generator, np.float64)
         self._ck(self._L.vd_tess_set_generator(self._h, int(index), _dp(g)))
 
+    def random_generators(self, count: int, seed: Optional[int] = None) -> int:
+        """Tessellation::random_generators (tessellation.rs:96-121): `count`
+        points uniform in the bounds and inside every wall (rejection, at most
+        count * 1000 attempts), generated on the device.  The reference seeds
+        from thread_rng; ``seed=None`` does the same with the OS's entropy,
+        an integer seed makes the points reproducible.  Returns the number
+        found."""
+        if seed is None:
+            seed = int.from_bytes(os.urandom(8), "little")
+        found = C.c_size_t()
+        self._ck(self._L.vd_tess_random_generators(self._h, int(count), int(seed) & (2**64 - 1),
+                                                   C.byref(found)))
+        return found.value
+
     def read_generators(self, text):
         """Tessellation::read_generators (tessellation.rs:153-171): one
         ``id x y z`` per line, the id ignored, a missing or unparsable
