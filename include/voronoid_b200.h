@@ -61,7 +61,10 @@ const char* vd_last_error(const vd_tess* t);
 
 /* ---- walls: Wall::new + PlaneGeometry/SphereGeometry + Tessellation::add_wall
  *      (wall/mod.rs:24-32, wall_3d.rs:23-27,66-68, tessellation.rs:197-200).
- *      Adding a wall prunes generators outside it (tessellation.rs:175-194). ---- */
+ *      Adding a wall prunes generators outside it (tessellation.rs:175-194).
+ *      At most 16 walls per tessellation (the kernels take them as a fixed
+ *      table in their parameters; the reference's Vec has no bound): one more
+ *      returns VD_EINVAL and changes nothing. ---- */
 int vd_tess_add_wall_plane(vd_tess* t, const double point[3], const double normal[3], int id);
 int vd_tess_add_wall_sphere(vd_tess* t, const double center[3], double radius, int id);
 /* CylinderGeometry (wall_3d.rs:107-174): inside an infinite cylinder; the

@@ -369,6 +369,67 @@ def test_degenerate_lattices_bitwise(oracle_mod, jitter, precision):
         assert 0.99 < vol.sum() < 1.0
 
 
+GEOMETRIES = {
+    # one bin: every cell walks the whole input in the reference's order
+    "one_bin": ([0, 0, 0], [1, 1, 1], (1, 1, 1), 300),
+    # flat, anisotropic box and grid
+    "slab": ([0, 0, 0], [100, 1, 0.01], (50, 3, 1), 3000),
+    "needle": ([-5, -5, -5], [-4.99, -4.99, 5], (1, 1, 200), 2000),
+    # large offset and tiny extent; large extent
+    "offset": ([1e6, 1e6, 1e6], [1e6 + 1e-3, 1e6 + 1e-3, 1e6 + 1e-3], (10, 10, 10), 4000),
+    "huge": ([-1e9, -1e9, -1e9], [1e9, 1e9, 1e9], (16, 16, 16), 4000),
+    # more bins than generators, odd resolutions
+    "sparse": ([0, 0, 0], [1, 2, 3], (37, 41, 43), 500),
+}
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+@pytest.mark.parametrize("name", list(GEOMETRIES))
+def test_geometry_extremes_bitwise(oracle_mod, name, precision):
+    """Boxes, grids and coordinate scales far from the unit cube, with some
+    generators exactly on bin boundaries and on the box's max faces (where
+    get_bin_index clamps to grid_limit, algo_3d_grid.rs:97-106)."""
+    lo, hi, grid, n = GEOMETRIES[name]
+    lo, hi = np.asarray(lo, np.float64), np.asarray(hi, np.float64)
+    rng = np.random.Generator(np.random.PCG64(91))
+    pts = lo + rng.uniform(0, 1, size=(n, 3)) * (hi - lo)
+    k = n // 10
+    cells = np.asarray(grid, np.float64)
+    pts[:k] = lo + np.floor(rng.uniform(0, 1, size=(k, 3)) * cells) / cells * (hi - lo)
+    pts[k:k + 5] = hi
+    pts[k + 5:k + 10, 0] = hi[0]
+    g = gpu_tess(lo, hi, grid, pts, precision=precision)
+    o = oracle_tess(oracle_mod, lo, hi, grid, pts)
+    # no volume-sum check: the five generators stacked on the max corner
+    # overlap (bisector of coincident points), and at a 1e6 offset the
+    # reference's volume formula, on absolute coordinates, cancels
+    # catastrophically -- the oracle shows both, and the device matches it
+    assert_same(g, o, sample_cells=6)
+
+
+def test_wall_limits():
+    """At most 16 walls and 256 convex-polyhedron planes per tessellation
+    (fixed tables in the kernels' parameters); one more is VD_EINVAL and
+    leaves the walls as they were."""
+    import vorothree_b200 as v
+    from vorothree_b200._lib import VD_EINVAL
+    t = v.Tessellation(v.BoundingBox([0, 0, 0], [1, 1, 1]), v.Algorithm3DGrid(2, 2, 2))
+    for k in range(16):
+        t.add_wall(v.Wall(WALL - k, v.PlaneGeometry([0.5, 0.5, 0.5], [0, 0, 1])))
+    with pytest.raises(v.VoronoidError) as e:
+        t.add_wall(v.Wall(WALL - 16, v.PlaneGeometry([0.5, 0.5, 0.5], [0, 0, 1])))
+    assert e.value.code == VD_EINVAL
+    t.set_generators(uniform(100, 0, 1, 3))
+    t.calculate()
+    assert t.count_cells() == int((uniform(100, 0, 1, 3)[:, 2] >= 0.5).sum())
+    t.clear_walls()
+    big = v.ConvexPolyhedronGeometry([[0.5, 0.5, 0.5]] * 200, [[0, 0, 1]] * 200)
+    t.add_wall(v.Wall(WALL, big))
+    with pytest.raises(v.VoronoidError) as e:
+        t.add_wall(v.Wall(WALL - 1, v.ConvexPolyhedronGeometry([[0.5, 0.5, 0.5]] * 57, [[0, 0, 1]] * 57)))
+    assert e.value.code == VD_EINVAL
+
+
 @pytest.mark.parametrize("precision", PRECISIONS)
 def test_degenerate_duplicates_and_planes(oracle_mod, precision):
     """Repeated generators, generators on the box faces and on a wall plane."""
