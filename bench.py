@@ -140,16 +140,29 @@ def load_traffic(precision: str):
     return load_profile(precision).get("dram_bytes_per_launch")
 
 
-def cpu_baseline(pts, nthreads: int, sample: int):
+def cpu_baseline(pts, nthreads: int, sample: int, extras: dict = None):
     """The oracle (a C restatement of the reference's calculate) on the host
-    cores over a bounded sample of the same tessellation's cells."""
+    cores over a bounded sample of the same tessellation's cells.  `extras`,
+    when given, gets the search-order table build (the Algorithm3DGrid::new
+    constructor, outside calculate) and a one-thread rate over a smaller
+    sample."""
     from oracle.oracle import OracleTessellation
+    t0 = time.perf_counter()
     t = OracleTessellation([0, 0, 0], [1, 1, 1], GRID, GRID, GRID)
+    build = time.perf_counter() - t0
     t.set_generators(pts)
     begin = (len(pts) - sample) // 2
     t0 = time.perf_counter()
     t.calculate_range(begin, begin + sample, nthreads)
     dt = time.perf_counter() - t0
+    if extras is not None:
+        one = min(sample, 65536)
+        b1 = (len(pts) - one) // 2
+        t1 = time.perf_counter()
+        t.calculate_range(b1, b1 + one, 1)
+        d1 = time.perf_counter() - t1
+        extras.update({"one_thread_value": one / d1, "one_thread_sample": f"{one} cells ({d1:.2f} s)",
+                       "search_order_build_s": build})
     return sample / dt, dt
 
 
@@ -426,10 +439,11 @@ def run_ours(args):
         if ws == 1 and not args.no_cpu_baseline:
             nthreads = os.cpu_count() or 1
             sample = min(args.cpu_sample or N_GEN, N_GEN)
-            cv, cdt = cpu_baseline(pts, nthreads, sample)
-            line["cpu_baseline"] = {"value": cv, "unit": "cells/s", "cores": nthreads, "kind": "port",
-                                    "sample": f"{sample} of {N_GEN} cells of the same tessellation "
-                                              f"({cdt:.2f} s wall)"}
+            extras = {}
+            cv, cdt = cpu_baseline(pts, nthreads, sample, extras)
+            line["cpu_baseline"] = dict({"value": cv, "unit": "cells/s", "cores": nthreads, "kind": "port",
+                                         "sample": f"{sample} of {N_GEN} cells of the same tessellation "
+                                                   f"({cdt:.2f} s wall)"}, **extras)
         print(json.dumps(line), flush=True)
     tess.close()
     if ws > 1:
