@@ -309,6 +309,11 @@ const char* vd_server_last_error(const vd_server* s);
 /* copies the inputs; *ticket identifies the request */
 int vd_server_submit(vd_server* s, const double bmin[3], const double bmax[3], int nx, int ny, int nz,
                      const vd_wall_desc* walls, int nwalls, const double* xyz, size_t n, uint64_t* ticket);
+/* the same with the generators as text in the read_generators format (see
+ * vd_tess_read_generators), parsed on the submitting thread; the request's
+ * latency includes the parse.  VD_EINVAL when the text is not UTF-8. */
+int vd_server_submit_text(vd_server* s, const double bmin[3], const double bmax[3], int nx, int ny, int nz,
+                          const vd_wall_desc* walls, int nwalls, const char* text, size_t len, uint64_t* ticket);
 /* blocks until the request is done: its cell count and submit-to-done latency */
 int vd_server_wait(vd_server* s, uint64_t ticket, size_t* n_cells, double* latency_s);
 /* copies the per-cell results (any pointer may be NULL) and releases the request */

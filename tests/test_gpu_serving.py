@@ -87,3 +87,26 @@ def test_request_over_budget_rejected():
     with pytest.raises(v.VoronoidError):
         srv.submit(v.BoundingBox([0, 0, 0], [1, 1, 1]), (10, 10, 10), uniform(20000, 0, 1, 1))
     srv.close()
+
+
+def test_text_requests_equal_alone():
+    """Requests whose generators arrive as read_generators text (tessellation.rs:
+    153-171), mixed with array requests: each equals the array request alone;
+    text that is not UTF-8 is refused at submit."""
+    import vorothree_b200 as v
+    reqs = requests(5)[:6]
+    srv = v.TessellationServer(slots=3, hbm_budget_bytes=8 << 30)
+    tickets = []
+    for k, (b, grid, pts, walls) in enumerate(reqs):
+        if k % 2 == 0:
+            text = "".join(f"{i} {x!r} {y!r} {z!r}\n" for i, (x, y, z) in enumerate(pts.tolist()))
+            tickets.append(srv.submit_text(b, grid, text, walls))
+        else:
+            tickets.append(srv.submit(b, grid, pts, walls))
+    for r, t in zip(reqs, tickets):
+        vol, cen, nf = srv.take(t)
+        av, ac, an = alone(r)
+        assert np.array_equal(nf, an) and np.array_equal(vol, av) and np.array_equal(cen, ac)
+    with pytest.raises(v.VoronoidError):
+        srv.submit_text(reqs[0][0], reqs[0][1], b"0 0.5 0.5 \xff\n")
+    srv.close()

@@ -102,6 +102,8 @@ SIGNATURES = {
     "vd_server_last_error": (C.c_char_p, [_vp]),
     "vd_server_submit": (C.c_int, [_vp, _d, _d, C.c_int, C.c_int, C.c_int, _vp, C.c_int, _d, C.c_size_t,
                                    C.POINTER(C.c_uint64)]),
+    "vd_server_submit_text": (C.c_int, [_vp, _d, _d, C.c_int, C.c_int, C.c_int, _vp, C.c_int, C.c_char_p,
+                                        C.c_size_t, C.POINTER(C.c_uint64)]),
     "vd_server_wait": (C.c_int, [_vp, C.c_uint64, _szp, _d]),
     "vd_server_take": (C.c_int, [_vp, C.c_uint64, _vp, _vp, _vp]),
     "vd_server_stats": (C.c_int, [_vp, _u64p, _u64p, _d, _d, _szp]),

@@ -180,6 +180,51 @@ void worker(vd_server* s, int slot) {
   }
 }
 
+// the request's clock starts at t0 (before parsing, for a text request)
+int submit_points(vd_server* s, const double bmin[3], const double bmax[3], int nx, int ny, int nz,
+                  const vd_wall_desc* walls, int nwalls, std::vector<double>&& pts, Clock::time_point t0,
+                  uint64_t* ticket) {
+  const size_t n = pts.size() / 3;
+  if (nx <= 0 || ny <= 0 || nz <= 0) return sfail(s, VD_EINVAL, "grid resolution must be positive");
+  for (int k = 0; k < nwalls; ++k) {
+    const vd_wall_desc& w = walls[k];
+    if (w.id > VD_WALL_ID_MAX || w.kind < 0 || w.kind > 5 ||
+        (w.kind == 5 && (w.nplanes < 0 || (w.nplanes > 0 && (!w.points || !w.normals)))))
+      return sfail(s, VD_EINVAL, "bad wall %d", k);
+  }
+  auto r = std::make_shared<Request>();
+  for (int a = 0; a < 3; ++a) {
+    r->bmin[a] = bmin[a];
+    r->bmax[a] = bmax[a];
+  }
+  r->n[0] = nx;
+  r->n[1] = ny;
+  r->n[2] = nz;
+  r->walls.assign(walls, walls + nwalls);
+  r->wall_planes.resize(nwalls);
+  for (int k = 0; k < nwalls; ++k) {
+    vd_wall_desc& w = r->walls[k];
+    if (w.kind == 5 && w.nplanes > 0) {
+      r->wall_planes[k].assign(w.points, w.points + 3 * w.nplanes);
+      r->wall_planes[k].insert(r->wall_planes[k].end(), w.normals, w.normals + 3 * w.nplanes);
+    }
+    w.points = w.normals = nullptr;  // the request keeps its own copy
+  }
+  r->pts = std::move(pts);
+  r->est_bytes = estimate_bytes(n, (size_t)nx * ny * nz);
+  if (r->est_bytes > s->budget) return sfail(s, VD_ENOMEM, "request needs %zu bytes, budget %zu", r->est_bytes, s->budget);
+  {
+    std::lock_guard<std::mutex> lock(s->mu);
+    r->id = s->next_id++;
+    r->t_submit = t0;
+    s->live[r->id] = r;
+    s->queue.push_back(r);
+    *ticket = r->id;
+  }
+  s->cv_work.notify_all();
+  return VD_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -240,48 +285,28 @@ int vd_server_destroy(vd_server* s) {
   return VD_OK;
 }
 
+
 int vd_server_submit(vd_server* s, const double bmin[3], const double bmax[3], int nx, int ny, int nz,
                      const vd_wall_desc* walls, int nwalls, const double* xyz, size_t n, uint64_t* ticket) {
   if (!s || !bmin || !bmax || !ticket || (!xyz && n) || (nwalls > 0 && !walls) || nwalls < 0)
     return VD_EINVAL;
-  if (nx <= 0 || ny <= 0 || nz <= 0) return sfail(s, VD_EINVAL, "grid resolution must be positive");
-  for (int k = 0; k < nwalls; ++k) {
-    const vd_wall_desc& w = walls[k];
-    if (w.id > VD_WALL_ID_MAX || w.kind < 0 || w.kind > 5 ||
-        (w.kind == 5 && (w.nplanes < 0 || (w.nplanes > 0 && (!w.points || !w.normals)))))
-      return sfail(s, VD_EINVAL, "bad wall %d", k);
-  }
-  auto r = std::make_shared<Request>();
-  for (int a = 0; a < 3; ++a) {
-    r->bmin[a] = bmin[a];
-    r->bmax[a] = bmax[a];
-  }
-  r->n[0] = nx;
-  r->n[1] = ny;
-  r->n[2] = nz;
-  r->walls.assign(walls, walls + nwalls);
-  r->wall_planes.resize(nwalls);
-  for (int k = 0; k < nwalls; ++k) {
-    vd_wall_desc& w = r->walls[k];
-    if (w.kind == 5 && w.nplanes > 0) {
-      r->wall_planes[k].assign(w.points, w.points + 3 * w.nplanes);
-      r->wall_planes[k].insert(r->wall_planes[k].end(), w.normals, w.normals + 3 * w.nplanes);
-    }
-    w.points = w.normals = nullptr;  // the request keeps its own copy
-  }
-  r->pts.assign(xyz, xyz + 3 * n);
-  r->est_bytes = estimate_bytes(n, (size_t)nx * ny * nz);
-  if (r->est_bytes > s->budget) return sfail(s, VD_ENOMEM, "request needs %zu bytes, budget %zu", r->est_bytes, s->budget);
-  {
-    std::lock_guard<std::mutex> lock(s->mu);
-    r->id = s->next_id++;
-    r->t_submit = Clock::now();
-    s->live[r->id] = r;
-    s->queue.push_back(r);
-    *ticket = r->id;
-  }
-  s->cv_work.notify_all();
-  return VD_OK;
+  const Clock::time_point t0 = Clock::now();
+  return submit_points(s, bmin, bmax, nx, ny, nz, walls, nwalls, std::vector<double>(xyz, xyz + 3 * n), t0,
+                       ticket);
+}
+
+// a request whose generators arrive in the text format of
+// Tessellation::read_generators (tessellation.rs:153-171); parsed here, on the
+// submitting thread, inside the request's latency
+int vd_server_submit_text(vd_server* s, const double bmin[3], const double bmax[3], int nx, int ny, int nz,
+                          const vd_wall_desc* walls, int nwalls, const char* text, size_t len, uint64_t* ticket) {
+  if (!s || !bmin || !bmax || !ticket || (!text && len) || (nwalls > 0 && !walls) || nwalls < 0)
+    return VD_EINVAL;
+  const Clock::time_point t0 = Clock::now();
+  std::vector<double> pts;
+  std::string err;
+  if (!vd::parse_generators(text, len, &pts, &err)) return sfail(s, VD_EINVAL, "%s", err.c_str());
+  return submit_points(s, bmin, bmax, nx, ny, nz, walls, nwalls, std::move(pts), t0, ticket);
 }
 
 int vd_server_wait(vd_server* s, uint64_t ticket, size_t* n_cells, double* latency_s) {

@@ -54,6 +54,20 @@ class TessellationServer:
                                            pts.ctypes.data_as(d), pts.size // 3, C.byref(t)))
         return t.value
 
+    def submit_text(self, bounds: BoundingBox, grid: Sequence[int], text, walls: Sequence[Wall] = ()) -> int:
+        """submit() with the generators in the read_generators text format
+        (``id x y z`` per line; str or UTF-8 bytes), parsed by the library."""
+        mn = np.asarray(bounds.min, np.float64)
+        mx = np.asarray(bounds.max, np.float64)
+        data = text.encode("utf-8") if isinstance(text, str) else bytes(text)
+        wd = _walls(walls)
+        t = C.c_uint64()
+        d = C.POINTER(C.c_double)
+        self._chk(self._L.vd_server_submit_text(self._h, mn.ctypes.data_as(d), mx.ctypes.data_as(d), int(grid[0]),
+                                                int(grid[1]), int(grid[2]), C.cast(wd.arr, C.c_void_p), len(walls),
+                                                data, len(data), C.byref(t)))
+        return t.value
+
     def wait(self, ticket: int):
         """(n_cells, latency_seconds) once the request is done."""
         n = C.c_size_t()
