@@ -609,6 +609,30 @@ def run_serving(args):
     return 0
 
 
+def blob_classes(t, pts, nb, kept, args):
+    """Time and count the blob cells and the background cells apart: the wall
+    filter keeps the input order, so the kept blob generators are cell ids
+    [0, nbk) and the background ones [nbk, kept).  Per-cell event counts come
+    from the instrumented kernel over the same range."""
+    d = pts[:nb] - 0.5
+    nbk = int(((d * d).sum(1) <= 0.45 ** 2).sum())
+    out = {}
+    for name, (b, e) in (("blob", (0, nbk)), ("background", (nbk, kept))):
+        times = []
+        for _ in range(max(3, args.steps)):
+            t.calculate_range(b, e)
+            tm = t.timings()
+            times.append(tm["clip_ms"] + tm["fallback_ms"])
+        t.set_instrumentation(True)
+        t.calculate_range(b, e)
+        c = t.counters()
+        t.set_instrumentation(False)
+        n = max(1, e - b)
+        out[name] = {"cells": e - b, "ms": min(times), "ns_per_cell": 1e6 * min(times) / n,
+                     "per_cell": {k: round(c[k] / n, 2) for k in ("offsets", "candidates", "clips", "modifying")}}
+    return out
+
+
 def run_blobs(args):
     """Config: 4,194,304 generators, 70% in 64 isotropic Gaussian blobs
     (sigma 0.01, centres uniform) + 30% uniform background, clipped by a
@@ -639,6 +663,8 @@ def run_blobs(args):
         ms = statistics.mean(times[args.warmup:])
         res.append({"grid": list(g), "kept": kept, "ms": ms, "cells_per_s": kept / (ms / 1e3),
                     "fallback_cells": t.fallback_counts()})
+        if g == tuned:
+            res[-1]["classes"] = blob_classes(t, pts, nb, kept, args)
         t.close()
     line = {"metric": "3D cells/s, clustered generators", "workload": "blobs", "unit": "cells/s",
             "value": res[0]["cells_per_s"], "n_gpus": 1, "higher_is_better": True, "dtype": "f64",
