@@ -1,4 +1,4 @@
-"""Sharding one tessellation's cells over processes (CPU, gloo, world 2).
+"""Sharding one tessellation's cells over processes (CPU, gloo, worlds 2 and 3).
 
 Each rank computes its id range -- here with the oracle, standing in for the
 GPU on this CPU-only test -- and gather_summaries assembles the full result
@@ -28,7 +28,7 @@ def _rank(rank, world, port, q):
     import datetime
     import torch.distributed as dist
     from oracle.oracle import OracleTessellation
-    from vorothree_b200.shard import cell_range, gather_summaries
+    from vorothree_b200.shard import cell_range, gather_summaries, gather_summaries_tensors
     try:
         dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world,
                                 timeout=datetime.timedelta(seconds=60))
@@ -46,6 +46,12 @@ def _rank(rank, world, port, q):
         full.calculate(1)
         fv, fc, fn = full.summaries()
         ok = np.array_equal(gv, fv) and np.array_equal(gc, fc) and np.array_equal(gn, fn)
+        # the tensor form (the one calculate_sharded_device runs over NCCL)
+        import torch
+        tv, tc, tn = gather_summaries_tensors(torch.from_numpy(vol[b:e].copy()), torch.from_numpy(cen[b:e].copy()),
+                                              torch.from_numpy(nf[b:e].copy()), n)
+        ok = ok and np.array_equal(tv.numpy(), fv) and np.array_equal(tc.numpy(), fc) and np.array_equal(tn.numpy(), fn)
+        ok = ok and tn.dtype == torch.int32
         dist.destroy_process_group()
         q.put((rank, ok, None))
     except Exception as ex:  # reported to the parent
@@ -65,12 +71,13 @@ def test_cell_range_partition():
         cell_range(10, 2, 2)
 
 
-def test_sharded_summaries_gloo_world2(oracle_mod):
+@pytest.mark.parametrize("world", [2, 3])
+def test_sharded_summaries_gloo(oracle_mod, world):
     import multiprocessing as mp
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_rank, args=(r, 2, port, q)) for r in range(2)]
+    procs = [ctx.Process(target=_rank, args=(r, world, port, q)) for r in range(world)]
     for p in procs:
         p.start()
     results = [q.get(timeout=180) for _ in procs]

@@ -9,7 +9,8 @@ reference's API over that ABI.
 from ._lib import VoronoidError, load
 from .batch import TessellationBatch
 from .server import TessellationServer
-from .shard import calculate_sharded, cell_range, gather_summaries
+from .shard import (calculate_sharded, calculate_sharded_device, cell_range, device_summaries, gather_summaries,
+                    gather_summaries_tensors)
 from .tessellation import (WALL_ID_MAX, Algorithm3DGrid, BoundingBox, Cell3DFaces, ConeGeometry,
                            ConvexPolyhedronGeometry, CylinderGeometry, PlaneGeometry, SphereGeometry, Tessellation,
                            TorusGeometry, Wall, box_side, parse_generators)
@@ -17,4 +18,5 @@ from .tessellation import (WALL_ID_MAX, Algorithm3DGrid, BoundingBox, Cell3DFace
 __all__ = ["Algorithm3DGrid", "BoundingBox", "Cell3DFaces", "ConeGeometry", "ConvexPolyhedronGeometry",
            "CylinderGeometry", "PlaneGeometry", "SphereGeometry", "TorusGeometry",
            "Tessellation", "TessellationBatch", "TessellationServer", "Wall", "WALL_ID_MAX", "box_side", "VoronoidError", "load",
-           "calculate_sharded", "cell_range", "gather_summaries", "parse_generators"]
+           "calculate_sharded", "calculate_sharded_device", "cell_range", "device_summaries", "gather_summaries",
+           "gather_summaries_tensors", "parse_generators"]

@@ -12,9 +12,15 @@ the end -- the only collective, and it moves results, not work.
     t = Tessellation(bounds, Algorithm3DGrid(100, 100, 100))
     t.set_generators(points)                   # same points on every rank
     vol, cen, nfaces = calculate_sharded(t)    # full arrays on every rank
+
+calculate_sharded_device does the same without leaving the GPU: each rank's
+slice is read in place from the library's device buffers and the all-gather
+runs over NCCL (NVLink between the GPUs of a node), so the results arrive as
+CUDA tensors on every rank and never pass through host memory.
 """
 from __future__ import annotations
 
+import ctypes as C
 from typing import Optional, Tuple
 
 import numpy as np
@@ -86,3 +92,76 @@ def calculate_sharded(tess, group=None, rank: Optional[int] = None, world: Optio
     tess.calculate_range(begin, end)
     vol, cen, nf = tess.summaries()
     return gather_summaries(vol[begin:end], cen[begin:end], nf[begin:end], n, group)
+
+
+class _DeviceView:
+    """A library device buffer as torch sees it through the CUDA array
+    interface (no copy)."""
+
+    def __init__(self, ptr: int, shape, typestr: str):
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": typestr, "data": (ptr, True),
+                                         "version": 3, "strides": None}
+
+
+def device_summaries(tess):
+    """(vol[n], cen[n, 3], nfaces[n]) of the last calculate as CUDA tensors
+    that view the tessellation's own device buffers (no copy), ordered after
+    its stream.  They stay valid until the next set_generators, calculate or
+    close of `tess`; clone them to keep them longer."""
+    import torch
+    from ._lib import check
+    n = tess.count_cells()
+    dev = torch.device("cuda", torch.cuda.current_device())
+    if n == 0:
+        return (torch.empty(0, dtype=torch.float64, device=dev), torch.empty((0, 3), dtype=torch.float64, device=dev),
+                torch.empty(0, dtype=torch.int32, device=dev))
+    dv, dc, dn = C.c_void_p(), C.c_void_p(), C.c_void_p()
+    check(tess._L.vd_tess_device_results(tess._h, C.byref(dv), C.byref(dc), C.byref(dn)), tess._h)
+    torch.cuda.current_stream().wait_stream(torch.cuda.ExternalStream(tess.stream()))
+    vol = torch.as_tensor(_DeviceView(dv.value, (n,), "<f8"), device=dev)
+    cen = torch.as_tensor(_DeviceView(dc.value, (n, 3), "<f8"), device=dev)
+    nf = torch.as_tensor(_DeviceView(dn.value, (n,), "<i4"), device=dev)
+    return vol, cen, nf
+
+
+def gather_summaries_tensors(vol, cen, nfaces, n: int, group=None):
+    """gather_summaries for tensors on the process group's device: rank r
+    passes the results of its cell range (cell_range(n, r, world)); every rank
+    gets (vol[n], cen[n, 3], nfaces[n]) on the same device.  One all-gather of
+    a padded (width, 5) float64 block per rank; face counts travel as exact
+    float64 integers."""
+    import torch
+    import torch.distributed as dist
+    world = dist.get_world_size(group)
+    rank = dist.get_rank(group)
+    begin, end = cell_range(n, rank, world)
+    k = end - begin
+    if vol.shape[0] != k or cen.shape[0] != k or nfaces.shape[0] != k:
+        raise ValueError(f"rank {rank} holds {vol.shape[0]} cells, its range has {k}")
+    width = -(-n // world) if n else 0
+    pack = torch.zeros((width, 5), dtype=torch.float64, device=vol.device)
+    pack[:k, 0] = vol
+    pack[:k, 1:4] = cen.reshape(-1, 3)
+    pack[:k, 4] = nfaces.to(torch.float64)
+    parts = [torch.empty_like(pack) for _ in range(world)]
+    dist.all_gather(parts, pack, group=group)
+    full = torch.cat([p[:cell_range(n, r, world)[1] - cell_range(n, r, world)[0]] for r, p in enumerate(parts)])
+    return full[:, 0].contiguous(), full[:, 1:4].contiguous(), full[:, 4].to(torch.int32)
+
+
+def calculate_sharded_device(tess, group=None):
+    """calculate_sharded with the results kept on the GPU: this rank computes
+    its id range, its slice of the summaries is read in place from the
+    library's device buffers, and an NCCL all-gather assembles the full
+    arrays as CUDA tensors on every rank.  Needs a process group on the NCCL
+    backend; every rank must hold the same generators and walls."""
+    import torch.distributed as dist
+    if dist.get_backend(group) != "nccl":
+        raise ValueError("calculate_sharded_device needs an NCCL process group; use calculate_sharded")
+    world = dist.get_world_size(group)
+    rank = dist.get_rank(group)
+    n = tess.count_generators()
+    begin, end = cell_range(n, rank, world)
+    tess.calculate_range(begin, end)
+    vol, cen, nf = device_summaries(tess)
+    return gather_summaries_tensors(vol[begin:end], cen[begin:end], nf[begin:end], n, group)
