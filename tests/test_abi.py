@@ -47,3 +47,38 @@ def test_wall_id_rejected_before_device():
     import vorothree_b200 as v
     with pytest.raises(ValueError):
         v.Wall(-999, v.SphereGeometry([0, 0, 0], 1.0))
+
+
+def test_header_is_plain_c(tmp_path):
+    """The header is what a C, Rust (bindgen) or Go (cgo) binding reads: it
+    must compile as strict C99, and a C program must link every declared
+    entry point against the library and call the host-only parser."""
+    import shutil
+    import subprocess
+    if not shutil.which("gcc"):
+        pytest.skip("no C compiler")
+    from vorothree_b200 import _lib
+    _lib.load()
+    syms = declared_symbols()
+    src = tmp_path / "abi.c"
+    src.write_text(
+        "#include <stdio.h>\n#include <string.h>\n#include \"voronoid_b200.h\"\n"
+        "typedef void (*fn)(void);\n"
+        "static const fn all[] = {" + ", ".join(f"(fn){s}" for s in syms) + "};\n"
+        "int main(void) {\n"
+        "  const char* text = \"0 1.5 2 3\\n\\n7 -4e-1\\n\";\n"
+        "  double xyz[6];\n  size_t n = 0;\n"
+        "  if (vd_parse_generators(text, strlen(text), xyz, 2, &n) != VD_OK || n != 2) return 1;\n"
+        "  if (xyz[0] != 1.5 || xyz[2] != 3.0 || xyz[3] != -0.4 || xyz[5] != 0.0) return 2;\n"
+        "  if (vd_parse_generators(\"0 \\xff\", 3, xyz, 2, &n) != VD_EINVAL) return 3;\n"
+        "  printf(\"%u\\n\", (unsigned)(sizeof(all) / sizeof(all[0])));\n"
+        "  return 0;\n}\n")
+    exe = tmp_path / "abi"
+    libdir = os.path.join(ROOT, "vorothree_b200")
+    cmd = ["gcc", "-std=c99", "-Wall", "-Wextra", "-Werror", "-pedantic", "-I", os.path.join(ROOT, "include"),
+           str(src), "-o", str(exe), "-L", libdir, "-lvoronoid_b200", f"-Wl,-rpath,{libdir}"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, (r.returncode, r.stderr)
+    assert int(r.stdout.strip()) == len(syms)
