@@ -33,6 +33,10 @@ def _child(port, q):
         torch.cuda.set_device(0)
         dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
                                 timeout=datetime.timedelta(seconds=60))
+    except Exception as ex:  # reported to the parent
+        q.put((False, repr(ex)))
+        return
+    try:
         pts = blobs(60000, 8, 0.03, 0.5, 44)
         t = v.Tessellation(v.BoundingBox([0, 0, 0], [1, 1, 1]), v.Algorithm3DGrid(30, 30, 30))
         t.add_wall(v.Wall(-1000, v.SphereGeometry([0.5, 0.5, 0.5], 0.47)))
@@ -47,10 +51,11 @@ def _child(port, q):
         ok = ok and (np.array_equal(sv.cpu().numpy(), hv) and np.array_equal(sc.cpu().numpy(), hc)
                      and np.array_equal(sn.cpu().numpy(), hn))
         t.close()
-        dist.destroy_process_group()
         q.put((ok, None))
     except Exception as ex:  # reported to the parent
         q.put((False, repr(ex)))
+    finally:
+        dist.destroy_process_group()
 
 
 def test_sharded_device_nccl_one_rank():

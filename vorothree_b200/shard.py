@@ -96,10 +96,11 @@ def calculate_sharded(tess, group=None, rank: Optional[int] = None, world: Optio
 
 class _DeviceView:
     """A library device buffer as torch sees it through the CUDA array
-    interface (no copy)."""
+    interface (no copy).  torch takes no read-only flag, so the views are
+    writable; writing them changes the tessellation's results."""
 
     def __init__(self, ptr: int, shape, typestr: str):
-        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": typestr, "data": (ptr, True),
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": typestr, "data": (ptr, False),
                                          "version": 3, "strides": None}
 
 
