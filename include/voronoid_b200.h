@@ -176,6 +176,18 @@ int vd_tess_get_cell(vd_tess* t, size_t i, int32_t* n_vertices, int32_t* n_faces
                      int32_t* n_face_indices, double* vertices, uint32_t* face_counts,
                      uint32_t* face_indices, int32_t* face_neighbors);
 
+/* Tessellation::cells / map (tessellation.rs:391-412, 524-526) in bulk: the
+ * Cell3DFaces of cells [begin, end) as CSR arrays.  v_off, f_off, h_off
+ * [end - begin + 1] always get the offsets of each cell's vertices, faces and
+ * face entries (cells outside the last calculate_range read as empty).  With
+ * vertices [3 * v_off[n]], face_counts and face_neighbors [f_off[n]] and
+ * face_indices [h_off[n]] given (all four, or none for the sizes only), each
+ * cell's polytope is written at its offsets, exactly as vd_tess_get_cell gives
+ * it; face_indices are local to the cell.  Device memory grows with the range:
+ * export a large tessellation in ranges. */
+int vd_tess_export_cells(vd_tess* t, size_t begin, size_t end, int64_t* v_off, int64_t* f_off, int64_t* h_off,
+                         double* vertices, uint32_t* face_counts, uint32_t* face_indices, int32_t* face_neighbors);
+
 /* ---- device-resident results (for callers that keep data on the GPU) ---- */
 int vd_tess_device_results(vd_tess* t, const double** d_volume, const double** d_centroid3,
                            const int32_t** d_n_faces);

@@ -69,6 +69,7 @@ SIGNATURES = {
     "vd_tess_get_neighbors": (C.c_int, [_vp, _vp, _vp]),
     "vd_tess_get_face_areas": (C.c_int, [_vp, _vp, _vp]),
     "vd_tess_get_cell": (C.c_int, [_vp, C.c_size_t, _i32p, _i32p, _i32p, _vp, _vp, _vp, _vp]),
+    "vd_tess_export_cells": (C.c_int, [_vp, C.c_size_t, C.c_size_t, _i64p, _i64p, _i64p, _vp, _vp, _vp, _vp]),
     "vd_tess_device_results": (C.c_int, [_vp, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp)]),
     "vd_tess_stream": (C.c_int, [_vp, C.POINTER(_vp)]),
     "vd_tess_timings": (C.c_int, [_vp, C.POINTER(C.c_float)]),

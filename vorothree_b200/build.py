@@ -32,6 +32,7 @@ SOURCES = [
     ("vd_cell.cu", False),
     ("vd_seal.cu", False),
     ("vd_text.cpp", False),
+    ("vd_export.cu", False),
 ]
 
 

@@ -264,6 +264,11 @@ struct vd_tess {
   DevBuf<double> d_ex_v;
   DevBuf<uint32_t> d_ex_fc, d_ex_fi;
   DevBuf<int32_t> d_ex_fn, d_ex_sizes;
+  // bulk export (vd_tess_export_cells)
+  DevBuf<uint32_t> d_bx_items, d_bx_fc, d_bx_fi;
+  DevBuf<int32_t> d_bx_sizes, d_bx_fn;
+  DevBuf<long long> d_bx_off;
+  DevBuf<double> d_bx_v;
 
   // instrumentation
   cudaEvent_t ev[8] = {};
@@ -942,6 +947,8 @@ int vd_tess_destroy(vd_tess* t) {
   for (auto& b : t->scan32) b.release();
   for (auto& b : t->scan64) b.release();
   t->d_ex_v.release(); t->d_ex_fc.release(); t->d_ex_fi.release(); t->d_ex_fn.release(); t->d_ex_sizes.release();
+  t->d_bx_items.release(); t->d_bx_fc.release(); t->d_bx_fi.release(); t->d_bx_sizes.release();
+  t->d_bx_fn.release(); t->d_bx_off.release(); t->d_bx_v.release();
   if (t->stream) cudaStreamSynchronize(t->stream);
   for (auto& ev : t->ev)
     if (ev) cudaEventDestroy(ev);
@@ -1594,6 +1601,121 @@ int vd_tess_get_cell(vd_tess* t, size_t i, int32_t* n_vertices, int32_t* n_faces
   if (face_indices && sz[2])
     VD_CK(t, cudaMemcpyAsync(face_indices, t->d_ex_fi.p, (size_t)sz[2] * 4, cudaMemcpyDeviceToHost, s));
   VD_CK(t, cudaStreamSynchronize(s));
+  return VD_OK;
+}
+
+// Tessellation::cells / map (tessellation.rs:391-412, 524-526) for the cells
+// [begin, end): sizes, offsets and, when the arrays are given, every polytope.
+// The device pass rebuilds the cells with calculate()'s code; cells it cannot
+// hold (beyond the shared-memory capacities) and every cell of a sealed
+// tessellation go through get_cell.
+int vd_tess_export_cells(vd_tess* t, size_t begin, size_t end, int64_t* v_off, int64_t* f_off, int64_t* h_off,
+                         double* vertices, uint32_t* face_counts, uint32_t* face_indices, int32_t* face_neighbors) {
+  int r = check_ready(t);
+  if (r != VD_OK) return r;
+  if (!v_off || !f_off || !h_off) return VD_EINVAL;
+  if (begin > end || end > t->ncells) return fail(t, VD_EINVAL, "bad cell range [%zu, %zu)", begin, end);
+  const bool fill = vertices || face_counts || face_indices || face_neighbors;
+  if (fill && !(vertices && face_counts && face_indices && face_neighbors))
+    return fail(t, VD_EINVAL, "give all four polytope arrays, or none for the sizes");
+  if (end - begin > 0xFFFFFFF0ull) return fail(t, VD_EINVAL, "range too large");
+  cudaStream_t s = t->stream;
+  const size_t n = end - begin;
+  // only the cells of the last calculate's range have polytopes
+  const size_t lo = std::max(begin, t->range_begin), hi = std::min(end, t->range_end);
+  std::vector<int32_t> sz(3 * n, 0);
+  std::vector<size_t> host_cells;
+  const bool device = !t->sealed && hi > lo;
+  ExportArgs A;
+  memset(&A, 0, sizeof(A));
+  TessDesc T = make_desc(t);
+  if (t->sealed) {
+    for (size_t c = lo; c < hi; ++c) host_cells.push_back(c);
+  } else if (device) {
+    const size_t all = t->ncells;
+    VD_CK(t, t->d_flags.ensure(all + 1, s));
+    VD_CK(t, t->d_pos.ensure(all + 1, s));
+    VD_CK(t, t->d_bx_items.ensure(hi - lo, s));
+    VD_CK(t, t->d_bx_sizes.ensure(3 * n, s));
+    k_range_flags<<<grid_blocks(t, all, 256), 256, 0, s>>>(t->d_sorted.p, all, (long long)lo, (long long)hi,
+                                                         t->d_flags.p);
+    g_launches++;
+    VD_CK(t, cudaGetLastError());
+    VD_CK(t, cudaMemsetAsync(t->d_flags.p + all, 0, sizeof(uint32_t), s));
+    r = scan_excl<uint32_t, uint32_t>(t, t->d_flags.p, t->d_pos.p, all + 1, t->scan32);
+    if (r != VD_OK) return r;
+    k_range_compact<<<grid_blocks(t, all, 256), 256, 0, s>>>(t->d_sorted.p, all, t->d_flags.p, t->d_pos.p,
+                                                             t->d_bx_items.p);
+    g_launches++;
+    VD_CK(t, cudaGetLastError());
+    VD_CK(t, cudaMemsetAsync(t->d_bx_sizes.p, 0, 3 * n * sizeof(int32_t), s));
+    VD_CK(t, cudaMemsetAsync(t->d_ctl.p, 0, 3 * sizeof(unsigned int), s));
+    A.items = t->d_bx_items.p;
+    A.nitems = (uint32_t)(hi - lo);
+    A.cursor = t->d_ctl.p + kCtlCursor;
+    A.begin = begin;
+    A.sizes = t->d_bx_sizes.p;
+    VD_CK(t, launch_export_cells(T, A, 0, t->num_sms, s));
+    g_launches++;
+    VD_CK(t, cudaMemcpyAsync(sz.data(), t->d_bx_sizes.p, 3 * n * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    VD_CK(t, cudaStreamSynchronize(s));
+    for (size_t k = 0; k < n; ++k)
+      if (sz[3 * k] < 0) host_cells.push_back(begin + k);
+  }
+  for (size_t c : host_cells) {
+    int32_t nv = 0, nf = 0, nh = 0;
+    r = vd_tess_get_cell(t, c, &nv, &nf, &nh, nullptr, nullptr, nullptr, nullptr);
+    if (r != VD_OK) return r;
+    const size_t k = c - begin;
+    sz[3 * k] = nv;
+    sz[3 * k + 1] = nf;
+    sz[3 * k + 2] = nh;
+  }
+  v_off[0] = f_off[0] = h_off[0] = 0;
+  for (size_t k = 0; k < n; ++k) {
+    v_off[k + 1] = v_off[k] + sz[3 * k];
+    f_off[k + 1] = f_off[k] + sz[3 * k + 1];
+    h_off[k + 1] = h_off[k] + sz[3 * k + 2];
+  }
+  if (!fill) return VD_OK;
+  if (device) {
+    const size_t tv = (size_t)v_off[n], tf = (size_t)f_off[n], th = (size_t)h_off[n];
+    VD_CK(t, t->d_bx_off.ensure(3 * (n + 1), s));
+    VD_CK(t, t->d_bx_v.ensure(std::max<size_t>(3 * tv, 1), s));
+    VD_CK(t, t->d_bx_fc.ensure(std::max<size_t>(tf, 1), s));
+    VD_CK(t, t->d_bx_fn.ensure(std::max<size_t>(tf, 1), s));
+    VD_CK(t, t->d_bx_fi.ensure(std::max<size_t>(th, 1), s));
+    static_assert(sizeof(long long) == sizeof(int64_t), "offsets are 64-bit");
+    VD_CK(t, cudaMemcpyAsync(t->d_bx_off.p, v_off, (n + 1) * 8, cudaMemcpyHostToDevice, s));
+    VD_CK(t, cudaMemcpyAsync(t->d_bx_off.p + (n + 1), f_off, (n + 1) * 8, cudaMemcpyHostToDevice, s));
+    VD_CK(t, cudaMemcpyAsync(t->d_bx_off.p + 2 * (n + 1), h_off, (n + 1) * 8, cudaMemcpyHostToDevice, s));
+    VD_CK(t, cudaMemsetAsync(t->d_ctl.p, 0, 3 * sizeof(unsigned int), s));
+    A.voff = t->d_bx_off.p;
+    A.foff = t->d_bx_off.p + (n + 1);
+    A.hoff = t->d_bx_off.p + 2 * (n + 1);
+    A.verts = t->d_bx_v.p;
+    A.fc = t->d_bx_fc.p;
+    A.fi = t->d_bx_fi.p;
+    A.fn = t->d_bx_fn.p;
+    A.sizes = nullptr;
+    VD_CK(t, launch_export_cells(T, A, 1, t->num_sms, s));
+    g_launches++;
+    if (tv) VD_CK(t, cudaMemcpyAsync(vertices, t->d_bx_v.p, 3 * tv * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (tf) {
+      VD_CK(t, cudaMemcpyAsync(face_counts, t->d_bx_fc.p, tf * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+      VD_CK(t, cudaMemcpyAsync(face_neighbors, t->d_bx_fn.p, tf * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    }
+    if (th) VD_CK(t, cudaMemcpyAsync(face_indices, t->d_bx_fi.p, th * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    VD_CK(t, cudaStreamSynchronize(s));
+  }
+  // the cells left to get_cell write straight into their slots
+  for (size_t c : host_cells) {
+    const size_t k = c - begin;
+    int32_t nv = 0, nf = 0, nh = 0;
+    r = vd_tess_get_cell(t, c, &nv, &nf, &nh, vertices + 3 * v_off[k], face_counts + f_off[k],
+                         face_indices + h_off[k], face_neighbors + f_off[k]);
+    if (r != VD_OK) return r;
+  }
   return VD_OK;
 }
 

@@ -51,6 +51,24 @@ cudaError_t launch_clip_fp64_big_batched(const TessDesc* descs, const uint32_t* 
 // false with a message for a bad descriptor.
 bool wall_from_desc(const vd_wall_desc& d, Wall* w, std::vector<double>* planes, std::string* err);
 
+// bulk polytope export (vd_export.cu): per-cell arrays are indexed by
+// cell id - begin
+struct ExportArgs {
+  const uint32_t* items;  // cell ids to rebuild, in bin order
+  uint32_t nitems;
+  unsigned int* cursor;   // persistent-warp work counter, zeroed before each pass
+  size_t begin;
+  int32_t* sizes;         // pass 0: nv, nf, nh of each cell (-1: left to the host)
+  const long long* voff;  // pass 1: each cell's first vertex, face and face entry
+  const long long* foff;
+  const long long* hoff;
+  double* verts;
+  uint32_t* fc;
+  uint32_t* fi;
+  int32_t* fn;
+};
+cudaError_t launch_export_cells(const TessDesc& T, const ExportArgs& A, int pass, int num_sms, cudaStream_t s);
+
 // the generator text format of Tessellation::read_generators (vd_text.cpp):
 // false with a message when the text is not UTF-8
 bool parse_generators(const char* text, size_t len, std::vector<double>* xyz, std::string* err);

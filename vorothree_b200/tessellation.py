@@ -678,13 +678,53 @@ class Tessellation:
         self._ck(self._L.vd_tess_timings(self._h, t))
         return tuple(t) + (self.count_cells(),)
 
+    def export_cells(self, begin: int = 0, end: Optional[int] = None) -> dict:
+        """The polytopes of cells [begin, end) in one device pass, as CSR:
+        ``v_off``, ``f_off``, ``h_off`` (offsets per cell), ``vertices``
+        (flat xyz), ``face_counts``, ``face_indices`` (local to each cell) and
+        ``face_neighbors`` -- each cell exactly as get_cell gives it."""
+        n_all = self.count_cells()
+        end = n_all if end is None else int(end)
+        begin = int(begin)
+        n = max(end - begin, 0)
+        vo = np.zeros(n + 1, np.int64)
+        fo = np.zeros(n + 1, np.int64)
+        ho = np.zeros(n + 1, np.int64)
+        i64 = C.POINTER(C.c_int64)
+        self._ck(self._L.vd_tess_export_cells(self._h, begin, end, vo.ctypes.data_as(i64), fo.ctypes.data_as(i64),
+                                              ho.ctypes.data_as(i64), None, None, None, None))
+        v = np.zeros(3 * max(int(vo[-1]), 1), np.float64)
+        fc = np.zeros(max(int(fo[-1]), 1), np.uint32)
+        fi = np.zeros(max(int(ho[-1]), 1), np.uint32)
+        fn = np.zeros(max(int(fo[-1]), 1), np.int32)
+        self._ck(self._L.vd_tess_export_cells(self._h, begin, end, vo.ctypes.data_as(i64), fo.ctypes.data_as(i64),
+                                              ho.ctypes.data_as(i64), _vp(v), _vp(fc), _vp(fi), _vp(fn)))
+        return {"v_off": vo, "f_off": fo, "h_off": ho, "vertices": v[:3 * int(vo[-1])],
+                "face_counts": fc[:int(fo[-1])], "face_indices": fi[:int(ho[-1])], "face_neighbors": fn[:int(fo[-1])]}
+
+    def _iter_cells(self, chunk: int = 1 << 18):
+        """Every cell as a Cell3DFaces, exported a range at a time."""
+        n = self.count_cells()
+        vol, cen, _ = self._summary_cache()
+        aoff, ar = self._area_cache()
+        for b in range(0, n, chunk):
+            e = min(n, b + chunk)
+            x = self.export_cells(b, e)
+            vo, fo, ho = x["v_off"], x["f_off"], x["h_off"]
+            for k in range(e - b):
+                i = b + k
+                yield Cell3DFaces(i, x["vertices"][3 * vo[k]:3 * vo[k + 1]], x["face_counts"][fo[k]:fo[k + 1]],
+                                  x["face_indices"][ho[k]:ho[k + 1]], x["face_neighbors"][fo[k]:fo[k + 1]],
+                                  vol[i], cen[i], ar[aoff[i]:aoff[i + 1]])
+
     def cells(self) -> List[Cell3DFaces]:
-        return [self.get_cell(i) for i in range(self.count_cells())]
+        """Tessellation::cells (tessellation.rs:524-526)."""
+        return list(self._iter_cells())
 
     def map(self, f: Callable[[Cell3DFaces], object]) -> list:
         """Tessellation::map (tessellation.rs:391-412): compute, then apply f."""
         self.calculate()
-        return [f(self.get_cell(i)) for i in range(self.count_cells())]
+        return [f(c) for c in self._iter_cells()]
 
     # ---- instrumentation -------------------------------------------------
     def stream(self) -> int:
