@@ -1606,9 +1606,9 @@ int vd_tess_get_cell(vd_tess* t, size_t i, int32_t* n_vertices, int32_t* n_faces
 
 // Tessellation::cells / map (tessellation.rs:391-412, 524-526) for the cells
 // [begin, end): sizes, offsets and, when the arrays are given, every polytope.
-// The device pass rebuilds the cells with calculate()'s code; cells it cannot
-// hold (beyond the shared-memory capacities) and every cell of a sealed
-// tessellation go through get_cell.
+// The device pass rebuilds the cells with calculate()'s code (and the seal
+// clips, when the tessellation is sealed); cells it cannot hold (beyond the
+// shared-memory capacities) go through get_cell.
 int vd_tess_export_cells(vd_tess* t, size_t begin, size_t end, int64_t* v_off, int64_t* f_off, int64_t* h_off,
                          double* vertices, uint32_t* face_counts, uint32_t* face_indices, int32_t* face_neighbors) {
   int r = check_ready(t);
@@ -1625,13 +1625,15 @@ int vd_tess_export_cells(vd_tess* t, size_t begin, size_t end, int64_t* v_off, i
   const size_t lo = std::max(begin, t->range_begin), hi = std::min(end, t->range_end);
   std::vector<int32_t> sz(3 * n, 0);
   std::vector<size_t> host_cells;
-  const bool device = !t->sealed && hi > lo;
+  const bool device = hi > lo;
   ExportArgs A;
   memset(&A, 0, sizeof(A));
   TessDesc T = make_desc(t);
-  if (t->sealed) {
-    for (size_t c = lo; c < hi; ++c) host_cells.push_back(c);
-  } else if (device) {
+  // a sealed tessellation's seal clips, as get_cell applies them: nothing logged
+  SealArgs SA = seal_args(t, 1);
+  SA.cnt = nullptr;
+  SA.rec_cap = 0;
+  if (device) {
     const size_t all = t->ncells;
     VD_CK(t, t->d_flags.ensure(all + 1, s));
     VD_CK(t, t->d_pos.ensure(all + 1, s));
@@ -1655,7 +1657,8 @@ int vd_tess_export_cells(vd_tess* t, size_t begin, size_t end, int64_t* v_off, i
     A.cursor = t->d_ctl.p + kCtlCursor;
     A.begin = begin;
     A.sizes = t->d_bx_sizes.p;
-    VD_CK(t, launch_export_cells(T, A, 0, t->num_sms, s));
+    VD_CK(t, t->sealed ? launch_seal_export_cells(T, A, SA, 0, t->num_sms, s)
+                       : launch_export_cells(T, A, 0, t->num_sms, s));
     g_launches++;
     VD_CK(t, cudaMemcpyAsync(sz.data(), t->d_bx_sizes.p, 3 * n * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
     VD_CK(t, cudaStreamSynchronize(s));
@@ -1698,7 +1701,8 @@ int vd_tess_export_cells(vd_tess* t, size_t begin, size_t end, int64_t* v_off, i
     A.fi = t->d_bx_fi.p;
     A.fn = t->d_bx_fn.p;
     A.sizes = nullptr;
-    VD_CK(t, launch_export_cells(T, A, 1, t->num_sms, s));
+    VD_CK(t, t->sealed ? launch_seal_export_cells(T, A, SA, 1, t->num_sms, s)
+                       : launch_export_cells(T, A, 1, t->num_sms, s));
     g_launches++;
     if (tv) VD_CK(t, cudaMemcpyAsync(vertices, t->d_bx_v.p, 3 * tv * sizeof(double), cudaMemcpyDeviceToHost, s));
     if (tf) {

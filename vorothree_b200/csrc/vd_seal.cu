@@ -17,6 +17,7 @@
 // These kernels are separate instantiations: the production clip kernel's
 // code is unchanged.  Compiled with -fmad=false, like every FP64 path.
 #include "vd_clip.cuh"
+#include "vd_export.cuh"
 #include "vd_internal.h"
 
 namespace vd {
@@ -280,6 +281,43 @@ cudaError_t launch_prune_log_place(const PruneRec* rec, uint32_t nrec, const Pru
   if (nrec == 0 && npos == 0) return cudaSuccess;
   k_prune_log_place<<<nblocks, 256, 0, s>>>(rec, nrec, pos, npos, off, poff, out, out_pos);
   return cudaGetLastError();
+}
+
+// bulk export of a sealed tessellation: every cell rebuilt with its seal
+// clips (none for a cell without a curved-wall face), nothing logged
+namespace {
+
+struct SealExtra {
+  SealArgs A;
+  template <class C>
+  __device__ int operator()(const TessDesc& T, uint32_t cell, WarpPoly<C>& P, PolyState& S) const {
+    int nlog = 0;
+    return seal_clips<C>(T, A, cell, P, S, false, &nlog);
+  }
+};
+
+template <class C, int PASS>
+__global__ void __launch_bounds__(kExportWarps * 32)
+    k_seal_export(const TessDesc T, const ExportArgs E, const SealArgs A) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  export_worker<C, PASS>(T, E, reinterpret_cast<WarpPoly<C>*>(smem)[threadIdx.x >> 5], SealExtra{A});
+}
+
+template <int PASS>
+cudaError_t seal_export_pass(const TessDesc& T, const ExportArgs& E, const SealArgs& A, int num_sms, cudaStream_t s) {
+  const size_t smem = sizeof(WarpPoly<FastCfg>) * kExportWarps;
+  int nblocks = 1;
+  cudaError_t e = export_launch_shape(k_seal_export<FastCfg, PASS>, smem, E.nitems, num_sms, &nblocks);
+  if (e != cudaSuccess) return e;
+  k_seal_export<FastCfg, PASS><<<nblocks, kExportWarps * 32, smem, s>>>(T, E, A);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launch_seal_export_cells(const TessDesc& T, const ExportArgs& E, const SealArgs& A, int pass,
+                                     int num_sms, cudaStream_t s) {
+  return pass == 0 ? seal_export_pass<0>(T, E, A, num_sms, s) : seal_export_pass<1>(T, E, A, num_sms, s);
 }
 
 }  // namespace vd
