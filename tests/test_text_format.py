@@ -135,3 +135,29 @@ def test_random_round_trip():
         got = parse(text)
         want = np.array([[float(fmt.format(c)) for c in p] for p in g])
         assert np.array_equal(got, want), fmt
+
+
+def test_random_tokens_against_grammar():
+    """20,000 random tokens over the characters the grammar uses, each read as
+    a model of Rust's f64 FromStr reads it: the token must match the grammar
+    (case-insensitive), and then its value is the correctly rounded one
+    (Python's float, which accepts every such token, rounds the same way)."""
+    import re
+    rust = re.compile(r"[+-]?(inf|infinity|nan|(\d+\.?\d*|\.\d+)(e[+-]?\d+)?)", re.I)
+    rng = np.random.Generator(np.random.PCG64(77))
+    alphabet = list("0123456789012345678901234567890123456789..eE+-+-infatyINFATY_x,")
+    toks = []
+    for _ in range(20000):
+        n = int(rng.integers(1, 14))
+        toks.append("".join(alphabet[i] for i in rng.integers(0, len(alphabet), n)))
+    text = "".join(f"{k} {toks[3 * k]} {toks[3 * k + 1]} {toks[3 * k + 2]}\n" for k in range(len(toks) // 3))
+    got = parse(text).reshape(-1)
+    valid = 0
+    for tok, g in zip(toks, got):
+        want = float(tok) if rust.fullmatch(tok) else 0.0
+        valid += rust.fullmatch(tok) is not None
+        if math.isnan(want):
+            assert math.isnan(g) and bool(np.signbit(g)) == tok.startswith("-"), tok
+        else:
+            assert bits(g) == bits(want), (tok, g, want)
+    assert valid > 2000
