@@ -46,6 +46,12 @@ def _child(port, q):
         dv, dc, dn = v.device_summaries(t)
         ok = (np.array_equal(dv.cpu().numpy(), hv) and np.array_equal(dc.cpu().numpy(), hc)
               and np.array_equal(dn.cpu().numpy(), hn))
+        # the same generators through an NCCL broadcast into device memory
+        t2 = v.Tessellation(v.BoundingBox([0, 0, 0], [1, 1, 1]), v.Algorithm3DGrid(30, 30, 30))
+        t2.add_wall(v.Wall(-1000, v.SphereGeometry([0.5, 0.5, 0.5], 0.47)))
+        ok = ok and v.set_generators_broadcast(t2, pts) == t.count_generators()
+        ok = ok and np.array_equal(t2.generators(), t.generators())
+        t2.close()
         sv, sc, sn = v.calculate_sharded_device(t)
         ok = ok and sv.is_cuda and sn.dtype == torch.int32
         ok = ok and (np.array_equal(sv.cpu().numpy(), hv) and np.array_equal(sc.cpu().numpy(), hc)

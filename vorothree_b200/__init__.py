@@ -10,7 +10,7 @@ from ._lib import VoronoidError, load
 from .batch import TessellationBatch
 from .server import TessellationServer
 from .shard import (calculate_sharded, calculate_sharded_device, cell_range, device_summaries, gather_summaries,
-                    gather_summaries_tensors)
+                    gather_summaries_tensors, set_generators_broadcast)
 from .tessellation import (WALL_ID_MAX, Algorithm3DGrid, BoundingBox, Cell3DFaces, ConeGeometry,
                            ConvexPolyhedronGeometry, CylinderGeometry, PlaneGeometry, SphereGeometry, Tessellation,
                            TorusGeometry, Wall, box_side, parse_generators)
@@ -19,4 +19,4 @@ __all__ = ["Algorithm3DGrid", "BoundingBox", "Cell3DFaces", "ConeGeometry", "Con
            "CylinderGeometry", "PlaneGeometry", "SphereGeometry", "TorusGeometry",
            "Tessellation", "TessellationBatch", "TessellationServer", "Wall", "WALL_ID_MAX", "box_side", "VoronoidError", "load",
            "calculate_sharded", "calculate_sharded_device", "cell_range", "device_summaries", "gather_summaries",
-           "gather_summaries_tensors", "parse_generators"]
+           "gather_summaries_tensors", "parse_generators", "set_generators_broadcast"]

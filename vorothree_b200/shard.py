@@ -166,3 +166,31 @@ def calculate_sharded_device(tess, group=None):
     tess.calculate_range(begin, end)
     vol, cen, nf = device_summaries(tess)
     return gather_summaries_tensors(vol[begin:end], cen[begin:end], nf[begin:end], n, group)
+
+
+def set_generators_broadcast(tess, points=None, src: int = 0, group=None) -> int:
+    """set_generators on every rank from the generators rank `src` holds: the
+    array (host array or CUDA tensor, (n, 3) float64) crosses to the other
+    GPUs in one NCCL broadcast into device memory and each rank filters and
+    bins it there (set_generators_device), so no rank stages it through host
+    memory.  Other ranks pass points=None.  Returns the kept count."""
+    import torch
+    import torch.distributed as dist
+    if dist.get_backend(group) != "nccl":
+        raise ValueError("set_generators_broadcast needs an NCCL process group")
+    dev = torch.device("cuda", torch.cuda.current_device())
+    rank = dist.get_rank(group)
+    n = torch.zeros(1, dtype=torch.int64, device=dev)
+    if rank == src:
+        pts = torch.as_tensor(points, dtype=torch.float64).reshape(-1, 3)
+        n[0] = pts.shape[0]
+    dist.broadcast(n, src=src, group=group)
+    buf = torch.empty((int(n.item()), 3), dtype=torch.float64, device=dev)
+    if rank == src:
+        buf.copy_(pts)
+    dist.broadcast(buf, src=src, group=group)
+    # the library reads the buffer on its own stream
+    torch.cuda.current_stream().synchronize()
+    kept = tess.set_generators_device(buf.data_ptr(), buf.shape[0])
+    torch.cuda.synchronize()
+    return kept
