@@ -280,6 +280,24 @@ typedef struct {
   const double* normals;
   int nplanes;
 } vd_wall_desc;
+
+/* ---- one wall, one grid, on the host (no device) ---- */
+/* Wall::contains (wall/mod.rs:38-40; each geometry's contains, wall_3d.rs:31-36,
+ * 73-78, 132-143, 202-214, 293-309, 691-701) for a wall described as for
+ * batches: *inside = 1 or 0.  VD_EINVAL for a bad descriptor. */
+int vd_wall_contains(const vd_wall_desc* wall, const double point[3], int* inside);
+/* Wall::cut (wall/mod.rs:42-44; wall_3d.rs:38-42, 80-100, 145-173, 216-261,
+ * 311-364, 703-708): the planes the wall emits for one generator, in the
+ * order the reference's callback receives them (point, normal pointing out of
+ * the valid region); *n = their count (0 or 1, or the polyhedron's planes),
+ * min(*n, cap) written.  Bit for bit the planes the clip kernels use. */
+int vd_wall_cut(const vd_wall_desc* wall, const double generator[3], double* points, double* normals, int cap,
+                int* n);
+/* Algorithm3DGrid::get_bin_index (algo_3d_grid.rs:97-107) of the grid
+ * Algorithm3DGrid::new(nx, ny, nz, bounds) builds */
+int vd_grid_bin_index(const double bmin[3], const double bmax[3], int nx, int ny, int nz, const double point[3],
+                      size_t* index);
+
 int vd_batch_create(vd_batch** out);
 int vd_batch_destroy(vd_batch* b);
 const char* vd_batch_last_error(const vd_batch* b);

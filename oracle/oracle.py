@@ -62,6 +62,10 @@ def lib():
     L.vdo_set_generator.argtypes = [vp, C.c_size_t, d3]
     L.vdo_random_generators.restype = C.c_size_t
     L.vdo_random_generators.argtypes = [vp, C.c_size_t, C.c_uint64]
+    L.vdo_wall_contains_at.restype = C.c_int
+    L.vdo_wall_contains_at.argtypes = [vp, C.c_int, d3]
+    L.vdo_wall_cut_at.restype = C.c_int
+    L.vdo_wall_cut_at.argtypes = [vp, C.c_int, d3, d3, d3]
     L.vdo_get_bins.restype = None
     L.vdo_get_bins.argtypes = [vp, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]
     L.vdo_calculate.argtypes = [vp, C.c_int]
@@ -314,6 +318,19 @@ class OracleTessellation:
 
     def random_generators(self, count: int, seed: int) -> int:
         return int(lib().vdo_random_generators(self._h, int(count), int(seed)))
+
+    def wall_contains(self, w: int, point) -> bool:
+        a, pa = _d(np.asarray(point, np.float64).reshape(3))
+        return bool(lib().vdo_wall_contains_at(self._h, int(w), pa))
+
+    def wall_cut(self, w: int, generator):
+        """[(point, normal), ...] wall w emits for the generator."""
+        a, pa = _d(np.asarray(generator, np.float64).reshape(3))
+        p = np.zeros(3 * 256, np.float64)
+        n = np.zeros(3 * 256, np.float64)
+        k = lib().vdo_wall_cut_at(self._h, int(w), pa, p.ctypes.data_as(C.POINTER(C.c_double)),
+                                  n.ctypes.data_as(C.POINTER(C.c_double)))
+        return [(p[3 * q:3 * q + 3].copy(), n[3 * q:3 * q + 3].copy()) for q in range(k)]
 
     def bins(self):
         """grid_bins as a list of id lists, in visit order."""

@@ -1150,6 +1150,12 @@ void vdo_relax(vdo_tess* t) {
   free(ng);
 }
 
+/* one wall's WallGeometry::contains / cut (the cut's planes into p, n; returns
+   their count), for the tests of the library's host-side wall queries */
+int vdo_wall_contains_at(const vdo_tess* t, int w, const double p[3]) { return wall_contains(&t->walls[w], p); }
+int vdo_wall_cut_at(const vdo_tess* t, int w, const double g[3], double* p, double* n) {
+  return wall_cut(&t->walls[w], g, p, n);
+}
 size_t vdo_count_generators(const vdo_tess* t) { return t->ngen; }
 void vdo_get_bins(const vdo_tess* t, size_t* start, size_t* members) {
   memcpy(start, t->bin_start, (t->nx * t->ny * t->nz + 1) * sizeof(size_t));

@@ -64,6 +64,9 @@ void vdo_clear_walls(vdo_tess* t);
 size_t vdo_set_generators(vdo_tess* t, const double* xyz, size_t n);
 void vdo_set_generator(vdo_tess* t, size_t index, const double xyz[3]);
 size_t vdo_random_generators(vdo_tess* t, size_t count, uint64_t seed);
+/* wall w's contains / cut (p, n get 3 * count doubles; count <= 64) */
+int vdo_wall_contains_at(const vdo_tess* t, int w, const double p[3]);
+int vdo_wall_cut_at(const vdo_tess* t, int w, const double g[3], double* p, double* n);
 /* grid_bins as CSR: start[nbins + 1], members[count_generators] */
 void vdo_get_bins(const vdo_tess* t, size_t* start, size_t* members);
 void vdo_calculate(vdo_tess* t, int nthreads);

@@ -240,3 +240,63 @@ def test_random_generators_oracle(oracle_mod):
     assert 5 < n < 50
     t.calculate(1)
     assert t.count_cells() == n
+
+
+def _oracle_wall(oracle_mod, w):
+    import vorothree_b200 as v
+    t = oracle_mod.OracleTessellation([0, 0, 0], [10, 10, 10], 2, 2, 2)
+    g = w.geometry
+    if isinstance(g, v.PlaneGeometry):
+        t.add_wall_plane(g.point, g.normal, w.id())
+    elif isinstance(g, v.SphereGeometry):
+        t.add_wall_sphere(g.center, g.radius, w.id())
+    elif isinstance(g, v.CylinderGeometry):
+        t.add_wall_cylinder(g.center, g.axis, g.radius, w.id())
+    elif isinstance(g, v.ConeGeometry):
+        t.add_wall_cone(g.tip, g.axis, g.angle, w.id())
+    elif isinstance(g, v.TorusGeometry):
+        t.add_wall_torus(g.center, g.axis, g.major_radius, g.minor_radius, w.id())
+    else:
+        t.add_wall_polyhedron(g.points, g.normals, w.id())
+    return t
+
+
+def test_host_wall_queries_match_oracle(oracle_mod):
+    """Wall::contains and Wall::cut through the library's host entry points
+    (the functions its kernels use) against the oracle, bit for bit, for every
+    wall kind at points spread over and around the walls."""
+    import vorothree_b200 as v
+    P = v.ConvexPolyhedronGeometry
+    walls = [v.Wall(WALL, v.PlaneGeometry([5, 5, 5], [0.3, -1.0, 0.2])),
+             v.Wall(WALL, v.SphereGeometry([5, 5, 5], 3.5)),
+             v.Wall(WALL, v.CylinderGeometry([5, 5, 5], [0.2, 0.1, 1.0], 4.0)),
+             v.Wall(WALL, v.ConeGeometry([5, 5, -1], [0.1, 0.0, 1.0], 0.45)),
+             v.Wall(WALL, v.TorusGeometry([5, 5, 5], [0.0, 0.3, 1.0], 3.0, 1.6)),
+             v.Wall(WALL, P.new_dodecahedron([5, 5, 5], 4.5)),
+             v.Wall(WALL, P.new_tetrahedron([5, 5, 5], 4.5))]
+    rng = np.random.Generator(np.random.PCG64(41))
+    pts = np.concatenate([rng.uniform(-2, 12, size=(1500, 3)), [[5, 5, 5], [5, 5, -1], [5, 5, 8], [8, 5, 5]]])
+    for w in walls:
+        o = _oracle_wall(oracle_mod, w)
+        for p in pts:
+            assert w.contains(p) == o.wall_contains(0, p), (w.geometry, p)
+            got = []
+            w.cut(p, lambda a, b: got.append((a, b)))
+            want = o.wall_cut(0, p)
+            assert len(got) == len(want), (w.geometry, p)
+            for (a, b), (c, d) in zip(got, want):
+                assert np.array_equal(a, c) and np.array_equal(b, d), (w.geometry, p)
+
+
+def test_grid_bin_index_matches_oracle(oracle_mod):
+    import vorothree_b200 as v
+    rng = np.random.Generator(np.random.PCG64(42))
+    for (lo, hi, n) in [([0, 0, 0], [1, 1, 1], (10, 10, 10)), ([-5, 2, 0], [7, 3, 0.5], (13, 4, 7))]:
+        b = v.BoundingBox(lo, hi)
+        g = v.Algorithm3DGrid.new(*n, b)
+        o = oracle_mod.OracleTessellation(lo, hi, *n)
+        ext = np.asarray(hi, float) - np.asarray(lo, float)
+        pts = np.asarray(lo) + rng.uniform(-0.2, 1.2, size=(3000, 3)) * ext
+        pts[:5] = hi
+        for p in pts:
+            assert g.get_bin_index(*p) == o.bin_index(*p), p

@@ -24,6 +24,7 @@
 
 #include "../../include/voronoid_b200.h"
 #include "vd_binning.cuh"
+#include "vd_wall.cuh"
 #include "vd_internal.h"
 #include "vd_order.h"
 
@@ -1163,6 +1164,69 @@ int vd_tess_random_generators(vd_tess* t, size_t count, uint64_t seed, size_t* n
   const int r = set_generators_from_device(t, t->d_in.p, found, &kept);
   if (r == VD_OK && n_found) *n_found = kept;
   return r;
+}
+
+// Wall::contains / Wall::cut and Algorithm3DGrid::get_bin_index on the host,
+// with the functions the kernels use (wall_contains, wall_plane) and the
+// binning's clamp-scale-truncate
+int vd_wall_contains(const vd_wall_desc* d, const double point[3], int* inside) {
+  if (!d || !point || !inside) return VD_EINVAL;
+  Wall w;
+  std::vector<double> planes;
+  std::string err;
+  if (!wall_from_desc(*d, &w, &planes, &err)) {
+    set_thread_error(err.c_str());
+    return VD_EINVAL;
+  }
+  *inside = wall_contains(w, planes.data(), point[0], point[1], point[2]) ? 1 : 0;
+  return VD_OK;
+}
+
+int vd_wall_cut(const vd_wall_desc* d, const double generator[3], double* points, double* normals, int cap,
+                int* n) {
+  if (!d || !generator || !n || cap < 0 || (cap > 0 && (!points || !normals))) return VD_EINVAL;
+  Wall w;
+  std::vector<double> planes;
+  std::string err;
+  if (!wall_from_desc(*d, &w, &planes, &err)) {
+    set_thread_error(err.c_str());
+    return VD_EINVAL;
+  }
+  if (w.kind == kWallPolyhedron) {
+    *n = w.np;
+    for (int k = 0; k < w.np && k < cap; ++k)
+      for (int a = 0; a < 3; ++a) {
+        points[3 * k + a] = planes[6 * k + a];
+        normals[3 * k + a] = planes[6 * k + 3 + a];
+      }
+    return VD_OK;
+  }
+  double p[3], q[3];
+  *n = wall_plane(w, generator[0], generator[1], generator[2], p, q) ? 1 : 0;
+  if (*n && cap > 0)
+    for (int a = 0; a < 3; ++a) {
+      points[a] = p[a];
+      normals[a] = q[a];
+    }
+  return VD_OK;
+}
+
+int vd_grid_bin_index(const double bmin[3], const double bmax[3], int nx, int ny, int nz, const double point[3],
+                      size_t* index) {
+  if (!bmin || !bmax || !point || !index || nx <= 0 || ny <= 0 || nz <= 0) return VD_EINVAL;
+  const int n[3] = {nx, ny, nz};
+  size_t idx = 0, stride = 1;
+  for (int a = 0; a < 3; ++a) {
+    const double scale = (double)n[a] / (bmax[a] - bmin[a]);
+    const double limit = (double)n[a] - 1e-5;
+    double u = (point[a] - bmin[a]) * scale;
+    if (u < 0.0) u = 0.0;
+    if (u > limit) u = limit;
+    idx += (u > 0.0 ? (size_t)u : 0) * stride;
+    stride *= (size_t)n[a];
+  }
+  *index = idx;
+  return VD_OK;
 }
 
 // Tessellation::read_generators / import_generators (tessellation.rs:126-171):

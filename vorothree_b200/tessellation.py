@@ -54,8 +54,60 @@ class Algorithm3DGrid:
         self.grid_res_x, self.grid_res_y, self.grid_res_z = int(nx), int(ny), int(nz)
         self.bounds = bounds
 
+    @classmethod
+    def new(cls, nx: int, ny: int, nz: int, bounds: Optional[BoundingBox] = None) -> "Algorithm3DGrid":
+        """Algorithm3DGrid::new (algo_3d_grid.rs:47-95)."""
+        return cls(nx, ny, nz, bounds)
 
-class PlaneGeometry:
+    def get_bin_index(self, x: float, y: float, z: float, bounds: Optional[BoundingBox] = None) -> int:
+        """Algorithm3DGrid::get_bin_index (algo_3d_grid.rs:97-107): the bin
+        of a point, x fastest, coordinates clamped into the grid."""
+        b = bounds if bounds is not None else self.bounds
+        if b is None:
+            raise ValueError("get_bin_index needs the grid's bounds")
+        L = load()
+        mn = np.asarray(b.min, np.float64)
+        mx = np.asarray(b.max, np.float64)
+        p = np.asarray([x, y, z], np.float64)
+        out = C.c_size_t()
+        check(L.vd_grid_bin_index(_dp(mn), _dp(mx), self.grid_res_x, self.grid_res_y, self.grid_res_z, _dp(p),
+                                  C.byref(out)))
+        return out.value
+
+
+class _WallQueries:
+    """WallGeometry::contains / cut (wall_3d.rs) on the host, through the same
+    functions the kernels use, so they agree with calculate() bit for bit."""
+
+    def _desc(self):
+        from .batch import _walls
+        return _walls([Wall(WALL_ID_MAX, self)])
+
+    def contains(self, point: Sequence[float]) -> bool:
+        L = load()
+        d = self._desc()
+        p = np.asarray(point, np.float64).reshape(3)
+        inside = C.c_int()
+        check(L.vd_wall_contains(C.cast(d.arr, C.c_void_p), _dp(p), C.byref(inside)))
+        return bool(inside.value)
+
+    def cut(self, generator: Sequence[float], callback: Callable[[np.ndarray, np.ndarray], object]) -> None:
+        """Calls callback(point, normal) for each plane the wall emits for
+        `generator`, in order (normal pointing out of the valid region)."""
+        L = load()
+        d = self._desc()
+        g = np.asarray(generator, np.float64).reshape(3)
+        n = C.c_int()
+        check(L.vd_wall_cut(C.cast(d.arr, C.c_void_p), _dp(g), None, None, 0, C.byref(n)))
+        k = n.value
+        pts = np.zeros(3 * max(k, 1), np.float64)
+        nrm = np.zeros(3 * max(k, 1), np.float64)
+        check(L.vd_wall_cut(C.cast(d.arr, C.c_void_p), _dp(g), _dp(pts), _dp(nrm), k, C.byref(n)))
+        for q in range(k):
+            callback(pts[3 * q:3 * q + 3].copy(), nrm[3 * q:3 * q + 3].copy())
+
+
+class PlaneGeometry(_WallQueries):
     """Plane wall; ``normal`` points into the valid region and is normalised."""
 
     def __init__(self, point: Sequence[float], normal: Sequence[float]):
@@ -66,7 +118,7 @@ class PlaneGeometry:
         return True
 
 
-class SphereGeometry:
+class SphereGeometry(_WallQueries):
     """Spherical wall; the valid region is inside."""
 
     def __init__(self, center: Sequence[float], radius: float):
@@ -77,7 +129,7 @@ class SphereGeometry:
         return False
 
 
-class CylinderGeometry:
+class CylinderGeometry(_WallQueries):
     """Infinite cylinder wall (wall_3d.rs:107-174); the valid region is inside.
     ``axis`` is normalised on the device side as the reference's constructor does."""
 
@@ -90,7 +142,7 @@ class CylinderGeometry:
         return False
 
 
-class ConeGeometry:
+class ConeGeometry(_WallQueries):
     """Infinite cone wall (wall_3d.rs:177-262): apex ``tip``, ``axis`` pointing
     into the cone, half-angle ``angle`` in radians; the valid region is inside."""
 
@@ -103,7 +155,7 @@ class ConeGeometry:
         return False
 
 
-class TorusGeometry:
+class TorusGeometry(_WallQueries):
     """Torus wall (wall_3d.rs:265-365); the valid region is inside the tube."""
 
     def __init__(self, center: Sequence[float], axis: Sequence[float], major_radius: float,
@@ -117,7 +169,7 @@ class TorusGeometry:
         return False
 
 
-class ConvexPolyhedronGeometry:
+class ConvexPolyhedronGeometry(_WallQueries):
     """Convex polyhedron wall (wall_3d.rs:462-708): the intersection of the
     half-spaces behind planes (point, normal pointing OUT of the valid
     region).  The ``new_*`` constructors build the regular solids exactly as
@@ -203,6 +255,19 @@ class Wall:
 
     def is_planar(self) -> bool:
         return self.geometry.is_planar()
+
+    @classmethod
+    def new(cls, id: int, geometry) -> "Wall":
+        """Wall::new (wall/mod.rs:24-32)."""
+        return cls(id, geometry)
+
+    def contains(self, point: Sequence[float]) -> bool:
+        """Wall::contains (wall/mod.rs:38-40)."""
+        return self.geometry.contains(point)
+
+    def cut(self, generator: Sequence[float], callback) -> None:
+        """Wall::cut (wall/mod.rs:42-44)."""
+        self.geometry.cut(generator, callback)
 
 
 def _dp(a: np.ndarray):
@@ -335,6 +400,12 @@ class Cell3DFaces:
         self._stale = True
         return bool(mod.value), r2.value
 
+    def clip_with_scratch(self, point: Sequence[float], normal: Sequence[float], neighbor_id: int, scratch=None,
+                          generator: Optional[Sequence[float]] = None):
+        """Cell3DFaces::clip_with_scratch (cell_3d_faces.rs:288-503): clip();
+        the scratch space lives on the device, so `scratch` is not used."""
+        return self.clip(point, normal, neighbor_id, generator)
+
     def max_radius_sq(self, center: Sequence[float]) -> float:
         h = self._device()
         c = np.asarray(center, np.float64)
@@ -440,6 +511,11 @@ class Tessellation:
         check(self._L.vd_tess_create(_dp(mn), _dp(mx), algorithm.grid_res_x, algorithm.grid_res_y,
                                      algorithm.grid_res_z, C.byref(h)))
         self._h = h
+
+    @classmethod
+    def new(cls, bounds: BoundingBox, algorithm: Algorithm3DGrid) -> "Tessellation":
+        """Tessellation::new (tessellation.rs:25-39)."""
+        return cls(bounds, algorithm)
 
     def close(self):
         if getattr(self, "_h", None) is not None and self._h.value:
