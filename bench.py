@@ -634,13 +634,13 @@ def blob_classes(t, pts, nb, kept, args):
 
 
 def run_blobs(args):
-    """Config: 4,194,304 generators, 70% in 64 isotropic Gaussian blobs
+    """Config: 4,194,304 generators (--blob-n), 70% in 64 isotropic Gaussian blobs
     (sigma 0.01, centres uniform) + 30% uniform background, clipped by a
     sphere wall r = 0.45 at the centre of the unit cube."""
     import torch
     import vorothree_b200 as v
     torch.cuda.set_device(0)
-    n = 4_194_304
+    n = args.blob_n
     rng = np.random.Generator(np.random.PCG64(0))
     nb = int(round(0.7 * n))
     centres = rng.uniform(0.0, 1.0, size=(64, 3))
@@ -739,6 +739,8 @@ def main():
                     help="uniform: 1M uniform generators (the headline); batched: many tessellations "
                          "+ Lloyd steps; blobs: 4M clustered generators with a sphere wall")
     ap.add_argument("--ntess", type=int, default=4096)
+    ap.add_argument("--blob-n", type=int, default=4_194_304,
+                    help="generators of the blobs workload (profiling runs use a smaller case)")
     ap.add_argument("--serve-requests", type=int, default=48)
     ap.add_argument("--serve-slots", type=int, default=4)
     ap.add_argument("--serve-budget-gb", type=int, default=32)
