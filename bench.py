@@ -656,13 +656,15 @@ def run_blobs(args):
         t.set_precision(args.precision)
         t.add_wall(v.Wall(v.WALL_ID_MAX, v.SphereGeometry([0.5, 0.5, 0.5], 0.45)))
         kept = t.set_generators(pts)
-        times = []
+        times, fall = [], []
         for _ in range(args.warmup + args.steps):
             t.calculate()
-            times.append(t.timings()["clip_ms"] + t.timings()["fallback_ms"])
+            tm = t.timings()
+            times.append(tm["clip_ms"] + tm["fallback_ms"])
+            fall.append(tm["fallback_ms"])
         ms = statistics.mean(times[args.warmup:])
         res.append({"grid": list(g), "kept": kept, "ms": ms, "cells_per_s": kept / (ms / 1e3),
-                    "fallback_cells": t.fallback_counts()})
+                    "fallback_cells": t.fallback_counts(), "fallback_ms": statistics.mean(fall[args.warmup:])})
         if g == tuned:
             res[-1]["classes"] = blob_classes(t, pts, nb, kept, args)
         t.close()
