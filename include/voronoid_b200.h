@@ -293,6 +293,13 @@ int vd_wall_contains(const vd_wall_desc* wall, const double point[3], int* insid
  * min(*n, cap) written.  Bit for bit the planes the clip kernels use. */
 int vd_wall_cut(const vd_wall_desc* wall, const double generator[3], double* points, double* normals, int cap,
                 int* n);
+/* Algorithm3DGrid::new's search order (algo_3d_grid.rs:56-76) as the kernels
+ * use it: the offsets of [-k, k]^3 (clipped to the grid) sorted by min_d2, ties
+ * in enumeration order; a table with k below the grid's size keeps the
+ * offsets with min_d2 < *bound and sets *complete = 0.  *n = its length,
+ * min(*n, cap) entries written (dxyz: 3 per entry). */
+int vd_search_order(const double bmin[3], const double bmax[3], int nx, int ny, int nz, int k, int32_t* dxyz,
+                    double* min_d2, size_t cap, size_t* n, int* complete, double* bound);
 /* Algorithm3DGrid::get_bin_index (algo_3d_grid.rs:97-107) of the grid
  * Algorithm3DGrid::new(nx, ny, nz, bounds) builds */
 int vd_grid_bin_index(const double bmin[3], const double bmax[3], int nx, int ny, int nz, const double point[3],

@@ -179,3 +179,40 @@ def test_interior_neighbours_match_delaunay(oracle_mod):
         assert set(int(x) for x in mine) == set(int(x) for x in nb[indptr[i]:indptr[i + 1]]), i
         checked += 1
     assert checked > 1500
+
+
+def _library_order(lo, hi, n, k):
+    import ctypes as C
+    from vorothree_b200 import _lib
+    L = _lib.load()
+    mn = np.asarray(lo, np.float64)
+    mx = np.asarray(hi, np.float64)
+    dp = C.POINTER(C.c_double)
+    cnt = C.c_size_t()
+    comp = C.c_int()
+    bound = C.c_double()
+    _lib.check(L.vd_search_order(mn.ctypes.data_as(dp), mx.ctypes.data_as(dp), *n, k, None, None, 0, C.byref(cnt),
+                                 C.byref(comp), C.byref(bound)))
+    d = np.zeros(3 * max(cnt.value, 1), np.int32)
+    m = np.zeros(max(cnt.value, 1), np.float64)
+    _lib.check(L.vd_search_order(mn.ctypes.data_as(dp), mx.ctypes.data_as(dp), *n, k,
+                                 d.ctypes.data_as(C.POINTER(C.c_int32)), m.ctypes.data_as(dp), cnt.value,
+                                 C.byref(cnt), C.byref(comp), C.byref(bound)))
+    return d[:3 * cnt.value].reshape(-1, 3), m[:cnt.value], bool(comp.value), bound.value
+
+
+@pytest.mark.parametrize("lo,hi,n", [([0, 0, 0], [1, 1, 1], (9, 9, 9)), ([0, 0, 0], [10, 10, 10], (12, 12, 12)),
+                                     ([-3, 0, 2], [4, 2, 9], (7, 5, 11)), ([0, 0, 0], [1, 2, 3], (10, 20, 30))])
+def test_search_order_matches_oracle(oracle_mod, lo, hi, n):
+    """Algorithm3DGrid::new's order as the kernels get it (a counting sort by
+    the integer key on cubic bins, a stable sort otherwise) equals the
+    oracle's stable sort, complete and truncated."""
+    o = oracle_mod.OracleTessellation(lo, hi, *n)
+    od, om = o.search_order()
+    d, m, comp, _ = _library_order(lo, hi, n, max(n))
+    assert comp and np.array_equal(d, od) and np.array_equal(m, om)
+    for k in (2, 4):
+        d, m, comp, bound = _library_order(lo, hi, n, k)
+        assert not comp
+        keep = om < bound
+        assert np.array_equal(d, od[keep]) and np.array_equal(m, om[keep])

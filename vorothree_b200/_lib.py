@@ -71,6 +71,8 @@ SIGNATURES = {
     "vd_tess_get_cell": (C.c_int, [_vp, C.c_size_t, _i32p, _i32p, _i32p, _vp, _vp, _vp, _vp]),
     "vd_wall_contains": (C.c_int, [_vp, _d, C.POINTER(C.c_int)]),
     "vd_wall_cut": (C.c_int, [_vp, _d, _d, _d, C.c_int, C.POINTER(C.c_int)]),
+    "vd_search_order": (C.c_int, [_d, _d, C.c_int, C.c_int, C.c_int, C.c_int, _i32p, _d, C.c_size_t, _szp,
+                                  C.POINTER(C.c_int), _d]),
     "vd_grid_bin_index": (C.c_int, [_d, _d, C.c_int, C.c_int, C.c_int, _d, _szp]),
     "vd_tess_export_cells": (C.c_int, [_vp, C.c_size_t, C.c_size_t, _i64p, _i64p, _i64p, _vp, _vp, _vp, _vp]),
     "vd_tess_device_results": (C.c_int, [_vp, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp)]),

@@ -36,6 +36,9 @@ thread_local std::string g_create_error;
 // grids whose complete search order has at most this many entries get the
 // complete table; larger ones start truncated (k = 8) and grow on demand
 constexpr int kCompleteOrderMax = 1 << 15;
+// longest truncated search order (in bins per axis) chosen from the density
+// before a first pass; longer ones come only from cells that ran off it
+constexpr int kMaxInitialOrder = 32;
 // kernels this library has launched in this process (all handles)
 std::atomic<unsigned long long> g_launches{0};
 
@@ -570,6 +573,18 @@ int run_calculate(vd_tess* t, const WorkList* extra = nullptr, const uint32_t* o
   VD_CK(t, cudaMemsetAsync(t->d_counters.p, 0, kNumCounters * sizeof(unsigned long long), s));
   VD_CK(t, cudaMemsetAsync(t->d_pool_cursor.p, 0, sizeof(unsigned long long), s));
   t->fallback[0] = t->fallback[1] = 0;
+  // A truncated search order long enough for the generator density before
+  // the first pass: on sparse grids (many bins per generator) cells walk past
+  // a short table and would be rerun from scratch with a longer one.  The walk
+  // reaches about twice the neighbour spacing, ~4x the spacing in bins.
+  if (!t->order_complete && !only_cell && n > 0) {
+    const double spacing = std::cbrt((double)t->nbins / (double)n);
+    const int k0 = std::min(kMaxInitialOrder, (int)std::ceil(4.0 * spacing) + 2);
+    if (k0 > t->order_k) {
+      r = upload_order(t, k0);
+      if (r != VD_OK) return r;
+    }
+  }
   VD_CK(t, cudaEventRecord(t->ev[2], s));
   uint32_t* in_list = nullptr;
   uint32_t nin = only_cell ? 1u : (uint32_t)n;
@@ -1208,6 +1223,37 @@ int vd_wall_cut(const vd_wall_desc* d, const double generator[3], double* points
       points[a] = p[a];
       normals[a] = q[a];
     }
+  return VD_OK;
+}
+
+int vd_search_order(const double bmin[3], const double bmax[3], int nx, int ny, int nz, int k, int32_t* dxyz,
+                    double* min_d2, size_t cap, size_t* n, int* complete, double* bound) {
+  if (!bmin || !bmax || !n || nx <= 0 || ny <= 0 || nz <= 0 || k <= 0 || (cap && (!dxyz || !min_d2)))
+    return VD_EINVAL;
+  Grid g;
+  memset(&g, 0, sizeof(g));
+  const int res[3] = {nx, ny, nz};
+  for (int a = 0; a < 3; ++a) {
+    g.bmin[a] = bmin[a];
+    g.bmax[a] = bmax[a];
+    g.n[a] = res[a];
+    g.scale[a] = (double)res[a] / (bmax[a] - bmin[a]);
+    g.limit[a] = (double)res[a] - 1e-5;
+    g.cs[a] = 1.0 / g.scale[a];
+  }
+  std::vector<Offset> h;
+  bool comp = false;
+  double bd = 0.0;
+  build_order(g, k, h, comp, bd);
+  *n = h.size();
+  if (complete) *complete = comp ? 1 : 0;
+  if (bound) *bound = bd;
+  for (size_t q = 0; q < h.size() && q < cap; ++q) {
+    dxyz[3 * q] = h[q].dx;
+    dxyz[3 * q + 1] = h[q].dy;
+    dxyz[3 * q + 2] = h[q].dz;
+    min_d2[q] = h[q].min_d2;
+  }
   return VD_OK;
 }
 

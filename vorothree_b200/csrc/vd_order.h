@@ -53,7 +53,34 @@ inline void build_order(const Grid& g, int k, std::vector<Offset>& out, bool& co
         }
         ++lin;
       }
-  std::stable_sort(v.begin(), v.end(), [](const E& a, const E& b) { return a.o.min_d2 < b.o.min_d2; });
+  const auto by_d2 = [](const E& a, const E& b) { return a.o.min_d2 < b.o.min_d2; };
+  const int rm = std::max(r[0], std::max(r[1], r[2]));
+  const uint64_t kmax = 3ull * (uint64_t)rm * (uint64_t)rm;
+  if (g.cs[0] == g.cs[1] && g.cs[1] == g.cs[2] && kmax < (1ull << 24)) {
+    // Cubic bins: min_d2 = cs^2 * K up to rounding, K = mx^2 + my^2 + mz^2 an
+    // integer.  Two different K never swap order under rounding (the relative
+    // error is ~1e-15, the relative gap between integers below 2^24 is
+    // >= 6e-8), so a stable counting sort by K followed by a stable sort of
+    // each bucket by the value gives exactly the stable sort by value, in
+    // linear time instead of n log n.
+    const auto key = [](const Offset& o) {
+      const uint64_t mx = o.dx > 0 ? o.dx - 1 : (o.dx < 0 ? -o.dx - 1 : 0);
+      const uint64_t my = o.dy > 0 ? o.dy - 1 : (o.dy < 0 ? -o.dy - 1 : 0);
+      const uint64_t mz = o.dz > 0 ? o.dz - 1 : (o.dz < 0 ? -o.dz - 1 : 0);
+      return mx * mx + my * my + mz * mz;
+    };
+    std::vector<uint32_t> start(kmax + 2, 0);
+    for (const E& e : v) ++start[key(e.o) + 1];
+    for (uint64_t q = 0; q <= kmax; ++q) start[q + 1] += start[q];
+    std::vector<E> w(v.size());
+    std::vector<uint32_t> pos(start.begin(), start.end() - 1);
+    for (const E& e : v) w[pos[key(e.o)]++] = e;
+    for (uint64_t q = 0; q <= kmax; ++q)
+      if (start[q + 1] - start[q] > 1) std::stable_sort(w.begin() + start[q], w.begin() + start[q + 1], by_d2);
+    v.swap(w);
+  } else {
+    std::stable_sort(v.begin(), v.end(), by_d2);
+  }
   out.resize(v.size());
   for (size_t i = 0; i < v.size(); ++i) out[i] = v[i].o;
 }
