@@ -79,3 +79,12 @@ def test_cells_and_map():
     vol, _, nf = t.summaries()
     got = t.map(lambda c: (c.volume(), len(c.face_counts())))
     assert [g[0] for g in got] == vol.tolist() and [g[1] for g in got] == nf.tolist()
+
+
+def test_export_huge_cell():
+    # the centre of generators on a sphere: a cell only the huge tier holds,
+    # exported through get_cell
+    from common import bench_distribution
+    t = gpu_tess([0, 0, 0], [100, 100, 100], (12, 12, 12), bench_distribution("sphere", 1500, 82))
+    x = assert_export_matches(t, 0, 40)
+    assert x["f_off"][1] - x["f_off"][0] == 1499

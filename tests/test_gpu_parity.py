@@ -445,3 +445,33 @@ def test_degenerate_duplicates_and_planes(oracle_mod, precision):
     g = gpu_tess([0, 0, 0], [1, 1, 1], (6, 6, 6), pts, walls, precision=precision)
     o = oracle_tess(oracle_mod, [0, 0, 0], [1, 1, 1], (6, 6, 6), pts, walls)
     assert_same(g, o, sample_cells=16)
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+@pytest.mark.parametrize("kind", ["axes", "central", "sphere"])
+def test_bench_distributions_bitwise(oracle_mod, kind, precision):
+    """The distributions of the reference's criterion benches
+    (benches/distributions.rs) on their box and bin heuristic (ceil(N^(1/3))
+    bins per axis): generators crowding three mid-planes, a dense central box
+    with an empty shell, and generators on a sphere (needle-shaped cells)."""
+    from common import bench_distribution
+    n = 3000
+    pts = bench_distribution(kind, n, 70 + len(kind))
+    g = int(np.ceil(n ** (1.0 / 3.0)))
+    gt = gpu_tess([0, 0, 0], [100, 100, 100], (g, g, g), pts, precision=precision)
+    o = oracle_tess(oracle_mod, [0, 0, 0], [100, 100, 100], (g, g, g), pts)
+    assert_same(gt, o, sample_cells=6)
+
+
+def test_sphere_surface_10k_huge_cell(oracle_mod):
+    """10,000 generators on a sphere plus its centre (the reference's own
+    benchmark distribution at its larger size): the centre's cell has 9,999
+    faces and ~20,000 vertices, beyond every shared-memory and large
+    capacity; the huge tier builds it with the oracle's bits."""
+    from common import bench_distribution
+    pts = bench_distribution("sphere", 10000, 81)
+    g = gpu_tess([0, 0, 0], [100, 100, 100], (22, 22, 22), pts)
+    o = oracle_tess(oracle_mod, [0, 0, 0], [100, 100, 100], (22, 22, 22), pts)
+    assert g.summaries()[2][0] == 9999
+    assert g.fallback_counts()["overflow"] > 0
+    assert_same(g, o, sample_cells=3)

@@ -32,7 +32,7 @@ namespace vd {
 constexpr unsigned kFull = 0xffffffffu;
 
 template <int V, int F, int H, int CC, int NC, int SC, typename VIdT, typename FIdT, typename KeyT,
-          typename CIdT, bool kCount, bool kMixed>
+          typename CIdT, bool kCount, bool kMixed, typename PosT = uint16_t, typename DelT = int16_t>
 struct PolyCfg {
   static constexpr bool COUNT = kCount;  // maintain the algorithmic event counters
   static constexpr bool MIXED = kMixed;  // FP32 classification under an error bound
@@ -46,6 +46,8 @@ struct PolyCfg {
   using FId = FIdT;
   using Key = KeyT;  // (min, max) vertex pair of an edge
   using CId = CIdT;  // crossing index
+  using Pos = PosT;  // face-entry position (and triangle prefix)
+  using Del = DelT;  // difference of two positions
   static constexpr int KSHIFT = 8 * (int)sizeof(VIdT);
   static constexpr unsigned VNONE = (unsigned)(VIdT)~(VIdT)0;
   static constexpr unsigned FNONE = (unsigned)(FIdT)~(FIdT)0;
@@ -71,6 +73,11 @@ using MedCfg = PolyCfg<224, 112, 672, 128, 64, 64, uint8_t, uint8_t, uint16_t, u
 // Large-capacity pass (global-memory storage): vertex ids stay u16 like the
 // reference's face_indices (cell_3d_faces.rs:31).
 using BigCfg = PolyCfg<2048, 512, 6144, 1024, 512, 512, uint16_t, uint16_t, uint32_t, uint16_t, true, false>;
+// Huge tier (global memory, few warps): cells adjacent to thousands of others,
+// such as the centre of generators on a sphere.  Vertex ids stay u16 like the
+// reference's face_indices; positions are 32-bit.
+using HugeCfg = PolyCfg<32768, 16384, 98304, 8192, 4096, 4096, uint16_t, uint16_t, uint32_t, uint16_t, true, false,
+                        uint32_t, int32_t>;
 
 // the new ids of the two ends of one face position's edge
 template <typename V>
@@ -90,10 +97,10 @@ struct alignas(16) WarpPoly {
   double tx[C::CCAP > 32 ? C::NCAP : 1], ty[C::CCAP > 32 ? C::NCAP : 1], tz[C::CCAP > 32 ? C::NCAP : 1];
   unsigned long long cnt[C::COUNT ? kNumCounters : 1];
   int32_t fn[2][C::FCAP];
-  uint16_t E[C::HCAP + 1];
-  uint16_t fs[2][C::FCAP + 1];
-  uint16_t fns[C::FCAP];
-  uint16_t cpos[C::CCAP];
+  typename C::Pos E[C::HCAP + 1];
+  typename C::Pos fs[2][C::FCAP + 1];
+  typename C::Pos fns[C::FCAP];
+  typename C::Pos cpos[C::CCAP];
   typename C::Key ckey[C::CCAP];
   typename C::VId cid[C::CCAP];
   typename C::VId fi[2][C::HCAP];
@@ -102,7 +109,7 @@ struct alignas(16) WarpPoly {
   typename C::CId cidx[C::HCAP];  // per clip: crossing index of a crossing position
   typename C::CId fcr[C::FCAP];   // per clip: index of each face's first crossing
   VPair<typename C::VId> pve[C::HCAP];  // per clip: new ids of each position's edge ends (or none)
-  int16_t fdel[C::FCAP];          // per clip: new entry offset of a face minus its first position's E
+  typename C::Del fdel[C::FCAP];          // per clip: new entry offset of a face minus its first position's E
   uint8_t cand_e[32];             // walk: search-order entry (lane) of each candidate of a round
   typename C::FId fnew[C::FCAP];
   typename C::VId o2n[C::VCAP];
@@ -167,7 +174,7 @@ __device__ void poly_init_box(WarpPoly<C>& P, PolyState& S, const Grid& g, doubl
     P.fi[0][lane] = (typename C::VId)idx;
     P.pf[0][lane] = (typename C::FId)(lane >> 2);
   }
-  if (lane < 7) P.fs[0][lane] = (uint16_t)(4 * lane);
+  if (lane < 7) P.fs[0][lane] = (typename C::Pos)(4 * lane);
   // face ids z-, z+, y-, y+, x-, x+ = box_side(axis, is_max) = -1 - (2*axis + is_max)
   if (lane < 6) P.fn[0][lane] = -1 - (2 * (2 - (int)(lane >> 1)) + (int)(lane & 1));
   S.nv = 8;
@@ -332,7 +339,7 @@ __device__ int warp_clip(WarpPoly<C>& P, PolyState& S, double px, double py, dou
         const unsigned before = m & lt;
         const int prevp = before ? b + 31 - __clz(before) : lastcross;
         if (k < C::CCAP) {
-          P.cpos[k] = (uint16_t)p;
+          P.cpos[k] = (typename C::Pos)p;
           P.ckey[k] = (typename C::Key)(s < e ? (s << C::KSHIFT | e) : (e << C::KSHIFT | s));
           P.cidx[p] = (typename C::CId)k;
           if (prevp < f0) P.fcr[f] = (typename C::CId)k;
@@ -344,10 +351,10 @@ __device__ int warp_clip(WarpPoly<C>& P, PolyState& S, double px, double py, dou
       // ballot populations
       const unsigned m1 = __ballot_sync(kFull, si);
       const unsigned m2 = __ballot_sync(kFull, !si && ei);
-      if (p < nh) P.E[p] = (uint16_t)(run + __popc(m1 & lt) + 2 * __popc(m2 & lt));
+      if (p < nh) P.E[p] = (typename C::Pos)(run + __popc(m1 & lt) + 2 * __popc(m2 & lt));
       run += __popc(m1) + 2 * __popc(m2);
     }
-    if (lane == 0) P.E[nh] = (uint16_t)run;
+    if (lane == 0) P.E[nh] = (typename C::Pos)run;
   }
   if (ncross > C::CCAP) return kClipOverflow;
   __syncwarp();
@@ -489,8 +496,8 @@ __device__ int warp_clip(WarpPoly<C>& P, PolyState& S, double px, double py, dou
     const int inc = warp_incl_scan(Lk);
     if (f < nf) {
       P.fnew[f] = kept ? (FId)(nfk + __popc(km & lt)) : (FId)C::FNONE;
-      P.fns[f] = (uint16_t)(hk + inc - Lk);
-      P.fdel[f] = (int16_t)(hk + inc - Lk - (int)P.E[P.fs[cb][f]]);
+      P.fns[f] = (typename C::Pos)(hk + inc - Lk);
+      P.fdel[f] = (typename C::Del)(hk + inc - Lk - (int)P.E[P.fs[cb][f]]);
     }
     nfk += __popc(km);
     hk += __shfl_sync(kFull, inc, 31);
@@ -552,7 +559,7 @@ __device__ int warp_clip(WarpPoly<C>& P, PolyState& S, double px, double py, dou
       P.fn[nb][fw] = P.fn[cb][f];
     }
   }
-  if (lane == 0) P.fs[nb][nfk] = (uint16_t)hk;
+  if (lane == 0) P.fs[nb][nfk] = (typename C::Pos)hk;
   if (nseg > C::SCAP) return kClipOverflow;
 
   // 8. lid (:470-495): lid_map (last writer wins) and the chain from the
@@ -644,9 +651,9 @@ __device__ int warp_clip(WarpPoly<C>& P, PolyState& S, double px, double py, dou
       if (nfk + 1 > C::FCAP || len > 255) return kClipOverflow;
       for (int q = lane; q < len; q += 32) P.pf[nb][hk + q] = (FId)nfk;
       if (lane == 0) {
-        P.fs[nb][nfk] = (uint16_t)hk;
+        P.fs[nb][nfk] = (typename C::Pos)hk;
         P.fn[nb][nfk] = nbr;
-        P.fs[nb][nfk + 1] = (uint16_t)(hk + len);
+        P.fs[nb][nfk + 1] = (typename C::Pos)(hk + len);
       }
       nhn = hk + len;
       nfn = nfk + 1;
@@ -855,7 +862,7 @@ __device__ void finalize_cell(const TessDesc& T, uint32_t i, WarpPoly<C>& P, con
       t = c >= 3 ? c - 2 : 0;
     }
     const int inc = warp_incl_scan(t);
-    if (f < nf) P.E[f] = (uint16_t)(ntri + inc - t);
+    if (f < nf) P.E[f] = (typename C::Pos)(ntri + inc - t);
     ntri += __shfl_sync(kFull, inc, 31);
   }
   __syncwarp();

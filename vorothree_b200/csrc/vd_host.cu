@@ -241,8 +241,8 @@ struct vd_tess {
   DevBuf<unsigned int> d_ctl;
   DevBuf<unsigned long long> d_counters, d_pool_cursor;
   DevBuf<uint32_t> d_list[3];
-  DevBuf<unsigned char> d_big;
-  size_t big_warps = 0;
+  DevBuf<unsigned char> d_big, d_huge;
+  size_t big_warps = 0, huge_warps = 0;
   long long pool_cap = 0;
 
   // scan scratch
@@ -507,8 +507,20 @@ int ensure_big(vd_tess* t, size_t cells) {
   return VD_OK;
 }
 
+int ensure_huge(vd_tess* t, size_t cells) {
+  // a few warps: each holds a multi-megabyte polytope in global memory
+  size_t want = std::min<size_t>(std::max<size_t>(cells, 1), 64);
+  want = (want + 3) / 4 * 4;
+  if (t->huge_warps < want) {
+    VD_CK(t, t->d_huge.ensure(want * clip_huge_scratch_per_warp(), t->stream));
+    t->huge_warps = want;
+  }
+  return VD_OK;
+}
+
 // one pass of the clip kernel over `items` (nullptr = all cells in bin order);
-// tier 0 = fast (shared memory), 1 = medium capacity, 2 = large capacity
+// tier 0 = fast (shared memory), 1 = medium capacity, 2 = large capacity,
+// 3 = huge capacity
 int clip_pass(vd_tess* t, int tier, const uint32_t* items, uint32_t nitems, uint32_t* ovf_list,
               uint32_t* tab_list, const WorkList* extra = nullptr) {
   cudaStream_t s = t->stream;
@@ -539,11 +551,18 @@ int clip_pass(vd_tess* t, int tier, const uint32_t* items, uint32_t nitems, uint
     VD_CK(t, mixed ? launch_clip_mixed_fast(T, W, nblocks, t->instrument, s)
                    : launch_clip_fp64_fast(T, W, nblocks, t->instrument, s));
     g_launches++;
-  } else {
+  } else if (tier == 2) {
     int r = ensure_big(t, nitems);
     if (r != VD_OK) return r;
     T = make_desc(t);
     VD_CK(t, launch_clip_fp64_big(T, W, t->d_big.p, (int)t->big_warps, s));
+    g_launches++;
+  } else {
+    int r = ensure_big(t, nitems);  // the face pool
+    if (r == VD_OK) r = ensure_huge(t, nitems);
+    if (r != VD_OK) return r;
+    T = make_desc(t);
+    VD_CK(t, launch_clip_fp64_huge(T, W, t->d_huge.p, (int)t->huge_warps, s));
     g_launches++;
   }
   return VD_OK;
@@ -648,9 +667,9 @@ int run_calculate(vd_tess* t, const WorkList* extra = nullptr, const uint32_t* o
       continue;
     }
     if (novf > 0) {
-      // medium capacity first, then the large-capacity pass for what remains
+      // medium capacity first, then the large and huge capacities for what remains
       unsigned int ntab_all = 0;
-      for (int tier = 1; tier <= 2 && novf > 0; ++tier) {
+      for (int tier = 1; tier <= 3 && novf > 0; ++tier) {
         std::swap(t->d_list[0], t->d_list[2]);
         r = clip_pass(t, tier, t->d_list[2].p, novf, t->d_list[0].p, t->d_list[1].p + ntab_all, extra);
         if (r != VD_OK) return r;
@@ -658,7 +677,7 @@ int run_calculate(vd_tess* t, const WorkList* extra = nullptr, const uint32_t* o
         r = read_ctl(t, &o2, &t2);
         if (r != VD_OK) return r;
         ntab_all += t2;
-        if (tier == 2 && o2 > 0) return fail(t, VD_EOVERFLOW, "%u cells exceed the large polytope capacity", o2);
+        if (tier == 3 && o2 > 0) return fail(t, VD_EOVERFLOW, "%u cells exceed the huge polytope capacity", o2);
         novf = o2;
       }
       novf = 0;
@@ -960,6 +979,7 @@ int vd_tess_destroy(vd_tess* t) {
   t->d_nf64.release(); t->d_ctl.release(); t->d_counters.release(); t->d_pool_cursor.release();
   for (auto& l : t->d_list) l.release();
   t->d_big.release();
+  t->d_huge.release();
   for (auto& b : t->scan32) b.release();
   for (auto& b : t->scan64) b.release();
   t->d_ex_v.release(); t->d_ex_fc.release(); t->d_ex_fi.release(); t->d_ex_fn.release(); t->d_ex_sizes.release();
@@ -1656,7 +1676,7 @@ int vd_tess_get_cell(vd_tess* t, size_t i, int32_t* n_vertices, int32_t* n_faces
     return VD_OK;
   }
   cudaStream_t s = t->stream;
-  const int cv = 2048, cf = 512, ch = 6144;
+  const int cv = 32768, cf = 16384, ch = 98304;  // the huge tier's capacities
   VD_CK(t, t->d_ex_v.ensure(3 * cv, t->stream));
   VD_CK(t, t->d_ex_fc.ensure(cf, t->stream));
   VD_CK(t, t->d_ex_fi.ensure(ch, t->stream));

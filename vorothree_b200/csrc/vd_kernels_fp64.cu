@@ -54,6 +54,13 @@ cudaError_t launch_clip_fp64_big(const TessDesc& T, const WorkList& W, void* scr
   return cudaGetLastError();
 }
 
+size_t clip_huge_scratch_per_warp() { return sizeof(WarpPoly<HugeCfg>); }
+
+cudaError_t launch_clip_fp64_huge(const TessDesc& T, const WorkList& W, void* scratch, int nwarps, cudaStream_t s) {
+  k_clip_big<HugeCfg><<<nwarps / 4, 128, 0, s>>>(T, W, reinterpret_cast<WarpPoly<HugeCfg>*>(scratch));
+  return cudaGetLastError();
+}
+
 cudaError_t launch_clip_fp64_fast_batched(const TessDesc* descs, const uint32_t* tess_off, int ntess,
                                           const WorkList& W, int nblocks, bool count, cudaStream_t s) {
   const size_t smem = sizeof(WarpPoly<FastCfg>) * kFastWarpsPerBlock;
