@@ -633,6 +633,79 @@ def blob_classes(t, pts, nb, kept, args):
     return out
 
 
+def run_suite(args):
+    """The grid cases of the reference's criterion benches on one B200, with
+    the oracle (the C restatement of calculate) timed on the host cores on the
+    same generators: benches/scaling.rs (N = 10 .. 1 M in a 100^3 box,
+    ceil(N^(1/3)) bins per axis), benches/capacity.rs (100 k generators, 0.25
+    to 20 per bin) and benches/distributions.rs (uniform, axes, central box,
+    sphere surface at 1 k and 10 k; the trefoil-knot wall is not built).  A
+    case's time is calculate() as a caller sees it (host wall clock, launches
+    and synchronisation included) after warm-up; device time beside it."""
+    import torch
+    import vorothree_b200 as v
+    from oracle.oracle import OracleTessellation
+    from vorothree_b200.workloads import bench_distribution
+    torch.cuda.set_device(0)
+    nthreads = os.cpu_count() or 1
+    box = ([0.0, 0.0, 0.0], [100.0, 100.0, 100.0])
+
+    def case(group, label, n, g, pts=None, seed=0):
+        t = v.Tessellation(v.BoundingBox(*box), v.Algorithm3DGrid(g, g, g))
+        if pts is None:
+            t.random_generators(n, seed)
+        else:
+            t.set_generators(pts)
+        t.calculate()
+        one = t.timings()["total_ms"]
+        reps = max(1, min(args.steps, int(2000.0 / max(one, 1e-3))))
+        wall, dev = [], []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            t.calculate()
+            wall.append(1e3 * (time.perf_counter() - t0))
+            tm = t.timings()
+            dev.append(tm["clip_ms"] + tm["fallback_ms"])
+        row = {"group": group, "case": label, "n": n, "grid": g, "gpu_ms": statistics.mean(wall),
+               "gpu_device_ms": statistics.mean(dev), "fallback_cells": t.fallback_counts()}
+        if n <= 100_000:
+            gens = t.generators()
+            o = OracleTessellation(*box, g, g, g)
+            o.set_generators(gens)
+            o.calculate(nthreads)
+            cw = []
+            for _ in range(3):
+                t0 = time.perf_counter()
+                o.calculate(nthreads)
+                cw.append(1e3 * (time.perf_counter() - t0))
+            row["cpu_ms"] = statistics.mean(cw)
+            row["speedup"] = row["cpu_ms"] / row["gpu_ms"]
+            gv, _, gn = t.summaries()
+            ov, _, on = o.summaries()
+            row["bitwise_equal"] = bool(np.array_equal(gv, ov) and np.array_equal(gn, on))
+        t.close()
+        return row
+
+    rows = []
+    for n in (10, 100, 1000, 10_000, 100_000, 1_000_000):
+        rows.append(case("scaling", "uniform", n, max(1, int(np.ceil(n ** (1.0 / 3.0)))), seed=n))
+    for cap in (0.25, 0.5, 1.0, 2.0, 3.0, 4.0, 6.0, 8.0, 12.0, 20.0):
+        g = max(1, int(np.ceil((100_000 / cap) ** (1.0 / 3.0))))
+        rows.append(case("capacity", f"{cap} per bin", 100_000, g, seed=7))
+    for n in (1000, 10_000):
+        g = max(1, int(np.ceil(n ** (1.0 / 3.0))))
+        for kind in ("uniform", "axes", "central", "sphere"):
+            rows.append(case("distributions", kind, n, g, pts=bench_distribution(kind, n, 11, *box)))
+    line = {"metric": "calculate() time on the reference's criterion bench cases", "workload": "suite",
+            "unit": "ms", "n_gpus": 1, "higher_is_better": False, "dtype": "f64",
+            "data": "synthetic (seeded: random_generators / PCG64)",
+            "cpu": {"kind": "port", "cores": nthreads,
+                    "note": "the oracle, a C restatement of the reference's calculate(), N <= 100 k"},
+            "rows": rows}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_blobs(args):
     """Config: 4,194,304 generators (--blob-n), 70% in 64 isotropic Gaussian blobs
     (sigma 0.01, centres uniform) + 30% uniform background, clipped by a
@@ -737,7 +810,8 @@ def run_sealed(args):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--workload", choices=["uniform", "batched", "blobs", "serving", "sealed"], default="uniform",
+    ap.add_argument("--workload", choices=["uniform", "batched", "blobs", "serving", "sealed", "suite"],
+                    default="uniform",
                     help="uniform: 1M uniform generators (the headline); batched: many tessellations "
                          "+ Lloyd steps; blobs: 4M clustered generators with a sphere wall")
     ap.add_argument("--ntess", type=int, default=4096)
@@ -774,6 +848,8 @@ def main():
         return run_reference(args)
     if args.workload == "batched":
         return run_batched(args)
+    if args.workload == "suite":
+        return run_suite(args)
     if args.workload == "blobs":
         return run_blobs(args)
     if args.workload == "serving":
