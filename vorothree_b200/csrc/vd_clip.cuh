@@ -73,10 +73,11 @@ using MedCfg = PolyCfg<224, 112, 672, 128, 64, 64, uint8_t, uint8_t, uint16_t, u
 // Large-capacity pass (global-memory storage): vertex ids stay u16 like the
 // reference's face_indices (cell_3d_faces.rs:31).
 using BigCfg = PolyCfg<2048, 512, 6144, 1024, 512, 512, uint16_t, uint16_t, uint32_t, uint16_t, true, false>;
-// Huge tier (global memory, few warps): cells adjacent to thousands of others,
-// such as the centre of generators on a sphere.  Vertex ids stay u16 like the
-// reference's face_indices; positions are 32-bit.
-using HugeCfg = PolyCfg<32768, 16384, 98304, 8192, 4096, 4096, uint16_t, uint16_t, uint32_t, uint16_t, true, false,
+// Huge tier (global memory, one thread block per cell, vd_clip_block.cuh):
+// cells adjacent to thousands of others, such as the centre of generators on a
+// sphere.  Vertex ids stay u16 like the reference's face_indices; positions
+// are 32-bit.  No event counters.
+using HugeCfg = PolyCfg<65534, 32767, 196608, 16384, 8192, 8192, uint16_t, uint16_t, uint32_t, uint16_t, false, false,
                         uint32_t, int32_t>;
 
 // the new ids of the two ends of one face position's edge

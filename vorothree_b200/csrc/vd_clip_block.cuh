@@ -1,0 +1,731 @@
+// vd_clip_block.cuh -- the huge tier: one thread block per cell.
+//
+// A cell adjacent to thousands of others (the centre of generators on a
+// sphere has N-1 faces) is clipped thousands of times while its polytope holds
+// tens of thousands of vertices and face entries.  One warp (warp_clip) walks
+// such a polytope 32 elements at a time through chains of dependent loads; here
+// the NW warps of a block split every pass over vertices, faces and face
+// positions into NW contiguous ranges.  Each prefix (vertex renumbering,
+// crossing numbers, emitted entries, surviving faces, lid segments) is computed
+// in two passes -- per-range totals, a scan of the NW totals, then the writes --
+// so every element gets exactly the index warp_clip gives it and the output is
+// the same polytope, bit for bit.  The short serial steps (the intersection
+// vertices' first-occurrence numbering, the lid chain) run on warp 0 as in
+// warp_clip.  The walk over candidates runs redundantly in every warp (each
+// reads the same data and makes the same decisions) with a staging row per
+// warp, and every warp enters each block_clip together.
+#pragma once
+#include "vd_clip.cuh"
+
+namespace vd {
+
+template <int NW>
+struct BlockShared {
+  int a[NW], b[NW], c[NW];     // per-range totals of a pass
+  int ia[NW], ib[NW], ic[NW];  // their exclusive scans (ic: last crossing before the range)
+  int val[8];                  // block-wide results
+  double r2[NW];
+  uint8_t cand[NW][32];        // the walk's candidate staging, a row per warp
+  unsigned idx;
+};
+
+// vertices compacted by a clip land here first: warps renumber different
+// ranges at once, and a kept vertex may move into another warp's range
+template <class C>
+struct BlockAux {
+  double x[C::VCAP], y[C::VCAP], z[C::VCAP];
+};
+
+// warp w's contiguous share [lo, hi) of [0, n), whole chunks of 32
+template <int NW>
+__device__ __forceinline__ void block_range(int n, int w, int* lo, int* hi) {
+  const int chunks = (n + 31) >> 5;
+  const int per = (chunks + NW - 1) / NW;
+  *lo = min(n, w * per * 32);
+  *hi = min(n, (w + 1) * per * 32);
+}
+
+// thread 0: exclusive sums of a[] and b[] into ia[] and ib[], the running
+// maximum of c[] before each range into ic[], totals into val[s0], val[s1]
+template <int NW>
+__device__ __forceinline__ void block_scan_totals(BlockShared<NW>& B, int s0, int s1) {
+  if (threadIdx.x == 0) {
+    int sa = 0, sb = 0, mc = -1;
+    for (int w = 0; w < NW; ++w) {
+      B.ia[w] = sa;
+      B.ib[w] = sb;
+      B.ic[w] = mc;
+      sa += B.a[w];
+      sb += B.b[w];
+      mc = max(mc, B.c[w]);
+    }
+    if (s0 >= 0) B.val[s0] = sa;
+    if (s1 >= 0) B.val[s1] = sb;
+  }
+}
+
+// clip_with_scratch (cell_3d_faces.rs:288-503) by the whole block; every
+// thread calls it with the same arguments and gets the same result.
+template <class C, int NW>
+__device__ int block_clip(WarpPoly<C>& P, BlockAux<C>& X, BlockShared<NW>& B, PolyState& S, double px, double py,
+                          double pz, double nx, double ny, double nz, int nbr, bool with_gen, double gx, double gy,
+                          double gz, double* r2out) {
+  static_assert(!C::MIXED && !C::COUNT, "the block clip is the plain FP64 path without counters");
+  using VId = typename C::VId;
+  using FId = typename C::FId;
+  const unsigned lane = lane_id();
+  const unsigned lt = (1u << lane) - 1u;
+  const int w = (int)(threadIdx.x >> 5);
+  const int nt = NW * 32;
+  const int tid = (int)threadIdx.x;
+  const int nv = S.nv, nf = S.nf, nh = S.nh, cb = S.cb, nb = cb ^ 1;
+
+  // 1. signed distances and the 3-band flags (:302-326)
+  bool out = false, sin = false;
+  for (int v = tid; v < nv; v += nt) {
+    const double d = (P.vx[v] - px) * nx + (P.vy[v] - py) * ny + (P.vz[v] - pz) * nz;
+    P.dist[v] = d;
+    P.o2n[v] = d > kTol ? (VId)C::VNONE : (VId)0;
+    out |= d > kTol;
+    sin |= d < -kTol;
+  }
+  const bool any_out = __syncthreads_or(out) != 0;
+  const bool any_sin = __syncthreads_or(sin) != 0;
+  if (!any_out) {
+    *r2out = 0.0;
+    return kClipNoop;
+  }
+  if (!any_sin) {
+    S.nv = S.nf = S.nh = 0;
+    *r2out = 0.0;
+    return kClipEmpty;
+  }
+
+  // 2. keep the inside vertices in order (:344-362)
+  double r2 = 0.0;
+  int lo, hi;
+  block_range<NW>(nv, w, &lo, &hi);
+  {
+    int cnt = 0;
+    for (int b = lo; b < hi; b += 32) {
+      const int v = b + lane;
+      cnt += __popc(__ballot_sync(kFull, v < hi && P.o2n[v] != C::VNONE));
+    }
+    if (lane == 0) B.a[w] = cnt;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    int s = 0;
+    for (int q = 0; q < NW; ++q) {
+      B.ia[q] = s;
+      s += B.a[q];
+    }
+    B.val[0] = s;
+  }
+  __syncthreads();
+  const int nkept = B.val[0];
+  {
+    int run = B.ia[w];
+    for (int b = lo; b < hi; b += 32) {
+      const int v = b + lane;
+      const bool k = v < hi && P.o2n[v] != C::VNONE;
+      const unsigned m = __ballot_sync(kFull, k);
+      if (v < hi) P.o2n[v] = k ? (VId)(run + __popc(m & lt)) : (VId)C::VNONE;
+      if (k && with_gen) {
+        double dx = P.vx[v] - gx;
+        double dy = P.vy[v] - gy;
+        double dz = P.vz[v] - gz;
+        double d2 = dx * dx + dy * dy + dz * dz;
+        r2 = fmax(r2, d2);
+      }
+      run += __popc(m);
+    }
+  }
+  __syncthreads();
+
+  // 3. the face walk (:369-452): end vertices, crossings in walk order, the
+  //    emitted-entry prefix E, each face's first crossing
+  block_range<NW>(nh, w, &lo, &hi);
+  {
+    int ncr = 0, emit = 0, lastc = -1;
+    for (int b = lo; b < hi; b += 32) {
+      const int p = b + lane;
+      bool cr = false, si = false, ei = false;
+      if (p < hi) {
+        const int f = P.pf[cb][p];
+        const int f0 = P.fs[cb][f];
+        const unsigned s = P.fi[cb][p];
+        const unsigned e = P.fi[cb][(p + 1 == (int)P.fs[cb][f + 1]) ? f0 : p + 1];
+        si = P.o2n[s] != C::VNONE;
+        ei = P.o2n[e] != C::VNONE;
+        cr = si != ei;
+      }
+      const unsigned m = __ballot_sync(kFull, cr);
+      ncr += __popc(m);
+      if (m) lastc = b + 31 - __clz(m);
+      emit += __popc(__ballot_sync(kFull, si)) + 2 * __popc(__ballot_sync(kFull, !si && ei));
+    }
+    if (lane == 0) {
+      B.a[w] = ncr;
+      B.b[w] = emit;
+      B.c[w] = lastc;
+    }
+  }
+  __syncthreads();
+  block_scan_totals<NW>(B, 1, 2);
+  __syncthreads();
+  const int ncross = B.val[1];
+  {
+    int nc = B.ia[w], run = B.ib[w], lastcross = B.ic[w];
+    for (int b = lo; b < hi; b += 32) {
+      const int p = b + lane;
+      bool cr = false, si = false, ei = false;
+      int f = 0, f0 = 0;
+      unsigned s = 0, e = 0;
+      if (p < hi) {
+        f = P.pf[cb][p];
+        f0 = P.fs[cb][f];
+        s = P.fi[cb][p];
+        e = P.fi[cb][(p + 1 == (int)P.fs[cb][f + 1]) ? f0 : p + 1];
+        const VId os = P.o2n[s], oe = P.o2n[e];
+        si = os != C::VNONE;
+        ei = oe != C::VNONE;
+        P.fe[p] = (VId)e;
+        P.pve[p] = VPair<VId>{os, oe};
+        cr = si != ei;
+      }
+      const unsigned m = __ballot_sync(kFull, cr);
+      if (cr) {
+        const int k = nc + __popc(m & lt);
+        const unsigned before = m & lt;
+        const int prevp = before ? b + 31 - __clz(before) : lastcross;
+        if (k < C::CCAP) {
+          P.cpos[k] = (typename C::Pos)p;
+          P.ckey[k] = (typename C::Key)(s < e ? (s << C::KSHIFT | e) : (e << C::KSHIFT | s));
+          P.cidx[p] = (typename C::CId)k;
+          if (prevp < f0) P.fcr[f] = (typename C::CId)k;
+        }
+      }
+      if (m) lastcross = b + 31 - __clz(m);
+      nc += __popc(m);
+      const unsigned m1 = __ballot_sync(kFull, si);
+      const unsigned m2 = __ballot_sync(kFull, !si && ei);
+      if (p < hi) P.E[p] = (typename C::Pos)(run + __popc(m1 & lt) + 2 * __popc(m2 & lt));
+      run += __popc(m1) + 2 * __popc(m2);
+    }
+    if (tid == 0) P.E[nh] = (typename C::Pos)B.val[2];
+  }
+  __syncthreads();
+  if (ncross > C::CCAP) return kClipOverflow;
+
+  // 4. intersection vertices (warp 0): the first occurrence of an edge key
+  //    creates the vertex, numbered in discovery order; repeats reuse it
+  if (w == 0) {
+    int nnew = 0;
+    for (int b = 0; b < ncross; b += 32) {
+      const int k = b + lane;
+      const bool act = k < ncross;
+      const unsigned key = act ? (unsigned)P.ckey[k] : (0xFFFF0000u | lane);
+      const unsigned mm = __match_any_sync(kFull, key);
+      const int leader = __ffs(mm) - 1;
+      const bool isleader = act && leader == (int)lane;
+      int id = -1;
+      if (isleader && b > 0) {
+        for (int j = 0; j < b; ++j)
+          if ((unsigned)P.ckey[j] == key) {
+            id = P.cid[j];
+            break;
+          }
+      }
+      const bool disc = isleader && id < 0;
+      const unsigned dm = __ballot_sync(kFull, disc);
+      if (disc) id = nkept + nnew + __popc(dm & lt);
+      id = __shfl_sync(kFull, id, leader);
+      if (act) P.cid[k] = (VId)id;
+      if (disc) {
+        const int r = id - nkept;
+        if (r < C::NCAP) {
+          const int p = P.cpos[k];
+          const int s = P.fi[cb][p], e = P.fe[p];
+          const double ds = P.dist[s], de = P.dist[e];
+          const double t = clamp01(ds / (ds - de));
+          const double ax = P.vx[s], ay = P.vy[s], az = P.vz[s];
+          const double bx = P.vx[e], by = P.vy[e], bz = P.vz[e];
+          const double ix = ax + t * (bx - ax);
+          const double iy = ay + t * (by - ay);
+          const double iz = az + t * (bz - az);
+          P.tx[r] = ix;
+          P.ty[r] = iy;
+          P.tz[r] = iz;
+          if (with_gen) {
+            double dx = ix - gx;
+            double dy = iy - gy;
+            double dz = iz - gz;
+            double d2 = dx * dx + dy * dy + dz * dz;
+            r2 = fmax(r2, d2);
+          }
+        }
+      }
+      nnew += __popc(dm);
+      __syncwarp();
+    }
+    if (lane == 0) B.val[3] = nnew;
+  }
+  __syncthreads();
+  const int nnew = B.val[3];
+  const int nvn = nkept + nnew;
+  if (nnew > C::NCAP || nvn > C::VCAP) return kClipOverflow;
+
+  // 5. new vertex list: kept vertices compacted (through X), then intersections
+  for (int v = tid; v < nv; v += nt) {
+    const unsigned o = P.o2n[v];
+    if (o != C::VNONE) {
+      X.x[o] = P.vx[v];
+      X.y[o] = P.vy[v];
+      X.z[o] = P.vz[v];
+    }
+  }
+  __syncthreads();
+  for (int o = tid; o < nkept; o += nt) {
+    P.vx[o] = X.x[o];
+    P.vy[o] = X.y[o];
+    P.vz[o] = X.z[o];
+  }
+  for (int r = tid; r < nnew; r += nt) {
+    P.vx[nkept + r] = P.tx[r];
+    P.vy[nkept + r] = P.ty[r];
+    P.vz[nkept + r] = P.tz[r];
+  }
+
+  // 6. surviving faces (>= 3 entries, :454-467) and their new starts
+  block_range<NW>(nf, w, &lo, &hi);
+  {
+    int kept = 0, sum = 0, longf = 0;
+    for (int b = lo; b < hi; b += 32) {
+      const int f = b + lane;
+      int L = 0;
+      if (f < hi) L = (int)P.E[P.fs[cb][f + 1]] - (int)P.E[P.fs[cb][f]];
+      const bool k = L >= 3;
+      longf |= __any_sync(kFull, L > 255) ? 1 : 0;
+      kept += __popc(__ballot_sync(kFull, k));
+      sum += __shfl_sync(kFull, warp_incl_scan(k ? L : 0), 31);
+    }
+    if (lane == 0) {
+      B.a[w] = kept;
+      B.b[w] = sum;
+      B.c[w] = longf;
+    }
+  }
+  __syncthreads();
+  block_scan_totals<NW>(B, 4, 5);
+  __syncthreads();
+  const int nfk = B.val[4], hk = B.val[5];
+  const bool longface = B.ic[NW - 1] > 0 || B.c[NW - 1] > 0;
+  {
+    int nfr = B.ia[w], hr = B.ib[w];
+    for (int b = lo; b < hi; b += 32) {
+      const int f = b + lane;
+      int L = 0;
+      if (f < hi) L = (int)P.E[P.fs[cb][f + 1]] - (int)P.E[P.fs[cb][f]];
+      const bool kept = L >= 3;
+      const unsigned km = __ballot_sync(kFull, kept);
+      const int Lk = kept ? L : 0;
+      const int inc = warp_incl_scan(Lk);
+      if (f < hi) {
+        P.fnew[f] = kept ? (FId)(nfr + __popc(km & lt)) : (FId)C::FNONE;
+        P.fns[f] = (typename C::Pos)(hr + inc - Lk);
+        P.fdel[f] = (typename C::Del)(hr + inc - Lk - (int)P.E[P.fs[cb][f]]);
+      }
+      nfr += __popc(km);
+      hr += __shfl_sync(kFull, inc, 31);
+    }
+  }
+  __syncthreads();
+  if (longface || hk > C::HCAP) return kClipOverflow;
+
+  // 7. the surviving faces' entries, and the lid segments (v, u) ordered by
+  //    the position of their in->out crossing
+  block_range<NW>(nh, w, &lo, &hi);
+  {
+    int nsg = 0;
+    for (int b = lo; b < hi; b += 32) {
+      const int p = b + lane;
+      bool segsrc = false;
+      if (p < hi) {
+        const int f = P.pf[cb][p];
+        const VPair<VId> ve = P.pve[p];
+        const unsigned os = ve.s, oe = ve.e;
+        const bool si = os != C::VNONE, ei = oe != C::VNONE;
+        const unsigned fw = P.fnew[f];
+        if (fw != C::FNONE) {
+          const int o = (int)P.fdel[f] + (int)P.E[p];
+          if (si) {
+            P.fi[nb][o] = (VId)(ei ? oe : (unsigned)P.cid[P.cidx[p]]);
+            P.pf[nb][o] = (FId)fw;
+            segsrc = !ei;
+          } else if (ei) {
+            P.fi[nb][o] = P.cid[P.cidx[p]];
+            P.pf[nb][o] = (FId)fw;
+            P.fi[nb][o + 1] = (VId)oe;
+            P.pf[nb][o + 1] = (FId)fw;
+          }
+        }
+      }
+      nsg += __popc(__ballot_sync(kFull, segsrc));
+    }
+    if (lane == 0) B.a[w] = nsg;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    int s = 0;
+    for (int q = 0; q < NW; ++q) {
+      B.ia[q] = s;
+      s += B.a[q];
+    }
+    B.val[6] = s;
+  }
+  __syncthreads();
+  const int nseg = B.val[6];
+  {
+    int k0 = B.ia[w];
+    for (int b = lo; b < hi; b += 32) {
+      const int p = b + lane;
+      bool segsrc = false;
+      int f = 0;
+      if (p < hi) {
+        f = P.pf[cb][p];
+        const VPair<VId> ve = P.pve[p];
+        segsrc = P.fnew[f] != C::FNONE && ve.s != C::VNONE && ve.e == C::VNONE;
+      }
+      const unsigned sm = __ballot_sync(kFull, segsrc);
+      if (segsrc) {
+        const int k = k0 + __popc(sm & lt);
+        if (k < C::SCAP) {
+          const int kc = P.cidx[p];
+          int kn = kc + 1;
+          if (kn >= ncross || (int)P.cpos[kn] >= (int)P.fs[cb][f + 1]) kn = P.fcr[f];
+          P.sega[k] = P.cid[kn];
+          P.segb[k] = P.cid[kc];
+        }
+      }
+      k0 += __popc(sm);
+    }
+  }
+  for (int f = tid; f < nf; f += nt) {
+    const unsigned fw = P.fnew[f];
+    if (fw != C::FNONE) {
+      P.fs[nb][fw] = P.fns[f];
+      P.fn[nb][fw] = P.fn[cb][f];
+    }
+  }
+  if (tid == 0) P.fs[nb][nfk] = (typename C::Pos)hk;
+  __syncthreads();
+  if (nseg > C::SCAP) return kClipOverflow;
+
+  // 8. the lid (:470-495), warp 0: lid_map (last writer wins) and the chain
+  //    from the first segment, appended as the last face
+  if (w == 0) {
+    int len = 0, ovf = 0;
+    if (nseg > 0) {
+      for (int v = nkept + lane; v < nvn; v += 32) P.lidmap[v] = (VId)C::VNONE;
+      __syncwarp();
+      bool fastlid = false;
+      if (nseg <= 32) {
+        const bool act = (int)lane < nseg;
+        const unsigned a = act ? (unsigned)P.sega[lane] : (0xFFFF0000u | lane);
+        const unsigned bend = act ? (unsigned)P.segb[lane] : (0xFFFE0000u | lane);
+        const unsigned ma = __match_any_sync(kFull, a);
+        const unsigned mb = __match_any_sync(kFull, bend);
+        if (act) P.lidmap[a] = (VId)lane;
+        __syncwarp();
+        unsigned succ = lane;
+        bool good = true;
+        if (act) {
+          succ = P.lidmap[bend];
+          good = __popc(ma) == 1 && __popc(mb) == 1 && succ < (unsigned)nseg;
+        }
+        __syncwarp();
+        if (__all_sync(kFull, good)) {
+          fastlid = true;
+          const int term = __ffs(__ballot_sync(kFull, act && succ == 0u)) - 1;
+          int nxt = (act && (int)lane != term) ? (int)succ : (int)lane;
+          int d = nxt != (int)lane ? 1 : 0;
+          for (int span = 1; span < nseg; span <<= 1) {
+            const int dn = __shfl_sync(kFull, d, nxt);
+            const int nn = __shfl_sync(kFull, nxt, nxt);
+            d += dn;
+            nxt = nn;
+          }
+          const int d0 = __shfl_sync(kFull, d, 0);
+          len = d0 + 1;
+          if (hk + len > C::HCAP) ovf = 1;
+          else if (act && nxt == term) P.fi[nb][hk + d0 - d] = (VId)a;
+        } else {
+          if (act) P.lidmap[a] = (VId)C::VNONE;
+          __syncwarp();
+        }
+      }
+      if (!fastlid) {
+        for (int b = 0; b < nseg; b += 32) {
+          const int k = b + lane;
+          const bool act = k < nseg;
+          const unsigned key = act ? (unsigned)P.sega[k] : (0xFFFF0000u | lane);
+          const unsigned mm = __match_any_sync(kFull, key);
+          const int last = 31 - __clz(mm);
+          if (act && last == (int)lane) P.lidmap[key] = P.segb[k];
+          __syncwarp();
+        }
+        if (lane == 0) {
+          const unsigned start = P.sega[0];
+          unsigned cur = P.segb[0];
+          if (hk < C::HCAP) {
+            P.fi[nb][hk] = (VId)start;
+            len = 1;
+            while (cur != start && len <= nseg) {
+              if (hk + len >= C::HCAP) {
+                ovf = 1;
+                break;
+              }
+              P.fi[nb][hk + len] = (VId)cur;
+              ++len;
+              cur = P.lidmap[cur];
+              if (cur == C::VNONE) break;
+            }
+          } else {
+            ovf = 1;
+          }
+        }
+        len = __shfl_sync(kFull, len, 0);
+        ovf = __shfl_sync(kFull, ovf, 0);
+      }
+      if (!ovf && len >= 3) {
+        if (nfk + 1 > C::FCAP || len > 255) {
+          ovf = 1;
+        } else {
+          for (int q = lane; q < len; q += 32) P.pf[nb][hk + q] = (FId)nfk;
+          if (lane == 0) {
+            P.fs[nb][nfk] = (typename C::Pos)hk;
+            P.fn[nb][nfk] = nbr;
+            P.fs[nb][nfk + 1] = (typename C::Pos)(hk + len);
+          }
+        }
+      }
+    }
+    if (lane == 0) {
+      B.val[7] = ovf ? -1 : len;
+    }
+  }
+  // the clip's max radius: every thread's kept and new vertices
+  const double wr = warp_max(r2);
+  if (lane == 0) B.r2[w] = wr;
+  __syncthreads();
+  const int lidlen = B.val[7];
+  double rm = 0.0;
+  for (int q = 0; q < NW; ++q) rm = fmax(rm, B.r2[q]);
+  __syncthreads();  // B is reused by the next clip
+  if (lidlen < 0) return kClipOverflow;
+  S.nv = nvn;
+  S.nf = lidlen >= 3 ? nfk + 1 : nfk;
+  S.nh = lidlen >= 3 ? hk + lidlen : hk;
+  S.cb = nb;
+  *r2out = with_gen ? rm : 0.0;
+  return kClipMod;
+}
+
+// compute_cell (tessellation.rs:414-475) by a whole block: the walk runs in
+// every warp (same data, same decisions, a staging row per warp), each clip
+// by all warps together
+template <class C, int NW>
+__device__ int compute_cell_block(const TessDesc& T, uint32_t i, WarpPoly<C>& P, BlockAux<C>& X,
+                                   BlockShared<NW>& B, PolyState& S) {
+  const unsigned lane = lane_id();
+  const double gx = T.gen[3 * (size_t)i], gy = T.gen[3 * (size_t)i + 1], gz = T.gen[3 * (size_t)i + 2];
+  double r2;
+  // the box, written by warp 0; every thread holds the same state
+  if ((threadIdx.x >> 5) == 0) poly_init_box(P, S, T.grid, gx, gy, gz);
+  S.nv = 8;
+  S.nf = 6;
+  S.nh = 24;
+  S.cb = 0;
+  S.umax = 0.0;
+  __syncthreads();
+  for (int w = 0; w < T.nwalls; ++w) {
+    const Wall& W = T.walls[w];
+    // one plane per generator, or a polyhedron's fixed planes in order
+    const int np = W.kind == kWallPolyhedron ? W.np : 1;
+    for (int k = 0; k < np; ++k) {
+      double p[3], n[3];
+      bool emit;
+      if (W.kind == kWallPolyhedron) {
+        const double* pl = T.planes + 6 * (W.p0 + k);
+        p[0] = pl[0];
+        p[1] = pl[1];
+        p[2] = pl[2];
+        n[0] = pl[3];
+        n[1] = pl[4];
+        n[2] = pl[5];
+        emit = true;
+      } else {
+        emit = wall_plane(W, gx, gy, gz, p, n);
+      }
+      if (emit) {
+        const int r = block_clip<C, NW>(P, X, B, S, p[0], p[1], p[2], n[0], n[1], n[2], W.id, false, gx, gy, gz, &r2);
+        if (r == kClipOverflow) return kCellOverflow;
+      }
+    }
+    if (S.nv == 0) return kCellOk;
+  }
+  double cur = poly_max_radius_sq(P, S, gx, gy, gz);
+
+  const Grid& G = T.grid;
+  const uint32_t bin = T.bin_of[i];
+  const uint32_t nxy = (uint32_t)G.n[0] * (uint32_t)G.n[1];
+  const int iz = (int)(bin / nxy);
+  const uint32_t rem = bin % nxy;
+  const int iy = (int)(rem / (uint32_t)G.n[0]);
+  const int ix = (int)(rem % (uint32_t)G.n[0]);
+  const double rx = (gx - G.bmin[0]) * G.scale[0] - (double)ix;
+  const double ry = (gy - G.bmin[1]) * G.scale[1] - (double)iy;
+  const double rz = (gz - G.bmin[2]) * G.scale[2] - (double)iz;
+
+  bool done = false;
+  for (int base = 0; base < T.norder && !done; base += 32) {
+    // ---- this lane's search-order entry ----
+    const int k = base + (int)lane;
+    const bool valid = k < T.norder;
+    double md2 = 0.0, b2 = 0.0;
+    bool inr = false, own = false;
+    uint32_t bs = 0, be = 0;
+    if (valid) {
+      const Offset o = T.order[k];
+      md2 = o.min_d2;
+      own = o.dx == 0 && o.dy == 0 && o.dz == 0;
+      const int bx = ix + o.dx, by = iy + o.dy, bz = iz + o.dz;
+      inr = bx >= 0 && bx < G.n[0] && by >= 0 && by < G.n[1] && bz >= 0 && bz < G.n[2];
+      if (inr) {
+        const double ddx = o.dx > 0 ? ((double)o.dx - rx) * G.cs[0]
+                                    : (o.dx < 0 ? ((double)(-(o.dx + 1)) + rx) * G.cs[0] : 0.0);
+        const double ddy = o.dy > 0 ? ((double)o.dy - ry) * G.cs[1]
+                                    : (o.dy < 0 ? ((double)(-(o.dy + 1)) + ry) * G.cs[1] : 0.0);
+        const double ddz = o.dz > 0 ? ((double)o.dz - rz) * G.cs[2]
+                                    : (o.dz < 0 ? ((double)(-(o.dz + 1)) + rz) * G.cs[2] : 0.0);
+        const double bdx = fmax(ddx, 0.0), bdy = fmax(ddy, 0.0), bdz = fmax(ddz, 0.0);
+        b2 = bdx * bdx + bdy * bdy + bdz * bdz;
+        const uint32_t bb = (uint32_t)bx + (uint32_t)by * (uint32_t)G.n[0] + (uint32_t)bz * nxy;
+        bs = T.bin_start[bb];
+        be = T.bin_start[bb + 1];
+      }
+    }
+    const int nvalid = min(32, T.norder - base);
+    // bins that can still open (R only shrinks), flattened: members of entry
+    // e are candidates [start, start + cnt)
+    const bool pot = valid && inr && be > bs && !(md2 > 4.0 * cur) && b2 <= 4.0 * cur;
+    if (!__any_sync(kFull, pot)) {
+      // no bin of this chunk can open (sparse regions, fine grids): only
+      // the end of the walk is decided here
+      const unsigned brk = __ballot_sync(kFull, valid && md2 > 4.0 * cur);
+      const int fbe = brk ? __ffs(brk) - 1 : 32;
+      if constexpr (C::COUNT) cnt_add(P, kCntOffsets, (unsigned long long)(fbe < 32 ? fbe + 1 : nvalid));
+      if (fbe < 32) done = true;
+      continue;
+    }
+    const int cnt = pot ? (int)(be - bs) : 0;
+    const int incl = warp_incl_scan(cnt);
+    const int start = incl - cnt;
+    const int total = __shfl_sync(kFull, incl, 31);
+    int ecur = -1;  // entry of the bin being processed (opened)
+    int pos = 0;    // next candidate to consider
+    int fb = 32;    // entry that ends the walk (32: none in this chunk)
+    for (int r0 = 0;; r0 += 32) {
+      if (r0 < total) {
+        const int lo = max(start, r0), hi = min(start + cnt, r0 + 32);
+        for (int q = lo; q < hi; ++q) B.cand[threadIdx.x >> 5][q - r0] = (uint8_t)lane;
+      }
+      __syncwarp();
+      const int idx = r0 + (int)lane;
+      const bool have = idx < total;
+      const int ce = have ? (int)B.cand[threadIdx.x >> 5][lane] : 0;
+      __syncwarp();
+      const uint32_t cbs = __shfl_sync(kFull, bs, ce);
+      const int cst = __shfl_sync(kFull, start, ce);
+      const double cb2 = __shfl_sync(kFull, b2, ce);
+      SortedGen sg = {0.0, 0.0, 0.0, -1};
+      if (have) sg = T.sorted[cbs + (uint32_t)(idx - cst)];
+      const bool cand = have && sg.id != (long long)i;
+      const double d0 = sg.x - gx, d1 = sg.y - gy, d2 = sg.z - gz;
+      const double dist_sq = d0 * d0 + d1 * d1 + d2 * d2;
+      while (true) {
+        const double c4 = 4.0 * cur;
+        const unsigned later = ecur < 0 ? kFull : (ecur >= 31 ? 0u : ~((2u << ecur) - 1u));
+        const unsigned brk = __ballot_sync(kFull, valid && md2 > c4) & later;
+        fb = brk ? __ffs(brk) - 1 : 32;
+        const bool ok = cand && idx >= pos && ce < fb && !(dist_sq > c4) && (ce == ecur || cb2 <= c4);
+        const unsigned pass = __ballot_sync(kFull, ok);
+        if (!pass) break;
+        const int j = __ffs(pass) - 1;
+        const int ej = __shfl_sync(kFull, ce, j);
+        if constexpr (C::COUNT) count_opened(P, ecur, ej, valid, inr, own, md2, b2, be - bs, c4);
+        const int jid = (int)__shfl_sync(kFull, sg.id, j);
+        const double e0 = __shfl_sync(kFull, d0, j);
+        const double e1 = __shfl_sync(kFull, d1, j);
+        const double e2 = __shfl_sync(kFull, d2, j);
+        const double mx = gx + e0 * 0.5, my = gy + e1 * 0.5, mz = gz + e2 * 0.5;
+        const int r = block_clip<C, NW>(P, X, B, S, mx, my, mz, e0, e1, e2, jid, true, gx, gy, gz, &r2);
+        if (r == kClipOverflow) return kCellOverflow;
+        if (r == kClipMod) cur = r2;
+        else if (r == kClipEmpty) cur = 0.0;
+        ecur = ej;
+        pos = r0 + j + 1;
+      }
+      if (r0 + 32 >= total) break;
+      // the next round starts at an entry the walk no longer reaches
+      const unsigned nxt = __ballot_sync(kFull, cnt > 0 && start <= r0 + 32);
+      if (fb < 32 && 31 - __clz(nxt) >= fb) break;
+    }
+    if constexpr (C::COUNT) {
+      count_opened(P, ecur, fb < 32 ? fb - 1 : 31, valid, inr, own, md2, b2, be - bs, 4.0 * cur);
+      cnt_add(P, kCntOffsets, (unsigned long long)(fb < 32 ? fb + 1 : nvalid));
+    }
+    if (fb < 32) done = true;
+  }
+  if (!done && !T.order_complete && !(T.order_bound > 4.0 * cur)) return kCellTable;
+  return kCellOk;
+}
+
+constexpr int kHugeBlockWarps = 32;
+
+// persistent blocks over the listed cells, one cell per block at a time; the
+// block's polytope and compaction buffer live in global memory
+template <class C, int NW>
+__global__ void __launch_bounds__(NW * 32)
+    k_clip_huge_block(const TessDesc T, const WorkList W, WarpPoly<C>* polys, BlockAux<C>* aux) {
+  __shared__ BlockShared<NW> B;
+  WarpPoly<C>& P = polys[blockIdx.x];
+  BlockAux<C>& X = aux[blockIdx.x];
+  const unsigned lane = lane_id();
+  const int w = (int)(threadIdx.x >> 5);
+  while (true) {
+    if (threadIdx.x == 0) B.idx = atomicAdd(W.cursor, 1u);
+    __syncthreads();
+    const unsigned idx = B.idx;
+    __syncthreads();
+    if (idx >= W.nitems) break;
+    const uint32_t cell = W.items ? W.items[idx] : (uint32_t)T.sorted[idx].id;
+    PolyState S;
+    const int st = compute_cell_block<C, NW>(T, cell, P, X, B, S);
+    __syncthreads();
+    if (w == 0) {
+      if (st == kCellOk) {
+        finalize_cell<C>(T, cell, P, S);
+        if (W.ex_verts) export_cell<C>(W, P, S);
+      } else if (lane == 0) {
+        T.status[cell] = (uint8_t)st;
+        if (st == kCellOverflow && W.ovf_list) W.ovf_list[atomicAdd(W.ovf_count, 1u)] = cell;
+        if (st == kCellTable && W.tab_list) W.tab_list[atomicAdd(W.tab_count, 1u)] = cell;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace vd

@@ -508,11 +508,10 @@ int ensure_big(vd_tess* t, size_t cells) {
 }
 
 int ensure_huge(vd_tess* t, size_t cells) {
-  // a few warps: each holds a multi-megabyte polytope in global memory
-  size_t want = std::min<size_t>(std::max<size_t>(cells, 1), 64);
-  want = (want + 3) / 4 * 4;
-  if (t->huge_warps < want) {
-    VD_CK(t, t->d_huge.ensure(want * clip_huge_scratch_per_warp(), t->stream));
+  // a few blocks: each holds a multi-megabyte polytope in global memory
+  const size_t want = std::min<size_t>(std::max<size_t>(cells, 1), 64);
+  if (t->huge_warps != want) {
+    VD_CK(t, t->d_huge.ensure(want * clip_huge_scratch_per_block(), t->stream));
     t->huge_warps = want;
   }
   return VD_OK;
@@ -1676,7 +1675,7 @@ int vd_tess_get_cell(vd_tess* t, size_t i, int32_t* n_vertices, int32_t* n_faces
     return VD_OK;
   }
   cudaStream_t s = t->stream;
-  const int cv = 32768, cf = 16384, ch = 98304;  // the huge tier's capacities
+  const int cv = 65534, cf = 32767, ch = 196608;  // the huge tier's capacities
   VD_CK(t, t->d_ex_v.ensure(3 * cv, t->stream));
   VD_CK(t, t->d_ex_fc.ensure(cf, t->stream));
   VD_CK(t, t->d_ex_fi.ensure(ch, t->stream));

@@ -28,9 +28,10 @@ cudaError_t launch_clip_fp64_fast(const TessDesc& T, const WorkList& W, int nblo
 cudaError_t launch_clip_fp64_big(const TessDesc& T, const WorkList& W, void* scratch, int nwarps,
                                  cudaStream_t s);
 
-// huge tier (global memory, a few warps): cells beyond the large capacities
-size_t clip_huge_scratch_per_warp();
-cudaError_t launch_clip_fp64_huge(const TessDesc& T, const WorkList& W, void* scratch, int nwarps, cudaStream_t s);
+// huge tier (global memory, one thread block per cell): cells beyond the
+// large capacities
+size_t clip_huge_scratch_per_block();
+cudaError_t launch_clip_fp64_huge(const TessDesc& T, const WorkList& W, void* scratch, int nblocks, cudaStream_t s);
 
 // medium-capacity tier (FP64, shared memory) for cells that overflow the fast path
 cudaError_t clip_med_setup(ClipLaunchInfo* info);

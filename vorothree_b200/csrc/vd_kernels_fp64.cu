@@ -4,6 +4,7 @@
 // add, so neither may this path, or its vertices would differ in the last bit
 // and the tie-breaking 1e-9 bands could classify differently.
 #include "vd_clip.cuh"
+#include "vd_clip_block.cuh"
 #include "vd_internal.h"
 
 namespace vd {
@@ -54,10 +55,14 @@ cudaError_t launch_clip_fp64_big(const TessDesc& T, const WorkList& W, void* scr
   return cudaGetLastError();
 }
 
-size_t clip_huge_scratch_per_warp() { return sizeof(WarpPoly<HugeCfg>); }
+// the huge tier's scratch: per block a polytope, then (after all of them) a
+// compaction buffer
+size_t clip_huge_scratch_per_block() { return sizeof(WarpPoly<HugeCfg>) + sizeof(BlockAux<HugeCfg>); }
 
-cudaError_t launch_clip_fp64_huge(const TessDesc& T, const WorkList& W, void* scratch, int nwarps, cudaStream_t s) {
-  k_clip_big<HugeCfg><<<nwarps / 4, 128, 0, s>>>(T, W, reinterpret_cast<WarpPoly<HugeCfg>*>(scratch));
+cudaError_t launch_clip_fp64_huge(const TessDesc& T, const WorkList& W, void* scratch, int nblocks, cudaStream_t s) {
+  WarpPoly<HugeCfg>* polys = reinterpret_cast<WarpPoly<HugeCfg>*>(scratch);
+  BlockAux<HugeCfg>* aux = reinterpret_cast<BlockAux<HugeCfg>*>(polys + nblocks);
+  k_clip_huge_block<HugeCfg, kHugeBlockWarps><<<nblocks, kHugeBlockWarps * 32, 0, s>>>(T, W, polys, aux);
   return cudaGetLastError();
 }
 
