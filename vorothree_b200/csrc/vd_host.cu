@@ -39,6 +39,8 @@ constexpr int kCompleteOrderMax = 1 << 15;
 // longest truncated search order (in bins per axis) chosen from the density
 // before a first pass; longer ones come only from cells that ran off it
 constexpr int kMaxInitialOrder = 32;
+// blocks of the huge tier (each holds its cell's polytope in global memory)
+constexpr int kHugeBlocksMax = 64;
 // kernels this library has launched in this process (all handles)
 std::atomic<unsigned long long> g_launches{0};
 
@@ -509,7 +511,7 @@ int ensure_big(vd_tess* t, size_t cells) {
 
 int ensure_huge(vd_tess* t, size_t cells) {
   // a few blocks: each holds a multi-megabyte polytope in global memory
-  const size_t want = std::min<size_t>(std::max<size_t>(cells, 1), 64);
+  const size_t want = std::min<size_t>(std::max<size_t>(cells, 1), (size_t)kHugeBlocksMax);
   if (t->huge_warps != want) {
     VD_CK(t, t->d_huge.ensure(want * clip_huge_scratch_per_block(), t->stream));
     t->huge_warps = want;
@@ -678,6 +680,10 @@ int run_calculate(vd_tess* t, const WorkList* extra = nullptr, const uint32_t* o
         ntab_all += t2;
         if (tier == 3 && o2 > 0) return fail(t, VD_EOVERFLOW, "%u cells exceed the huge polytope capacity", o2);
         novf = o2;
+        // few cells left after the medium tier: straight to the block tier,
+        // which takes them all at once, so that a cell outgrowing the large
+        // tier is not built twice
+        if (tier == 1 && novf > 0 && novf <= (unsigned)kHugeBlocksMax) tier = 2;
       }
       novf = 0;
       ntab = ntab_all;
