@@ -244,7 +244,7 @@ struct vd_tess {
   DevBuf<unsigned long long> d_counters, d_pool_cursor;
   DevBuf<uint32_t> d_list[3];
   DevBuf<unsigned char> d_big, d_huge;
-  size_t big_warps = 0, huge_warps = 0;
+  size_t big_warps = 0, huge_blocks = 0;
   long long pool_cap = 0;
 
   // scan scratch
@@ -512,9 +512,9 @@ int ensure_big(vd_tess* t, size_t cells) {
 int ensure_huge(vd_tess* t, size_t cells) {
   // a few blocks: each holds a multi-megabyte polytope in global memory
   const size_t want = std::min<size_t>(std::max<size_t>(cells, 1), (size_t)kHugeBlocksMax);
-  if (t->huge_warps != want) {
+  if (t->huge_blocks != want) {
     VD_CK(t, t->d_huge.ensure(want * clip_huge_scratch_per_block(), t->stream));
-    t->huge_warps = want;
+    t->huge_blocks = want;
   }
   return VD_OK;
 }
@@ -563,7 +563,7 @@ int clip_pass(vd_tess* t, int tier, const uint32_t* items, uint32_t nitems, uint
     if (r == VD_OK) r = ensure_huge(t, nitems);
     if (r != VD_OK) return r;
     T = make_desc(t);
-    VD_CK(t, launch_clip_fp64_huge(T, W, t->d_huge.p, (int)t->huge_warps, s));
+    VD_CK(t, launch_clip_fp64_huge(T, W, t->d_huge.p, (int)t->huge_blocks, s));
     g_launches++;
   }
   return VD_OK;
