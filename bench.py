@@ -264,6 +264,28 @@ def issue_roof(args, clip_ms: float, clk: dict):
                     "warp instructions per cell from the committed ncu profile"}
 
 
+# algorithmic bytes per cell of the clip kernel: the generator (24 B) and its
+# bin-ordered copy (32 B) in; volume, centroid, face and vertex counts
+# (8 + 24 + 4 + 4 B) and ~15.5 face slots of neighbour id + area (12 B) out
+CLIP_BYTES_PER_CELL = 24 + 32 + 8 + 24 + 4 + 4 + 15.5 * 12
+
+
+def hbm_roof(clip_ms: float):
+    """The HBM roof of the clip kernel: algorithmic bytes over its event time,
+    against the measured copy bandwidth (MEASURED_PEAKS.json) or the pool's
+    earlier measurement of 6.65 TB/s when that file is absent."""
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "MEASURED_PEAKS.json")
+    peak, src = 6650.0, "fallback 6.65 TB/s (MEASURED_PEAKS.json absent)"
+    if os.path.exists(path):
+        with open(path) as f:
+            m = json.load(f)
+        if m.get("hbm_gbs"):
+            peak, src = float(m["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs"
+    achieved = CLIP_BYTES_PER_CELL * N_GEN / (clip_ms / 1e3) / 1e9
+    return {"achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": src,
+            "bytes_per_cell": CLIP_BYTES_PER_CELL}
+
+
 def autotuned_leg(args, v, d_pts, flush):
     """The same generators on the grid the autotuner picks for them (a
     different bin grid, so a different but equally exact tessellation: each
@@ -409,7 +431,9 @@ def run_ours(args):
                          "frac": achieved / peak.value,
                          "peak_source": "FP64 FMA-chain microbenchmark run live by bench.py on this GPU",
                          "flops_per_launch": flops, "traffic": traffic,
-                         "issue": issue_roof(args, clip, clk)},
+                         "issue": issue_roof(args, clip, clk), "hbm": hbm_roof(clip),
+                         "note": "bound names the kernel's only arithmetic roof (FP64 pipe, no tensor cores);"
+                                 " it is issue-bound (roofline.issue), far from HBM (roofline.hbm)"},
             "e2e": None if e2e is None else {
                 "value": N_GEN / (e2e / 1e3) * ws, "unit": "cells/s", "ms_per_step": e2e,
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
