@@ -156,3 +156,25 @@ def test_batch_and_server_take_every_wall_kind():
         tv, tc, tn = t.summaries()
         assert np.array_equal(vol, tv) and np.array_equal(cen, tc) and np.array_equal(nf, tn)
     srv.close()
+
+
+def test_batch_huge_cells():
+    """Members whose cells outgrow the large tier (the centres of generators on
+    a sphere, 1,999 and 2,999 faces) go to the batch's block tier and equal
+    standalone tessellations bit for bit; Lloyd steps take them too."""
+    from common import bench_distribution
+    ms = [([0, 0, 0], [100, 100, 100], (13, 13, 13), bench_distribution("sphere", 2000, 90), []),
+          ([0, 0, 0], [1, 1, 1], (10, 10, 10), uniform(1000, 0, 1, 91), []),
+          ([0, 0, 0], [100, 100, 100], (15, 15, 15), bench_distribution("sphere", 3000, 92), [])]
+    b = build_batch(ms)
+    ts = [standalone(m) for m in ms]
+    for k, t in enumerate(ts):
+        assert_member_equal(b, k, t)
+    assert b.summaries(2)[2][0] == 2999
+    b.lloyd(2)
+    for t in ts:
+        for _ in range(2):
+            t.relax()
+            t.calculate()
+    for k, t in enumerate(ts):
+        assert_member_equal(b, k, t)

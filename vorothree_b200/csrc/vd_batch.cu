@@ -181,7 +181,11 @@ __global__ void k_brelax(const double* __restrict__ gen, const int32_t* __restri
 
 // control words: work cursors of the three passes, the overflow counts they
 // hand on, the search-order list count, and the big-bin sort count
-enum : int { kBCursor = 0, kBOvf, kBTab, kBBig, kBCursor2, kBMedOvf, kBCursor3, kBBigOvf, kBWords = 8 };
+enum : int {
+  kBCursor = 0, kBOvf, kBTab, kBBig, kBCursor2, kBMedOvf, kBCursor3, kBBigOvf, kBCursor4, kBHugeOvf, kBWords = 10
+};
+// blocks of the batch's huge tier (one cell each at a time)
+constexpr int kBHugeBlocks = 8;
 
 }  // namespace vd_batch_impl
 
@@ -217,7 +221,7 @@ struct vd_batch {
   Buf<long long> d_pool_off;
   Buf<unsigned int> d_ctl, d_tess_flags;
   Buf<unsigned long long> d_counters, d_pool_cursor;
-  Buf<unsigned char> d_big;
+  Buf<unsigned char> d_big, d_huge;
   int big_warps = 0;
   long long pool_cap = 0;
   std::vector<Buf<uint32_t>> scan_pool;
@@ -389,7 +393,7 @@ int clip_chain(vd_batch* b, const uint32_t* items, uint32_t nitems) {
   cudaStream_t s = b->stream;
   const int nt = (int)b->m.size();
   B_CK(b, cudaMemsetAsync(b->d_ctl.p, 0, 3 * sizeof(unsigned int), s));
-  B_CK(b, cudaMemsetAsync(b->d_ctl.p + kBCursor2, 0, 4 * sizeof(unsigned int), s));
+  B_CK(b, cudaMemsetAsync(b->d_ctl.p + kBCursor2, 0, 6 * sizeof(unsigned int), s));
   WorkList W;
   memset(&W, 0, sizeof(W));
   W.items = items;
@@ -416,7 +420,7 @@ int clip_chain(vd_batch* b, const uint32_t* items, uint32_t nitems) {
   W2.ovf_count = b->d_ctl.p + kBMedOvf;
   B_CK(b, launch_clip_med_batched(b->d_descs.p, b->d_off.p, nt, W2,
                                   std::max(1, b->num_sms * std::max(1, b->infomed.blocks_per_sm)), s));
-  // large capacity (global-memory storage); what overflows here is an error
+  // large capacity (global-memory storage)
   WorkList W3 = W;
   W3.items = b->d_list2.p;
   W3.nitems = 0;
@@ -425,6 +429,15 @@ int clip_chain(vd_batch* b, const uint32_t* items, uint32_t nitems) {
   W3.ovf_list = b->d_list0.p;
   W3.ovf_count = b->d_ctl.p + kBBigOvf;
   B_CK(b, launch_clip_fp64_big_batched(b->d_descs.p, b->d_off.p, nt, W3, b->d_big.p, b->big_warps, s));
+  // huge capacity (a thread block per cell); what overflows here is an error
+  WorkList W4 = W;
+  W4.items = b->d_list0.p;
+  W4.nitems = 0;
+  W4.nitems_dev = b->d_ctl.p + kBBigOvf;
+  W4.cursor = b->d_ctl.p + kBCursor4;
+  W4.ovf_list = b->d_list2.p;
+  W4.ovf_count = b->d_ctl.p + kBHugeOvf;
+  B_CK(b, launch_clip_fp64_huge_batched(b->d_descs.p, b->d_off.p, nt, W4, b->d_huge.p, kBHugeBlocks, s));
   return VD_OK;
 }
 
@@ -442,7 +455,7 @@ int resolve_tables(vd_batch* b) {
     unsigned int h[kBWords];
     B_CK(b, cudaMemcpyAsync(h, b->d_ctl.p, sizeof(h), cudaMemcpyDeviceToHost, s));
     B_CK(b, cudaStreamSynchronize(s));
-    if (h[kBBigOvf] > 0) return bfail(b, VD_EOVERFLOW, "%u cells exceed the large polytope capacity", h[kBBigOvf]);
+    if (h[kBHugeOvf] > 0) return bfail(b, VD_EOVERFLOW, "%u cells exceed the huge polytope capacity", h[kBHugeOvf]);
     const unsigned ntab = h[kBTab];
     if (ntab == 0) return VD_OK;
     std::vector<unsigned int> flags(nt);
@@ -538,7 +551,7 @@ int vd_batch_destroy(vd_batch* b) {
   b->d_list0.release(); b->d_list1.release(); b->d_list2.release(); b->d_list3.release(); b->d_sorted.release(); b->d_order.release();
   b->d_descs.release(); b->d_planes.release(); b->d_nf.release(); b->d_nv.release(); b->d_fnb.release(); b->d_pool_fnb.release();
   b->d_status.release(); b->d_pool_off.release(); b->d_ctl.release(); b->d_tess_flags.release();
-  b->d_counters.release(); b->d_pool_cursor.release(); b->d_big.release();
+  b->d_counters.release(); b->d_pool_cursor.release(); b->d_big.release(); b->d_huge.release();
   for (auto& p : b->scan_pool) p.release();
   if (b->ev0) cudaEventDestroy(b->ev0);
   if (b->ev1) cudaEventDestroy(b->ev1);
@@ -656,6 +669,7 @@ int vd_batch_commit(vd_batch* b) {
   B_CK(b, b->d_pool_area.ensure(b->pool_cap));
   b->big_warps = std::max(4, b->num_sms * 4);
   B_CK(b, b->d_big.ensure((size_t)b->big_warps * b->info64.big_scratch_per_warp));
+  B_CK(b, b->d_huge.ensure((size_t)kBHugeBlocks * clip_huge_scratch_per_block()));
   cudaStream_t s = b->stream;
   std::vector<double> cat(3 * n);
   for (int t = 0; t < nt; ++t) std::copy(b->m[t].pts.begin(), b->m[t].pts.end(), cat.begin() + 3 * b->h_in_off[t]);

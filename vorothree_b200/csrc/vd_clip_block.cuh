@@ -728,4 +728,45 @@ __global__ void __launch_bounds__(NW * 32)
   }
 }
 
+// the same over a batch's work list: items are global positions in the
+// concatenated bin-ordered generators (clip_worker_batched)
+template <class C, int NW>
+__global__ void __launch_bounds__(NW * 32)
+    k_clip_huge_block_batched(const TessDesc* descs, const uint32_t* tess_off, int ntess, const WorkList W,
+                              WarpPoly<C>* polys, BlockAux<C>* aux) {
+  __shared__ BlockShared<NW> B;
+  WarpPoly<C>& P = polys[blockIdx.x];
+  BlockAux<C>& X = aux[blockIdx.x];
+  const unsigned lane = lane_id();
+  const int w = (int)(threadIdx.x >> 5);
+  const uint32_t nitems = W.nitems_dev ? *W.nitems_dev : W.nitems;
+  while (true) {
+    if (threadIdx.x == 0) B.idx = atomicAdd(W.cursor, 1u);
+    __syncthreads();
+    const unsigned idx = B.idx;
+    __syncthreads();
+    if (idx >= nitems) break;
+    const uint32_t item = W.items ? W.items[idx] : idx;
+    const int t = find_tess(tess_off, ntess, item);
+    const TessDesc& T = descs[t];
+    const uint32_t cell = (uint32_t)T.sorted[item].id;
+    PolyState S;
+    const int st = compute_cell_block<C, NW>(T, cell, P, X, B, S);
+    __syncthreads();
+    if (w == 0) {
+      if (st == kCellOk) {
+        finalize_cell<C>(T, cell, P, S);
+      } else if (lane == 0) {
+        T.status[cell] = (uint8_t)st;
+        if (st == kCellOverflow && W.ovf_list) W.ovf_list[atomicAdd(W.ovf_count, 1u)] = item;
+        if (st == kCellTable) {
+          if (W.tab_list) W.tab_list[atomicAdd(W.tab_count, 1u)] = item;
+          if (W.tess_flags) atomicOr(&W.tess_flags[t], 1u);
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
 }  // namespace vd

@@ -32,6 +32,8 @@ cudaError_t launch_clip_fp64_big(const TessDesc& T, const WorkList& W, void* scr
 // large capacities
 size_t clip_huge_scratch_per_block();
 cudaError_t launch_clip_fp64_huge(const TessDesc& T, const WorkList& W, void* scratch, int nblocks, cudaStream_t s);
+cudaError_t launch_clip_fp64_huge_batched(const TessDesc* descs, const uint32_t* tess_off, int ntess,
+                                          const WorkList& W, void* scratch, int nblocks, cudaStream_t s);
 
 // medium-capacity tier (FP64, shared memory) for cells that overflow the fast path
 cudaError_t clip_med_setup(ClipLaunchInfo* info);

@@ -66,6 +66,15 @@ cudaError_t launch_clip_fp64_huge(const TessDesc& T, const WorkList& W, void* sc
   return cudaGetLastError();
 }
 
+cudaError_t launch_clip_fp64_huge_batched(const TessDesc* descs, const uint32_t* tess_off, int ntess,
+                                          const WorkList& W, void* scratch, int nblocks, cudaStream_t s) {
+  WarpPoly<HugeCfg>* polys = reinterpret_cast<WarpPoly<HugeCfg>*>(scratch);
+  BlockAux<HugeCfg>* aux = reinterpret_cast<BlockAux<HugeCfg>*>(polys + nblocks);
+  k_clip_huge_block_batched<HugeCfg, kHugeBlockWarps>
+      <<<nblocks, kHugeBlockWarps * 32, 0, s>>>(descs, tess_off, ntess, W, polys, aux);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_clip_fp64_fast_batched(const TessDesc* descs, const uint32_t* tess_off, int ntess,
                                           const WorkList& W, int nblocks, bool count, cudaStream_t s) {
   const size_t smem = sizeof(WarpPoly<FastCfg>) * kFastWarpsPerBlock;
