@@ -32,8 +32,8 @@ extern "C" {
 #define VD_OK 0
 #define VD_EINVAL 1     /* bad argument; e.g. wall id > -1000 (reference panics, wall/mod.rs:25-27) */
 #define VD_ENOMEM 2     /* device allocation failed or HBM budget exceeded */
-#define VD_EOVERFLOW 3  /* a cell exceeded every polytope capacity (calculate and batches: 65534
-                           vertices, 32767 faces; sealing, vd_cell: 2048 vertices, 512 faces) */
+#define VD_EOVERFLOW 3  /* a cell exceeded every polytope capacity (65534 vertices, 32767
+                           faces; the standalone vd_cell: 2048 vertices, 512 faces) */
 #define VD_ETIMEOUT 4   /* a bounded device wait gave up */
 #define VD_ECUDA 5      /* CUDA runtime error / no device */
 #define VD_ESTATE 6     /* call out of order (e.g. results before calculate) */

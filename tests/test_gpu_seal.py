@@ -92,3 +92,29 @@ def test_sealed_dense_blob_and_relax(oracle_mod):
     o.calculate_sealed()
     assert_same(g, o, check_counters=False, sample_cells=4)
     assert np.array_equal(g.seal_log, o.seal_log())
+
+
+def test_sealed_huge_cell(oracle_mod):
+    """A cell that only the block tier holds, sealed: the centre of generators
+    on a sphere inside a cylinder wall is adjacent to the ~2,000 sphere
+    generators the wall keeps and gains ~1,400 seal clips (3,469 faces); the
+    seal pass rebuilds it with a thread block, bit for bit the oracle's."""
+    import vorothree_b200 as v
+    from common import bench_distribution
+    pts = bench_distribution("sphere", 10000, 93)
+    w = v.Wall(WALL, v.CylinderGeometry([50.3, 50, 50], [0, 0, 1], 20.0))
+    g = v.Tessellation(v.BoundingBox([0, 0, 0], [100, 100, 100]), v.Algorithm3DGrid(13, 13, 13))
+    o = oracle_mod.OracleTessellation([0, 0, 0], [100, 100, 100], 13, 13, 13)
+    for t in (g, o):
+        t.set_generators(pts)
+    g.add_wall(w)
+    oracle_add(o, w)
+    g.calculate_sealed()
+    o.calculate_sealed()
+    assert g.summaries()[2][0] == 3469
+    assert_same(g, o, check_counters=False, sample_cells=3)
+    assert np.array_equal(g.seal_log, o.seal_log())
+    g.prune_boundaries()
+    o.prune_boundaries()
+    assert np.array_equal(g.prune_log, o.prune_log())
+    assert np.array_equal(g.prune_pos_log, o.prune_pos_log())

@@ -780,7 +780,8 @@ int seal_pass(vd_tess* t, const SealArgs& A, const uint32_t* items, uint32_t nit
               const WorkList* extra = nullptr) {
   cudaStream_t s = t->stream;
   if (nitems == 0) return VD_OK;
-  auto pass = [&](bool big, const uint32_t* list, uint32_t n, unsigned* novf, unsigned* ntab) -> int {
+  // tier 0: shared memory, 1: large (global memory, a warp per cell), 2: huge (a block per cell)
+  auto pass = [&](int tier, const uint32_t* list, uint32_t n, unsigned* novf, unsigned* ntab) -> int {
     VD_CK(t, cudaMemsetAsync(t->d_ctl.p, 0, 3 * sizeof(unsigned int), s));
     WorkList W;
     memset(&W, 0, sizeof(W));
@@ -792,10 +793,15 @@ int seal_pass(vd_tess* t, const SealArgs& A, const uint32_t* items, uint32_t nit
     W.ovf_count = t->d_ctl.p + kCtlOvfCount;
     W.tab_list = t->d_list[1].p;
     W.tab_count = t->d_ctl.p + kCtlTabCount;
-    if (big) {
+    if (tier == 1) {
       int r = ensure_big(t, n);
       if (r != VD_OK) return r;
       VD_CK(t, launch_seal_big(make_desc(t), W, A, t->d_big.p, (int)t->big_warps, s));
+    } else if (tier == 2) {
+      int r = ensure_big(t, n);  // the face pool
+      if (r == VD_OK) r = ensure_huge(t, n);
+      if (r != VD_OK) return r;
+      VD_CK(t, launch_seal_block(make_desc(t), W, A, t->d_huge.p, (int)t->huge_blocks, s));
     } else {
       const ClipLaunchInfo& li = t->info64;
       const size_t want = (n + li.warps_per_block - 1) / li.warps_per_block;
@@ -807,7 +813,7 @@ int seal_pass(vd_tess* t, const SealArgs& A, const uint32_t* items, uint32_t nit
   };
   // the input list lives in d_sel; overflow and table lists in d_list[0/1]
   unsigned novf = 0, ntab = 0;
-  int r = pass(false, items, nitems, &novf, &ntab);
+  int r = pass(0, items, nitems, &novf, &ntab);
   for (int guard = 0; r == VD_OK && guard < 64 && (novf > 0 || ntab > 0); ++guard) {
     if (ntab > 0) {
       if (t->order_complete) return fail(t, VD_ECUDA, "search order exhausted on a complete table");
@@ -818,13 +824,21 @@ int seal_pass(vd_tess* t, const SealArgs& A, const uint32_t* items, uint32_t nit
       VD_CK(t, cudaMemcpyAsync(t->d_list[2].p + ntab, t->d_list[0].p, novf * sizeof(uint32_t),
                                cudaMemcpyDeviceToDevice, s));
       const unsigned n2 = ntab + novf;
-      r = pass(false, t->d_list[2].p, n2, &novf, &ntab);
+      r = pass(0, t->d_list[2].p, n2, &novf, &ntab);
       continue;
     }
     VD_CK(t, cudaMemcpyAsync(t->d_list[2].p, t->d_list[0].p, novf * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
-    r = pass(true, t->d_list[2].p, novf, &novf, &ntab);
-    if (r == VD_OK && novf > 0) return fail(t, VD_EOVERFLOW, "%u cells exceed the large polytope capacity", novf);
+    r = pass(1, t->d_list[2].p, novf, &novf, &ntab);
+    // (cells that ran off the table as well are rerun from tier 0 with it, by
+    // the loop, before any goes to the huge tier)
+    if (r == VD_OK && novf > 0 && ntab == 0) {
+      VD_CK(t, cudaMemcpyAsync(t->d_list[2].p, t->d_list[0].p, novf * sizeof(uint32_t), cudaMemcpyDeviceToDevice,
+                               s));
+      r = pass(2, t->d_list[2].p, novf, &novf, &ntab);
+      if (r == VD_OK && novf > 0) return fail(t, VD_EOVERFLOW, "%u cells exceed the huge polytope capacity", novf);
+    }
   }
+  if (r == VD_OK && novf > 0) return fail(t, VD_EOVERFLOW, "%u cells exceed the polytope capacities", novf);
   return r;
 }
 
@@ -1477,8 +1491,9 @@ int vd_tess_calculate_sealed(vd_tess* t) {
   r = select_cells(t, t->d_s_mask.p, &nsel);
   if (r != VD_OK) return r;
   // logs: at most one entry per (face, curved wall) of a selected cell;
-  // entries of an attempt that a larger pass redoes repeat, so twice that
-  const uint32_t cap = (uint32_t)std::min<size_t>((size_t)2 * nsel * t->fout * (size_t)std::max<int>(1, __builtin_popcount(curved_bits(t))) + 1024, 1u << 30);
+  // entries of an attempt that a larger pass redoes repeat (up to three
+  // attempts: shared memory, large, huge), so three times that
+  const uint32_t cap = (uint32_t)std::min<size_t>((size_t)3 * nsel * t->fout * (size_t)std::max<int>(1, __builtin_popcount(curved_bits(t))) + 1024, 1u << 30);
   VD_CK(t, t->d_seal_rec.ensure(cap, t->stream));
   VD_CK(t, t->d_rec_cursor.ensure(2, t->stream));
   VD_CK(t, t->d_lcnt.ensure(n + 1, t->stream));

@@ -96,6 +96,10 @@ cudaError_t seal_setup();
 cudaError_t launch_seal_fast(const TessDesc& T, const WorkList& W, const SealArgs& A, int nblocks, cudaStream_t s);
 cudaError_t launch_seal_big(const TessDesc& T, const WorkList& W, const SealArgs& A, void* scratch, int nwarps,
                             cudaStream_t s);
+// the seal / prune pass's huge tier (a thread block per cell; scratch as
+// for launch_clip_fp64_huge)
+cudaError_t launch_seal_block(const TessDesc& T, const WorkList& W, const SealArgs& A, void* scratch, int nblocks,
+                              cudaStream_t s);
 cudaError_t launch_curved_mask(const int32_t* nf, const int32_t* fnb, const long long* pool_off,
                                const int32_t* pool_fnb, int fout, uint32_t n, const TessDesc& T,
                                uint32_t first_curved, uint32_t* mask, int nblocks, cudaStream_t s);

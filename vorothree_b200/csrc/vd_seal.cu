@@ -17,6 +17,7 @@
 // These kernels are separate instantiations: the production clip kernel's
 // code is unchanged.  Compiled with -fmad=false, like every FP64 path.
 #include "vd_clip.cuh"
+#include "vd_clip_block.cuh"
 #include "vd_export.cuh"
 #include "vd_internal.h"
 
@@ -61,6 +62,48 @@ __device__ int seal_clips(const TessDesc& T, const SealArgs& A, uint32_t i, Warp
       if (r == kClipOverflow) return kCellOverflow;
       if (r != kClipNoop) {
         if (log && lane_id() == 0) {
+          const unsigned at = atomicAdd(&A.rec_cursor[0], 1u);
+          if (at < A.rec_cap) A.seal_rec[at] = SealLogRec{(int32_t)i, cnt, j, T.walls[k].id};
+        }
+        ++cnt;
+      }
+    }
+  }
+  *nlog = cnt;
+  return kCellOk;
+}
+
+// seal_clips by a whole block (the huge tier, vd_clip_block.cuh); thread 0 logs
+template <class C, int NW>
+__device__ int seal_clips_block(const TessDesc& T, const SealArgs& A, uint32_t i, WarpPoly<C>& P, BlockAux<C>& X,
+                                BlockShared<NW>& B, PolyState& S, bool log, int* nlog) {
+  *nlog = 0;
+  const uint32_t mi = A.s_mask[i];
+  if (mi == 0) return kCellOk;
+  const double gx = T.gen[3 * (size_t)i], gy = T.gen[3 * (size_t)i + 1], gz = T.gen[3 * (size_t)i + 2];
+  int nfi;
+  const int32_t* fl = face_list(A.s_nf, A.s_fnb, A.s_pool_off, A.s_pool_fnb, A.fout, i, &nfi);
+  int cnt = 0;
+  for (int q = 0; q < nfi; ++q) {
+    const int32_t j = fl[q];
+    if (j < 0 || (uint32_t)j >= T.ncells) continue;
+    const uint32_t both = mi & A.s_mask[j] & A.curved;
+    if (!both) continue;
+    const double jx = T.gen[3 * (size_t)j], jy = T.gen[3 * (size_t)j + 1], jz = T.gen[3 * (size_t)j + 2];
+    for (int k = 0; k < T.nwalls; ++k) {
+      if (!((both >> k) & 1u)) continue;
+      double p[3], n[3];
+      if (!wall_plane(T.walls[k], jx, jy, jz, p, n)) continue;
+      double dot = 0.0;
+      dot += (gx - p[0]) * n[0];
+      dot += (gy - p[1]) * n[1];
+      dot += (gz - p[2]) * n[2];
+      if (!(dot <= 1e-9)) continue;
+      double r2;
+      const int r = block_clip<C, NW>(P, X, B, S, p[0], p[1], p[2], n[0], n[1], n[2], T.walls[k].id, false, gx, gy, gz, &r2);
+      if (r == kClipOverflow) return kCellOverflow;
+      if (r != kClipNoop) {
+        if (log && threadIdx.x == 0) {
           const unsigned at = atomicAdd(&A.rec_cursor[0], 1u);
           if (at < A.rec_cap) A.seal_rec[at] = SealLogRec{(int32_t)i, cnt, j, T.walls[k].id};
         }
@@ -174,6 +217,46 @@ __device__ void seal_worker(const TessDesc& T, const WorkList& W, const SealArgs
   }
 }
 
+// the seal / prune pass's huge tier: a thread block per cell
+template <class C, int NW>
+__global__ void __launch_bounds__(NW * 32)
+    k_seal_block(const TessDesc T, const WorkList W, const SealArgs A, WarpPoly<C>* polys, BlockAux<C>* aux) {
+  __shared__ BlockShared<NW> B;
+  WarpPoly<C>& P = polys[blockIdx.x];
+  BlockAux<C>& X = aux[blockIdx.x];
+  const unsigned lane = lane_id();
+  const int w = (int)(threadIdx.x >> 5);
+  while (true) {
+    if (threadIdx.x == 0) B.idx = atomicAdd(W.cursor, 1u);
+    __syncthreads();
+    const unsigned idx = B.idx;
+    __syncthreads();
+    if (idx >= W.nitems) break;
+    const uint32_t cell = W.items[idx];
+    PolyState S;
+    int st = compute_cell_block<C, NW>(T, cell, P, X, B, S);
+    int nlog = 0;
+    if (st == kCellOk && (A.mode == 1 || A.sealed))
+      st = seal_clips_block<C, NW>(T, A, cell, P, X, B, S, A.mode == 1, &nlog);
+    __syncthreads();
+    if (w == 0) {
+      if (st == kCellOk) {
+        if (A.mode == 1) {
+          finalize_cell<C>(T, cell, P, S);
+          if (W.ex_verts) export_cell<C>(W, P, S);
+          if (lane == 0 && A.cnt) A.cnt[cell] = nlog;
+        } else {
+          prune_cell<C>(T, A, cell, P, S);
+        }
+      } else if (lane == 0) {
+        if (st == kCellOverflow && W.ovf_list) W.ovf_list[atomicAdd(W.ovf_count, 1u)] = cell;
+        if (st == kCellTable && W.tab_list) W.tab_list[atomicAdd(W.tab_count, 1u)] = cell;
+      }
+    }
+    __syncthreads();
+  }
+}
+
 template <class C, int WPB, int MINB>
 __global__ void __launch_bounds__(WPB * 32, MINB) k_seal_fast(const TessDesc T, const WorkList W, const SealArgs A) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -257,6 +340,14 @@ cudaError_t launch_seal_fast(const TessDesc& T, const WorkList& W, const SealArg
 cudaError_t launch_seal_big(const TessDesc& T, const WorkList& W, const SealArgs& A, void* scratch, int nwarps,
                             cudaStream_t s) {
   k_seal_big<BigCfg><<<nwarps / 4, 128, 0, s>>>(T, W, A, reinterpret_cast<WarpPoly<BigCfg>*>(scratch));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_seal_block(const TessDesc& T, const WorkList& W, const SealArgs& A, void* scratch, int nblocks,
+                              cudaStream_t s) {
+  WarpPoly<HugeCfg>* polys = reinterpret_cast<WarpPoly<HugeCfg>*>(scratch);
+  BlockAux<HugeCfg>* aux = reinterpret_cast<BlockAux<HugeCfg>*>(polys + nblocks);
+  k_seal_block<HugeCfg, kHugeBlockWarps><<<nblocks, kHugeBlockWarps * 32, 0, s>>>(T, W, A, polys, aux);
   return cudaGetLastError();
 }
 
