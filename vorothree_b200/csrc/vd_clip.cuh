@@ -70,6 +70,8 @@ using MixedCfgCount = PolyCfg<96, 48, 288, 32, 32, 32, uint8_t, uint8_t, uint16_
 // outgrew the fast capacities -- typical of dense clustered inputs, where
 // the reference's bin-order walk clips a cell with thousands of candidates.
 using MedCfg = PolyCfg<224, 112, 672, 128, 64, 64, uint8_t, uint8_t, uint16_t, uint8_t, true, false>;
+// the same without the event counters (uninstrumented single tessellations)
+using MedCfgNC = PolyCfg<224, 112, 672, 128, 64, 64, uint8_t, uint8_t, uint16_t, uint8_t, false, false>;
 // Large-capacity pass (global-memory storage): vertex ids stay u16 like the
 // reference's face_indices (cell_3d_faces.rs:31).
 using BigCfg = PolyCfg<2048, 512, 6144, 1024, 512, 512, uint16_t, uint16_t, uint32_t, uint16_t, true, false>;

@@ -541,7 +541,7 @@ int clip_pass(vd_tess* t, int tier, const uint32_t* items, uint32_t nitems, uint
   if (tier == 1) {
     const int nblocks = (int)std::max<size_t>(
         1, std::min<size_t>((nitems + 1) / 2, (size_t)t->num_sms * std::max(1, t->infomed.blocks_per_sm)));
-    VD_CK(t, launch_clip_med(T, W, nblocks, s));
+    VD_CK(t, launch_clip_med(T, W, nblocks, t->instrument, s));
     g_launches++;
   } else if (tier == 0) {
     const bool mixed = t->precision == VD_PREC_MIXED;

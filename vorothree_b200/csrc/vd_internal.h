@@ -37,7 +37,8 @@ cudaError_t launch_clip_fp64_huge_batched(const TessDesc* descs, const uint32_t*
 
 // medium-capacity tier (FP64, shared memory) for cells that overflow the fast path
 cudaError_t clip_med_setup(ClipLaunchInfo* info);
-cudaError_t launch_clip_med(const TessDesc& T, const WorkList& W, int nblocks, cudaStream_t s);
+// count: the instrumented variant (event counters kept)
+cudaError_t launch_clip_med(const TessDesc& T, const WorkList& W, int nblocks, bool count, cudaStream_t s);
 cudaError_t launch_clip_med_batched(const TessDesc* descs, const uint32_t* tess_off, int ntess,
                                     const WorkList& W, int nblocks, cudaStream_t s);
 

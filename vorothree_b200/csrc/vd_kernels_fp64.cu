@@ -117,6 +117,10 @@ cudaError_t clip_med_setup(ClipLaunchInfo* info) {
   cudaError_t e = cudaFuncSetAttribute(k_clip_fast<MedCfg, kMedWarpsPerBlock, 1>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
+  static_assert(sizeof(WarpPoly<MedCfgNC>) <= sizeof(WarpPoly<MedCfg>), "one shared-memory size serves both");
+  e = cudaFuncSetAttribute(k_clip_fast<MedCfgNC, kMedWarpsPerBlock, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem);
+  if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(k_clip_fast_batched<MedCfg, kMedWarpsPerBlock, 1>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
@@ -127,9 +131,12 @@ cudaError_t clip_med_setup(ClipLaunchInfo* info) {
   return e;
 }
 
-cudaError_t launch_clip_med(const TessDesc& T, const WorkList& W, int nblocks, cudaStream_t s) {
+cudaError_t launch_clip_med(const TessDesc& T, const WorkList& W, int nblocks, bool count, cudaStream_t s) {
   const size_t smem = sizeof(WarpPoly<MedCfg>) * kMedWarpsPerBlock;
-  k_clip_fast<MedCfg, kMedWarpsPerBlock, 1><<<nblocks, kMedWarpsPerBlock * 32, smem, s>>>(T, W);
+  if (count)
+    k_clip_fast<MedCfg, kMedWarpsPerBlock, 1><<<nblocks, kMedWarpsPerBlock * 32, smem, s>>>(T, W);
+  else
+    k_clip_fast<MedCfgNC, kMedWarpsPerBlock, 1><<<nblocks, kMedWarpsPerBlock * 32, smem, s>>>(T, W);
   return cudaGetLastError();
 }
 
