@@ -781,6 +781,8 @@ class Tessellation:
     def _iter_cells(self, chunk: int = 1 << 18):
         """Every cell as a Cell3DFaces, exported a range at a time."""
         n = self.count_cells()
+        if n == 0:
+            return
         vol, cen, _ = self._summary_cache()
         aoff, ar = self._area_cache()
         for b in range(0, n, chunk):
