@@ -41,9 +41,9 @@ def test_export_equals_get_cell(precision):
     assert e["v_off"].tolist() == [0] and e["vertices"].size == 0
 
 
-def test_export_overflow_cells_through_get_cell():
-    # a dense blob on a coarse grid: some polytopes outgrow the device pass's
-    # capacities and are exported through get_cell's tiers
+def test_export_overflow_cells():
+    # a dense blob on a coarse grid: some cells outgrow the shared-memory
+    # capacities and are rebuilt by the medium and large export tiers
     rng = np.random.Generator(np.random.PCG64(17))
     pts = np.concatenate([0.5 + rng.normal(0.0, 0.01, size=(2500, 3)), rng.uniform(0, 1, size=(300, 3))])
     t = gpu_tess([0, 0, 0], [1, 1, 1], (4, 4, 4), pts)
@@ -84,6 +84,27 @@ def test_cells_and_map():
     vol, _, nf = t.summaries()
     got = t.map(lambda c: (c.volume(), len(c.face_counts())))
     assert [g[0] for g in got] == vol.tolist() and [g[1] for g in got] == nf.tolist()
+
+
+@pytest.mark.parametrize("n", [90, 400])
+def test_export_large_cell(n):
+    # the centre of generators on a sphere with n-1 faces: 89 fit the medium
+    # tier, 399 only the large one (global scratch)
+    from common import bench_distribution
+    t = gpu_tess([0, 0, 0], [100, 100, 100], (6, 6, 6), bench_distribution("sphere", n, 83))
+    x = assert_export_matches(t)
+    assert x["f_off"][1] - x["f_off"][0] == n - 1
+
+
+def test_export_sealed_large_cell():
+    import vorothree_b200 as v
+    from common import bench_distribution
+    t = v.Tessellation(v.BoundingBox([0, 0, 0], [100, 100, 100]), v.Algorithm3DGrid(6, 6, 6))
+    t.set_generators(bench_distribution("sphere", 400, 84))
+    t.add_wall(v.Wall(WALL, v.CylinderGeometry([50, 50, 50], [0.1, 0.2, 1], 45.0)))
+    t.calculate_sealed()
+    x = assert_export_matches(t)
+    assert x["f_off"][1] - x["f_off"][0] >= 399
 
 
 def test_export_huge_cell():

@@ -171,3 +171,48 @@ def test_random_generators_attempt_cap(oracle_mod):
         assert n == o.random_generators(50, seed) and 5 < n < 50
         assert np.array_equal(g.generators(), o.generators())
     assert g.random_generators(0, 1) == 0 and g.count_generators() == 0
+
+
+def _random_wall(rng, lo, hi, k):
+    """A wall of a random kind around the box's middle, sized to keep a good
+    share of the generators."""
+    import vorothree_b200 as v
+    c = lo + (hi - lo) * rng.uniform(0.4, 0.6, 3)
+    ext = float(np.linalg.norm(hi - lo)) / 2.0
+    axis = rng.normal(size=3)
+    kind = int(rng.integers(0, 6))
+    wid = WALL - k
+    if kind == 0:
+        return v.Wall(wid, v.PlaneGeometry(list(c), list(axis)))
+    if kind == 1:
+        return v.Wall(wid, v.SphereGeometry(list(c), ext * rng.uniform(0.6, 0.9)))
+    if kind == 2:
+        return v.Wall(wid, v.CylinderGeometry(list(c), list(axis), ext * rng.uniform(0.5, 0.8)))
+    if kind == 3:
+        tip = c - axis / np.linalg.norm(axis) * ext * 1.5
+        return v.Wall(wid, v.ConeGeometry(list(tip), list(axis), rng.uniform(0.7, 1.2)))
+    if kind == 4:
+        return v.Wall(wid, v.TorusGeometry(list(c), list(axis), ext * 0.45, ext * rng.uniform(0.35, 0.45)))
+    P = v.ConvexPolyhedronGeometry
+    maker = [P.new_tetrahedron, P.new_hexahedron, P.new_octahedron, P.new_dodecahedron, P.new_icosahedron][
+        int(rng.integers(0, 5))]
+    return v.Wall(wid, maker(list(c), ext * rng.uniform(0.9, 1.3)))
+
+
+@pytest.mark.parametrize("seed", range(12))
+def test_random_configurations_bitwise(oracle_mod, seed):
+    """Random boxes, grids, generator distributions and 0-3 walls of random
+    kinds, in both precisions: every cell equal to the oracle's."""
+    from common import bench_distribution
+    rng = np.random.Generator(np.random.PCG64(500 + seed))
+    lo = rng.uniform(-50, 50, 3)
+    hi = lo + rng.uniform(0.5, 20, 3)
+    n = int(rng.integers(500, 4000))
+    kind = ["uniform", "axes", "central", "uniform"][seed % 4]
+    pts = bench_distribution(kind, n, 600 + seed, lo, hi)
+    grid = tuple(int(x) for x in rng.integers(1, 16, 3))
+    walls = [_random_wall(rng, lo, hi, k) for k in range(int(rng.integers(0, 4)))]
+    precision = "mixed" if seed % 3 == 2 else "fp64"
+    g = gpu_tess(list(lo), list(hi), grid, pts, walls, walls_first=bool(seed % 2), precision=precision)
+    o = oracle_tess(oracle_mod, list(lo), list(hi), grid, pts, walls, bool(seed % 2))
+    assert_same(g, o, check_counters=(precision == "fp64"), sample_cells=4)

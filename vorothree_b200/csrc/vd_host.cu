@@ -1756,9 +1756,11 @@ int vd_tess_get_cell(vd_tess* t, size_t i, int32_t* n_vertices, int32_t* n_faces
 
 // Tessellation::cells / map (tessellation.rs:391-412, 524-526) for the cells
 // [begin, end): sizes, offsets and, when the arrays are given, every polytope.
-// The device pass rebuilds the cells with calculate()'s code (and the seal
-// clips, when the tessellation is sealed); cells it cannot hold (beyond the
-// shared-memory capacities) go through get_cell.
+// The device passes rebuild the cells with calculate()'s code (and the seal
+// clips, when the tessellation is sealed): first with the shared-memory
+// capacities, then the cells that overflowed with the medium ones, then with
+// the large ones in global scratch; the few cells beyond those go through
+// get_cell.
 int vd_tess_export_cells(vd_tess* t, size_t begin, size_t end, int64_t* v_off, int64_t* f_off, int64_t* h_off,
                          double* vertices, uint32_t* face_counts, uint32_t* face_indices, int32_t* face_neighbors) {
   int r = check_ready(t);
@@ -1783,11 +1785,31 @@ int vd_tess_export_cells(vd_tess* t, size_t begin, size_t end, int64_t* v_off, i
   SealArgs SA = seal_args(t, 1);
   SA.cnt = nullptr;
   SA.rec_cap = 0;
+  // the item list of each tier inside d_bx_items: all cells of the range (in
+  // the spatial order), then the medium tier's, then the large tier's
+  const size_t nr = hi - lo;
+  size_t tier_at[3] = {0, nr, nr};
+  uint32_t tier_n[3] = {(uint32_t)nr, 0, 0};
+  auto run_tier = [&](int pass, int tier) -> int {
+    if (tier == 2) {
+      int rb = ensure_big(t, tier_n[2]);
+      if (rb != VD_OK) return rb;
+    }
+    VD_CK(t, cudaMemsetAsync(t->d_ctl.p, 0, 3 * sizeof(unsigned int), s));
+    A.items = t->d_bx_items.p + tier_at[tier];
+    A.nitems = tier_n[tier];
+    void* scratch = tier == 2 ? (void*)t->d_big.p : nullptr;
+    const int nwarps = tier == 2 ? (int)t->big_warps : 0;
+    VD_CK(t, t->sealed ? launch_seal_export_cells(T, A, SA, pass, tier, t->num_sms, scratch, nwarps, s)
+                       : launch_export_cells(T, A, pass, tier, t->num_sms, scratch, nwarps, s));
+    g_launches++;
+    return VD_OK;
+  };
   if (device) {
     const size_t all = t->ncells;
     VD_CK(t, t->d_flags.ensure(all + 1, s));
     VD_CK(t, t->d_pos.ensure(all + 1, s));
-    VD_CK(t, t->d_bx_items.ensure(hi - lo, s));
+    VD_CK(t, t->d_bx_items.ensure(3 * nr, s));
     VD_CK(t, t->d_bx_sizes.ensure(3 * n, s));
     k_range_flags<<<grid_blocks(t, all, 256), 256, 0, s>>>(t->d_sorted.p, all, (long long)lo, (long long)hi,
                                                          t->d_flags.p);
@@ -1801,19 +1823,27 @@ int vd_tess_export_cells(vd_tess* t, size_t begin, size_t end, int64_t* v_off, i
     g_launches++;
     VD_CK(t, cudaGetLastError());
     VD_CK(t, cudaMemsetAsync(t->d_bx_sizes.p, 0, 3 * n * sizeof(int32_t), s));
-    VD_CK(t, cudaMemsetAsync(t->d_ctl.p, 0, 3 * sizeof(unsigned int), s));
-    A.items = t->d_bx_items.p;
-    A.nitems = (uint32_t)(hi - lo);
     A.cursor = t->d_ctl.p + kCtlCursor;
     A.begin = begin;
     A.sizes = t->d_bx_sizes.p;
-    VD_CK(t, t->sealed ? launch_seal_export_cells(T, A, SA, 0, t->num_sms, s)
-                       : launch_export_cells(T, A, 0, t->num_sms, s));
-    g_launches++;
-    VD_CK(t, cudaMemcpyAsync(sz.data(), t->d_bx_sizes.p, 3 * n * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
-    VD_CK(t, cudaStreamSynchronize(s));
-    for (size_t k = 0; k < n; ++k)
-      if (sz[3 * k] < 0) host_cells.push_back(begin + k);
+    std::vector<uint32_t> next;
+    for (int tier = 0; tier < 3; ++tier) {
+      if (tier > 0) {
+        if (next.empty()) break;
+        tier_at[tier] = tier == 1 ? nr : nr + tier_n[1];
+        tier_n[tier] = (uint32_t)next.size();
+        VD_CK(t, cudaMemcpyAsync(t->d_bx_items.p + tier_at[tier], next.data(), next.size() * sizeof(uint32_t),
+                                 cudaMemcpyHostToDevice, s));
+      }
+      r = run_tier(0, tier);
+      if (r != VD_OK) return r;
+      VD_CK(t, cudaMemcpyAsync(sz.data(), t->d_bx_sizes.p, 3 * n * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+      VD_CK(t, cudaStreamSynchronize(s));
+      next.clear();
+      for (size_t k = 0; k < n; ++k)
+        if (sz[3 * k] < 0) next.push_back((uint32_t)(begin + k));
+    }
+    for (uint32_t c : next) host_cells.push_back(c);
   }
   for (size_t c : host_cells) {
     int32_t nv = 0, nf = 0, nh = 0;
@@ -1842,7 +1872,6 @@ int vd_tess_export_cells(vd_tess* t, size_t begin, size_t end, int64_t* v_off, i
     VD_CK(t, cudaMemcpyAsync(t->d_bx_off.p, v_off, (n + 1) * 8, cudaMemcpyHostToDevice, s));
     VD_CK(t, cudaMemcpyAsync(t->d_bx_off.p + (n + 1), f_off, (n + 1) * 8, cudaMemcpyHostToDevice, s));
     VD_CK(t, cudaMemcpyAsync(t->d_bx_off.p + 2 * (n + 1), h_off, (n + 1) * 8, cudaMemcpyHostToDevice, s));
-    VD_CK(t, cudaMemsetAsync(t->d_ctl.p, 0, 3 * sizeof(unsigned int), s));
     A.voff = t->d_bx_off.p;
     A.foff = t->d_bx_off.p + (n + 1);
     A.hoff = t->d_bx_off.p + 2 * (n + 1);
@@ -1851,9 +1880,13 @@ int vd_tess_export_cells(vd_tess* t, size_t begin, size_t end, int64_t* v_off, i
     A.fi = t->d_bx_fi.p;
     A.fn = t->d_bx_fn.p;
     A.sizes = nullptr;
-    VD_CK(t, t->sealed ? launch_seal_export_cells(T, A, SA, 1, t->num_sms, s)
-                       : launch_export_cells(T, A, 1, t->num_sms, s));
-    g_launches++;
+    // a cell writes in the first tier that holds it (the rebuild is the same
+    // in every tier, so the sizes agree with pass 0's)
+    for (int tier = 0; tier < 3; ++tier) {
+      if (tier_n[tier] == 0) continue;
+      r = run_tier(1, tier);
+      if (r != VD_OK) return r;
+    }
     if (tv) VD_CK(t, cudaMemcpyAsync(vertices, t->d_bx_v.p, 3 * tv * sizeof(double), cudaMemcpyDeviceToHost, s));
     if (tf) {
       VD_CK(t, cudaMemcpyAsync(face_counts, t->d_bx_fc.p, tf * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));

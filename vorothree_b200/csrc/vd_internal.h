@@ -75,10 +75,13 @@ struct ExportArgs {
   uint32_t* fi;
   int32_t* fn;
 };
-cudaError_t launch_export_cells(const TessDesc& T, const ExportArgs& A, int pass, int num_sms, cudaStream_t s);
+// tier 0: fast (shared memory), 1: medium (shared memory), 2: large (global
+// scratch of nwarps polytopes, a multiple of 4)
+cudaError_t launch_export_cells(const TessDesc& T, const ExportArgs& A, int pass, int tier, int num_sms,
+                                void* scratch, int nwarps, cudaStream_t s);
 // the same for a sealed tessellation (vd_seal.cu): the seal clips applied
-cudaError_t launch_seal_export_cells(const TessDesc& T, const ExportArgs& E, const SealArgs& A, int pass,
-                                     int num_sms, cudaStream_t s);
+cudaError_t launch_seal_export_cells(const TessDesc& T, const ExportArgs& E, const SealArgs& A, int pass, int tier,
+                                     int num_sms, void* scratch, int nwarps, cudaStream_t s);
 
 // the generator text format of Tessellation::read_generators (vd_text.cpp):
 // false with a message when the text is not UTF-8

@@ -394,21 +394,40 @@ __global__ void __launch_bounds__(kExportWarps * 32)
   export_worker<C, PASS>(T, E, reinterpret_cast<WarpPoly<C>*>(smem)[threadIdx.x >> 5], SealExtra{A});
 }
 
-template <int PASS>
-cudaError_t seal_export_pass(const TessDesc& T, const ExportArgs& E, const SealArgs& A, int num_sms, cudaStream_t s) {
-  const size_t smem = sizeof(WarpPoly<FastCfg>) * kExportWarps;
+template <class C, int PASS>
+__global__ void __launch_bounds__(kExportWarps * 32)
+    k_seal_export_global(const TessDesc T, const ExportArgs E, const SealArgs A, WarpPoly<C>* scratch) {
+  const size_t gw = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  export_worker<C, PASS>(T, E, scratch[gw], SealExtra{A});
+}
+
+template <class C, int PASS>
+cudaError_t seal_export_smem(const TessDesc& T, const ExportArgs& E, const SealArgs& A, int num_sms,
+                             cudaStream_t s) {
+  const size_t smem = sizeof(WarpPoly<C>) * kExportWarps;
   int nblocks = 1;
-  cudaError_t e = export_launch_shape(k_seal_export<FastCfg, PASS>, smem, E.nitems, num_sms, &nblocks);
+  cudaError_t e = export_launch_shape(k_seal_export<C, PASS>, smem, E.nitems, num_sms, &nblocks);
   if (e != cudaSuccess) return e;
-  k_seal_export<FastCfg, PASS><<<nblocks, kExportWarps * 32, smem, s>>>(T, E, A);
+  k_seal_export<C, PASS><<<nblocks, kExportWarps * 32, smem, s>>>(T, E, A);
+  return cudaGetLastError();
+}
+
+template <int PASS>
+cudaError_t seal_export_pass(const TessDesc& T, const ExportArgs& E, const SealArgs& A, int tier, int num_sms,
+                             void* scratch, int nwarps, cudaStream_t s) {
+  if (tier == 0) return seal_export_smem<FastCfg, PASS>(T, E, A, num_sms, s);
+  if (tier == 1) return seal_export_smem<MedCfgNC, PASS>(T, E, A, num_sms, s);
+  k_seal_export_global<BigCfg, PASS><<<nwarps / kExportWarps, kExportWarps * 32, 0, s>>>(
+      T, E, A, reinterpret_cast<WarpPoly<BigCfg>*>(scratch));
   return cudaGetLastError();
 }
 
 }  // namespace
 
-cudaError_t launch_seal_export_cells(const TessDesc& T, const ExportArgs& E, const SealArgs& A, int pass,
-                                     int num_sms, cudaStream_t s) {
-  return pass == 0 ? seal_export_pass<0>(T, E, A, num_sms, s) : seal_export_pass<1>(T, E, A, num_sms, s);
+cudaError_t launch_seal_export_cells(const TessDesc& T, const ExportArgs& E, const SealArgs& A, int pass, int tier,
+                                     int num_sms, void* scratch, int nwarps, cudaStream_t s) {
+  return pass == 0 ? seal_export_pass<0>(T, E, A, tier, num_sms, scratch, nwarps, s)
+                   : seal_export_pass<1>(T, E, A, tier, num_sms, scratch, nwarps, s);
 }
 
 }  // namespace vd
