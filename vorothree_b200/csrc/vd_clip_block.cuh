@@ -144,7 +144,10 @@ __device__ int block_clip(WarpPoly<C>& P, BlockAux<C>& X, BlockShared<NW>& B, Po
   __syncthreads();
 
   // 3. the face walk (:369-452): end vertices, crossings in walk order, the
-  //    emitted-entry prefix E, each face's first crossing
+  //    emitted-entry prefix E, each face's first crossing.  The first pass
+  //    follows each position's chain of loads (face, its bounds, the edge's
+  //    ends, their new ids) and keeps the end vertex and the new ids; the
+  //    second reads those back and follows the chain again only at crossings.
   block_range<NW>(nh, w, &lo, &hi);
   {
     int ncr = 0, emit = 0, lastc = -1;
@@ -156,8 +159,11 @@ __device__ int block_clip(WarpPoly<C>& P, BlockAux<C>& X, BlockShared<NW>& B, Po
         const int f0 = P.fs[cb][f];
         const unsigned s = P.fi[cb][p];
         const unsigned e = P.fi[cb][(p + 1 == (int)P.fs[cb][f + 1]) ? f0 : p + 1];
-        si = P.o2n[s] != C::VNONE;
-        ei = P.o2n[e] != C::VNONE;
+        const VId os = P.o2n[s], oe = P.o2n[e];
+        si = os != C::VNONE;
+        ei = oe != C::VNONE;
+        P.fe[p] = (VId)e;
+        P.pve[p] = VPair<VId>{os, oe};
         cr = si != ei;
       }
       const unsigned m = __ballot_sync(kFull, cr);
@@ -180,18 +186,10 @@ __device__ int block_clip(WarpPoly<C>& P, BlockAux<C>& X, BlockShared<NW>& B, Po
     for (int b = lo; b < hi; b += 32) {
       const int p = b + lane;
       bool cr = false, si = false, ei = false;
-      int f = 0, f0 = 0;
-      unsigned s = 0, e = 0;
       if (p < hi) {
-        f = P.pf[cb][p];
-        f0 = P.fs[cb][f];
-        s = P.fi[cb][p];
-        e = P.fi[cb][(p + 1 == (int)P.fs[cb][f + 1]) ? f0 : p + 1];
-        const VId os = P.o2n[s], oe = P.o2n[e];
-        si = os != C::VNONE;
-        ei = oe != C::VNONE;
-        P.fe[p] = (VId)e;
-        P.pve[p] = VPair<VId>{os, oe};
+        const VPair<VId> ve = P.pve[p];
+        si = ve.s != C::VNONE;
+        ei = ve.e != C::VNONE;
         cr = si != ei;
       }
       const unsigned m = __ballot_sync(kFull, cr);
@@ -200,6 +198,10 @@ __device__ int block_clip(WarpPoly<C>& P, BlockAux<C>& X, BlockShared<NW>& B, Po
         const unsigned before = m & lt;
         const int prevp = before ? b + 31 - __clz(before) : lastcross;
         if (k < C::CCAP) {
+          const int f = P.pf[cb][p];
+          const int f0 = P.fs[cb][f];
+          const unsigned s = P.fi[cb][p];
+          const unsigned e = P.fe[p];
           P.cpos[k] = (typename C::Pos)p;
           P.ckey[k] = (typename C::Key)(s < e ? (s << C::KSHIFT | e) : (e << C::KSHIFT | s));
           P.cidx[p] = (typename C::CId)k;
@@ -343,65 +345,46 @@ __device__ int block_clip(WarpPoly<C>& P, BlockAux<C>& X, BlockShared<NW>& B, Po
   __syncthreads();
   if (longface || hk > C::HCAP) return kClipOverflow;
 
-  // 7. the surviving faces' entries, and the lid segments (v, u) ordered by
-  //    the position of their in->out crossing
-  block_range<NW>(nh, w, &lo, &hi);
-  {
-    int nsg = 0;
-    for (int b = lo; b < hi; b += 32) {
-      const int p = b + lane;
-      bool segsrc = false;
-      if (p < hi) {
-        const int f = P.pf[cb][p];
-        const VPair<VId> ve = P.pve[p];
-        const unsigned os = ve.s, oe = ve.e;
-        const bool si = os != C::VNONE, ei = oe != C::VNONE;
-        const unsigned fw = P.fnew[f];
-        if (fw != C::FNONE) {
-          const int o = (int)P.fdel[f] + (int)P.E[p];
-          if (si) {
-            P.fi[nb][o] = (VId)(ei ? oe : (unsigned)P.cid[P.cidx[p]]);
-            P.pf[nb][o] = (FId)fw;
-            segsrc = !ei;
-          } else if (ei) {
-            P.fi[nb][o] = P.cid[P.cidx[p]];
-            P.pf[nb][o] = (FId)fw;
-            P.fi[nb][o + 1] = (VId)oe;
-            P.pf[nb][o + 1] = (FId)fw;
-          }
-        }
+  // 7. the surviving faces' entries (every thread), and the lid segments
+  //    (v, u) ordered by the position of their in->out crossing: the crossing
+  //    list is in position order, so warp 0 takes them from it
+  for (int p = tid; p < nh; p += nt) {
+    const int f = P.pf[cb][p];
+    const unsigned fw = P.fnew[f];
+    if (fw != C::FNONE) {
+      const VPair<VId> ve = P.pve[p];
+      const unsigned os = ve.s, oe = ve.e;
+      const bool si = os != C::VNONE, ei = oe != C::VNONE;
+      const int o = (int)P.fdel[f] + (int)P.E[p];
+      if (si) {
+        P.fi[nb][o] = (VId)(ei ? oe : (unsigned)P.cid[P.cidx[p]]);
+        P.pf[nb][o] = (FId)fw;
+      } else if (ei) {
+        P.fi[nb][o] = P.cid[P.cidx[p]];
+        P.pf[nb][o] = (FId)fw;
+        P.fi[nb][o + 1] = (VId)oe;
+        P.pf[nb][o + 1] = (FId)fw;
       }
-      nsg += __popc(__ballot_sync(kFull, segsrc));
     }
-    if (lane == 0) B.a[w] = nsg;
   }
-  __syncthreads();
-  if (tid == 0) {
-    int s = 0;
-    for (int q = 0; q < NW; ++q) {
-      B.ia[q] = s;
-      s += B.a[q];
-    }
-    B.val[6] = s;
-  }
-  __syncthreads();
-  const int nseg = B.val[6];
-  {
-    int k0 = B.ia[w];
-    for (int b = lo; b < hi; b += 32) {
-      const int p = b + lane;
+  if (w == 0) {
+    int k0 = 0;
+    for (int b = 0; b < ncross; b += 32) {
+      const int kc = b + (int)lane;
       bool segsrc = false;
       int f = 0;
-      if (p < hi) {
-        f = P.pf[cb][p];
+      if (kc < ncross) {
+        const int p = P.cpos[kc];
         const VPair<VId> ve = P.pve[p];
-        segsrc = P.fnew[f] != C::FNONE && ve.s != C::VNONE && ve.e == C::VNONE;
+        if (ve.s != C::VNONE && ve.e == C::VNONE) {
+          f = P.pf[cb][p];
+          segsrc = P.fnew[f] != C::FNONE;
+        }
       }
       const unsigned sm = __ballot_sync(kFull, segsrc);
       if (segsrc) {
         const int k = k0 + __popc(sm & lt);
         if (k < C::SCAP) {
-          const int kc = P.cidx[p];
           int kn = kc + 1;
           if (kn >= ncross || (int)P.cpos[kn] >= (int)P.fs[cb][f + 1]) kn = P.fcr[f];
           P.sega[k] = P.cid[kn];
@@ -410,6 +393,7 @@ __device__ int block_clip(WarpPoly<C>& P, BlockAux<C>& X, BlockShared<NW>& B, Po
       }
       k0 += __popc(sm);
     }
+    if (lane == 0) B.val[6] = k0;
   }
   for (int f = tid; f < nf; f += nt) {
     const unsigned fw = P.fnew[f];
@@ -420,6 +404,7 @@ __device__ int block_clip(WarpPoly<C>& P, BlockAux<C>& X, BlockShared<NW>& B, Po
   }
   if (tid == 0) P.fs[nb][nfk] = (typename C::Pos)hk;
   __syncthreads();
+  const int nseg = B.val[6];
   if (nseg > C::SCAP) return kClipOverflow;
 
   // 8. the lid (:470-495), warp 0: lid_map (last writer wins) and the chain
