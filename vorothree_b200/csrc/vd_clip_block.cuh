@@ -27,13 +27,7 @@ struct BlockShared {
   double r2[NW];
   uint8_t cand[NW][32];        // the walk's candidate staging, a row per warp
   unsigned idx;
-};
-
-// vertices compacted by a clip land here first: warps renumber different
-// ranges at once, and a kept vertex may move into another warp's range
-template <class C>
-struct BlockAux {
-  double x[C::VCAP], y[C::VCAP], z[C::VCAP];
+  int vfirst;                  // a clip's first removed vertex
 };
 
 // warp w's contiguous share [lo, hi) of [0, n), whole chunks of 32
@@ -67,7 +61,7 @@ __device__ __forceinline__ void block_scan_totals(BlockShared<NW>& B, int s0, in
 // clip_with_scratch (cell_3d_faces.rs:288-503) by the whole block; every
 // thread calls it with the same arguments and gets the same result.
 template <class C, int NW>
-__device__ int block_clip(WarpPoly<C>& P, BlockAux<C>& X, BlockShared<NW>& B, PolyState& S, double px, double py,
+__device__ int block_clip(WarpPoly<C>& P, BlockShared<NW>& B, PolyState& S, double px, double py,
                           double pz, double nx, double ny, double nz, int nbr, bool with_gen, double gx, double gy,
                           double gz, double* r2out) {
   static_assert(!C::MIXED && !C::COUNT, "the block clip is the plain FP64 path without counters");
@@ -80,14 +74,24 @@ __device__ int block_clip(WarpPoly<C>& P, BlockAux<C>& X, BlockShared<NW>& B, Po
   const int tid = (int)threadIdx.x;
   const int nv = S.nv, nf = S.nf, nh = S.nh, cb = S.cb, nb = cb ^ 1;
 
-  // 1. signed distances and the 3-band flags (:302-326)
+  // 1. signed distances and the 3-band flags (:302-326); the kept vertices'
+  //    squared distance from the generator (the clip's max radius)
   bool out = false, sin = false;
+  double r2 = 0.0;
   for (int v = tid; v < nv; v += nt) {
-    const double d = (P.vx[v] - px) * nx + (P.vy[v] - py) * ny + (P.vz[v] - pz) * nz;
+    const double vx = P.vx[v], vy = P.vy[v], vz = P.vz[v];
+    const double d = (vx - px) * nx + (vy - py) * ny + (vz - pz) * nz;
     P.dist[v] = d;
     P.o2n[v] = d > kTol ? (VId)C::VNONE : (VId)0;
     out |= d > kTol;
     sin |= d < -kTol;
+    if (!(d > kTol) && with_gen) {
+      double dx = vx - gx;
+      double dy = vy - gy;
+      double dz = vz - gz;
+      double d2 = dx * dx + dy * dy + dz * dz;
+      r2 = fmax(r2, d2);
+    }
   }
   const bool any_out = __syncthreads_or(out) != 0;
   const bool any_sin = __syncthreads_or(sin) != 0;
@@ -102,25 +106,32 @@ __device__ int block_clip(WarpPoly<C>& P, BlockAux<C>& X, BlockShared<NW>& B, Po
   }
 
   // 2. keep the inside vertices in order (:344-362)
-  double r2 = 0.0;
   int lo, hi;
   block_range<NW>(nv, w, &lo, &hi);
   {
-    int cnt = 0;
+    int cnt = 0, first = nv;
     for (int b = lo; b < hi; b += 32) {
       const int v = b + lane;
-      cnt += __popc(__ballot_sync(kFull, v < hi && P.o2n[v] != C::VNONE));
+      const unsigned km = __ballot_sync(kFull, v < hi && P.o2n[v] != C::VNONE);
+      cnt += __popc(km);
+      const unsigned rm = ~km & (hi - b >= 32 ? kFull : ((1u << (hi - b)) - 1u));
+      if (rm && first == nv) first = b + __ffs(rm) - 1;
     }
-    if (lane == 0) B.a[w] = cnt;
+    if (lane == 0) {
+      B.a[w] = cnt;
+      B.c[w] = first;
+    }
   }
   __syncthreads();
   if (tid == 0) {
-    int s = 0;
+    int s = 0, first = nv;
     for (int q = 0; q < NW; ++q) {
       B.ia[q] = s;
       s += B.a[q];
+      first = min(first, B.c[q]);
     }
     B.val[0] = s;
+    B.vfirst = first;
   }
   __syncthreads();
   const int nkept = B.val[0];
@@ -131,13 +142,6 @@ __device__ int block_clip(WarpPoly<C>& P, BlockAux<C>& X, BlockShared<NW>& B, Po
       const bool k = v < hi && P.o2n[v] != C::VNONE;
       const unsigned m = __ballot_sync(kFull, k);
       if (v < hi) P.o2n[v] = k ? (VId)(run + __popc(m & lt)) : (VId)C::VNONE;
-      if (k && with_gen) {
-        double dx = P.vx[v] - gx;
-        double dy = P.vy[v] - gy;
-        double dz = P.vz[v] - gz;
-        double d2 = dx * dx + dy * dy + dz * dz;
-        r2 = fmax(r2, d2);
-      }
       run += __popc(m);
     }
   }
@@ -278,21 +282,43 @@ __device__ int block_clip(WarpPoly<C>& P, BlockAux<C>& X, BlockShared<NW>& B, Po
   const int nvn = nkept + nnew;
   if (nnew > C::NCAP || nvn > C::VCAP) return kClipOverflow;
 
-  // 5. new vertex list: kept vertices compacted (through X), then intersections
-  for (int v = tid; v < nv; v += nt) {
-    const unsigned o = P.o2n[v];
-    if (o != C::VNONE) {
-      X.x[o] = P.vx[v];
-      X.y[o] = P.vy[v];
-      X.z[o] = P.vz[v];
+  // 5. new vertex list: kept vertices compacted in place, then intersections.
+  //    Vertices below the first removed one keep their index.  A kept vertex
+  //    only moves down (o2n[v] <= v), so in rounds of consecutive vertices,
+  //    read into registers before a barrier and written after it, no write
+  //    reaches a vertex that is still to be read.
+  {
+    constexpr int K = 1;
+    const int v0 = B.vfirst;
+    for (int base = v0; base < nv; base += K * nt) {
+      double bx[K], by[K], bz[K];
+      int bo[K];
+#pragma unroll
+      for (int j = 0; j < K; ++j) {
+        const int v = base + j * nt + tid;
+        bo[j] = -1;
+        if (v < nv) {
+          const unsigned o = P.o2n[v];
+          if (o != C::VNONE) {
+            bo[j] = (int)o;
+            bx[j] = P.vx[v];
+            by[j] = P.vy[v];
+            bz[j] = P.vz[v];
+          }
+        }
+      }
+      __syncthreads();
+#pragma unroll
+      for (int j = 0; j < K; ++j) {
+        if (bo[j] >= 0) {
+          P.vx[bo[j]] = bx[j];
+          P.vy[bo[j]] = by[j];
+          P.vz[bo[j]] = bz[j];
+        }
+      }
     }
   }
-  __syncthreads();
-  for (int o = tid; o < nkept; o += nt) {
-    P.vx[o] = X.x[o];
-    P.vy[o] = X.y[o];
-    P.vz[o] = X.z[o];
-  }
+  // (positions >= nkept were last read before the final round's barrier)
   for (int r = tid; r < nnew; r += nt) {
     P.vx[nkept + r] = P.tx[r];
     P.vy[nkept + r] = P.ty[r];
@@ -521,8 +547,8 @@ __device__ int block_clip(WarpPoly<C>& P, BlockAux<C>& X, BlockShared<NW>& B, Po
 // every warp (same data, same decisions, a staging row per warp), each clip
 // by all warps together
 template <class C, int NW>
-__device__ int compute_cell_block(const TessDesc& T, uint32_t i, WarpPoly<C>& P, BlockAux<C>& X,
-                                   BlockShared<NW>& B, PolyState& S) {
+__device__ int compute_cell_block(const TessDesc& T, uint32_t i, WarpPoly<C>& P, BlockShared<NW>& B,
+                                   PolyState& S) {
   const unsigned lane = lane_id();
   const double gx = T.gen[3 * (size_t)i], gy = T.gen[3 * (size_t)i + 1], gz = T.gen[3 * (size_t)i + 2];
   double r2;
@@ -554,7 +580,7 @@ __device__ int compute_cell_block(const TessDesc& T, uint32_t i, WarpPoly<C>& P,
         emit = wall_plane(W, gx, gy, gz, p, n);
       }
       if (emit) {
-        const int r = block_clip<C, NW>(P, X, B, S, p[0], p[1], p[2], n[0], n[1], n[2], W.id, false, gx, gy, gz, &r2);
+        const int r = block_clip<C, NW>(P, B, S, p[0], p[1], p[2], n[0], n[1], n[2], W.id, false, gx, gy, gz, &r2);
         if (r == kClipOverflow) return kCellOverflow;
       }
     }
@@ -655,7 +681,7 @@ __device__ int compute_cell_block(const TessDesc& T, uint32_t i, WarpPoly<C>& P,
         const double e1 = __shfl_sync(kFull, d1, j);
         const double e2 = __shfl_sync(kFull, d2, j);
         const double mx = gx + e0 * 0.5, my = gy + e1 * 0.5, mz = gz + e2 * 0.5;
-        const int r = block_clip<C, NW>(P, X, B, S, mx, my, mz, e0, e1, e2, jid, true, gx, gy, gz, &r2);
+        const int r = block_clip<C, NW>(P, B, S, mx, my, mz, e0, e1, e2, jid, true, gx, gy, gz, &r2);
         if (r == kClipOverflow) return kCellOverflow;
         if (r == kClipMod) cur = r2;
         else if (r == kClipEmpty) cur = 0.0;
@@ -680,13 +706,12 @@ __device__ int compute_cell_block(const TessDesc& T, uint32_t i, WarpPoly<C>& P,
 constexpr int kHugeBlockWarps = 32;
 
 // persistent blocks over the listed cells, one cell per block at a time; the
-// block's polytope and compaction buffer live in global memory
+// block's polytope lives in global memory
 template <class C, int NW>
 __global__ void __launch_bounds__(NW * 32)
-    k_clip_huge_block(const TessDesc T, const WorkList W, WarpPoly<C>* polys, BlockAux<C>* aux) {
+    k_clip_huge_block(const TessDesc T, const WorkList W, WarpPoly<C>* polys) {
   __shared__ BlockShared<NW> B;
   WarpPoly<C>& P = polys[blockIdx.x];
-  BlockAux<C>& X = aux[blockIdx.x];
   const unsigned lane = lane_id();
   const int w = (int)(threadIdx.x >> 5);
   while (true) {
@@ -697,7 +722,7 @@ __global__ void __launch_bounds__(NW * 32)
     if (idx >= W.nitems) break;
     const uint32_t cell = W.items ? W.items[idx] : (uint32_t)T.sorted[idx].id;
     PolyState S;
-    const int st = compute_cell_block<C, NW>(T, cell, P, X, B, S);
+    const int st = compute_cell_block<C, NW>(T, cell, P, B, S);
     __syncthreads();
     if (w == 0) {
       if (st == kCellOk) {
@@ -718,10 +743,9 @@ __global__ void __launch_bounds__(NW * 32)
 template <class C, int NW>
 __global__ void __launch_bounds__(NW * 32)
     k_clip_huge_block_batched(const TessDesc* descs, const uint32_t* tess_off, int ntess, const WorkList W,
-                              WarpPoly<C>* polys, BlockAux<C>* aux) {
+                              WarpPoly<C>* polys) {
   __shared__ BlockShared<NW> B;
   WarpPoly<C>& P = polys[blockIdx.x];
-  BlockAux<C>& X = aux[blockIdx.x];
   const unsigned lane = lane_id();
   const int w = (int)(threadIdx.x >> 5);
   const uint32_t nitems = W.nitems_dev ? *W.nitems_dev : W.nitems;
@@ -736,7 +760,7 @@ __global__ void __launch_bounds__(NW * 32)
     const TessDesc& T = descs[t];
     const uint32_t cell = (uint32_t)T.sorted[item].id;
     PolyState S;
-    const int st = compute_cell_block<C, NW>(T, cell, P, X, B, S);
+    const int st = compute_cell_block<C, NW>(T, cell, P, B, S);
     __syncthreads();
     if (w == 0) {
       if (st == kCellOk) {

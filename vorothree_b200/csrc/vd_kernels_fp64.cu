@@ -55,23 +55,20 @@ cudaError_t launch_clip_fp64_big(const TessDesc& T, const WorkList& W, void* scr
   return cudaGetLastError();
 }
 
-// the huge tier's scratch: per block a polytope, then (after all of them) a
-// compaction buffer
-size_t clip_huge_scratch_per_block() { return sizeof(WarpPoly<HugeCfg>) + sizeof(BlockAux<HugeCfg>); }
+// the huge tier's scratch: a polytope per block
+size_t clip_huge_scratch_per_block() { return sizeof(WarpPoly<HugeCfg>); }
 
 cudaError_t launch_clip_fp64_huge(const TessDesc& T, const WorkList& W, void* scratch, int nblocks, cudaStream_t s) {
   WarpPoly<HugeCfg>* polys = reinterpret_cast<WarpPoly<HugeCfg>*>(scratch);
-  BlockAux<HugeCfg>* aux = reinterpret_cast<BlockAux<HugeCfg>*>(polys + nblocks);
-  k_clip_huge_block<HugeCfg, kHugeBlockWarps><<<nblocks, kHugeBlockWarps * 32, 0, s>>>(T, W, polys, aux);
+  k_clip_huge_block<HugeCfg, kHugeBlockWarps><<<nblocks, kHugeBlockWarps * 32, 0, s>>>(T, W, polys);
   return cudaGetLastError();
 }
 
 cudaError_t launch_clip_fp64_huge_batched(const TessDesc* descs, const uint32_t* tess_off, int ntess,
                                           const WorkList& W, void* scratch, int nblocks, cudaStream_t s) {
   WarpPoly<HugeCfg>* polys = reinterpret_cast<WarpPoly<HugeCfg>*>(scratch);
-  BlockAux<HugeCfg>* aux = reinterpret_cast<BlockAux<HugeCfg>*>(polys + nblocks);
   k_clip_huge_block_batched<HugeCfg, kHugeBlockWarps>
-      <<<nblocks, kHugeBlockWarps * 32, 0, s>>>(descs, tess_off, ntess, W, polys, aux);
+      <<<nblocks, kHugeBlockWarps * 32, 0, s>>>(descs, tess_off, ntess, W, polys);
   return cudaGetLastError();
 }
 

@@ -75,7 +75,7 @@ __device__ int seal_clips(const TessDesc& T, const SealArgs& A, uint32_t i, Warp
 
 // seal_clips by a whole block (the huge tier, vd_clip_block.cuh); thread 0 logs
 template <class C, int NW>
-__device__ int seal_clips_block(const TessDesc& T, const SealArgs& A, uint32_t i, WarpPoly<C>& P, BlockAux<C>& X,
+__device__ int seal_clips_block(const TessDesc& T, const SealArgs& A, uint32_t i, WarpPoly<C>& P,
                                 BlockShared<NW>& B, PolyState& S, bool log, int* nlog) {
   *nlog = 0;
   const uint32_t mi = A.s_mask[i];
@@ -100,7 +100,7 @@ __device__ int seal_clips_block(const TessDesc& T, const SealArgs& A, uint32_t i
       dot += (gz - p[2]) * n[2];
       if (!(dot <= 1e-9)) continue;
       double r2;
-      const int r = block_clip<C, NW>(P, X, B, S, p[0], p[1], p[2], n[0], n[1], n[2], T.walls[k].id, false, gx, gy, gz, &r2);
+      const int r = block_clip<C, NW>(P, B, S, p[0], p[1], p[2], n[0], n[1], n[2], T.walls[k].id, false, gx, gy, gz, &r2);
       if (r == kClipOverflow) return kCellOverflow;
       if (r != kClipNoop) {
         if (log && threadIdx.x == 0) {
@@ -220,10 +220,9 @@ __device__ void seal_worker(const TessDesc& T, const WorkList& W, const SealArgs
 // the seal / prune pass's huge tier: a thread block per cell
 template <class C, int NW>
 __global__ void __launch_bounds__(NW * 32)
-    k_seal_block(const TessDesc T, const WorkList W, const SealArgs A, WarpPoly<C>* polys, BlockAux<C>* aux) {
+    k_seal_block(const TessDesc T, const WorkList W, const SealArgs A, WarpPoly<C>* polys) {
   __shared__ BlockShared<NW> B;
   WarpPoly<C>& P = polys[blockIdx.x];
-  BlockAux<C>& X = aux[blockIdx.x];
   const unsigned lane = lane_id();
   const int w = (int)(threadIdx.x >> 5);
   while (true) {
@@ -234,10 +233,10 @@ __global__ void __launch_bounds__(NW * 32)
     if (idx >= W.nitems) break;
     const uint32_t cell = W.items[idx];
     PolyState S;
-    int st = compute_cell_block<C, NW>(T, cell, P, X, B, S);
+    int st = compute_cell_block<C, NW>(T, cell, P, B, S);
     int nlog = 0;
     if (st == kCellOk && (A.mode == 1 || A.sealed))
-      st = seal_clips_block<C, NW>(T, A, cell, P, X, B, S, A.mode == 1, &nlog);
+      st = seal_clips_block<C, NW>(T, A, cell, P, B, S, A.mode == 1, &nlog);
     __syncthreads();
     if (w == 0) {
       if (st == kCellOk) {
@@ -346,8 +345,7 @@ cudaError_t launch_seal_big(const TessDesc& T, const WorkList& W, const SealArgs
 cudaError_t launch_seal_block(const TessDesc& T, const WorkList& W, const SealArgs& A, void* scratch, int nblocks,
                               cudaStream_t s) {
   WarpPoly<HugeCfg>* polys = reinterpret_cast<WarpPoly<HugeCfg>*>(scratch);
-  BlockAux<HugeCfg>* aux = reinterpret_cast<BlockAux<HugeCfg>*>(polys + nblocks);
-  k_seal_block<HugeCfg, kHugeBlockWarps><<<nblocks, kHugeBlockWarps * 32, 0, s>>>(T, W, A, polys, aux);
+  k_seal_block<HugeCfg, kHugeBlockWarps><<<nblocks, kHugeBlockWarps * 32, 0, s>>>(T, W, A, polys);
   return cudaGetLastError();
 }
 
