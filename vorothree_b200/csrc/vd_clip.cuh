@@ -508,33 +508,42 @@ __device__ int warp_clip(WarpPoly<C>& P, PolyState& S, double px, double py, dou
   if (__any_sync(kFull, longface) || hk > C::HCAP) return kClipOverflow;
   __syncwarp();
 
-  // 7. write the surviving faces' entries, and collect the lid segments.  In
-  //    a face buffer two intersection entries are adjacent exactly when an
-  //    in->out position is followed (after out->out positions) by an out->in
-  //    one; the reference records (v, u) = (X of the out->in, X of the
-  //    in->out), ordered by u's place in the buffer, i.e. by position.
-  int nseg = 0;
-  for (int b = 0; b < nh; b += 32) {
-    const int p = b + lane;
-    bool segsrc = false;
-    if (p < nh) {
-      const int f = P.pf[cb][p];
+  // 7. write the surviving faces' entries
+  for (int p = lane; p < nh; p += 32) {
+    const int f = P.pf[cb][p];
+    const unsigned fw = P.fnew[f];
+    if (fw != C::FNONE) {
       const VPair<VId> ve = P.pve[p];
       const unsigned os = ve.s, oe = ve.e;
       const bool si = os != C::VNONE, ei = oe != C::VNONE;
-      const unsigned fw = P.fnew[f];
-      if (fw != C::FNONE) {
-        const int o = (int)P.fdel[f] + (int)P.E[p];
-        if (si) {
-          P.fi[nb][o] = (VId)(ei ? oe : (unsigned)P.cid[P.cidx[p]]);
-          P.pf[nb][o] = (FId)fw;
-          segsrc = !ei;
-        } else if (ei) {
-          P.fi[nb][o] = P.cid[P.cidx[p]];
-          P.pf[nb][o] = (FId)fw;
-          P.fi[nb][o + 1] = (VId)oe;
-          P.pf[nb][o + 1] = (FId)fw;
-        }
+      const int o = (int)P.fdel[f] + (int)P.E[p];
+      if (si) {
+        P.fi[nb][o] = (VId)(ei ? oe : (unsigned)P.cid[P.cidx[p]]);
+        P.pf[nb][o] = (FId)fw;
+      } else if (ei) {
+        P.fi[nb][o] = P.cid[P.cidx[p]];
+        P.pf[nb][o] = (FId)fw;
+        P.fi[nb][o + 1] = (VId)oe;
+        P.pf[nb][o + 1] = (FId)fw;
+      }
+    }
+  }
+  //    and collect the lid segments.  In a face buffer two intersection
+  //    entries are adjacent exactly when an in->out position is followed
+  //    (after out->out positions) by an out->in one; the reference records
+  //    (v, u) = (X of the out->in, X of the in->out), ordered by u's place in
+  //    the buffer, i.e. by position -- the order of the crossing list
+  int nseg = 0;
+  for (int b = 0; b < ncross; b += 32) {
+    const int kc = b + (int)lane;
+    bool segsrc = false;
+    int f = 0;
+    if (kc < ncross) {
+      const int p = P.cpos[kc];
+      const VPair<VId> ve = P.pve[p];
+      if (ve.s != C::VNONE && ve.e == C::VNONE) {
+        f = P.pf[cb][p];
+        segsrc = P.fnew[f] != C::FNONE;
       }
     }
     const unsigned sm = __ballot_sync(kFull, segsrc);
@@ -545,8 +554,6 @@ __device__ int warp_clip(WarpPoly<C>& P, PolyState& S, double px, double py, dou
         // crossing along the face (the positions between are out->out):
         // the next crossing in walk order if it lies in the same face, else
         // the face's first crossing
-        const int f = P.pf[cb][p];
-        const int kc = P.cidx[p];
         int kn = kc + 1;
         if (kn >= ncross || (int)P.cpos[kn] >= (int)P.fs[cb][f + 1]) kn = P.fcr[f];
         P.sega[k] = P.cid[kn];
