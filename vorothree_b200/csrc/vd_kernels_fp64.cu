@@ -60,7 +60,10 @@ size_t clip_huge_scratch_per_block() { return sizeof(WarpPoly<HugeCfg>); }
 
 cudaError_t launch_clip_fp64_huge(const TessDesc& T, const WorkList& W, void* scratch, int nblocks, cudaStream_t s) {
   WarpPoly<HugeCfg>* polys = reinterpret_cast<WarpPoly<HugeCfg>*>(scratch);
-  k_clip_huge_block<HugeCfg, kHugeBlockWarps><<<nblocks, kHugeBlockWarps * 32, 0, s>>>(T, W, polys);
+  if (T.ncells <= kHugeNarrowMaxCells)
+    k_clip_huge_block<HugeCfg, kHugeBlockWarpsNarrow><<<nblocks, kHugeBlockWarpsNarrow * 32, 0, s>>>(T, W, polys);
+  else
+    k_clip_huge_block<HugeCfg, kHugeBlockWarps><<<nblocks, kHugeBlockWarps * 32, 0, s>>>(T, W, polys);
   return cudaGetLastError();
 }
 
