@@ -447,15 +447,17 @@ def test_degenerate_duplicates_and_planes(oracle_mod, precision):
     assert_same(g, o, sample_cells=16)
 
 
+@pytest.mark.parametrize("n", [1000, 3000])
 @pytest.mark.parametrize("precision", PRECISIONS)
 @pytest.mark.parametrize("kind", ["axes", "central", "sphere"])
-def test_bench_distributions_bitwise(oracle_mod, kind, precision):
+def test_bench_distributions_bitwise(oracle_mod, kind, precision, n):
     """The distributions of the reference's criterion benches
     (benches/distributions.rs) on their box and bin heuristic (ceil(N^(1/3))
     bins per axis): generators crowding three mid-planes, a dense central box
-    with an empty shell, and generators on a sphere (needle-shaped cells)."""
+    with an empty shell, and generators on a sphere (needle-shaped cells).
+    The sphere's centre cell takes the block tier: 16-warp blocks at 1,000
+    generators, 32-warp blocks at 3,000."""
     from common import bench_distribution
-    n = 3000
     pts = bench_distribution(kind, n, 70 + len(kind))
     g = int(np.ceil(n ** (1.0 / 3.0)))
     gt = gpu_tess([0, 0, 0], [100, 100, 100], (g, g, g), pts, precision=precision)
