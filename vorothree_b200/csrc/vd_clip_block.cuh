@@ -22,12 +22,10 @@ namespace vd {
 template <int NW>
 struct BlockShared {
   int a[NW], b[NW], c[NW];     // per-range totals of a pass
-  int ia[NW], ib[NW], ic[NW];  // their exclusive scans (ic: last crossing before the range)
   int val[8];                  // block-wide results
   double r2[NW];
   uint8_t cand[NW][32];        // the walk's candidate staging, a row per warp
   unsigned idx;
-  int vfirst;                  // a clip's first removed vertex
 };
 
 // warp w's contiguous share [lo, hi) of [0, n), whole chunks of 32
@@ -39,23 +37,31 @@ __device__ __forceinline__ void block_range(int n, int w, int* lo, int* hi) {
   *hi = min(n, (w + 1) * per * 32);
 }
 
-// thread 0: exclusive sums of a[] and b[] into ia[] and ib[], the running
-// maximum of c[] before each range into ic[], totals into val[s0], val[s1]
+// every warp reads the NW range totals after the barrier that follows their
+// writes and derives its own prefixes: exclusive sums of a[] and b[] before
+// range w, the running maximum of c[] before it (-1 for none), and the
+// totals (sums of a[] and b[], maximum of c[]) -- no second barrier.  The
+// totals are rewritten only after the barrier that ends the pass using them.
 template <int NW>
-__device__ __forceinline__ void block_scan_totals(BlockShared<NW>& B, int s0, int s1) {
-  if (threadIdx.x == 0) {
-    int sa = 0, sb = 0, mc = -1;
-    for (int w = 0; w < NW; ++w) {
-      B.ia[w] = sa;
-      B.ib[w] = sb;
-      B.ic[w] = mc;
-      sa += B.a[w];
-      sb += B.b[w];
-      mc = max(mc, B.c[w]);
-    }
-    if (s0 >= 0) B.val[s0] = sa;
-    if (s1 >= 0) B.val[s1] = sb;
+__device__ __forceinline__ void range_prefix(const BlockShared<NW>& B, int w, int* pa, int* pb, int* pc, int* ta,
+                                             int* tb, int* tc) {
+  static_assert(NW <= 32, "one range total per lane");
+  const unsigned lane = lane_id();
+  const bool in = (int)lane < NW;
+  const int a = in ? B.a[lane] : 0, b = in ? B.b[lane] : 0, c = in ? B.c[lane] : -1;
+  const int sa = warp_incl_scan(a), sb = warp_incl_scan(b);
+  int mc = c;
+  for (int d = 1; d < 32; d <<= 1) {
+    const int o = __shfl_up_sync(kFull, mc, d);
+    if ((int)lane >= d) mc = max(mc, o);
   }
+  const int mprev = __shfl_up_sync(kFull, mc, 1);
+  *pa = __shfl_sync(kFull, sa - a, w);
+  *pb = __shfl_sync(kFull, sb - b, w);
+  *pc = __shfl_sync(kFull, lane == 0 ? -1 : mprev, w);
+  *ta = __shfl_sync(kFull, sa, 31);
+  *tb = __shfl_sync(kFull, sb, 31);
+  *tc = __shfl_sync(kFull, mc, 31);
 }
 
 // clip_with_scratch (cell_3d_faces.rs:288-503) by the whole block; every
@@ -123,20 +129,17 @@ __device__ int block_clip(WarpPoly<C>& P, BlockShared<NW>& B, PolyState& S, doub
     }
   }
   __syncthreads();
-  if (tid == 0) {
-    int s = 0, first = nv;
-    for (int q = 0; q < NW; ++q) {
-      B.ia[q] = s;
-      s += B.a[q];
-      first = min(first, B.c[q]);
-    }
-    B.val[0] = s;
-    B.vfirst = first;
-  }
-  __syncthreads();
-  const int nkept = B.val[0];
+  int nkept, run0, vfirst;
   {
-    int run = B.ia[w];
+    const bool in = (int)lane < NW;
+    const int a = in ? B.a[lane] : 0;
+    const int sa = warp_incl_scan(a);
+    run0 = __shfl_sync(kFull, sa - a, w);
+    nkept = __shfl_sync(kFull, sa, 31);
+    vfirst = __reduce_min_sync(kFull, in ? B.c[lane] : nv);
+  }
+  {
+    int run = run0;
     for (int b = lo; b < hi; b += 32) {
       const int v = b + lane;
       const bool k = v < hi && P.o2n[v] != C::VNONE;
@@ -182,11 +185,10 @@ __device__ int block_clip(WarpPoly<C>& P, BlockShared<NW>& B, PolyState& S, doub
     }
   }
   __syncthreads();
-  block_scan_totals<NW>(B, 1, 2);
-  __syncthreads();
-  const int ncross = B.val[1];
+  int ncross, emitted;
   {
-    int nc = B.ia[w], run = B.ib[w], lastcross = B.ic[w];
+    int nc, run, lastcross, unused;
+    range_prefix<NW>(B, w, &nc, &run, &lastcross, &ncross, &emitted, &unused);
     for (int b = lo; b < hi; b += 32) {
       const int p = b + lane;
       bool cr = false, si = false, ei = false;
@@ -219,7 +221,7 @@ __device__ int block_clip(WarpPoly<C>& P, BlockShared<NW>& B, PolyState& S, doub
       if (p < hi) P.E[p] = (typename C::Pos)(run + __popc(m1 & lt) + 2 * __popc(m2 & lt));
       run += __popc(m1) + 2 * __popc(m2);
     }
-    if (tid == 0) P.E[nh] = (typename C::Pos)B.val[2];
+    if (tid == 0) P.E[nh] = (typename C::Pos)emitted;
   }
   __syncthreads();
   if (ncross > C::CCAP) return kClipOverflow;
@@ -289,7 +291,7 @@ __device__ int block_clip(WarpPoly<C>& P, BlockShared<NW>& B, PolyState& S, doub
   //    reaches a vertex that is still to be read.
   {
     constexpr int K = 1;
-    const int v0 = B.vfirst;
+    const int v0 = vfirst;
     for (int base = v0; base < nv; base += K * nt) {
       double bx[K], by[K], bz[K];
       int bo[K];
@@ -345,12 +347,14 @@ __device__ int block_clip(WarpPoly<C>& P, BlockShared<NW>& B, PolyState& S, doub
     }
   }
   __syncthreads();
-  block_scan_totals<NW>(B, 4, 5);
-  __syncthreads();
-  const int nfk = B.val[4], hk = B.val[5];
-  const bool longface = B.ic[NW - 1] > 0 || B.c[NW - 1] > 0;
+  int nfk, hk, lmax;
+  int nfr, hr;
   {
-    int nfr = B.ia[w], hr = B.ib[w];
+    int unused;
+    range_prefix<NW>(B, w, &nfr, &hr, &unused, &nfk, &hk, &lmax);
+  }
+  const bool longface = lmax > 0;
+  {
     for (int b = lo; b < hi; b += 32) {
       const int f = b + lane;
       int L = 0;
