@@ -61,8 +61,8 @@ def flop_count(cnt: dict) -> int:
 
 
 def uniform(n, seed):
-    rng = np.random.Generator(np.random.PCG64(seed))
-    return rng.uniform(0.0, 1.0, size=(n, 3))
+    from vorothree_b200.workloads import uniform_cube
+    return uniform_cube(n, seed)
 
 
 class ClockSampler:
@@ -140,22 +140,21 @@ def load_traffic(precision: str):
     return load_profile(precision).get("dram_bytes_per_launch")
 
 
-def cpu_baseline(pts, nthreads: int, sample: int, extras: dict = None):
+def cpu_baseline(pts, nthreads: int, sample: int, extras: dict = None, keep: list = None):
     """The oracle (a C restatement of the reference's calculate) on the host
     cores over a bounded sample of the same tessellation's cells.  `extras`,
     when given, gets the search-order table build (the Algorithm3DGrid::new
     constructor, outside calculate) and a one-thread rate over a smaller
-    sample."""
+    sample.  `keep`, when given, receives the oracle tessellation if the
+    sample is every cell (the parity check compares against it)."""
     from oracle.oracle import OracleTessellation
     t0 = time.perf_counter()
     t = OracleTessellation([0, 0, 0], [1, 1, 1], GRID, GRID, GRID)
     build = time.perf_counter() - t0
     t.set_generators(pts)
-    begin = (len(pts) - sample) // 2
-    t0 = time.perf_counter()
-    t.calculate_range(begin, begin + sample, nthreads)
-    dt = time.perf_counter() - t0
     if extras is not None:
+        # one thread first: the timed run below is the last calculate, so the
+        # oracle then holds every cell of the sample
         one = min(sample, 65536)
         b1 = (len(pts) - one) // 2
         t1 = time.perf_counter()
@@ -163,7 +162,35 @@ def cpu_baseline(pts, nthreads: int, sample: int, extras: dict = None):
         d1 = time.perf_counter() - t1
         extras.update({"one_thread_value": one / d1, "one_thread_sample": f"{one} cells ({d1:.2f} s)",
                        "search_order_build_s": build})
+    begin = (len(pts) - sample) // 2
+    t0 = time.perf_counter()
+    t.calculate_range(begin, begin + sample, nthreads)
+    dt = time.perf_counter() - t0
+    if keep is not None and sample == len(pts):
+        keep.append(t)
     return sample / dt, dt
+
+
+def parity_leg(tess, step, oracle, precisions) -> dict:
+    """Every cell of the benchmark tessellation against the oracle's, bit for
+    bit, in each precision: volumes, centroids, face counts, neighbour ids in
+    face order and face areas."""
+    ov, oc, on = oracle.summaries()
+    ooff, oids = oracle.neighbors()
+    _, oar = oracle.face_areas()
+    out = {"cells": int(len(ov)), "compared": "volume, centroid, face count, neighbour ids, face areas",
+           "checker": "oracle (C restatement of the reference's calculate), every cell"}
+    for p in precisions:
+        tess.set_precision(p)
+        step()
+        gv, gc, gn = tess.summaries()
+        goff, gids = tess.neighbors()
+        _, gar = tess.face_areas()
+        bad = (gv != ov) | (gn != on) | np.any(gc != oc, axis=1)
+        ok_csr = np.array_equal(goff, ooff) and np.array_equal(gids, oids) and np.array_equal(gar, oar)
+        out[p] = {"bitwise_equal": bool(not bad.any() and ok_csr), "mismatched_cells": int(bad.sum()),
+                  "neighbour_csr_equal": bool(ok_csr)}
+    return out
 
 
 def run_reference(args):
@@ -464,10 +491,21 @@ def run_ours(args):
             nthreads = os.cpu_count() or 1
             sample = min(args.cpu_sample or N_GEN, N_GEN)
             extras = {}
-            cv, cdt = cpu_baseline(pts, nthreads, sample, extras)
+            keep = []
+            cv, cdt = cpu_baseline(pts, nthreads, sample, extras, keep)
             line["cpu_baseline"] = dict({"value": cv, "unit": "cells/s", "cores": nthreads, "kind": "port",
                                          "sample": f"{sample} of {N_GEN} cells of the same tessellation "
                                                    f"({cdt:.2f} s wall)"}, **extras)
+            if keep:
+                line["parity"] = parity_leg(tess, step, keep[0], ["fp64", "mixed"])
+                tess.set_precision(args.precision)
+                del keep[:]
+        if ws == 1 and not args.no_side_configs:
+            # the other benchmark configurations, each in its own key: the
+            # clustered input, the batch with Lloyd steps, the serving sweep
+            line["clustered"] = blobs_leg(args, 4_194_304, args.precision, 3)
+            line["batched"] = batched_leg(args, args.ntess, 3, args.lloyd_steps)
+            line["serving_sweep"] = serving_leg(args, args.serve_requests, args.serve_rates)
         print(json.dumps(line), flush=True)
     tess.close()
     if ws > 1:
@@ -477,22 +515,8 @@ def run_ours(args):
 
 
 def batched_members(ntess: int, seed: int = 0):
-    """4096 tessellations (configurable), N log-uniform in [64, 65536], box
-    edges U[1,10], even members with a centred sphere wall of radius
-    0.5*min(edge); near-cubic bins at the autotuner's density for uniform
-    input of the member's size."""
-    from vorothree_b200 import autotune
-    rng = np.random.Generator(np.random.PCG64(seed))
-    out = []
-    for k in range(ntess):
-        n = int(round(np.exp(rng.uniform(np.log(64), np.log(65536)))))
-        edge = rng.uniform(1.0, 10.0, size=3)
-        # bin density from the autotuner's table for uniform input of this size
-        grid = list(autotune.grid_for(n, bounds_of(edge), autotune.lookup("uniform", n)))
-        pts = rng.uniform(0.0, 1.0, size=(n, 3)) * edge
-        sphere = (list(edge / 2.0), 0.5 * float(edge.min())) if k % 2 == 0 else None
-        out.append((edge, grid, pts, sphere))
-    return out
+    from vorothree_b200.workloads import batch_members
+    return batch_members(ntess, seed)
 
 
 def bounds_of(edge):
@@ -500,14 +524,12 @@ def bounds_of(edge):
     return v.BoundingBox([0, 0, 0], list(edge))
 
 
-def run_batched(args):
+def batched_leg(args, ntess: int, calc_steps: int, lloyd_steps: int) -> dict:
     """Config: many independent tessellations in one persistent launch, then
     Lloyd steps (relax -> calculate) replayed from a CUDA graph."""
-    import torch
     import vorothree_b200 as v
-    torch.cuda.set_device(0)
     t0 = time.perf_counter()
-    ms = batched_members(args.ntess)
+    ms = batched_members(ntess)
     b = v.TessellationBatch()
     b.set_precision(args.precision)
     for edge, grid, pts, sphere in ms:
@@ -518,62 +540,43 @@ def run_batched(args):
     n_in = sum(len(m[2]) for m in ms)
     cells = b.total_cells()
     calc = []
-    for _ in range(args.warmup + args.steps):
+    for _ in range(1 + calc_steps):
         b.calculate()
         calc.append(b.timing_ms())
-    calc_ms = statistics.mean(calc[args.warmup:])
+    calc_ms = statistics.mean(calc[1:])
     b.lloyd(1)  # captures the step graph
-    b.lloyd(args.lloyd_steps)
+    b.lloyd(lloyd_steps)
     lloyd_ms = b.timing_ms()
     cells_after = b.total_cells()
-    line = {
-        "metric": "3D cells/s, batched tessellations", "workload": "batched", "unit": "cells/s",
-        "value": cells / (calc_ms / 1e3), "ms_per_calculate": calc_ms, "n_gpus": 1,
-        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "dtype": "f64",
-        "precision": args.precision, "data": "synthetic (seeded PCG64)",
-        "config": {"tessellations": args.ntess, "generators_in": n_in, "cells": cells,
-                   "sizes": "log-uniform [64, 65536]", "box_edges": "U[1,10]",
-                   "walls": "even members: centred sphere r = 0.5 min(edge)",
-                   "grid": "bins per axis ~ edge * (N/V)^(1/3)"},
-        "lloyd": {"steps": args.lloyd_steps, "ms_total": lloyd_ms, "ms_per_step": lloyd_ms / args.lloyd_steps,
-                  "cells_per_s": cells_after * args.lloyd_steps / (lloyd_ms / 1e3),
-                  "cells_after": cells_after, "note": "each step = relax + wall filter + re-bin + calculate, "
-                  "replayed from one CUDA graph"},
-        "setup_s": setup_s,
-    }
+    b.close()
+    return {"value": cells / (calc_ms / 1e3), "unit": "cells/s", "ms_per_calculate": calc_ms,
+            "calculates_timed": calc_steps,
+            "config": {"tessellations": ntess, "generators_in": n_in, "cells": cells,
+                       "sizes": "log-uniform [64, 65536]", "box_edges": "U[1,10]",
+                       "walls": "even members: centred sphere r = 0.5 min(edge)",
+                       "grid": "bins per axis ~ edge * (N/V)^(1/3) at the autotuner's density"},
+            "lloyd": {"steps": lloyd_steps, "ms_total": lloyd_ms, "ms_per_step": lloyd_ms / lloyd_steps,
+                      "cells_per_s": cells_after * lloyd_steps / (lloyd_ms / 1e3),
+                      "cells_after": cells_after, "note": "each step = relax + wall filter + re-bin + calculate, "
+                      "replayed from one CUDA graph"},
+            "setup_s": setup_s, "timing": "CUDA events on the batch's stream (device time)"}
+
+
+def run_batched(args):
+    import torch
+    torch.cuda.set_device(0)
+    res = batched_leg(args, args.ntess, args.steps, args.lloyd_steps)
+    line = {"metric": "3D cells/s, batched tessellations", "workload": "batched", "unit": "cells/s",
+            "value": res["value"], "n_gpus": 1, "steps": args.steps, "warmup": 1, "higher_is_better": True,
+            "dtype": "f64", "precision": args.precision, "data": "synthetic (seeded PCG64)"}
+    line.update(res)
     print(json.dumps(line), flush=True)
     return 0
 
 
 def serving_requests(count: int, seed: int = 0):
-    """Requests of the serving workload: sizes log-uniform in [1e3, 1e6];
-    half uniform, half clustered (8 Gaussian blobs, sigma 0.03, 70% of the
-    points); 0-2 walls drawn from {plane through the centre with a random
-    normal, centred sphere of radius U[0.3, 0.5]}; grid from the autotuner."""
-    import vorothree_b200 as v
-    from vorothree_b200 import autotune
-    bounds = v.BoundingBox([0, 0, 0], [1, 1, 1])
-    rng = np.random.Generator(np.random.PCG64(seed))
-    out = []
-    for k in range(count):
-        n = int(round(np.exp(rng.uniform(np.log(1e3), np.log(1e6)))))
-        clustered = rng.uniform() < 0.5
-        if clustered:
-            nb = int(0.7 * n)
-            c = rng.uniform(0.1, 0.9, size=(8, 3))
-            pts = np.concatenate([c[np.arange(nb) % 8] + rng.normal(0.0, 0.03, size=(nb, 3)),
-                                  rng.uniform(0.0, 1.0, size=(n - nb, 3))])
-        else:
-            pts = rng.uniform(0.0, 1.0, size=(n, 3))
-        grid = autotune.choose_grid(pts, bounds)
-        walls = []
-        for w in range(int(rng.integers(0, 3))):
-            if rng.uniform() < 0.5:
-                walls.append(v.Wall(v.WALL_ID_MAX - w, v.PlaneGeometry([0.5, 0.5, 0.5], list(rng.normal(size=3)))))
-            else:
-                walls.append(v.Wall(v.WALL_ID_MAX - w, v.SphereGeometry([0.5, 0.5, 0.5], float(rng.uniform(0.3, 0.5)))))
-        out.append((bounds, grid, pts, walls))
-    return out
+    from vorothree_b200.workloads import serving_requests as make
+    return make(count, seed)
 
 
 def serve_at_rate(srv, reqs, rate: float, seed: int = 1):
@@ -611,24 +614,29 @@ def serve_at_rate(srv, reqs, rate: float, seed: int = 1):
             "cells": cells, "cells_per_s": cells / wall, "wall_s": wall, "peak_admitted_bytes": st["peak_bytes"]}
 
 
-def run_serving(args):
-    import torch
+def serving_leg(args, nreq: int, rates) -> dict:
     import vorothree_b200 as v
-    torch.cuda.set_device(0)
-    reqs = serving_requests(args.serve_requests)
+    reqs = serving_requests(nreq)
     srv = v.TessellationServer(slots=args.serve_slots, hbm_budget_bytes=args.serve_budget_gb << 30,
                                precision=args.precision)
     for r in reqs[:4]:  # warm the slots' buffers
         srv.take(srv.submit(*r))
-    sweep = [serve_at_rate(srv, reqs, rate) for rate in args.serve_rates]
+    sweep = [serve_at_rate(srv, reqs, rate) for rate in rates]
     srv.close()
-    line = {"metric": "serve p50/p99 latency", "workload": "serving", "unit": "ms", "n_gpus": 1,
-            "higher_is_better": False, "value": sweep[0]["p99_ms"], "precision": args.precision,
-            "data": "synthetic (seeded PCG64)",
-            "config": {"slots": args.serve_slots, "hbm_budget_gb": args.serve_budget_gb,
+    return {"config": {"slots": args.serve_slots, "hbm_budget_gb": args.serve_budget_gb, "requests": nreq,
                        "sizes": "log-uniform [1e3, 1e6]", "mix": "half uniform, half 8-blob clustered",
                        "walls": "0-2 of plane / centred sphere", "arrivals": "Poisson"},
-            "sweep": sweep}
+            "sweep": sweep, "latency": "submit-to-result wall clock per request"}
+
+
+def run_serving(args):
+    import torch
+    torch.cuda.set_device(0)
+    res = serving_leg(args, args.serve_requests, args.serve_rates)
+    line = {"metric": "serve p50/p99 latency", "workload": "serving", "unit": "ms", "n_gpus": 1,
+            "higher_is_better": False, "value": res["sweep"][0]["p99_ms"], "precision": args.precision,
+            "data": "synthetic (seeded PCG64)"}
+    line.update(res)
     print(json.dumps(line), flush=True)
     return 0
 
@@ -730,49 +738,53 @@ def run_suite(args):
     return 0
 
 
-def run_blobs(args):
-    """Config: 4,194,304 generators (--blob-n), 70% in 64 isotropic Gaussian blobs
+def blobs_leg(args, n: int, precision: str, steps: int, extra_grids=()) -> dict:
+    """Config: n generators (4,194,304), 70% in 64 isotropic Gaussian blobs
     (sigma 0.01, centres uniform) + 30% uniform background, clipped by a
-    sphere wall r = 0.45 at the centre of the unit cube."""
-    import torch
+    sphere wall r = 0.45 at the centre of the unit cube, on the autotuner's
+    grid.  A step is calculate() on the resident, binned generators."""
     import vorothree_b200 as v
-    torch.cuda.set_device(0)
-    n = args.blob_n
-    rng = np.random.Generator(np.random.PCG64(0))
-    nb = int(round(0.7 * n))
-    centres = rng.uniform(0.0, 1.0, size=(64, 3))
-    pts = np.concatenate([centres[np.arange(nb) % 64] + rng.normal(0.0, 0.01, size=(nb, 3)),
-                          rng.uniform(0.0, 1.0, size=(n - nb, 3))])
     from vorothree_b200 import autotune
+    from vorothree_b200.workloads import clustered_blobs
+    pts, nb = clustered_blobs(n, 0)
     bounds = v.BoundingBox([0, 0, 0], [1, 1, 1])
     tuned = autotune.choose_grid(pts, bounds)
-    grids = [tuned] + [(g, g, g) for g in args.blob_grids if (g, g, g) != tuned]
+    grids = [tuned] + [(g, g, g) for g in extra_grids if (g, g, g) != tuned]
     res = []
     for g in grids:
         t = v.Tessellation(bounds, v.Algorithm3DGrid(*g))
-        t.set_precision(args.precision)
+        t.set_precision(precision)
         t.add_wall(v.Wall(v.WALL_ID_MAX, v.SphereGeometry([0.5, 0.5, 0.5], 0.45)))
         kept = t.set_generators(pts)
         times, fall = [], []
-        for _ in range(args.warmup + args.steps):
+        for _ in range(3 + steps):
             t.calculate()
             tm = t.timings()
             times.append(tm["clip_ms"] + tm["fallback_ms"])
             fall.append(tm["fallback_ms"])
-        ms = statistics.mean(times[args.warmup:])
+        ms = statistics.mean(times[3:])
         res.append({"grid": list(g), "kept": kept, "ms": ms, "cells_per_s": kept / (ms / 1e3),
-                    "fallback_cells": t.fallback_counts(), "fallback_ms": statistics.mean(fall[args.warmup:])})
+                    "fallback_cells": t.fallback_counts(), "fallback_ms": statistics.mean(fall[3:])})
         if g == tuned:
             res[-1]["classes"] = blob_classes(t, pts, nb, kept, args)
         t.close()
-    line = {"metric": "3D cells/s, clustered generators", "workload": "blobs", "unit": "cells/s",
-            "value": res[0]["cells_per_s"], "n_gpus": 1, "higher_is_better": True, "dtype": "f64",
-            "precision": args.precision, "data": "synthetic (seeded PCG64)",
+    return {"value": res[0]["cells_per_s"], "unit": "cells/s", "precision": precision,
             "config": {"generators": n, "blobs": 64, "sigma": 0.01, "blob_fraction": 0.7,
                        "wall": "sphere r=0.45 at (0.5,0.5,0.5)", "grid": list(tuned),
                        "grid_source": "autotuner table (vorothree_b200/autotune_table.json)",
                        "distribution_class": autotune.distribution_class(pts, bounds)},
+            "timing": "CUDA events on the tessellation's stream (clip passes incl. fallback tiers)",
             "per_grid": res}
+
+
+def run_blobs(args):
+    import torch
+    torch.cuda.set_device(0)
+    res = blobs_leg(args, args.blob_n, args.precision, args.steps, args.blob_grids)
+    line = {"metric": "3D cells/s, clustered generators", "workload": "blobs", "unit": "cells/s",
+            "value": res["value"], "n_gpus": 1, "higher_is_better": True, "dtype": "f64",
+            "data": "synthetic (seeded PCG64)"}
+    line.update(res)
     print(json.dumps(line), flush=True)
     return 0
 
@@ -861,6 +873,8 @@ def main():
     ap.add_argument("--ref-sample", type=int, default=0,
                     help="cells per step of the reference arm (0 = every cell of the workload)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-side-configs", action="store_true",
+                    help="skip the clustered, batched and serving-sweep keys of the default line")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--n", type=int, default=N_GEN, help="generators (profiling runs use a smaller case)")
     ap.add_argument("--grid", type=int, default=GRID)

@@ -373,11 +373,16 @@ int vd_server_reset_stats(vd_server* s);
  * holds until exit.  Limits: n <= 8192 generators and a grid whose complete
  * search order fits, (2nx+1)(2ny+1)(2nz+1) <= 68921 (e.g. 20x20x20); larger
  * requests return VD_EINVAL (message via vd_last_error(NULL)).  No walls.
+ * Cells are built with at most 2048 vertices and 512 faces each: a cell
+ * beyond that (e.g. the centre of generators on a sphere, adjacent to
+ * thousands of others), which the regular entry points build in their
+ * block-per-cell tier, makes the call return VD_EOVERFLOW.
  * Calls share the array: calls that overlap on the GPU race, so order them
  * (e.g. on one stream).  The first call on a device resolves the array's
- * device address; make it before any stream capture.  stream may be NULL
- * (the default stream).  Results equal vd_tess_set_generators_device +
- * vd_tess_calculate bit for bit. */
+ * device address; make that first call before any stream capture begins.
+ * Each call waits for its work on `stream` to finish before it returns.
+ * stream may be NULL (the default stream).  Every result equals
+ * vd_tess_set_generators_device + vd_tess_calculate bit for bit. */
 int vd_calculate_noalloc(const double bmin[3], const double bmax[3], int nx, int ny, int nz,
                          const double* d_xyz, size_t n, double* d_volume, double* d_centroid3,
                          int32_t* d_n_faces, void* stream);

@@ -39,6 +39,10 @@ def lib():
     vp = C.c_void_p
     L.vdo_create.restype = vp
     L.vdo_create.argtypes = [d3, d3, C.c_int, C.c_int, C.c_int]
+    L.vdo_create_truncated.restype = vp
+    L.vdo_create_truncated.argtypes = [d3, d3, C.c_int, C.c_int, C.c_int, C.c_int]
+    L.vdo_table_exhausted.restype = C.c_size_t
+    L.vdo_table_exhausted.argtypes = [vp]
     L.vdo_destroy.argtypes = [vp]
     L.vdo_add_wall_plane.argtypes = [vp, d3, d3, C.c_int]
     L.vdo_add_wall_sphere.argtypes = [vp, d3, C.c_double, C.c_int]
@@ -212,10 +216,13 @@ def regular_polyhedron(faces: int, center, radius: float):
 class OracleTessellation:
     """Tessellation<3, Cell3DFaces, Algorithm3DGrid> restated on the CPU."""
 
-    def __init__(self, bmin, bmax, nx: int, ny: int, nz: int):
+    def __init__(self, bmin, bmax, nx: int, ny: int, nz: int, order_k: int = 0):
+        """order_k > 0 truncates the search order to offsets of at most
+        order_k bins per axis (grids whose complete table does not fit in
+        memory); calculate() then raises if a cell's walk ran off it."""
         mn, pmn = _d(bmin)
         mx, pmx = _d(bmax)
-        self._h = lib().vdo_create(pmn, pmx, int(nx), int(ny), int(nz))
+        self._h = lib().vdo_create_truncated(pmn, pmx, int(nx), int(ny), int(nz), int(order_k))
         self.nx, self.ny, self.nz = int(nx), int(ny), int(nz)
         if not self._h:
             raise ValueError("invalid grid resolution")
@@ -273,6 +280,12 @@ class OracleTessellation:
 
     def calculate(self, nthreads: int = 0):
         lib().vdo_calculate(self._h, int(nthreads))
+        self._check_table()
+
+    def _check_table(self):
+        n = int(lib().vdo_table_exhausted(self._h))
+        if n:
+            raise RuntimeError(f"{n} cells walked off the truncated search order: use a larger order_k")
 
     def calculate_range(self, begin: int, end: int, nthreads: int = 0):
         lib().vdo_calculate_range(self._h, int(begin), int(end), int(nthreads))

@@ -505,7 +505,7 @@ static int wall_cut(const wall_t* w, const double* g, double* p, double* n) {
 /* ------------------------------------------------------------------ */
 typedef struct {
   int32_t dx, dy, dz;
-  int32_t lin; /* enumeration index: ties keep this order */
+  long long lin; /* enumeration index: ties keep this order */
   double min_d2;
 } offset_t;
 
@@ -515,6 +515,10 @@ struct vdo_tess {
   double sx, sy, sz;       /* grid_scale */
   double lx, ly, lz;       /* grid_limit = n - 1e-5 */
   offset_t* order; size_t norder;
+  /* a truncated order (vdo_create_truncated) holds every entry with
+   * min_d2 < order_bound; cells whose walk reaches its end unfinished are
+   * counted in `exhausted` */
+  int truncated; double order_bound; size_t exhausted;
   wall_t walls[VDO_MAX_WALLS]; int nwalls;
   double* gen; size_t ngen;
   size_t* bin_of;          /* generator_bin_ids */
@@ -536,8 +540,13 @@ static int cmp_offset(const void* a, const void* b) {
   return (x->lin > y->lin) - (x->lin < y->lin);
 }
 
-/* Algorithm3DGrid::new (algo_3d_grid.rs:47-95), stable tie order */
-vdo_tess* vdo_create(const double bmin[3], const double bmax[3], int nx, int ny, int nz) {
+/* Algorithm3DGrid::new (algo_3d_grid.rs:47-95), stable tie order.
+ * k > 0 keeps only the offsets with |dx|, |dy|, |dz| <= k, each with its
+ * enumeration index in the complete table, so the kept entries are in the
+ * complete table's order; every omitted entry has min_d2 >= the smallest
+ * (k cs)^2 over the truncated axes, and a walk that breaks before reaching
+ * that bound visits exactly what the complete table gives it. */
+vdo_tess* vdo_create_truncated(const double bmin[3], const double bmax[3], int nx, int ny, int nz, int k) {
   if (nx <= 0 || ny <= 0 || nz <= 0) return NULL;
   vdo_tess* t = (vdo_tess*)calloc(1, sizeof(vdo_tess));
   memcpy(t->bmin, bmin, 3 * sizeof(double));
@@ -548,23 +557,37 @@ vdo_tess* vdo_create(const double bmin[3], const double bmax[3], int nx, int ny,
   t->sz = (double)nz / (bmax[2] - bmin[2]);
   t->lx = (double)nx - 1e-5; t->ly = (double)ny - 1e-5; t->lz = (double)nz - 1e-5;
   double csx = 1.0 / t->sx, csy = 1.0 / t->sy, csz = 1.0 / t->sz;
-  size_t n = (size_t)(2 * nx + 1) * (size_t)(2 * ny + 1) * (size_t)(2 * nz + 1);
+  const int kx = (k > 0 && k < nx) ? k : nx, ky = (k > 0 && k < ny) ? k : ny, kz = (k > 0 && k < nz) ? k : nz;
+  t->truncated = kx < nx || ky < ny || kz < nz;
+  t->order_bound = INFINITY;
+  if (kx < nx) t->order_bound = fmin(t->order_bound, ((double)kx * csx) * ((double)kx * csx));
+  if (ky < ny) t->order_bound = fmin(t->order_bound, ((double)ky * csy) * ((double)ky * csy));
+  if (kz < nz) t->order_bound = fmin(t->order_bound, ((double)kz * csz) * ((double)kz * csz));
+  size_t n = (size_t)(2 * kx + 1) * (size_t)(2 * ky + 1) * (size_t)(2 * kz + 1);
   t->order = (offset_t*)malloc(n * sizeof(offset_t));
-  size_t k = 0;
-  for (int z = -nz; z <= nz; ++z)
-    for (int y = -ny; y <= ny; ++y)
-      for (int x = -nx; x <= nx; ++x) {
+  size_t q = 0;
+  for (int z = -kz; z <= kz; ++z)
+    for (int y = -ky; y <= ky; ++y)
+      for (int x = -kx; x <= kx; ++x) {
         double mx = x > 0 ? (double)(x - 1) * csx : (x < 0 ? (double)(-x - 1) * csx : 0.0);
         double my = y > 0 ? (double)(y - 1) * csy : (y < 0 ? (double)(-y - 1) * csy : 0.0);
         double mz = z > 0 ? (double)(z - 1) * csz : (z < 0 ? (double)(-z - 1) * csz : 0.0);
-        offset_t o = {x, y, z, (int32_t)k, mx * mx + my * my + mz * mz};
-        t->order[k++] = o;
+        /* the index in the complete z-outer, x-inner enumeration */
+        long long lin = (((long long)z + nz) * (2LL * ny + 1) + ((long long)y + ny)) * (2LL * nx + 1) + (x + nx);
+        offset_t o = {x, y, z, lin, mx * mx + my * my + mz * mz};
+        t->order[q++] = o;
       }
   qsort(t->order, n, sizeof(offset_t), cmp_offset);
   t->norder = n;
   t->bin_start = (size_t*)calloc(t->nx * t->ny * t->nz + 1, sizeof(size_t));
   return t;
 }
+
+vdo_tess* vdo_create(const double bmin[3], const double bmax[3], int nx, int ny, int nz) {
+  return vdo_create_truncated(bmin, bmax, nx, ny, nz, 0);
+}
+
+size_t vdo_table_exhausted(const vdo_tess* t) { return t->exhausted; }
 
 static void free_cells(vdo_tess* t) {
   for (size_t i = 0; i < t->ncells; ++i) {
@@ -860,7 +883,8 @@ void vdo_clear_walls(vdo_tess* t) { t->nwalls = 0; }
 
 /* compute_cell (tessellation.rs:414-475) with visit_neighbors
  * (algo_3d_grid.rs:145-202) and the visitor (tessellation.rs:446-471) */
-static void compute_cell(const vdo_tess* t, size_t i, vdo_cell* cell, scratch_t* s, uint64_t* cnt) {
+/* returns 1 when the walk ran off a truncated search order unfinished */
+static int compute_cell(const vdo_tess* t, size_t i, vdo_cell* cell, scratch_t* s, uint64_t* cnt) {
   const double g[3] = {t->gen[3 * i], t->gen[3 * i + 1], t->gen[3 * i + 2]};
   double r2;
   cell_init_box(cell, i, t->bmin, t->bmax);
@@ -868,7 +892,7 @@ static void compute_cell(const vdo_tess* t, size_t i, vdo_cell* cell, scratch_t*
     double p[3 * VDO_MAX_PLANES], n[3 * VDO_MAX_PLANES];
     int np = wall_cut(&t->walls[w], g, p, n);
     for (int k = 0; k < np; ++k) cell_clip(cell, &p[3 * k], &n[3 * k], t->walls[w].id, s, NULL, &r2, cnt);
-    if (cell->nv == 0) return;
+    if (cell->nv == 0) return 0;
   }
   double cur = cell_max_radius_sq(cell, g);
 
@@ -879,10 +903,14 @@ static void compute_cell(const vdo_tess* t, size_t i, vdo_cell* cell, scratch_t*
   double rx = (g[0] - t->bmin[0]) * t->sx - (double)ix;
   double ry = (g[1] - t->bmin[1]) * t->sy - (double)iy;
   double rz = (g[2] - t->bmin[2]) * t->sz - (double)iz;
+  int broke = 0;
   for (size_t k = 0; k < t->norder; ++k) {
     const offset_t* o = &t->order[k];
     if (cnt) cnt[VDO_CNT_OFFSETS]++;
-    if (o->min_d2 > 4.0 * cur) break;
+    if (o->min_d2 > 4.0 * cur) {
+      broke = 1;
+      break;
+    }
     long bx = (long)ix + o->dx, by = (long)iy + o->dy, bz = (long)iz + o->dz;
     if (bx < 0 || bx >= (long)t->nx || by < 0 || by >= (long)t->ny || bz < 0 || bz >= (long)t->nz)
       continue;
@@ -910,6 +938,7 @@ static void compute_cell(const vdo_tess* t, size_t i, vdo_cell* cell, scratch_t*
       }
     }
   }
+  return t->truncated && !broke && !(t->order_bound > 4.0 * cur);
 }
 
 void vdo_calculate_range(vdo_tess* t, size_t begin, size_t end, int nthreads) {
@@ -919,6 +948,7 @@ void vdo_calculate_range(vdo_tess* t, size_t begin, size_t end, int nthreads) {
   t->ncells = t->ngen;
   t->cells = (vdo_cell*)calloc(t->ncells ? t->ncells : 1, sizeof(vdo_cell));
   memset(t->counters, 0, sizeof(t->counters));
+  t->exhausted = 0;
   if (end > t->ngen) end = t->ngen;
 #ifdef _OPENMP
   if (nthreads <= 0) nthreads = omp_get_max_threads();
@@ -929,17 +959,21 @@ void vdo_calculate_range(vdo_tess* t, size_t begin, size_t end, int nthreads) {
     memset(&s, 0, sizeof(s));
     uint64_t cnt[VDO_NCOUNTERS];
     memset(cnt, 0, sizeof(cnt));
+    size_t exh = 0;
 #ifdef _OPENMP
 #pragma omp for schedule(dynamic, 64)
 #endif
     for (long long i = (long long)begin; i < (long long)end; ++i) {
-      compute_cell(t, (size_t)i, &t->cells[i], &s, cnt);
+      exh += (size_t)compute_cell(t, (size_t)i, &t->cells[i], &s, cnt);
       cell_measure(&t->cells[i], NULL, NULL, cnt);
     }
 #ifdef _OPENMP
 #pragma omp critical
 #endif
-    for (int k = 0; k < VDO_NCOUNTERS; ++k) t->counters[k] += cnt[k];
+    {
+      for (int k = 0; k < VDO_NCOUNTERS; ++k) t->counters[k] += cnt[k];
+      t->exhausted += exh;
+    }
     scratch_free(&s);
   }
   (void)nthreads;

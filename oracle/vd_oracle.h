@@ -46,6 +46,12 @@ enum {
 
 /* ---- tessellation (tessellation.rs + algo_3d_grid.rs) ---- */
 vdo_tess* vdo_create(const double bmin[3], const double bmax[3], int nx, int ny, int nz);
+/* the same with the search order truncated to offsets |d| <= k on each axis
+ * (for grids whose complete (2n+1)^3 table does not fit in memory); the
+ * cells of the last calculate whose walk ran off it are counted by
+ * vdo_table_exhausted, and their results are then not the reference's */
+vdo_tess* vdo_create_truncated(const double bmin[3], const double bmax[3], int nx, int ny, int nz, int k);
+size_t vdo_table_exhausted(const vdo_tess* t);
 void vdo_destroy(vdo_tess* t);
 /* returns 0, or -1 if id > -1000 (the reference panics, wall/mod.rs:25) */
 int vdo_add_wall_plane(vdo_tess* t, const double point[3], const double normal[3], int id);

@@ -216,3 +216,25 @@ def test_search_order_matches_oracle(oracle_mod, lo, hi, n):
         assert not comp
         keep = om < bound
         assert np.array_equal(d, od[keep]) and np.array_equal(m, om[keep])
+
+
+def test_truncated_search_order_equals_complete(oracle_mod):
+    """The oracle's truncated search order (for grids whose complete table
+    does not fit in memory) keeps the complete table's order: with enough
+    bins per axis every result and event counter is the complete table's,
+    and a table too short for some cell raises instead of answering."""
+    pts = uniform(20000, 0.0, 1.0, 5)
+    full = oracle_mod.OracleTessellation([0, 0, 0], [1, 1, 1], 40, 40, 40)
+    full.set_generators(pts)
+    full.calculate()
+    cut = oracle_mod.OracleTessellation([0, 0, 0], [1, 1, 1], 40, 40, 40, order_k=6)
+    cut.set_generators(pts)
+    cut.calculate()
+    for a, b in zip(full.summaries(), cut.summaries()):
+        assert np.array_equal(a, b)
+    assert np.array_equal(full.neighbors()[1], cut.neighbors()[1])
+    assert full.counters() == cut.counters()
+    short = oracle_mod.OracleTessellation([0, 0, 0], [1, 1, 1], 40, 40, 40, order_k=2)
+    short.set_generators(pts)
+    with pytest.raises(RuntimeError):
+        short.calculate()

@@ -14,7 +14,7 @@ import ctypes as C
 import numpy as np
 import pytest
 
-from common import uniform
+from common import bench_distribution, blobs, uniform
 
 pytestmark = pytest.mark.gpu
 
@@ -43,8 +43,9 @@ def regular(bmin, bmax, grid, pts):
     t.set_generators(pts)
     t.calculate()
     out = t.summaries()
+    fb = t.fallback_counts()
     t.close()
-    return out
+    return out + (fb,)
 
 
 def test_noalloc_matches_regular_two_calls():
@@ -57,7 +58,7 @@ def test_noalloc_matches_regular_two_calls():
     for bmin, bmax, grid, pts in cases:
         rc, vol, cen, nf = noalloc(L, bmin, bmax, grid, pts)
         assert rc == 0, L.vd_last_error(None)
-        rv, rcen, rnf = regular(bmin, bmax, grid, pts)
+        rv, rcen, rnf, _ = regular(bmin, bmax, grid, pts)
         assert np.array_equal(nf, rnf)
         assert np.array_equal(vol, rv)
         assert np.array_equal(cen, rcen)
@@ -72,3 +73,37 @@ def test_noalloc_rejects_oversized_requests():
     assert rc == 1 and b"8192" in L.vd_last_error(None)
     rc, *_ = noalloc(L, [0, 0, 0], [1, 1, 1], (21, 21, 21), uniform(100, 0.0, 1.0, 1))
     assert rc == 1 and b"search-order" in L.vd_last_error(None)
+
+
+def test_noalloc_large_capacity_pass_two_calls():
+    """Inputs whose cells outgrow the shared-memory pass go through the
+    large-capacity pass in the scratch array: the centre of 80 points on a
+    sphere (79 faces, pooled beyond the 48 per-cell face slots) and a dense
+    blob on a coarse grid.  Each call equals the regular path exactly."""
+    import vorothree_b200 as v
+    L = v.load()
+    cases = [
+        ([0, 0, 0], [100, 100, 100], (4, 4, 4), bench_distribution("sphere", 80, 31)),
+        ([0, 0, 0], [1, 1, 1], (6, 6, 6), np.clip(blobs(5000, 2, 0.02, 0.9, 32), 0.0, 1.0)),
+    ]
+    for bmin, bmax, grid, pts in cases:
+        rc, vol, cen, nf = noalloc(L, bmin, bmax, grid, pts)
+        assert rc == 0, L.vd_last_error(None)
+        rv, rcen, rnf, fb = regular(bmin, bmax, grid, pts)
+        assert sum(fb.values()) > 0, "the case must leave the shared-memory pass"
+        assert np.array_equal(nf, rnf)
+        assert np.array_equal(vol, rv)
+        assert np.array_equal(cen, rcen)
+
+
+def test_noalloc_block_tier_cell_is_an_overflow():
+    """The centre of 3,000 points on a sphere has 2,999 faces: beyond the
+    large-capacity pass, so the call reports VD_EOVERFLOW instead of a result
+    (the regular entry points build it in their block-per-cell tier)."""
+    import vorothree_b200 as v
+    from vorothree_b200._lib import VD_EOVERFLOW
+    L = v.load()
+    pts = bench_distribution("sphere", 3000, 33)
+    rc, *_ = noalloc(L, [0, 0, 0], [100, 100, 100], (14, 14, 14), pts)
+    assert rc == VD_EOVERFLOW
+    assert b"large polytope capacity" in L.vd_last_error(None)

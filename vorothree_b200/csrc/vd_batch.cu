@@ -232,6 +232,7 @@ struct vd_batch {
   float last_ms = 0.f;
   unsigned long long counters[kNumCounters] = {};
   unsigned long long table_reruns = 0;
+  unsigned long long pool_reruns = 0;  // chains rerun after the face pool grew
 };
 
 namespace {
@@ -446,16 +447,54 @@ int clip_all(vd_batch* b) {
   return clip_chain(b, nullptr, 0);
 }
 
+void drop_graph(vd_batch* b) {
+  if (b->graph_exec) cudaGraphExecDestroy(b->graph_exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->graph_exec = nullptr;
+  b->graph = nullptr;
+}
+
+// The face pool (face slots of cells with more than 48 faces) was too small
+// for the last clip chain: cells that found no room have no face slots and a
+// face count of -1.  Grow the pool to what the chain asked for and run the
+// whole chain again on the same generators (a captured Lloyd step holds the
+// old pool in its descriptors, so it is dropped and captured again later).
+int grow_pool_and_rerun(vd_batch* b, unsigned long long used) {
+  cudaStream_t s = b->stream;
+  const int nt = (int)b->m.size();
+  b->pool_cap = std::max<long long>(2 * b->pool_cap, (long long)(used + used / 4));
+  B_CK(b, cudaStreamSynchronize(s));
+  B_CK(b, b->d_pool_fnb.ensure(b->pool_cap));
+  B_CK(b, b->d_pool_area.ensure(b->pool_cap));
+  drop_graph(b);
+  int r = upload_static(b);
+  if (r != VD_OK) return r;
+  k_bdesc_update<<<blocks_for(b, nt, 128), 128, 0, s>>>(b->d_descs.p, nt, b->d_off.p, b->d_bin_off.p, bases(b));
+  B_CK(b, cudaGetLastError());
+  B_CK(b, cudaMemsetAsync(b->d_tess_flags.p, 0, nt * sizeof(unsigned int), s));
+  B_CK(b, cudaMemsetAsync(b->d_counters.p, 0, kNumCounters * sizeof(unsigned long long), s));
+  ++b->pool_reruns;
+  return clip_all(b);
+}
+
 // cells that ran off a truncated search order: lengthen that member's table
-// and run them again (host loop; rare for uniform inputs)
+// and run them again (host loop; rare for uniform inputs); a face pool that
+// was too small is grown and the chain rerun
 int resolve_tables(vd_batch* b) {
   cudaStream_t s = b->stream;
   const int nt = (int)b->m.size();
   for (int guard = 0; guard < 32; ++guard) {
     unsigned int h[kBWords];
+    unsigned long long used = 0;
     B_CK(b, cudaMemcpyAsync(h, b->d_ctl.p, sizeof(h), cudaMemcpyDeviceToHost, s));
+    B_CK(b, cudaMemcpyAsync(&used, b->d_pool_cursor.p, sizeof(used), cudaMemcpyDeviceToHost, s));
     B_CK(b, cudaStreamSynchronize(s));
     if (h[kBHugeOvf] > 0) return bfail(b, VD_EOVERFLOW, "%u cells exceed the huge polytope capacity", h[kBHugeOvf]);
+    if ((long long)used > b->pool_cap) {
+      int r = grow_pool_and_rerun(b, used);
+      if (r != VD_OK) return r;
+      continue;
+    }
     const unsigned ntab = h[kBTab];
     if (ntab == 0) return VD_OK;
     std::vector<unsigned int> flags(nt);
@@ -595,12 +634,7 @@ int vd_batch_set_precision(vd_batch* b, int precision) {
   if (!b) return VD_EINVAL;
   if (precision != VD_PREC_FP64 && precision != VD_PREC_MIXED) return bfail(b, VD_EINVAL, "unknown precision");
   b->precision = precision;
-  if (b->graph_exec) {  // the captured step uses the previous kernel
-    cudaGraphExecDestroy(b->graph_exec);
-    cudaGraphDestroy(b->graph);
-    b->graph_exec = nullptr;
-    b->graph = nullptr;
-  }
+  drop_graph(b);  // the captured step uses the previous kernel
   return VD_OK;
 }
 
@@ -737,7 +771,12 @@ int vd_batch_lloyd(vd_batch* b, int steps) {
     B_CK(b, cudaEventRecord(b->ev0, s));
   }
   for (int i = 0; i < steps; ++i) {
-    B_CK(b, cudaGraphLaunch(b->graph_exec, s));
+    if (b->graph_exec) {
+      B_CK(b, cudaGraphLaunch(b->graph_exec, s));
+    } else {  // dropped by a pool growth: the remaining steps run eagerly
+      int r = lloyd_step(b);
+      if (r != VD_OK) return r;
+    }
     int r = resolve_tables(b);
     if (r != VD_OK) return r;
   }

@@ -356,6 +356,9 @@ __global__ void k_csr_gather(const int32_t* __restrict__ nf, size_t n, const lon
     if (c <= 0) continue;
     const long long o = off[i];
     const bool pooled = c > fout;
+    // a pooled cell without slots (-1) has nothing to copy; the host reports
+    // pool overflow as an error before results can be read
+    if (pooled && pool_off[i] < 0) continue;
     for (int f = lane; f < c; f += 32) {
       const size_t src = pooled ? (size_t)pool_off[i] + f : i * (size_t)fout + f;
       if (out_ids) out_ids[o + f] = pooled ? pool_fnb[src] : fnb[src];

@@ -41,6 +41,9 @@ constexpr int kCompleteOrderMax = 1 << 15;
 constexpr int kMaxInitialOrder = 32;
 // blocks of the huge tier (each holds its cell's polytope in global memory)
 constexpr int kHugeBlocksMax = 64;
+// face capacities of the tiers whose cells can have more faces than the
+// per-cell slots hold (medium, large, huge): their faces go to the pool
+constexpr long long kMedFaces = 112, kBigFaces = 512, kHugeFaces = 32767;
 // kernels this library has launched in this process (all handles)
 std::atomic<unsigned long long> g_launches{0};
 
@@ -246,6 +249,8 @@ struct vd_tess {
   DevBuf<unsigned char> d_big, d_huge;
   size_t big_warps = 0, huge_blocks = 0;
   long long pool_cap = 0;
+  // the pool cursor as the host last read it (after every clip pass)
+  unsigned long long pool_used = 0;
 
   // scan scratch
   std::vector<DevBuf<uint32_t>> scan32;
@@ -500,12 +505,45 @@ int ensure_big(vd_tess* t, size_t cells) {
     VD_CK(t, t->d_big.ensure(want * t->info64.big_scratch_per_warp, t->stream));
     t->big_warps = want;
   }
-  if (t->pool_cap == 0) {
-    const long long cap = 1 << 20;
-    VD_CK(t, t->d_pool_fnb.ensure(cap, t->stream));
-    VD_CK(t, t->d_pool_area.ensure(cap, t->stream));
-    t->pool_cap = cap;
+  return VD_OK;
+}
+
+// Most faces one cell can have in a tier of face capacity fcap: a face per
+// other generator, per box side and per wall plane; seal clips add at most
+// one more face per other generator.
+long long faces_bound(const vd_tess* t, long long fcap, bool seal) {
+  long long planes = 0;
+  for (const Wall& w : t->walls) planes += w.kind == kWallPolyhedron ? w.np : 1;
+  const long long others = t->ngen > 0 ? (long long)t->ngen - 1 : 0;
+  return std::min(fcap, (seal ? 2 : 1) * others + 6 + planes);
+}
+
+// The face pool holds the face slots of cells with more faces than the
+// per-cell slots.  Before a pass of a tier that can finish such cells, the
+// pool is grown to hold every cell of the pass at the tier's largest face
+// count beyond what earlier passes used, so a finished cell always gets its
+// slots; the used part is kept when the pool grows.
+int ensure_pool(vd_tess* t, size_t cells, long long faces_per_cell) {
+  const unsigned long long need = t->pool_used + (unsigned long long)cells * (unsigned long long)faces_per_cell;
+  if ((long long)need <= t->pool_cap) return VD_OK;
+  const long long cap = std::max<long long>({(long long)need, 2 * t->pool_cap, 1LL << 20});
+  DevBuf<int32_t> fnb;
+  DevBuf<double> area;
+  VD_CK(t, fnb.ensure((size_t)cap, t->stream));
+  VD_CK(t, area.ensure((size_t)cap, t->stream));
+  if (t->pool_used > 0) {
+    VD_CK(t, cudaMemcpyAsync(fnb.p, t->d_pool_fnb.p, t->pool_used * sizeof(int32_t), cudaMemcpyDeviceToDevice,
+                             t->stream));
+    VD_CK(t, cudaMemcpyAsync(area.p, t->d_pool_area.p, t->pool_used * sizeof(double), cudaMemcpyDeviceToDevice,
+                             t->stream));
   }
+  t->d_pool_fnb.release();
+  t->d_pool_area.release();
+  t->d_pool_fnb = fnb;
+  t->d_pool_area = area;
+  fnb.p = nullptr;
+  area.p = nullptr;
+  t->pool_cap = cap;
   return VD_OK;
 }
 
@@ -537,6 +575,11 @@ int clip_pass(vd_tess* t, int tier, const uint32_t* items, uint32_t nitems, uint
   W.tab_list = tab_list;
   W.tab_count = t->d_ctl.p + kCtlTabCount;
   W.counters = t->d_counters.p;
+  if (tier >= 1) {
+    const long long fcap = tier == 1 ? kMedFaces : (tier == 2 ? kBigFaces : kHugeFaces);
+    int r = ensure_pool(t, nitems, faces_bound(t, fcap, false));
+    if (r != VD_OK) return r;
+  }
   TessDesc T = make_desc(t);
   if (tier == 1) {
     const int nblocks = (int)std::max<size_t>(
@@ -559,8 +602,7 @@ int clip_pass(vd_tess* t, int tier, const uint32_t* items, uint32_t nitems, uint
     VD_CK(t, launch_clip_fp64_big(T, W, t->d_big.p, (int)t->big_warps, s));
     g_launches++;
   } else {
-    int r = ensure_big(t, nitems);  // the face pool
-    if (r == VD_OK) r = ensure_huge(t, nitems);
+    int r = ensure_huge(t, nitems);
     if (r != VD_OK) return r;
     T = make_desc(t);
     VD_CK(t, launch_clip_fp64_huge(T, W, t->d_huge.p, (int)t->huge_blocks, s));
@@ -569,12 +611,20 @@ int clip_pass(vd_tess* t, int tier, const uint32_t* items, uint32_t nitems, uint
   return VD_OK;
 }
 
+// the pass's overflow and table counts, and the face pool's cursor; a cell
+// whose faces found no room in the pool is an error (ensure_pool sizes the
+// pool so that this cannot happen)
 int read_ctl(vd_tess* t, unsigned int* ovf, unsigned int* tab) {
   unsigned int h[3];
   VD_CK(t, cudaMemcpyAsync(h, t->d_ctl.p, sizeof(h), cudaMemcpyDeviceToHost, t->stream));
+  VD_CK(t, cudaMemcpyAsync(&t->pool_used, t->d_pool_cursor.p, sizeof(t->pool_used), cudaMemcpyDeviceToHost,
+                           t->stream));
   VD_CK(t, cudaStreamSynchronize(t->stream));
   *ovf = h[kCtlOvfCount];
   *tab = h[kCtlTabCount];
+  if ((long long)t->pool_used > t->pool_cap)
+    return fail(t, VD_EOVERFLOW, "face pool overflow: %llu face slots needed, %lld available", t->pool_used,
+                t->pool_cap);
   return VD_OK;
 }
 
@@ -591,7 +641,14 @@ int run_calculate(vd_tess* t, const WorkList* extra = nullptr, const uint32_t* o
   int r = ensure_outputs(t, n);
   if (r != VD_OK) return r;
   VD_CK(t, cudaMemsetAsync(t->d_counters.p, 0, kNumCounters * sizeof(unsigned long long), s));
-  VD_CK(t, cudaMemsetAsync(t->d_pool_cursor.p, 0, sizeof(unsigned long long), s));
+  if (!only_cell) {
+    // a new tessellation: the pool starts empty and no cell has pooled faces
+    // (-1); one cell rebuilt for get_cell appends to the pool instead, so the
+    // other cells' pooled faces stay where they are
+    VD_CK(t, cudaMemsetAsync(t->d_pool_cursor.p, 0, sizeof(unsigned long long), s));
+    VD_CK(t, cudaMemsetAsync(t->d_pool_off.p, 0xFF, n * sizeof(long long), s));
+    t->pool_used = 0;
+  }
   t->fallback[0] = t->fallback[1] = 0;
   // A truncated search order long enough for the generator density before
   // the first pass: on sparse grids (many bins per generator) cells walk past
@@ -795,10 +852,11 @@ int seal_pass(vd_tess* t, const SealArgs& A, const uint32_t* items, uint32_t nit
     W.tab_count = t->d_ctl.p + kCtlTabCount;
     if (tier == 1) {
       int r = ensure_big(t, n);
+      if (r == VD_OK) r = ensure_pool(t, n, faces_bound(t, kBigFaces, true));
       if (r != VD_OK) return r;
       VD_CK(t, launch_seal_big(make_desc(t), W, A, t->d_big.p, (int)t->big_warps, s));
     } else if (tier == 2) {
-      int r = ensure_big(t, n);  // the face pool
+      int r = ensure_pool(t, n, faces_bound(t, kHugeFaces, true));
       if (r == VD_OK) r = ensure_huge(t, n);
       if (r != VD_OK) return r;
       VD_CK(t, launch_seal_block(make_desc(t), W, A, t->d_huge.p, (int)t->huge_blocks, s));

@@ -25,8 +25,15 @@
 //  * Limits: at most kNaMaxGen generators, and a grid whose complete shell
 //    search order fits kNaMaxOrder entries ((2nx+1)(2ny+1)(2nz+1) <= 68921,
 //    e.g. 20x20x20).  Larger requests are rejected with VD_EINVAL.
-//  * No walls.  Results equal vd_tess_set_generators_device +
-//    vd_tess_calculate bit for bit (same kernels, same arithmetic).
+//  * Cells are built by the shared-memory pass and, when they outgrow it, by
+//    the large-capacity pass (2048 vertices, 512 faces); the regular entry
+//    points send cells beyond that to a block-per-cell tier whose storage
+//    (several MB per cell) this array does not hold.  Such a cell -- e.g. the
+//    centre of generators on a sphere, adjacent to thousands of others --
+//    makes the call return VD_EOVERFLOW, as does a total of more than
+//    kNaPoolFaces faces in cells with more than 48 faces.
+//  * No walls.  Every cell the call returns equals vd_tess_set_generators_device
+//    + vd_tess_calculate bit for bit (same kernels, same arithmetic).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -48,7 +55,9 @@ namespace {
 
 constexpr size_t kNaMaxGen = 8192;
 constexpr size_t kNaMaxOrder = 68921;  // complete search order of a 20x20x20 grid
-constexpr size_t kNaMaxBins = 8616;    // implied by the order limit
+// (2nx+1)(2ny+1)(2nz+1) > 8 nx ny nz, so the order limit admits fewer than
+// 68921 / 8 bins
+constexpr size_t kNaMaxBins = 8616;
 constexpr int kNaFout = 48;
 constexpr size_t kNaPoolFaces = 16384;
 constexpr int kNaBigWarps = 4;         // large-capacity pass: one block of 4 warps
@@ -84,6 +93,7 @@ constexpr size_t kOffBig = kOffSums1 + al(kNaSums * 4);
 constexpr size_t kNaBytes = kOffBig + al(kNaBigWarps * sizeof(WarpPoly<BigCfg>));
 
 static_assert((kNaMaxBins + 1 + kScanTile - 1) / kScanTile <= kNaSums, "scan sums");
+static_assert(kNaMaxBins * 8 >= kNaMaxOrder, "every grid within the order limit fits the bin regions");
 
 __device__ __align__(256) unsigned char g_vd_noalloc_scratch[kNaBytes];
 
@@ -159,7 +169,10 @@ extern "C" int vd_calculate_noalloc(const double bmin[3], const double bmax[3], 
   if (nx <= 0 || ny <= 0 || nz <= 0) return na_fail(VD_EINVAL, "grid resolution must be positive");
   const double order_full = (2.0 * nx + 1) * (2.0 * ny + 1) * (2.0 * nz + 1);
   const size_t nbins = (size_t)nx * ny * nz;
-  if (order_full > (double)kNaMaxOrder || nbins > kNaMaxBins)
+  if (order_full <= (double)kNaMaxOrder && nbins > kNaMaxBins)  // excluded by the static_assert above
+    return na_fail(VD_EINVAL, "vd_calculate_noalloc: grid %dx%dx%d has %zu bins, limit %zu", nx, ny, nz, nbins,
+                   kNaMaxBins);
+  if (order_full > (double)kNaMaxOrder)
     return na_fail(VD_EINVAL,
                    "vd_calculate_noalloc: grid %dx%dx%d needs %.0f search-order entries, limit %zu "
                    "((2nx+1)(2ny+1)(2nz+1) <= %zu, e.g. 20x20x20)",
@@ -302,10 +315,19 @@ extern "C" int vd_calculate_noalloc(const double bmin[3], const double bmax[3], 
     W.ovf_list = list1;
     W.tab_list = list1;
     NA_CK(launch_clip_fp64_big(T, W, base + kOffBig, kNaBigWarps, s));
+    unsigned long long used = 0;
     NA_CK(cudaMemcpyAsync(h, ctl, sizeof(h), cudaMemcpyDeviceToHost, s));
+    NA_CK(cudaMemcpyAsync(&used, pool_cursor, sizeof(used), cudaMemcpyDeviceToHost, s));
     NA_CK(cudaStreamSynchronize(s));
     if (h[1] > 0 || h[2] > 0)
-      return na_fail(VD_EOVERFLOW, "%u cells exceed the large polytope capacity", h[1] + h[2]);
+      return na_fail(VD_EOVERFLOW,
+                     "vd_calculate_noalloc: %u cells exceed the large polytope capacity (2048 vertices, 512 faces); "
+                     "the regular entry points build them",
+                     h[1] + h[2]);
+    if (used > kNaPoolFaces)
+      return na_fail(VD_EOVERFLOW,
+                     "vd_calculate_noalloc: cells with more than %d faces need %llu face slots, limit %zu", kNaFout,
+                     used, kNaPoolFaces);
   }
   return VD_OK;
 }

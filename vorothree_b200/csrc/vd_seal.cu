@@ -27,7 +27,12 @@ namespace {
 __device__ __forceinline__ const int32_t* face_list(const int32_t* nf, const int32_t* fnb, const long long* pool_off,
                                                     const int32_t* pool_fnb, int fout, uint32_t i, int* n) {
   *n = nf[i];
-  return *n <= fout ? fnb + (size_t)i * fout : pool_fnb + pool_off[i];
+  if (*n <= fout) return fnb + (size_t)i * fout;
+  if (pool_off[i] < 0) {  // no pool slots (the host reports pool overflow as an error)
+    *n = 0;
+    return fnb + (size_t)i * fout;
+  }
+  return pool_fnb + pool_off[i];
 }
 
 // the seal clips of cell i (tessellation.rs:263-311); *nlog gets the number
