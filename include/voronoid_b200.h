@@ -38,10 +38,17 @@ extern "C" {
 #define VD_ECUDA 5      /* CUDA runtime error / no device */
 #define VD_ESTATE 6     /* call out of order (e.g. results before calculate) */
 #define VD_EIO 7        /* a file could not be read (import_generators) */
+#define VD_ECANCELED 8  /* a served request was cancelled before it started */
 
 /* precision of the clipping path */
 #define VD_PREC_FP64 0  /* plain FP64, bitwise the reference's arithmetic */
 #define VD_PREC_MIXED 1 /* FP32 classification under an error bound, FP64 construction */
+
+/* layout of the shared-memory tier's polytope (a tuning choice; results are
+ * identical): slots rewrite only the faces a clip cuts (default), full
+ * rewrites every face loop on each modifying clip, as the reference does */
+#define VD_FAST_SLOTS 0
+#define VD_FAST_FULL 1
 
 /* WALL_ID_MAX (wall/mod.rs:8) */
 #define VD_WALL_ID_MAX (-1000)
@@ -50,6 +57,9 @@ typedef struct vd_tess vd_tess;
 
 /* ---- Tessellation::new + Algorithm3DGrid::new
  *      (tessellation.rs:25-36, algo_3d_grid.rs:47-95) ---- */
+/* Errors: VD_EINVAL for a grid resolution outside [1, 16000] or a box whose
+ * extent is not positive and finite on every axis (the reference's grid scale
+ * n / (max - min) would be infinite or NaN); VD_ECUDA without a device. */
 int vd_tess_create(const double bmin[3], const double bmax[3], int nx, int ny, int nz,
                    vd_tess** out);
 /* drop of Tessellation */
@@ -123,6 +133,10 @@ int vd_tess_get_generators(vd_tess* t, double* xyz);
 /* ---- the hot path ---- */
 /* select VD_PREC_FP64 (default) or VD_PREC_MIXED for the next calculate */
 int vd_tess_set_precision(vd_tess* t, int precision);
+/* select VD_FAST_SLOTS (default) or VD_FAST_FULL for the next calculate (no
+ * counterpart in the reference: a layout choice of this library's first
+ * tier, made by the autotuner; every choice gives the same results) */
+int vd_tess_set_fast_layout(vd_tess* t, int layout);
 /* Tessellation::calculate (tessellation.rs:213-230) over compute_cell
  * (:414-475), Algorithm3DGrid::visit_neighbors (algo_3d_grid.rs:145-202) and
  * Cell3DFaces::clip_with_scratch (cell_3d_faces.rs:288-503), with the volume,
@@ -135,6 +149,15 @@ int vd_tess_calculate(vd_tess* t);
  * the reference's per-cell map (tessellation.rs:223-229) restricted to the
  * range.  VD_EINVAL unless begin <= end <= count_generators. */
 int vd_tess_calculate_range(vd_tess* t, size_t begin, size_t end);
+/* The same over interleaved chunks (no counterpart in the reference): the
+ * cells with ids in [begin, end) and ((id - begin) / chunk) % stride == phase.
+ * With stride = the number of GPUs and phase = this GPU's rank, each GPU gets
+ * an equal share of every part of the id order, so inputs whose cost varies
+ * along the id order (clustered generators first, background after) balance
+ * across GPUs.  VD_EINVAL unless chunk >= 1 and phase < stride.  A polytope
+ * export (vd_tess_export_cells) needs a contiguous calculate: VD_ESTATE
+ * after a strided one. */
+int vd_tess_calculate_strided(vd_tess* t, size_t begin, size_t end, size_t chunk, size_t stride, size_t phase);
 /* Tessellation::calculate_sealed (tessellation.rs:234-318): calculate, then
  * every cell on a curved wall (sphere, cylinder, cone, torus) is clipped with
  * the wall's tangent plane at each face neighbour on the same wall, when its
@@ -192,6 +215,12 @@ int vd_tess_export_cells(vd_tess* t, size_t begin, size_t end, int64_t* v_off, i
 /* ---- device-resident results (for callers that keep data on the GPU) ---- */
 int vd_tess_device_results(vd_tess* t, const double** d_volume, const double** d_centroid3,
                            const int32_t** d_n_faces);
+/* the neighbour-id and face-area CSR (as vd_tess_get_neighbors /
+ * vd_tess_get_face_areas give it) in device memory owned by t:
+ * d_offsets[n_cells + 1], d_ids[*total], d_areas[*total]; valid until the next
+ * call that changes t; the data is complete when the call returns */
+int vd_tess_device_neighbors(vd_tess* t, const int64_t** d_offsets, const int32_t** d_ids, const double** d_areas,
+                             int64_t* total);
 
 /* ---- instrumentation ---- */
 /* the CUDA stream (cudaStream_t) all work of t is ordered on */
@@ -314,6 +343,8 @@ const char* vd_batch_last_error(const vd_batch* b);
 int vd_batch_add(vd_batch* b, const double bmin[3], const double bmax[3], int nx, int ny, int nz,
                  const vd_wall_desc* walls, int nwalls, const double* xyz, size_t n, int* index);
 int vd_batch_set_precision(vd_batch* b, int precision);
+/* VD_FAST_SLOTS (default) or VD_FAST_FULL, as vd_tess_set_fast_layout */
+int vd_batch_set_fast_layout(vd_batch* b, int layout);
 int vd_batch_set_instrumentation(vd_batch* b, int on);
 /* upload every member and bin it (after the last vd_batch_add) */
 int vd_batch_commit(vd_batch* b);
@@ -360,6 +391,27 @@ int vd_server_take(vd_server* s, uint64_t ticket, double* volume, double* centro
 int vd_server_stats(vd_server* s, uint64_t* completed, uint64_t* cells, double* p50_s, double* p99_s,
                     size_t* peak_bytes);
 int vd_server_reset_stats(vd_server* s);
+/* requests on the GPU now and the most at once since the last reset_stats */
+int vd_server_concurrency(vd_server* s, int* running, int* peak_running);
+/* on = 1: requests submitted afterwards also return each cell's neighbour
+ * ids and face areas (Cell3DFaces::face_neighbors / face_area,
+ * cell_3d_faces.rs:97-99,207-254) as a CSR over cells (vd_server_take_faces) */
+int vd_server_set_face_results(vd_server* s, int on);
+/* blocks until the request is done; *total = its faces over all cells (the
+ * size of the CSR arrays), 0 for a request submitted without face results */
+int vd_server_total_faces(vd_server* s, uint64_t ticket, int64_t* total);
+/* vd_server_take plus the CSR: offsets[n_cells + 1], ids[total], areas[total]
+ * (any pointer may be NULL); releases the request */
+int vd_server_take_faces(vd_server* s, uint64_t ticket, double* volume, double* centroid3, int32_t* n_faces,
+                         int64_t* offsets, int32_t* ids, double* areas);
+/* a request still in the queue is dropped (its wait/take return VD_ECANCELED);
+ * one that has started runs to completion and this returns VD_ESTATE */
+int vd_server_cancel(vd_server* s, uint64_t ticket);
+
+/* ---- fault injection for tests (no counterpart in the reference) ----
+ * the next `count` device allocations this library makes (in any thread)
+ * fail as out of memory (VD_ENOMEM), as a full GPU would; 0 clears it */
+int vd_debug_fail_allocations(int count);
 
 /* ---- allocation-free variant (no counterpart in the reference) ----
  * set_generators + calculate for a small tessellation without any device

@@ -82,3 +82,20 @@ def test_header_is_plain_c(tmp_path):
     r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
     assert r.returncode == 0, (r.returncode, r.stderr)
     assert int(r.stdout.strip()) == len(syms)
+
+
+@pytest.mark.parametrize("bmin,bmax", [([0, 0, 0], [1, 0, 1]), ([0, 0, 0], [1, 1, -1]),
+                                       ([0, 0, float("nan")], [1, 1, 1]), ([0, 0, 0], [1, float("inf"), 1])])
+def test_degenerate_box_rejected_before_device(bmin, bmax):
+    """A box with no positive finite extent on an axis is refused with
+    VD_EINVAL before any device is touched (so also on a host without GPU)."""
+    import numpy as np
+    from vorothree_b200 import _lib
+    L = _lib.load()
+    mn = np.asarray(bmin, np.float64)
+    mx = np.asarray(bmax, np.float64)
+    h = ctypes.c_void_p()
+    rc = L.vd_tess_create(mn.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                          mx.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 2, 2, 2, ctypes.byref(h))
+    assert rc == _lib.VD_EINVAL
+    assert b"extent" in L.vd_last_error(None)

@@ -97,3 +97,36 @@ def test_export_argument_checks():
                                   off.ctypes.data_as(i64), None, None, None, None) == _lib.VD_EINVAL
     x = t.export_cells(0, 50)
     assert x["v_off"][-1] > 0
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_nan_and_inf_generators_match_the_oracle(oracle_mod, precision):
+    """Non-finite generators are not an error in the reference: without walls
+    set_generators keeps them (tessellation.rs:43-67), get_bin_index clamps
+    and truncates them (NaN to bin 0, +-inf to the edge bins,
+    algo_3d_grid.rs:98-107), and every comparison with a NaN distance is
+    false, so such a cell stays the box and no other cell is clipped by it.
+    With a sphere wall the filter drops them.  Each case equals the oracle
+    (NaN outputs compare equal to NaN)."""
+    import vorothree_b200 as v
+    pts = uniform(3000, 0.0, 1.0, 71)
+    pts[10] = [np.nan, 0.5, 0.5]
+    pts[20] = [0.5, np.inf, 0.5]
+    pts[30] = [-np.inf, 0.2, 0.9]
+    pts[40] = [np.nan, np.nan, np.nan]
+    for walls in ((), (("sphere", [0.5, 0.5, 0.5], 0.45),)):
+        t = v.Tessellation(v.BoundingBox([0, 0, 0], [1, 1, 1]), v.Algorithm3DGrid(12, 12, 12))
+        t.set_precision(precision)
+        o = oracle_mod.OracleTessellation([0, 0, 0], [1, 1, 1], 12, 12, 12)
+        for _, c, r in walls:
+            t.add_wall(v.Wall(v.WALL_ID_MAX, v.SphereGeometry(c, r)))
+            o.add_wall_sphere(c, r, v.WALL_ID_MAX)
+        assert t.set_generators(pts) == o.set_generators(pts)
+        t.calculate()
+        o.calculate()
+        assert np.array_equal(t.generators(), o.generators(), equal_nan=True)
+        for a, b in zip(t.summaries(), o.summaries()):
+            assert np.array_equal(a, b, equal_nan=True)
+        assert np.array_equal(t.neighbors()[1], o.neighbors()[1])
+        assert np.array_equal(t.face_areas()[1], o.face_areas()[1], equal_nan=True)
+        t.close()

@@ -477,3 +477,36 @@ def test_sphere_surface_10k_huge_cell(oracle_mod):
     assert g.summaries()[2][0] == 9999
     assert g.fallback_counts()["overflow"] > 0
     assert_same(g, o, sample_cells=3)
+
+
+@pytest.mark.parametrize("stride", [2, 3])
+def test_calculate_strided_shards(oracle_mod, stride):
+    """calculate_strided computes interleaved chunks of cell ids; the shards'
+    cells together equal one calculate() (each cell bitwise the oracle's), and
+    the cells a shard skips read as empty."""
+    import vorothree_b200 as v
+    pts = blobs(20000, 6, 0.03, 0.6, 91)
+    t = v.Tessellation(v.BoundingBox([0, 0, 0], [1, 1, 1]), v.Algorithm3DGrid(20, 20, 20))
+    t.set_generators(pts)
+    o = oracle_tess(oracle_mod, [0, 0, 0], [1, 1, 1], (20, 20, 20), pts)
+    ov, oc, on = o.summaries()
+    ooff, oids = o.neighbors()
+    n = len(pts)
+    chunk = 999
+    seen = np.zeros(n, bool)
+    for phase in range(stride):
+        t.calculate_strided(chunk, stride, phase)
+        gv, gc, gn = t.summaries()
+        goff, gids = t.neighbors()
+        mine = ((np.arange(n) // chunk) % stride) == phase
+        assert np.array_equal(gv[mine], ov[mine]) and np.array_equal(gn[mine], on[mine])
+        assert np.array_equal(gc[mine], oc[mine])
+        assert not gv[~mine].any() and not gn[~mine].any()
+        for i in np.nonzero(mine)[0][::97]:
+            assert np.array_equal(gids[goff[i]:goff[i + 1]], oids[ooff[i]:ooff[i + 1]])
+        assert t.get_cell(int(np.nonzero(~mine)[0][0])).face_neighbors().size == 0
+        seen |= mine
+    assert seen.all()
+    with pytest.raises(v.VoronoidError):
+        t.export_cells(0, 10)
+    t.close()

@@ -61,7 +61,7 @@ def test_admission_respects_budget_and_threads():
     import vorothree_b200 as v
     reqs = requests(4)
     # a budget that admits about one large request at a time still serves all
-    srv = v.TessellationServer(slots=3, hbm_budget_bytes=64 << 20)
+    srv = v.TessellationServer(slots=3, hbm_budget_bytes=200 << 20)
     results = {}
 
     def client(idx):
@@ -73,7 +73,7 @@ def test_admission_respects_budget_and_threads():
     for x in th:
         x.join()
     st = srv.stats()
-    assert st["completed"] == len(reqs) and st["peak_bytes"] <= (64 << 20)
+    assert st["completed"] == len(reqs) and st["peak_bytes"] <= (200 << 20)
     for i, r in enumerate(reqs):
         av, ac, an = alone(r)
         vol, cen, nf = results[i]
@@ -109,4 +109,86 @@ def test_text_requests_equal_alone():
         assert np.array_equal(nf, an) and np.array_equal(vol, av) and np.array_equal(cen, ac)
     with pytest.raises(v.VoronoidError):
         srv.submit_text(reqs[0][0], reqs[0][1], b"0 0.5 0.5 \xff\n")
+    srv.close()
+
+
+def alone_faces(req):
+    import vorothree_b200 as v
+    b, grid, pts, walls = req
+    t = v.Tessellation(b, v.Algorithm3DGrid(*grid))
+    for w in walls:
+        t.add_wall(w)
+    t.set_generators(pts)
+    t.calculate()
+    out = t.summaries() + t.neighbors() + (t.face_areas()[1],)
+    t.close()
+    return out
+
+
+def test_face_results_equal_alone_and_requests_overlap():
+    """With face results on, each request also returns its neighbour-id and
+    face-area CSR, equal to the standalone tessellation's; with four slots
+    and a queue of twelve, at least two requests run on the GPU at once."""
+    import vorothree_b200 as v
+    reqs = requests(6)
+    srv = v.TessellationServer(slots=4, hbm_budget_bytes=8 << 30)
+    srv.set_face_results(True)
+    tickets = [srv.submit(*r) for r in reqs]
+    got = [srv.take_faces(t) for t in tickets]
+    assert srv.concurrency()["peak_running"] >= 2
+    for r, (vol, cen, nf, off, ids, ar) in zip(reqs, got):
+        av, ac, an, aoff, aids, aar = alone_faces(r)
+        assert np.array_equal(nf, an) and np.array_equal(vol, av) and np.array_equal(cen, ac)
+        assert np.array_equal(off, aoff) and np.array_equal(ids, aids) and np.array_equal(ar, aar)
+    srv.close()
+
+
+def test_cancel_queued_request():
+    """One slot: a large request runs while two wait; cancelling a waiting
+    one drops it (its take reports VD_ECANCELED), the other still runs and
+    equals its standalone result; a finished request cannot be cancelled."""
+    import vorothree_b200 as v
+    from vorothree_b200._lib import VD_ECANCELED
+    srv = v.TessellationServer(slots=1, hbm_budget_bytes=8 << 30)
+    b = v.BoundingBox([0, 0, 0], [1, 1, 1])
+    big = (b, (100, 100, 100), uniform(1_000_000, 0, 1, 81), [])
+    small = requests(7)[:2]
+    t0 = srv.submit(*big)
+    t1 = srv.submit(*small[0])
+    t2 = srv.submit(*small[1])
+    assert srv.cancel(t2) is True
+    with pytest.raises(v.VoronoidError) as e:
+        srv.take(t2)
+    assert e.value.code == VD_ECANCELED
+    vol, cen, nf = srv.take(t1)
+    av, ac, an = alone(small[0])
+    assert np.array_equal(vol, av) and np.array_equal(nf, an)
+    srv.wait(t0)
+    assert srv.cancel(t0) is False
+    srv.take(t0)
+    srv.close()
+
+
+def test_allocation_failure_inside_a_request():
+    """A device allocation that fails inside a request (injected on the host:
+    the library's next allocation reports out-of-memory, as a full GPU would)
+    fails that request with VD_ENOMEM; the slot then serves the next request,
+    whose result equals its standalone result."""
+    import vorothree_b200 as v
+    from vorothree_b200._lib import VD_ENOMEM, load
+    L = load()
+    srv = v.TessellationServer(slots=1, hbm_budget_bytes=8 << 30)
+    reqs = requests(8)
+    try:
+        L.vd_debug_fail_allocations(1)
+        t0 = srv.submit(*reqs[0])
+        with pytest.raises(v.VoronoidError) as e:
+            srv.take(t0)
+        assert e.value.code == VD_ENOMEM
+    finally:
+        L.vd_debug_fail_allocations(0)
+    for r in reqs[:3]:
+        vol, cen, nf = srv.take(srv.submit(*r))
+        av, ac, an = alone(r)
+        assert np.array_equal(vol, av) and np.array_equal(nf, an) and np.array_equal(cen, ac)
     srv.close()

@@ -56,6 +56,15 @@ def _child(port, q):
         ok = ok and sv.is_cuda and sn.dtype == torch.int32
         ok = ok and (np.array_equal(sv.cpu().numpy(), hv) and np.array_equal(sc.cpu().numpy(), hc)
                      and np.array_equal(sn.cpu().numpy(), hn))
+        # the interleaved split with the face CSR, on the device and via the host
+        t.calculate()
+        hoff, hids = t.neighbors()
+        _, har = t.face_areas()
+        for fn in (v.calculate_sharded_faces_device, v.calculate_sharded_faces):
+            out = fn(t, chunk=777)
+            out = [x.cpu().numpy() if hasattr(x, "cpu") else x for x in out]
+            for got, want in zip(out, (hv, hc, hn, hoff, hids, har)):
+                ok = ok and np.array_equal(got, want)
         t.close()
         q.put((ok, None))
     except Exception as ex:  # reported to the parent

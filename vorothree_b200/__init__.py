@@ -9,8 +9,9 @@ reference's API over that ABI.
 from ._lib import VoronoidError, load
 from .batch import TessellationBatch
 from .server import TessellationServer
-from .shard import (calculate_sharded, calculate_sharded_device, cell_range, device_summaries, gather_summaries,
-                    gather_summaries_tensors, set_generators_broadcast)
+from .shard import (calculate_sharded, calculate_sharded_device, calculate_sharded_faces,
+                    calculate_sharded_faces_device, cell_chunks, cell_range, device_neighbors, device_summaries,
+                    gather_cells_tensors, gather_summaries, gather_summaries_tensors, set_generators_broadcast)
 from .tessellation import (WALL_ID_MAX, Algorithm3DGrid, BoundingBox, Cell3DFaces, ConeGeometry,
                            ConvexPolyhedronGeometry, CylinderGeometry, PlaneGeometry, SphereGeometry, Tessellation,
                            TorusGeometry, Wall, box_side, parse_generators)
@@ -18,5 +19,7 @@ from .tessellation import (WALL_ID_MAX, Algorithm3DGrid, BoundingBox, Cell3DFace
 __all__ = ["Algorithm3DGrid", "BoundingBox", "Cell3DFaces", "ConeGeometry", "ConvexPolyhedronGeometry",
            "CylinderGeometry", "PlaneGeometry", "SphereGeometry", "TorusGeometry",
            "Tessellation", "TessellationBatch", "TessellationServer", "Wall", "WALL_ID_MAX", "box_side", "VoronoidError", "load",
-           "calculate_sharded", "calculate_sharded_device", "cell_range", "device_summaries", "gather_summaries",
+           "calculate_sharded", "calculate_sharded_device", "calculate_sharded_faces", "calculate_sharded_faces_device",
+           "cell_chunks", "cell_range", "device_neighbors", "device_summaries", "gather_cells_tensors",
+           "gather_summaries",
            "gather_summaries_tensors", "parse_generators", "set_generators_broadcast"]

@@ -20,11 +20,16 @@ VD_ETIMEOUT = 4
 VD_ECUDA = 5
 VD_ESTATE = 6
 VD_EIO = 7
+VD_ECANCELED = 8
 VD_PREC_FP64 = 0
 VD_PREC_MIXED = 1
+VD_FAST_SLOTS = 0
+VD_FAST_FULL = 1
+FAST_LAYOUTS = {"slots": VD_FAST_SLOTS, "full": VD_FAST_FULL}
 
 STATUS_NAMES = {VD_EINVAL: "VD_EINVAL", VD_ENOMEM: "VD_ENOMEM", VD_EOVERFLOW: "VD_EOVERFLOW",
-                VD_ETIMEOUT: "VD_ETIMEOUT", VD_ECUDA: "VD_ECUDA", VD_ESTATE: "VD_ESTATE", VD_EIO: "VD_EIO"}
+                VD_ETIMEOUT: "VD_ETIMEOUT", VD_ECUDA: "VD_ECUDA", VD_ESTATE: "VD_ESTATE", VD_EIO: "VD_EIO",
+                VD_ECANCELED: "VD_ECANCELED"}
 
 # every symbol the header declares, with its ctypes signature
 _d = C.POINTER(C.c_double)
@@ -56,8 +61,10 @@ SIGNATURES = {
     "vd_tess_count_generators": (C.c_int, [_vp, _szp]),
     "vd_tess_get_generators": (C.c_int, [_vp, _d]),
     "vd_tess_set_precision": (C.c_int, [_vp, C.c_int]),
+    "vd_tess_set_fast_layout": (C.c_int, [_vp, C.c_int]),
     "vd_tess_calculate": (C.c_int, [_vp]),
     "vd_tess_calculate_range": (C.c_int, [_vp, C.c_size_t, C.c_size_t]),
+    "vd_tess_calculate_strided": (C.c_int, [_vp, C.c_size_t, C.c_size_t, C.c_size_t, C.c_size_t, C.c_size_t]),
     "vd_tess_relax": (C.c_int, [_vp]),
     "vd_tess_calculate_sealed": (C.c_int, [_vp]),
     "vd_tess_prune_boundaries": (C.c_int, [_vp]),
@@ -76,6 +83,7 @@ SIGNATURES = {
     "vd_grid_bin_index": (C.c_int, [_d, _d, C.c_int, C.c_int, C.c_int, _d, _szp]),
     "vd_tess_export_cells": (C.c_int, [_vp, C.c_size_t, C.c_size_t, _i64p, _i64p, _i64p, _vp, _vp, _vp, _vp]),
     "vd_tess_device_results": (C.c_int, [_vp, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp)]),
+    "vd_tess_device_neighbors": (C.c_int, [_vp, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp), C.POINTER(C.c_int64)]),
     "vd_tess_stream": (C.c_int, [_vp, C.POINTER(_vp)]),
     "vd_tess_timings": (C.c_int, [_vp, C.POINTER(C.c_float)]),
     "vd_tess_counters": (C.c_int, [_vp, _u64p]),
@@ -91,6 +99,7 @@ SIGNATURES = {
     "vd_batch_add": (C.c_int, [_vp, _d, _d, C.c_int, C.c_int, C.c_int, _vp, C.c_int, _d, C.c_size_t,
                                C.POINTER(C.c_int)]),
     "vd_batch_set_precision": (C.c_int, [_vp, C.c_int]),
+    "vd_batch_set_fast_layout": (C.c_int, [_vp, C.c_int]),
     "vd_batch_set_instrumentation": (C.c_int, [_vp, C.c_int]),
     "vd_batch_commit": (C.c_int, [_vp]),
     "vd_batch_calculate": (C.c_int, [_vp]),
@@ -114,6 +123,12 @@ SIGNATURES = {
     "vd_server_take": (C.c_int, [_vp, C.c_uint64, _vp, _vp, _vp]),
     "vd_server_stats": (C.c_int, [_vp, _u64p, _u64p, _d, _d, _szp]),
     "vd_server_reset_stats": (C.c_int, [_vp]),
+    "vd_server_concurrency": (C.c_int, [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "vd_server_set_face_results": (C.c_int, [_vp, C.c_int]),
+    "vd_server_total_faces": (C.c_int, [_vp, C.c_uint64, C.POINTER(C.c_int64)]),
+    "vd_server_take_faces": (C.c_int, [_vp, C.c_uint64, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "vd_server_cancel": (C.c_int, [_vp, C.c_uint64]),
+    "vd_debug_fail_allocations": (C.c_int, [C.c_int]),
     "vd_cell_last_error": (C.c_char_p, [_vp]),
     "vd_cell_create_box": (C.c_int, [C.c_size_t, _d, _d, C.POINTER(_vp)]),
     "vd_cell_create": (C.c_int, [C.c_size_t, C.c_int32, C.c_int32, _vp, _vp, _vp, _vp, C.POINTER(_vp)]),

@@ -13,7 +13,7 @@ from typing import List, Sequence
 
 import numpy as np
 
-from ._lib import VD_PREC_FP64, VD_PREC_MIXED, VoronoidError, load
+from ._lib import FAST_LAYOUTS, VD_PREC_FP64, VD_PREC_MIXED, VoronoidError, load
 from .tessellation import (BoundingBox, ConeGeometry, CylinderGeometry, PlaneGeometry, SphereGeometry,
                            TorusGeometry, Wall)
 
@@ -113,6 +113,10 @@ class TessellationBatch:
 
     def set_precision(self, precision: str):
         self._chk(self._L.vd_batch_set_precision(self._h, {"fp64": VD_PREC_FP64, "mixed": VD_PREC_MIXED}[precision]))
+
+    def set_fast_layout(self, layout: str):
+        """'slots' (default) or 'full': the first tier's polytope layout."""
+        self._chk(self._L.vd_batch_set_fast_layout(self._h, FAST_LAYOUTS[layout]))
 
     def set_instrumentation(self, on: bool):
         self._chk(self._L.vd_batch_set_instrumentation(self._h, 1 if on else 0))

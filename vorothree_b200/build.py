@@ -24,6 +24,7 @@ COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=o
 SOURCES = [
     ("vd_kernels_fp64.cu", False),
     ("vd_kernels_mixed.cu", False),
+    ("vd_kernels_sparse.cu", False),
     ("vd_host.cu", False),
     ("vd_measure.cu", True),
     ("vd_noalloc.cu", False),

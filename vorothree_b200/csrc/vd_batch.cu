@@ -41,6 +41,7 @@ struct Buf {
     if (p) cudaFree(p);
     p = nullptr;
     cap = 0;
+    if (vd::injected_alloc_failure()) return cudaErrorMemoryAllocation;
     const size_t want = std::max<size_t>(n, 1);
     cudaError_t e = cudaMalloc(&p, want * sizeof(T));
     if (e == cudaSuccess) cap = want;
@@ -208,6 +209,8 @@ struct vd_batch {
   std::vector<uint32_t> h_in_off, h_bin_off, h_off;
   ClipLaunchInfo info64{}, infomx{}, infomed{};
   int blocks64 = 0, blocksmx = 0;  // resident blocks per SM of the batched fast kernels
+  int blockssp64 = 0, blocksspmx = 0;  // the same on the slot layout
+  int fast_layout = VD_FAST_SLOTS;
 
   Buf<double> d_in, d_gen, d_vol, d_cen, d_farea, d_pool_area;
   Buf<uint32_t> d_flags, d_pos, d_off, d_off_next, d_in_off, d_total, d_bin_off, d_bin_of, d_counts, d_start,
@@ -408,9 +411,14 @@ int clip_chain(vd_batch* b, const uint32_t* items, uint32_t nitems) {
   W.counters = b->d_counters.p;
   W.tess_flags = b->d_tess_flags.p;
   const bool mixed = b->precision == VD_PREC_MIXED;
-  const int nblocks = std::max(1, b->num_sms * std::max(1, mixed ? b->blocksmx : b->blocks64));
-  B_CK(b, mixed ? launch_clip_mixed_fast_batched(b->d_descs.p, b->d_off.p, nt, W, nblocks, b->instrument, s)
-                : launch_clip_fp64_fast_batched(b->d_descs.p, b->d_off.p, nt, W, nblocks, b->instrument, s));
+  if (b->fast_layout == VD_FAST_SLOTS) {
+    const int nblocks = std::max(1, b->num_sms * std::max(1, mixed ? b->blocksspmx : b->blockssp64));
+    B_CK(b, launch_clip_sparse_batched(b->d_descs.p, b->d_off.p, nt, W, nblocks, b->instrument, mixed, s));
+  } else {
+    const int nblocks = std::max(1, b->num_sms * std::max(1, mixed ? b->blocksmx : b->blocks64));
+    B_CK(b, mixed ? launch_clip_mixed_fast_batched(b->d_descs.p, b->d_off.p, nt, W, nblocks, b->instrument, s)
+                  : launch_clip_fp64_fast_batched(b->d_descs.p, b->d_off.p, nt, W, nblocks, b->instrument, s));
+  }
   // medium capacity (FP64; the same decisions as both precisions)
   WorkList W2 = W;
   W2.items = b->d_list0.p;
@@ -566,6 +574,8 @@ int vd_batch_create(vd_batch** out) {
   if (e == cudaSuccess) e = clip_med_setup(&b->infomed);
   if (e == cudaSuccess) e = clip_fp64_batched_setup(&b->blocks64);
   if (e == cudaSuccess) e = clip_mixed_batched_setup(&b->blocksmx);
+  if (e == cudaSuccess) e = clip_sparse_batched_setup(false, &b->blockssp64);
+  if (e == cudaSuccess) e = clip_sparse_batched_setup(true, &b->blocksspmx);
   if (e == cudaSuccess) e = cudaEventCreate(&b->ev0);
   if (e == cudaSuccess) e = cudaEventCreate(&b->ev1);
   if (e != cudaSuccess) {
@@ -634,6 +644,14 @@ int vd_batch_set_precision(vd_batch* b, int precision) {
   if (!b) return VD_EINVAL;
   if (precision != VD_PREC_FP64 && precision != VD_PREC_MIXED) return bfail(b, VD_EINVAL, "unknown precision");
   b->precision = precision;
+  drop_graph(b);  // the captured step uses the previous kernel
+  return VD_OK;
+}
+
+int vd_batch_set_fast_layout(vd_batch* b, int layout) {
+  if (!b) return VD_EINVAL;
+  if (layout != VD_FAST_SLOTS && layout != VD_FAST_FULL) return bfail(b, VD_EINVAL, "unknown fast-tier layout");
+  b->fast_layout = layout;
   drop_graph(b);  // the captured step uses the previous kernel
   return VD_OK;
 }

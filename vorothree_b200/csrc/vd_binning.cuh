@@ -380,15 +380,16 @@ __global__ void k_relax(const double* __restrict__ gen, const int32_t* __restric
   }
 }
 
-// ---- cell-id ranges (calculate_range) ------------------------------------------
+// ---- cell-id ranges (calculate_range, calculate_strided) ---------------------
 // flags[k] = 1 when the generator at bin-order position k has an id in
-// [begin, end); the scan of the flags then lists the range in bin order, so a
-// shard's warps still walk neighbouring cells one after another.
+// [begin, end) whose chunk index (id - begin) / chunk is phase modulo stride;
+// the scan of the flags then lists those cells in bin order, so a shard's
+// warps still walk neighbouring cells one after another.
 __global__ void k_range_flags(const SortedGen* __restrict__ sorted, size_t n, long long begin, long long end,
-                              uint32_t* __restrict__ flags) {
+                              long long chunk, long long stride, long long phase, uint32_t* __restrict__ flags) {
   for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
     const long long id = sorted[k].id;
-    flags[k] = (id >= begin && id < end) ? 1u : 0u;
+    flags[k] = (id >= begin && id < end && ((id - begin) / chunk) % stride == phase) ? 1u : 0u;
   }
 }
 

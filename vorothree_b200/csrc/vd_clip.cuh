@@ -88,8 +88,12 @@ struct alignas(2 * sizeof(V)) VPair {
   V s, e;
 };
 
+struct PolyState;
+
 template <class C>
 struct alignas(16) WarpPoly {
+  using State = PolyState;
+  static constexpr bool kExport = true;  // vertices in the reference's order: exportable
   double vx[C::VCAP], vy[C::VCAP], vz[C::VCAP];
   // plain path: the FP64 signed distances of the current clip
   double dist[C::MIXED ? 1 : C::VCAP];
@@ -124,6 +128,8 @@ struct PolyState {
   int nv, nf, nh, cb;
   double umax;  // mixed path: bound on |v - g| (max norm) over the vertices
 };
+
+__device__ __forceinline__ bool state_empty(const PolyState& S) { return S.nv == 0; }
 
 __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
 
@@ -681,8 +687,8 @@ __device__ int warp_clip(WarpPoly<C>& P, PolyState& S, double px, double py, dou
 // instrumented runs: the candidates of the bins the walk opens when it
 // reaches entries (elo, ehi] of this chunk at radius^2 c4/4 -- every member
 // but the cell's own generator (algo_3d_grid.rs:190-196)
-template <class C>
-__device__ __forceinline__ void count_opened(WarpPoly<C>& P, int elo, int ehi, bool valid, bool inr, bool own,
+template <class PolyT>
+__device__ __forceinline__ void count_opened(PolyT& P, int elo, int ehi, bool valid, bool inr, bool own,
                                              double md2, double b2, uint32_t members, double c4) {
   const int l = (int)lane_id();
   const bool open = l > elo && l <= ehi && valid && inr && !(md2 > c4) && b2 <= c4;
@@ -706,8 +712,8 @@ __device__ __forceinline__ void count_opened(WarpPoly<C>& P, int elo, int ehi, b
 //    the current R; the bin being processed already opened;
 //  - a member is clipped with when dist^2 <= 4R^2 at its turn.
 // Each clip may shrink R, and the ballots are re-evaluated after it.
-template <class C>
-__device__ int compute_cell(const TessDesc& T, uint32_t i, WarpPoly<C>& P, PolyState& S) {
+template <class C, class PolyT>
+__device__ int compute_cell(const TessDesc& T, uint32_t i, PolyT& P, typename PolyT::State& S) {
   const unsigned lane = lane_id();
   const double gx = T.gen[3 * (size_t)i], gy = T.gen[3 * (size_t)i + 1], gz = T.gen[3 * (size_t)i + 2];
   double r2;
@@ -736,7 +742,7 @@ __device__ int compute_cell(const TessDesc& T, uint32_t i, WarpPoly<C>& P, PolyS
         if (r == kClipOverflow) return kCellOverflow;
       }
     }
-    if (S.nv == 0) return kCellOk;
+    if (state_empty(S)) return kCellOk;
   }
   double cur = poly_max_radius_sq(P, S, gx, gy, gz);
 
@@ -990,8 +996,8 @@ __device__ void export_cell(const WorkList& W, const WarpPoly<C>& P, const PolyS
 }
 
 // Persistent warps pull cells from the work list and build them.
-template <class C>
-__device__ void clip_worker(const TessDesc& T, const WorkList& W, WarpPoly<C>& P) {
+template <class C, class PolyT>
+__device__ void clip_worker(const TessDesc& T, const WorkList& W, PolyT& P) {
   const unsigned lane = lane_id();
   if constexpr (C::COUNT) {
     if (lane < kNumCounters) P.cnt[lane] = 0;
@@ -1003,11 +1009,13 @@ __device__ void clip_worker(const TessDesc& T, const WorkList& W, WarpPoly<C>& P
     idx = __shfl_sync(kFull, idx, 0);
     if (idx >= W.nitems) break;
     const uint32_t cell = W.items ? W.items[idx] : (uint32_t)T.sorted[idx].id;
-    PolyState S;
+    typename PolyT::State S;
     const int st = compute_cell<C>(T, cell, P, S);
     if (st == kCellOk) {
       finalize_cell<C>(T, cell, P, S);
-      if (W.ex_verts) export_cell<C>(W, P, S);
+      if constexpr (PolyT::kExport) {
+        if (W.ex_verts) export_cell<C>(W, P, S);
+      }
     } else if (lane == 0) {
       T.status[cell] = (uint8_t)st;
       if (st == kCellOverflow && W.ovf_list) W.ovf_list[atomicAdd(W.ovf_count, 1u)] = cell;
@@ -1034,9 +1042,9 @@ __device__ __forceinline__ int find_tess(const uint32_t* tess_off, int ntess, ui
   return lo;
 }
 
-template <class C>
+template <class C, class PolyT>
 __device__ void clip_worker_batched(const TessDesc* descs, const uint32_t* tess_off, int ntess,
-                                    const WorkList& W, WarpPoly<C>& P) {
+                                    const WorkList& W, PolyT& P) {
   const unsigned lane = lane_id();
   if constexpr (C::COUNT) {
     if (lane < kNumCounters) P.cnt[lane] = 0;
@@ -1052,7 +1060,7 @@ __device__ void clip_worker_batched(const TessDesc* descs, const uint32_t* tess_
     const int t = find_tess(tess_off, ntess, item);
     const TessDesc& T = descs[t];
     const uint32_t cell = (uint32_t)T.sorted[item].id;
-    PolyState S;
+    typename PolyT::State S;
     const int st = compute_cell<C>(T, cell, P, S);
     if (st == kCellOk) {
       finalize_cell<C>(T, cell, P, S);

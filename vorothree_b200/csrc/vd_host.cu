@@ -93,6 +93,7 @@ struct DevBuf {
     p = nullptr;
     cap = 0;
     s = stream;
+    if (vd::injected_alloc_failure()) return cudaErrorMemoryAllocation;
     const size_t want = std::max<size_t>(n, 1);
     cudaMemPool_t pool;
     cudaError_t e = lib_pool(&pool);
@@ -137,6 +138,19 @@ static void unit_axis(const double axis[3], double out[3]) {
 
 namespace vd {
 void set_thread_error(const char* msg) { g_create_error = msg; }
+
+namespace {
+std::atomic<int> g_fail_allocs{0};
+}
+
+bool injected_alloc_failure() {
+  int k = g_fail_allocs.load();
+  while (k > 0)
+    if (g_fail_allocs.compare_exchange_weak(k, k - 1)) return true;
+  return false;
+}
+
+void set_scratch_caps(vd_tess* t, size_t big_warps, size_t huge_blocks);
 
 cudaError_t reserve_pool(size_t bytes, cudaStream_t s) {
   cudaMemPool_t pool;
@@ -241,6 +255,8 @@ struct vd_tess {
   bool csr_valid = false;
   long long csr_total = 0;
   size_t range_begin = 0, range_end = 0;  // cells computed by the last calculate
+  // ... of which those with ((id - range_begin) / range_chunk) % range_stride == range_phase
+  size_t range_chunk = 1, range_stride = 1, range_phase = 0;
 
   // control
   DevBuf<unsigned int> d_ctl;
@@ -248,6 +264,9 @@ struct vd_tess {
   DevBuf<uint32_t> d_list[3];
   DevBuf<unsigned char> d_big, d_huge;
   size_t big_warps = 0, huge_blocks = 0;
+  // most warps / blocks the large and huge tiers may hold scratch for (the
+  // persistent kernels take any number; a server bounds a slot's scratch)
+  size_t big_warps_cap = (size_t)-1, huge_blocks_cap = (size_t)-1;
   long long pool_cap = 0;
   // the pool cursor as the host last read it (after every clip pass)
   unsigned long long pool_used = 0;
@@ -286,7 +305,8 @@ struct vd_tess {
   float timings[4] = {0, 0, 0, 0};
   unsigned long long counters[kNumCounters] = {};
   unsigned long long fallback[2] = {0, 0};
-  ClipLaunchInfo info64{}, infomx{}, infomed{};
+  ClipLaunchInfo info64{}, infomx{}, infomed{}, infosp64{}, infospmx{};
+  int fast_layout = VD_FAST_SLOTS;
   int num_sms = 0;
 };
 
@@ -500,6 +520,7 @@ int ensure_big(vd_tess* t, size_t cells) {
   // enough warps to spread the listed cells, capped to bound the scratch
   // the big kernel runs 4 warps per block: scratch covers whole blocks
   size_t want = std::min<size_t>(std::max<size_t>(cells, 1), (size_t)std::max(1, t->num_sms) * 4);
+  want = std::min(want, std::max<size_t>(t->big_warps_cap, 4));
   want = (want + 3) / 4 * 4;
   if (t->big_warps < want) {
     VD_CK(t, t->d_big.ensure(want * t->info64.big_scratch_per_warp, t->stream));
@@ -549,7 +570,8 @@ int ensure_pool(vd_tess* t, size_t cells, long long faces_per_cell) {
 
 int ensure_huge(vd_tess* t, size_t cells) {
   // a few blocks: each holds a multi-megabyte polytope in global memory
-  const size_t want = std::min<size_t>(std::max<size_t>(cells, 1), (size_t)kHugeBlocksMax);
+  const size_t want = std::min<size_t>(std::min<size_t>(std::max<size_t>(cells, 1), (size_t)kHugeBlocksMax),
+                                       std::max<size_t>(t->huge_blocks_cap, 1));
   if (t->huge_blocks != want) {
     VD_CK(t, t->d_huge.ensure(want * clip_huge_scratch_per_block(), t->stream));
     t->huge_blocks = want;
@@ -588,12 +610,18 @@ int clip_pass(vd_tess* t, int tier, const uint32_t* items, uint32_t nitems, uint
     g_launches++;
   } else if (tier == 0) {
     const bool mixed = t->precision == VD_PREC_MIXED;
-    const ClipLaunchInfo& li = mixed ? t->infomx : t->info64;
+    // the slot layout cannot export a polytope in the reference's vertex
+    // order: get_cell's rebuild runs the full-rewrite kernel
+    const bool slots = t->fast_layout == VD_FAST_SLOTS && !W.ex_verts;
+    const ClipLaunchInfo& li = slots ? (mixed ? t->infospmx : t->infosp64) : (mixed ? t->infomx : t->info64);
     const size_t warps_needed = (nitems + li.warps_per_block - 1) / li.warps_per_block;
     const int nblocks = (int)std::max<size_t>(
         1, std::min<size_t>(warps_needed, (size_t)t->num_sms * std::max(1, li.blocks_per_sm)));
-    VD_CK(t, mixed ? launch_clip_mixed_fast(T, W, nblocks, t->instrument, s)
-                   : launch_clip_fp64_fast(T, W, nblocks, t->instrument, s));
+    if (slots)
+      VD_CK(t, launch_clip_sparse(T, W, nblocks, t->instrument, mixed, s));
+    else
+      VD_CK(t, mixed ? launch_clip_mixed_fast(T, W, nblocks, t->instrument, s)
+                     : launch_clip_fp64_fast(T, W, nblocks, t->instrument, s));
     g_launches++;
   } else if (tier == 2) {
     int r = ensure_big(t, nitems);
@@ -628,6 +656,20 @@ int read_ctl(vd_tess* t, unsigned int* ovf, unsigned int* tab) {
   return VD_OK;
 }
 
+// cells of [begin, end) whose chunk index (id - begin) / chunk is phase
+// modulo stride
+size_t strided_count(const size_t* range) {
+  const size_t len = range[1] - range[0], chunk = range[2], stride = range[3], phase = range[4];
+  const size_t period = chunk * stride, full = len / period, rest = len % period;
+  const size_t lo = phase * chunk;
+  return full * chunk + (rest > lo ? std::min(chunk, rest - lo) : 0);
+}
+
+bool cell_computed(const vd_tess* t, size_t i) {
+  return i >= t->range_begin && i < t->range_end &&
+         ((i - t->range_begin) / t->range_chunk) % t->range_stride == t->range_phase;
+}
+
 // Runs the fast pass over all cells, then resolves the cells it could not
 // finish: a longer search order for cells that walked off a truncated one,
 // the large-capacity pass for polytopes that outgrew shared memory.
@@ -636,6 +678,8 @@ int read_ctl(vd_tess* t, unsigned int* ovf, unsigned int* tab) {
 // cells with ids in [range[0], range[1]) and clear the others.
 int run_calculate(vd_tess* t, const WorkList* extra = nullptr, const uint32_t* only_cell = nullptr,
                   const size_t* range = nullptr) {
+  // range: {begin, end, chunk, stride, phase} -- the cells with ids in
+  // [begin, end) and ((id - begin) / chunk) % stride == phase
   cudaStream_t s = t->stream;
   const size_t n = t->ngen;
   int r = ensure_outputs(t, n);
@@ -668,7 +712,7 @@ int run_calculate(vd_tess* t, const WorkList* extra = nullptr, const uint32_t* o
   if (only_cell) {
     VD_CK(t, cudaMemcpyAsync(t->d_list[2].p, only_cell, sizeof(uint32_t), cudaMemcpyHostToDevice, s));
     in_list = t->d_list[2].p;
-  } else if (range && (range[0] > 0 || range[1] < n)) {
+  } else if (range && (range[0] > 0 || range[1] < n || range[3] > 1)) {
     VD_CK(t, t->d_flags.ensure(n + 1, t->stream));
     VD_CK(t, t->d_pos.ensure(n + 1, t->stream));
     if (n) {
@@ -676,7 +720,8 @@ int run_calculate(vd_tess* t, const WorkList* extra = nullptr, const uint32_t* o
       g_launches++;
       VD_CK(t, cudaGetLastError());
       k_range_flags<<<grid_blocks(t, n, 256), 256, 0, s>>>(t->d_sorted.p, n, (long long)range[0],
-                                                           (long long)range[1], t->d_flags.p);
+                                                           (long long)range[1], (long long)range[2],
+                                                           (long long)range[3], (long long)range[4], t->d_flags.p);
       g_launches++;
       VD_CK(t, cudaGetLastError());
     }
@@ -690,7 +735,7 @@ int run_calculate(vd_tess* t, const WorkList* extra = nullptr, const uint32_t* o
       VD_CK(t, cudaGetLastError());
     }
     in_list = t->d_list[2].p;
-    nin = (uint32_t)(range[1] - range[0]);
+    nin = (uint32_t)strided_count(range);
   }
   if (nin > 0) {
     r = clip_pass(t, 0, in_list, nin, t->d_list[0].p, t->d_list[1].p, extra);
@@ -949,6 +994,13 @@ int check_ready(vd_tess* t) {
 
 }  // namespace
 
+namespace vd {
+void set_scratch_caps(vd_tess* t, size_t big_warps, size_t huge_blocks) {
+  t->big_warps_cap = big_warps;
+  t->huge_blocks_cap = huge_blocks;
+}
+}  // namespace vd
+
 extern "C" {
 
 const char* vd_last_error(const vd_tess* t) { return t ? t->err.c_str() : g_create_error.c_str(); }
@@ -959,6 +1011,13 @@ int vd_tess_create(const double bmin[3], const double bmax[3], int nx, int ny, i
   if (nx <= 0 || ny <= 0 || nz <= 0 || nx > 16000 || ny > 16000 || nz > 16000)
     return fail(nullptr, VD_EINVAL, "grid resolution must be in [1, 16000]");
   if ((double)nx * ny * nz > 2.0e9) return fail(nullptr, VD_EINVAL, "too many bins");
+  // A box without a positive, finite extent on every axis has no grid (the
+  // reference's bin scale n / (max - min) would be infinite or NaN).
+  for (int a = 0; a < 3; ++a)
+    if (!(bmax[a] > bmin[a]) || !std::isfinite(bmin[a]) || !std::isfinite(bmax[a]) ||
+        !std::isfinite(bmax[a] - bmin[a]))
+      return fail(nullptr, VD_EINVAL, "bounding box axis %d: [%g, %g] has no positive finite extent", a, bmin[a],
+                  bmax[a]);
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return fail(nullptr, VD_ECUDA, "no CUDA device: %s", cudaGetErrorString(e));
@@ -973,6 +1032,8 @@ int vd_tess_create(const double bmin[3], const double bmax[3], int nx, int ny, i
   for (auto& ev : t->ev) cudaEventCreate(&ev);
   e = clip_fp64_info(&t->info64);
   if (e == cudaSuccess) e = clip_mixed_info(&t->infomx);
+  if (e == cudaSuccess) e = clip_sparse_info(false, &t->infosp64);
+  if (e == cudaSuccess) e = clip_sparse_info(true, &t->infospmx);
   if (e == cudaSuccess) e = clip_med_setup(&t->infomed);
   if (e == cudaSuccess) e = seal_setup();
   if (e != cudaSuccess) {
@@ -1011,6 +1072,11 @@ int vd_tess_reset(vd_tess* t, const double bmin[3], const double bmax[3], int nx
   if (nx <= 0 || ny <= 0 || nz <= 0 || nx > 16000 || ny > 16000 || nz > 16000)
     return fail(t, VD_EINVAL, "grid resolution must be in [1, 16000]");
   if ((double)nx * ny * nz > 2.0e9) return fail(t, VD_EINVAL, "too many bins");
+  for (int a = 0; a < 3; ++a)
+    if (!(bmax[a] > bmin[a]) || !std::isfinite(bmin[a]) || !std::isfinite(bmax[a]) ||
+        !std::isfinite(bmax[a] - bmin[a]))
+      return fail(t, VD_EINVAL, "bounding box axis %d: [%g, %g] has no positive finite extent", a, bmin[a],
+                  bmax[a]);
   VD_CK(t, cudaSetDevice(t->device));
   Grid& g = t->grid;
   const int n[3] = {nx, ny, nz};
@@ -1477,6 +1543,18 @@ int vd_tess_set_precision(vd_tess* t, int precision) {
   return VD_OK;
 }
 
+int vd_debug_fail_allocations(int count) {
+  g_fail_allocs.store(count > 0 ? count : 0);
+  return VD_OK;
+}
+
+int vd_tess_set_fast_layout(vd_tess* t, int layout) {
+  if (!t) return VD_EINVAL;
+  if (layout != VD_FAST_SLOTS && layout != VD_FAST_FULL) return fail(t, VD_EINVAL, "unknown fast-tier layout");
+  t->fast_layout = layout;
+  return VD_OK;
+}
+
 int vd_tess_set_instrumentation(vd_tess* t, int on) {
   if (!t) return VD_EINVAL;
   t->instrument = on != 0;
@@ -1495,18 +1573,24 @@ int vd_tess_calculate(vd_tess* t) {
   t->ncells = t->ngen;
   t->range_begin = 0;
   t->range_end = t->ngen;
+  t->range_chunk = 1;
+  t->range_stride = 1;
+  t->range_phase = 0;
   t->calculated = true;
   return VD_OK;
 }
 
-int vd_tess_calculate_range(vd_tess* t, size_t begin, size_t end) {
+int vd_tess_calculate_strided(vd_tess* t, size_t begin, size_t end, size_t chunk, size_t stride, size_t phase) {
   if (!t) return VD_EINVAL;
   if (begin > end || end > t->ngen)
     return fail(t, VD_EINVAL, "cell range [%zu, %zu) is not inside [0, %zu)", begin, end, t->ngen);
+  if (chunk == 0 || stride == 0 || phase >= stride)
+    return fail(t, VD_EINVAL, "chunk %zu, stride %zu, phase %zu: need chunk >= 1 and phase < stride", chunk,
+                stride, phase);
   VD_CK(t, cudaSetDevice(t->device));
   t->calculated = false;
   t->csr_valid = false;
-  const size_t range[2] = {begin, end};
+  const size_t range[5] = {begin, end, chunk, stride, phase};
   t->sealed = false;
   t->nseal = t->nprune = t->nprune_pos = 0;
   int r = run_calculate(t, nullptr, nullptr, range);
@@ -1514,8 +1598,15 @@ int vd_tess_calculate_range(vd_tess* t, size_t begin, size_t end) {
   t->ncells = t->ngen;
   t->range_begin = begin;
   t->range_end = end;
+  t->range_chunk = chunk;
+  t->range_stride = stride;
+  t->range_phase = phase;
   t->calculated = true;
   return VD_OK;
+}
+
+int vd_tess_calculate_range(vd_tess* t, size_t begin, size_t end) {
+  return vd_tess_calculate_strided(t, begin, end, 1, 1, 0);
 }
 
 int vd_tess_calculate_sealed(vd_tess* t) {
@@ -1746,7 +1837,7 @@ int vd_tess_get_cell(vd_tess* t, size_t i, int32_t* n_vertices, int32_t* n_faces
   int r = check_ready(t);
   if (r != VD_OK) return r;
   if (i >= t->ncells) return fail(t, VD_EINVAL, "cell index %zu out of range", i);
-  if (i < t->range_begin || i >= t->range_end) {
+  if (!cell_computed(t, i)) {
     // outside the range of the last calculate_range: an empty cell
     if (n_vertices) *n_vertices = 0;
     if (n_faces) *n_faces = 0;
@@ -1829,6 +1920,9 @@ int vd_tess_export_cells(vd_tess* t, size_t begin, size_t end, int64_t* v_off, i
   if (fill && !(vertices && face_counts && face_indices && face_neighbors))
     return fail(t, VD_EINVAL, "give all four polytope arrays, or none for the sizes");
   if (end - begin > 0xFFFFFFF0ull) return fail(t, VD_EINVAL, "range too large");
+  if (t->range_stride > 1)
+    return fail(t, VD_ESTATE, "the last calculate computed interleaved chunks of cells; export after a "
+                              "calculate or calculate_range");
   cudaStream_t s = t->stream;
   const size_t n = end - begin;
   // only the cells of the last calculate's range have polytopes
@@ -1869,8 +1963,8 @@ int vd_tess_export_cells(vd_tess* t, size_t begin, size_t end, int64_t* v_off, i
     VD_CK(t, t->d_pos.ensure(all + 1, s));
     VD_CK(t, t->d_bx_items.ensure(3 * nr, s));
     VD_CK(t, t->d_bx_sizes.ensure(3 * n, s));
-    k_range_flags<<<grid_blocks(t, all, 256), 256, 0, s>>>(t->d_sorted.p, all, (long long)lo, (long long)hi,
-                                                         t->d_flags.p);
+    k_range_flags<<<grid_blocks(t, all, 256), 256, 0, s>>>(t->d_sorted.p, all, (long long)lo, (long long)hi, 1LL,
+                                                         1LL, 0LL, t->d_flags.p);
     g_launches++;
     VD_CK(t, cudaGetLastError());
     VD_CK(t, cudaMemsetAsync(t->d_flags.p + all, 0, sizeof(uint32_t), s));
@@ -1971,6 +2065,33 @@ int vd_tess_device_results(vd_tess* t, const double** d_volume, const double** d
   if (d_volume) *d_volume = t->d_vol.p;
   if (d_centroid3) *d_centroid3 = t->d_cen.p;
   if (d_n_faces) *d_n_faces = t->d_nf.p;
+  return VD_OK;
+}
+
+int vd_tess_device_neighbors(vd_tess* t, const int64_t** d_offsets, const int32_t** d_ids, const double** d_areas,
+                             int64_t* total) {
+  int r = check_ready(t);
+  if (r != VD_OK) return r;
+  r = ensure_csr(t);
+  if (r != VD_OK) return r;
+  const size_t n = t->ncells;
+  const size_t tot = (size_t)t->csr_total;
+  cudaStream_t s = t->stream;
+  VD_CK(t, t->d_csr_ids.ensure(tot, t->stream));
+  VD_CK(t, t->d_csr_area.ensure(tot, t->stream));
+  if (n && tot) {
+    const int blocks = grid_blocks(t, n * 32, 256);
+    k_csr_gather<<<blocks, 256, 0, s>>>(t->d_nf.p, n, t->d_csr_off.p, t->fout, t->d_fnb.p, t->d_farea.p,
+                                        t->d_pool_fnb.p, t->d_pool_area.p, t->d_pool_off.p, t->d_csr_ids.p,
+                                        t->d_csr_area.p);
+    g_launches++;
+    VD_CK(t, cudaGetLastError());
+  }
+  VD_CK(t, cudaStreamSynchronize(s));
+  if (d_offsets) *d_offsets = reinterpret_cast<const int64_t*>(t->d_csr_off.p);
+  if (d_ids) *d_ids = t->d_csr_ids.p;
+  if (d_areas) *d_areas = t->d_csr_area.p;
+  if (total) *total = t->csr_total;
   return VD_OK;
 }
 

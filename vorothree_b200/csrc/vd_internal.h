@@ -90,6 +90,14 @@ bool parse_generators(const char* text, size_t len, std::vector<double>* xyz, st
 // message returned by vd_last_error(NULL) on the calling thread
 void set_thread_error(const char* msg);
 
+// true when an injected allocation failure is pending (vd_debug_fail_allocations);
+// consumes it
+bool injected_alloc_failure();
+
+// the most warps of large-tier scratch and blocks of huge-tier scratch a
+// handle may hold (a server slot's bound); the kernels run with fewer
+void set_scratch_caps(vd_tess* t, size_t big_warps, size_t huge_blocks);
+
 // Reserve `bytes` in the library's memory pool on the current device (an
 // allocation freed at once; the pool keeps freed memory), so that later
 // buffer growth is served from the pool without going to the driver.
@@ -115,6 +123,16 @@ cudaError_t launch_prune_log_place(const PruneRec* rec, uint32_t nrec, const Pru
 
 // Mixed path (vd_kernels_mixed.cu)
 cudaError_t clip_mixed_info(ClipLaunchInfo* info);
+
+// the shared-memory tier on the slot layout (vd_kernels_sparse.cu): a
+// modifying clip rewrites only the faces that lose a vertex; cells it cannot
+// finish are listed as overflowing, for the medium tier
+cudaError_t clip_sparse_info(bool mixed, ClipLaunchInfo* info);
+cudaError_t launch_clip_sparse(const TessDesc& T, const WorkList& W, int nblocks, bool count, bool mixed,
+                               cudaStream_t s);
+cudaError_t clip_sparse_batched_setup(bool mixed, int* blocks_per_sm);
+cudaError_t launch_clip_sparse_batched(const TessDesc* descs, const uint32_t* tess_off, int ntess, const WorkList& W,
+                                       int nblocks, bool count, bool mixed, cudaStream_t s);
 cudaError_t launch_clip_mixed_fast(const TessDesc& T, const WorkList& W, int nblocks, bool count,
                                    cudaStream_t s);
 

@@ -1,0 +1,101 @@
+// vd_kernels_sparse.cu -- the shared-memory tier on the slot layout
+// (vd_clip_sparse.cuh): plain FP64 and mixed-precision classification,
+// single tessellations and batches.
+//
+// Compiled with -fmad=false like every FP64 path: the reference never fuses
+// a multiply and an add, so neither may this one.
+#include "vd_clip_sparse.cuh"
+#include "vd_internal.h"
+
+namespace vd {
+
+// blocks of 4 warps per SM the register budget must admit (shared memory
+// admits this many too)
+constexpr int kSparseMinBlocks = 7;
+constexpr int kSparseMixedMinBlocks = 7;
+constexpr int kSparseBatchMinBlocks = 6;
+
+namespace {
+
+template <class C, int MINB>
+cudaError_t setup_one(ClipLaunchInfo* info) {
+  const size_t smem = sizeof(SparsePoly<C>) * kFastWarpsPerBlock;
+  cudaError_t e = cudaFuncSetAttribute(k_clip_sparse<C, kFastWarpsPerBlock, MINB>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess || !info) return e;
+  info->smem_per_warp = sizeof(SparsePoly<C>);
+  info->warps_per_block = kFastWarpsPerBlock;
+  info->big_scratch_per_warp = 0;
+  int nb = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_clip_sparse<C, kFastWarpsPerBlock, MINB>,
+                                                    kFastWarpsPerBlock * 32, smem);
+  info->blocks_per_sm = nb;
+  return e;
+}
+
+template <class C, int MINB>
+cudaError_t setup_batched(int* blocks_per_sm) {
+  const size_t smem = sizeof(SparsePoly<C>) * kFastWarpsPerBlock;
+  cudaError_t e = cudaFuncSetAttribute(k_clip_sparse_batched<C, kFastWarpsPerBlock, MINB>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess || !blocks_per_sm) return e;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      blocks_per_sm, k_clip_sparse_batched<C, kFastWarpsPerBlock, MINB>, kFastWarpsPerBlock * 32, smem);
+}
+
+template <class C, int MINB>
+void launch_one(const TessDesc& T, const WorkList& W, int nblocks, cudaStream_t s) {
+  k_clip_sparse<C, kFastWarpsPerBlock, MINB>
+      <<<nblocks, kFastWarpsPerBlock * 32, sizeof(SparsePoly<C>) * kFastWarpsPerBlock, s>>>(T, W);
+}
+
+template <class C, int MINB>
+void launch_batched(const TessDesc* descs, const uint32_t* tess_off, int ntess, const WorkList& W, int nblocks,
+                    cudaStream_t s) {
+  k_clip_sparse_batched<C, kFastWarpsPerBlock, MINB>
+      <<<nblocks, kFastWarpsPerBlock * 32, sizeof(SparsePoly<C>) * kFastWarpsPerBlock, s>>>(descs, tess_off,
+                                                                                              ntess, W);
+}
+
+}  // namespace
+
+cudaError_t clip_sparse_info(bool mixed, ClipLaunchInfo* info) {
+  cudaError_t e = mixed ? setup_one<MixedSparseCount, kSparseMixedMinBlocks>(nullptr)
+                        : setup_one<FastSparseCount, kSparseMinBlocks>(nullptr);
+  if (e != cudaSuccess) return e;
+  return mixed ? setup_one<MixedSparse, kSparseMixedMinBlocks>(info) : setup_one<FastSparse, kSparseMinBlocks>(info);
+}
+
+cudaError_t launch_clip_sparse(const TessDesc& T, const WorkList& W, int nblocks, bool count, bool mixed,
+                               cudaStream_t s) {
+  if (mixed) {
+    if (count) launch_one<MixedSparseCount, kSparseMixedMinBlocks>(T, W, nblocks, s);
+    else launch_one<MixedSparse, kSparseMixedMinBlocks>(T, W, nblocks, s);
+  } else {
+    if (count) launch_one<FastSparseCount, kSparseMinBlocks>(T, W, nblocks, s);
+    else launch_one<FastSparse, kSparseMinBlocks>(T, W, nblocks, s);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t clip_sparse_batched_setup(bool mixed, int* blocks_per_sm) {
+  cudaError_t e = mixed ? setup_batched<MixedSparseCount, kSparseBatchMinBlocks>(nullptr)
+                        : setup_batched<FastSparseCount, kSparseBatchMinBlocks>(nullptr);
+  if (e != cudaSuccess) return e;
+  return mixed ? setup_batched<MixedSparse, kSparseBatchMinBlocks>(blocks_per_sm)
+               : setup_batched<FastSparse, kSparseBatchMinBlocks>(blocks_per_sm);
+}
+
+cudaError_t launch_clip_sparse_batched(const TessDesc* descs, const uint32_t* tess_off, int ntess, const WorkList& W,
+                                       int nblocks, bool count, bool mixed, cudaStream_t s) {
+  if (mixed) {
+    if (count) launch_batched<MixedSparseCount, kSparseBatchMinBlocks>(descs, tess_off, ntess, W, nblocks, s);
+    else launch_batched<MixedSparse, kSparseBatchMinBlocks>(descs, tess_off, ntess, W, nblocks, s);
+  } else {
+    if (count) launch_batched<FastSparseCount, kSparseBatchMinBlocks>(descs, tess_off, ntess, W, nblocks, s);
+    else launch_batched<FastSparse, kSparseBatchMinBlocks>(descs, tess_off, ntess, W, nblocks, s);
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace vd

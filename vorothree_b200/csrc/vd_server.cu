@@ -44,19 +44,37 @@ struct Request {
   size_t est_bytes = 0;
   Clock::time_point t_submit, t_start, t_done;
   bool done = false;
+  bool started = false;
+  bool faces = false;  // also return the neighbour-id / face-area CSR
   int status = VD_OK;
   std::string err;
   size_t ncells = 0;
   std::vector<double> vol, cen;
   std::vector<int32_t> nf;
+  std::vector<int64_t> off;
+  std::vector<int32_t> ids;
+  std::vector<double> areas;
 };
 
-// device bytes a request of n generators on b bins needs (the buffers of a
-// vd_tess: generators, bins, bin-ordered copy, per-cell outputs and 48 face
-// slots, fallback lists) plus its search order
+// scratch a slot may hold for cells beyond the shared-memory tiers: warps of
+// large-tier polytopes and blocks of huge-tier polytopes (the persistent
+// kernels run with fewer when a request has more such cells)
+constexpr size_t kSlotBigWarps = 64;
+constexpr size_t kSlotHugeBlocks = 8;
+
+// device bytes a request of n generators on b bins needs: the buffers of a
+// vd_tess (generators, bins, bin-ordered copy, per-cell outputs and 48 face
+// slots, fallback lists), its search order, the slot's bounded large- and
+// huge-tier scratch and a face pool of 2^20 slots
 size_t estimate_bytes(size_t n, size_t bins) {
   const size_t per_cell = 24 * 3 + 32 + 4 * 6 + (8 + 24 + 4 + 4 + 1 + 8) + 48 * 12 + 3 * 4 + 8;
-  return n * per_cell + bins * 16 + (1u << 20);
+  static const size_t scratch = [] {
+    vd::ClipLaunchInfo info{};
+    vd::clip_fp64_info(&info);
+    return kSlotBigWarps * info.big_scratch_per_warp + kSlotHugeBlocks * vd::clip_huge_scratch_per_block() +
+           ((size_t)1 << 20) * 12;
+  }();
+  return n * per_cell + bins * 16 + (1u << 20) + scratch;
 }
 
 double percentile(std::vector<double> v, double q) {
@@ -80,6 +98,8 @@ struct vd_server {
   std::deque<std::shared_ptr<Request>> queue;
   std::unordered_map<uint64_t, std::shared_ptr<Request>> live;
   size_t in_use = 0, peak = 0;
+  int running = 0, peak_running = 0;
+  bool face_results = false;
   uint64_t next_id = 1;
   bool stop = false;
   std::vector<std::thread> workers;
@@ -134,6 +154,17 @@ int run_request(vd_tess* t, int precision, Request& r) {
     r.nf.resize(kept);
     rc = vd_tess_get_cell_summaries(t, r.vol.data(), r.cen.data(), r.nf.data());
   }
+  if (rc == VD_OK && r.faces) {
+    int64_t total = 0;
+    rc = vd_tess_total_faces(t, &total);
+    if (rc == VD_OK) {
+      r.off.resize(kept + 1);
+      r.ids.resize((size_t)total);
+      r.areas.resize((size_t)total);
+      rc = vd_tess_get_neighbors(t, r.off.data(), r.ids.data());
+    }
+    if (rc == VD_OK) rc = vd_tess_get_face_areas(t, nullptr, r.areas.data());
+  }
   if (rc != VD_OK) r.err = vd_last_error(t);
   return rc;
 }
@@ -156,6 +187,9 @@ void worker(vd_server* s, int slot) {
       s->queue.pop_front();
       s->in_use += r->est_bytes;
       s->peak = std::max(s->peak, s->in_use);
+      s->running++;
+      s->peak_running = std::max(s->peak_running, s->running);
+      r->started = true;
       r->t_start = Clock::now();
     }
     // the next queued request may fit beside this one
@@ -164,6 +198,7 @@ void worker(vd_server* s, int slot) {
     {
       std::lock_guard<std::mutex> lock(s->mu);
       s->in_use -= r->est_bytes;
+      s->running--;
       r->status = rc;
       r->t_done = Clock::now();
       r->done = true;
@@ -211,6 +246,7 @@ int submit_points(vd_server* s, const double bmin[3], const double bmax[3], int 
     w.points = w.normals = nullptr;  // the request keeps its own copy
   }
   r->pts = std::move(pts);
+  r->faces = s->face_results;
   r->est_bytes = estimate_bytes(n, (size_t)nx * ny * nz);
   if (r->est_bytes > s->budget) return sfail(s, VD_ENOMEM, "request needs %zu bytes, budget %zu", r->est_bytes, s->budget);
   {
@@ -254,6 +290,7 @@ int vd_server_create(int slots, size_t hbm_budget_bytes, int precision, vd_serve
       delete s;
       return sfail(nullptr, rc, "slot setup: %s", m.c_str());
     }
+    vd::set_scratch_caps(t, kSlotBigWarps, kSlotHugeBlocks);
     s->handles.push_back(t);
   }
   // Reserve the budget in the library's memory pool up front (as much of it
@@ -346,6 +383,94 @@ int vd_server_take(vd_server* s, uint64_t ticket, double* volume, double* centro
   return VD_OK;
 }
 
+int vd_server_take_faces(vd_server* s, uint64_t ticket, double* volume, double* centroid3, int32_t* n_faces,
+                         int64_t* offsets, int32_t* ids, double* areas) {
+  if (!s) return VD_EINVAL;
+  std::shared_ptr<Request> r;
+  {
+    std::unique_lock<std::mutex> lock(s->mu);
+    auto it = s->live.find(ticket);
+    if (it == s->live.end()) {
+      s->err = "unknown ticket";
+      return VD_EINVAL;
+    }
+    r = it->second;
+    s->cv_done.wait(lock, [&] { return r->done; });
+    if (r->status == VD_OK && !r->faces && (offsets || ids || areas)) {
+      s->err = "the request was submitted without face results (vd_server_set_face_results)";
+      return VD_ESTATE;
+    }
+    s->live.erase(it);
+  }
+  if (r->status != VD_OK) return r->status;
+  if (volume) memcpy(volume, r->vol.data(), r->ncells * sizeof(double));
+  if (centroid3) memcpy(centroid3, r->cen.data(), 3 * r->ncells * sizeof(double));
+  if (n_faces) memcpy(n_faces, r->nf.data(), r->ncells * sizeof(int32_t));
+  if (r->faces) {
+    if (offsets) memcpy(offsets, r->off.data(), r->off.size() * sizeof(int64_t));
+    if (ids) memcpy(ids, r->ids.data(), r->ids.size() * sizeof(int32_t));
+    if (areas) memcpy(areas, r->areas.data(), r->areas.size() * sizeof(double));
+  }
+  return VD_OK;
+}
+
+int vd_server_total_faces(vd_server* s, uint64_t ticket, int64_t* total) {
+  if (!s || !total) return VD_EINVAL;
+  std::unique_lock<std::mutex> lock(s->mu);
+  auto it = s->live.find(ticket);
+  if (it == s->live.end()) {
+    s->err = "unknown ticket";
+    return VD_EINVAL;
+  }
+  std::shared_ptr<Request> r = it->second;
+  s->cv_done.wait(lock, [&] { return r->done; });
+  *total = (int64_t)r->ids.size();
+  if (r->status != VD_OK) s->err = r->err;
+  return r->status;
+}
+
+int vd_server_set_face_results(vd_server* s, int on) {
+  if (!s) return VD_EINVAL;
+  std::lock_guard<std::mutex> lock(s->mu);
+  s->face_results = on != 0;
+  return VD_OK;
+}
+
+int vd_server_cancel(vd_server* s, uint64_t ticket) {
+  if (!s) return VD_EINVAL;
+  {
+    std::lock_guard<std::mutex> lock(s->mu);
+    auto it = s->live.find(ticket);
+    if (it == s->live.end()) {
+      s->err = "unknown ticket";
+      return VD_EINVAL;
+    }
+    std::shared_ptr<Request> r = it->second;
+    if (r->started || r->done) {
+      s->err = "the request has already started";
+      return VD_ESTATE;
+    }
+    s->queue.erase(std::find(s->queue.begin(), s->queue.end(), r));
+    r->status = VD_ECANCELED;
+    r->err = "cancelled";
+    r->t_done = Clock::now();
+    r->done = true;
+    r->pts.clear();
+    r->pts.shrink_to_fit();
+  }
+  s->cv_done.notify_all();
+  s->cv_work.notify_all();  // the next request may fit now
+  return VD_OK;
+}
+
+int vd_server_concurrency(vd_server* s, int* running, int* peak_running) {
+  if (!s) return VD_EINVAL;
+  std::lock_guard<std::mutex> lock(s->mu);
+  if (running) *running = s->running;
+  if (peak_running) *peak_running = s->peak_running;
+  return VD_OK;
+}
+
 int vd_server_stats(vd_server* s, uint64_t* completed, uint64_t* cells, double* p50_s, double* p99_s,
                     size_t* peak_bytes) {
   if (!s) return VD_EINVAL;
@@ -365,6 +490,7 @@ int vd_server_reset_stats(vd_server* s) {
   s->completed = 0;
   s->cells = 0;
   s->peak = s->in_use;
+  s->peak_running = s->running;
   return VD_OK;
 }
 

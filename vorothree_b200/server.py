@@ -11,7 +11,7 @@ from typing import Sequence
 
 import numpy as np
 
-from ._lib import VD_PREC_FP64, VD_PREC_MIXED, VoronoidError, load
+from ._lib import VD_ESTATE, VD_PREC_FP64, VD_PREC_MIXED, VoronoidError, load
 from .batch import _walls
 from .tessellation import BoundingBox, Wall
 
@@ -84,6 +84,45 @@ class TessellationServer:
         self._chk(self._L.vd_server_take(self._h, C.c_uint64(ticket), C.c_void_p(vol.ctypes.data),
                                          C.c_void_p(cen.ctypes.data), C.c_void_p(nf.ctypes.data)))
         return vol, cen, nf
+
+    def set_face_results(self, on: bool = True):
+        """Requests submitted afterwards also return each cell's neighbour ids
+        and face areas (take_faces)."""
+        self._chk(self._L.vd_server_set_face_results(self._h, 1 if on else 0))
+
+    def take_faces(self, ticket: int):
+        """(volume, centroid, n_faces, offsets[n+1], neighbour ids, face areas)
+        of a request submitted with face results; releases the request."""
+        n, _ = self.wait(ticket)
+        tot = C.c_int64()
+        self._chk(self._L.vd_server_total_faces(self._h, C.c_uint64(ticket), C.byref(tot)))
+        vol = np.zeros(n, np.float64)
+        cen = np.zeros((n, 3), np.float64)
+        nf = np.zeros(n, np.int32)
+        off = np.zeros(n + 1, np.int64)
+        ids = np.zeros(max(tot.value, 1), np.int32)
+        ar = np.zeros(max(tot.value, 1), np.float64)
+        vp = C.c_void_p
+        self._chk(self._L.vd_server_take_faces(self._h, C.c_uint64(ticket), vp(vol.ctypes.data), vp(cen.ctypes.data),
+                                               vp(nf.ctypes.data), vp(off.ctypes.data), vp(ids.ctypes.data),
+                                               vp(ar.ctypes.data)))
+        return vol, cen, nf, off, ids[:tot.value], ar[:tot.value]
+
+    def cancel(self, ticket: int) -> bool:
+        """Drop a request still in the queue (True); False when it has already
+        started (it runs to completion)."""
+        rc = self._L.vd_server_cancel(self._h, C.c_uint64(ticket))
+        if rc == VD_ESTATE:
+            return False
+        self._chk(rc)
+        return True
+
+    def concurrency(self) -> dict:
+        """Requests on the GPU now, and the most at once since reset_stats."""
+        run = C.c_int()
+        peak = C.c_int()
+        self._chk(self._L.vd_server_concurrency(self._h, C.byref(run), C.byref(peak)))
+        return {"running": run.value, "peak_running": peak.value}
 
     def stats(self) -> dict:
         done = C.c_uint64()

@@ -21,7 +21,7 @@ CUDA tensors on every rank and never pass through host memory.
 from __future__ import annotations
 
 import ctypes as C
-from typing import Optional, Tuple
+from typing import List, Optional, Tuple
 
 import numpy as np
 
@@ -34,6 +34,21 @@ def cell_range(n: int, rank: int, world: int) -> Tuple[int, int]:
     q, r = divmod(n, world)
     begin = rank * q + min(rank, r)
     return begin, begin + q + (1 if rank < r else 0)
+
+
+def cell_chunks(n: int, rank: int, world: int, chunk: int) -> List[Tuple[int, int]]:
+    """The id ranges of this rank in an interleaved split: chunk k of
+    [0, n) (ids [k chunk, (k + 1) chunk)) belongs to rank k % world.  Every
+    rank gets an equal share of every part of the id order, so an input whose
+    cost varies along it -- the clustered configuration lists its 64 blobs'
+    generators first and the background after -- keeps the ranks balanced."""
+    if world <= 0 or not 0 <= rank < world or n < 0 or chunk <= 0:
+        raise ValueError(f"bad shard: n={n} rank={rank} world={world} chunk={chunk}")
+    return [(b, min(b + chunk, n)) for b in range(rank * chunk, n, world * chunk)]
+
+
+def chunk_count(n: int, rank: int, world: int, chunk: int) -> int:
+    return sum(e - b for b, e in cell_chunks(n, rank, world, chunk))
 
 
 def _device_for(group):
@@ -194,3 +209,150 @@ def set_generators_broadcast(tess, points=None, src: int = 0, group=None) -> int
     kept = tess.set_generators_device(buf.data_ptr(), buf.shape[0])
     torch.cuda.synchronize()
     return kept
+
+
+def gather_cells_tensors(vol, cen, nfaces, n: int, chunk: int, group=None, ids=None, areas=None):
+    """The all-gather of an interleaved split (cell_chunks): rank r passes the
+    results of its cells in id order -- vol[k], cen[k], nfaces[k] and, when
+    ids / areas are given, the concatenation of those cells' neighbour ids and
+    face areas (nfaces[k] each, face order) -- as tensors on the process
+    group's device.  Every rank gets the full arrays on that device:
+    (vol[n], cen[n, 3], nfaces[n]) and, with ids / areas, the CSR
+    (offsets[n + 1] int64, ids int32, areas float64) of the whole
+    tessellation, as Tessellation.neighbors / face_areas give it.  One
+    all-gather of a padded (width, 5) float64 block; with faces, one of the
+    face totals and one each of the padded ids and areas."""
+    import torch
+    import torch.distributed as dist
+    world = dist.get_world_size(group)
+    rank = dist.get_rank(group)
+    counts = [chunk_count(n, r, world, chunk) for r in range(world)]
+    k = counts[rank]
+    if vol.shape[0] != k or cen.shape[0] != k or nfaces.shape[0] != k:
+        raise ValueError(f"rank {rank} holds {vol.shape[0]} cells, its chunks have {k}")
+    dev = vol.device
+    width = max(counts) if counts else 0
+    pack = torch.zeros((width, 5), dtype=torch.float64, device=dev)
+    pack[:k, 0] = vol
+    pack[:k, 1:4] = cen.reshape(-1, 3)
+    pack[:k, 4] = nfaces.to(torch.float64)
+    parts = [torch.empty_like(pack) for _ in range(world)]
+    dist.all_gather(parts, pack, group=group)
+    full = torch.empty((n, 5), dtype=torch.float64, device=dev)
+    for r, p in enumerate(parts):
+        o = 0
+        for b, e in cell_chunks(n, r, world, chunk):
+            full[b:e] = p[o:o + e - b]
+            o += e - b
+    out_v = full[:, 0].contiguous()
+    out_c = full[:, 1:4].contiguous()
+    out_f = full[:, 4].to(torch.int32)
+    if ids is None and areas is None:
+        return out_v, out_c, out_f
+    # the face CSR: totals, then the padded ids and areas
+    tot = torch.tensor([int(ids.shape[0]) if ids is not None else int(areas.shape[0])], dtype=torch.int64,
+                       device=dev)
+    tots = [torch.empty_like(tot) for _ in range(world)]
+    dist.all_gather(tots, tot, group=group)
+    tots = [int(t.item()) for t in tots]
+    tmax = max(tots) if tots else 0
+    fcount = out_f.clamp(min=0).to(torch.int64)
+    off = torch.zeros(n + 1, dtype=torch.int64, device=dev)
+    off[1:] = torch.cumsum(fcount, 0)
+    offh = off.cpu().numpy()
+    res_ids = res_ar = None
+    for name, src, dt in (("ids", ids, torch.int32), ("areas", areas, torch.float64)):
+        if src is None:
+            continue
+        padded = torch.zeros(max(tmax, 1), dtype=dt, device=dev)
+        padded[:src.shape[0]] = src
+        got = [torch.empty_like(padded) for _ in range(world)]
+        dist.all_gather(got, padded, group=group)
+        out = torch.empty(int(offh[n]), dtype=dt, device=dev)
+        for r, g in enumerate(got):
+            o = 0
+            for b, e in cell_chunks(n, r, world, chunk):
+                lo, hi = int(offh[b]), int(offh[e])
+                out[lo:hi] = g[o:o + hi - lo]
+                o += hi - lo
+        if name == "ids":
+            res_ids = out
+        else:
+            res_ar = out
+    return out_v, out_c, out_f, off, res_ids, res_ar
+
+
+def _local_cells(n: int, rank: int, world: int, chunk: int) -> np.ndarray:
+    cc = cell_chunks(n, rank, world, chunk)
+    return np.concatenate([np.arange(b, e) for b, e in cc]) if cc else np.zeros(0, np.int64)
+
+
+def calculate_sharded_faces(tess, group=None, chunk: int = 4096):
+    """calculate() of `tess` split over the ranks of `group` in interleaved
+    chunks (cell_chunks): this rank computes its chunks on its GPU
+    (calculate_strided), and every rank receives the whole tessellation's
+    summaries and face CSR as host arrays: (vol[n], cen[n, 3], nfaces[n],
+    offsets[n + 1], neighbour ids, face areas).  Every rank must hold the same
+    generators and walls."""
+    import torch
+    import torch.distributed as dist
+    world = dist.get_world_size(group)
+    rank = dist.get_rank(group)
+    n = tess.count_generators()
+    tess.calculate_strided(chunk, world, rank)
+    vol, cen, nf = tess.summaries()
+    off, ids = tess.neighbors()
+    _, ar = tess.face_areas()
+    mine = _local_cells(n, rank, world, chunk)
+    sel = np.concatenate([np.arange(off[i], off[i + 1]) for i in mine]) if len(mine) else np.zeros(0, np.int64)
+    dev = _device_for(group)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+    out = gather_cells_tensors(t(vol[mine]), t(cen[mine]), t(nf[mine]), n, chunk, group,
+                               ids=t(ids[sel]), areas=t(ar[sel]))
+    return tuple(x.cpu().numpy() for x in out)
+
+
+def device_neighbors(tess):
+    """(offsets[n + 1] int64, ids int32, areas float64) of the last calculate
+    as CUDA tensors that view the tessellation's own device buffers (no
+    copy); valid until the next call that changes `tess`."""
+    import torch
+    from ._lib import check
+    n = tess.count_cells()
+    dev = torch.device("cuda", torch.cuda.current_device())
+    do, di, da = C.c_void_p(), C.c_void_p(), C.c_void_p()
+    tot = C.c_int64()
+    check(tess._L.vd_tess_device_neighbors(tess._h, C.byref(do), C.byref(di), C.byref(da), C.byref(tot)), tess._h)
+    off = torch.as_tensor(_DeviceView(do.value, (n + 1,), "<i8"), device=dev)
+    if tot.value == 0:
+        return off, torch.empty(0, dtype=torch.int32, device=dev), torch.empty(0, dtype=torch.float64, device=dev)
+    ids = torch.as_tensor(_DeviceView(di.value, (tot.value,), "<i4"), device=dev)
+    ar = torch.as_tensor(_DeviceView(da.value, (tot.value,), "<f8"), device=dev)
+    return off, ids, ar
+
+
+def calculate_sharded_faces_device(tess, group=None, chunk: int = 4096):
+    """calculate_sharded_faces with every result kept on the GPU: this rank's
+    cells and their face CSR are selected in place from the library's device
+    buffers and the NCCL all-gathers assemble the whole tessellation's
+    summaries and CSR as CUDA tensors on every rank."""
+    import torch
+    import torch.distributed as dist
+    if dist.get_backend(group) != "nccl":
+        raise ValueError("calculate_sharded_faces_device needs an NCCL process group")
+    world = dist.get_world_size(group)
+    rank = dist.get_rank(group)
+    n = tess.count_generators()
+    tess.calculate_strided(chunk, world, rank)
+    vol, cen, nf = device_summaries(tess)
+    off, ids, ar = device_neighbors(tess)
+    dev = vol.device
+    mine = torch.from_numpy(_local_cells(n, rank, world, chunk)).to(dev)
+    # the face entries of this rank's chunks, in id order (each chunk's faces
+    # are contiguous in the CSR)
+    offh = off.cpu().numpy()
+    segs = [(int(offh[b]), int(offh[e])) for b, e in cell_chunks(n, rank, world, chunk)]
+    fsel = torch.cat([torch.arange(lo, hi, device=dev) for lo, hi in segs]) if segs else \
+        torch.zeros(0, dtype=torch.int64, device=dev)
+    return gather_cells_tensors(vol.index_select(0, mine), cen.index_select(0, mine), nf.index_select(0, mine), n,
+                                chunk, group, ids=ids.index_select(0, fsel), areas=ar.index_select(0, fsel))

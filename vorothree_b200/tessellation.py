@@ -25,7 +25,7 @@ from typing import Callable, List, Optional, Sequence
 
 import numpy as np
 
-from ._lib import VD_PREC_FP64, VD_PREC_MIXED, check, load
+from ._lib import FAST_LAYOUTS, VD_PREC_FP64, VD_PREC_MIXED, check, load
 
 WALL_ID_MAX = -1000
 
@@ -537,6 +537,12 @@ class Tessellation:
         code = {"fp64": VD_PREC_FP64, "mixed": VD_PREC_MIXED}[precision]
         self._ck(self._L.vd_tess_set_precision(self._h, code))
 
+    def set_fast_layout(self, layout: str):
+        """'slots' (default: a clip rewrites only the faces it cuts) or 'full'
+        (every face loop rewritten per clip): the first tier's polytope
+        layout, a tuning choice with identical results."""
+        self._ck(self._L.vd_tess_set_fast_layout(self._h, FAST_LAYOUTS[layout]))
+
     def add_wall(self, wall: Wall):
         g = wall.geometry
         L, h, wid = self._L, self._h, wall.id()
@@ -641,6 +647,16 @@ class Tessellation:
         if begin < 0 or end < begin:
             raise ValueError(f"bad cell range [{begin}, {end})")
         self._ck(self._L.vd_tess_calculate_range(self._h, int(begin), int(end)))
+
+    def calculate_strided(self, chunk: int, stride: int, phase: int, begin: int = 0, end: Optional[int] = None):
+        """calculate() for the cells with ids in [begin, end) whose chunk index
+        (id - begin) // chunk equals phase modulo stride (one GPU's share of an
+        interleaved split); the other cells read as empty."""
+        end = self.count_generators() if end is None else end
+        if begin < 0 or end < begin or chunk < 1 or not 0 <= phase < stride:
+            raise ValueError(f"bad strided range [{begin}, {end}) chunk={chunk} stride={stride} phase={phase}")
+        self._ck(self._L.vd_tess_calculate_strided(self._h, int(begin), int(end), int(chunk), int(stride),
+                                                   int(phase)))
 
     def calculate_sealed(self):
         """Tessellation::calculate_sealed (tessellation.rs:234-318)."""
