@@ -137,6 +137,23 @@ int vd_tess_set_precision(vd_tess* t, int precision);
  * counterpart in the reference: a layout choice of this library's first
  * tier, made by the autotuner; every choice gives the same results) */
 int vd_tess_set_fast_layout(vd_tess* t, int layout);
+
+/* Launch choices the autotuner makes (no counterpart in the reference; every
+ * setting gives the same results bit for bit, only the time changes).  A
+ * field of 0 keeps the library's default. */
+typedef struct {
+  int fast_layout;         /* VD_FAST_SLOTS (default) or VD_FAST_FULL */
+  int fast_blocks_per_sm;  /* slot layout: 6, 7 (default) or 8 blocks of four warps per SM (the register budget
+                              of the compiled variant; the shared-memory tier's polytopes always fit) */
+  int huge_direct_max;     /* cells left after the medium tier, at most this many (default 64) go straight to
+                              the block-per-cell tier instead of through the large tier */
+  int huge_blocks_max;     /* most concurrent blocks of the block-per-cell tier (default 64, at most 256) */
+  int huge_narrow_max;     /* tessellations of at most this many cells run that tier with 16-warp blocks,
+                              larger ones with 32 (default 2000) */
+} vd_tuning;
+int vd_tess_set_tuning(vd_tess* t, const vd_tuning* k);
+/* the settings in force (defaults filled in) */
+int vd_tess_get_tuning(const vd_tess* t, vd_tuning* k);
 /* Tessellation::calculate (tessellation.rs:213-230) over compute_cell
  * (:414-475), Algorithm3DGrid::visit_neighbors (algo_3d_grid.rs:145-202) and
  * Cell3DFaces::clip_with_scratch (cell_3d_faces.rs:288-503), with the volume,

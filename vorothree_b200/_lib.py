@@ -27,6 +27,12 @@ VD_FAST_SLOTS = 0
 VD_FAST_FULL = 1
 FAST_LAYOUTS = {"slots": VD_FAST_SLOTS, "full": VD_FAST_FULL}
 
+
+class Tuning(C.Structure):
+    """vd_tuning: launch choices that change no result (0 = default)."""
+    _fields_ = [("fast_layout", C.c_int), ("fast_blocks_per_sm", C.c_int), ("huge_direct_max", C.c_int),
+                ("huge_blocks_max", C.c_int), ("huge_narrow_max", C.c_int)]
+
 STATUS_NAMES = {VD_EINVAL: "VD_EINVAL", VD_ENOMEM: "VD_ENOMEM", VD_EOVERFLOW: "VD_EOVERFLOW",
                 VD_ETIMEOUT: "VD_ETIMEOUT", VD_ECUDA: "VD_ECUDA", VD_ESTATE: "VD_ESTATE", VD_EIO: "VD_EIO",
                 VD_ECANCELED: "VD_ECANCELED"}
@@ -62,6 +68,8 @@ SIGNATURES = {
     "vd_tess_get_generators": (C.c_int, [_vp, _d]),
     "vd_tess_set_precision": (C.c_int, [_vp, C.c_int]),
     "vd_tess_set_fast_layout": (C.c_int, [_vp, C.c_int]),
+    "vd_tess_set_tuning": (C.c_int, [_vp, _vp]),
+    "vd_tess_get_tuning": (C.c_int, [_vp, _vp]),
     "vd_tess_calculate": (C.c_int, [_vp]),
     "vd_tess_calculate_range": (C.c_int, [_vp, C.c_size_t, C.c_size_t]),
     "vd_tess_calculate_strided": (C.c_int, [_vp, C.c_size_t, C.c_size_t, C.c_size_t, C.c_size_t, C.c_size_t]),

@@ -1,22 +1,30 @@
-"""Autotuner for the grid's bin density.
+"""Autotuner: the bin density and the launch choices of the clip tiers.
 
-The one launch parameter of the hot path that depends on the input is the
-bin grid of Algorithm3DGrid: too coarse and a cell scans many far
-generators of its own bin (dense clusters), too fine and the shell walk
-opens many empty bins (sparse regions).  The clip kernel's own shape (one
-warp per cell, 4 warps per block, 7 blocks per SM, the polytope staged in
-shared memory) is fixed by its register and shared-memory budget and needs
-no tuning.
+What it picks, per input class (distribution, size bucket):
+  * the bin grid of Algorithm3DGrid: too coarse and a cell scans many far
+    generators of its own bin (dense clusters), too fine and the shell walk
+    opens many empty bins (sparse regions);
+  * the first tier's polytope layout ("slots": a clip rewrites only the
+    faces it cuts; "full": every face loop per clip) and, for the slot
+    layout, its register budget -- 6, 7 or 8 blocks of four warps per SM, the
+    compiled variants (more resident warps against more spills).
+and once for the tessellation, on inputs with cells adjacent to thousands of
+others (the reference's sphere-surface benchmark distribution):
+  * the hand-off to the block-per-cell tier: how few cells left after the
+    medium tier go there directly, how many blocks it runs at once, and up to
+    which tessellation size its blocks are 16 warps wide instead of 32.
+None of these changes a result: every choice computes the same doubles.
 
-The tuner times Tessellation.calculate on the GPU for a ladder of bin
-densities and records the fastest per input class: (distribution, size
-bucket).  `choose_grid` looks the class of a new input up in the table
-(the committed `autotune_table.json` next to this file, or one given) and
-falls back to a density rule when the class was never tuned.
+The tuner times Tessellation.calculate on the GPU (coordinate descent: bin
+density first, then the layout, then its blocks per SM) and records the
+fastest per class in a table (the committed `autotune_table.json` next to
+this file, or one given).  `choose` looks the class of a new input up and
+falls back to the defaults when the class was never tuned.
 
     from vorothree_b200 import autotune
-    grid = autotune.choose_grid(points, bounds)          # (nx, ny, nz)
-    table = autotune.tune(points, bounds, walls)          # measure and record
+    grid, tuning = autotune.choose(points, bounds)      # (nx, ny, nz), settings
+    t = Tessellation(bounds, Algorithm3DGrid(*grid)); t.set_tuning(tuning)
+    table = autotune.tune(points, bounds, walls)         # measure and record
 """
 from __future__ import annotations
 
@@ -36,6 +44,15 @@ FACTORS = (0.6, 0.8, 1.0, 1.25, 1.6, 2.0, 2.5, 3.2, 4.0, 5.0)
 LADDER = {"uniform": (0.6, 0.8, 1.0, 1.25, 1.6, 2.0), "clustered": (1.0, 1.6, 2.0, 2.5, 3.2, 4.0, 5.0)}
 DEFAULT_FACTOR = {"uniform": 1.0, "clustered": 2.5}
 _SAMPLE = 1 << 16
+# the first tier's choices the tuner searches, and the library's defaults
+LAYOUTS = ("slots", "full")
+BLOCKS_PER_SM = (6, 7, 8)
+DEFAULT_TUNING = {"fast_layout": "slots", "fast_blocks_per_sm": 7}
+# the block-per-cell tier's hand-off, searched once (HANDOFF_KEY)
+HANDOFF_KEY = "handoff"
+DIRECT_MAX = (1, 16, 64, 256)
+NARROW_MAX = (500, 2000, 5000)
+DEFAULT_HANDOFF = {"huge_direct_max": 64, "huge_blocks_max": 64, "huge_narrow_max": 2000}
 
 
 def grid_for(n: int, bounds, factor: float) -> Tuple[int, int, int]:
@@ -87,27 +104,51 @@ def load_table(path: Optional[str] = None) -> Dict[str, dict]:
 
 def record(entries: Dict[str, dict], path: Optional[str] = None, device: str = ""):
     p = path or TABLE_PATH
-    data = {"what": "bin density factor per (distribution, size bucket); "
-                    "bins per axis = factor * (N/V)^(1/3) * edge",
+    data = {"what": "per (distribution, size bucket): bin density factor (bins per axis = factor * (N/V)^(1/3) "
+                    "* edge) and the first tier's layout / blocks per SM; 'handoff': the block-per-cell "
+                    "tier's thresholds (results never depend on any of these)",
             "device": device, "entries": entries}
     with open(p, "w") as f:
         json.dump(data, f, indent=1, sort_keys=True)
+
+
+def _nearest(cls: str, n: int, entries: Dict[str, dict]) -> Optional[dict]:
+    want = size_bucket(n)
+    best, dist = None, None
+    for k, e in entries.items():
+        if "/2^" not in k:
+            continue
+        c, b = k.split("/2^")
+        if c != cls:
+            continue
+        d = abs(int(b) - want)
+        if dist is None or d < dist:
+            best, dist = e, d
+    return best
 
 
 def lookup(cls: str, n: int, entries: Optional[Dict[str, dict]] = None) -> float:
     """Tuned factor of the nearest tuned size bucket of this class, or the
     class default."""
     entries = load_table() if entries is None else entries
-    want = size_bucket(n)
-    best, dist = None, None
-    for k, e in entries.items():
-        c, b = k.split("/2^")
-        if c != cls:
-            continue
-        d = abs(int(b) - want)
-        if dist is None or d < dist:
-            best, dist = e["factor"], d
-    return DEFAULT_FACTOR[cls] if best is None else float(best)
+    e = _nearest(cls, n, entries)
+    return DEFAULT_FACTOR[cls] if e is None else float(e["factor"])
+
+
+def lookup_tuning(cls: str, n: int, entries: Optional[Dict[str, dict]] = None) -> dict:
+    """The launch settings (Tessellation.set_tuning) for this class and size:
+    the first tier's choices of the nearest tuned size bucket and the table's
+    hand-off thresholds, each falling back to the library's defaults."""
+    entries = load_table() if entries is None else entries
+    out = dict(DEFAULT_TUNING)
+    e = _nearest(cls, n, entries)
+    if e is not None:
+        out.update({k: e["tuning"][k] for k in DEFAULT_TUNING if k in e.get("tuning", {})})
+    out.update(DEFAULT_HANDOFF)
+    h = entries.get(HANDOFF_KEY)
+    if h is not None:
+        out.update({k: h["tuning"][k] for k in DEFAULT_HANDOFF if k in h.get("tuning", {})})
+    return out
 
 
 def choose_grid(points, bounds, entries: Optional[Dict[str, dict]] = None) -> Tuple[int, int, int]:
@@ -117,36 +158,83 @@ def choose_grid(points, bounds, entries: Optional[Dict[str, dict]] = None) -> Tu
     return grid_for(len(pts), bounds, lookup(cls, len(pts), entries))
 
 
-def tune(points, bounds, walls: Sequence = (), factors: Iterable[float] = FACTORS, reps: int = 3,
-         precision: str = "fp64", entries: Optional[Dict[str, dict]] = None) -> Dict[str, dict]:
-    """Time calculate() on the GPU for each density factor (best of `reps`
-    after one warm-up) and record the fastest under this input's class.
-    Returns the updated table entries (not written to disk; see record)."""
+def choose(points, bounds, entries: Optional[Dict[str, dict]] = None) -> Tuple[Tuple[int, int, int], dict]:
+    """(grid, launch settings) the tuner would use for this input."""
+    pts = np.asarray(points, np.float64).reshape(-1, 3)
+    cls = distribution_class(pts, bounds)
+    return grid_for(len(pts), bounds, lookup(cls, len(pts), entries)), lookup_tuning(cls, len(pts), entries)
+
+
+def _time(points, bounds, grid, walls, tuning: dict, reps: int, precision: str) -> float:
+    """Best device time of calculate() (clip passes, fallback tiers included)
+    over `reps` runs after one warm-up."""
     from .tessellation import Algorithm3DGrid, Tessellation
+    t = Tessellation(bounds, Algorithm3DGrid(*grid))
+    try:
+        t.set_precision(precision)
+        t.set_tuning(tuning)
+        for w in walls:
+            t.add_wall(w)
+        t.set_generators(points)
+        t.calculate()
+        best = None
+        for _ in range(reps):
+            t.calculate()
+            tm = t.timings()
+            ms = tm["clip_ms"] + tm["fallback_ms"]
+            best = ms if best is None else min(best, ms)
+        return best
+    finally:
+        t.close()
+
+
+def tune(points, bounds, walls: Sequence = (), factors: Iterable[float] = FACTORS, reps: int = 3,
+         precision: str = "fp64", entries: Optional[Dict[str, dict]] = None, layouts: Sequence[str] = LAYOUTS,
+         blocks: Sequence[int] = BLOCKS_PER_SM) -> Dict[str, dict]:
+    """Time calculate() on the GPU (best of `reps` after one warm-up) over the
+    density factors with the default launch settings, then over the first
+    tier's layouts and (slot layout) blocks per SM at the best factor, and
+    record the fastest under this input's class.  Returns the updated table
+    entries (not written to disk; see record)."""
     pts = np.asarray(points, np.float64).reshape(-1, 3)
     cls = distribution_class(pts, bounds)
     entries = dict(load_table() if entries is None else entries)
     trials = []
     for f in factors:
         g = grid_for(len(pts), bounds, f)
-        t = Tessellation(bounds, Algorithm3DGrid(*g))
-        try:
-            t.set_precision(precision)
-            for w in walls:
-                t.add_wall(w)
-            t.set_generators(pts)
-            t.calculate()
-            best = None
-            for _ in range(reps):
-                t.calculate()
-                tm = t.timings()
-                ms = tm["clip_ms"] + tm["fallback_ms"]
-                best = ms if best is None else min(best, ms)
-            trials.append({"factor": f, "grid": list(g), "ms": best})
-        finally:
-            t.close()
+        trials.append({"factor": f, "grid": list(g), "tuning": dict(DEFAULT_TUNING),
+                       "ms": _time(pts, bounds, g, walls, DEFAULT_TUNING, reps, precision)})
     win = min(trials, key=lambda r: r["ms"])
-    entries[key(cls, len(pts))] = {"factor": win["factor"], "ms": win["ms"], "n": len(pts), "trials": trials}
+    g = win["grid"]
+    for layout in layouts:
+        for nb in (blocks if layout == "slots" else (7,)):
+            tun = {"fast_layout": layout, "fast_blocks_per_sm": nb}
+            if tun == DEFAULT_TUNING:
+                continue
+            trials.append({"factor": win["factor"], "grid": list(g), "tuning": tun,
+                           "ms": _time(pts, bounds, g, walls, tun, reps, precision)})
+    best = min((r for r in trials if r["factor"] == win["factor"]), key=lambda r: r["ms"])
+    entries[key(cls, len(pts))] = {"factor": win["factor"], "tuning": best["tuning"], "ms": best["ms"],
+                                   "n": len(pts), "trials": trials}
+    return entries
+
+
+def tune_handoff(cases, reps: int = 2, entries: Optional[Dict[str, dict]] = None) -> Dict[str, dict]:
+    """The block-per-cell tier's thresholds: `cases` is a list of (points,
+    bounds, grid) whose cells include ones beyond the large tier (e.g. the
+    sphere-surface distribution); the setting with the least total time over
+    them is recorded under HANDOFF_KEY."""
+    entries = dict(load_table() if entries is None else entries)
+    trials = []
+    for dm in DIRECT_MAX:
+        for nm in NARROW_MAX:
+            tun = dict(DEFAULT_TUNING, huge_direct_max=dm, huge_narrow_max=nm,
+                       huge_blocks_max=DEFAULT_HANDOFF["huge_blocks_max"])
+            ms = [_time(p, b, g, (), tun, reps, "fp64") for p, b, g in cases]
+            trials.append({"tuning": {k: tun[k] for k in DEFAULT_HANDOFF}, "ms": ms, "total_ms": sum(ms)})
+    win = min(trials, key=lambda r: r["total_ms"])
+    entries[HANDOFF_KEY] = {"tuning": win["tuning"], "total_ms": win["total_ms"], "trials": trials,
+                            "cases": [len(p) for p, _, _ in cases]}
     return entries
 
 
@@ -175,6 +263,7 @@ def main(argv=None):
     ap.add_argument("--out", default=TABLE_PATH)
     ap.add_argument("--max-log2", type=int, default=22)
     a = ap.parse_args(argv)
+    from .workloads import bench_distribution
     b = BoundingBox([0, 0, 0], [1, 1, 1])
     entries: Dict[str, dict] = {}
     for cls in ("uniform", "clustered"):
@@ -184,7 +273,16 @@ def main(argv=None):
                 continue
             entries = tune(pts, b, factors=LADDER[cls], reps=3 if e < 22 else 1, entries=entries)
             k = key(cls, len(pts))
-            print(k, entries[k]["factor"], round(entries[k]["ms"], 3), flush=True)
+            print(k, entries[k]["factor"], entries[k]["tuning"], round(entries[k]["ms"], 3), flush=True)
+    # the reference's sphere-surface distribution: one cell per tessellation
+    # adjacent to every other generator
+    box = BoundingBox([0, 0, 0], [100, 100, 100])
+    cases = []
+    for n in (1000, 3000):
+        g = int(np.ceil(n ** (1.0 / 3.0)))
+        cases.append((bench_distribution("sphere", n, 11), box, (g, g, g)))
+    entries = tune_handoff(cases, entries=entries)
+    print(HANDOFF_KEY, entries[HANDOFF_KEY]["tuning"], round(entries[HANDOFF_KEY]["total_ms"], 3), flush=True)
     record(entries, a.out, device=torch.cuda.get_device_name(0))
 
 

@@ -708,12 +708,13 @@ __device__ int compute_cell_block(const TessDesc& T, uint32_t i, WarpPoly<C>& P,
 }
 
 constexpr int kHugeBlockWarps = 32;
-// blocks for small tessellations: a cell's faces are at most its walls' planes
+// blocks for small tessellations (the host picks them for at most 2,000 cells
+// by default, a tuning setting): a cell's faces are at most its walls' planes
 // plus one per other generator, so its polytope stays small and the clip's
-// barriers, not its passes, set the time (the width changes no result) (the centre of 1,000 generators on a sphere: 14.2 ms
-// with 16 warps, 18.1 ms with 32; at 3,000 generators 32 warps win)
+// barriers, not its passes, set the time (the width changes no result) (the
+// centre of 1,000 generators on a sphere: 14.2 ms with 16 warps, 18.1 ms with
+// 32; at 3,000 generators 32 warps win)
 constexpr int kHugeBlockWarpsNarrow = 16;
-constexpr uint32_t kHugeNarrowMaxCells = 2000;
 
 // persistent blocks over the listed cells, one cell per block at a time; the
 // block's polytope lives in global memory

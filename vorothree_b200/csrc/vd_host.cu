@@ -305,8 +305,13 @@ struct vd_tess {
   float timings[4] = {0, 0, 0, 0};
   unsigned long long counters[kNumCounters] = {};
   unsigned long long fallback[2] = {0, 0};
-  ClipLaunchInfo info64{}, infomx{}, infomed{}, infosp64{}, infospmx{};
+  ClipLaunchInfo info64{}, infomx{}, infomed{};
+  ClipLaunchInfo infosp64[3]{}, infospmx[3]{};  // slot layout at 6, 7, 8 blocks per SM
   int fast_layout = VD_FAST_SLOTS;
+  int fast_minb = 7;
+  int huge_direct_max = 64;
+  int huge_blocks_max = 64;
+  int huge_narrow_max = 2000;
   int num_sms = 0;
 };
 
@@ -570,7 +575,7 @@ int ensure_pool(vd_tess* t, size_t cells, long long faces_per_cell) {
 
 int ensure_huge(vd_tess* t, size_t cells) {
   // a few blocks: each holds a multi-megabyte polytope in global memory
-  const size_t want = std::min<size_t>(std::min<size_t>(std::max<size_t>(cells, 1), (size_t)kHugeBlocksMax),
+  const size_t want = std::min<size_t>(std::min<size_t>(std::max<size_t>(cells, 1), (size_t)t->huge_blocks_max),
                                        std::max<size_t>(t->huge_blocks_cap, 1));
   if (t->huge_blocks != want) {
     VD_CK(t, t->d_huge.ensure(want * clip_huge_scratch_per_block(), t->stream));
@@ -613,12 +618,14 @@ int clip_pass(vd_tess* t, int tier, const uint32_t* items, uint32_t nitems, uint
     // the slot layout cannot export a polytope in the reference's vertex
     // order: get_cell's rebuild runs the full-rewrite kernel
     const bool slots = t->fast_layout == VD_FAST_SLOTS && !W.ex_verts;
-    const ClipLaunchInfo& li = slots ? (mixed ? t->infospmx : t->infosp64) : (mixed ? t->infomx : t->info64);
+    const int mv = t->fast_minb - 6;
+    const ClipLaunchInfo& li =
+        slots ? (mixed ? t->infospmx[mv] : t->infosp64[mv]) : (mixed ? t->infomx : t->info64);
     const size_t warps_needed = (nitems + li.warps_per_block - 1) / li.warps_per_block;
     const int nblocks = (int)std::max<size_t>(
         1, std::min<size_t>(warps_needed, (size_t)t->num_sms * std::max(1, li.blocks_per_sm)));
     if (slots)
-      VD_CK(t, launch_clip_sparse(T, W, nblocks, t->instrument, mixed, s));
+      VD_CK(t, launch_clip_sparse(T, W, nblocks, t->instrument, mixed, t->fast_minb, s));
     else
       VD_CK(t, mixed ? launch_clip_mixed_fast(T, W, nblocks, t->instrument, s)
                      : launch_clip_fp64_fast(T, W, nblocks, t->instrument, s));
@@ -633,7 +640,8 @@ int clip_pass(vd_tess* t, int tier, const uint32_t* items, uint32_t nitems, uint
     int r = ensure_huge(t, nitems);
     if (r != VD_OK) return r;
     T = make_desc(t);
-    VD_CK(t, launch_clip_fp64_huge(T, W, t->d_huge.p, (int)t->huge_blocks, s));
+    VD_CK(t, launch_clip_fp64_huge(T, W, t->d_huge.p, (int)t->huge_blocks,
+                                   T.ncells <= (uint32_t)t->huge_narrow_max, s));
     g_launches++;
   }
   return VD_OK;
@@ -785,7 +793,7 @@ int run_calculate(vd_tess* t, const WorkList* extra = nullptr, const uint32_t* o
         // few cells left after the medium tier: straight to the block tier,
         // which takes them all at once, so that a cell outgrowing the large
         // tier is not built twice
-        if (tier == 1 && novf > 0 && novf <= (unsigned)kHugeBlocksMax) tier = 2;
+        if (tier == 1 && novf > 0 && novf <= (unsigned)t->huge_direct_max) tier = 2;
       }
       novf = 0;
       ntab = ntab_all;
@@ -1032,8 +1040,10 @@ int vd_tess_create(const double bmin[3], const double bmax[3], int nx, int ny, i
   for (auto& ev : t->ev) cudaEventCreate(&ev);
   e = clip_fp64_info(&t->info64);
   if (e == cudaSuccess) e = clip_mixed_info(&t->infomx);
-  if (e == cudaSuccess) e = clip_sparse_info(false, &t->infosp64);
-  if (e == cudaSuccess) e = clip_sparse_info(true, &t->infospmx);
+  for (int k = 0; k < 3 && e == cudaSuccess; ++k) {
+    e = clip_sparse_info(false, 6 + k, &t->infosp64[k]);
+    if (e == cudaSuccess) e = clip_sparse_info(true, 6 + k, &t->infospmx[k]);
+  }
   if (e == cudaSuccess) e = clip_med_setup(&t->infomed);
   if (e == cudaSuccess) e = seal_setup();
   if (e != cudaSuccess) {
@@ -1552,6 +1562,32 @@ int vd_tess_set_fast_layout(vd_tess* t, int layout) {
   if (!t) return VD_EINVAL;
   if (layout != VD_FAST_SLOTS && layout != VD_FAST_FULL) return fail(t, VD_EINVAL, "unknown fast-tier layout");
   t->fast_layout = layout;
+  return VD_OK;
+}
+
+int vd_tess_set_tuning(vd_tess* t, const vd_tuning* k) {
+  if (!t || !k) return VD_EINVAL;
+  if (k->fast_layout != 0 && k->fast_layout != VD_FAST_FULL)
+    return fail(t, VD_EINVAL, "unknown fast-tier layout %d", k->fast_layout);
+  if (k->fast_blocks_per_sm != 0 && (k->fast_blocks_per_sm < 6 || k->fast_blocks_per_sm > 8))
+    return fail(t, VD_EINVAL, "fast_blocks_per_sm must be 6, 7 or 8");
+  if (k->huge_direct_max < 0 || k->huge_blocks_max < 0 || k->huge_blocks_max > 256 || k->huge_narrow_max < 0)
+    return fail(t, VD_EINVAL, "huge-tier settings out of range");
+  t->fast_layout = k->fast_layout;
+  t->fast_minb = k->fast_blocks_per_sm ? k->fast_blocks_per_sm : 7;
+  t->huge_direct_max = k->huge_direct_max ? k->huge_direct_max : 64;
+  t->huge_blocks_max = k->huge_blocks_max ? k->huge_blocks_max : kHugeBlocksMax;
+  t->huge_narrow_max = k->huge_narrow_max ? k->huge_narrow_max : 2000;
+  return VD_OK;
+}
+
+int vd_tess_get_tuning(const vd_tess* t, vd_tuning* k) {
+  if (!t || !k) return VD_EINVAL;
+  k->fast_layout = t->fast_layout;
+  k->fast_blocks_per_sm = t->fast_minb;
+  k->huge_direct_max = t->huge_direct_max;
+  k->huge_blocks_max = t->huge_blocks_max;
+  k->huge_narrow_max = t->huge_narrow_max;
   return VD_OK;
 }
 

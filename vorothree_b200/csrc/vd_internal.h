@@ -31,7 +31,9 @@ cudaError_t launch_clip_fp64_big(const TessDesc& T, const WorkList& W, void* scr
 // huge tier (global memory, one thread block per cell): cells beyond the
 // large capacities
 size_t clip_huge_scratch_per_block();
-cudaError_t launch_clip_fp64_huge(const TessDesc& T, const WorkList& W, void* scratch, int nblocks, cudaStream_t s);
+// narrow: 16-warp blocks (small tessellations), else 32
+cudaError_t launch_clip_fp64_huge(const TessDesc& T, const WorkList& W, void* scratch, int nblocks, bool narrow,
+                                  cudaStream_t s);
 cudaError_t launch_clip_fp64_huge_batched(const TessDesc* descs, const uint32_t* tess_off, int ntess,
                                           const WorkList& W, void* scratch, int nblocks, cudaStream_t s);
 
@@ -127,8 +129,9 @@ cudaError_t clip_mixed_info(ClipLaunchInfo* info);
 // the shared-memory tier on the slot layout (vd_kernels_sparse.cu): a
 // modifying clip rewrites only the faces that lose a vertex; cells it cannot
 // finish are listed as overflowing, for the medium tier
-cudaError_t clip_sparse_info(bool mixed, ClipLaunchInfo* info);
-cudaError_t launch_clip_sparse(const TessDesc& T, const WorkList& W, int nblocks, bool count, bool mixed,
+// minb: the register budget of 6, 7 or 8 blocks of four warps per SM
+cudaError_t clip_sparse_info(bool mixed, int minb, ClipLaunchInfo* info);
+cudaError_t launch_clip_sparse(const TessDesc& T, const WorkList& W, int nblocks, bool count, bool mixed, int minb,
                                cudaStream_t s);
 cudaError_t clip_sparse_batched_setup(bool mixed, int* blocks_per_sm);
 cudaError_t launch_clip_sparse_batched(const TessDesc* descs, const uint32_t* tess_off, int ntess, const WorkList& W,

@@ -58,9 +58,10 @@ cudaError_t launch_clip_fp64_big(const TessDesc& T, const WorkList& W, void* scr
 // the huge tier's scratch: a polytope per block
 size_t clip_huge_scratch_per_block() { return sizeof(WarpPoly<HugeCfg>); }
 
-cudaError_t launch_clip_fp64_huge(const TessDesc& T, const WorkList& W, void* scratch, int nblocks, cudaStream_t s) {
+cudaError_t launch_clip_fp64_huge(const TessDesc& T, const WorkList& W, void* scratch, int nblocks, bool narrow,
+                                  cudaStream_t s) {
   WarpPoly<HugeCfg>* polys = reinterpret_cast<WarpPoly<HugeCfg>*>(scratch);
-  if (T.ncells <= kHugeNarrowMaxCells)
+  if (narrow)
     k_clip_huge_block<HugeCfg, kHugeBlockWarpsNarrow><<<nblocks, kHugeBlockWarpsNarrow * 32, 0, s>>>(T, W, polys);
   else
     k_clip_huge_block<HugeCfg, kHugeBlockWarps><<<nblocks, kHugeBlockWarps * 32, 0, s>>>(T, W, polys);

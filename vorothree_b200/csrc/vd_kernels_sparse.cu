@@ -10,9 +10,9 @@
 namespace vd {
 
 // blocks of 4 warps per SM the register budget must admit (shared memory
-// admits this many too)
-constexpr int kSparseMinBlocks = 7;
-constexpr int kSparseMixedMinBlocks = 7;
+// admits this many too): single tessellations are compiled for 6, 7 and 8
+// (a tuning setting, 7 by default; the instrumented variant for 7 only),
+// batches for 6 (their member lookup needs more registers)
 constexpr int kSparseBatchMinBlocks = 6;
 
 namespace {
@@ -59,21 +59,32 @@ void launch_batched(const TessDesc* descs, const uint32_t* tess_off, int ntess, 
 
 }  // namespace
 
-cudaError_t clip_sparse_info(bool mixed, ClipLaunchInfo* info) {
-  cudaError_t e = mixed ? setup_one<MixedSparseCount, kSparseMixedMinBlocks>(nullptr)
-                        : setup_one<FastSparseCount, kSparseMinBlocks>(nullptr);
+cudaError_t clip_sparse_info(bool mixed, int minb, ClipLaunchInfo* info) {
+  cudaError_t e = mixed ? setup_one<MixedSparseCount, 7>(nullptr) : setup_one<FastSparseCount, 7>(nullptr);
   if (e != cudaSuccess) return e;
-  return mixed ? setup_one<MixedSparse, kSparseMixedMinBlocks>(info) : setup_one<FastSparse, kSparseMinBlocks>(info);
+  if (mixed) {
+    if (minb == 6) return setup_one<MixedSparse, 6>(info);
+    if (minb == 8) return setup_one<MixedSparse, 8>(info);
+    return setup_one<MixedSparse, 7>(info);
+  }
+  if (minb == 6) return setup_one<FastSparse, 6>(info);
+  if (minb == 8) return setup_one<FastSparse, 8>(info);
+  return setup_one<FastSparse, 7>(info);
 }
 
-cudaError_t launch_clip_sparse(const TessDesc& T, const WorkList& W, int nblocks, bool count, bool mixed,
+// count: the instrumented variant (always at 7 blocks per SM)
+cudaError_t launch_clip_sparse(const TessDesc& T, const WorkList& W, int nblocks, bool count, bool mixed, int minb,
                                cudaStream_t s) {
   if (mixed) {
-    if (count) launch_one<MixedSparseCount, kSparseMixedMinBlocks>(T, W, nblocks, s);
-    else launch_one<MixedSparse, kSparseMixedMinBlocks>(T, W, nblocks, s);
+    if (count) launch_one<MixedSparseCount, 7>(T, W, nblocks, s);
+    else if (minb == 6) launch_one<MixedSparse, 6>(T, W, nblocks, s);
+    else if (minb == 8) launch_one<MixedSparse, 8>(T, W, nblocks, s);
+    else launch_one<MixedSparse, 7>(T, W, nblocks, s);
   } else {
-    if (count) launch_one<FastSparseCount, kSparseMinBlocks>(T, W, nblocks, s);
-    else launch_one<FastSparse, kSparseMinBlocks>(T, W, nblocks, s);
+    if (count) launch_one<FastSparseCount, 7>(T, W, nblocks, s);
+    else if (minb == 6) launch_one<FastSparse, 6>(T, W, nblocks, s);
+    else if (minb == 8) launch_one<FastSparse, 8>(T, W, nblocks, s);
+    else launch_one<FastSparse, 7>(T, W, nblocks, s);
   }
   return cudaGetLastError();
 }

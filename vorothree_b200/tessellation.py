@@ -25,7 +25,7 @@ from typing import Callable, List, Optional, Sequence
 
 import numpy as np
 
-from ._lib import FAST_LAYOUTS, VD_PREC_FP64, VD_PREC_MIXED, check, load
+from ._lib import FAST_LAYOUTS, VD_PREC_FP64, VD_PREC_MIXED, Tuning, check, load
 
 WALL_ID_MAX = -1000
 
@@ -536,6 +536,25 @@ class Tessellation:
         """'fp64' (default, bitwise the reference's arithmetic) or 'mixed'."""
         code = {"fp64": VD_PREC_FP64, "mixed": VD_PREC_MIXED}[precision]
         self._ck(self._L.vd_tess_set_precision(self._h, code))
+
+    def set_tuning(self, tuning: dict):
+        """Launch choices that change no result (the autotuner's): any of
+        fast_layout ('slots' / 'full'), fast_blocks_per_sm (6, 7, 8),
+        huge_direct_max, huge_blocks_max, huge_narrow_max; keys left out keep
+        their current value."""
+        cur = self.get_tuning()
+        cur.update(tuning)
+        k = Tuning(FAST_LAYOUTS[cur["fast_layout"]], int(cur["fast_blocks_per_sm"]), int(cur["huge_direct_max"]),
+                   int(cur["huge_blocks_max"]), int(cur["huge_narrow_max"]))
+        self._ck(self._L.vd_tess_set_tuning(self._h, C.byref(k)))
+
+    def get_tuning(self) -> dict:
+        k = Tuning()
+        self._ck(self._L.vd_tess_get_tuning(self._h, C.byref(k)))
+        names = {v: n for n, v in FAST_LAYOUTS.items()}
+        return {"fast_layout": names[k.fast_layout], "fast_blocks_per_sm": k.fast_blocks_per_sm,
+                "huge_direct_max": k.huge_direct_max, "huge_blocks_max": k.huge_blocks_max,
+                "huge_narrow_max": k.huge_narrow_max}
 
     def set_fast_layout(self, layout: str):
         """'slots' (default: a clip rewrites only the faces it cuts) or 'full'
