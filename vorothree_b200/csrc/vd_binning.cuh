@@ -221,6 +221,24 @@ __global__ void k_bin_scatter(const uint32_t* __restrict__ bin_of, size_t n, uin
     ids[atomicAdd(&cursor[bin_of[i]], 1u)] = (uint32_t)i;
 }
 
+// occ[w] bit j = 1 when bin 32 w + j has members: the walk's test for an
+// empty bin without reading bin_start (on a sparse grid the bin table is
+// large and mostly empty; the bit map is 1/32 of it and stays in L2)
+__global__ void k_bin_occupancy(const uint32_t* __restrict__ start, size_t nbins, uint32_t* __restrict__ occ) {
+  const size_t nw = (nbins + 31) / 32;
+  for (size_t w = (size_t)blockIdx.x * blockDim.x + threadIdx.x; w < nw; w += (size_t)gridDim.x * blockDim.x) {
+    uint32_t m = 0;
+    const size_t b0 = 32 * w;
+    uint32_t prev = start[b0];
+    for (int j = 0; j < 32 && b0 + j < nbins; ++j) {
+      const uint32_t next = start[b0 + j + 1];
+      if (next > prev) m |= 1u << j;
+      prev = next;
+    }
+    occ[w] = m;
+  }
+}
+
 constexpr uint32_t kSmallBin = 16;
 
 // The atomic scatter leaves members in arbitrary order; the reference pushes

@@ -781,8 +781,12 @@ __device__ int compute_cell(const TessDesc& T, uint32_t i, PolyT& P, typename Po
         const double bdx = fmax(ddx, 0.0), bdy = fmax(ddy, 0.0), bdz = fmax(ddz, 0.0);
         b2 = bdx * bdx + bdy * bdy + bdz * bdz;
         const uint32_t bb = (uint32_t)bx + (uint32_t)by * (uint32_t)G.n[0] + (uint32_t)bz * nxy;
-        bs = T.bin_start[bb];
-        be = T.bin_start[bb + 1];
+        // on sparse grids an empty bin is known from its occupancy bit (an
+        // L2-resident map) without reading the bin table
+        if (!T.occ || ((__ldg(&T.occ[bb >> 5]) >> (bb & 31u)) & 1u)) {
+          bs = T.bin_start[bb];
+          be = T.bin_start[bb + 1];
+        }
       }
     }
     const int nvalid = min(32, T.norder - base);

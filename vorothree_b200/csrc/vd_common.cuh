@@ -86,6 +86,7 @@ struct TessDesc {
   const double* gen;
   const uint32_t* bin_of;
   const uint32_t* bin_start;
+  const uint32_t* occ;  // optional: bit b set when bin b has members (sparse grids)
   const SortedGen* sorted;
   uint32_t ncells;
   // outputs

@@ -242,6 +242,8 @@ struct vd_tess {
   DevBuf<uint32_t> d_flags, d_pos;
   DevBuf<uint32_t> d_bin_of, d_bin_count, d_bin_start, d_cursor, d_ids, d_ids_tmp, d_big_list;
   DevBuf<SortedGen> d_sorted;
+  DevBuf<uint32_t> d_occ;   // bin occupancy bits (sparse grids)
+  bool occ_valid = false;
 
   // outputs
   size_t ncells = 0;
@@ -392,6 +394,24 @@ WallSet wallset(const vd_tess* t) {
   return ws;
 }
 
+// bins per generator from which the walk tests bins through the occupancy
+// bit map: on such sparse grids most bins it reaches are empty, and the bit
+// map (1/32 of the bin table) stays in L2 where the table does not
+constexpr size_t kOccupancyBinsPerGen = 8;
+
+// the occupancy bit map of the current bins, on sparse grids
+int build_occupancy(vd_tess* t) {
+  const size_t nb = t->nbins;
+  t->occ_valid = false;
+  if (nb < kOccupancyBinsPerGen * std::max<size_t>(t->ngen, 1)) return VD_OK;
+  VD_CK(t, t->d_occ.ensure((nb + 31) / 32, t->stream));
+  k_bin_occupancy<<<grid_blocks(t, (nb + 31) / 32, 256), 256, 0, t->stream>>>(t->d_bin_start.p, nb, t->d_occ.p);
+  g_launches++;
+  VD_CK(t, cudaGetLastError());
+  t->occ_valid = true;
+  return VD_OK;
+}
+
 // Algorithm3DGrid::set_generators on the device: bin index, counting sort
 // with members in ascending id order, then the bin-ordered copy.
 int rebin(vd_tess* t) {
@@ -432,6 +452,8 @@ int rebin(vd_tess* t) {
     g_launches++;
     VD_CK(t, cudaGetLastError());
   }
+  r = build_occupancy(t);
+  if (r != VD_OK) return r;
   t->calculated = false;
   t->csr_valid = false;
   return VD_OK;
@@ -487,6 +509,7 @@ TessDesc make_desc(vd_tess* t) {
   T.gen = t->d_gen.p;
   T.bin_of = t->d_bin_of.p;
   T.bin_start = t->d_bin_start.p;
+  T.occ = t->occ_valid ? t->d_occ.p : nullptr;
   T.sorted = t->d_sorted.p;
   T.ncells = (uint32_t)t->ngen;
   T.vol = t->d_vol.p;
@@ -1525,6 +1548,8 @@ int vd_tess_set_generator(vd_tess* t, size_t index, const double xyz[3]) {
   k_gather_sorted<<<grid_blocks(t, n, 256), 256, 0, s>>>(t->d_ids.p, t->d_gen.p, n, t->d_sorted.p);
   g_launches++;
   VD_CK(t, cudaGetLastError());
+  int ro = build_occupancy(t);
+  if (ro != VD_OK) return ro;
   VD_CK(t, cudaStreamSynchronize(s));
   t->calculated = false;
   t->csr_valid = false;
