@@ -291,7 +291,7 @@ __device__ int warp_clip(SparsePoly<C>& P, SparseState& S, double px, double py,
   const int src = S.cb;
   const bool fv = (int)lane < nf;
   unsigned m0 = 0u, m1 = 0u, m2 = 0u;
-  int c = 0, st = 0, rot = 0, fnv = 0;
+  int c = 0, st = 0, rot = 0;
   if (fv) {
     m0 = P.fm0[lane];
     m1 = P.fm1[lane];
@@ -299,7 +299,6 @@ __device__ int warp_clip(SparsePoly<C>& P, SparseState& S, double px, double py,
     c = P.fc[lane];
     st = P.fst[lane];
     rot = P.fr[lane];
-    fnv = P.fn[lane];
   }
   const bool kept = fv && ((m0 & I0) | (m1 & I1) | (m2 & I2)) != 0u;
   const bool touched = kept && ((m0 & O0) | (m1 & O1) | (m2 & O2)) != 0u;
@@ -317,7 +316,7 @@ __device__ int warp_clip(SparsePoly<C>& P, SparseState& S, double px, double py,
 
   // entry space: append after the live entries, or copy the untouched faces
   // (in logical order) to the front of the other buffer first
-  int dst = src, base = S.etop, ust = st, urot = rot;
+  int dst = src, base = S.etop;
   if (base + need > C::ECAP) {
     const int csz = (kept && !touched) ? c : 0;
     const int cinc = warp_incl_scan(csz);
@@ -331,8 +330,10 @@ __device__ int warp_clip(SparsePoly<C>& P, SparseState& S, double px, double py,
         P.ent[dst][cofs + j] = P.ent[src][st + q];
         q = (q + 1 == c) ? 0 : q + 1;
       }
-      ust = cofs;
-      urot = 0;
+      // the face's table entry now points at its logical-order copy (only
+      // this lane reads it again)
+      P.fst[lane] = (uint16_t)cofs;
+      P.fr[lane] = 0;
     }
   }
 
@@ -486,17 +487,29 @@ __device__ int warp_clip(SparsePoly<C>& P, SparseState& S, double px, double py,
   const unsigned A2 = __reduce_or_sync(kFull, (oncyc && a >= 64u && a < 96u) ? 1u << (a - 64u) : 0u);
 
   // 6. the face table: surviving faces in order, then the lid
+  //    (each lane reads its face's entry again rather than keeping it in
+  //    registers through steps 3-5)
   const int xio = __shfl_sync(kFull, id, (2 * trank) & 31);
   const int xoi = __shfl_sync(kFull, id, (2 * trank + 1) & 31);
-  int nst = ust, nc = c, nr = (urot + 1 == c) ? 0 : urot + 1;
-  unsigned w0 = m0, w1 = m1, w2 = m2;
+  int nst = 0, nc = 0, nr = 0, fnv = 0;
+  unsigned w0 = 0u, w1 = 0u, w2 = 0u;
+  if (kept) {
+    fnv = P.fn[lane];
+    w0 = P.fm0[lane];
+    w1 = P.fm1[lane];
+    w2 = P.fm2[lane];
+    nst = P.fst[lane];
+    nc = P.fc[lane];
+    const int fr0 = P.fr[lane];
+    nr = (fr0 + 1 == nc) ? 0 : fr0 + 1;
+  }
   if (touched) {
     nst = base + eoff;
     nc = nsz;
     nr = 0;
-    w0 = m0 & I0;
-    w1 = m1 & I1;
-    w2 = m2 & I2;
+    w0 &= I0;
+    w1 &= I1;
+    w2 &= I2;
     if (xio < 32) w0 |= 1u << xio;
     else if (xio < 64) w1 |= 1u << (xio - 32);
     else w2 |= 1u << (xio - 64);
