@@ -345,6 +345,17 @@ def autotuned_leg(args, v, d_pts, flush):
             "note": "same step on the autotuner's grid for this input"}
 
 
+def tuning_args(args) -> dict:
+    """The first tier's launch settings from the command line (profiling and
+    A/B runs; the defaults are the library's)."""
+    out = {}
+    if args.fast_layout:
+        out["fast_layout"] = args.fast_layout
+    if args.fast_blocks:
+        out["fast_blocks_per_sm"] = args.fast_blocks
+    return out
+
+
 def run_ours(args):
     import torch
     ws, rank, local = dist_env()
@@ -362,6 +373,7 @@ def run_ours(args):
     d_pts = torch.from_numpy(pts).to(f"cuda:{local}")
     tess = v.Tessellation(v.BoundingBox([0, 0, 0], [1, 1, 1]), v.Algorithm3DGrid(GRID, GRID, GRID))
     tess.set_precision(args.precision)
+    tess.set_tuning(tuning_args(args))
     stream = torch.cuda.ExternalStream(tess.stream(), device=f"cuda:{local}")
     flush = torch.empty(512 << 20, dtype=torch.uint8, device=f"cuda:{local}")
 
@@ -873,6 +885,10 @@ def main():
     ap.add_argument("--ref-sample", type=int, default=0,
                     help="cells per step of the reference arm (0 = every cell of the workload)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--fast-layout", choices=["slots", "full"], default=None,
+                    help="first-tier polytope layout (default: the library's)")
+    ap.add_argument("--fast-blocks", type=int, choices=[6, 7, 8], default=None,
+                    help="first-tier blocks per SM, slot layout (default: the library's)")
     ap.add_argument("--no-side-configs", action="store_true",
                     help="skip the clustered, batched and serving-sweep keys of the default line")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")

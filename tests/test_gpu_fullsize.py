@@ -110,15 +110,22 @@ def batch_4096():
 
 
 def member_oracle(oracle_mod, member, relax_steps=0):
+    """A batch member's oracle tessellation after `relax_steps` Lloyd steps;
+    its truncated search order (large grids) is doubled and the whole chain
+    redone whenever a cell walks off it."""
     edge, grid, pts, sphere = member
     walls = [sphere] if sphere else []
     k = 8 if (2 * grid[0] + 1) * (2 * grid[1] + 1) * (2 * grid[2] + 1) > 20000 else 0
-    o = oracle_with_table(oracle_mod, [0, 0, 0], list(edge), grid, pts, walls, k=k)
-    for _ in range(relax_steps):
-        o.relax()
-        o.calculate(NTHREADS)
-        o._check_table()
-    return o
+    while True:
+        o = oracle_with_table(oracle_mod, [0, 0, 0], list(edge), grid, pts, walls, k=k)
+        try:
+            for _ in range(relax_steps):
+                o.relax()
+                o.calculate(NTHREADS)
+            return o
+        except RuntimeError:
+            assert k > 0
+            k *= 2
 
 
 def test_batch_4096_members_bitwise(oracle_mod, batch_4096):
