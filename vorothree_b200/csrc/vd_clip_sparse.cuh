@@ -44,6 +44,7 @@ struct SparseCfg {
   static constexpr int FCAP = F;   // faces (one lane each)
   static constexpr int ECAP = E;   // face entries per entry buffer
   static constexpr int XCAP = 32;  // crossing edges per clip (one lane each)
+  static constexpr int TCAP = 128; // edges of the touched faces per clip (32 per round)
   static_assert(V > 64 && V <= 96, "vertex slots take three 32-bit mask words");
   static_assert(V < 255, "vertex slots are bytes; 255 marks an empty lid-map entry");
   static_assert(F <= 32, "one lane per face");
@@ -86,10 +87,14 @@ struct alignas(16) SparsePoly {
   uint8_t fc[C::FCAP];                               // entry count
   uint8_t fr[C::FCAP];                               // rotation: logical entry j is ent[fst + (j + fr) % fc]
   uint8_t ent[2][C::ECAP];                           // face entries (vertex slots); the second buffer for compaction
-  // per clip: crossing edge g (touched face of rank k: g = 2k in->out, 2k+1 out->in)
+  // per clip: the crossing edges in walk order (touched faces in face order,
+  // each from its logical first entry); touched face k's two are 2k, 2k+1
   uint16_t xkey[C::XCAP];  // (min, max) slot pair of the edge
   uint8_t xs[C::XCAP], xe[C::XCAP];  // the edge as the face walks it
   uint16_t xpos[C::XCAP];  // entry that receives the intersection vertex; finalize: first triangle of face g
+  uint8_t xt[C::XCAP];     // 1: in->out, 0: out->in
+  uint8_t xf[C::XCAP];     // rank of the crossing's face among the touched faces
+  uint8_t tpf[C::TCAP];    // face of each touched-face edge (edges in walk order)
   uint8_t lidmap[C::VCAP];
   uint8_t cand_e[32];  // walk: search-order entry of each candidate of a round
 };
@@ -337,43 +342,68 @@ __device__ int warp_clip(SparsePoly<C>& P, SparseState& S, double px, double py,
     }
   }
 
-  // 3. each touched face walks its loop from its logical first entry, as the
-  //    face walk of :369-452 does: in->in emits the end, in->out the
-  //    intersection, out->in the intersection and the end
-  bool bad = false;
-  if (touched) {
-    const uint8_t* Es = &P.ent[src][st];
-    uint8_t* D = &P.ent[dst][base + eoff];
-    int q = rot, k = 0, nio = 0, noi = 0;
-    unsigned s = Es[q];
-    bool si = sp_bit(I0, I1, I2, s);
-    for (int j = 0; j < c; ++j) {
-      const int q2 = (q + 1 == c) ? 0 : q + 1;
-      const unsigned e = Es[q2];
-      const bool ei = sp_bit(I0, I1, I2, e);
-      if (si != ei) {
-        const int g = 2 * trank + (si ? 0 : 1);
-        if ((si ? nio : noi) == 0) {
-          P.xkey[g] = (uint16_t)(s < e ? (s << 8 | e) : (e << 8 | s));
-          P.xs[g] = (uint8_t)s;
-          P.xe[g] = (uint8_t)e;
-          P.xpos[g] = (uint16_t)(base + eoff + k);
+  // 3. the touched faces' edges in walk order (faces in order, each from its
+  //    logical first entry), one lane per edge, 32 per round -- the face walk
+  //    of :369-452: in->in emits the end, in->out the intersection, out->in
+  //    the intersection and the end.  The new faces follow one another in
+  //    face order, so an emitted entry's place is the running count of the
+  //    entries emitted before it.  Crossings are listed in walk order.
+  {
+    const int tsz = touched ? c : 0;
+    const int tinc = warp_incl_scan(tsz);
+    const int tpos0 = tinc - tsz;
+    const int np = __shfl_sync(kFull, tinc, 31);
+    if (np > C::TCAP) return kClipOverflow;
+    for (int j = 0; j < tsz; ++j) P.tpf[tpos0 + j] = (uint8_t)lane;
+    __syncwarp();
+    uint8_t* D = P.ent[dst];
+    const int dend = base + tot_new;
+    int run = base, ncr = 0;
+    for (int r0 = 0; r0 < np; r0 += 32) {
+      const int i = r0 + (int)lane;
+      const bool act = i < np;
+      const int f = act ? P.tpf[i] : 0;
+      const int fst0 = __shfl_sync(kFull, st, f), frot = __shfl_sync(kFull, rot, f);
+      const int fcn = __shfl_sync(kFull, c, f), ftp = __shfl_sync(kFull, tpos0, f);
+      const int frank = __shfl_sync(kFull, trank, f);
+      unsigned sv = 0, ev = 0;
+      bool si = false, ei = false;
+      if (act) {
+        int q = i - ftp + frot;
+        if (q >= fcn) q -= fcn;
+        const int q2 = (q + 1 == fcn) ? 0 : q + 1;
+        sv = P.ent[src][fst0 + q];
+        ev = P.ent[src][fst0 + q2];
+        si = sp_bit(I0, I1, I2, sv);
+        ei = sp_bit(I0, I1, I2, ev);
+      }
+      const int emit = act ? (si ? 1 : (ei ? 2 : 0)) : 0;
+      const int einc = warp_incl_scan(emit);
+      const int idx = run + einc - emit;
+      const bool cr = act && si != ei;
+      const unsigned cm = __ballot_sync(kFull, cr);
+      if (cr) {
+        const int g = ncr + __popc(cm & lt);
+        if (g < C::XCAP) {
+          P.xkey[g] = (uint16_t)(sv < ev ? (sv << 8 | ev) : (ev << 8 | sv));
+          P.xs[g] = (uint8_t)sv;
+          P.xe[g] = (uint8_t)ev;
+          P.xpos[g] = (uint16_t)idx;  // the intersection's entry, written once its slot is known
+          P.xt[g] = si ? 1 : 0;
+          P.xf[g] = (uint8_t)frank;
         }
-        if (si) ++nio;
-        else ++noi;
-        ++k;  // the intersection's entry, written once its slot is known
       }
       if (ei) {
-        if (k < nsz) D[k] = (uint8_t)e;
-        ++k;
+        const int k = idx + (si ? 0 : 1);
+        if (k < dend) D[k] = (uint8_t)ev;
       }
-      s = e;
-      si = ei;
-      q = q2;
+      run += __shfl_sync(kFull, einc, 31);
+      ncr += __popc(cm);
     }
-    bad = nio != 1 || noi != 1 || k != nsz;
+    // every touched face has one in->out and one out->in crossing (then it
+    // emitted exactly its kept vertices and two intersections)
+    if (run != dend || ncr != 2 * ntouch) return kClipOverflow;
   }
-  if (__any_sync(kFull, bad)) return kClipOverflow;
   __syncwarp();
 
   // 4. intersection vertices: crossing g is lane g; the first of the two
@@ -382,6 +412,10 @@ __device__ int warp_clip(SparsePoly<C>& P, SparseState& S, double px, double py,
   //    (the intersection_map of :391-417 / :422-448)
   const int ncross = 2 * ntouch;
   const bool act = (int)lane < ncross;
+  // crossings 2k and 2k+1 belong to touched face k, one of each direction
+  const unsigned tg = act ? (unsigned)P.xt[lane] : 0u;
+  const unsigned tother = __shfl_xor_sync(kFull, tg, 1);
+  if (__any_sync(kFull, act && ((int)P.xf[lane] != ((int)lane >> 1) || tg == tother))) return kClipOverflow;
   const unsigned key = act ? (unsigned)P.xkey[lane] : (0xFFFF0000u | lane);
   const unsigned mm = __match_any_sync(kFull, key);
   const int leader = __ffs(mm) - 1;
@@ -451,8 +485,11 @@ __device__ int warp_clip(SparsePoly<C>& P, SparseState& S, double px, double py,
   //    segments' starts are distinct, their ends are distinct, and every end
   //    is the start of a segment -- otherwise the full clip takes the cell)
   const bool sact = (int)lane < ntouch;
-  const int ida = __shfl_sync(kFull, id, (2 * (int)lane + 1) & 31);
-  const int idb = __shfl_sync(kFull, id, (2 * (int)lane) & 31);
+  const int id0 = __shfl_sync(kFull, id, (2 * (int)lane) & 31);
+  const int id1 = __shfl_sync(kFull, id, (2 * (int)lane + 1) & 31);
+  const bool io0 = __shfl_sync(kFull, tg, (2 * (int)lane) & 31) != 0u;  // crossing 2k is the in->out one
+  const int ida = io0 ? id1 : id0;
+  const int idb = io0 ? id0 : id1;
   const unsigned a = sact ? (unsigned)ida : (0xFFFF0000u | lane);
   const unsigned bend = sact ? (unsigned)idb : (0xFFFE0000u | lane);
   const unsigned ma = __match_any_sync(kFull, a);
@@ -489,8 +526,11 @@ __device__ int warp_clip(SparsePoly<C>& P, SparseState& S, double px, double py,
   // 6. the face table: surviving faces in order, then the lid
   //    (each lane reads its face's entry again rather than keeping it in
   //    registers through steps 3-5)
-  const int xio = __shfl_sync(kFull, id, (2 * trank) & 31);
-  const int xoi = __shfl_sync(kFull, id, (2 * trank + 1) & 31);
+  const int xk0 = __shfl_sync(kFull, id, (2 * trank) & 31);
+  const int xk1 = __shfl_sync(kFull, id, (2 * trank + 1) & 31);
+  const bool kio0 = __shfl_sync(kFull, tg, (2 * trank) & 31) != 0u;
+  const int xio = kio0 ? xk0 : xk1;
+  const int xoi = kio0 ? xk1 : xk0;
   int nst = 0, nc = 0, nr = 0, fnv = 0;
   unsigned w0 = 0u, w1 = 0u, w2 = 0u;
   if (kept) {
