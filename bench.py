@@ -887,7 +887,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--fast-layout", choices=["slots", "full"], default=None,
                     help="first-tier polytope layout (default: the library's)")
-    ap.add_argument("--fast-blocks", type=int, choices=[6, 7, 8], default=None,
+    ap.add_argument("--fast-blocks", type=int, choices=[5, 6, 7], default=None,
                     help="first-tier blocks per SM, slot layout (default: the library's)")
     ap.add_argument("--no-side-configs", action="store_true",
                     help="skip the clustered, batched and serving-sweep keys of the default line")

@@ -57,14 +57,14 @@ def test_lookup_tuning_defaults_and_overrides():
     from vorothree_b200 import autotune as at
     d = at.lookup_tuning("uniform", 1 << 20, {})
     assert d == dict(at.DEFAULT_TUNING, **at.DEFAULT_HANDOFF)
-    entries = {at.key("uniform", 1 << 20): {"factor": 1.6, "tuning": {"fast_layout": "full", "fast_blocks_per_sm": 7}},
+    entries = {at.key("uniform", 1 << 20): {"factor": 1.6, "tuning": {"fast_layout": "full", "fast_blocks_per_sm": 6}},
                at.key("clustered", 1 << 20): {"factor": 2.5, "tuning": {"fast_layout": "slots",
-                                                                         "fast_blocks_per_sm": 8}},
+                                                                         "fast_blocks_per_sm": 5}},
                at.HANDOFF_KEY: {"tuning": {"huge_direct_max": 16, "huge_blocks_max": 64, "huge_narrow_max": 5000}}}
     u = at.lookup_tuning("uniform", 1 << 19, entries)
     assert u["fast_layout"] == "full" and u["huge_direct_max"] == 16 and u["huge_narrow_max"] == 5000
     c = at.lookup_tuning("clustered", 1 << 21, entries)
-    assert c["fast_blocks_per_sm"] == 8 and c["fast_layout"] == "slots"
+    assert c["fast_blocks_per_sm"] == 5 and c["fast_layout"] == "slots"
 
 
 @pytest.mark.gpu
@@ -74,10 +74,10 @@ def test_tune_on_gpu(oracle_mod):
     b = v.BoundingBox([0, 0, 0], [1, 1, 1])
     pts = blobs(40_000, 8, 0.02, 0.7, 5)
     entries = at.tune(pts, b, factors=(0.8, 1.6, 3.2), reps=1, entries={}, layouts=("slots", "full"),
-                      blocks=(7, 8))
+                      blocks=(6, 7))
     (k, e), = entries.items()
     assert k == at.key("clustered", len(pts)) and e["factor"] in (0.8, 1.6, 3.2)
-    # three densities, then slots at 8 blocks per SM and the full layout
+    # three densities, then slots at 7 blocks per SM and the full layout
     assert len(e["trials"]) == 5 and all(t["ms"] > 0 for t in e["trials"])
     assert e["tuning"]["fast_layout"] in ("slots", "full")
     # the chosen grid computes the oracle's cells on that grid
@@ -109,7 +109,7 @@ def test_every_tuning_choice_gives_the_oracles_cells(oracle_mod):
         ov, oc, on = o.summaries()
         oids = o.neighbors()[1]
         choices = [dict(fast_layout=l, fast_blocks_per_sm=nb) for l, nb in
-                   (("slots", 6), ("slots", 7), ("slots", 8), ("full", 7))]
+                   (("slots", 5), ("slots", 6), ("slots", 7), ("full", 6))]
         handoffs = [dict(huge_direct_max=dm, huge_narrow_max=nm, huge_blocks_max=hb)
                     for dm, nm, hb in itertools.product((1, 256), (500, 5000), (2, 64))]
         for tun in choices + [dict(choices[1], **h) for h in handoffs]:

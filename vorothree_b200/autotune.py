@@ -6,7 +6,7 @@ What it picks, per input class (distribution, size bucket):
     opens many empty bins (sparse regions);
   * the first tier's polytope layout ("slots": a clip rewrites only the
     faces it cuts; "full": every face loop per clip) and, for the slot
-    layout, its register budget -- 6, 7 or 8 blocks of four warps per SM, the
+    layout, its register budget -- 5, 6 or 7 blocks of four warps per SM, the
     compiled variants (more resident warps against more spills).
 and once for the tessellation, on inputs with cells adjacent to thousands of
 others (the reference's sphere-surface benchmark distribution):
@@ -46,8 +46,8 @@ DEFAULT_FACTOR = {"uniform": 1.0, "clustered": 2.5}
 _SAMPLE = 1 << 16
 # the first tier's choices the tuner searches, and the library's defaults
 LAYOUTS = ("slots", "full")
-BLOCKS_PER_SM = (6, 7, 8)
-DEFAULT_TUNING = {"fast_layout": "slots", "fast_blocks_per_sm": 7}
+BLOCKS_PER_SM = (5, 6, 7)
+DEFAULT_TUNING = {"fast_layout": "slots", "fast_blocks_per_sm": 6}
 # the block-per-cell tier's hand-off, searched once (HANDOFF_KEY)
 HANDOFF_KEY = "handoff"
 DIRECT_MAX = (1, 16, 64, 256)
@@ -207,7 +207,7 @@ def tune(points, bounds, walls: Sequence = (), factors: Iterable[float] = FACTOR
     win = min(trials, key=lambda r: r["ms"])
     g = win["grid"]
     for layout in layouts:
-        for nb in (blocks if layout == "slots" else (7,)):
+        for nb in (blocks if layout == "slots" else (6,)):
             tun = {"fast_layout": layout, "fast_blocks_per_sm": nb}
             if tun == DEFAULT_TUNING:
                 continue

@@ -95,7 +95,7 @@ struct alignas(16) SparsePoly {
   uint8_t xt[C::XCAP];     // 1: in->out, 0: out->in
   uint8_t xf[C::XCAP];     // rank of the crossing's face among the touched faces
   uint8_t tpf[C::TCAP];    // face of each touched-face edge (edges in walk order)
-  uint8_t lidmap[C::VCAP];
+  uint8_t freel[C::VCAP];   // per clip: the free slots in order
   uint8_t cand_e[32];  // walk: search-order entry of each candidate of a round
 };
 
@@ -114,10 +114,15 @@ __device__ __forceinline__ bool sp_bit(unsigned a, unsigned b, unsigned c, unsig
   return (sp_word(a, b, c, s) >> (s & 31u)) & 1u;
 }
 
-// position of the r-th (from 0) set bit of m, or -1
-__device__ __forceinline__ int sp_nth_bit(unsigned m, int r) {
-  for (; r > 0 && m; --r) m &= m - 1u;
-  return m ? __ffs(m) - 1 : -1;
+// The largest of the lanes' values, each a non-negative double or NaN (NaN
+// counts as 0, as fmax and the reference's `d2 > max` comparison treat it).
+// Non-negative doubles order like their bit patterns as unsigned integers, so
+// two 32-bit reductions give exactly fmax's result.
+__device__ __forceinline__ double sp_warp_max_nonneg(double x) {
+  const unsigned long long b = (x >= 0.0) ? (unsigned long long)__double_as_longlong(x) : 0ull;
+  const unsigned hi = __reduce_max_sync(kFull, (unsigned)(b >> 32));
+  const unsigned lo = __reduce_max_sync(kFull, (unsigned)(b >> 32) == hi ? (unsigned)b : 0u);
+  return __longlong_as_double((long long)(((unsigned long long)hi << 32) | lo));
 }
 
 // Cell3DFaces::new (cell_3d_faces.rs:37-74): the box, faces z-, z+, y-, y+,
@@ -193,7 +198,7 @@ __device__ double poly_max_radius_sq(const SparsePoly<C>& P, const SparseState& 
     const unsigned Lw = w == 0 ? S.live0 : (w == 1 ? S.live1 : S.live2);
     if ((Lw >> lane) & 1u) m = fmax(m, P.vr2[32 * w + lane]);
   }
-  return warp_max(m);
+  return sp_warp_max_nonneg(m);
 }
 
 // clip_with_scratch (cell_3d_faces.rs:288-503) on the slot layout.  All lanes
@@ -421,22 +426,30 @@ __device__ int warp_clip(SparsePoly<C>& P, SparseState& S, double px, double py,
   const int leader = __ffs(mm) - 1;
   const bool isl = act && leader == (int)lane;
   if (__any_sync(kFull, act && __popc(mm) != 2)) return kClipOverflow;
+  // the other crossing of the same edge: the neighbouring touched face walks
+  // the edge the other way, so an in->out crossing's partner is out->in
+  const int partner = act ? __ffs(mm & ~(1u << lane)) - 1 : (int)lane;
+  if (__any_sync(kFull, act && tg == __shfl_sync(kFull, tg, partner & 31))) return kClipOverflow;
   const unsigned dm = __ballot_sync(kFull, isl);
   cnt_add(P, kCntIntersections, (unsigned long long)__popc(dm));
-  // the new vertex takes the r-th free slot (cut-away slots are free again)
-  int slot = -1;
-  if (isl) {
-    const int r = __popc(dm & lt);
+  // the new vertex of discovery rank r takes the r-th free slot (cut-away
+  //    slots are free again): the free slots listed in order, word by word,
+  //    as far as the new vertices need
+  const int nnew = __popc(dm);
+  {
     unsigned F2 = ~I2;
     if constexpr (C::VCAP < 96) F2 &= (1u << (C::VCAP < 96 ? C::VCAP - 64 : 0)) - 1u;
     const unsigned F0 = ~I0, F1 = ~I1;
-    const int c0 = __popc(F0), c1 = __popc(F1);
-    const int w = r < c0 ? 0 : (r < c0 + c1 ? 1 : 2);
-    const int nb = sp_nth_bit(w == 0 ? F0 : (w == 1 ? F1 : F2), r - (w >= 1 ? c0 : 0) - (w == 2 ? c1 : 0));
-    slot = nb < 0 ? -1 : 32 * w + nb;
-    if (slot >= C::VCAP) slot = -1;
+    const int c0 = __popc(F0), c1 = __popc(F1), c2 = __popc(F2);
+    if (nnew > c0 + c1 + c2) return kClipOverflow;
+    if ((F0 >> lane) & 1u) P.freel[__popc(F0 & lt)] = (uint8_t)lane;
+    if (nnew > c0) {
+      if ((F1 >> lane) & 1u) P.freel[c0 + __popc(F1 & lt)] = (uint8_t)(32 + lane);
+      if (nnew > c0 + c1 && ((F2 >> lane) & 1u)) P.freel[c0 + c1 + __popc(F2 & lt)] = (uint8_t)(64 + lane);
+    }
+    __syncwarp();
   }
-  if (__any_sync(kFull, isl && slot < 0)) return kClipOverflow;
+  const int slot = isl ? (int)P.freel[__popc(dm & lt)] : -1;
   double ix = 0.0, iy = 0.0, iz = 0.0, d2 = 0.0;
   if (isl) {
     const unsigned s = P.xs[lane], e = P.xe[lane];
@@ -463,7 +476,6 @@ __device__ int warp_clip(SparsePoly<C>& P, SparseState& S, double px, double py,
     P.vy[slot] = iy;
     P.vz[slot] = iz;
     P.vr2[slot] = d2;
-    P.lidmap[slot] = 0xFF;
     if constexpr (C::MIXED) {
       const float fx = (float)(ix - gx), fy = (float)(iy - gy), fz = (float)(iz - gz);
       P.ux[slot] = fx;
@@ -480,30 +492,20 @@ __device__ int warp_clip(SparsePoly<C>& P, SparseState& S, double px, double py,
   const int nhw = max(hw, (int)__reduce_max_sync(kFull, isl ? (unsigned)(slot + 1) : 0u));
 
   // 5. the lid (:470-495): touched face k gives the segment (X of its
-  //    out->in crossing, X of its in->out crossing); lid_map[start] = end,
-  //    and the chain from segment 0 is ranked by pointer jumping (the
-  //    segments' starts are distinct, their ends are distinct, and every end
-  //    is the start of a segment -- otherwise the full clip takes the cell)
+  //    out->in crossing, X of its in->out crossing), and lid_map[start] = end.
+  //    The end of segment k is the intersection on its in->out edge, which
+  //    is the out->in intersection -- the start -- of the face across that
+  //    edge: the segment that follows k in the chain is the face of its
+  //    in->out crossing's partner.  Every face has one crossing of each
+  //    direction and crossings pair up, so the successors form a
+  //    permutation; the chain from segment 0 is ranked by pointer jumping.
   const bool sact = (int)lane < ntouch;
   const int id0 = __shfl_sync(kFull, id, (2 * (int)lane) & 31);
   const int id1 = __shfl_sync(kFull, id, (2 * (int)lane + 1) & 31);
   const bool io0 = __shfl_sync(kFull, tg, (2 * (int)lane) & 31) != 0u;  // crossing 2k is the in->out one
-  const int ida = io0 ? id1 : id0;
-  const int idb = io0 ? id0 : id1;
-  const unsigned a = sact ? (unsigned)ida : (0xFFFF0000u | lane);
-  const unsigned bend = sact ? (unsigned)idb : (0xFFFE0000u | lane);
-  const unsigned ma = __match_any_sync(kFull, a);
-  const unsigned mb = __match_any_sync(kFull, bend);
-  __syncwarp();
-  if (sact) P.lidmap[a] = (uint8_t)lane;
-  __syncwarp();
-  unsigned succ = lane;
-  bool good = true;
-  if (sact) {
-    succ = P.lidmap[bend];
-    good = __popc(ma) == 1 && __popc(mb) == 1 && succ < (unsigned)ntouch;
-  }
-  if (!__all_sync(kFull, good)) return kClipOverflow;
+  const unsigned a = (unsigned)(io0 ? id1 : id0);
+  const int pio = __shfl_sync(kFull, partner, (2 * (int)lane + (io0 ? 0 : 1)) & 31);
+  const unsigned succ = sact ? (unsigned)(pio >> 1) : lane;
   const int term = __ffs(__ballot_sync(kFull, sact && succ == 0u)) - 1;
   int nxt = (sact && (int)lane != term) ? (int)succ : (int)lane;
   int dd = nxt != (int)lane ? 1 : 0;
@@ -602,10 +604,11 @@ __device__ int warp_clip(SparsePoly<C>& P, SparseState& S, double px, double py,
       }
     }
   }
-  if constexpr (C::MIXED) S.umax = warp_max((double)um) * (1.0 + 0x1p-20);
+  if constexpr (C::MIXED)  // non-negative floats order like their bits
+    S.umax = (double)__uint_as_float(__reduce_max_sync(kFull, __float_as_uint(um))) * (1.0 + 0x1p-20);
   if (with_gen) cnt_add(P, kCntKept, (unsigned long long)(__popc(I0) + __popc(I1) + __popc(I2)));
   __syncwarp();
-  *r2out = with_gen ? warp_max(r2) : 0.0;
+  *r2out = with_gen ? sp_warp_max_nonneg(r2) : 0.0;
   return kClipMod;
 }
 

@@ -308,9 +308,9 @@ struct vd_tess {
   unsigned long long counters[kNumCounters] = {};
   unsigned long long fallback[2] = {0, 0};
   ClipLaunchInfo info64{}, infomx{}, infomed{};
-  ClipLaunchInfo infosp64[3]{}, infospmx[3]{};  // slot layout at 6, 7, 8 blocks per SM
+  ClipLaunchInfo infosp64[3]{}, infospmx[3]{};  // slot layout at 5, 6, 7 blocks per SM
   int fast_layout = VD_FAST_SLOTS;
-  int fast_minb = 7;
+  int fast_minb = 6;
   int huge_direct_max = 64;
   int huge_blocks_max = 64;
   int huge_narrow_max = 2000;
@@ -641,7 +641,7 @@ int clip_pass(vd_tess* t, int tier, const uint32_t* items, uint32_t nitems, uint
     // the slot layout cannot export a polytope in the reference's vertex
     // order: get_cell's rebuild runs the full-rewrite kernel
     const bool slots = t->fast_layout == VD_FAST_SLOTS && !W.ex_verts;
-    const int mv = t->fast_minb - 6;
+    const int mv = t->fast_minb - 5;
     const ClipLaunchInfo& li =
         slots ? (mixed ? t->infospmx[mv] : t->infosp64[mv]) : (mixed ? t->infomx : t->info64);
     const size_t warps_needed = (nitems + li.warps_per_block - 1) / li.warps_per_block;
@@ -1064,8 +1064,8 @@ int vd_tess_create(const double bmin[3], const double bmax[3], int nx, int ny, i
   e = clip_fp64_info(&t->info64);
   if (e == cudaSuccess) e = clip_mixed_info(&t->infomx);
   for (int k = 0; k < 3 && e == cudaSuccess; ++k) {
-    e = clip_sparse_info(false, 6 + k, &t->infosp64[k]);
-    if (e == cudaSuccess) e = clip_sparse_info(true, 6 + k, &t->infospmx[k]);
+    e = clip_sparse_info(false, 5 + k, &t->infosp64[k]);
+    if (e == cudaSuccess) e = clip_sparse_info(true, 5 + k, &t->infospmx[k]);
   }
   if (e == cudaSuccess) e = clip_med_setup(&t->infomed);
   if (e == cudaSuccess) e = seal_setup();
@@ -1594,12 +1594,12 @@ int vd_tess_set_tuning(vd_tess* t, const vd_tuning* k) {
   if (!t || !k) return VD_EINVAL;
   if (k->fast_layout != 0 && k->fast_layout != VD_FAST_FULL)
     return fail(t, VD_EINVAL, "unknown fast-tier layout %d", k->fast_layout);
-  if (k->fast_blocks_per_sm != 0 && (k->fast_blocks_per_sm < 6 || k->fast_blocks_per_sm > 8))
-    return fail(t, VD_EINVAL, "fast_blocks_per_sm must be 6, 7 or 8");
+  if (k->fast_blocks_per_sm != 0 && (k->fast_blocks_per_sm < 5 || k->fast_blocks_per_sm > 7))
+    return fail(t, VD_EINVAL, "fast_blocks_per_sm must be 5, 6 or 7");
   if (k->huge_direct_max < 0 || k->huge_blocks_max < 0 || k->huge_blocks_max > 256 || k->huge_narrow_max < 0)
     return fail(t, VD_EINVAL, "huge-tier settings out of range");
   t->fast_layout = k->fast_layout;
-  t->fast_minb = k->fast_blocks_per_sm ? k->fast_blocks_per_sm : 7;
+  t->fast_minb = k->fast_blocks_per_sm ? k->fast_blocks_per_sm : 6;
   t->huge_direct_max = k->huge_direct_max ? k->huge_direct_max : 64;
   t->huge_blocks_max = k->huge_blocks_max ? k->huge_blocks_max : kHugeBlocksMax;
   t->huge_narrow_max = k->huge_narrow_max ? k->huge_narrow_max : 2000;

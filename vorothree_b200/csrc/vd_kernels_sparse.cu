@@ -10,9 +10,10 @@
 namespace vd {
 
 // blocks of 4 warps per SM the register budget must admit (shared memory
-// admits this many too): single tessellations are compiled for 6, 7 and 8
-// (a tuning setting, 7 by default; the instrumented variant for 7 only),
-// batches for 6 (their member lookup needs more registers)
+// admits this many too): single tessellations are compiled for 5, 6 and 7
+// (a tuning setting; 6 by default, measured fastest on 1 M uniform cells:
+// 40.8 ms against 44.4 at 7 and 45.6 at 8, where the tighter register budget
+// spills more; the instrumented variant for 6 only), batches for 6
 constexpr int kSparseBatchMinBlocks = 6;
 
 namespace {
@@ -60,31 +61,31 @@ void launch_batched(const TessDesc* descs, const uint32_t* tess_off, int ntess, 
 }  // namespace
 
 cudaError_t clip_sparse_info(bool mixed, int minb, ClipLaunchInfo* info) {
-  cudaError_t e = mixed ? setup_one<MixedSparseCount, 7>(nullptr) : setup_one<FastSparseCount, 7>(nullptr);
+  cudaError_t e = mixed ? setup_one<MixedSparseCount, 6>(nullptr) : setup_one<FastSparseCount, 6>(nullptr);
   if (e != cudaSuccess) return e;
   if (mixed) {
-    if (minb == 6) return setup_one<MixedSparse, 6>(info);
-    if (minb == 8) return setup_one<MixedSparse, 8>(info);
-    return setup_one<MixedSparse, 7>(info);
+    if (minb == 5) return setup_one<MixedSparse, 5>(info);
+    if (minb == 7) return setup_one<MixedSparse, 7>(info);
+    return setup_one<MixedSparse, 6>(info);
   }
-  if (minb == 6) return setup_one<FastSparse, 6>(info);
-  if (minb == 8) return setup_one<FastSparse, 8>(info);
-  return setup_one<FastSparse, 7>(info);
+  if (minb == 5) return setup_one<FastSparse, 5>(info);
+  if (minb == 7) return setup_one<FastSparse, 7>(info);
+  return setup_one<FastSparse, 6>(info);
 }
 
-// count: the instrumented variant (always at 7 blocks per SM)
+// count: the instrumented variant (always at 6 blocks per SM)
 cudaError_t launch_clip_sparse(const TessDesc& T, const WorkList& W, int nblocks, bool count, bool mixed, int minb,
                                cudaStream_t s) {
   if (mixed) {
-    if (count) launch_one<MixedSparseCount, 7>(T, W, nblocks, s);
-    else if (minb == 6) launch_one<MixedSparse, 6>(T, W, nblocks, s);
-    else if (minb == 8) launch_one<MixedSparse, 8>(T, W, nblocks, s);
-    else launch_one<MixedSparse, 7>(T, W, nblocks, s);
+    if (count) launch_one<MixedSparseCount, 6>(T, W, nblocks, s);
+    else if (minb == 5) launch_one<MixedSparse, 5>(T, W, nblocks, s);
+    else if (minb == 7) launch_one<MixedSparse, 7>(T, W, nblocks, s);
+    else launch_one<MixedSparse, 6>(T, W, nblocks, s);
   } else {
-    if (count) launch_one<FastSparseCount, 7>(T, W, nblocks, s);
-    else if (minb == 6) launch_one<FastSparse, 6>(T, W, nblocks, s);
-    else if (minb == 8) launch_one<FastSparse, 8>(T, W, nblocks, s);
-    else launch_one<FastSparse, 7>(T, W, nblocks, s);
+    if (count) launch_one<FastSparseCount, 6>(T, W, nblocks, s);
+    else if (minb == 5) launch_one<FastSparse, 5>(T, W, nblocks, s);
+    else if (minb == 7) launch_one<FastSparse, 7>(T, W, nblocks, s);
+    else launch_one<FastSparse, 6>(T, W, nblocks, s);
   }
   return cudaGetLastError();
 }

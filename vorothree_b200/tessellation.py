@@ -539,7 +539,7 @@ class Tessellation:
 
     def set_tuning(self, tuning: dict):
         """Launch choices that change no result (the autotuner's): any of
-        fast_layout ('slots' / 'full'), fast_blocks_per_sm (6, 7, 8),
+        fast_layout ('slots' / 'full'), fast_blocks_per_sm (5, 6, 7),
         huge_direct_max, huge_blocks_max, huge_narrow_max; keys left out keep
         their current value."""
         cur = self.get_tuning()
