@@ -429,7 +429,8 @@ __device__ int warp_clip(SparsePoly<C>& P, SparseState& S, double px, double py,
   // the other crossing of the same edge: the neighbouring touched face walks
   // the edge the other way, so an in->out crossing's partner is out->in
   const int partner = act ? __ffs(mm & ~(1u << lane)) - 1 : (int)lane;
-  if (__any_sync(kFull, act && tg == __shfl_sync(kFull, tg, partner & 31))) return kClipOverflow;
+  const unsigned ptg = __shfl_sync(kFull, tg, partner & 31);  // every lane shuffles
+  if (__any_sync(kFull, act && tg == ptg)) return kClipOverflow;
   const unsigned dm = __ballot_sync(kFull, isl);
   cnt_add(P, kCntIntersections, (unsigned long long)__popc(dm));
   // the new vertex of discovery rank r takes the r-th free slot (cut-away
