@@ -44,7 +44,7 @@ struct SparseCfg {
   static constexpr int FCAP = F;   // faces (one lane each)
   static constexpr int ECAP = E;   // face entries per entry buffer
   static constexpr int XCAP = 32;  // crossing edges per clip (one lane each)
-  static constexpr int TCAP = 128; // edges of the touched faces per clip (32 per round)
+  static constexpr int TCAP = 256; // edges of the touched faces per clip (32 per round)
   static_assert(V > 64 && V <= 96, "vertex slots take three 32-bit mask words");
   static_assert(V < 255, "vertex slots are bytes; 255 marks an empty lid-map entry");
   static_assert(F <= 32, "one lane per face");
@@ -94,7 +94,7 @@ struct alignas(16) SparsePoly {
   uint16_t xpos[C::XCAP];  // entry that receives the intersection vertex; finalize: first triangle of face g
   uint8_t xt[C::XCAP];     // 1: in->out, 0: out->in
   uint8_t xf[C::XCAP];     // rank of the crossing's face among the touched faces
-  uint8_t tpf[C::TCAP];    // face of each touched-face edge (edges in walk order)
+  uint8_t tmap[32];        // face of each touched-face rank
   uint8_t freel[C::VCAP];   // per clip: the free slots in order
   uint8_t cand_e[32];  // walk: search-order entry of each candidate of a round
 };
@@ -219,7 +219,7 @@ __device__ int warp_clip(SparsePoly<C>& P, SparseState& S, double px, double py,
   unsigned O0 = 0u, O1 = 0u, O2 = 0u;
   bool sin = false;
   {
-    double bound = 0.0, hi_out = 0.0, lo_sin = 0.0, band_lo = 0.0, band_hi = 0.0, c = 0.0;
+    float hi_out = 0.f, lo_sin = 0.f, band_lo = 0.f, band_hi = 0.f;
     float fnx = 0.f, fny = 0.f, fnz = 0.f, fc = 0.f;
     bool fp32_ok = false;
     if constexpr (C::MIXED) {
@@ -230,19 +230,22 @@ __device__ int warp_clip(SparsePoly<C>& P, SparseState& S, double px, double py,
       // A vertex whose d32 lies within that bound of +-1e-9 is re-evaluated
       // with the FP64 formula, so every decision equals the plain path's.
       const double qx = px - gx, qy = py - gy, qz = pz - gz;
-      c = qx * nx + qy * ny + qz * nz;
+      const double c = qx * nx + qy * ny + qz * nz;
       const double qn = fabs(qx * nx) + fabs(qy * ny) + fabs(qz * nz);
       const double scale = S.umax * (fabs(nx) + fabs(ny) + fabs(nz)) + fabs(c);
-      bound = 0x1p-21 * (scale + qn) + 1e-30;
+      const double bound = 0x1p-21 * (scale + qn) + 1e-30;
       fp32_ok = scale > 1e-24 && scale < 1e24;
       fnx = (float)nx;
       fny = (float)ny;
       fnz = (float)nz;
       fc = (float)c;
-      hi_out = kTol + bound;
-      lo_sin = -kTol - bound;
-      band_lo = -kTol + bound;
-      band_hi = kTol - bound;
+      // the thresholds rounded outward (out/inside) and the exact-free band
+      // rounded inward, so comparing the FP32 value with them decides no
+      // vertex that the FP64 comparison would decide differently
+      hi_out = __double2float_ru(kTol + bound);
+      lo_sin = __double2float_rd(-kTol - bound);
+      band_lo = __double2float_ru(-kTol + bound);
+      band_hi = __double2float_rd(kTol - bound);
     }
 #pragma unroll
     for (int w = 0; w < 3; ++w) {
@@ -259,7 +262,7 @@ __device__ int warp_clip(SparsePoly<C>& P, SparseState& S, double px, double py,
           } else {
             bool exact = !fp32_ok;
             if (fp32_ok) {
-              const double d32 = (double)(fmaf(P.ux[v], fnx, fmaf(P.uy[v], fny, P.uz[v] * fnz)) - fc);
+              const float d32 = fmaf(P.ux[v], fnx, fmaf(P.uy[v], fny, P.uz[v] * fnz)) - fc;
               if (d32 > hi_out) o = true;
               else if (d32 < lo_sin) si = true;
               else exact = !(d32 >= band_lo && d32 <= band_hi);
@@ -359,7 +362,7 @@ __device__ int warp_clip(SparsePoly<C>& P, SparseState& S, double px, double py,
     const int tpos0 = tinc - tsz;
     const int np = __shfl_sync(kFull, tinc, 31);
     if (np > C::TCAP) return kClipOverflow;
-    for (int j = 0; j < tsz; ++j) P.tpf[tpos0 + j] = (uint8_t)lane;
+    if (touched) P.tmap[trank] = (uint8_t)lane;
     __syncwarp();
     uint8_t* D = P.ent[dst];
     const int dend = base + tot_new;
@@ -367,7 +370,14 @@ __device__ int warp_clip(SparsePoly<C>& P, SparseState& S, double px, double py,
     for (int r0 = 0; r0 < np; r0 += 32) {
       const int i = r0 + (int)lane;
       const bool act = i < np;
-      const int f = act ? P.tpf[i] : 0;
+      // the face of edge i: the touched faces that start at or before it (a
+      // start bit per face starting in this round, a count for the earlier
+      // ones)
+      const unsigned sb = __reduce_or_sync(
+          kFull, (touched && tpos0 >= r0 && tpos0 < r0 + 32) ? 1u << (tpos0 - r0) : 0u);
+      const int before = __popc(__ballot_sync(kFull, touched && tpos0 < r0));
+      const int rk = before + __popc(sb & (lane == 31 ? kFull : (2u << lane) - 1u)) - 1;
+      const int f = act ? P.tmap[rk] : 0;
       const int fst0 = __shfl_sync(kFull, st, f), frot = __shfl_sync(kFull, rot, f);
       const int fcn = __shfl_sync(kFull, c, f), ftp = __shfl_sync(kFull, tpos0, f);
       const int frank = __shfl_sync(kFull, trank, f);
@@ -487,10 +497,20 @@ __device__ int warp_clip(SparsePoly<C>& P, SparseState& S, double px, double py,
   }
   const int id = __shfl_sync(kFull, slot, leader);
   if (act) P.ent[dst][P.xpos[lane]] = (uint8_t)id;
-  const unsigned N0 = __reduce_or_sync(kFull, (isl && slot < 32) ? 1u << slot : 0u);
-  const unsigned N1 = __reduce_or_sync(kFull, (isl && slot >= 32 && slot < 64) ? 1u << (slot - 32) : 0u);
-  const unsigned N2 = __reduce_or_sync(kFull, (isl && slot >= 64) ? 1u << (slot - 64) : 0u);
-  const int nhw = max(hw, (int)__reduce_max_sync(kFull, isl ? (unsigned)(slot + 1) : 0u));
+  // the new vertices took the free slots up to the last one's: the lowest
+  // nnew free slots
+  unsigned N0, N1, N2;
+  int nhw;
+  {
+    const int sl = P.freel[nnew - 1];  // (nnew >= 3: a touched face has two crossings, three faces at least)
+    unsigned F2 = ~I2;
+    if constexpr (C::VCAP < 96) F2 &= (1u << (C::VCAP < 96 ? C::VCAP - 64 : 0)) - 1u;
+    auto upto = [](int b) { return b >= 31 ? kFull : (2u << b) - 1u; };  // bits 0..b of a word
+    N0 = ~I0 & (sl >= 32 ? kFull : upto(sl));
+    N1 = sl < 32 ? 0u : (~I1 & (sl >= 64 ? kFull : upto(sl - 32)));
+    N2 = sl < 64 ? 0u : (F2 & upto(sl - 64));
+    nhw = max(hw, sl + 1);
+  }
 
   // 5. the lid (:470-495): touched face k gives the segment (X of its
   //    out->in crossing, X of its in->out crossing), and lid_map[start] = end.
