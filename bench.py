@@ -465,7 +465,7 @@ def run_ours(args):
                        "l2": "flushed (512 MiB write) before every timed step",
                        "parallelism": f"{ws} independent tessellations, one per GPU"},
             "phases_ms": {"binning": statistics.mean(bin_ms), "clip_kernel": clip},
-            "roofline": {"bound": "fp64", "kernel": "k_clip_fast (warp-per-cell clip + reductions)",
+            "roofline": {"bound": "fp64", "kernel": "k_clip_sparse (warp-per-cell clip + reductions, slot layout)",
                          "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
                          "frac": achieved / peak.value,
                          "peak_source": "FP64 FMA-chain microbenchmark run live by bench.py on this GPU",
