@@ -772,20 +772,21 @@ __device__ int compute_cell(const TessDesc& T, uint32_t i, PolyT& P, typename Po
       const int bx = ix + o.dx, by = iy + o.dy, bz = iz + o.dz;
       inr = bx >= 0 && bx < G.n[0] && by >= 0 && by < G.n[1] && bz >= 0 && bz < G.n[2];
       if (inr) {
-        const double ddx = o.dx > 0 ? ((double)o.dx - rx) * G.cs[0]
-                                    : (o.dx < 0 ? ((double)(-(o.dx + 1)) + rx) * G.cs[0] : 0.0);
-        const double ddy = o.dy > 0 ? ((double)o.dy - ry) * G.cs[1]
-                                    : (o.dy < 0 ? ((double)(-(o.dy + 1)) + ry) * G.cs[1] : 0.0);
-        const double ddz = o.dz > 0 ? ((double)o.dz - rz) * G.cs[2]
-                                    : (o.dz < 0 ? ((double)(-(o.dz + 1)) + rz) * G.cs[2] : 0.0);
-        const double bdx = fmax(ddx, 0.0), bdy = fmax(ddy, 0.0), bdz = fmax(ddz, 0.0);
-        b2 = bdx * bdx + bdy * bdy + bdz * bdz;
         const uint32_t bb = (uint32_t)bx + (uint32_t)by * (uint32_t)G.n[0] + (uint32_t)bz * nxy;
         // on sparse grids an empty bin is known from its occupancy bit (an
-        // L2-resident map) without reading the bin table
+        // L2-resident map) without reading the bin table; an empty bin opens
+        // nothing, so its lower bound is needed only for occupied bins
         if (!T.occ || ((__ldg(&T.occ[bb >> 5]) >> (bb & 31u)) & 1u)) {
           bs = T.bin_start[bb];
           be = T.bin_start[bb + 1];
+          const double ddx = o.dx > 0 ? ((double)o.dx - rx) * G.cs[0]
+                                      : (o.dx < 0 ? ((double)(-(o.dx + 1)) + rx) * G.cs[0] : 0.0);
+          const double ddy = o.dy > 0 ? ((double)o.dy - ry) * G.cs[1]
+                                      : (o.dy < 0 ? ((double)(-(o.dy + 1)) + ry) * G.cs[1] : 0.0);
+          const double ddz = o.dz > 0 ? ((double)o.dz - rz) * G.cs[2]
+                                      : (o.dz < 0 ? ((double)(-(o.dz + 1)) + rz) * G.cs[2] : 0.0);
+          const double bdx = fmax(ddx, 0.0), bdy = fmax(ddy, 0.0), bdz = fmax(ddz, 0.0);
+          b2 = bdx * bdx + bdy * bdy + bdz * bdz;
         }
       }
     }
