@@ -183,7 +183,8 @@ __global__ void k_brelax(const double* __restrict__ gen, const int32_t* __restri
 // control words: work cursors of the three passes, the overflow counts they
 // hand on, the search-order list count, and the big-bin sort count
 enum : int {
-  kBCursor = 0, kBOvf, kBTab, kBBig, kBCursor2, kBMedOvf, kBCursor3, kBBigOvf, kBCursor4, kBHugeOvf, kBWords = 10
+  kBCursor = 0, kBOvf, kBTab, kBBig, kBCursor2, kBMedOvf, kBCursor3, kBBigOvf, kBCursor4, kBHugeOvf, kBCursorF,
+  kBFullOvf, kBWords = 12
 };
 // blocks of the batch's huge tier (one cell each at a time)
 constexpr int kBHugeBlocks = 8;
@@ -397,7 +398,7 @@ int clip_chain(vd_batch* b, const uint32_t* items, uint32_t nitems) {
   cudaStream_t s = b->stream;
   const int nt = (int)b->m.size();
   B_CK(b, cudaMemsetAsync(b->d_ctl.p, 0, 3 * sizeof(unsigned int), s));
-  B_CK(b, cudaMemsetAsync(b->d_ctl.p + kBCursor2, 0, 6 * sizeof(unsigned int), s));
+  B_CK(b, cudaMemsetAsync(b->d_ctl.p + kBCursor2, 0, 8 * sizeof(unsigned int), s));
   WorkList W;
   memset(&W, 0, sizeof(W));
   W.items = items;
@@ -419,11 +420,28 @@ int clip_chain(vd_batch* b, const uint32_t* items, uint32_t nitems) {
     B_CK(b, mixed ? launch_clip_mixed_fast_batched(b->d_descs.p, b->d_off.p, nt, W, nblocks, b->instrument, s)
                   : launch_clip_fp64_fast_batched(b->d_descs.p, b->d_off.p, nt, W, nblocks, b->instrument, s));
   }
+  // the slot layout's hand-offs: the full-rewrite first tier (48 faces)
+  const uint32_t* med_in = b->d_list0.p;
+  unsigned int* med_n = b->d_ctl.p + kBOvf;
+  if (b->fast_layout == VD_FAST_SLOTS) {
+    WorkList WF = W;
+    WF.items = b->d_list0.p;
+    WF.nitems = 0;
+    WF.nitems_dev = b->d_ctl.p + kBOvf;
+    WF.cursor = b->d_ctl.p + kBCursorF;
+    WF.ovf_list = b->d_list3.p;
+    WF.ovf_count = b->d_ctl.p + kBFullOvf;
+    const int nbf = std::max(1, b->num_sms * std::max(1, mixed ? b->blocksmx : b->blocks64));
+    B_CK(b, mixed ? launch_clip_mixed_fast_batched(b->d_descs.p, b->d_off.p, nt, WF, nbf, b->instrument, s)
+                  : launch_clip_fp64_fast_batched(b->d_descs.p, b->d_off.p, nt, WF, nbf, b->instrument, s));
+    med_in = b->d_list3.p;
+    med_n = b->d_ctl.p + kBFullOvf;
+  }
   // medium capacity (FP64; the same decisions as both precisions)
   WorkList W2 = W;
-  W2.items = b->d_list0.p;
+  W2.items = med_in;
   W2.nitems = 0;
-  W2.nitems_dev = b->d_ctl.p + kBOvf;
+  W2.nitems_dev = med_n;
   W2.cursor = b->d_ctl.p + kBCursor2;
   W2.ovf_list = b->d_list2.p;
   W2.ovf_count = b->d_ctl.p + kBMedOvf;
@@ -702,6 +720,7 @@ int vd_batch_commit(vd_batch* b) {
   B_CK(b, b->d_list0.ensure(n));
   B_CK(b, b->d_list1.ensure(n));
   B_CK(b, b->d_list2.ensure(n));
+  B_CK(b, b->d_list3.ensure(n));
   B_CK(b, b->d_sorted.ensure(n));
   B_CK(b, b->d_descs.ensure(nt));
   B_CK(b, b->d_vol.ensure(n));

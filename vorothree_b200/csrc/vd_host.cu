@@ -608,8 +608,9 @@ int ensure_huge(vd_tess* t, size_t cells) {
 }
 
 // one pass of the clip kernel over `items` (nullptr = all cells in bin order);
-// tier 0 = fast (shared memory), 1 = medium capacity, 2 = large capacity,
-// 3 = huge capacity
+// tier 0 = first tier (shared memory, the handle's layout), -1 = first tier on
+// the full-rewrite layout (the slot layout's hand-offs), 1 = medium capacity,
+// 2 = large capacity, 3 = huge capacity
 int clip_pass(vd_tess* t, int tier, const uint32_t* items, uint32_t nitems, uint32_t* ovf_list,
               uint32_t* tab_list, const WorkList* extra = nullptr) {
   cudaStream_t s = t->stream;
@@ -636,11 +637,11 @@ int clip_pass(vd_tess* t, int tier, const uint32_t* items, uint32_t nitems, uint
         1, std::min<size_t>((nitems + 1) / 2, (size_t)t->num_sms * std::max(1, t->infomed.blocks_per_sm)));
     VD_CK(t, launch_clip_med(T, W, nblocks, t->instrument, s));
     g_launches++;
-  } else if (tier == 0) {
+  } else if (tier <= 0) {
     const bool mixed = t->precision == VD_PREC_MIXED;
     // the slot layout cannot export a polytope in the reference's vertex
     // order: get_cell's rebuild runs the full-rewrite kernel
-    const bool slots = t->fast_layout == VD_FAST_SLOTS && !W.ex_verts;
+    const bool slots = tier == 0 && t->fast_layout == VD_FAST_SLOTS && !W.ex_verts;
     const int mv = t->fast_minb - 5;
     const ClipLaunchInfo& li =
         slots ? (mixed ? t->infospmx[mv] : t->infosp64[mv]) : (mixed ? t->infomx : t->info64);
@@ -801,9 +802,12 @@ int run_calculate(vd_tess* t, const WorkList* extra = nullptr, const uint32_t* o
       continue;
     }
     if (novf > 0) {
-      // medium capacity first, then the large and huge capacities for what remains
+      // the slot layout's hand-offs to the full-rewrite first tier (48 faces,
+      // every cell's layout equal in results), then medium capacity, then the
+      // large and huge capacities for what remains
       unsigned int ntab_all = 0;
-      for (int tier = 1; tier <= 3 && novf > 0; ++tier) {
+      const bool slots = t->fast_layout == VD_FAST_SLOTS && !(extra && extra->ex_verts);
+      for (int tier = slots ? -1 : 1; tier <= 3 && novf > 0;) {
         std::swap(t->d_list[0], t->d_list[2]);
         r = clip_pass(t, tier, t->d_list[2].p, novf, t->d_list[0].p, t->d_list[1].p + ntab_all, extra);
         if (r != VD_OK) return r;
@@ -816,7 +820,9 @@ int run_calculate(vd_tess* t, const WorkList* extra = nullptr, const uint32_t* o
         // few cells left after the medium tier: straight to the block tier,
         // which takes them all at once, so that a cell outgrowing the large
         // tier is not built twice
-        if (tier == 1 && novf > 0 && novf <= (unsigned)t->huge_direct_max) tier = 2;
+        int next = tier == -1 ? 1 : tier + 1;
+        if (tier == 1 && novf > 0 && novf <= (unsigned)t->huge_direct_max) next = 3;
+        tier = next;
       }
       novf = 0;
       ntab = ntab_all;
