@@ -694,12 +694,19 @@ def run_suite(args):
     nthreads = os.cpu_count() or 1
     box = ([0.0, 0.0, 0.0], [100.0, 100.0, 100.0])
 
+    from vorothree_b200 import autotune
+
     def case(group, label, n, g, pts=None, seed=0):
         t = v.Tessellation(v.BoundingBox(*box), v.Algorithm3DGrid(g, g, g))
         if pts is None:
             t.random_generators(n, seed)
         else:
             t.set_generators(pts)
+        # the library's tuned launch settings for this input's class and size
+        # (the grid stays the bench's own heuristic)
+        cls = autotune.distribution_class(t.generators(), v.BoundingBox(*box))
+        tun = autotune.lookup_tuning(cls, n)
+        t.set_tuning(tun)
         t.calculate()
         one = t.timings()["total_ms"]
         reps = max(1, min(args.steps, int(2000.0 / max(one, 1e-3))))
@@ -711,7 +718,8 @@ def run_suite(args):
             tm = t.timings()
             dev.append(tm["clip_ms"] + tm["fallback_ms"])
         row = {"group": group, "case": label, "n": n, "grid": g, "gpu_ms": statistics.mean(wall),
-               "gpu_device_ms": statistics.mean(dev), "fallback_cells": t.fallback_counts()}
+               "gpu_device_ms": statistics.mean(dev), "fallback_cells": t.fallback_counts(),
+               "class": cls, "tuning": tun}
         if n <= 100_000:
             gens = t.generators()
             o = OracleTessellation(*box, g, g, g)

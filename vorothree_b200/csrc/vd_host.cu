@@ -44,6 +44,9 @@ constexpr int kHugeBlocksMax = 64;
 // face capacities of the tiers whose cells can have more faces than the
 // per-cell slots hold (medium, large, huge): their faces go to the pool
 constexpr long long kMedFaces = 112, kBigFaces = 512, kHugeFaces = 32767;
+// cells the slot layout hands off, from which they go through the
+// full-rewrite first tier before the medium tier
+constexpr int kFullHandoffMin = 256;
 // kernels this library has launched in this process (all handles)
 std::atomic<unsigned long long> g_launches{0};
 
@@ -806,7 +809,10 @@ int run_calculate(vd_tess* t, const WorkList* extra = nullptr, const uint32_t* o
       // every cell's layout equal in results), then medium capacity, then the
       // large and huge capacities for what remains
       unsigned int ntab_all = 0;
-      const bool slots = t->fast_layout == VD_FAST_SLOTS && !(extra && extra->ex_verts);
+      // (for a few cells the extra pass's launch and read-back cost more than
+      // the medium tier's slower per-cell build)
+      const bool slots = t->fast_layout == VD_FAST_SLOTS && !(extra && extra->ex_verts) &&
+                         novf >= (unsigned)kFullHandoffMin;
       for (int tier = slots ? -1 : 1; tier <= 3 && novf > 0;) {
         std::swap(t->d_list[0], t->d_list[2]);
         r = clip_pass(t, tier, t->d_list[2].p, novf, t->d_list[0].p, t->d_list[1].p + ntab_all, extra);
