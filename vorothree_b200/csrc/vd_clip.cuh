@@ -149,6 +149,17 @@ __device__ __forceinline__ double warp_max(double x) {
   return x;
 }
 
+// The largest of the lanes' values, each a non-negative double or NaN (NaN
+// counts as 0, as fmax and the reference's `d2 > max` comparison treat it).
+// Non-negative doubles order like their bit patterns as unsigned integers, so
+// two 32-bit reductions give exactly fmax's result.
+__device__ __forceinline__ double sp_warp_max_nonneg(double x) {
+  const unsigned long long b = (x >= 0.0) ? (unsigned long long)__double_as_longlong(x) : 0ull;
+  const unsigned hi = __reduce_max_sync(kFull, (unsigned)(b >> 32));
+  const unsigned lo = __reduce_max_sync(kFull, (unsigned)(b >> 32) == hi ? (unsigned)b : 0u);
+  return __longlong_as_double((long long)(((unsigned long long)hi << 32) | lo));
+}
+
 __device__ __forceinline__ double clamp01(double t) {
   // f64::clamp(0.0, 1.0); NaN passes through
   if (t < 0.0) return 0.0;

@@ -547,23 +547,18 @@ __device__ int block_clip(WarpPoly<C>& P, BlockShared<NW>& B, PolyState& S, doub
   return kClipMod;
 }
 
-// compute_cell (tessellation.rs:414-475) by a whole block: the walk runs in
-// every warp (same data, same decisions, a staging row per warp), each clip
-// by all warps together
-template <class C, int NW>
-__device__ int compute_cell_block(const TessDesc& T, uint32_t i, WarpPoly<C>& P, BlockShared<NW>& B,
-                                   PolyState& S) {
+// compute_cell (tessellation.rs:414-475) over a block-wide polytope X: the
+// walls' planes, then the candidates in search order.  The walk runs in every
+// warp (same data, same decisions, a staging row per warp) and all warps enter
+// each clip together.  X provides init (the box), clip (clip_with_scratch's
+// result and the new largest radius), empty and max_radius; the layouts that
+// use it give the same results, bit for bit.
+template <int NW, class X>
+__device__ int block_walk(const TessDesc& T, uint32_t i, BlockShared<NW>& B, X& poly) {
   const unsigned lane = lane_id();
   const double gx = T.gen[3 * (size_t)i], gy = T.gen[3 * (size_t)i + 1], gz = T.gen[3 * (size_t)i + 2];
   double r2;
-  // the box, written by warp 0; every thread holds the same state
-  if ((threadIdx.x >> 5) == 0) poly_init_box(P, S, T.grid, gx, gy, gz);
-  S.nv = 8;
-  S.nf = 6;
-  S.nh = 24;
-  S.cb = 0;
-  S.umax = 0.0;
-  __syncthreads();
+  poly.init(T.grid, gx, gy, gz);
   for (int w = 0; w < T.nwalls; ++w) {
     const Wall& W = T.walls[w];
     // one plane per generator, or a polyhedron's fixed planes in order
@@ -584,13 +579,13 @@ __device__ int compute_cell_block(const TessDesc& T, uint32_t i, WarpPoly<C>& P,
         emit = wall_plane(W, gx, gy, gz, p, n);
       }
       if (emit) {
-        const int r = block_clip<C, NW>(P, B, S, p[0], p[1], p[2], n[0], n[1], n[2], W.id, false, gx, gy, gz, &r2);
+        const int r = poly.clip(p[0], p[1], p[2], n[0], n[1], n[2], W.id, false, gx, gy, gz, &r2);
         if (r == kClipOverflow) return kCellOverflow;
       }
     }
-    if (S.nv == 0) return kCellOk;
+    if (poly.empty()) return kCellOk;
   }
-  double cur = poly_max_radius_sq(P, S, gx, gy, gz);
+  double cur = poly.max_radius(gx, gy, gz);
 
   const Grid& G = T.grid;
   const uint32_t bin = T.bin_of[i];
@@ -609,12 +604,11 @@ __device__ int compute_cell_block(const TessDesc& T, uint32_t i, WarpPoly<C>& P,
     const int k = base + (int)lane;
     const bool valid = k < T.norder;
     double md2 = 0.0, b2 = 0.0;
-    bool inr = false, own = false;
+    bool inr = false;
     uint32_t bs = 0, be = 0;
     if (valid) {
       const Offset o = T.order[k];
       md2 = o.min_d2;
-      own = o.dx == 0 && o.dy == 0 && o.dz == 0;
       const int bx = ix + o.dx, by = iy + o.dy, bz = iz + o.dz;
       inr = bx >= 0 && bx < G.n[0] && by >= 0 && by < G.n[1] && bz >= 0 && bz < G.n[2];
       if (inr) {
@@ -635,7 +629,6 @@ __device__ int compute_cell_block(const TessDesc& T, uint32_t i, WarpPoly<C>& P,
         }
       }
     }
-    const int nvalid = min(32, T.norder - base);
     // bins that can still open (R only shrinks), flattened: members of entry
     // e are candidates [start, start + cnt)
     const bool pot = valid && inr && be > bs && !(md2 > 4.0 * cur) && b2 <= 4.0 * cur;
@@ -644,7 +637,6 @@ __device__ int compute_cell_block(const TessDesc& T, uint32_t i, WarpPoly<C>& P,
       // the end of the walk is decided here
       const unsigned brk = __ballot_sync(kFull, valid && md2 > 4.0 * cur);
       const int fbe = brk ? __ffs(brk) - 1 : 32;
-      if constexpr (C::COUNT) cnt_add(P, kCntOffsets, (unsigned long long)(fbe < 32 ? fbe + 1 : nvalid));
       if (fbe < 32) done = true;
       continue;
     }
@@ -683,13 +675,12 @@ __device__ int compute_cell_block(const TessDesc& T, uint32_t i, WarpPoly<C>& P,
         if (!pass) break;
         const int j = __ffs(pass) - 1;
         const int ej = __shfl_sync(kFull, ce, j);
-        if constexpr (C::COUNT) count_opened(P, ecur, ej, valid, inr, own, md2, b2, be - bs, c4);
         const int jid = (int)__shfl_sync(kFull, sg.id, j);
         const double e0 = __shfl_sync(kFull, d0, j);
         const double e1 = __shfl_sync(kFull, d1, j);
         const double e2 = __shfl_sync(kFull, d2, j);
         const double mx = gx + e0 * 0.5, my = gy + e1 * 0.5, mz = gz + e2 * 0.5;
-        const int r = block_clip<C, NW>(P, B, S, mx, my, mz, e0, e1, e2, jid, true, gx, gy, gz, &r2);
+        const int r = poly.clip(mx, my, mz, e0, e1, e2, jid, true, gx, gy, gz, &r2);
         if (r == kClipOverflow) return kCellOverflow;
         if (r == kClipMod) cur = r2;
         else if (r == kClipEmpty) cur = 0.0;
@@ -701,14 +692,43 @@ __device__ int compute_cell_block(const TessDesc& T, uint32_t i, WarpPoly<C>& P,
       const unsigned nxt = __ballot_sync(kFull, cnt > 0 && start <= r0 + 32);
       if (fb < 32 && 31 - __clz(nxt) >= fb) break;
     }
-    if constexpr (C::COUNT) {
-      count_opened(P, ecur, fb < 32 ? fb - 1 : 31, valid, inr, own, md2, b2, be - bs, 4.0 * cur);
-      cnt_add(P, kCntOffsets, (unsigned long long)(fb < 32 ? fb + 1 : nvalid));
-    }
     if (fb < 32) done = true;
   }
   if (!done && !T.order_complete && !(T.order_bound > 4.0 * cur)) return kCellTable;
   return kCellOk;
+}
+
+
+// the full-rewrite layout's operations for block_walk
+template <class C, int NW>
+struct BlockPolyOps {
+  WarpPoly<C>& P;
+  BlockShared<NW>& B;
+  PolyState& S;
+  __device__ void init(const Grid& g, double gx, double gy, double gz) {
+    // the box, written by warp 0; every thread holds the same state
+    if ((threadIdx.x >> 5) == 0) poly_init_box(P, S, g, gx, gy, gz);
+    S.nv = 8;
+    S.nf = 6;
+    S.nh = 24;
+    S.cb = 0;
+    S.umax = 0.0;
+    __syncthreads();
+  }
+  __device__ int clip(double px, double py, double pz, double nx, double ny, double nz, int nbr, bool with_gen,
+                      double gx, double gy, double gz, double* r2out) {
+    return block_clip<C, NW>(P, B, S, px, py, pz, nx, ny, nz, nbr, with_gen, gx, gy, gz, r2out);
+  }
+  __device__ bool empty() const { return S.nv == 0; }
+  __device__ double max_radius(double gx, double gy, double gz) { return poly_max_radius_sq(P, S, gx, gy, gz); }
+};
+
+// compute_cell by a whole block on the full-rewrite layout
+template <class C, int NW>
+__device__ int compute_cell_block(const TessDesc& T, uint32_t i, WarpPoly<C>& P, BlockShared<NW>& B,
+                                   PolyState& S) {
+  BlockPolyOps<C, NW> ops{P, B, S};
+  return block_walk<NW>(T, i, B, ops);
 }
 
 constexpr int kHugeBlockWarps = 32;
@@ -719,78 +739,5 @@ constexpr int kHugeBlockWarps = 32;
 // centre of 1,000 generators on a sphere: 14.2 ms with 16 warps, 18.1 ms with
 // 32; at 3,000 generators 32 warps win)
 constexpr int kHugeBlockWarpsNarrow = 16;
-
-// persistent blocks over the listed cells, one cell per block at a time; the
-// block's polytope lives in global memory
-template <class C, int NW>
-__global__ void __launch_bounds__(NW * 32)
-    k_clip_huge_block(const TessDesc T, const WorkList W, WarpPoly<C>* polys) {
-  __shared__ BlockShared<NW> B;
-  WarpPoly<C>& P = polys[blockIdx.x];
-  const unsigned lane = lane_id();
-  const int w = (int)(threadIdx.x >> 5);
-  while (true) {
-    if (threadIdx.x == 0) B.idx = atomicAdd(W.cursor, 1u);
-    __syncthreads();
-    const unsigned idx = B.idx;
-    __syncthreads();
-    if (idx >= W.nitems) break;
-    const uint32_t cell = W.items ? W.items[idx] : (uint32_t)T.sorted[idx].id;
-    PolyState S;
-    const int st = compute_cell_block<C, NW>(T, cell, P, B, S);
-    __syncthreads();
-    if (w == 0) {
-      if (st == kCellOk) {
-        finalize_cell<C>(T, cell, P, S);
-        if (W.ex_verts) export_cell<C>(W, P, S);
-      } else if (lane == 0) {
-        T.status[cell] = (uint8_t)st;
-        if (st == kCellOverflow && W.ovf_list) W.ovf_list[atomicAdd(W.ovf_count, 1u)] = cell;
-        if (st == kCellTable && W.tab_list) W.tab_list[atomicAdd(W.tab_count, 1u)] = cell;
-      }
-    }
-    __syncthreads();
-  }
-}
-
-// the same over a batch's work list: items are global positions in the
-// concatenated bin-ordered generators (clip_worker_batched)
-template <class C, int NW>
-__global__ void __launch_bounds__(NW * 32)
-    k_clip_huge_block_batched(const TessDesc* descs, const uint32_t* tess_off, int ntess, const WorkList W,
-                              WarpPoly<C>* polys) {
-  __shared__ BlockShared<NW> B;
-  WarpPoly<C>& P = polys[blockIdx.x];
-  const unsigned lane = lane_id();
-  const int w = (int)(threadIdx.x >> 5);
-  const uint32_t nitems = W.nitems_dev ? *W.nitems_dev : W.nitems;
-  while (true) {
-    if (threadIdx.x == 0) B.idx = atomicAdd(W.cursor, 1u);
-    __syncthreads();
-    const unsigned idx = B.idx;
-    __syncthreads();
-    if (idx >= nitems) break;
-    const uint32_t item = W.items ? W.items[idx] : idx;
-    const int t = find_tess(tess_off, ntess, item);
-    const TessDesc& T = descs[t];
-    const uint32_t cell = (uint32_t)T.sorted[item].id;
-    PolyState S;
-    const int st = compute_cell_block<C, NW>(T, cell, P, B, S);
-    __syncthreads();
-    if (w == 0) {
-      if (st == kCellOk) {
-        finalize_cell<C>(T, cell, P, S);
-      } else if (lane == 0) {
-        T.status[cell] = (uint8_t)st;
-        if (st == kCellOverflow && W.ovf_list) W.ovf_list[atomicAdd(W.ovf_count, 1u)] = item;
-        if (st == kCellTable) {
-          if (W.tab_list) W.tab_list[atomicAdd(W.tab_count, 1u)] = item;
-          if (W.tess_flags) atomicOr(&W.tess_flags[t], 1u);
-        }
-      }
-    }
-    __syncthreads();
-  }
-}
 
 }  // namespace vd

@@ -114,17 +114,6 @@ __device__ __forceinline__ bool sp_bit(unsigned a, unsigned b, unsigned c, unsig
   return (sp_word(a, b, c, s) >> (s & 31u)) & 1u;
 }
 
-// The largest of the lanes' values, each a non-negative double or NaN (NaN
-// counts as 0, as fmax and the reference's `d2 > max` comparison treat it).
-// Non-negative doubles order like their bit patterns as unsigned integers, so
-// two 32-bit reductions give exactly fmax's result.
-__device__ __forceinline__ double sp_warp_max_nonneg(double x) {
-  const unsigned long long b = (x >= 0.0) ? (unsigned long long)__double_as_longlong(x) : 0ull;
-  const unsigned hi = __reduce_max_sync(kFull, (unsigned)(b >> 32));
-  const unsigned lo = __reduce_max_sync(kFull, (unsigned)(b >> 32) == hi ? (unsigned)b : 0u);
-  return __longlong_as_double((long long)(((unsigned long long)hi << 32) | lo));
-}
-
 // Cell3DFaces::new (cell_3d_faces.rs:37-74): the box, faces z-, z+, y-, y+,
 // x-, x+ with ids box_side (bounds/mod.rs:21-22)
 template <class C>

@@ -4,7 +4,7 @@
 // add, so neither may this path, or its vertices would differ in the last bit
 // and the tie-breaking 1e-9 bands could classify differently.
 #include "vd_clip.cuh"
-#include "vd_clip_block.cuh"
+#include "vd_clip_hub.cuh"
 #include "vd_internal.h"
 
 namespace vd {
@@ -58,21 +58,38 @@ cudaError_t launch_clip_fp64_big(const TessDesc& T, const WorkList& W, void* scr
 // the huge tier's scratch: a polytope per block
 size_t clip_huge_scratch_per_block() { return sizeof(WarpPoly<HugeCfg>); }
 
+// the huge kernels' dynamic shared memory (the slot layout's per-clip state,
+// above the 48 KB a kernel gets without asking)
+template <class K>
+static cudaError_t huge_smem(K kernel, size_t bytes) {
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
 cudaError_t launch_clip_fp64_huge(const TessDesc& T, const WorkList& W, void* scratch, int nblocks, bool narrow,
                                   cudaStream_t s) {
   WarpPoly<HugeCfg>* polys = reinterpret_cast<WarpPoly<HugeCfg>*>(scratch);
-  if (narrow)
-    k_clip_huge_block<HugeCfg, kHugeBlockWarpsNarrow><<<nblocks, kHugeBlockWarpsNarrow * 32, 0, s>>>(T, W, polys);
-  else
-    k_clip_huge_block<HugeCfg, kHugeBlockWarps><<<nblocks, kHugeBlockWarps * 32, 0, s>>>(T, W, polys);
+  if (narrow) {
+    constexpr size_t sm = sizeof(HubShared<kHugeBlockWarpsNarrow>);
+    cudaError_t e = huge_smem(k_clip_huge_block<HugeCfg, kHugeBlockWarpsNarrow>, sm);
+    if (e != cudaSuccess) return e;
+    k_clip_huge_block<HugeCfg, kHugeBlockWarpsNarrow><<<nblocks, kHugeBlockWarpsNarrow * 32, sm, s>>>(T, W, polys);
+  } else {
+    constexpr size_t sm = sizeof(HubShared<kHugeBlockWarps>);
+    cudaError_t e = huge_smem(k_clip_huge_block<HugeCfg, kHugeBlockWarps>, sm);
+    if (e != cudaSuccess) return e;
+    k_clip_huge_block<HugeCfg, kHugeBlockWarps><<<nblocks, kHugeBlockWarps * 32, sm, s>>>(T, W, polys);
+  }
   return cudaGetLastError();
 }
 
 cudaError_t launch_clip_fp64_huge_batched(const TessDesc* descs, const uint32_t* tess_off, int ntess,
                                           const WorkList& W, void* scratch, int nblocks, cudaStream_t s) {
   WarpPoly<HugeCfg>* polys = reinterpret_cast<WarpPoly<HugeCfg>*>(scratch);
+  constexpr size_t sm = sizeof(HubShared<kHugeBlockWarps>);
+  cudaError_t e = huge_smem(k_clip_huge_block_batched<HugeCfg, kHugeBlockWarps>, sm);
+  if (e != cudaSuccess) return e;
   k_clip_huge_block_batched<HugeCfg, kHugeBlockWarps>
-      <<<nblocks, kHugeBlockWarps * 32, 0, s>>>(descs, tess_off, ntess, W, polys);
+      <<<nblocks, kHugeBlockWarps * 32, sm, s>>>(descs, tess_off, ntess, W, polys);
   return cudaGetLastError();
 }
 
