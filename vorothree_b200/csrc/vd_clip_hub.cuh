@@ -52,7 +52,8 @@ struct HubCfg {
 };
 
 struct alignas(16) HubPoly {
-  double vx[HubCfg::VCAP], vy[HubCfg::VCAP], vz[HubCfg::VCAP];
+  // (whole words of slots: the classification reads every slot of a word)
+  double vx[32 * HubCfg::VWORDS], vy[32 * HubCfg::VWORDS], vz[32 * HubCfg::VWORDS];
   uint32_t vf[3 * HubCfg::VCAP];  // the three faces of each vertex
   uint32_t freev[HubCfg::VCAP];   // free slots below the high-water mark (a stack)
   int32_t fn[HubCfg::FCAP];       // face neighbour id
@@ -260,33 +261,54 @@ struct HubOps {
     if (threadIdx.x == 0) H.pcnt[(b + 1) % 3] = 0;
 
     // 1. signed distances of the live vertices and the 3-band flags
-    //    (:302-326), a word of slots per warp at a time; the cut-away slots
-    //    listed; the kept vertices' largest radius
+    //    (:302-326), a word of slots per warp at a time, four words' loads
+    //    in flight (every slot below the high-water mark is read, a free one
+    //    ignored); the cut-away slots listed; the kept vertices' largest radius
     const int nwd = (H.hw + 31) >> 5;
     bool sin = false;
     double r2 = 0.0;
-    for (int k = w; k < nwd; k += NW) {
-      const int v = 32 * k + (int)lane;
-      bool o = false;
-      if ((H.live[k] >> lane) & 1u) {
-        const double x = P.vx[v], y = P.vy[v], z = P.vz[v];
-        const double d = (x - px) * nx + (y - py) * ny + (z - pz) * nz;
-        o = d > kTol;
-        sin |= d < -kTol;
-        if (!o && with_gen) {
-          const double dx = x - gx, dy = y - gy, dz = z - gz;
-          r2 = fmax(r2, dx * dx + dy * dy + dz * dz);
+    constexpr int U = 4;
+    for (int k0 = w; k0 < nwd; k0 += U * NW) {
+      double x[U], y[U], z[U];
+      unsigned lw[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int k = k0 + u * NW;
+        lw[u] = 0u;
+        x[u] = y[u] = z[u] = 0.0;
+        if (k < nwd) {
+          const int v = 32 * k + (int)lane;
+          lw[u] = H.live[k];
+          x[u] = P.vx[v];
+          y[u] = P.vy[v];
+          z[u] = P.vz[v];
         }
       }
-      const unsigned om = __ballot_sync(kFull, o);
-      if (lane == 0) H.u.c.out[k] = om;
-      if (om) {
-        int pos = 0;
-        if (lane == 0) pos = atomicAdd(&H.pcnt[b], __popc(om));
-        pos = __shfl_sync(kFull, pos, 0);
-        if (o) {
-          const int q = pos + __popc(om & lt);
-          if (q < Cf::OCAP) H.u.c.olist[q] = (uint32_t)v;
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int k = k0 + u * NW;
+        if (k >= nwd) break;
+        const int v = 32 * k + (int)lane;
+        bool o = false;
+        if ((lw[u] >> lane) & 1u) {
+          const double d = (x[u] - px) * nx + (y[u] - py) * ny + (z[u] - pz) * nz;
+          o = d > kTol;
+          sin |= d < -kTol;
+          if (!o && with_gen) {
+            const double dx = x[u] - gx, dy = y[u] - gy, dz = z[u] - gz;
+            r2 = fmax(r2, dx * dx + dy * dy + dz * dz);
+          }
+        }
+        const unsigned om = __ballot_sync(kFull, o);
+        if (lane == 0) H.u.c.out[k] = om;
+        if (om) {
+          int pos = 0;
+          if (lane == 0) pos = atomicAdd(&H.pcnt[b], __popc(om));
+          pos = __shfl_sync(kFull, pos, 0);
+          if (o) {
+            const int q = pos + __popc(om & lt);
+            if (q < Cf::OCAP) H.u.c.olist[q] = (uint32_t)v;
+          }
         }
       }
     }
@@ -496,6 +518,7 @@ struct HubOps {
     //    a cut-away endpoint that a later round still reads.
     int nnew = 0;
     double r2n = 0.0;
+    double kx = 0.0, ky = 0.0, kz = 0.0;  // the first round's vertices stay in registers
     for (int g0 = 0; g0 < ncr; g0 += 32) {
       const int g = g0 + (int)lane;
       const bool isx = g < ncr;
@@ -574,9 +597,15 @@ struct HubOps {
         const double de = (bx - px) * nx + (by - py) * ny + (bz - pz) * nz;
         const double t = clamp01(ds / (ds - de));
         const double ix = ax + t * (bx - ax), iy = ay + t * (by - ay), iz = az + t * (bz - az);
-        P.tx[r] = ix;
-        P.ty[r] = iy;
-        P.tz[r] = iz;
+        if (g0 == 0) {
+          kx = ix;
+          ky = iy;
+          kz = iz;
+        } else {
+          P.tx[r] = ix;
+          P.ty[r] = iy;
+          P.tz[r] = iz;
+        }
         const double dx = ix - gx, dy = iy - gy, dz = iz - gz;
         r2n = fmax(r2n, dx * dx + dy * dy + dz * dz);
         S.xid[g] = (uint16_t)min(slot, Cf::VCAP);
@@ -609,9 +638,9 @@ struct HubOps {
         const int slot = S.xid[g];
         const int r = S.xr[g];
         if (r != Cf::kNone) {
-          P.vx[slot] = P.tx[r];
-          P.vy[slot] = P.ty[r];
-          P.vz[slot] = P.tz[r];
+          P.vx[slot] = g0 == 0 ? kx : P.tx[r];
+          P.vy[slot] = g0 == 0 ? ky : P.ty[r];
+          P.vz[slot] = g0 == 0 ? kz : P.tz[r];
           P.vf[3 * slot] = S.cs[S.xf[g]];
           P.vf[3 * slot + 1] = S.cs[S.xf[S.xpart[g]]];
           P.vf[3 * slot + 2] = (uint32_t)nfs;
