@@ -518,6 +518,7 @@ def run_ours(args):
             line["clustered"] = blobs_leg(args, 4_194_304, args.precision, 3)
             line["batched"] = batched_leg(args, args.ntess, 3, args.lloyd_steps)
             line["serving_sweep"] = serving_leg(args, args.serve_requests, args.serve_rates)
+            line["serving_sweep"]["burst"] = burst_leg(args)
         print(json.dumps(line), flush=True)
     tess.close()
     if ws > 1:
@@ -586,9 +587,9 @@ def run_batched(args):
     return 0
 
 
-def serving_requests(count: int, seed: int = 0):
+def serving_requests(count: int, seed: int = 0, sizes=(1e3, 1e6)):
     from vorothree_b200.workloads import serving_requests as make
-    return make(count, seed)
+    return make(count, seed, sizes)
 
 
 def serve_at_rate(srv, reqs, rate: float, seed: int = 1):
@@ -641,10 +642,41 @@ def serving_leg(args, nreq: int, rates) -> dict:
             "sweep": sweep, "latency": "submit-to-result wall clock per request"}
 
 
+def burst_leg(args, nreq: int = 256) -> dict:
+    """A burst of small requests (sizes log-uniform in [1e3, 3.2e4], the
+    serving mix otherwise) submitted at once, served with the merging of small
+    requests into batches and without it: wall time from the first submit to
+    the last result, cells/s, p50/p99 latency and the batches formed."""
+    import vorothree_b200 as v
+    reqs = serving_requests(nreq, seed=5, sizes=(1e3, 3.2e4))
+    out = {"config": {"requests": nreq, "sizes": "log-uniform [1e3, 3.2e4]", "slots": args.serve_slots,
+                      "arrivals": "all at once"}}
+    for mode in ("merged", "alone"):
+        srv = v.TessellationServer(slots=args.serve_slots, hbm_budget_bytes=args.serve_budget_gb << 30,
+                                   precision=args.precision)
+        if mode == "merged":
+            srv.set_merging(max_members=64)
+        for _ in range(2):  # warm the slots' buffers (and batches)
+            srv.reset_stats()
+            t0 = time.perf_counter()
+            tickets = [srv.submit(*r) for r in reqs]
+            cells = sum(srv.wait(t)[0] for t in tickets)
+            for t in tickets:
+                srv.take(t)
+            wall = time.perf_counter() - t0
+        st = srv.stats()
+        ms = srv.merge_stats()
+        srv.close()
+        out[mode] = {"wall_ms": 1e3 * wall, "cells": cells, "cells_per_s": cells / wall,
+                     "p50_ms": 1e3 * st["p50_s"], "p99_ms": 1e3 * st["p99_s"], **ms}
+    return out
+
+
 def run_serving(args):
     import torch
     torch.cuda.set_device(0)
     res = serving_leg(args, args.serve_requests, args.serve_rates)
+    res["burst"] = burst_leg(args)
     line = {"metric": "serve p50/p99 latency", "workload": "serving", "unit": "ms", "n_gpus": 1,
             "higher_is_better": False, "value": res["sweep"][0]["p99_ms"], "precision": args.precision,
             "data": "synthetic (seeded PCG64)"}

@@ -149,7 +149,7 @@ typedef struct {
                               the block-per-cell tier instead of through the large tier */
   int huge_blocks_max;     /* most concurrent blocks of the block-per-cell tier (default 64, at most 256) */
   int huge_narrow_max;     /* tessellations of at most this many cells run that tier with 16-warp blocks,
-                              larger ones with 32 (default 2000) */
+                              larger ones with 32 (default 2^30: always 16) */
 } vd_tuning;
 int vd_tess_set_tuning(vd_tess* t, const vd_tuning* k);
 /* the settings in force (defaults filled in) */
@@ -363,6 +363,9 @@ int vd_batch_set_precision(vd_batch* b, int precision);
 /* VD_FAST_SLOTS (default) or VD_FAST_FULL, as vd_tess_set_fast_layout */
 int vd_batch_set_fast_layout(vd_batch* b, int layout);
 int vd_batch_set_instrumentation(vd_batch* b, int on);
+/* drop the members so that the batch takes new ones (vd_batch_add again);
+ * device buffers are kept and only grow */
+int vd_batch_reset(vd_batch* b);
 /* upload every member and bin it (after the last vd_batch_add) */
 int vd_batch_commit(vd_batch* b);
 /* Tessellation::calculate for every member, one persistent launch */
@@ -424,6 +427,16 @@ int vd_server_take_faces(vd_server* s, uint64_t ticket, double* volume, double* 
 /* a request still in the queue is dropped (its wait/take return VD_ECANCELED);
  * one that has started runs to completion and this returns VD_ESTATE */
 int vd_server_cancel(vd_server* s, uint64_t ticket);
+/* merging of small requests (off by default; limits 65,536 generators a
+ * request and 2^20 a group unless given): a slot that starts a request without face results
+ * of at most max_request generators also takes the run of such requests
+ * behind it in the queue (up to max_members, max_group generators in all,
+ * within the HBM budget) and computes them as one batch (vd_batch); each
+ * result equals the request's standalone result.  max_members <= 1 turns it
+ * off; a zero size keeps the current one. */
+int vd_server_set_merging(vd_server* s, int max_members, size_t max_request, size_t max_group);
+/* merged batches run and the requests they served, since the last reset_stats */
+int vd_server_merge_stats(vd_server* s, uint64_t* groups, uint64_t* merged_requests);
 
 /* ---- fault injection for tests (no counterpart in the reference) ----
  * the next `count` device allocations this library makes (in any thread)

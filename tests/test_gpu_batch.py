@@ -178,3 +178,26 @@ def test_batch_huge_cells():
             t.calculate()
     for k, t in enumerate(ts):
         assert_member_equal(b, k, t)
+
+
+def test_batch_reset_takes_new_members():
+    """A batch reset after a calculate (and a Lloyd step) takes a new set of
+    members, larger than the first, and computes them as a fresh batch does:
+    each equals its standalone tessellation bit for bit."""
+    import vorothree_b200 as v
+    first, second = members(5)[:6], members(9)
+    b = build_batch(first)
+    b.calculate()
+    b.lloyd(1)
+    b.reset()
+    for bmin, bmax, grid, pts, walls in second:
+        b.add(v.BoundingBox(bmin, bmax), grid, pts, walls)
+    b.commit()
+    b.calculate()
+    for k, m in enumerate(second):
+        t = standalone(m)
+        gv, gc, gn = b.summaries(k)
+        sv, sc, sn = t.summaries()
+        assert np.array_equal(gn, sn) and np.array_equal(gv, sv) and np.array_equal(gc, sc), k
+        t.close()
+    b.close()

@@ -192,3 +192,43 @@ def test_allocation_failure_inside_a_request():
         av, ac, an = alone(r)
         assert np.array_equal(vol, av) and np.array_equal(nf, an) and np.array_equal(cen, ac)
     srv.close()
+
+
+def test_small_requests_merge_into_batches_and_equal_alone():
+    """Small requests waiting together are computed as one batch (one binning
+    pass, one persistent clip launch over all their cells): with one slot and
+    a burst of submissions the queue holds runs of them.  Each result equals
+    the request computed alone, bit for bit; a request asking for face
+    results in the middle of the burst runs alone and its CSR is complete;
+    with merging off no batch is formed."""
+    import vorothree_b200 as v
+    reqs = requests(7) + requests(8)
+    for merge in (True, False):
+        srv = v.TessellationServer(slots=1, hbm_budget_bytes=8 << 30)
+        if merge:
+            srv.set_merging(max_members=64)
+        tickets = [srv.submit(*r) for r in reqs]
+        srv.set_face_results(True)
+        b, grid, pts, walls = reqs[5]
+        tf = srv.submit(b, grid, pts, walls)
+        srv.set_face_results(False)
+        tickets += [srv.submit(*r) for r in reqs[:6]]
+        got = [srv.take(t) for t in tickets]
+        vol, cen, nf, off, ids, ar = srv.take_faces(tf)
+        ms = srv.merge_stats()
+        if merge:
+            assert ms["groups"] >= 1 and ms["merged_requests"] >= 2
+        else:
+            assert ms == {"groups": 0, "merged_requests": 0}
+        for r, (gv, gc, gn) in zip(reqs + reqs[:6], got):
+            av, ac, an = alone(r)
+            assert np.array_equal(gn, an) and np.array_equal(gv, av) and np.array_equal(gc, ac)
+        t = v.Tessellation(b, v.Algorithm3DGrid(*grid))
+        for w in walls:
+            t.add_wall(w)
+        t.set_generators(pts)
+        t.calculate()
+        so, si = t.neighbors()
+        assert np.array_equal(off, so) and np.array_equal(ids, si) and np.array_equal(nf, t.summaries()[2])
+        assert srv.stats()["completed"] == len(tickets) + 1
+        srv.close()

@@ -109,6 +109,7 @@ SIGNATURES = {
     "vd_batch_set_precision": (C.c_int, [_vp, C.c_int]),
     "vd_batch_set_fast_layout": (C.c_int, [_vp, C.c_int]),
     "vd_batch_set_instrumentation": (C.c_int, [_vp, C.c_int]),
+    "vd_batch_reset": (C.c_int, [_vp]),
     "vd_batch_commit": (C.c_int, [_vp]),
     "vd_batch_calculate": (C.c_int, [_vp]),
     "vd_batch_lloyd": (C.c_int, [_vp, C.c_int]),
@@ -136,6 +137,8 @@ SIGNATURES = {
     "vd_server_total_faces": (C.c_int, [_vp, C.c_uint64, C.POINTER(C.c_int64)]),
     "vd_server_take_faces": (C.c_int, [_vp, C.c_uint64, _vp, _vp, _vp, _vp, _vp, _vp]),
     "vd_server_cancel": (C.c_int, [_vp, C.c_uint64]),
+    "vd_server_set_merging": (C.c_int, [_vp, C.c_int, C.c_size_t, C.c_size_t]),
+    "vd_server_merge_stats": (C.c_int, [_vp, _u64p, _u64p]),
     "vd_debug_fail_allocations": (C.c_int, [C.c_int]),
     "vd_cell_last_error": (C.c_char_p, [_vp]),
     "vd_cell_create_box": (C.c_int, [C.c_size_t, _d, _d, C.POINTER(_vp)]),

@@ -51,8 +51,8 @@ DEFAULT_TUNING = {"fast_layout": "slots", "fast_blocks_per_sm": 6}
 # the block-per-cell tier's hand-off, searched once (HANDOFF_KEY)
 HANDOFF_KEY = "handoff"
 DIRECT_MAX = (1, 16, 64, 256)
-NARROW_MAX = (500, 2000, 5000)
-DEFAULT_HANDOFF = {"huge_direct_max": 64, "huge_blocks_max": 64, "huge_narrow_max": 2000}
+NARROW_MAX = (500, 2000, 5000, 1 << 30)
+DEFAULT_HANDOFF = {"huge_direct_max": 64, "huge_blocks_max": 64, "huge_narrow_max": 1 << 30}
 
 
 def grid_for(n: int, bounds, factor: float) -> Tuple[int, int, int]:
@@ -254,7 +254,10 @@ def main(argv=None):
     """Tune the default table on this GPU over seeded synthetic inputs of
     both classes, sizes 2^10 .. 2^22, and write it next to this file.
 
-        python -m vorothree_b200.autotune [--out PATH] [--max-log2 22]
+        python -m vorothree_b200.autotune [--out PATH] [--max-log2 22] [--handoff-only]
+
+    --handoff-only keeps the table's first-tier entries and searches the
+    block-per-cell tier's thresholds again.
     """
     import argparse
     import torch
@@ -262,11 +265,12 @@ def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=TABLE_PATH)
     ap.add_argument("--max-log2", type=int, default=22)
+    ap.add_argument("--handoff-only", action="store_true")
     a = ap.parse_args(argv)
     from .workloads import bench_distribution
     b = BoundingBox([0, 0, 0], [1, 1, 1])
-    entries: Dict[str, dict] = {}
-    for cls in ("uniform", "clustered"):
+    entries: Dict[str, dict] = dict(load_table()) if a.handoff_only else {}
+    for cls in () if a.handoff_only else ("uniform", "clustered"):
         for e in range(10, a.max_log2 + 1, 2):
             pts = synthetic(cls, 1 << e, seed=e)
             if distribution_class(pts, b) != cls:
@@ -278,7 +282,7 @@ def main(argv=None):
     # adjacent to every other generator
     box = BoundingBox([0, 0, 0], [100, 100, 100])
     cases = []
-    for n in (1000, 3000):
+    for n in (1000, 3000, 10000):
         g = int(np.ceil(n ** (1.0 / 3.0)))
         cases.append((bench_distribution("sphere", n, 11), box, (g, g, g)))
     entries = tune_handoff(cases, entries=entries)

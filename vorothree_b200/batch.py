@@ -121,6 +121,12 @@ class TessellationBatch:
     def set_instrumentation(self, on: bool):
         self._chk(self._L.vd_batch_set_instrumentation(self._h, 1 if on else 0))
 
+    def reset(self):
+        """Drop the members so that the batch takes new ones (add, commit and
+        calculate again); its device buffers are kept."""
+        self._chk(self._L.vd_batch_reset(self._h))
+        self._n = 0
+
     def commit(self):
         self._chk(self._L.vd_batch_commit(self._h))
 

@@ -573,6 +573,17 @@ int lloyd_step(vd_batch* b) {
 
 }  // namespace
 
+namespace vd {
+// device bytes a committed batch holds beyond its members' own buffers: the
+// large tier's warps, the huge tier's blocks and the first face pool
+size_t batch_scratch_bytes(int num_sms) {
+  ClipLaunchInfo info{};
+  clip_fp64_info(&info);
+  return (size_t)std::max(4, num_sms * 4) * info.big_scratch_per_warp +
+         (size_t)kBHugeBlocks * clip_huge_scratch_per_block() + ((size_t)1 << 20) * 12;
+}
+}  // namespace vd
+
 extern "C" {
 
 const char* vd_batch_last_error(const vd_batch* b) { return b ? b->err.c_str() : g_batch_create_error.c_str(); }
@@ -624,6 +635,27 @@ int vd_batch_destroy(vd_batch* b) {
   if (b->ev1) cudaEventDestroy(b->ev1);
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
+  return VD_OK;
+}
+
+// the members are dropped and the batch takes new ones; device buffers and
+// the stream are kept (they only grow), so a batch reused for batches of
+// similar size allocates nothing
+int vd_batch_reset(vd_batch* b) {
+  if (!b) return VD_EINVAL;
+  B_CK(b, cudaSetDevice(b->device));
+  B_CK(b, cudaStreamSynchronize(b->stream));
+  drop_graph(b);
+  b->m.clear();
+  b->planes.clear();
+  b->committed = false;
+  b->calculated = false;
+  b->nmax = 0;
+  b->nbins = 0;
+  b->last_ms = 0.f;
+  memset(b->counters, 0, sizeof(b->counters));
+  b->table_reruns = 0;
+  b->pool_reruns = 0;
   return VD_OK;
 }
 
@@ -735,7 +767,7 @@ int vd_batch_commit(vd_batch* b) {
   B_CK(b, b->d_tess_flags.ensure(nt));
   B_CK(b, b->d_counters.ensure(kNumCounters));
   B_CK(b, b->d_pool_cursor.ensure(1));
-  b->pool_cap = 1 << 20;
+  b->pool_cap = std::max<long long>(b->pool_cap, 1 << 20);  // (a reused batch keeps a grown pool)
   B_CK(b, b->d_pool_fnb.ensure(b->pool_cap));
   B_CK(b, b->d_pool_area.ensure(b->pool_cap));
   b->big_warps = std::max(4, b->num_sms * 4);

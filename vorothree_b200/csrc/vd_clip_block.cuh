@@ -732,12 +732,12 @@ __device__ int compute_cell_block(const TessDesc& T, uint32_t i, WarpPoly<C>& P,
 }
 
 constexpr int kHugeBlockWarps = 32;
-// blocks for small tessellations (the host picks them for at most 2,000 cells
-// by default, a tuning setting): a cell's faces are at most its walls' planes
-// plus one per other generator, so its polytope stays small and the clip's
-// barriers, not its passes, set the time (the width changes no result) (the
-// centre of 1,000 generators on a sphere: 14.2 ms with 16 warps, 18.1 ms with
-// 32; at 3,000 generators 32 warps win)
+// the narrower blocks (the host's default width for the huge tier, a tuning
+// setting; the width changes no result): on the slot layout the clip's
+// one-warp rewrite and its barriers, not the classification's passes, set the
+// time, and 16 warps win at every size measured (the centre of 3,000 /
+// 10,000 / 20,000 generators on a sphere: 30.4 / 147.6 / 435 ms against 38.1 /
+// 163.8 / 450 ms with 32)
 constexpr int kHugeBlockWarpsNarrow = 16;
 
 }  // namespace vd

@@ -526,7 +526,9 @@ struct HubOps {
       const unsigned mm = __match_any_sync(kFull, key);
       const int grp = __popc(mm);
       int hprev = -1, hpos = -1;
-      if (isx) {
+      if (isx && g0 == 0) {
+        hpos = (int)((key * 2654435761u) >> 21);  // the table is empty in the first round
+      } else if (isx) {
         unsigned h = (key * 2654435761u) >> 21;  // 11 bits: HCAP = 2048
         for (int s = 0; s < Cf::HCAP; ++s) {
           const uint32_t k = S.hkey[h];
@@ -552,8 +554,8 @@ struct HubOps {
           part = g0 + o;
           ldr = (int)lane < o;
         } else if (grp == 1) {
-          ldr = true;  // its partner comes in a later round
-          bad |= hpos < 0;
+          ldr = true;  // its partner comes in a later round (there is none in one round)
+          bad |= hpos < 0 || ncr <= 32;
         } else {
           bad = true;
         }

@@ -220,6 +220,11 @@ bool wall_from_desc(const vd_wall_desc& d, Wall* w, std::vector<double>* planes,
 }
 }  // namespace vd
 
+// the block-per-cell tier's width: tessellations of at most this many cells
+// run it with 16-warp blocks (on the slot layout 16 warps win at every size
+// measured, 1,000 to 20,000 generators on a sphere), larger ones with 32
+constexpr int kHugeNarrowDefault = 1 << 30;
+
 struct vd_tess {
   std::string err;
   int device = 0;
@@ -316,7 +321,7 @@ struct vd_tess {
   int fast_minb = 6;
   int huge_direct_max = 64;
   int huge_blocks_max = 64;
-  int huge_narrow_max = 2000;
+  int huge_narrow_max = kHugeNarrowDefault;
   int num_sms = 0;
 };
 
@@ -1614,7 +1619,7 @@ int vd_tess_set_tuning(vd_tess* t, const vd_tuning* k) {
   t->fast_minb = k->fast_blocks_per_sm ? k->fast_blocks_per_sm : 6;
   t->huge_direct_max = k->huge_direct_max ? k->huge_direct_max : 64;
   t->huge_blocks_max = k->huge_blocks_max ? k->huge_blocks_max : kHugeBlocksMax;
-  t->huge_narrow_max = k->huge_narrow_max ? k->huge_narrow_max : 2000;
+  t->huge_narrow_max = k->huge_narrow_max ? k->huge_narrow_max : kHugeNarrowDefault;
   return VD_OK;
 }
 

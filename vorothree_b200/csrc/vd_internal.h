@@ -134,6 +134,8 @@ cudaError_t clip_sparse_info(bool mixed, int minb, ClipLaunchInfo* info);
 cudaError_t launch_clip_sparse(const TessDesc& T, const WorkList& W, int nblocks, bool count, bool mixed, int minb,
                                cudaStream_t s);
 cudaError_t clip_sparse_batched_setup(bool mixed, int* blocks_per_sm);
+// device bytes a committed batch holds beyond its members' buffers
+size_t batch_scratch_bytes(int num_sms);
 cudaError_t launch_clip_sparse_batched(const TessDesc* descs, const uint32_t* tess_off, int ntess, const WorkList& W,
                                        int nblocks, bool count, bool mixed, cudaStream_t s);
 cudaError_t launch_clip_mixed_fast(const TessDesc& T, const WorkList& W, int nblocks, bool count,

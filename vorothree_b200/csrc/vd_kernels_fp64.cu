@@ -85,11 +85,12 @@ cudaError_t launch_clip_fp64_huge(const TessDesc& T, const WorkList& W, void* sc
 cudaError_t launch_clip_fp64_huge_batched(const TessDesc* descs, const uint32_t* tess_off, int ntess,
                                           const WorkList& W, void* scratch, int nblocks, cudaStream_t s) {
   WarpPoly<HugeCfg>* polys = reinterpret_cast<WarpPoly<HugeCfg>*>(scratch);
-  constexpr size_t sm = sizeof(HubShared<kHugeBlockWarps>);
-  cudaError_t e = huge_smem(k_clip_huge_block_batched<HugeCfg, kHugeBlockWarps>, sm);
+  // (16-warp blocks: the width that wins on the slot layout)
+  constexpr size_t sm = sizeof(HubShared<kHugeBlockWarpsNarrow>);
+  cudaError_t e = huge_smem(k_clip_huge_block_batched<HugeCfg, kHugeBlockWarpsNarrow>, sm);
   if (e != cudaSuccess) return e;
-  k_clip_huge_block_batched<HugeCfg, kHugeBlockWarps>
-      <<<nblocks, kHugeBlockWarps * 32, sm, s>>>(descs, tess_off, ntess, W, polys);
+  k_clip_huge_block_batched<HugeCfg, kHugeBlockWarpsNarrow>
+      <<<nblocks, kHugeBlockWarpsNarrow * 32, sm, s>>>(descs, tess_off, ntess, W, polys);
   return cudaGetLastError();
 }
 

@@ -9,11 +9,17 @@
 // as soon as a slot is free and its estimated footprint fits beside the
 // requests already running.  Requests that arrive while others are on the
 // GPU are admitted without waiting for them, and the slots' streams overlap
-// on the device.  Each request's result is computed by the same kernels as a
-// standalone vd_tess, so it is the same alone and in the mix.
+// on the device.  Small requests waiting together can be merged
+// (vd_server_set_merging; off by default): a slot takes
+// the run of small requests at the head of the queue and computes them as one
+// batch (vd_batch: one binning pass and one persistent clip launch over a
+// device work list of all their cells) instead of one calculate chain each.
+// Each request's result is computed by the same kernels as a standalone
+// vd_tess, so it is the same alone, in the mix and in a merged batch.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <chrono>
 #include <condition_variable>
 #include <cstdarg>
@@ -41,7 +47,8 @@ struct Request {
   std::vector<vd_wall_desc> walls;
   std::vector<std::vector<double>> wall_planes;  // owned copies of polyhedron planes (points then normals)
   std::vector<double> pts;
-  size_t est_bytes = 0;
+  size_t est_bytes = 0;   // admission estimate when it runs alone
+  size_t data_bytes = 0;  // its share of a merged batch's buffers
   Clock::time_point t_submit, t_start, t_done;
   bool done = false;
   bool started = false;
@@ -66,15 +73,34 @@ constexpr size_t kSlotHugeBlocks = 8;
 // vd_tess (generators, bins, bin-ordered copy, per-cell outputs and 48 face
 // slots, fallback lists), its search order, the slot's bounded large- and
 // huge-tier scratch and a face pool of 2^20 slots
-size_t estimate_bytes(size_t n, size_t bins) {
+size_t estimate_data_bytes(size_t n, size_t bins) {
   const size_t per_cell = 24 * 3 + 32 + 4 * 6 + (8 + 24 + 4 + 4 + 1 + 8) + 48 * 12 + 3 * 4 + 8;
+  return n * per_cell + bins * 16 + (1u << 20);
+}
+
+size_t estimate_bytes(size_t n, size_t bins) {
   static const size_t scratch = [] {
     vd::ClipLaunchInfo info{};
     vd::clip_fp64_info(&info);
     return kSlotBigWarps * info.big_scratch_per_warp + kSlotHugeBlocks * vd::clip_huge_scratch_per_block() +
            ((size_t)1 << 20) * 12;
   }();
-  return n * per_cell + bins * 16 + (1u << 20) + scratch;
+  return estimate_data_bytes(n, bins) + scratch;
+}
+
+// merging: a request joins a merged batch when it asks for no face results,
+// has at most max_request generators and a box and grid the standalone path
+// accepts (anything else runs alone and gets the standalone path's answer)
+bool mergeable(const Request& r, size_t max_request) {
+  const size_t n = r.pts.size() / 3;
+  if (r.faces || n == 0 || n > max_request || r.walls.size() > (size_t)vd::kMaxWalls) return false;
+  for (int a = 0; a < 3; ++a) {
+    if (r.n[a] <= 0 || r.n[a] > 16000) return false;
+    if (!(r.bmax[a] > r.bmin[a]) || !std::isfinite(r.bmin[a]) || !std::isfinite(r.bmax[a]) ||
+        !std::isfinite(r.bmax[a] - r.bmin[a]))
+      return false;
+  }
+  return (double)r.n[0] * r.n[1] * r.n[2] <= 1.0e7;
 }
 
 double percentile(std::vector<double> v, double q) {
@@ -100,6 +126,11 @@ struct vd_server {
   size_t in_use = 0, peak = 0;
   int running = 0, peak_running = 0;
   bool face_results = false;
+  // merging of small requests (max_members <= 1: off)
+  int merge_members = 0;
+  size_t merge_request = 65536, merge_group = (size_t)1 << 20;
+  size_t batch_scratch = 0;
+  uint64_t groups = 0, merged = 0;
   uint64_t next_id = 1;
   bool stop = false;
   std::vector<std::thread> workers;
@@ -169,11 +200,47 @@ int run_request(vd_tess* t, int precision, Request& r) {
   return rc;
 }
 
+// the requests of a merged group computed as one batch (vd_batch_add for
+// each, one commit, one calculate); false if the batch failed, and then each
+// request runs alone
+bool run_group(vd_batch* b, int precision, std::vector<std::shared_ptr<Request>>& g) {
+  int rc = vd_batch_reset(b);
+  if (rc == VD_OK) rc = vd_batch_set_precision(b, precision);
+  std::vector<int> idx(g.size(), -1);
+  for (size_t k = 0; k < g.size() && rc == VD_OK; ++k) {
+    Request& r = *g[k];
+    std::vector<vd_wall_desc> w = r.walls;
+    for (size_t j = 0; j < w.size(); ++j)
+      if (w[j].kind == 5 && w[j].nplanes > 0) {
+        w[j].points = r.wall_planes[j].data();
+        w[j].normals = r.wall_planes[j].data() + 3 * w[j].nplanes;
+      }
+    rc = vd_batch_add(b, r.bmin, r.bmax, r.n[0], r.n[1], r.n[2], w.data(), (int)w.size(), r.pts.data(),
+                      r.pts.size() / 3, &idx[k]);
+  }
+  if (rc == VD_OK) rc = vd_batch_commit(b);
+  if (rc == VD_OK) rc = vd_batch_calculate(b);
+  for (size_t k = 0; k < g.size() && rc == VD_OK; ++k) {
+    Request& r = *g[k];
+    size_t n = 0;
+    rc = vd_batch_count_cells(b, idx[k], &n);
+    if (rc != VD_OK) break;
+    r.ncells = n;
+    r.vol.resize(n);
+    r.cen.resize(3 * n);
+    r.nf.resize(n);
+    rc = vd_batch_get_summaries(b, idx[k], r.vol.data(), r.cen.data(), r.nf.data());
+  }
+  return rc == VD_OK;
+}
+
 void worker(vd_server* s, int slot) {
   cudaSetDevice(s->device);
   vd_tess* t = s->handles[slot];
+  vd_batch* b = nullptr;  // this slot's merged batches (made for its first)
   for (;;) {
-    std::shared_ptr<Request> r;
+    std::vector<std::shared_ptr<Request>> g;
+    size_t charge = 0;
     {
       std::unique_lock<std::mutex> lock(s->mu);
       s->cv_work.wait(lock, [&] {
@@ -182,37 +249,75 @@ void worker(vd_server* s, int slot) {
         const size_t need = s->queue.front()->est_bytes;
         return s->in_use == 0 || s->in_use + need <= s->budget;
       });
-      if (s->stop) return;
-      r = s->queue.front();
+      if (s->stop) break;
+      std::shared_ptr<Request> r = s->queue.front();
       s->queue.pop_front();
-      s->in_use += r->est_bytes;
+      g.push_back(r);
+      charge = r->est_bytes;
+      // the run of small requests behind it joins it, as far as the budget
+      // and the group limits allow (FIFO order is kept: the run ends at the
+      // first request that cannot join)
+      if (s->merge_members > 1 && mergeable(*r, s->merge_request)) {
+        size_t cells = r->pts.size() / 3, data = r->data_bytes;
+        while ((int)g.size() < s->merge_members && !s->queue.empty()) {
+          const std::shared_ptr<Request>& q = s->queue.front();
+          const size_t qn = q->pts.size() / 3;
+          if (!mergeable(*q, s->merge_request) || cells + qn > s->merge_group) break;
+          if (s->in_use + data + q->data_bytes + s->batch_scratch > s->budget) break;
+          cells += qn;
+          data += q->data_bytes;
+          g.push_back(q);
+          s->queue.pop_front();
+        }
+        if (g.size() > 1) charge = data + s->batch_scratch;
+      }
+      s->in_use += charge;
       s->peak = std::max(s->peak, s->in_use);
-      s->running++;
+      s->running += (int)g.size();
       s->peak_running = std::max(s->peak_running, s->running);
-      r->started = true;
-      r->t_start = Clock::now();
+      const Clock::time_point now = Clock::now();
+      for (auto& q : g) {
+        q->started = true;
+        q->t_start = now;
+      }
     }
-    // the next queued request may fit beside this one
+    // the next queued request may fit beside these
     s->cv_work.notify_all();
-    const int rc = run_request(t, s->precision, *r);
+    std::vector<int> rcs(g.size(), VD_OK);
+    bool grouped = false;
+    if (g.size() > 1) {
+      if (!b && vd_batch_create(&b) != VD_OK) b = nullptr;
+      if (b) grouped = run_group(b, s->precision, g);
+    }
+    if (!grouped)
+      for (size_t k = 0; k < g.size(); ++k) rcs[k] = run_request(t, s->precision, *g[k]);
     {
       std::lock_guard<std::mutex> lock(s->mu);
-      s->in_use -= r->est_bytes;
-      s->running--;
-      r->status = rc;
-      r->t_done = Clock::now();
-      r->done = true;
-      r->pts.clear();
-      r->pts.shrink_to_fit();
-      if (rc == VD_OK) {
-        s->latencies.push_back(std::chrono::duration<double>(r->t_done - r->t_submit).count());
-        s->completed++;
-        s->cells += r->ncells;
+      s->in_use -= charge;
+      s->running -= (int)g.size();
+      if (grouped) {
+        s->groups++;
+        s->merged += g.size();
+      }
+      const Clock::time_point now = Clock::now();
+      for (size_t k = 0; k < g.size(); ++k) {
+        Request& r = *g[k];
+        r.status = rcs[k];
+        r.t_done = now;
+        r.done = true;
+        r.pts.clear();
+        r.pts.shrink_to_fit();
+        if (rcs[k] == VD_OK) {
+          s->latencies.push_back(std::chrono::duration<double>(r.t_done - r.t_submit).count());
+          s->completed++;
+          s->cells += r.ncells;
+        }
       }
     }
     s->cv_done.notify_all();
     s->cv_work.notify_all();
   }
+  if (b) vd_batch_destroy(b);
 }
 
 // the request's clock starts at t0 (before parsing, for a text request)
@@ -248,6 +353,7 @@ int submit_points(vd_server* s, const double bmin[3], const double bmax[3], int 
   r->pts = std::move(pts);
   r->faces = s->face_results;
   r->est_bytes = estimate_bytes(n, (size_t)nx * ny * nz);
+  r->data_bytes = estimate_data_bytes(n, (size_t)nx * ny * nz);
   if (r->est_bytes > s->budget) return sfail(s, VD_ENOMEM, "request needs %zu bytes, budget %zu", r->est_bytes, s->budget);
   {
     std::lock_guard<std::mutex> lock(s->mu);
@@ -280,6 +386,11 @@ int vd_server_create(int slots, size_t hbm_budget_bytes, int precision, vd_serve
   }
   s->budget = hbm_budget_bytes;
   s->precision = precision;
+  {
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
+    s->batch_scratch = vd::batch_scratch_bytes(sms);
+  }
   const double lo[3] = {0, 0, 0}, hi[3] = {1, 1, 1};
   for (int k = 0; k < slots; ++k) {
     vd_tess* t = nullptr;
@@ -463,6 +574,23 @@ int vd_server_cancel(vd_server* s, uint64_t ticket) {
   return VD_OK;
 }
 
+int vd_server_set_merging(vd_server* s, int max_members, size_t max_request, size_t max_group) {
+  if (!s || max_members < 0) return VD_EINVAL;
+  std::lock_guard<std::mutex> lock(s->mu);
+  s->merge_members = max_members;
+  if (max_request) s->merge_request = max_request;
+  if (max_group) s->merge_group = max_group;
+  return VD_OK;
+}
+
+int vd_server_merge_stats(vd_server* s, uint64_t* groups, uint64_t* merged_requests) {
+  if (!s) return VD_EINVAL;
+  std::lock_guard<std::mutex> lock(s->mu);
+  if (groups) *groups = s->groups;
+  if (merged_requests) *merged_requests = s->merged;
+  return VD_OK;
+}
+
 int vd_server_concurrency(vd_server* s, int* running, int* peak_running) {
   if (!s) return VD_EINVAL;
   std::lock_guard<std::mutex> lock(s->mu);
@@ -491,6 +619,8 @@ int vd_server_reset_stats(vd_server* s) {
   s->cells = 0;
   s->peak = s->in_use;
   s->peak_running = s->running;
+  s->groups = 0;
+  s->merged = 0;
   return VD_OK;
 }
 

@@ -117,6 +117,21 @@ class TessellationServer:
         self._chk(rc)
         return True
 
+    def set_merging(self, max_members: int = 64, max_request: int = 65536, max_group: int = 1 << 20):
+        """Merging of small requests (off by default): a slot
+        that starts a request without face results of at most max_request
+        generators also takes the run of such requests behind it in the queue
+        (up to max_members, max_group generators in all, within the HBM budget)
+        and computes them as one batch; max_members <= 1 turns it off."""
+        self._chk(self._L.vd_server_set_merging(self._h, int(max_members), int(max_request), int(max_group)))
+
+    def merge_stats(self) -> dict:
+        """Merged batches run and the requests they served since reset_stats."""
+        g = C.c_uint64()
+        m = C.c_uint64()
+        self._chk(self._L.vd_server_merge_stats(self._h, C.byref(g), C.byref(m)))
+        return {"groups": g.value, "merged_requests": m.value}
+
     def concurrency(self) -> dict:
         """Requests on the GPU now, and the most at once since reset_stats."""
         run = C.c_int()

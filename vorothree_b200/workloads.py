@@ -46,8 +46,9 @@ def batch_members(ntess=4096, seed=0):
     return out
 
 
-def serving_requests(count, seed=0):
-    """Requests of the serving configuration: sizes log-uniform in [1e3, 1e6];
+def serving_requests(count, seed=0, sizes=(1e3, 1e6)):
+    """Requests of the serving configuration: sizes log-uniform in [1e3, 1e6]
+    (or the given range);
     half uniform, half clustered (8 Gaussian blobs, sigma 0.03, 70% of the
     points); 0-2 walls drawn from {plane through the centre with a random
     normal, centred sphere of radius U[0.3, 0.5]}; grid from the autotuner.
@@ -58,7 +59,7 @@ def serving_requests(count, seed=0):
     rng = np.random.Generator(np.random.PCG64(seed))
     out = []
     for k in range(count):
-        n = int(round(np.exp(rng.uniform(np.log(1e3), np.log(1e6)))))
+        n = int(round(np.exp(rng.uniform(np.log(sizes[0]), np.log(sizes[1])))))
         clustered = rng.uniform() < 0.5
         if clustered:
             nb = int(0.7 * n)
