@@ -645,17 +645,17 @@ def serving_leg(args, nreq: int, rates) -> dict:
 def burst_leg(args, nreq: int = 256) -> dict:
     """A burst of small requests (sizes log-uniform in [1e3, 3.2e4], the
     serving mix otherwise) submitted at once, served with the merging of small
-    requests into batches and without it: wall time from the first submit to
+    requests into batches (up to 64 or 8 a batch) and without it: wall time from the first submit to
     the last result, cells/s, p50/p99 latency and the batches formed."""
     import vorothree_b200 as v
     reqs = serving_requests(nreq, seed=5, sizes=(1e3, 3.2e4))
     out = {"config": {"requests": nreq, "sizes": "log-uniform [1e3, 3.2e4]", "slots": args.serve_slots,
                       "arrivals": "all at once"}}
-    for mode in ("merged", "alone"):
+    for mode, members in (("merged", 64), ("merged_8", 8), ("alone", 0)):
         srv = v.TessellationServer(slots=args.serve_slots, hbm_budget_bytes=args.serve_budget_gb << 30,
                                    precision=args.precision)
-        if mode == "merged":
-            srv.set_merging(max_members=64)
+        if members:
+            srv.set_merging(max_members=members)
         for _ in range(2):  # warm the slots' buffers (and batches)
             srv.reset_stats()
             t0 = time.perf_counter()
