@@ -737,7 +737,7 @@ def run_suite(args):
         # the library's tuned launch settings for this input's class and size
         # (the grid stays the bench's own heuristic)
         cls = autotune.distribution_class(t.generators(), v.BoundingBox(*box))
-        tun = autotune.lookup_tuning(cls, n)
+        tun = autotune.input_tuning(t.generators(), v.BoundingBox(*box))
         t.set_tuning(tun)
         t.calculate()
         one = t.timings()["total_ms"]

@@ -150,6 +150,9 @@ typedef struct {
   int huge_blocks_max;     /* most concurrent blocks of the block-per-cell tier (default 64, at most 256) */
   int huge_narrow_max;     /* tessellations of at most this many cells run that tier with 16-warp blocks,
                               larger ones with 32 (default 2^30: always 16) */
+  int noop_run;            /* after this many clips in a row that changed nothing, the walk tests the next
+                              candidates' planes together, one per lane, and passes over those that cut
+                              nothing (-1: never; 0 keeps the default, -1) */
 } vd_tuning;
 int vd_tess_set_tuning(vd_tess* t, const vd_tuning* k);
 /* the settings in force (defaults filled in) */

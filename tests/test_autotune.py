@@ -123,3 +123,19 @@ def test_every_tuning_choice_gives_the_oracles_cells(oracle_mod):
             assert np.array_equal(gn, on) and np.array_equal(gv, ov) and np.array_equal(gc, oc), tun
             assert np.array_equal(t.neighbors()[1], oids), tun
             t.close()
+
+def test_hollow_inputs_get_batched_plane_tests():
+    """A dense central box or generators on a sphere leave most of the box
+    empty: the per-input settings turn the walk's batched plane tests on for
+    them and leave them off for uniform, plane-crowded and blob inputs."""
+    from vorothree_b200 import autotune as at
+    from vorothree_b200.tessellation import BoundingBox
+    from vorothree_b200.workloads import bench_distribution
+    box = BoundingBox([0, 0, 0], [100, 100, 100])
+    for kind, want in (("central", True), ("sphere", True), ("uniform", False), ("axes", False)):
+        pts = bench_distribution(kind, 5000, 3)
+        assert at.hollow(pts, box) == want, kind
+        assert at.input_tuning(pts, box, {})["noop_run"] == (at.NOOP_RUN_HOLLOW if want else -1), kind
+    unit = BoundingBox([0, 0, 0], [1, 1, 1])
+    assert not at.hollow(at.synthetic("clustered", 1 << 14, 1), unit)
+    assert at.choose(bench_distribution("central", 2000, 4), box, {})[1]["noop_run"] == at.NOOP_RUN_HOLLOW

@@ -510,3 +510,26 @@ def test_calculate_strided_shards(oracle_mod, stride):
     with pytest.raises(v.VoronoidError):
         t.export_cells(0, 10)
     t.close()
+
+
+@pytest.mark.parametrize("kind,n", [("central", 3000), ("axes", 3000), ("sphere", 1000), ("uniform", 20000)])
+def test_batched_plane_tests_bitwise(oracle_mod, kind, n):
+    """The walk's variant that tests the candidates' planes together after a
+    run of clips that changed nothing (tuning noop_run) passes over exactly
+    the clips the reference makes without effect: every cell equals the
+    oracle's, bit for bit, on the reference's bench distributions (the
+    central box's edge cells clip with thousands of candidates, nearly all
+    without effect)."""
+    import vorothree_b200 as v
+    from common import bench_distribution
+    pts = bench_distribution(kind, n, 90 + len(kind))
+    g = int(np.ceil(n ** (1.0 / 3.0)))
+    o = oracle_tess(oracle_mod, [0, 0, 0], [100, 100, 100], (g, g, g), pts)
+    for run, layout in ((1, "slots"), (3, "slots"), (2, "full")):
+        t = v.Tessellation(v.BoundingBox([0, 0, 0], [100, 100, 100]), v.Algorithm3DGrid(g, g, g))
+        t.set_tuning({"noop_run": run, "fast_layout": layout})
+        assert t.get_tuning()["noop_run"] == run
+        t.set_generators(pts)
+        t.calculate()
+        assert_same(t, o, check_counters=False)
+        t.close()

@@ -31,7 +31,7 @@ FAST_LAYOUTS = {"slots": VD_FAST_SLOTS, "full": VD_FAST_FULL}
 class Tuning(C.Structure):
     """vd_tuning: launch choices that change no result (0 = default)."""
     _fields_ = [("fast_layout", C.c_int), ("fast_blocks_per_sm", C.c_int), ("huge_direct_max", C.c_int),
-                ("huge_blocks_max", C.c_int), ("huge_narrow_max", C.c_int)]
+                ("huge_blocks_max", C.c_int), ("huge_narrow_max", C.c_int), ("noop_run", C.c_int)]
 
 STATUS_NAMES = {VD_EINVAL: "VD_EINVAL", VD_ENOMEM: "VD_ENOMEM", VD_EOVERFLOW: "VD_EOVERFLOW",
                 VD_ETIMEOUT: "VD_ETIMEOUT", VD_ECUDA: "VD_ECUDA", VD_ESTATE: "VD_ESTATE", VD_EIO: "VD_EIO",

@@ -12,7 +12,10 @@ and once for the tessellation, on inputs with cells adjacent to thousands of
 others (the reference's sphere-surface benchmark distribution):
   * the hand-off to the block-per-cell tier: how few cells left after the
     medium tier go there directly, how many blocks it runs at once, and up to
-    which tessellation size its blocks are 16 warps wide instead of 32.
+    which tessellation size its blocks are 16 warps wide instead of 32;
+and per input, from its coarse occupancy (`hollow`):
+  * the walk's batched plane tests, for inputs that leave large parts of the
+    box empty.
 None of these changes a result: every choice computes the same doubles.
 
 The tuner times Tessellation.calculate on the GPU (coordinate descent: bin
@@ -47,7 +50,7 @@ _SAMPLE = 1 << 16
 # the first tier's choices the tuner searches, and the library's defaults
 LAYOUTS = ("slots", "full")
 BLOCKS_PER_SM = (5, 6, 7)
-DEFAULT_TUNING = {"fast_layout": "slots", "fast_blocks_per_sm": 6}
+DEFAULT_TUNING = {"fast_layout": "slots", "fast_blocks_per_sm": 6, "noop_run": -1}
 # the block-per-cell tier's hand-off, searched once (HANDOFF_KEY)
 HANDOFF_KEY = "handoff"
 DIRECT_MAX = (1, 16, 64, 256)
@@ -158,11 +161,45 @@ def choose_grid(points, bounds, entries: Optional[Dict[str, dict]] = None) -> Tu
     return grid_for(len(pts), bounds, lookup(cls, len(pts), entries))
 
 
+# the walk's batched plane tests (tuning noop_run) for hollow inputs: after
+# this many clips in a row that changed nothing
+NOOP_RUN_HOLLOW = 8
+HOLLOW_EMPTY = 0.25
+
+
+def hollow(points, bounds) -> bool:
+    """Whether the generators leave large parts of the box empty: more than a
+    quarter of the 4 x 4 x 4 equal parts of the box hold none (a dense central
+    box, generators on a sphere).  The cells at the edge of such a region reach
+    far into the empty part, and their walks clip with thousands of candidates,
+    nearly all without effect; the walk's batched plane tests pass over those
+    clips (central box, 10,000 generators: 7.2 against 3.6 ms), and cost
+    instructions on other inputs (uniform: about 10%)."""
+    pts = np.asarray(points, np.float64).reshape(-1, 3)
+    if len(pts) == 0:
+        return False
+    lo = np.asarray(bounds.min, np.float64)
+    hi = np.asarray(bounds.max, np.float64)
+    idx = np.clip(((pts - lo) / (hi - lo) * 4).astype(np.int64), 0, 3)
+    lin = idx[:, 0] + 4 * (idx[:, 1] + 4 * idx[:, 2])
+    return 1.0 - len(np.unique(lin)) / 64.0 > HOLLOW_EMPTY
+
+
+def input_tuning(points, bounds, entries: Optional[Dict[str, dict]] = None) -> dict:
+    """The launch settings for this input: the table's for its class and size,
+    with the walk's batched plane tests on when the input is hollow."""
+    pts = np.asarray(points, np.float64).reshape(-1, 3)
+    tun = lookup_tuning(distribution_class(pts, bounds), len(pts), entries)
+    if hollow(pts, bounds):
+        tun["noop_run"] = NOOP_RUN_HOLLOW
+    return tun
+
+
 def choose(points, bounds, entries: Optional[Dict[str, dict]] = None) -> Tuple[Tuple[int, int, int], dict]:
     """(grid, launch settings) the tuner would use for this input."""
     pts = np.asarray(points, np.float64).reshape(-1, 3)
     cls = distribution_class(pts, bounds)
-    return grid_for(len(pts), bounds, lookup(cls, len(pts), entries)), lookup_tuning(cls, len(pts), entries)
+    return grid_for(len(pts), bounds, lookup(cls, len(pts), entries)), input_tuning(pts, bounds, entries)
 
 
 def _time(points, bounds, grid, walls, tuning: dict, reps: int, precision: str) -> float:
@@ -208,7 +245,7 @@ def tune(points, bounds, walls: Sequence = (), factors: Iterable[float] = FACTOR
     g = win["grid"]
     for layout in layouts:
         for nb in (blocks if layout == "slots" else (6,)):
-            tun = {"fast_layout": layout, "fast_blocks_per_sm": nb}
+            tun = dict(DEFAULT_TUNING, fast_layout=layout, fast_blocks_per_sm=nb)
             if tun == DEFAULT_TUNING:
                 continue
             trials.append({"factor": win["factor"], "grid": list(g), "tuning": tun,

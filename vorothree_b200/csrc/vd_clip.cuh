@@ -695,6 +695,34 @@ __device__ int warp_clip(WarpPoly<C>& P, PolyState& S, double px, double py, dou
   return kClipMod;
 }
 
+// Whether clip_with_scratch with this lane's own plane (a different one per
+// lane) would change the polytope: some vertex lies outside, d > 1e-9, with d
+// computed as the clip computes it (:302-326).  Every lane walks every vertex
+// in the same order (broadcast reads).
+template <class C>
+__device__ __forceinline__ bool plane_cuts(const WarpPoly<C>& P, const PolyState& S, double px, double py,
+                                           double pz, double nx, double ny, double nz) {
+  bool cut = false;
+  for (int v = 0; v < S.nv; ++v) {
+    const double d = (P.vx[v] - px) * nx + (P.vy[v] - py) * ny + (P.vz[v] - pz) * nz;
+    cut |= d > kTol;
+  }
+  return cut;
+}
+
+template <class C>
+__device__ __forceinline__ int poly_nverts(const WarpPoly<C>&, const PolyState& S) {
+  return S.nv;
+}
+
+// in the walk's variant with batched plane tests (compute_cell<C, true>):
+// with a run of TessDesc::noop_run clips that changed nothing and at least
+// kNoopBatch candidates passing the radius tests, the candidates' planes are
+// tested together.  The variant is a separate kernel: the test's code in the
+// walk costs the common path registers (uniform input: 40.3 against 34.8 ms
+// per 1 M cells with the test compiled in and never taken).
+constexpr int kNoopBatch = 8;
+
 // instrumented runs: the candidates of the bins the walk opens when it
 // reaches entries (elo, ehi] of this chunk at radius^2 c4/4 -- every member
 // but the cell's own generator (algo_3d_grid.rs:190-196)
@@ -723,7 +751,7 @@ __device__ __forceinline__ void count_opened(PolyT& P, int elo, int ehi, bool va
 //    the current R; the bin being processed already opened;
 //  - a member is clipped with when dist^2 <= 4R^2 at its turn.
 // Each clip may shrink R, and the ballots are re-evaluated after it.
-template <class C, class PolyT>
+template <class C, bool NOOP = false, class PolyT>
 __device__ int compute_cell(const TessDesc& T, uint32_t i, PolyT& P, typename PolyT::State& S) {
   const unsigned lane = lane_id();
   const double gx = T.gen[3 * (size_t)i], gy = T.gen[3 * (size_t)i + 1], gz = T.gen[3 * (size_t)i + 2];
@@ -769,6 +797,7 @@ __device__ int compute_cell(const TessDesc& T, uint32_t i, PolyT& P, typename Po
   const double rz = (gz - G.bmin[2]) * G.scale[2] - (double)iz;
 
   bool done = false;
+  [[maybe_unused]] int nnoop = 0;  // clips in a row that changed nothing (NOOP)
   for (int base = 0; base < T.norder && !done; base += 32) {
     // ---- this lane's search-order entry ----
     const int k = base + (int)lane;
@@ -847,6 +876,32 @@ __device__ int compute_cell(const TessDesc& T, uint32_t i, PolyT& P, typename Po
         const bool ok = cand && idx >= pos && ce < fb && !(dist_sq > c4) && (ce == ecur || cb2 <= c4);
         const unsigned pass = __ballot_sync(kFull, ok);
         if (!pass) break;
+        if constexpr (NOOP) {
+          if (T.noop_run > 0 && nnoop >= T.noop_run && __popc(pass) >= kNoopBatch) {
+            // in a run of clips that changed nothing (a cell whose radius still
+            // reaches far, e.g. at the edge of a populated region), the passing
+            // candidates' planes are tested together, one per lane, and those
+            // before the first plane that cuts are passed over: clipping with
+            // them would change neither the polytope nor R, and the candidates
+            // that pass do not change either (the reference's sequence, bit for bit)
+            const bool cuts =
+                plane_cuts(P, S, gx + d0 * 0.5, gy + d1 * 0.5, gz + d2 * 0.5, d0, d1, d2);
+            const unsigned cm = __ballot_sync(kFull, cuts) & pass;
+            const unsigned skip = cm ? pass & ((1u << (__ffs(cm) - 1)) - 1u) : pass;
+            if (skip) {
+              const int jl = 31 - __clz(skip);
+              const int el = __shfl_sync(kFull, ce, jl);
+              if constexpr (C::COUNT) {
+                count_opened(P, ecur, el, valid, inr, own, md2, b2, be - bs, c4);
+                cnt_add(P, kCntClips, (unsigned long long)__popc(skip));
+                cnt_add(P, kCntClassified, (unsigned long long)__popc(skip) * (unsigned long long)poly_nverts(P, S));
+              }
+              ecur = el;
+              pos = r0 + jl + 1;
+              continue;
+            }
+          }
+        }
         const int j = __ffs(pass) - 1;
         const int ej = __shfl_sync(kFull, ce, j);
         if constexpr (C::COUNT) count_opened(P, ecur, ej, valid, inr, own, md2, b2, be - bs, c4);
@@ -859,6 +914,7 @@ __device__ int compute_cell(const TessDesc& T, uint32_t i, PolyT& P, typename Po
         if (r == kClipOverflow) return kCellOverflow;
         if (r == kClipMod) cur = r2;
         else if (r == kClipEmpty) cur = 0.0;
+        if constexpr (NOOP) nnoop = r == kClipNoop ? nnoop + 1 : 0;
         ecur = ej;
         pos = r0 + j + 1;
       }
@@ -1012,7 +1068,7 @@ __device__ void export_cell(const WorkList& W, const WarpPoly<C>& P, const PolyS
 }
 
 // Persistent warps pull cells from the work list and build them.
-template <class C, class PolyT>
+template <class C, bool NOOP = false, class PolyT>
 __device__ void clip_worker(const TessDesc& T, const WorkList& W, PolyT& P) {
   const unsigned lane = lane_id();
   if constexpr (C::COUNT) {
@@ -1026,7 +1082,7 @@ __device__ void clip_worker(const TessDesc& T, const WorkList& W, PolyT& P) {
     if (idx >= W.nitems) break;
     const uint32_t cell = W.items ? W.items[idx] : (uint32_t)T.sorted[idx].id;
     typename PolyT::State S;
-    const int st = compute_cell<C>(T, cell, P, S);
+    const int st = compute_cell<C, NOOP>(T, cell, P, S);
     if (st == kCellOk) {
       finalize_cell<C>(T, cell, P, S);
       if constexpr (PolyT::kExport) {
@@ -1101,18 +1157,19 @@ __device__ void clip_worker_batched(const TessDesc* descs, const uint32_t* tess_
 // global scratch buffer.
 constexpr int kFastWarpsPerBlock = 4;
 
-// MINB: blocks per SM the register budget must admit (shared memory sets it)
-template <class C, int WPB, int MINB>
+// MINB: blocks per SM the register budget must admit (shared memory sets it);
+// NOOP: the walk's variant with batched plane tests (compute_cell)
+template <class C, int WPB, int MINB, bool NOOP = false>
 __global__ void __launch_bounds__(WPB * 32, MINB) k_clip_fast(const TessDesc T, const WorkList W) {
   extern __shared__ __align__(16) unsigned char smem[];
   WarpPoly<C>* polys = reinterpret_cast<WarpPoly<C>*>(smem);
-  clip_worker<C>(T, W, polys[threadIdx.x >> 5]);
+  clip_worker<C, NOOP>(T, W, polys[threadIdx.x >> 5]);
 }
 
-template <class C>
+template <class C, bool NOOP = false>
 __global__ void __launch_bounds__(128) k_clip_big(const TessDesc T, const WorkList W, WarpPoly<C>* scratch) {
   const size_t gw = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  clip_worker<C>(T, W, scratch[gw]);
+  clip_worker<C, NOOP>(T, W, scratch[gw]);
 }
 
 template <class C, int WPB, int MINB>

@@ -190,6 +190,31 @@ __device__ double poly_max_radius_sq(const SparsePoly<C>& P, const SparseState& 
   return sp_warp_max_nonneg(m);
 }
 
+// whether clip_with_scratch with this lane's own plane would change the
+// polytope: some live vertex outside, d > 1e-9, computed as the clip does
+// (every lane walks every live slot in the same order)
+template <class C>
+__device__ __forceinline__ bool plane_cuts(const SparsePoly<C>& P, const SparseState& S, double px, double py,
+                                           double pz, double nx, double ny, double nz) {
+  bool cut = false;
+#pragma unroll
+  for (int w = 0; w < 3; ++w) {
+    unsigned L = w == 0 ? S.live0 : (w == 1 ? S.live1 : S.live2);
+    while (L) {
+      const int v = 32 * w + __ffs(L) - 1;
+      L &= L - 1u;
+      const double d = (P.vx[v] - px) * nx + (P.vy[v] - py) * ny + (P.vz[v] - pz) * nz;
+      cut |= d > kTol;
+    }
+  }
+  return cut;
+}
+
+template <class C>
+__device__ __forceinline__ int poly_nverts(const SparsePoly<C>&, const SparseState& S) {
+  return __popc(S.live0) + __popc(S.live1) + __popc(S.live2);
+}
+
 // clip_with_scratch (cell_3d_faces.rs:288-503) on the slot layout.  All lanes
 // call it with the same arguments; the return value and *r2out are the
 // reference's (*r2out: the largest |v - g|^2 over the new vertex set when
@@ -723,11 +748,12 @@ __device__ void finalize_cell(const TessDesc& T, uint32_t i, SparsePoly<C>& P, c
 }
 
 // The kernels: persistent warps, each with its polytope in shared memory.
-template <class C, int WPB, int MINB>
+// NOOP: the walk's variant with batched plane tests (compute_cell)
+template <class C, int WPB, int MINB, bool NOOP = false>
 __global__ void __launch_bounds__(WPB * 32, MINB) k_clip_sparse(const TessDesc T, const WorkList W) {
   extern __shared__ __align__(16) unsigned char smem[];
   SparsePoly<C>* polys = reinterpret_cast<SparsePoly<C>*>(smem);
-  clip_worker<C>(T, W, polys[threadIdx.x >> 5]);
+  clip_worker<C, NOOP>(T, W, polys[threadIdx.x >> 5]);
 }
 
 template <class C, int WPB, int MINB>

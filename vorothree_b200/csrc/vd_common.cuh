@@ -87,6 +87,8 @@ struct TessDesc {
   const uint32_t* bin_of;
   const uint32_t* bin_start;
   const uint32_t* occ;  // optional: bit b set when bin b has members (sparse grids)
+  int noop_run;         // > 0: a run of this many clips that changed nothing batches the walk's
+                        // plane tests (compute_cell); 0: never
   const SortedGen* sorted;
   uint32_t ncells;
   // outputs

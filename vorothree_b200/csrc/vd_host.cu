@@ -224,6 +224,9 @@ bool wall_from_desc(const vd_wall_desc& d, Wall* w, std::vector<double>* planes,
 // run it with 16-warp blocks (on the slot layout 16 warps win at every size
 // measured, 1,000 to 20,000 generators on a sphere), larger ones with 32
 constexpr int kHugeNarrowDefault = 1 << 30;
+// the walk's batched plane tests after a run of clips that change nothing
+// (-1: off)
+constexpr int kNoopRunDefault = -1;
 
 struct vd_tess {
   std::string err;
@@ -322,6 +325,7 @@ struct vd_tess {
   int huge_direct_max = 64;
   int huge_blocks_max = 64;
   int huge_narrow_max = kHugeNarrowDefault;
+  int noop_run = kNoopRunDefault;
   int num_sms = 0;
 };
 
@@ -518,6 +522,7 @@ TessDesc make_desc(vd_tess* t) {
   T.bin_of = t->d_bin_of.p;
   T.bin_start = t->d_bin_start.p;
   T.occ = t->occ_valid ? t->d_occ.p : nullptr;
+  T.noop_run = t->noop_run > 0 ? t->noop_run : 0;
   T.sorted = t->d_sorted.p;
   T.ncells = (uint32_t)t->ngen;
   T.vol = t->d_vol.p;
@@ -643,7 +648,7 @@ int clip_pass(vd_tess* t, int tier, const uint32_t* items, uint32_t nitems, uint
   if (tier == 1) {
     const int nblocks = (int)std::max<size_t>(
         1, std::min<size_t>((nitems + 1) / 2, (size_t)t->num_sms * std::max(1, t->infomed.blocks_per_sm)));
-    VD_CK(t, launch_clip_med(T, W, nblocks, t->instrument, s));
+    VD_CK(t, launch_clip_med(T, W, nblocks, t->instrument, s, t->noop_run > 0));
     g_launches++;
   } else if (tier <= 0) {
     const bool mixed = t->precision == VD_PREC_MIXED;
@@ -657,16 +662,16 @@ int clip_pass(vd_tess* t, int tier, const uint32_t* items, uint32_t nitems, uint
     const int nblocks = (int)std::max<size_t>(
         1, std::min<size_t>(warps_needed, (size_t)t->num_sms * std::max(1, li.blocks_per_sm)));
     if (slots)
-      VD_CK(t, launch_clip_sparse(T, W, nblocks, t->instrument, mixed, t->fast_minb, s));
+      VD_CK(t, launch_clip_sparse(T, W, nblocks, t->instrument, mixed, t->fast_minb, t->noop_run > 0, s));
     else
       VD_CK(t, mixed ? launch_clip_mixed_fast(T, W, nblocks, t->instrument, s)
-                     : launch_clip_fp64_fast(T, W, nblocks, t->instrument, s));
+                     : launch_clip_fp64_fast(T, W, nblocks, t->instrument, s, t->noop_run > 0));
     g_launches++;
   } else if (tier == 2) {
     int r = ensure_big(t, nitems);
     if (r != VD_OK) return r;
     T = make_desc(t);
-    VD_CK(t, launch_clip_fp64_big(T, W, t->d_big.p, (int)t->big_warps, s));
+    VD_CK(t, launch_clip_fp64_big(T, W, t->d_big.p, (int)t->big_warps, s, t->noop_run > 0));
     g_launches++;
   } else {
     int r = ensure_huge(t, nitems);
@@ -1620,6 +1625,7 @@ int vd_tess_set_tuning(vd_tess* t, const vd_tuning* k) {
   t->huge_direct_max = k->huge_direct_max ? k->huge_direct_max : 64;
   t->huge_blocks_max = k->huge_blocks_max ? k->huge_blocks_max : kHugeBlocksMax;
   t->huge_narrow_max = k->huge_narrow_max ? k->huge_narrow_max : kHugeNarrowDefault;
+  t->noop_run = k->noop_run ? k->noop_run : kNoopRunDefault;
   return VD_OK;
 }
 
@@ -1630,6 +1636,7 @@ int vd_tess_get_tuning(const vd_tess* t, vd_tuning* k) {
   k->huge_direct_max = t->huge_direct_max;
   k->huge_blocks_max = t->huge_blocks_max;
   k->huge_narrow_max = t->huge_narrow_max;
+  k->noop_run = t->noop_run;
   return VD_OK;
 }
 

@@ -24,9 +24,9 @@ struct ClipLaunchInfo {
 cudaError_t clip_fp64_info(ClipLaunchInfo* info);
 // count: the instrumented variant that maintains the algorithmic event counters
 cudaError_t launch_clip_fp64_fast(const TessDesc& T, const WorkList& W, int nblocks, bool count,
-                                  cudaStream_t s);
+                                  cudaStream_t s, bool noop = false);
 cudaError_t launch_clip_fp64_big(const TessDesc& T, const WorkList& W, void* scratch, int nwarps,
-                                 cudaStream_t s);
+                                 cudaStream_t s, bool noop = false);
 
 // huge tier (global memory, one thread block per cell): cells beyond the
 // large capacities
@@ -40,7 +40,7 @@ cudaError_t launch_clip_fp64_huge_batched(const TessDesc* descs, const uint32_t*
 // medium-capacity tier (FP64, shared memory) for cells that overflow the fast path
 cudaError_t clip_med_setup(ClipLaunchInfo* info);
 // count: the instrumented variant (event counters kept)
-cudaError_t launch_clip_med(const TessDesc& T, const WorkList& W, int nblocks, bool count, cudaStream_t s);
+cudaError_t launch_clip_med(const TessDesc& T, const WorkList& W, int nblocks, bool count, cudaStream_t s, bool noop = false);
 cudaError_t launch_clip_med_batched(const TessDesc* descs, const uint32_t* tess_off, int ntess,
                                     const WorkList& W, int nblocks, cudaStream_t s);
 
@@ -131,8 +131,9 @@ cudaError_t clip_mixed_info(ClipLaunchInfo* info);
 // finish are listed as overflowing, for the medium tier
 // minb: the register budget of 6, 7 or 8 blocks of four warps per SM
 cudaError_t clip_sparse_info(bool mixed, int minb, ClipLaunchInfo* info);
+// noop: the walk's variant with batched plane tests (TessDesc::noop_run)
 cudaError_t launch_clip_sparse(const TessDesc& T, const WorkList& W, int nblocks, bool count, bool mixed, int minb,
-                               cudaStream_t s);
+                               bool noop, cudaStream_t s);
 cudaError_t clip_sparse_batched_setup(bool mixed, int* blocks_per_sm);
 // device bytes a committed batch holds beyond its members' buffers
 size_t batch_scratch_bytes(int num_sms);

@@ -30,6 +30,9 @@ cudaError_t clip_fp64_info(ClipLaunchInfo* info) {
   e = cudaFuncSetAttribute(k_clip_fast<FastCfgCount, kFastWarpsPerBlock, kFp64MinBlocks>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemc);
   if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(k_clip_fast<FastCfg, kFastWarpsPerBlock, kFp64MinBlocks, true>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
   int nb = 0;
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_clip_fast<FastCfg, kFastWarpsPerBlock, kFp64MinBlocks>,
                                                     kFastWarpsPerBlock * 32, smem);
@@ -38,20 +41,25 @@ cudaError_t clip_fp64_info(ClipLaunchInfo* info) {
 }
 
 cudaError_t launch_clip_fp64_fast(const TessDesc& T, const WorkList& W, int nblocks, bool count,
-                                  cudaStream_t s) {
+                                  cudaStream_t s, bool noop) {
   const size_t smem = sizeof(WarpPoly<FastCfg>) * kFastWarpsPerBlock;
   const size_t smemc = sizeof(WarpPoly<FastCfgCount>) * kFastWarpsPerBlock;
   if (count)
     k_clip_fast<FastCfgCount, kFastWarpsPerBlock, kFp64MinBlocks><<<nblocks, kFastWarpsPerBlock * 32, smemc, s>>>(T, W);
+  else if (noop)
+    k_clip_fast<FastCfg, kFastWarpsPerBlock, kFp64MinBlocks, true><<<nblocks, kFastWarpsPerBlock * 32, smem, s>>>(T, W);
   else
     k_clip_fast<FastCfg, kFastWarpsPerBlock, kFp64MinBlocks><<<nblocks, kFastWarpsPerBlock * 32, smem, s>>>(T, W);
   return cudaGetLastError();
 }
 
 cudaError_t launch_clip_fp64_big(const TessDesc& T, const WorkList& W, void* scratch, int nwarps,
-                                 cudaStream_t s) {
+                                 cudaStream_t s, bool noop) {
   const int nblocks = nwarps / 4;  // the caller sizes scratch for whole blocks of 4 warps
-  k_clip_big<BigCfg><<<nblocks, 128, 0, s>>>(T, W, reinterpret_cast<WarpPoly<BigCfg>*>(scratch));
+  if (noop)
+    k_clip_big<BigCfg, true><<<nblocks, 128, 0, s>>>(T, W, reinterpret_cast<WarpPoly<BigCfg>*>(scratch));
+  else
+    k_clip_big<BigCfg><<<nblocks, 128, 0, s>>>(T, W, reinterpret_cast<WarpPoly<BigCfg>*>(scratch));
   return cudaGetLastError();
 }
 
@@ -140,6 +148,9 @@ cudaError_t clip_med_setup(ClipLaunchInfo* info) {
   e = cudaFuncSetAttribute(k_clip_fast<MedCfgNC, kMedWarpsPerBlock, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)smem);
   if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(k_clip_fast<MedCfgNC, kMedWarpsPerBlock, 1, true>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(k_clip_fast_batched<MedCfg, kMedWarpsPerBlock, 1>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
@@ -150,10 +161,13 @@ cudaError_t clip_med_setup(ClipLaunchInfo* info) {
   return e;
 }
 
-cudaError_t launch_clip_med(const TessDesc& T, const WorkList& W, int nblocks, bool count, cudaStream_t s) {
+cudaError_t launch_clip_med(const TessDesc& T, const WorkList& W, int nblocks, bool count, cudaStream_t s,
+                            bool noop) {
   const size_t smem = sizeof(WarpPoly<MedCfg>) * kMedWarpsPerBlock;
   if (count)
     k_clip_fast<MedCfg, kMedWarpsPerBlock, 1><<<nblocks, kMedWarpsPerBlock * 32, smem, s>>>(T, W);
+  else if (noop)
+    k_clip_fast<MedCfgNC, kMedWarpsPerBlock, 1, true><<<nblocks, kMedWarpsPerBlock * 32, smem, s>>>(T, W);
   else
     k_clip_fast<MedCfgNC, kMedWarpsPerBlock, 1><<<nblocks, kMedWarpsPerBlock * 32, smem, s>>>(T, W);
   return cudaGetLastError();

@@ -18,17 +18,17 @@ constexpr int kSparseBatchMinBlocks = 6;
 
 namespace {
 
-template <class C, int MINB>
+template <class C, int MINB, bool NOOP = false>
 cudaError_t setup_one(ClipLaunchInfo* info) {
   const size_t smem = sizeof(SparsePoly<C>) * kFastWarpsPerBlock;
-  cudaError_t e = cudaFuncSetAttribute(k_clip_sparse<C, kFastWarpsPerBlock, MINB>,
+  cudaError_t e = cudaFuncSetAttribute(k_clip_sparse<C, kFastWarpsPerBlock, MINB, NOOP>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess || !info) return e;
   info->smem_per_warp = sizeof(SparsePoly<C>);
   info->warps_per_block = kFastWarpsPerBlock;
   info->big_scratch_per_warp = 0;
   int nb = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_clip_sparse<C, kFastWarpsPerBlock, MINB>,
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_clip_sparse<C, kFastWarpsPerBlock, MINB, NOOP>,
                                                     kFastWarpsPerBlock * 32, smem);
   info->blocks_per_sm = nb;
   return e;
@@ -44,9 +44,9 @@ cudaError_t setup_batched(int* blocks_per_sm) {
       blocks_per_sm, k_clip_sparse_batched<C, kFastWarpsPerBlock, MINB>, kFastWarpsPerBlock * 32, smem);
 }
 
-template <class C, int MINB>
+template <class C, int MINB, bool NOOP = false>
 void launch_one(const TessDesc& T, const WorkList& W, int nblocks, cudaStream_t s) {
-  k_clip_sparse<C, kFastWarpsPerBlock, MINB>
+  k_clip_sparse<C, kFastWarpsPerBlock, MINB, NOOP>
       <<<nblocks, kFastWarpsPerBlock * 32, sizeof(SparsePoly<C>) * kFastWarpsPerBlock, s>>>(T, W);
 }
 
@@ -68,14 +68,23 @@ cudaError_t clip_sparse_info(bool mixed, int minb, ClipLaunchInfo* info) {
     if (minb == 7) return setup_one<MixedSparse, 7>(info);
     return setup_one<MixedSparse, 6>(info);
   }
-  if (minb == 5) return setup_one<FastSparse, 5>(info);
-  if (minb == 7) return setup_one<FastSparse, 7>(info);
-  return setup_one<FastSparse, 6>(info);
+  // (the walk's variant with batched plane tests has the same launch shape)
+  if (minb == 5) {
+    e = setup_one<FastSparse, 5, true>(nullptr);
+    return e != cudaSuccess ? e : setup_one<FastSparse, 5>(info);
+  }
+  if (minb == 7) {
+    e = setup_one<FastSparse, 7, true>(nullptr);
+    return e != cudaSuccess ? e : setup_one<FastSparse, 7>(info);
+  }
+  e = setup_one<FastSparse, 6, true>(nullptr);
+  return e != cudaSuccess ? e : setup_one<FastSparse, 6>(info);
 }
 
-// count: the instrumented variant (always at 6 blocks per SM)
+// count: the instrumented variant (always at 6 blocks per SM); noop: the
+// walk's variant with batched plane tests (plain FP64, uninstrumented)
 cudaError_t launch_clip_sparse(const TessDesc& T, const WorkList& W, int nblocks, bool count, bool mixed, int minb,
-                               cudaStream_t s) {
+                               bool noop, cudaStream_t s) {
   if (mixed) {
     if (count) launch_one<MixedSparseCount, 6>(T, W, nblocks, s);
     else if (minb == 5) launch_one<MixedSparse, 5>(T, W, nblocks, s);
@@ -83,6 +92,9 @@ cudaError_t launch_clip_sparse(const TessDesc& T, const WorkList& W, int nblocks
     else launch_one<MixedSparse, 6>(T, W, nblocks, s);
   } else {
     if (count) launch_one<FastSparseCount, 6>(T, W, nblocks, s);
+    else if (noop && minb == 5) launch_one<FastSparse, 5, true>(T, W, nblocks, s);
+    else if (noop && minb == 7) launch_one<FastSparse, 7, true>(T, W, nblocks, s);
+    else if (noop) launch_one<FastSparse, 6, true>(T, W, nblocks, s);
     else if (minb == 5) launch_one<FastSparse, 5>(T, W, nblocks, s);
     else if (minb == 7) launch_one<FastSparse, 7>(T, W, nblocks, s);
     else launch_one<FastSparse, 6>(T, W, nblocks, s);

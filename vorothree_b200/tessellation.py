@@ -540,12 +540,12 @@ class Tessellation:
     def set_tuning(self, tuning: dict):
         """Launch choices that change no result (the autotuner's): any of
         fast_layout ('slots' / 'full'), fast_blocks_per_sm (5, 6, 7),
-        huge_direct_max, huge_blocks_max, huge_narrow_max; keys left out keep
-        their current value."""
+        huge_direct_max, huge_blocks_max, huge_narrow_max, noop_run; keys left
+        out keep their current value."""
         cur = self.get_tuning()
         cur.update(tuning)
         k = Tuning(FAST_LAYOUTS[cur["fast_layout"]], int(cur["fast_blocks_per_sm"]), int(cur["huge_direct_max"]),
-                   int(cur["huge_blocks_max"]), int(cur["huge_narrow_max"]))
+                   int(cur["huge_blocks_max"]), int(cur["huge_narrow_max"]), int(cur["noop_run"]))
         self._ck(self._L.vd_tess_set_tuning(self._h, C.byref(k)))
 
     def get_tuning(self) -> dict:
@@ -554,7 +554,7 @@ class Tessellation:
         names = {v: n for n, v in FAST_LAYOUTS.items()}
         return {"fast_layout": names[k.fast_layout], "fast_blocks_per_sm": k.fast_blocks_per_sm,
                 "huge_direct_max": k.huge_direct_max, "huge_blocks_max": k.huge_blocks_max,
-                "huge_narrow_max": k.huge_narrow_max}
+                "huge_narrow_max": k.huge_narrow_max, "noop_run": k.noop_run}
 
     def set_fast_layout(self, layout: str):
         """'slots' (default: a clip rewrites only the faces it cuts) or 'full'
