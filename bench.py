@@ -468,7 +468,9 @@ def run_ours(args):
             "roofline": {"bound": "fp64", "kernel": "k_clip_sparse (warp-per-cell clip + reductions, slot layout)",
                          "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
                          "frac": achieved / peak.value,
-                         "peak_source": "FP64 FMA-chain microbenchmark run live by bench.py on this GPU",
+                         "peak_source": "FP64 FMA-chain microbenchmark run live by bench.py on this GPU, right "
+                                        "after the timed steps (MEASURED_PEAKS.json has no FP64 figure)",
+                         "peak_clock_mhz": clk.get("sm_mhz"),
                          "flops_per_launch": flops, "traffic": traffic,
                          "issue": issue_roof(args, clip, clk), "hbm": hbm_roof(clip),
                          "note": "bound names the kernel's only arithmetic roof (FP64 pipe, no tensor cores);"
