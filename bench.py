@@ -658,7 +658,7 @@ def burst_leg(args, nreq: int = 256) -> dict:
                                    precision=args.precision)
         if members:
             srv.set_merging(max_members=members)
-        for _ in range(2):  # warm the slots' buffers (and batches)
+        for _ in range(3):  # warm the slots' buffers and batches twice, measure the third pass
             srv.reset_stats()
             t0 = time.perf_counter()
             tickets = [srv.submit(*r) for r in reqs]
