@@ -533,3 +533,26 @@ def test_batched_plane_tests_bitwise(oracle_mod, kind, n):
         t.calculate()
         assert_same(t, o, check_counters=False)
         t.close()
+
+
+@pytest.mark.parametrize("m", [4, 5])
+def test_symmetric_hub_cell_bitwise(oracle_mod, m):
+    """A centre generator and one generator in every primitive lattice
+    direction (|coordinates| <= m) on a sphere: the centre's cell (578 faces at
+    m = 4, 1,154 at m = 5) reaches the block-per-cell tier, and the symmetric
+    directions make many planes meet at one point (the reference keeps a
+    vertex per plane triple there: 3,456 vertices at m = 4).  The slot layout
+    follows the reference's vertices there too; every cell equals the
+    oracle's bit for bit."""
+    import itertools
+    import math
+    dirs = [v for v in itertools.product(range(-m, m + 1), repeat=3)
+            if v != (0, 0, 0) and math.gcd(math.gcd(abs(v[0]), abs(v[1])), abs(v[2])) == 1]
+    d = np.asarray(dirs, np.float64)
+    d /= np.linalg.norm(d, axis=1)[:, None]
+    pts = np.vstack([[50.0, 50.0, 50.0], 50.0 + 30.0 * d])
+    g = int(np.ceil(len(pts) ** (1.0 / 3.0)))
+    gt = gpu_tess([0, 0, 0], [100, 100, 100], (g, g, g), pts)
+    o = oracle_tess(oracle_mod, [0, 0, 0], [100, 100, 100], (g, g, g), pts)
+    assert gt.summaries()[2][0] == len(pts) - 1
+    assert_same(gt, o, sample_cells=4)

@@ -50,7 +50,7 @@ _SAMPLE = 1 << 16
 # the first tier's choices the tuner searches, and the library's defaults
 LAYOUTS = ("slots", "full")
 BLOCKS_PER_SM = (5, 6, 7)
-DEFAULT_TUNING = {"fast_layout": "slots", "fast_blocks_per_sm": 6, "noop_run": -1}
+DEFAULT_TUNING = {"fast_layout": "slots", "fast_blocks_per_sm": 7, "noop_run": -1}
 # the block-per-cell tier's hand-off, searched once (HANDOFF_KEY)
 HANDOFF_KEY = "handoff"
 DIRECT_MAX = (1, 16, 64, 256)

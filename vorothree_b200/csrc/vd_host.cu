@@ -224,6 +224,10 @@ bool wall_from_desc(const vd_wall_desc& d, Wall* w, std::vector<double>* planes,
 // run it with 16-warp blocks (on the slot layout 16 warps win at every size
 // measured, 1,000 to 20,000 generators on a sphere), larger ones with 32
 constexpr int kHugeNarrowDefault = 1 << 30;
+// the slot layout's register budget: 7 blocks of four warps per SM (the
+// autotuner's choice for uniform input from 2^16 cells and clustered from
+// 2^18: 1 M uniform cells 32.5 ms against 33.5 at 6 and 33.7 at 5)
+constexpr int kFastMinbDefault = 7;
 // the walk's batched plane tests after a run of clips that change nothing
 // (-1: off)
 constexpr int kNoopRunDefault = -1;
@@ -321,7 +325,7 @@ struct vd_tess {
   ClipLaunchInfo info64{}, infomx{}, infomed{};
   ClipLaunchInfo infosp64[3]{}, infospmx[3]{};  // slot layout at 5, 6, 7 blocks per SM
   int fast_layout = VD_FAST_SLOTS;
-  int fast_minb = 6;
+  int fast_minb = kFastMinbDefault;
   int huge_direct_max = 64;
   int huge_blocks_max = 64;
   int huge_narrow_max = kHugeNarrowDefault;
@@ -1621,7 +1625,7 @@ int vd_tess_set_tuning(vd_tess* t, const vd_tuning* k) {
   if (k->huge_direct_max < 0 || k->huge_blocks_max < 0 || k->huge_blocks_max > 256 || k->huge_narrow_max < 0)
     return fail(t, VD_EINVAL, "huge-tier settings out of range");
   t->fast_layout = k->fast_layout;
-  t->fast_minb = k->fast_blocks_per_sm ? k->fast_blocks_per_sm : 6;
+  t->fast_minb = k->fast_blocks_per_sm ? k->fast_blocks_per_sm : kFastMinbDefault;
   t->huge_direct_max = k->huge_direct_max ? k->huge_direct_max : 64;
   t->huge_blocks_max = k->huge_blocks_max ? k->huge_blocks_max : kHugeBlocksMax;
   t->huge_narrow_max = k->huge_narrow_max ? k->huge_narrow_max : kHugeNarrowDefault;

@@ -11,9 +11,9 @@ namespace vd {
 
 // blocks of 4 warps per SM the register budget must admit (shared memory
 // admits this many too): single tessellations are compiled for 5, 6 and 7
-// (a tuning setting; 6 by default, measured fastest on 1 M uniform cells:
-// 40.8 ms against 44.4 at 7 and 45.6 at 8, where the tighter register budget
-// spills more; the instrumented variant for 6 only), batches for 6
+// (a tuning setting, 7 by default: 1 M uniform cells 32.5 ms against 33.5 at
+// 6 and 33.7 at 5; 8 spills more and was slower; the instrumented variant for
+// 6 only), batches for 6
 constexpr int kSparseBatchMinBlocks = 6;
 
 namespace {
