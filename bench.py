@@ -634,8 +634,10 @@ def serving_leg(args, nreq: int, rates) -> dict:
     reqs = serving_requests(nreq)
     srv = v.TessellationServer(slots=args.serve_slots, hbm_budget_bytes=args.serve_budget_gb << 30,
                                precision=args.precision)
-    for r in reqs[:4]:  # warm the slots' buffers
-        srv.take(srv.submit(*r))
+    # warm every slot's buffers on the whole request set (the sweep measures
+    # the steady state, not the first growth of a slot's buffers)
+    for t in [srv.submit(*r) for r in reqs]:
+        srv.take(t)
     sweep = [serve_at_rate(srv, reqs, rate) for rate in rates]
     srv.close()
     return {"config": {"slots": args.serve_slots, "hbm_budget_gb": args.serve_budget_gb, "requests": nreq,

@@ -143,7 +143,8 @@ int vd_tess_set_fast_layout(vd_tess* t, int layout);
  * field of 0 keeps the library's default. */
 typedef struct {
   int fast_layout;         /* VD_FAST_SLOTS (default) or VD_FAST_FULL */
-  int fast_blocks_per_sm;  /* slot layout: 5, 6 or 7 (default) blocks of four warps per SM (the register budget
+  int fast_blocks_per_sm;  /* slot layout: 5, 6 or 7 blocks of four warps per SM (default 7 for FP64, 6 for
+                              mixed precision; vd_tess_get_tuning reports the one in force) (the register budget
                               of the compiled variant; the shared-memory tier's polytopes always fit) */
   int huge_direct_max;     /* cells left after the medium tier, at most this many (default 64) go straight to
                               the block-per-cell tier instead of through the large tier */

@@ -224,10 +224,13 @@ bool wall_from_desc(const vd_wall_desc& d, Wall* w, std::vector<double>* planes,
 // run it with 16-warp blocks (on the slot layout 16 warps win at every size
 // measured, 1,000 to 20,000 generators on a sphere), larger ones with 32
 constexpr int kHugeNarrowDefault = 1 << 30;
-// the slot layout's register budget: 7 blocks of four warps per SM (the
-// autotuner's choice for uniform input from 2^16 cells and clustered from
-// 2^18: 1 M uniform cells 32.5 ms against 33.5 at 6 and 33.7 at 5)
+// the slot layout's register budget: 7 blocks of four warps per SM for FP64
+// (the autotuner's choice for uniform input from 2^16 cells and clustered
+// from 2^18: 1 M uniform cells 32.5 ms against 33.5 at 6 and 33.7 at 5), 6
+// for the mixed path (whose FP32 copies spill more at 7: 0.80 against 0.86 of
+// FP64 on 1 M uniform cells)
 constexpr int kFastMinbDefault = 7;
+constexpr int kFastMinbDefaultMixed = 6;
 // the walk's batched plane tests after a run of clips that change nothing
 // (-1: off)
 constexpr int kNoopRunDefault = -1;
@@ -325,7 +328,7 @@ struct vd_tess {
   ClipLaunchInfo info64{}, infomx{}, infomed{};
   ClipLaunchInfo infosp64[3]{}, infospmx[3]{};  // slot layout at 5, 6, 7 blocks per SM
   int fast_layout = VD_FAST_SLOTS;
-  int fast_minb = kFastMinbDefault;
+  int fast_minb = 0;  // 0: the precision's default (fast_minb_for)
   int huge_direct_max = 64;
   int huge_blocks_max = 64;
   int huge_narrow_max = kHugeNarrowDefault;
@@ -624,6 +627,13 @@ int ensure_huge(vd_tess* t, size_t cells) {
   return VD_OK;
 }
 
+// the slot layout's blocks per SM in force: the tuning setting, else the
+// precision's default
+int fast_minb_for(const vd_tess* t) {
+  if (t->fast_minb) return t->fast_minb;
+  return t->precision == VD_PREC_MIXED ? kFastMinbDefaultMixed : kFastMinbDefault;
+}
+
 // one pass of the clip kernel over `items` (nullptr = all cells in bin order);
 // tier 0 = first tier (shared memory, the handle's layout), -1 = first tier on
 // the full-rewrite layout (the slot layout's hand-offs), 1 = medium capacity,
@@ -659,14 +669,15 @@ int clip_pass(vd_tess* t, int tier, const uint32_t* items, uint32_t nitems, uint
     // the slot layout cannot export a polytope in the reference's vertex
     // order: get_cell's rebuild runs the full-rewrite kernel
     const bool slots = tier == 0 && t->fast_layout == VD_FAST_SLOTS && !W.ex_verts;
-    const int mv = t->fast_minb - 5;
+    const int minb = fast_minb_for(t);
+    const int mv = minb - 5;
     const ClipLaunchInfo& li =
         slots ? (mixed ? t->infospmx[mv] : t->infosp64[mv]) : (mixed ? t->infomx : t->info64);
     const size_t warps_needed = (nitems + li.warps_per_block - 1) / li.warps_per_block;
     const int nblocks = (int)std::max<size_t>(
         1, std::min<size_t>(warps_needed, (size_t)t->num_sms * std::max(1, li.blocks_per_sm)));
     if (slots)
-      VD_CK(t, launch_clip_sparse(T, W, nblocks, t->instrument, mixed, t->fast_minb, t->noop_run > 0, s));
+      VD_CK(t, launch_clip_sparse(T, W, nblocks, t->instrument, mixed, minb, t->noop_run > 0, s));
     else
       VD_CK(t, mixed ? launch_clip_mixed_fast(T, W, nblocks, t->instrument, s)
                      : launch_clip_fp64_fast(T, W, nblocks, t->instrument, s, t->noop_run > 0));
@@ -1625,7 +1636,7 @@ int vd_tess_set_tuning(vd_tess* t, const vd_tuning* k) {
   if (k->huge_direct_max < 0 || k->huge_blocks_max < 0 || k->huge_blocks_max > 256 || k->huge_narrow_max < 0)
     return fail(t, VD_EINVAL, "huge-tier settings out of range");
   t->fast_layout = k->fast_layout;
-  t->fast_minb = k->fast_blocks_per_sm ? k->fast_blocks_per_sm : kFastMinbDefault;
+  t->fast_minb = k->fast_blocks_per_sm;
   t->huge_direct_max = k->huge_direct_max ? k->huge_direct_max : 64;
   t->huge_blocks_max = k->huge_blocks_max ? k->huge_blocks_max : kHugeBlocksMax;
   t->huge_narrow_max = k->huge_narrow_max ? k->huge_narrow_max : kHugeNarrowDefault;
@@ -1636,7 +1647,7 @@ int vd_tess_set_tuning(vd_tess* t, const vd_tuning* k) {
 int vd_tess_get_tuning(const vd_tess* t, vd_tuning* k) {
   if (!t || !k) return VD_EINVAL;
   k->fast_layout = t->fast_layout;
-  k->fast_blocks_per_sm = t->fast_minb;
+  k->fast_blocks_per_sm = fast_minb_for(t);
   k->huge_direct_max = t->huge_direct_max;
   k->huge_blocks_max = t->huge_blocks_max;
   k->huge_narrow_max = t->huge_narrow_max;
