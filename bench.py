@@ -287,7 +287,7 @@ def issue_roof(args, clip_ms: float, clk: dict):
     achieved = per_cell * N_GEN / (clip_ms / 1e3) / 1e9
     peak = sms * 4 * mhz * 1e6 / 1e9
     return {"achieved": achieved, "peak": peak, "unit": "G warp-instructions/s", "frac": achieved / peak,
-            "note": "instruction issue, the roof this kernel meets (ncu: issue active ~77%); "
+            "note": "instruction issue, the roof this kernel meets (ncu: issue active ~80%); "
                     "warp instructions per cell from the committed ncu profile"}
 
 
