@@ -556,3 +556,27 @@ def test_symmetric_hub_cell_bitwise(oracle_mod, m):
     o = oracle_tess(oracle_mod, [0, 0, 0], [100, 100, 100], (g, g, g), pts)
     assert gt.summaries()[2][0] == len(pts) - 1
     assert_same(gt, o, sample_cells=4)
+
+
+def test_hub_cell_with_walls_and_batched_plane_tests(oracle_mod):
+    """The centre of generators on a sphere (a cell the block-per-cell tier
+    builds on the slot layout) with a plane wall and a sphere wall clipping it
+    first, and the same input with the walk's batched plane tests on: every
+    cell equals the oracle's, bit for bit."""
+    import vorothree_b200 as v
+    from common import bench_distribution
+    pts = bench_distribution("sphere", 2500, 77)
+    walls = [v.Wall(WALL, v.PlaneGeometry([50.0, 50.0, 58.0], [-0.1, -0.2, -1.0])),
+             v.Wall(WALL - 1, v.SphereGeometry([50.0, 50.0, 50.0], 40.0))]
+    g = int(np.ceil(len(pts) ** (1.0 / 3.0)))
+    o = oracle_tess(oracle_mod, [0, 0, 0], [100, 100, 100], (g, g, g), pts, walls)
+    for run in (-1, 4):
+        t = v.Tessellation(v.BoundingBox([0, 0, 0], [100, 100, 100]), v.Algorithm3DGrid(g, g, g))
+        t.set_tuning({"noop_run": run})
+        t.set_generators(pts)
+        for w in walls:
+            t.add_wall(w)
+        t.calculate()
+        assert t.summaries()[2][0] > 500
+        assert_same(t, o, check_counters=False)
+        t.close()
