@@ -737,7 +737,8 @@ constexpr int kHugeBlockWarps = 32;
 // one-warp rewrite and its barriers, not the classification's passes, set the
 // time, and 16 warps win at every size measured (the centre of 3,000 /
 // 10,000 / 20,000 generators on a sphere: 30.4 / 147.6 / 435 ms against 38.1 /
-// 163.8 / 450 ms with 32)
+// 163.8 / 450 ms with 32, and 35.1 / 204 / 655 ms with 8, too few warps for
+// the classification's pass)
 constexpr int kHugeBlockWarpsNarrow = 16;
 
 }  // namespace vd
